@@ -1,0 +1,488 @@
+"""Python face of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+``OracleSR`` exposes the subset of the reference ``oscars.sr`` API that the radiation hot path uses,
+with the same keyword names, defaults, return shapes and error behaviour, on top of the C
+restatement in ``oscars_oracle.c``.  Tests drive the reference build (``oracle/_ref``), this oracle
+and the oscars_b200 product with the same calls and compare the results.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module; the
+product never does.
+
+Front-end logic restated here (reference file:line):
+  * rectangle surfaces: TSurfacePoints_Rectangle::Init/GetXYZ/GetX1/GetX2
+    (src/TSurfacePoints_Rectangle.cc:140-315)
+  * RotateSelfXYZ (src/TVector3D.cc RotateSelfX/Y/Z)
+  * spectrum energies: TSpectrumContainer::Init (src/TSpectrumContainer.cc:57-92)
+  * polarization strings: src/OSCARSSR.cc:4129-4150 and the binding defaults
+    (src/OSCARSSR_Python.cc:5889-5899)
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import sys
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboscars_oracle.so")
+_ANGLE_UNSET = 112188979912321.0
+_PARTICLE_TYPES = {
+    "electron": 0, "anti-positron": 0, "positron": 1, "anti-electron": 1, "muon": 2,
+    "anti-muon": 3, "proton": 4, "anti-proton": 5, "pi+": 6, "pi-": 7, "custom": 8,
+}
+
+_lib = None
+
+
+def load():
+    """Load (building if needed) the oracle shared library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        import subprocess
+        subprocess.check_call(["make", "-s", "-C", _HERE, "oracle"])
+    lib = ctypes.CDLL(_LIB_PATH)
+    D = ctypes.c_double
+    P = ctypes.POINTER
+    dp = P(D)
+    ip = P(ctypes.c_int)
+    lib.orc_new.restype = ctypes.c_void_p
+    lib.orc_free.argtypes = [ctypes.c_void_p]
+    lib.orc_last_error.restype = ctypes.c_char_p
+    lib.orc_last_error.argtypes = [ctypes.c_void_p]
+    lib.orc_clear_fields.argtypes = [ctypes.c_void_p]
+    lib.orc_add_undulator.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_int, dp, D, D, D, D, D]
+    lib.orc_add_epu.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_int, dp, D, D, D, D, D]
+    lib.orc_get_bfield.argtypes = [ctypes.c_void_p, dp, D, dp]
+    lib.orc_set_beam.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D, D, dp, dp, D, D, dp,
+                                 ctypes.c_int, D, dp, ctypes.c_int, dp, dp, ctypes.c_int,
+                                 ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int]
+    lib.orc_set_ctstartstop.argtypes = [ctypes.c_void_p, D, D]
+    lib.orc_set_npoints_trajectory.argtypes = [ctypes.c_void_p, ctypes.c_long]
+    lib.orc_get_npoints_trajectory.argtypes = [ctypes.c_void_p]
+    lib.orc_get_npoints_trajectory.restype = ctypes.c_long
+    lib.orc_set_seed.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.orc_uniform.argtypes = [ctypes.c_void_p]
+    lib.orc_uniform.restype = D
+    lib.orc_normal.argtypes = [ctypes.c_void_p]
+    lib.orc_normal.restype = D
+    lib.orc_set_new_particle.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.orc_get_particle.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp]
+    lib.orc_calculate_trajectory.argtypes = [ctypes.c_void_p]
+    lib.orc_trajectory_npoints.argtypes = [ctypes.c_void_p]
+    lib.orc_trajectory_npoints.restype = ctypes.c_long
+    lib.orc_get_trajectory.argtypes = [ctypes.c_void_p, dp, ctypes.c_long]
+    lib.orc_get_spline_ypp.argtypes = [ctypes.c_void_p, dp, ctypes.c_long]
+    lib.orc_get_level.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, ctypes.c_long]
+    lib.orc_flux.argtypes = [ctypes.c_void_p, dp, ctypes.c_long, D, ctypes.c_int, D, dp, dp, D,
+                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ip]
+    lib.orc_spectrum.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_long, ctypes.c_int, D, dp, dp,
+                                 D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ip]
+    lib.orc_power_density.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_long, ctypes.c_int, D,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ip]
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _v3(x, name="vector"):
+    if x is None:
+        return None
+    x = list(x)
+    if len(x) != 3:
+        raise ValueError("Incorrect format in '%s'" % name)
+    return [float(v) for v in x]
+
+
+# ---- vector helpers restating src/TVector3D.cc (pure Python floats are IEEE doubles) ----------
+def rotate_xyz(v, r):
+    """TVector3D::RotateSelfXYZ: about X, then Y, then Z."""
+    x, y, z = v
+    s, c = math.sin(r[0]), math.cos(r[0])
+    yy = y
+    y = c * yy - s * z
+    z = s * yy + c * z
+    s, c = math.sin(r[1]), math.cos(r[1])
+    zz = z
+    z = c * zz - s * x
+    x = s * zz + c * x
+    s, c = math.sin(r[2]), math.cos(r[2])
+    xx = x
+    x = c * xx - s * y
+    y = s * xx + c * y
+    return [x, y, z]
+
+
+def _mag(v):
+    return math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+
+
+def rectangle(plane, nx1, nx2, w1, w2, rotations, translation, normal):
+    """TSurfacePoints_Rectangle::Init(plane, ...) + GetXYZ/GetX1/GetX2.  Returns (xyz, normals,
+    x1x2) arrays in point order i = ix1*NX2 + ix2."""
+    P = plane.upper()
+    s1 = w1 / (nx1 - 1) if nx1 > 1 else 0
+    s2 = w2 / (nx2 - 1) if nx2 > 1 else 0
+
+    def start(a, b, c):
+        return [a, b, c]
+    table = {
+        "XY": ((-w1 / 2., -w2 / 2., 0), (0, 0, 0), (0., -w2 / 2., 0), (-w1 / 2., 0, 0), (s1, 0, 0), (0, s2, 0), (0, 0, 1)),
+        "YX": ((-w2 / 2., -w1 / 2., 0), (0, 0, 0), (-w2 / 2., 0, 0), (0, -w1 / 2., 0), (0, s1, 0), (s2, 0, 0), (0, 0, -1)),
+        "XZ": ((-w1 / 2., 0, -w2 / 2.), (0, 0, 0), (0, 0, -w2 / 2.), (-w1 / 2., 0, 0), (s1, 0, 0), (0, 0, s2), (0, -1, 0)),
+        "ZX": ((-w2 / 2., 0, -w1 / 2.), (0, 0, 0), (-w2 / 2., 0, 0), (0., 0, -w1 / 2.), (0, 0, s1), (s2, 0, 0), (0, 1, 0)),
+        "YZ": ((0, -w1 / 2., -w2 / 2.), (0, 0, 0), (0, 0, -w2 / 2.), (0, -w1 / 2., 0), (0, s1, 0), (0, 0, s2), (1, 0, 0)),
+        "ZY": ((0, -w2 / 2., -w1 / 2.), (0, 0, 0), (0, -w2 / 2., 0), (0, 0, -w1 / 2.), (0, 0, s1), (0, s2, 0), (-1, 0, 0)),
+    }
+    if P not in table:
+        raise ValueError("not a valid surface string: XY YX XZ ZX YZ ZY")
+    both, none, only2, only1, v1, v2, nv = table[P]
+    if nx1 > 1 and nx2 > 1:
+        st = list(both)
+    elif nx1 <= 1 and nx2 <= 1:
+        st = list(none)
+    elif nx1 <= 1:
+        st = list(only2)
+    else:
+        st = list(only1)
+    st = [float(a) for a in st]
+    v1 = [float(a) for a in v1]
+    v2 = [float(a) for a in v2]
+    nv = [float(a) for a in nv]
+    st = rotate_xyz(st, rotations)
+    v1 = rotate_xyz(v1, rotations)
+    v2 = rotate_xyz(v2, rotations)
+    st = [st[0] + translation[0], st[1] + translation[1], st[2] + translation[2]]
+    nv = rotate_xyz(nv, rotations)
+    if normal == -1:
+        nv = [nv[0] * -1, nv[1] * -1, nv[2] * -1]
+    elif normal not in (0, 1):
+        raise ValueError("normal must be -1, 0, or 1")
+    n = nx1 * nx2
+    xyz = np.empty((n, 3))
+    x1x2 = np.zeros((n, 3))
+    m1, m2 = _mag(v1), _mag(v2)
+    for i in range(n):
+        ix1 = i // nx2
+        ix2 = i % nx2
+        a = [st[k] + ix1 * v1[k] for k in range(3)]
+        xyz[i] = [a[k] + ix2 * v2[k] for k in range(3)]
+        x1x2[i, 0] = s1 * ix1 - m1 * (nx1 - 1) / 2.
+        x1x2[i, 1] = s2 * ix2 - m2 * (nx2 - 1) / 2.
+    normals = np.tile(np.array(nv), (n, 1))
+    return xyz, normals, x1x2
+
+
+def polarization_code(polarization, angle):
+    """Binding default (src/OSCARSSR_Python.cc:5889-5899) + string match (src/OSCARSSR.cc:4129-4150)."""
+    if polarization == "all" and angle != _ANGLE_UNSET:
+        raise ValueError("cannot specify 'all' and 'angle'.  This is to save you")
+    pol = "all"
+    if len(polarization) != 0:
+        pol = polarization
+    elif angle != _ANGLE_UNSET:
+        pol = "linear"
+    p = pol.lower().replace(" ", "-")
+    if "all" in p:
+        return 0
+    if "linear-horizontal" in p or "lh" in p:
+        return 1
+    if "linear-vertical" in p or "lv" in p:
+        return 2
+    if p == "linear":
+        return 3
+    if "circular-left" in p or "cl" in p:
+        return 4
+    if "circular-right" in p or "cr" in p:
+        return 5
+    raise ValueError("Polarization requested not recognized")
+
+
+def spectrum_energies(npoints, energy_range_eV, energy_points_eV):
+    if energy_points_eV is not None:
+        if len(energy_points_eV) == 0:
+            raise ValueError("Number of points to calculate is zero.  Check input.")
+        return np.array([float(e) for e in energy_points_eV])
+    e0, e1 = 0.0, 0.0
+    if energy_range_eV is not None:
+        if len(energy_range_eV) != 2:
+            raise ValueError("'energy_range_eV' must be a list of length 2")
+        e0, e1 = float(energy_range_eV[0]), float(energy_range_eV[1])
+    if npoints < 1:
+        npoints = abs(int(e1 - e0) + 1) if abs(e1 - e0) + 1 > 100 else 100
+    if npoints == 1:
+        return np.array([e0])
+    return np.array([e0 + (e1 - e0) / (npoints - 1) * float(i) for i in range(npoints)])
+
+
+def _quantity(q, pd=False):
+    Q = q.upper()
+    if pd and Q in ("POWER DENSITY", "POWERDENSITY"):
+        return 0
+    if not pd and Q == "FLUX":
+        return 0
+    if Q == "PRECISION":
+        return 1
+    if Q == "LEVEL":
+        return 2
+    raise ValueError("'quantity' must be: 'flux', 'precision', 'level', or blank")
+
+
+class OracleSR:
+    """CPU oracle with the ``oscars.sr.sr`` method names used on the radiation hot path."""
+
+    def __init__(self, nthreads=0, gpu=0):
+        self._lib = load()
+        self._h = ctypes.c_void_p(self._lib.orc_new())
+        self.last_levels = None
+
+    def __del__(self):
+        try:
+            self._lib.orc_free(self._h)
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise ValueError(self._lib.orc_last_error(self._h).decode())
+
+    # ---- setup ------------------------------------------------------------------------------
+    def set_seed(self, seed):
+        self._lib.orc_set_seed(self._h, int(float(seed)))
+
+    def clear_bfields(self):
+        self._lib.orc_clear_fields(self._h)
+
+    def add_bfield_undulator(self, bfield, period, nperiods, phase=0, rotations=[], translation=[],
+                             taper=0, frequency=0, frequency_phase=0, time_offset=0, name=""):
+        f = _v3(bfield, "bfield")
+        p = _v3(period, "period")
+        r = _v3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        t = _v3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
+        f = rotate_xyz(f, r)
+        p = rotate_xyz(p, r)
+        a = lambda v: np.array(v, dtype=np.float64)
+        F, Pp, T = a(f), a(p), a(t)
+        self._check(self._lib.orc_add_undulator(self._h, _dp(F), _dp(Pp), int(nperiods), _dp(T),
+                                                float(phase), float(taper), float(frequency),
+                                                float(frequency_phase), float(time_offset)))
+
+    def add_bfield_epu(self, period, nperiods, bfieldA=[], bfieldB=[], phase=0, rotations=[],
+                       translation=[], taper=0, frequency=0, frequency_phase=0, time_offset=0, name=""):
+        if len(bfieldA) == 0 and len(bfieldB) == 0:
+            raise ValueError("Must define at least one of 'bfieldA', 'bfieldB'")
+        r = _v3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        t = _v3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
+        fa = rotate_xyz(_v3(bfieldA, "bfieldA") if len(bfieldA) else [0.0, 0.0, 0.0], r)
+        fb = rotate_xyz(_v3(bfieldB, "bfieldB") if len(bfieldB) else [0.0, 0.0, 0.0], r)
+        p = rotate_xyz(_v3(period, "period"), r)
+        a = lambda v: np.array(v, dtype=np.float64)
+        A, B, Pp, T = a(fa), a(fb), a(p), a(t)
+        self._check(self._lib.orc_add_epu(self._h, _dp(A), _dp(B), _dp(Pp), int(nperiods), _dp(T),
+                                          float(phase), float(taper), float(frequency),
+                                          float(frequency_phase), float(time_offset)))
+
+    def get_bfield(self, x, t=0):
+        X = np.array(_v3(x), dtype=np.float64)
+        out = np.zeros(3)
+        self._lib.orc_get_bfield(self._h, _dp(X), float(t), _dp(out))
+        return list(out)
+
+    def set_particle_beam(self, type="electron", name="", energy_GeV=-1, d0=None, x0=None, beam="",
+                          sigma_energy_GeV=0, t0=0, current=0, weight=1, rotations=None,
+                          translation=None, horizontal_direction=None, beta=None, alpha=None,
+                          gamma=None, emittance=None, eta=None, lattice_reference=None, mass=0,
+                          charge=0, ctstartstop=None, distribution=""):
+        if beam:
+            raise ValueError("predefined beams are not part of the oracle")
+        if type not in _PARTICLE_TYPES:
+            raise ValueError("invalid argument in adding particle beam.  possibly 'name' already exists")
+        d = _v3(d0, "d0") if d0 is not None else [0.0, 0.0, 1.0]
+        x = _v3(x0, "x0") if x0 is not None else [0.0, 0.0, 0.0]
+        r = _v3(rotations, "rotations") if rotations is not None else [0.0, 0.0, 0.0]
+        tr = _v3(translation, "translation") if translation is not None else [0.0, 0.0, 0.0]
+        if horizontal_direction is not None:
+            hd = _v3(horizontal_direction, "horizontal_direction")
+        else:  # -Direction.Orthogonal() of the un-rotated direction (Python.cc:3912-3915)
+            ax, ay, az = [abs(v) if v < 0 else v for v in d]
+            if ax < ay:
+                o = [0.0, d[2], -d[1]] if ax < az else [d[1], -d[0], 0.0]
+            else:
+                o = [-d[2], 0.0, d[0]] if ay < az else [d[1], -d[0], 0.0]
+            hd = [-o[0], -o[1], -o[2]]
+        x = rotate_xyz(x, r)
+        d = rotate_xyz(d, r)
+        x = [x[0] + tr[0], x[1] + tr[1], x[2] + tr[2]]
+        a = lambda v: np.array(v, dtype=np.float64)
+        X, Dd, H = a(x), a(d), a(hd)
+        em = a(emittance if emittance is not None else [0, 0])
+        bt = a(beta if beta is not None else [0, 0])
+        al = a(alpha if alpha is not None else [0, 0])
+        et = a(eta if eta is not None else [0, 0])
+        cs = a(ctstartstop if ctstartstop is not None else [0, 0])
+        dist = {"": -1, "filament": 1, "gaussian": 2, "kv": 3}[distribution.lower()]
+        self._check(self._lib.orc_set_beam(
+            self._h, _PARTICLE_TYPES[type], float(charge), float(mass), float(energy_GeV), _dp(X),
+            _dp(Dd), float(t0), float(current), _dp(H), 1, float(sigma_energy_GeV), _dp(em),
+            int(emittance is not None), _dp(bt), _dp(al), int(beta is not None),
+            int(alpha is not None), _dp(et), dist, _dp(cs), int(ctstartstop is not None)))
+
+    def set_ctstartstop(self, start, stop):
+        self._lib.orc_set_ctstartstop(self._h, float(start), float(stop))
+
+    def set_npoints_trajectory(self, n):
+        self._lib.orc_set_npoints_trajectory(self._h, int(n))
+
+    def get_npoints_trajectory(self):
+        return self._lib.orc_get_npoints_trajectory(self._h)
+
+    def set_new_particle(self, beam="", particle=""):
+        self._check(self._lib.orc_set_new_particle(self._h, int(particle == "ideal")))
+
+    def get_particle(self):
+        vals = [np.zeros(3), np.zeros(3)] + [np.zeros(1) for _ in range(5)]
+        self._lib.orc_get_particle(self._h, *[_dp(v) for v in vals])
+        return vals
+
+    def uniform(self):
+        return self._lib.orc_uniform(self._h)
+
+    def normal(self):
+        return self._lib.orc_normal(self._h)
+
+    # ---- trajectory -------------------------------------------------------------------------
+    def calculate_trajectory(self, ofile="", bofile="", oformat=""):
+        self._check(self._lib.orc_calculate_trajectory(self._h))
+        return self.get_trajectory()
+
+    def trajectory_array(self):
+        """(10, n) SoA: t, x, y, z, bx, by, bz, ax, ay, az."""
+        n = self._lib.orc_trajectory_npoints(self._h)
+        out = np.zeros(10 * n)
+        self._lib.orc_get_trajectory(self._h, _dp(out), out.size)
+        return out.reshape(10, n)
+
+    def spline_ypp(self):
+        n = self._lib.orc_trajectory_npoints(self._h)
+        out = np.zeros(9 * n)
+        self._lib.orc_get_spline_ypp(self._h, _dp(out), out.size)
+        return out.reshape(9, n)
+
+    def level_samples(self, level):
+        out = np.zeros(10 * (1 << level))
+        self._check(self._lib.orc_get_level(self._h, int(level), _dp(out), out.size))
+        return out.reshape(10, 1 << level)
+
+    def get_trajectory(self):
+        a = self.trajectory_array()
+        return [[a[0, i], list(a[1:4, i]), list(a[4:7, i]), list(a[7:10, i])] for i in range(a.shape[1])]
+
+    # ---- radiation --------------------------------------------------------------------------
+    def _pol_args(self, polarization, angle, horizontal_direction, propogation_direction):
+        code = polarization_code(polarization, angle)
+        h = np.array(_v3(horizontal_direction) if horizontal_direction else [1.0, 0.0, 0.0])
+        p = np.array(_v3(propogation_direction) if propogation_direction else [0.0, 0.0, 1.0])
+        return code, float(angle), h, p
+
+    def calculate_spectrum(self, obs, npoints=0, energy_range_eV=None, energy_points_eV=None,
+                           points_eV=None, polarization="", angle=_ANGLE_UNSET,
+                           horizontal_direction=None, propogation_direction=None, precision=0.01,
+                           max_level=-2, max_level_extended=0, nparticles=0, nthreads=0, gpu=-1,
+                           ngpu=None, quantity="flux", ofile="", bofile=""):
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        if points_eV is not None:
+            energy_points_eV = points_eV
+        E = spectrum_energies(npoints, energy_range_eV, energy_points_eV)
+        O = np.array(_v3(obs, "obs"))
+        q = _quantity(quantity)
+        code, ang, h, p = self._pol_args(polarization, angle, horizontal_direction, propogation_direction)
+        out = np.zeros(E.size)
+        lv = np.zeros(E.size, dtype=np.int32)
+        self._check(self._lib.orc_spectrum(self._h, _dp(O), _dp(E), E.size, code, ang, _dp(h), _dp(p),
+                                           float(precision), int(max_level), int(max_level_extended),
+                                           int(nparticles), q, _dp(out),
+                                           lv.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.last_levels = lv
+        return [[float(E[i]), float(out[i])] for i in range(E.size)]
+
+    def _surface(self, npoints, plane, width, x0x1x2, rotations, translation, normal, pd):
+        if len(npoints) != 2:
+            raise ValueError("'npoints' must be [int, int]")
+        nx1, nx2 = int(npoints[0]), int(npoints[1])
+        if nx1 <= 0 or nx2 <= 0:
+            raise ValueError("an entry in 'npoints' is <= 0")
+        r = _v3(rotations) if rotations else [0.0, 0.0, 0.0]
+        t = _v3(translation) if translation else [0.0, 0.0, 0.0]
+        w1, w2 = (0.010, 0.010) if pd else (0.0, 0.0)
+        if width is not None and len(width) == 2:
+            w1, w2 = float(width[0]), float(width[1])
+        if abs(normal) > 1:
+            raise ValueError("'normal' must be -1, 0, or 1")
+        if x0x1x2 is not None:
+            raise ValueError("x0x1x2 surfaces are not part of the oracle")
+        if pd and (w1 <= 0 or w2 <= 0):
+            raise ValueError("'width' must be > 0")
+        return rectangle(plane, nx1, nx2, w1, w2, r, t, normal)
+
+    def calculate_flux_rectangle(self, energy_eV, npoints=[51, 51], plane="XY", normal=0, dim=2,
+                                 width=None, rotations=None, translation=None, x0x1x2=None,
+                                 polarization="", angle=_ANGLE_UNSET, horizontal_direction=None,
+                                 propogation_direction=None, nparticles=0, nthreads=0, gpu=-1,
+                                 ngpu=None, precision=0.01, max_level=-2, max_level_extended=0,
+                                 quantity="flux", ofile="", bofile=""):
+        if dim not in (2, 3):
+            raise ValueError("'dim' must be 2 or 3")
+        xyz, normals, x1x2 = self._surface(npoints, plane, width, x0x1x2, rotations, translation, normal, False)
+        q = _quantity(quantity)
+        code, ang, h, p = self._pol_args(polarization, angle, horizontal_direction, propogation_direction)
+        n = xyz.shape[0]
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        X = np.ascontiguousarray(xyz)
+        self._check(self._lib.orc_flux(self._h, _dp(X), n, float(energy_eV), code, ang, _dp(h), _dp(p),
+                                       float(precision), int(max_level), int(max_level_extended),
+                                       int(nparticles), q, _dp(out),
+                                       lv.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.last_levels = lv
+        pos = xyz if dim == 3 else x1x2
+        return [[list(pos[i]), float(out[i])] for i in range(n)]
+
+    def calculate_power_density_rectangle(self, npoints=[51, 51], plane="XY", width=None,
+                                          x0x1x2=None, rotations=None, translation=None, ofile="",
+                                          bofile="", normal=0, nparticles=0, gpu=-1, ngpu=None,
+                                          nthreads=0, precision=0.01, max_level=-2,
+                                          max_level_extended=0, dim=2, quantity="power density"):
+        if dim not in (2, 3):
+            raise ValueError("'dim' must be 2 or 3")
+        xyz, normals, x1x2 = self._surface(npoints, plane, width, x0x1x2, rotations, translation, normal, True)
+        q = _quantity(quantity, pd=True)
+        n = xyz.shape[0]
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        X = np.ascontiguousarray(xyz)
+        Nn = np.ascontiguousarray(normals)
+        self._check(self._lib.orc_power_density(self._h, _dp(X), _dp(Nn), n, int(normal != 0),
+                                                float(precision), int(max_level),
+                                                int(max_level_extended), int(nparticles), q,
+                                                _dp(out), lv.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.last_levels = lv
+        pos = xyz if dim == 3 else x1x2
+        return [[list(pos[i]), float(out[i])] for i in range(n)]
+
+
+def reference_module():
+    """Import the reference's own CPU build from oracle/_ref when it exists (None otherwise)."""
+    ref = os.path.join(_HERE, "_ref")
+    if not os.path.isdir(os.path.join(ref, "oscars")):
+        return None
+    if ref not in sys.path:
+        sys.path.insert(0, ref)
+    import importlib
+    return importlib.import_module("oscars.sr")
