@@ -1,0 +1,334 @@
+"""Benchmark of the OSCARS radiation hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference] [--compute fp64|mixed]
+
+Workload (one "step"): single-electron flux on a 201 x 201 XY rectangle, 10 mm x 10 mm at z = 30 m,
+at the first harmonic E1 = 458.9458 eV of a 41-period planar undulator (B0 = 0.5 T, 50 mm period),
+3 GeV electron, 20001-point FP64 RK4 trajectory, adaptive level ladder (precision 0.01).  Inputs
+are seeded synthetic stand-ins for the reference's example workloads.  Metric: Gsamples/s, one
+sample = one (observer, energy, trajectory point) term of the radiation sum, counted as
+2^(L+1)-1 per entry for stop level L.
+
+``value``  flux integral with trajectory and observers resident in HBM (level samples rebuilt
+           every step); CUDA events per step on the launching stream, L2 flushed between steps.
+``e2e``    the same job through the C ABI with host buffers: host RK4 + spline, host->device
+           copies, kernels, device->host copy of the results, every step.
+Under torchrun each rank runs its own job (energy E1 * (1 + 1e-3 rank)): no collective on the data
+path, weak scaling; the reported time is the max over ranks.
+
+``--impl reference`` times the reference's own CPU implementation (oracle/_ref, built from the
+reference sources by oracle/Makefile; the CPU restatement in oracle/ when that build is absent)
+on all host cores, on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("flux-integral Gsamples/s (obs×E×traj), mixed vs FP64 GPU at ≤1e-4 rel; grad/s")
+E1 = 458.9458
+GRID = 201
+WORKLOAD = ("flux 201x201 XY rectangle 10mm x 10mm at z=30m, E=E1=458.9458 eV; planar undulator "
+            "B0=0.5T lambda=50mm 41 periods; 3 GeV electron; 20001-point RK4; adaptive levels (precision 0.01)")
+FLOP_PER_SAMPLE = 83  # algorithmic work per sample of the frequency-domain integrand
+
+
+def setup(o):
+    o.add_bfield_undulator(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, phase=-math.pi / 2)
+    o.set_particle_beam(type="electron", energy_GeV=3, x0=[0, 0, 0], d0=[0, 0, 1], current=0.5)
+    o.set_ctstartstop(-1.5, 1.5)
+    o.set_npoints_trajectory(20001)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        if not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = [r for r in csv.reader(io.StringIO(self.out)) if len(r) >= 9]
+        sm = sorted(float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def _quiet_import_reference():
+    """Import the reference build with its start-up banner kept off stdout (the JSON line is ours)."""
+    from oracle.oracle import reference_module
+    sys.stdout.flush()
+    saved = os.dup(1)
+    try:
+        os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+        return reference_module()
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
+def _cpu_flux_rows(o, kind, cores, nrows):
+    """Flux on the central `nrows` rows of the 201 x 201 grid (same point spacing); returns
+    (seconds, samples) with samples counted from the CPU path's own stop levels."""
+    import numpy as np
+    w1 = 0.01 * (nrows - 1) / (GRID - 1)
+    kw = dict(energy_eV=E1, npoints=[nrows, GRID], width=[w1 if nrows > 1 else 1e-9, 0.01], translation=[0, 0, 30])
+    if kind == "reference":
+        kw["nthreads"] = cores
+    t0 = time.perf_counter()
+    o.calculate_flux_rectangle(**kw)
+    dt = time.perf_counter() - t0
+    lev = np.array([v for _, v in o.calculate_flux_rectangle(**dict(kw, quantity="level"))])
+    return dt, float(np.sum(2.0 ** (lev + 1) - 1))
+
+
+def _cpu_impl():
+    from oracle.oracle import OracleSR
+    S = _quiet_import_reference()
+    cores = os.cpu_count() or 1
+    if S is not None:
+        return "reference", cores, S.sr(nthreads=cores, gpu=0)
+    return "port", 1, OracleSR()
+
+
+def reference_arm(args):
+    """The reference's own CPU implementation on all host cores (rank 0 only), same workload and
+    metric; each step is the largest set of central grid rows that keeps the run to ~20 s."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    kind, cores, o = _cpu_impl()
+    setup(o)
+    o.calculate_trajectory()
+    dt, _ = _cpu_flux_rows(o, kind, cores, 5)
+    rows = int(max(5, min(GRID, (20.0 / max(1, args.steps)) / max(dt / 5, 1e-6))))
+    rows -= (rows + 1) % 2  # odd: the row set stays centred on the axis
+    times, samples = [], 0.0
+    for _ in range(args.steps):
+        dt, s = _cpu_flux_rows(o, kind, cores, rows)
+        times.append(dt)
+        samples += s
+    total = sum(times)
+    value = samples / total / 1e9
+    desc = "central %d of 201 rows x 201 columns per step, %d steps, %d threads" % (rows, args.steps, cores)
+    line = {"metric": METRIC, "value": value, "unit": "Gsamples/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": desc}, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "Gsamples/s", "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": "Gsamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_leg():
+    """The reference CPU path on all host cores, bounded to ~10-20 s of work."""
+    kind, cores, o = _cpu_impl()
+    setup(o)
+    o.calculate_trajectory()
+    dt, _ = _cpu_flux_rows(o, kind, cores, 5)
+    rows = int(max(5, min(GRID, 15.0 / max(dt / 5, 1e-6))))
+    rows -= (rows + 1) % 2
+    dt, samples = _cpu_flux_rows(o, kind, cores, rows)
+    return {"value": samples / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": kind,
+            "sample": "central %d of 201 rows x 201 columns, one pass, %.2f s" % (rows, dt)}
+
+
+def product_arm(args):
+    import ctypes
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from oscars_b200 import _lib
+    from oscars_b200._lib import RadOpts
+    from oscars_b200.sr import sr
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    energy = E1 * (1 + 1e-3 * rank)
+    s = sr(gpu=1, device=local)
+    setup(s)
+    s.calculate_trajectory()
+    ctx = s._ctx
+    xyz, nrm, x12 = s._rectangle([GRID, GRID], "XY", [0.01, 0.01], None, None, [0, 0, 30], 0, False)
+    n = GRID * GRID
+    o = RadOpts(precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, quantity=0,
+                precision_mode=1 if args.compute == "mixed" else 0)
+    o.horizontal[:] = [1, 0, 0]
+    o.propagation[:] = [0, 0, 1]
+    dev = torch.device("cuda", local)
+    d_obs = torch.tensor(xyz, dtype=torch.float64, device=dev)
+    d_out = torch.zeros(n, dtype=torch.float64, device=dev)
+    d_lvl = torch.zeros(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        ctx.call("osc_drop_level_cache")
+        ctx.call("osc_flux_device", ctypes.c_void_p(d_obs.data_ptr()), n, energy, ctypes.byref(o),
+                 ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_lvl.data_ptr()), sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.call("osc_set_profiling", 1)
+    ctx.call("osc_get_profile", None, None, None, 1)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    samples = 0
+    launches = 0
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            step()
+            evs[i][1].record(stream)
+            sm, ln = ctypes.c_longlong(), ctypes.c_longlong()
+            ctx.call("osc_last_stats", ctypes.byref(sm), ctypes.byref(ln))
+            samples += sm.value
+            launches += ln.value
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    kms, kl, ks = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
+    ctx.call("osc_get_profile", ctypes.byref(kms), ctypes.byref(kl), ctypes.byref(ks), 1)
+    ctx.call("osc_set_profiling", 0)
+    t = torch.tensor([ms, float(samples)], dtype=torch.float64, device=dev)
+    if world > 1:
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        ms_max, samples_all = float(tmax[0]), float(tsum[1])
+    else:
+        ms_max, samples_all = ms, float(samples)
+    value = samples_all / (ms_max * 1e-3) / 1e9
+
+    # e2e: host buffers through the C ABI, new trajectory every step (host RK4 + spline included)
+    out_h = np.zeros(n)
+    lvl_h = np.zeros(n, dtype=np.int32)
+    nnc = ctypes.c_longlong()
+
+    def e2e_step():
+        s.set_new_particle(particle="ideal")  # drops the trajectory: RK4 + spline + upload again
+        ctx.call("osc_flux", _lib.dptr(xyz), n, energy, ctypes.byref(o), _lib.dptr(out_h), _lib.i32ptr(lvl_h),
+                 ctypes.byref(nnc))
+    e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2e_times = []
+    e2e_samples = 0
+    for i in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_times.append(time.perf_counter() - t0)
+        sm = ctypes.c_longlong()
+        ctx.call("osc_last_stats", ctypes.byref(sm), None)
+        e2e_samples += sm.value
+    e2e_s = sum(e2e_times)
+    te = torch.tensor([e2e_s, float(e2e_samples)], dtype=torch.float64, device=dev)
+    if world > 1:
+        tm = te.clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        ts = te.clone()
+        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+        e2e_value = float(ts[1]) / float(tm[0]) / 1e9
+    else:
+        e2e_value = e2e_samples / e2e_s / 1e9
+    h2d = xyz.nbytes + 19 * 20001 * 8 + 8
+    d2h = out_h.nbytes + lvl_h.nbytes
+
+    peak = ctypes.c_double()
+    ctx.call("osc_measure_fma_peak", 0 if args.compute == "fp64" else 1, ctypes.byref(peak))
+    achieved = ks.value * FLOP_PER_SAMPLE / (kms.value * 1e-3) / 1e12 if kms.value > 0 else None
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof_path):
+        traffic = json.load(open(prof_path)).get("fd_wave_%s" % args.compute)
+    roof = {"bound": "fp64" if args.compute == "fp64" else "fp32", "achieved": achieved, "peak": peak.value,
+            "unit": "TFLOP/s", "frac": (achieved / peak.value) if achieved else None, "traffic": traffic,
+            "kernel": "k_fd_wave_%s" % args.compute, "flop_per_sample": FLOP_PER_SAMPLE,
+            "kernel_ms_per_step": kms.value / max(1, args.steps), "kernel_launches": kl.value,
+            "peak_source": "in-run FMA-throughput loop on this GPU (osc_measure_fma_peak); the sample-sum "
+                           "kernels run on the FP64/FP32 pipes, not the tensor cores or HBM"}
+    clocks = clk.summary()
+    if rank == 0:
+        cpu = cpu_baseline_leg() if world == 1 else None
+        line = {"metric": METRIC, "value": value, "unit": "Gsamples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.compute == "fp64" else "f32+f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "compute": args.compute, "l2": "flushed between steps (256 MB write)",
+                           "parallelism": "independent job per rank" if world > 1 else "single GPU"},
+                "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--compute", default="fp64", choices=["fp64", "mixed"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        product_arm(args)
+
+
+if __name__ == "__main__":
+    main()

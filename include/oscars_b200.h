@@ -1,0 +1,199 @@
+/*
+ * oscars_b200.h -- C ABI of the B200 (sm_100a) implementation of the OSCARS radiation hot path.
+ *
+ * Plain C types, caller-owned buffers, an int status return on every call (0 = OSC_OK, never an
+ * exception across the boundary), one osc_ctx per host thread.  osc_last_error() gives the message
+ * for the last non-zero status, worded like the reference's ValueError texts.
+ *
+ * The reference GPU seam these entry points replace is include/OSCARSSR_Cuda.h:28-66
+ * (OSCARSSR_Cuda_CalculateFluxGPU / _CalculateSpectrumGPU / _CalculatePowerDensityGPU /
+ * _GetDeviceCount), called from OSCARSSR::Calculate*GPU (src/OSCARSSR.cc:2429, 3125, 4428).
+ * Those take C++ references to OSCARSSR, TSurfacePoints and the result containers; here the same
+ * information crosses as plain arrays and descriptors, and the simulation state (fields, beam,
+ * trajectory) lives in the osc_ctx.
+ */
+#ifndef OSCARS_B200_H
+#define OSCARS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OSC_API __attribute__((visibility("default")))
+
+/* Status codes.  The reference maps std::length_error / out_of_range / invalid_argument to
+ * ValueError (src/OSCARSSR_Python.cc:5892-5915); the three are kept apart here. */
+enum osc_status {
+  OSC_OK = 0,
+  OSC_ERR_INVALID = 1,      /* std::invalid_argument in the reference */
+  OSC_ERR_RANGE = 2,        /* std::out_of_range */
+  OSC_ERR_LENGTH = 3,       /* std::length_error */
+  OSC_ERR_STATE = 4,        /* call order (no beam, no trajectory ...) */
+  OSC_ERR_CUDA = 5,         /* a CUDA runtime call failed; message has the CUDA error string */
+  OSC_ERR_NO_DEVICE = 6,    /* no usable sm_100 device */
+  OSC_ERR_ALLOC = 7,        /* device or host allocation failed */
+  OSC_ERR_TIMEOUT = 8       /* a bounded device-side wait gave up */
+};
+
+enum osc_field_kind { OSC_FIELD_UNDULATOR = 0, OSC_FIELD_EPU = 1 };
+
+/* Particle types of TParticleA::SetParticleType (src/TParticleA.cc:78-121). */
+enum osc_particle_type {
+  OSC_PARTICLE_ELECTRON = 0, OSC_PARTICLE_POSITRON = 1, OSC_PARTICLE_MUON = 2,
+  OSC_PARTICLE_ANTIMUON = 3, OSC_PARTICLE_PROTON = 4, OSC_PARTICLE_ANTIPROTON = 5,
+  OSC_PARTICLE_PIPLUS = 6, OSC_PARTICLE_PIMINUS = 7, OSC_PARTICLE_CUSTOM = 8
+};
+
+/* Beam distributions, TParticleBeam_BeamDistribution order (include/TParticleBeam.h). */
+enum osc_distribution { OSC_DIST_DEFAULT = -1, OSC_DIST_FILAMENT = 1, OSC_DIST_GAUSSIAN = 2, OSC_DIST_KV = 3 };
+
+/* Polarization selectors (string matching of src/OSCARSSR.cc:4129-4150 is done by the caller). */
+enum osc_polarization { OSC_POL_ALL = 0, OSC_POL_LH = 1, OSC_POL_LV = 2, OSC_POL_LINEAR = 3,
+                        OSC_POL_CL = 4, OSC_POL_CR = 5 };
+
+/* Quantity returned per entry, src/OSCARSSR_Python.cc:5865-5875 ('flux', 'precision', 'level'). */
+enum osc_quantity { OSC_Q_VALUE = 0, OSC_Q_PRECISION = 1, OSC_Q_LEVEL = 2 };
+
+/* Arithmetic of the radiation integral. */
+enum osc_precision_mode {
+  OSC_FP64 = 0,   /* the reference's FP64 method; matches the reference CPU path to <= 1e-9 */
+  OSC_MIXED = 1   /* FP64 trajectory and retarded phase, FP32 amplitudes, sincos and sums */
+};
+
+typedef struct osc_ctx osc_ctx;
+
+typedef struct {
+  int kind;                 /* osc_field_kind */
+  double bfield[3];         /* peak field [T] (EPU: field A) */
+  double bfield_b[3];       /* EPU field B [T]; ignored for the undulator */
+  double period[3];         /* period vector [m]: magnitude = period, direction = axis */
+  int nperiods;
+  double center[3];         /* translation [m] */
+  double phase;             /* [rad] */
+  double taper;             /* [1/m] */
+  double frequency;         /* [Hz], 0 = static */
+  double frequency_phase;   /* [rad] */
+  double time_offset;       /* [s] */
+} osc_field_desc;
+
+typedef struct {
+  int particle;             /* osc_particle_type */
+  double charge, mass;      /* [C], [kg]; custom particles only */
+  double energy_GeV;        /* -1 = not given (the binding default) */
+  double x0[3];             /* initial position [m] (already rotated/translated) */
+  double d0[3];             /* direction (already rotated) */
+  double horizontal[3];     /* horizontal direction before normalisation, see add_particle_beam */
+  double t0;                /* [m] */
+  double current;           /* [A]; 0 = use the particle charge (TParticleA::SetCurrent) */
+  double sigma_energy_GeV;
+  double emittance[2];
+  int has_emittance;
+  double beta[2], alpha[2];
+  int has_beta, has_alpha;
+  double eta[2];
+  int distribution;         /* osc_distribution */
+  double ctstartstop[2];
+  int has_ctstartstop;
+} osc_beam_desc;
+
+typedef struct {
+  int polarization;         /* osc_polarization */
+  double angle;             /* [rad], OSC_POL_LINEAR */
+  double horizontal[3];     /* horizontal_direction, default (1,0,0) */
+  double propagation[3];    /* propogation_direction, default (0,0,1) */
+  double precision;         /* relative convergence target, default 0.01 */
+  int max_level;            /* default -2 (= 26) */
+  int max_level_extended;   /* default 0 */
+  int nparticles;           /* 0 = the current particle; N = N random particles, weight 1/N */
+  int quantity;             /* osc_quantity */
+  int precision_mode;       /* osc_precision_mode */
+} osc_rad_opts;
+
+/* ---- device / context ---------------------------------------------------------------------- */
+/* Replaces OSCARSSR_Cuda_GetDeviceCount (include/OSCARSSR_Cuda.h:66). */
+OSC_API int osc_get_device_count(int* count);
+/* device -1 creates a host-only context (fields, beam, trajectory, surfaces; radiation calls
+ * return OSC_ERR_NO_DEVICE).  On failure osc_last_error(NULL) has the reason. */
+OSC_API int osc_ctx_create(int device, osc_ctx** out);
+OSC_API void osc_ctx_destroy(osc_ctx* ctx);
+OSC_API const char* osc_last_error(const osc_ctx* ctx);
+OSC_API const char* osc_version(void);
+
+/* ---- fields: OSCARSSR::AddMagneticField (src/OSCARSSR.cc:157-169) with TField3D_IdealUndulator
+ *      (src/TField3D_IdealUndulator.cc:113-152) and TField3D_IdealEPU (src/TField3D_IdealEPU.cc:116-170) */
+OSC_API int osc_clear_fields(osc_ctx* ctx);
+OSC_API int osc_add_field(osc_ctx* ctx, const osc_field_desc* field);
+OSC_API int osc_get_bfield(osc_ctx* ctx, const double x[3], double t, double out[3]);
+
+/* ---- beam: set_particle_beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) ------------------ */
+OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* beam);
+OSC_API int osc_set_seed(osc_ctx* ctx, int seed);                  /* TRandomA::SetSeed */
+OSC_API int osc_set_new_particle(osc_ctx* ctx, int ideal);         /* OSCARSSR::SetNewParticle */
+OSC_API int osc_get_particle(osc_ctx* ctx, double x0[3], double beta0[3], double* t0, double* gamma);
+OSC_API int osc_set_ctstartstop(osc_ctx* ctx, double start, double stop);       /* :637-647 */
+OSC_API int osc_get_ctstartstop(osc_ctx* ctx, double* start, double* stop);
+OSC_API int osc_set_npoints_trajectory(osc_ctx* ctx, long long n);
+OSC_API int osc_get_npoints_trajectory(osc_ctx* ctx, long long* n);
+
+/* ---- trajectory: OSCARSSR::CalculateTrajectory (src/OSCARSSR.cc:853-1009) -------------------- */
+OSC_API int osc_calculate_trajectory(osc_ctx* ctx);
+/* out: 10 x n SoA (t, x, y, z, beta_x, beta_y, beta_z, a_x/c, a_y/c, a_z/c); n_out = points. */
+OSC_API int osc_get_trajectory(osc_ctx* ctx, double* out, long long capacity, long long* n_out);
+
+/* ---- observation surfaces: TSurfacePoints_Rectangle::Init/GetXYZ/GetX1/GetX2
+ *      (src/TSurfacePoints_Rectangle.cc:140-315).  Any pointer may be NULL. */
+OSC_API int osc_surface_rectangle(const char* plane, int nx1, int nx2, double width1,
+                                  double width2, const double rotations[3],
+                                  const double translation[3], int normal, double* xyz,
+                                  double* normals, double* x1x2);
+
+/* ---- radiation: host buffers in and out; results are written (not accumulated). -------------
+ * osc_flux          replaces OSCARSSR_Cuda_CalculateFluxGPU         (src/OSCARSSR_Cuda.cu:516)
+ * osc_spectrum      replaces OSCARSSR_Cuda_CalculateSpectrumGPU     (src/OSCARSSR_Cuda.cu:1607)
+ * osc_power_density replaces OSCARSSR_Cuda_CalculatePowerDensityGPU (src/OSCARSSR_Cuda.cu:2678)
+ * out[i] is the value selected by opts->quantity; level_out (may be NULL) gets the stop level,
+ * -1 for entries that did not converge; *n_not_converged (may be NULL) counts those. */
+OSC_API int osc_flux(osc_ctx* ctx, const double* obs_xyz, long long n_obs, double energy_eV,
+                     const osc_rad_opts* opts, double* out, int32_t* level_out,
+                     long long* n_not_converged);
+OSC_API int osc_spectrum(osc_ctx* ctx, const double obs[3], const double* energies_eV,
+                         long long n_energies, const osc_rad_opts* opts, double* out,
+                         int32_t* level_out, long long* n_not_converged);
+OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double* normals,
+                              long long n_obs, int directional, const osc_rad_opts* opts,
+                              double* out, int32_t* level_out, long long* n_not_converged);
+
+/* ---- device-resident variants: same arithmetic, pointers are device memory on the context's
+ *      device, work is queued on `stream` (a cudaStream_t, NULL = the context's stream) and the
+ *      call returns without synchronising.  Single particle (opts->nparticles must be 0). */
+OSC_API int osc_flux_device(osc_ctx* ctx, const double* d_obs_xyz, long long n_obs,
+                            double energy_eV, const osc_rad_opts* opts, double* d_out,
+                            int32_t* d_level, void* stream);
+OSC_API int osc_power_density_device(osc_ctx* ctx, const double* d_obs_xyz,
+                                     const double* d_normals, long long n_obs, int directional,
+                                     const osc_rad_opts* opts, double* d_out, int32_t* d_level,
+                                     void* stream);
+
+/* Number of trajectory samples integrated by the last radiation call (sum over entries and
+ * particles of 2^(L+1)-1 for stop level L), and the number of kernel launches it made. */
+OSC_API int osc_last_stats(osc_ctx* ctx, long long* samples, long long* launches);
+
+/* Profiling: when enabled, every sample-integration kernel launch is bracketed by CUDA events on
+ * its stream; osc_get_profile returns the summed device time [ms] of those launches since the last
+ * reset, their number, and the samples they integrated (reset = 1 clears the counters). */
+OSC_API int osc_set_profiling(osc_ctx* ctx, int enable);
+OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches, long long* samples,
+                            int reset);
+/* Drop the device-side level-sample cache (it is rebuilt by the next radiation call). */
+OSC_API int osc_drop_level_cache(osc_ctx* ctx);
+/* Measured arithmetic peak of this GPU: an FMA-throughput loop in FP64 (kind 0) or FP32 (kind 1),
+ * returned in TFLOP/s counting one FMA as two floating-point operations. */
+OSC_API int osc_measure_fma_peak(osc_ctx* ctx, int kind, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

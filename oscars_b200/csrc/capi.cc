@@ -1,0 +1,433 @@
+// capi.cc -- the extern "C" boundary (include/oscars_b200.h).  Every entry point catches osc::Error
+// and any other exception and turns it into a status code plus a message for osc_last_error().
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/oscars_b200.h"
+#include "engine.h"
+
+struct osc_ctx {
+  osc::Engine* eng = nullptr;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(osc_ctx* ctx, F&& f) {
+  if (!ctx) return OSC_ERR_INVALID;
+  try {
+    f();
+    ctx->err.clear();
+    return OSC_OK;
+  } catch (const osc::Error& e) {
+    ctx->err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    ctx->err = "host allocation failed";
+    return OSC_ERR_ALLOC;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return OSC_ERR_INVALID;
+  } catch (...) {
+    ctx->err = "unexpected exception";
+    return OSC_ERR_INVALID;
+  }
+}
+
+osc::Vec3 V3(const double* p) { return p ? osc::v3(p[0], p[1], p[2]) : osc::Vec3{}; }
+
+int particle_qm(int code, double charge, double mass, double& q, double& m) {
+  using namespace osc;
+  switch (code) {  // TParticleA::SetParticleType (src/TParticleA.cc:78-121)
+    case OSC_PARTICLE_ELECTRON: q = -kQe; m = kMe; return 0;
+    case OSC_PARTICLE_POSITRON: q = kQe; m = kMe; return 0;
+    case OSC_PARTICLE_MUON: q = -kQe; m = gev_to_kg(0.1056583715); return 0;
+    case OSC_PARTICLE_ANTIMUON: q = kQe; m = gev_to_kg(0.1056583715); return 0;
+    case OSC_PARTICLE_PROTON: q = kQe; m = gev_to_kg(0.938272046); return 0;
+    case OSC_PARTICLE_ANTIPROTON: q = -kQe; m = gev_to_kg(0.938272046); return 0;
+    case OSC_PARTICLE_PIPLUS: q = kQe; m = gev_to_kg(0.13957018); return 0;
+    case OSC_PARTICLE_PIMINUS: q = -kQe; m = gev_to_kg(0.13957018); return 0;
+    case OSC_PARTICLE_CUSTOM: q = charge; m = mass; return 0;
+    default: return -1;
+  }
+}
+
+void check_opts(const osc_rad_opts* o) {
+  if (!o) throw osc::Error{OSC_ERR_INVALID, "options are required"};
+  if (o->nparticles < 0) throw osc::Error{OSC_ERR_INVALID, "'nparticles' must be >= 1 (sort of)"};
+  if (o->quantity < 0 || o->quantity > 2)
+    throw osc::Error{OSC_ERR_INVALID, "'quantity' must be: 'flux', 'precision', 'level', or blank"};
+  if (o->precision_mode != OSC_FP64 && o->precision_mode != OSC_MIXED)
+    throw osc::Error{OSC_ERR_INVALID, "unknown precision mode"};
+}
+
+}  // namespace
+
+extern "C" {
+
+OSC_API const char* osc_version(void) { return "oscars_b200 0.1 (sm_100a)"; }
+
+OSC_API int osc_get_device_count(int* count) {
+  if (!count) return OSC_ERR_INVALID;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+    return OSC_OK;
+  }
+  int usable = 0;
+  for (int d = 0; d < n; ++d) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10 && p.minor == 0) ++usable;
+  }
+  *count = usable;
+  return OSC_OK;
+}
+
+OSC_API int osc_ctx_create(int device, osc_ctx** out) {
+  if (!out) return OSC_ERR_INVALID;
+  *out = nullptr;
+  if (device == -1) {  // host-only context
+    osc_ctx* c = new (std::nothrow) osc_ctx;
+    if (!c) return OSC_ERR_ALLOC;
+    c->eng = new osc::Engine(-1);
+    *out = c;
+    return OSC_OK;
+  }
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    g_create_error = "no CUDA device is visible";
+    return OSC_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) {
+    g_create_error = "device index out of range";
+    return OSC_ERR_RANGE;
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess || p.major != 10 || p.minor != 0) {
+    g_create_error = "device is not an sm_100 (B200) GPU";
+    return OSC_ERR_NO_DEVICE;
+  }
+  osc_ctx* c = new (std::nothrow) osc_ctx;
+  if (!c) return OSC_ERR_ALLOC;
+  try {
+    c->eng = new osc::Engine(device);
+  } catch (const osc::Error& e) {
+    g_create_error = e.msg;
+    delete c;
+    return e.code;
+  }
+  *out = c;
+  return OSC_OK;
+}
+
+OSC_API void osc_ctx_destroy(osc_ctx* ctx) {
+  if (!ctx) return;
+  delete ctx->eng;
+  delete ctx;
+}
+
+OSC_API const char* osc_last_error(const osc_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+OSC_API int osc_clear_fields(osc_ctx* ctx) {
+  return guarded(ctx, [&] { ctx->eng->model.clear_fields(); });
+}
+
+OSC_API int osc_add_field(osc_ctx* ctx, const osc_field_desc* f) {
+  return guarded(ctx, [&] {
+    if (!f) throw osc::Error{OSC_ERR_INVALID, "field descriptor is NULL"};
+    if (f->kind != OSC_FIELD_UNDULATOR && f->kind != OSC_FIELD_EPU) throw osc::Error{OSC_ERR_INVALID, "unknown field kind"};
+    osc::FieldSpec s;
+    s.kind = f->kind;
+    s.a = V3(f->bfield);
+    s.b = V3(f->bfield_b);
+    s.period = V3(f->period);
+    s.nperiods = f->nperiods;
+    s.center = V3(f->center);
+    s.phase = f->phase;
+    s.taper = f->taper;
+    s.frequency = f->frequency;
+    s.frequency_phase = f->frequency_phase;
+    s.time_offset = f->time_offset;
+    ctx->eng->model.add_field(s);
+  });
+}
+
+OSC_API int osc_get_bfield(osc_ctx* ctx, const double x[3], double t, double out[3]) {
+  return guarded(ctx, [&] {
+    const osc::Vec3 b = osc::field_sum(ctx->eng->model.fields, V3(x), t);
+    out[0] = b.x; out[1] = b.y; out[2] = b.z;
+  });
+}
+
+// add_particle_beam + set_particle_beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) for a
+// single user-defined beam; the TParticleBeam 10-argument constructor (src/TParticleBeam.cc:68-101).
+OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* d) {
+  return guarded(ctx, [&] {
+    using namespace osc;
+    if (!d) throw Error{OSC_ERR_INVALID, "beam descriptor is NULL"};
+    Model& M = ctx->eng->model;
+    BeamSpec b;
+    if (particle_qm(d->particle, d->charge, d->mass, b.q, b.m))
+      throw Error{OSC_ERR_INVALID, "invalid argument in adding particle beam.  possibly 'name' already exists"};
+    if (d->particle == OSC_PARTICLE_CUSTOM && (d->mass == 0 || d->charge == 0))
+      throw Error{OSC_ERR_INVALID, "'mass' or 'charge' is zero"};
+    double e = d->energy_GeV == -1 ? 0 : d->energy_GeV;
+    if (e < 0) throw Error{OSC_ERR_INVALID, "We do not currently support negative energy beams.  Please change 'energy_GeV' to >= 0"};
+    if (d->sigma_energy_GeV < 0) throw Error{OSC_ERR_INVALID, "'sigma_energy_GeV' cannot be less than zero"};
+    const Vec3 dir = V3(d->d0);
+    const Vec3 hd = unit(V3(d->horizontal));  // binding normalises once ...
+    b.x0 = V3(d->x0);
+    b.u0 = mag2(dir) > 0 ? unit(dir) : Vec3{};
+    b.e0 = e < kg_to_gev(b.m) ? b.m : e;
+    b.t0 = d->t0;
+    b.current = d->current != 0 ? d->current : b.q;
+    b.hdir = unit(hd);  // ... and SetHorizontalDirection again (src/TParticleBeam.cc:306-312)
+    b.vdir = -unit(cross(hd, b.u0));
+    b.distribution = OSC_DIST_FILAMENT;
+    if (d->has_emittance) {
+      b.emit[0] = d->emittance[0];
+      b.emit[1] = d->emittance[1];
+      b.distribution = OSC_DIST_GAUSSIAN;
+    }
+    if (d->distribution != OSC_DIST_DEFAULT) b.distribution = d->distribution;
+    b.sigma_e = d->sigma_energy_GeV;
+    b.twiss_at_x0();
+    if (d->has_beta) {  // SetTwissBetaAlpha (src/TParticleBeam.cc:177-196)
+      const double a0 = d->has_alpha ? d->alpha[0] : 0, a1 = d->has_alpha ? d->alpha[1] : 0;
+      if (d->beta[0] <= 0 || d->beta[1] <= 0) throw Error{OSC_ERR_RANGE, "Beta cannot be <= 0"};
+      b.tw_beta[0] = d->beta[0]; b.tw_beta[1] = d->beta[1];
+      b.tw_gamma[0] = (1. + a0 * a0) / d->beta[0];
+      b.tw_gamma[1] = (1. + a1 * a1) / d->beta[1];
+      b.tw_alpha[0] = a0; b.tw_alpha[1] = a1;
+      b.twiss_at_x0();
+    }
+    b.eta[0] = d->eta[0];
+    b.eta[1] = d->eta[1];
+    M.beam = b;
+    M.has_beam = true;
+    if (d->has_ctstartstop) M.set_ctstartstop(d->ctstartstop[0], d->ctstartstop[1]);
+    else M.set_ctstartstop(-3, 3);
+    M.ideal_particle();
+  });
+}
+
+OSC_API int osc_set_seed(osc_ctx* ctx, int seed) {
+  return guarded(ctx, [&] { ctx->eng->model.rng.seed(seed); });
+}
+
+OSC_API int osc_set_new_particle(osc_ctx* ctx, int ideal) {
+  return guarded(ctx, [&] {
+    osc::Model& M = ctx->eng->model;
+    if (!M.has_beam) throw osc::Error{OSC_ERR_RANGE, "no beam defined"};
+    if (ideal) M.ideal_particle();
+    else M.random_particle();
+  });
+}
+
+OSC_API int osc_get_particle(osc_ctx* ctx, double x0[3], double beta0[3], double* t0, double* gamma) {
+  return guarded(ctx, [&] {
+    const osc::Particle& p = ctx->eng->model.particle;
+    if (x0) { x0[0] = p.x0.x; x0[1] = p.x0.y; x0[2] = p.x0.z; }
+    if (beta0) { beta0[0] = p.b0.x; beta0[1] = p.b0.y; beta0[2] = p.b0.z; }
+    if (t0) *t0 = p.t0;
+    if (gamma) *gamma = p.gamma;
+  });
+}
+
+OSC_API int osc_set_ctstartstop(osc_ctx* ctx, double start, double stop) {
+  return guarded(ctx, [&] { ctx->eng->model.set_ctstartstop(start, stop); });
+}
+
+OSC_API int osc_get_ctstartstop(osc_ctx* ctx, double* start, double* stop) {
+  return guarded(ctx, [&] {
+    if (start) *start = ctx->eng->model.ctstart;
+    if (stop) *stop = ctx->eng->model.ctstop;
+  });
+}
+
+OSC_API int osc_set_npoints_trajectory(osc_ctx* ctx, long long n) {
+  return guarded(ctx, [&] { ctx->eng->model.npoints = n; });
+}
+
+OSC_API int osc_get_npoints_trajectory(osc_ctx* ctx, long long* n) {
+  return guarded(ctx, [&] { if (n) *n = ctx->eng->model.npoints; });
+}
+
+OSC_API int osc_calculate_trajectory(osc_ctx* ctx) {
+  return guarded(ctx, [&] {
+    osc::Model& M = ctx->eng->model;
+    if (!M.particle.set) {
+      if (!M.has_beam) throw osc::Error{OSC_ERR_RANGE, "particle not initialized.  make sure you have a particle or beam defined"};
+      M.random_particle();
+    }
+    M.compute_trajectory();
+  });
+}
+
+OSC_API int osc_get_trajectory(osc_ctx* ctx, double* out, long long capacity, long long* n_out) {
+  return guarded(ctx, [&] {
+    const osc::Knots& k = ctx->eng->model.knots;
+    if (n_out) *n_out = k.n;
+    if (!out) return;
+    if (capacity < 10 * k.n) throw osc::Error{OSC_ERR_LENGTH, "trajectory buffer too small"};
+    std::memcpy(out, k.t.data(), sizeof(double) * k.n);
+    std::memcpy(out + k.n, k.y.data(), sizeof(double) * 9 * k.n);
+  });
+}
+
+OSC_API int osc_surface_rectangle(const char* plane, int nx1, int nx2, double width1, double width2,
+                                  const double rotations[3], const double translation[3], int normal, double* xyz,
+                                  double* normals, double* x1x2) {
+  try {
+    if (!plane) return OSC_ERR_INVALID;
+    if (nx1 <= 0 || nx2 <= 0) {
+      g_create_error = "an entry in 'npoints' is <= 0";
+      return OSC_ERR_INVALID;
+    }
+    osc::surface_rectangle(plane, nx1, nx2, width1, width2, V3(rotations), V3(translation), normal, xyz, normals, x1x2);
+    return OSC_OK;
+  } catch (const osc::Error& e) {
+    g_create_error = e.msg;
+    return e.code;
+  }
+}
+
+OSC_API int osc_flux(osc_ctx* ctx, const double* obs_xyz, long long n_obs, double energy_eV, const osc_rad_opts* opts,
+                     double* out, int32_t* level_out, long long* n_not_converged) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (n_obs < 0 || (n_obs > 0 && (!obs_xyz || !out))) throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    osc::RadRequest rq;
+    rq.obs = obs_xyz;
+    rq.n_obs = n_obs;
+    rq.omega = {osc::ev_to_omega(energy_eV)};
+    rq.opts = *opts;
+    rq.out = out;
+    rq.level_out = level_out;
+    ctx->eng->radiation(rq);
+    if (n_not_converged) *n_not_converged = ctx->eng->last_not_converged;
+  });
+}
+
+OSC_API int osc_spectrum(osc_ctx* ctx, const double obs[3], const double* energies_eV, long long n_energies,
+                         const osc_rad_opts* opts, double* out, int32_t* level_out, long long* n_not_converged) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (!obs || n_energies < 0 || (n_energies > 0 && (!energies_eV || !out))) throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    osc::RadRequest rq;
+    rq.obs = obs;
+    rq.n_obs = 1;
+    rq.omega.resize(n_energies);
+    for (long long i = 0; i < n_energies; ++i) rq.omega[i] = osc::ev_to_omega(energies_eV[i]);
+    rq.opts = *opts;
+    rq.spectrum_current_abs = true;
+    rq.out = out;
+    rq.level_out = level_out;
+    ctx->eng->radiation(rq);
+    if (n_not_converged) *n_not_converged = ctx->eng->last_not_converged;
+  });
+}
+
+OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double* normals, long long n_obs,
+                              int directional, const osc_rad_opts* opts, double* out, int32_t* level_out,
+                              long long* n_not_converged) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (n_obs < 0 || (n_obs > 0 && (!obs_xyz || !out))) throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    osc::RadRequest rq;
+    rq.power_density = true;
+    rq.obs = obs_xyz;
+    rq.normals = normals;
+    rq.n_obs = n_obs;
+    rq.directional = directional != 0;
+    rq.opts = *opts;
+    rq.out = out;
+    rq.level_out = level_out;
+    ctx->eng->radiation(rq);
+    if (n_not_converged) *n_not_converged = ctx->eng->last_not_converged;
+  });
+}
+
+OSC_API int osc_flux_device(osc_ctx* ctx, const double* d_obs_xyz, long long n_obs, double energy_eV,
+                            const osc_rad_opts* opts, double* d_out, int32_t* d_level, void* stream) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (opts->nparticles != 0) throw osc::Error{OSC_ERR_INVALID, "device-resident calls take one particle"};
+    osc::RadRequest rq;
+    rq.obs = d_obs_xyz;
+    rq.obs_on_device = true;
+    rq.n_obs = n_obs;
+    rq.omega = {osc::ev_to_omega(energy_eV)};
+    rq.opts = *opts;
+    rq.out = d_out;
+    rq.level_out = d_level;
+    rq.out_on_device = true;
+    rq.stream = static_cast<cudaStream_t>(stream);
+    ctx->eng->radiation(rq);
+  });
+}
+
+OSC_API int osc_power_density_device(osc_ctx* ctx, const double* d_obs_xyz, const double* d_normals, long long n_obs,
+                                     int directional, const osc_rad_opts* opts, double* d_out, int32_t* d_level,
+                                     void* stream) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (opts->nparticles != 0) throw osc::Error{OSC_ERR_INVALID, "device-resident calls take one particle"};
+    osc::RadRequest rq;
+    rq.power_density = true;
+    rq.obs = d_obs_xyz;
+    rq.normals = d_normals;
+    rq.obs_on_device = true;
+    rq.n_obs = n_obs;
+    rq.directional = directional != 0;
+    rq.opts = *opts;
+    rq.out = d_out;
+    rq.level_out = d_level;
+    rq.out_on_device = true;
+    rq.stream = static_cast<cudaStream_t>(stream);
+    ctx->eng->radiation(rq);
+  });
+}
+
+OSC_API int osc_last_stats(osc_ctx* ctx, long long* samples, long long* launches) {
+  return guarded(ctx, [&] {
+    if (samples) *samples = ctx->eng->last_samples;
+    if (launches) *launches = ctx->eng->last_launches;
+  });
+}
+
+OSC_API int osc_set_profiling(osc_ctx* ctx, int enable) {
+  return guarded(ctx, [&] { ctx->eng->profiling = enable != 0; });
+}
+
+OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches, long long* samples, int reset) {
+  return guarded(ctx, [&] {
+    osc::Engine& E = *ctx->eng;
+    if (kernel_ms) *kernel_ms = E.prof_ms;
+    if (launches) *launches = E.prof_launches;
+    if (samples) *samples = E.prof_samples;
+    if (reset) { E.prof_ms = 0; E.prof_launches = 0; E.prof_samples = 0; }
+  });
+}
+
+OSC_API int osc_drop_level_cache(osc_ctx* ctx) {
+  return guarded(ctx, [&] { ctx->eng->drop_level_cache(); });
+}
+
+OSC_API int osc_measure_fma_peak(osc_ctx* ctx, int kind, double* tflops) {
+  return guarded(ctx, [&] {
+    const double v = ctx->eng->measure_fma_peak(kind);
+    if (tflops) *tflops = v;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,457 @@
+// engine.cu -- device state of one context and the wave scheduler of the radiation integrals.
+//
+// Data layout in HBM for one trajectory:
+//   knots   19 x n doubles: t, y[9] (x y z, beta, a/c), y''[9]      (from the host RK4 + spline)
+//   levels  10 x cap doubles, cap = 2^(Lmax+1): level L sample i at index 2^L + i
+// Per request: observers (3 x n_obs), angular frequencies, per-entry state (running complex sum and
+// last magnitude), two active-entry lists, span partials, outputs.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kernels.h"
+
+namespace osc {
+
+namespace {
+// Compensated accumulation of one particle's values (T3DScalarContainer::AddToPoint,
+// src/T3DScalarContainer.cc:35-51), unfused like the reference.
+__global__ void k_kahan_add(double* sum, double* comp, const double* v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double S = sum[i];
+  const double y = __dsub_rn(v[i], comp[i]);
+  const double t = __dadd_rn(S, y);
+  comp[i] = __dsub_rn(__dsub_rn(t, S), y);
+  sum[i] = t;
+}
+}  // namespace
+
+void DevBuf::reserve(size_t n) {
+  if (n <= bytes) return;
+  release();
+  if (cudaMalloc(&p, n) != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    cudaGetLastError();
+    throw Error{OSC_ERR_ALLOC, "device allocation of " + std::to_string(n) + " bytes failed"};
+  }
+  bytes = n;
+}
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+Engine::Engine(int dev) : device(dev) {
+  if (dev < 0) return;  // host-only context: model, trajectory and surfaces, no radiation calls
+  check(cudaSetDevice(dev), "cudaSetDevice");
+  check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  bd_bits_.reserve(32 * sizeof(unsigned long long));
+  cnt_.reserve(64);
+}
+
+Engine::~Engine() {
+  if (device < 0) return;
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto& e : ev_pending_) { ev_pool_.push_back(e.first); ev_pool_.push_back(e.second); }
+  for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
+  for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
+                    &act_[1], &cnt_, &acc_, &acc_comp_})
+    b->release();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void Engine::check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error{OSC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+void Engine::upload_trajectory() {
+  const Knots& k = model.knots;
+  if (knots_version_ == model.knots_version && nknots_ == k.n) return;
+  levels_dropped_ = false;
+  const int64_t n = k.n;
+  knots_.reserve(sizeof(double) * 19 * n);
+  double* d = knots_.as<double>();
+  check(cudaMemcpyAsync(d, k.t.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload t");
+  check(cudaMemcpyAsync(d + n, k.y.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, stream), "upload y");
+  check(cudaMemcpyAsync(d + 10 * n, k.ypp.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, stream),
+        "upload ypp");
+  nknots_ = n;
+  tstart_ = k.tstart;
+  tstop_ = k.tstop;
+  knots_version_ = model.knots_version;
+  lev_filled_ = -1;
+  bdmax_valid_ = false;
+  check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), stream), "memset");
+}
+
+// Make levels 0..L resident.  The cache grows by doubling; growing refills from level 0.
+void Engine::ensure_levels(int L) {
+  if (L <= lev_filled_) return;
+  const int64_t need = (int64_t)2 << L;
+  if (need > lev_cap_) {
+    int64_t cap = std::max<int64_t>(need, (int64_t)2 << 13);
+    if (lev_cap_ > 0 && lev_filled_ >= 0) {
+      // keep what is filled: copy the 10 arrays into the larger cache
+      DevBuf nb;
+      nb.reserve(sizeof(double) * 10 * cap);
+      const int64_t used = (int64_t)2 << lev_filled_;
+      for (int a = 0; a < 10; ++a)
+        check(cudaMemcpyAsync(nb.as<double>() + a * cap, lev_.as<double>() + a * lev_cap_, sizeof(double) * used,
+                              cudaMemcpyDeviceToDevice, stream),
+              "level cache grow");
+      check(cudaStreamSynchronize(stream), "level cache grow");
+      lev_.release();
+      lev_ = nb;
+      nb.p = nullptr;
+    } else {
+      lev_.reserve(sizeof(double) * 10 * cap);
+    }
+    lev_cap_ = cap;
+  }
+  if (lev_filled_ < 0)
+    check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), stream), "memset");
+  const int64_t s_begin = lev_filled_ < 0 ? 1 : ((int64_t)2 << lev_filled_);
+  const int64_t s_end = (int64_t)2 << L;
+  check(launch_level_fill(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, lev_.as<double>(), lev_cap_,
+                          -1, bd_bits_.as<unsigned long long>(), stream),
+        "level fill");
+  last_launches += 2;
+  lev_filled_ = L;
+  bdmax_valid_ = false;
+}
+
+void Engine::refresh_bdmax() {
+  if (bdmax_valid_) return;
+  unsigned long long bits[32];
+  check(cudaMemcpyAsync(bits, bd_bits_.p, sizeof(bits), cudaMemcpyDeviceToHost, stream), "bdmax");
+  check(cudaStreamSynchronize(stream), "bdmax");
+  bdmax_.assign(32, -1.0);
+  for (int L = 1; L < 32; ++L) {
+    double d;
+    std::memcpy(&d, &bits[L], sizeof d);
+    bdmax_[L] = d;
+  }
+  bdmax_valid_ = true;
+}
+
+static double dt_inclusive(double tstart, double tstop, int L) {  // :224-237
+  return (tstop - tstart) / (std::pow(2., L + 1) - 1);
+}
+
+// Polarization vector of src/OSCARSSR.cc:4116-4150 (host double arithmetic, reference order).
+static void polarization_vector(const osc_rad_opts& o, double P[6], bool& project) {
+  const Vec3 hor = v3(o.horizontal[0], o.horizontal[1], o.horizontal[2]);
+  const Vec3 prop = v3(o.propagation[0], o.propagation[1], o.propagation[2]);
+  const Vec3 vert = unit(cross(prop, hor));
+  const double k = 1. / std::sqrt(2);
+  for (int i = 0; i < 6; ++i) P[i] = 0;
+  switch (o.polarization) {
+    case OSC_POL_ALL: break;
+    case OSC_POL_LH: P[0] = hor.x; P[2] = hor.y; P[4] = hor.z; break;
+    case OSC_POL_LV: P[0] = vert.x; P[2] = vert.y; P[4] = vert.z; break;
+    case OSC_POL_LINEAR: {
+      const Vec3 r = rotate_about(hor, o.angle, prop);
+      P[0] = r.x; P[2] = r.y; P[4] = r.z;
+      break;
+    }
+    case OSC_POL_CL:
+    case OSC_POL_CR: {
+      const double sg = o.polarization == OSC_POL_CL ? 1.0 : -1.0;
+      const double h[3] = {hor.x, hor.y, hor.z}, v[3] = {vert.x, vert.y, vert.z};
+      for (int c = 0; c < 3; ++c) {
+        P[2 * c] = (sg > 0 ? h[c] + v[c] * 0 : h[c] - v[c] * 0) * k;
+        P[2 * c + 1] = (sg > 0 ? 0 + v[c] * 1 : 0 - v[c] * 1) * k;
+      }
+      break;
+    }
+    default: throw Error{OSC_ERR_INVALID, "Polarization requested not recognized"};
+  }
+  const double m2 = (P[0] * P[0] + P[1] * P[1]) + (P[2] * P[2] + P[3] * P[3]) + (P[4] * P[4] + P[5] * P[5]);
+  project = o.polarization != OSC_POL_ALL && m2 > 0.001;
+}
+
+// Spans per wave: enough CTAs to fill the machine, each span at least one staged chunk.
+static int choose_spans(int64_t n_act, int64_t level_len) {
+  const int64_t tiles = (n_act + 127) / 128;
+  const int64_t target = 148 * 6;
+  int64_t spans = 1;
+  while (tiles * spans < target && level_len / (spans * 2) >= 128) spans *= 2;
+  return (int)spans;
+}
+
+void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,
+                        cudaStream_t st) {
+  const osc_rad_opts& o = rq.opts;
+  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
+  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
+  if (lstop > kMaxLevelMemory)
+    throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
+  if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
+  const Particle& P = model.particle;
+  const int Lfirst = std::min(9, lstop);
+  ensure_levels(std::min(lstop, std::max(Lfirst, 12)));
+  if (rq.power_density) refresh_bdmax();
+
+  unsigned* cnt = cnt_.as<unsigned>();  // [0] n_act A, [1] n_act B, [2] err
+  unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);  // [0] not conv, [1] samples
+  check(cudaMemsetAsync(cnt, 0, 64, st), "memset");
+  const int64_t N = n_items;
+  act_[0].reserve(sizeof(int) * N);
+  act_[1].reserve(sizeof(int) * N);
+  state_.reserve(sizeof(double) * 7 * N);
+
+  const double* d_obs = obs_.as<double>();
+  const double* d_nrm = rq.normals ? nrm_.as<double>() : nullptr;
+  double pol[6];
+  bool project = false;
+  double c0 = 0, c2 = 0, scale = 0;
+  if (!rq.power_density) {
+    polarization_vector(o, pol, project);
+    c0 = P.q / (four_pi() * kC * kEps0 * kSqrt2Pi);                                       // :4106
+    const double cur = rq.spectrum_current_abs ? std::fabs(P.current) : P.current;
+    c2 = four_pi() * cur / (kH * std::fabs(P.q) * kMu0 * kC) * 1e-6 * 0.001;              // :4109
+  } else {
+    scale = std::fabs(P.q * P.current) / (16 * (kPi * kPi) * kEps0 * kC);                 // :2945
+  }
+
+  int cur_list = 0;
+  int64_t n_act = N;  // host bound on the current list size
+  for (int L = Lfirst; L <= lstop; ++L) {
+    const bool first = L == Lfirst;
+    if (!first) {
+      // the finalize of the previous wave appended the survivors to list (cur_list ^ 1)
+      unsigned nn = 0;
+      check(cudaMemcpyAsync(&nn, cnt + (cur_list ^ 1), sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
+      check(cudaStreamSynchronize(st), "count");
+      if (nn == 0) break;
+      cur_list ^= 1;
+      check(cudaMemsetAsync(cnt + (cur_list ^ 1), 0, sizeof(unsigned), st), "memset");
+      n_act = nn;
+      ensure_levels(L);
+      if (rq.power_density) refresh_bdmax();
+    }
+    const int nseg = first && L >= 1 ? 2 : 1;
+    int64_t sb[2], se[2];
+    if (first) {
+      if (nseg == 2) { sb[0] = 1; se[0] = (int64_t)1 << L; sb[1] = (int64_t)1 << L; se[1] = (int64_t)2 << L; }
+      else { sb[0] = 1; se[0] = 2; }
+    } else {
+      sb[0] = (int64_t)1 << L; se[0] = (int64_t)2 << L;
+    }
+    const int spans = choose_spans(n_act, (int64_t)1 << L);
+    int64_t sl[2] = {0, 0};
+    for (int g = 0; g < nseg; ++g) {
+      const int64_t len = se[g] - (sb[g] & ~(int64_t)1);
+      sl[g] = ((len + spans - 1) / spans + 1) & ~(int64_t)1;
+    }
+    const int64_t part_stride = n_act;
+    const int* act_in = first ? nullptr : act_[cur_list].as<int>();
+    const unsigned* nact_in = first ? nullptr : cnt + cur_list;
+    if (!rq.power_density) {
+      part_.reserve(sizeof(double) * (size_t)nseg * spans * kFdPartials * part_stride);
+      FdWaveArgs w{};
+      w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
+      w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in; w.nseg = nseg;
+      for (int g = 0; g < nseg; ++g) { w.seg_b[g] = sb[g] & ~(int64_t)1; w.seg_e[g] = se[g]; w.span_len[g] = sl[g]; }
+      w.part = part_.as<double>(); w.part_stride = part_stride; w.err = cnt + 2;
+      auto ev = timed_begin(st);
+      check(launch_fd_wave_fp64(w, n_act, spans, st), "flux wave");
+      timed_end(ev, st);
+      FdFinalArgs f{};
+      f.part = part_.as<double>(); f.part_stride = part_stride; f.spans = spans; f.nseg = nseg; f.first = first;
+      f.level = L; f.max_level = lstop; f.quantity = o.quantity; f.project = project;
+      f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
+      f.precision = o.precision; f.c0 = c0; f.c2 = c2; f.weight = weight;
+      for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
+      f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
+      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = cnt + (cur_list ^ 1);
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1;
+      check(launch_fd_finalize(f, n_act, st), "flux finalize");
+    } else {
+      part_.reserve(sizeof(double) * (size_t)nseg * spans * part_stride);
+      PdWaveArgs w{};
+      w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
+      w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in; w.nseg = nseg;
+      for (int g = 0; g < nseg; ++g) { w.seg_b[g] = sb[g] & ~(int64_t)1; w.seg_e[g] = se[g]; w.span_len[g] = sl[g]; }
+      w.part = part_.as<double>(); w.part_stride = part_stride; w.err = cnt + 2;
+      auto ev = timed_begin(st);
+      check(launch_pd_wave_fp64(w, n_act, spans, st), "power density wave");
+      timed_end(ev, st);
+      PdFinalArgs f{};
+      f.part = part_.as<double>(); f.part_stride = part_stride; f.spans = spans; f.nseg = nseg; f.first = first;
+      f.level = L; f.max_level = lstop; f.quantity = o.quantity; f.directional = rq.directional;
+      f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
+      f.precision = o.precision; f.scale = scale; f.weight = weight; f.bdmax = bdmax_[L];
+      f.two_over_gamma = 2. / P.gamma;
+      f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
+      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = cnt + (cur_list ^ 1);
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1;
+      check(launch_pd_finalize(f, n_act, st), "power density finalize");
+    }
+    last_launches += 2;
+  }
+  unsigned long long h64[2];
+  unsigned err = 0;
+  check(cudaMemcpyAsync(h64, c64, sizeof h64, cudaMemcpyDeviceToHost, st), "stats");
+  check(cudaMemcpyAsync(&err, cnt + 2, sizeof err, cudaMemcpyDeviceToHost, st), "stats");
+  check(cudaStreamSynchronize(st), "radiation");
+  if (err) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+  last_not_converged += (long long)h64[0];
+  last_samples += (long long)h64[1];
+  if (profiling) {
+    collect_timings();
+    prof_samples += (long long)h64[1];
+  }
+}
+
+std::pair<cudaEvent_t, cudaEvent_t> Engine::timed_begin(cudaStream_t st) {
+  if (!profiling) return {nullptr, nullptr};
+  auto get = [&]() {
+    cudaEvent_t e;
+    if (!ev_pool_.empty()) { e = ev_pool_.back(); ev_pool_.pop_back(); }
+    else check(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+  };
+  std::pair<cudaEvent_t, cudaEvent_t> e{get(), get()};
+  check(cudaEventRecord(e.first, st), "cudaEventRecord");
+  return e;
+}
+
+void Engine::timed_end(std::pair<cudaEvent_t, cudaEvent_t> e, cudaStream_t st) {
+  if (!e.first) return;
+  check(cudaEventRecord(e.second, st), "cudaEventRecord");
+  ev_pending_.push_back(e);
+}
+
+void Engine::collect_timings() {
+  for (auto& e : ev_pending_) {
+    check(cudaEventSynchronize(e.second), "cudaEventSynchronize");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, e.first, e.second), "cudaEventElapsedTime");
+    prof_ms += ms;
+    ++prof_launches;
+    ev_pool_.push_back(e.first);
+    ev_pool_.push_back(e.second);
+  }
+  ev_pending_.clear();
+}
+
+namespace {
+// FMA-throughput probe: 8 independent chains per thread, long enough that launch cost vanishes.
+template <class T>
+__global__ void k_fma_peak(T* out, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = (T)(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = x[k] * a + b;
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == (T)-1.2345) out[threadIdx.x] = s;  // keeps the chains live
+}
+}  // namespace
+
+double Engine::measure_fma_peak(int kind) {
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  check(cudaSetDevice(device), "cudaSetDevice");
+  int sms = 0;
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
+  out_.reserve(4096 * sizeof(double));
+  const int threads = 256, blocks = sms * 8, iters = kind == 0 ? 4096 : 16384;
+  cudaEvent_t a, b;
+  check(cudaEventCreate(&a), "event");
+  check(cudaEventCreate(&b), "event");
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    check(cudaEventRecord(a, stream), "event");
+    if (kind == 0) k_fma_peak<double><<<blocks, threads, 0, stream>>>(out_.as<double>(), iters, 0.999999, 1e-7);
+    else k_fma_peak<float><<<blocks, threads, 0, stream>>>(out_.as<float>(), iters, 0.999999f, 1e-7f);
+    check(cudaGetLastError(), "fma peak");
+    check(cudaEventRecord(b, stream), "event");
+    check(cudaEventSynchronize(b), "event");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, a, b), "event");
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+  return flops / (best * 1e-3) / 1e12;
+}
+
+void Engine::radiation(RadRequest& rq) {
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  check(cudaSetDevice(device), "cudaSetDevice");
+  last_samples = last_launches = last_not_converged = 0;
+  cudaStream_t st = rq.stream ? rq.stream : stream;
+  const int64_t n_e = rq.power_density ? 1 : (int64_t)rq.omega.size();
+  const int64_t N = rq.n_obs * n_e;
+  if (N <= 0) return;
+  // inputs
+  obs_.reserve(sizeof(double) * 3 * rq.n_obs);
+  if (rq.obs_on_device) {
+    check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, cudaMemcpyDeviceToDevice, st), "obs");
+    if (rq.normals) {
+      nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
+      check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, cudaMemcpyDeviceToDevice, st), "normals");
+    }
+  } else {
+    check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, cudaMemcpyHostToDevice, st), "obs");
+    if (rq.normals) {
+      nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
+      check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, cudaMemcpyHostToDevice, st), "normals");
+    }
+  }
+  if (!rq.power_density) {
+    omega_.reserve(sizeof(double) * n_e);
+    check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
+  }
+  out_.reserve(sizeof(double) * N);
+  lvl_.reserve(sizeof(int32_t) * N);
+  double* d_out = rq.out_on_device ? rq.out : out_.as<double>();
+  int32_t* d_lvl = rq.out_on_device ? rq.level_out : lvl_.as<int32_t>();
+  if (!d_lvl) d_lvl = lvl_.as<int32_t>();
+
+  const int np = rq.opts.nparticles;
+  if (np <= 0) {
+    model.ensure_trajectory();
+    upload_trajectory();
+    run_single(rq, N, 1.0, d_out, d_lvl, st);
+  } else {
+    // src/OSCARSSR.cc:4026-4062: new random particle, its trajectory, weight 1/N, compensated sum
+    const double weight = 1.0 / (double)np;
+    acc_.reserve(sizeof(double) * N);
+    acc_comp_.reserve(sizeof(double) * N);
+    check(cudaMemsetAsync(acc_.p, 0, sizeof(double) * N, st), "memset");
+    check(cudaMemsetAsync(acc_comp_.p, 0, sizeof(double) * N, st), "memset");
+    for (int ip = 0; ip < np; ++ip) {
+      model.random_particle();
+      model.compute_trajectory();
+      check(cudaStreamSynchronize(st), "particle");  // the previous trajectory's buffers are free
+      upload_trajectory();
+      run_single(rq, N, weight, out_.as<double>(), d_lvl, st);
+      k_kahan_add<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(acc_.as<double>(), acc_comp_.as<double>(),
+                                                                out_.as<double>(), N);
+      check(cudaGetLastError(), "accumulate");
+      ++last_launches;
+    }
+    check(cudaMemcpyAsync(d_out, acc_.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "result");
+  }
+  if (!rq.out_on_device) {
+    check(cudaMemcpyAsync(rq.out, d_out, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
+    if (rq.level_out)
+      check(cudaMemcpyAsync(rq.level_out, d_lvl, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st), "download");
+    check(cudaStreamSynchronize(st), "download");
+  }
+}
+
+}  // namespace osc

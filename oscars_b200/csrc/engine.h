@@ -1,0 +1,94 @@
+// engine.h -- per-context device state and the wave scheduler of the radiation integrals.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/oscars_b200.h"
+#include "host_core.h"
+
+namespace osc {
+
+// Device buffer that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t n);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct RadRequest {
+  // frequency domain: entries = n_obs x n_e ; power density: entries = n_obs
+  bool power_density = false;
+  const double* obs = nullptr;      // 3*n_obs
+  const double* normals = nullptr;  // 3*n_obs or NULL
+  int64_t n_obs = 0;
+  std::vector<double> omega;        // n_e angular frequencies
+  bool obs_on_device = false;
+  bool directional = false;
+  osc_rad_opts opts{};
+  bool spectrum_current_abs = false;  // spectrum uses |I| in C2 (src/OSCARSSR.cc:1888)
+  double* out = nullptr;            // n_items
+  int32_t* level_out = nullptr;
+  bool out_on_device = false;
+  cudaStream_t stream = nullptr;
+};
+
+class Engine {
+ public:
+  explicit Engine(int device);
+  ~Engine();
+
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Model model;
+  std::string last_error;
+  long long last_samples = 0, last_launches = 0;
+  long long last_not_converged = 0;
+
+  // Run one radiation request for the current model state (single or multi particle).
+  void radiation(RadRequest& rq);
+
+  // profiling of the sample-integration kernels
+  bool profiling = false;
+  double prof_ms = 0;
+  long long prof_launches = 0, prof_samples = 0;
+  void drop_level_cache() { lev_filled_ = -1; bdmax_valid_ = false; levels_dropped_ = true; }
+  double measure_fma_peak(int kind);
+
+ private:
+  // trajectory on device
+  DevBuf knots_;
+  uint64_t knots_version_ = ~0ull;
+  int64_t nknots_ = 0;
+  double tstart_ = 0, tstop_ = 0;
+  // level cache
+  DevBuf lev_;
+  int64_t lev_cap_ = 0;
+  int lev_filled_ = -1;
+  DevBuf bd_bits_;                 // 32 x u64
+  std::vector<double> bdmax_;      // per level, host copy
+  bool bdmax_valid_ = false;
+  bool levels_dropped_ = false;
+  std::vector<cudaEvent_t> ev_pool_;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending_;
+  std::pair<cudaEvent_t, cudaEvent_t> timed_begin(cudaStream_t st);
+  void timed_end(std::pair<cudaEvent_t, cudaEvent_t> e, cudaStream_t st);
+  void collect_timings();
+  // request scratch
+  DevBuf obs_, nrm_, omega_, out_, lvl_, state_, part_, act_[2], cnt_;
+  DevBuf acc_, acc_comp_;          // multi-particle compensated accumulation
+
+  void upload_trajectory();
+  void ensure_levels(int L);
+  void refresh_bdmax();
+  void run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,
+                  cudaStream_t st);
+  void check(cudaError_t e, const char* what);
+};
+
+}  // namespace osc

@@ -1,0 +1,443 @@
+// host_core.cc -- host model of the radiation path (see host_core.h).  Every expression keeps the
+// association order of the reference expression it reproduces (file:line of the OSCARS sources).
+#include "host_core.h"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <thread>
+
+#include "../../include/oscars_b200.h"
+
+namespace osc {
+
+Vec3 orthogonal(Vec3 a) {  // include/TVector3D.h:132-142
+  double xx = a.x < 0.0 ? -a.x : a.x;
+  double yy = a.y < 0.0 ? -a.y : a.y;
+  double zz = a.z < 0.0 ? -a.z : a.z;
+  if (xx < yy) return xx < zz ? v3(0, a.z, -a.y) : v3(a.y, -a.x, 0);
+  return yy < zz ? v3(-a.z, 0, a.x) : v3(a.y, -a.x, 0);
+}
+
+Vec3 rotate_about(Vec3 o, double A, Vec3 axis) {  // TVector3D::RotateSelf (Rodrigues matrix)
+  Vec3 v = unit(axis);
+  double c = std::cos(A), s = std::sin(A);
+  double m00 = c + v.x * v.x * (1 - c), m01 = v.x * v.y * (1 - c) - v.z * s;
+  double m02 = v.x * v.z * (1 - c) + v.y * s, m10 = v.y * v.x * (1 - c) + v.z * s;
+  double m11 = c + v.y * v.y * (1 - c), m12 = v.y * v.z * (1 - c) - v.x * s;
+  double m20 = v.z * v.x * (1 - c) - v.y * s, m21 = v.z * v.y * (1 - c) + v.x * s;
+  double m22 = c + v.z * v.z * (1 - c);
+  return {m00 * o.x + m01 * o.y + m02 * o.z, m10 * o.x + m11 * o.y + m12 * o.z,
+          m20 * o.x + m21 * o.y + m22 * o.z};
+}
+
+Vec3 rotate_xyz(Vec3 v, Vec3 r) {  // TVector3D::RotateSelfX, Y, Z in that order
+  double s = std::sin(r.x), c = std::cos(r.x), t = v.y;
+  v.y = c * t - s * v.z;
+  v.z = s * t + c * v.z;
+  s = std::sin(r.y); c = std::cos(r.y); t = v.z;
+  v.z = c * t - s * v.x;
+  v.x = s * t + c * v.x;
+  s = std::sin(r.z); c = std::cos(r.z); t = v.x;
+  v.x = c * t - s * v.y;
+  v.y = s * t + c * v.y;
+  return v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fields
+// ---------------------------------------------------------------------------------------------
+void FieldSpec::finish() {  // TField3D_IdealUndulator::Init :94-98
+  period_length = mag(period);
+  period_unit = unit(period);
+  length = mag(period) * (nperiods + 2);
+}
+
+// One sinusoidal block with 1/4 and 3/4 end poles (src/TField3D_IdealUndulator.cc:125-142).
+static Vec3 pole_block(const FieldSpec& f, Vec3 amp, double d, double shift, double taper_corr) {
+  const double L = f.length, lam = f.period_length;
+  if (d > L / 2. + shift || d < -L / 2. + shift) return Vec3{};
+  const double s = std::sin(two_pi() * (d - shift) / lam);
+  if (d < -L / 2. + shift + lam || d > L / 2. + shift - lam) {
+    if (d < -L / 2. + shift + lam / 2. || d > L / 2. + shift - lam / 2.)
+      return amp * 0.25 * s * taper_corr;
+    return amp * 0.75 * s * taper_corr;
+  }
+  return amp * s * taper_corr;
+}
+
+Vec3 field_value(const FieldSpec& f, Vec3 x, double t) {
+  const double d = dot(x - f.center, f.period_unit);
+  const double taper_corr = 1 + d * f.taper;
+  Vec3 F;
+  if (f.kind == 0) {
+    F = pole_block(f, f.a, d, f.phase * mag(f.period) / two_pi(), taper_corr);
+  } else {  // src/TField3D_IdealEPU.cc:127-165: A shifted by +phase/2, B by -phase/2
+    F = pole_block(f, f.a, d, f.phase / 2. * mag(f.period) / two_pi(), taper_corr);
+    F = F + pole_block(f, f.b, d, -f.phase / 2. * mag(f.period) / two_pi(), taper_corr);
+  }
+  if (f.frequency == 0) return F;
+  return F * std::cos(two_pi() * f.frequency * (t + f.time_offset) + f.frequency_phase);
+}
+
+Vec3 field_sum(const std::vector<FieldSpec>& fields, Vec3 x, double t) {  // TFieldContainer::GetF
+  Vec3 s{0, 0, 0};
+  for (const FieldSpec& f : fields) s = s + field_value(f, x, t);
+  return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Particle / beam
+// ---------------------------------------------------------------------------------------------
+void Particle::set_conditions(Vec3 x, Vec3 b, double t) {  // TParticleA.cc SetGamma/SetQoverMGamma
+  x0 = x; b0 = b; t0 = t;
+  const double beta2 = mag2(b) > 0 ? mag2(b) : 0;
+  if (beta2 != 1) {
+    gamma = beta2 != 0 ? 1.0 / std::sqrt(1.0 - beta2) : 1;
+    if (!(m == 0 || gamma == 0)) qomg = q / m / gamma;
+  }
+  set = true;
+}
+
+void BeamSpec::twiss_at_x0() {  // TParticleBeam::SetTwissParametersAtX0
+  const Vec3 dx = x0 - lattice_ref;
+  const double D = mag(dx);
+  const double L = dot(dx, u0) >= 0 ? D : -1. * D;
+  for (int i = 0; i < 2; ++i) {
+    beta_x0[i] = tw_beta[i] - 2 * L * tw_alpha[i] + L * L * tw_gamma[i];
+    alpha_x0[i] = tw_alpha[i] - L * tw_gamma[i];
+    gamma_x0[i] = tw_gamma[i];
+  }
+}
+
+void Model::add_field(const FieldSpec& f) {
+  fields.push_back(f);
+  fields.back().finish();
+  knots.clear();  // OSCARSSR::AddMagneticField clears the particle's trajectory
+  ++knots_version;
+}
+
+void Model::clear_fields() {
+  fields.clear();
+  knots.clear();
+  ++knots_version;
+}
+
+void Model::set_ctstartstop(double a, double b) {  // OSCARSSR::SetCTStartStop (:637-647)
+  npoints = (int64_t)(npoints_per_meter * (b - a));
+  ctstart = a;
+  ctstop = b;
+}
+
+void Model::ideal_particle() {  // TParticleBeam::GetNewParticle("ideal") (:667-688)
+  const double g = beam.e0 / kg_to_gev(beam.m) < 1 ? 1 : beam.e0 / kg_to_gev(beam.m);
+  const double b = g != 1 ? std::sqrt(1.0 - 1.0 / (g * g)) : 0;
+  particle = Particle{};
+  particle.q = beam.q;
+  particle.m = beam.m;
+  particle.current = beam.current;
+  particle.set_conditions(beam.x0, beam.u0 * b, beam.t0);
+  knots.clear();
+  ++knots_version;
+}
+
+void Model::random_particle() {  // TParticleBeam::GetNewParticle() (:692-850)
+  if (beam.distribution != 2 && beam.distribution != 3) {
+    ideal_particle();
+    return;
+  }
+  const double PI = kPi;
+  const double mg = kg_to_gev(beam.m);
+  double enew = beam.e0 + beam.sigma_e * rng.normal(rng.mt);
+  if (enew < mg) enew = mg;
+  const double ge = enew / mg < 1 ? 1 : enew / mg;
+  const double beta = ge != 1 ? std::sqrt(1.0 - 1.0 / (ge * ge)) : 0;
+  const double de = (enew - beam.e0) / beam.e0;
+  Vec3 xn = beam.x0;
+  Vec3 bn = cross(beam.hdir, beam.vdir) * beta;
+  auto U = [&]() { return rng.uniform(rng.mt); };
+  if (beam.distribution == 2) {
+    if (beam.emit[0] * beam.emit[0] + beam.emit[1] * beam.emit[1] > 1e-99) {
+      const int hc = beam.alpha_x0[0] > 0 ? -1 : 1, vc = beam.alpha_x0[1] > 0 ? -1 : 1;
+      const double hsx = std::sqrt(beam.emit[0] * beam.beta_x0[0]);
+      const double hsxp = std::sqrt(beam.emit[0] * beam.gamma_x0[0]);
+      const double hr = beam.emit[0] / (hsx * hsxp);
+      const double hrho = std::sqrt(1 - hr * hr);
+      const double vsx = std::sqrt(beam.emit[1] * beam.beta_x0[1]);
+      const double vsxp = std::sqrt(beam.emit[1] * beam.gamma_x0[1]);
+      const double vr = beam.emit[1] / (vsx * vsxp);
+      const double vrho = std::sqrt(1 - vr * vr);
+      const double hu = U(), hv = U();
+      const double hX = hsx * std::sqrt(-2 * std::log(hu)) *
+                        (std::sqrt(1 - hrho * hrho) * std::cos(2 * PI * hv) + hrho * std::sin(2 * PI * hv));
+      const double hXP = hc * hsxp * std::sqrt(-2 * std::log(hu)) * std::sin(2 * PI * hv);
+      const double vu = U(), vv = U();
+      const double vX = vsx * std::sqrt(-2 * std::log(vu)) *
+                        (std::sqrt(1 - vrho * vrho) * std::cos(2 * PI * vv) + vrho * std::sin(2 * PI * vv));
+      const double vXP = vc * vsxp * std::sqrt(-2 * std::log(vu)) * std::sin(2 * PI * vv);
+      // `X += H * hX + eta * dE/E` adds the scalar term to each component
+      const double eh = beam.eta[0] * de, ev = beam.eta[1] * de;
+      const Vec3 th = beam.hdir * hX, tv = beam.vdir * vX;
+      xn = xn + v3(th.x + eh, th.y + eh, th.z + eh);
+      xn = xn + v3(tv.x + ev, tv.y + ev, tv.z + ev);
+      bn = rotate_about(bn, hXP, beam.vdir);
+      bn = rotate_about(bn, vXP, -beam.hdir);
+    }
+  } else {  // KV
+    const int hc = beam.alpha_x0[0] > 0 ? -1 : 1, vc = beam.alpha_x0[1] > 0 ? -1 : 1;
+    const double hT = U() * 2 * PI;
+    const double vT = U() * 2 * PI;
+    const double hAX = std::sqrt(beam.emit[0] * beam.beta_x0[0]) * std::cos(hT);
+    const double vAX = std::sqrt(beam.emit[1] * beam.beta_x0[1]) * std::cos(vT);
+    const double hAXP = -std::sqrt(beam.emit[0] / beam.beta_x0[0]) * (beam.alpha_x0[0] * std::cos(hT) + std::sin(hT));
+    const double vAXP = -std::sqrt(beam.emit[1] / beam.beta_x0[1]) * (beam.alpha_x0[1] * std::cos(vT) + std::sin(vT));
+    const double hR = std::sqrt(hAX * hAX + hAXP * hAXP), vR = std::sqrt(vAX * vAX + vAXP * vAXP);
+    double hRT = std::atan(hAXP / hAX), vRT = std::atan(vAXP / vAX);
+    if (hAX < 0 && hAXP > 0) hRT += PI; else if (hAX < 0 && hAXP < 0) hRT -= PI;
+    if (vAX < 0 && vAXP > 0) vRT += PI; else if (vAX < 0 && vAXP < 0) vRT -= PI;
+    const double hNR = std::sqrt(U()) * hR;
+    const double vNR = std::sqrt(U()) * vR;
+    xn = xn + beam.hdir * (hNR * std::cos(hRT));
+    xn = xn + beam.vdir * (vNR * std::cos(vRT));
+    bn = rotate_about(bn, hNR * std::sin(hRT) * hc, beam.vdir);
+    bn = rotate_about(bn, vNR * std::sin(vRT) * vc, -beam.hdir);
+  }
+  particle = Particle{};
+  particle.q = beam.q;
+  particle.m = beam.m;
+  particle.current = beam.current;
+  particle.set_conditions(xn, bn, beam.t0);
+  knots.clear();
+  ++knots_version;
+}
+
+// ---------------------------------------------------------------------------------------------
+// RK4 (src/OSCARSSR.cc:910-1009 driver, :1247-1279 DerivativesB, :1321-1386 RK4 step)
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+struct Integrator {
+  const std::vector<FieldSpec>& fields;
+  double qomg;
+  bool error_gamma = false;
+
+  void derivs(double t, const double* x, double* dxdt) {
+    const double one_minus = (1. - (x[1] * x[1] + x[3] * x[3] + x[5] * x[5]) / (kC * kC));
+    if (one_minus <= 0) {  // leaves dxdt untouched, as the reference does
+      error_gamma = true;
+      return;
+    }
+    const Vec3 B = field_sum(fields, v3(x[0], x[2], x[4]), t);
+    dxdt[0] = x[1];
+    dxdt[1] = qomg * (-x[5] * B.y + x[3] * B.z);
+    dxdt[2] = x[3];
+    dxdt[3] = qomg * (x[5] * B.x - x[1] * B.z);
+    dxdt[4] = x[5];
+    dxdt[5] = qomg * (x[1] * B.y - x[3] * B.x);
+  }
+
+  // y and yout may alias; dydx is overwritten by the step-halving branch like the reference's.
+  void step(const double* y, double* dydx, double x, double h, double* yout) {
+    double dym[6], dyt[6], yt[6], yo[6];
+    const double hh = h * 0.5, h6 = h / 6.0, xh = x + hh;
+    for (int i = 0; i < 6; ++i) yt[i] = y[i] + hh * dydx[i];
+    derivs(xh, yt, dyt);
+    for (int i = 0; i < 6; ++i) yt[i] = y[i] + hh * dyt[i];
+    derivs(xh, yt, dym);
+    for (int i = 0; i < 6; ++i) {
+      yt[i] = y[i] + h * dym[i];
+      dym[i] += dyt[i];
+    }
+    derivs(x + h, yt, dyt);
+    for (int i = 0; i < 6; ++i) yo[i] = y[i] + h6 * (dydx[i] + dyt[i] + 2.0 * dym[i]);
+    const bool this_err = 1. - (yo[1] * yo[1] + yo[3] * yo[3] + yo[5] * yo[5]) / (kC * kC) <= 0;
+    if (error_gamma || this_err) {
+      error_gamma = false;
+      double yhalf[6], ysave[6];
+      for (int i = 0; i < 6; ++i) ysave[i] = y[i];
+      derivs(x, ysave, dydx);
+      step(ysave, dydx, x, h / 2., yhalf);
+      derivs(x + h / 2., yhalf, dydx);
+      step(yhalf, dydx, x + h / 2., h / 2., yo);
+    }
+    for (int i = 0; i < 6; ++i) yout[i] = yo[i];
+  }
+};
+
+inline void push_point(std::vector<double>& buf, const double* x, const double* dxdt, double t) {
+  buf.push_back(t);
+  buf.push_back(x[0]); buf.push_back(x[2]); buf.push_back(x[4]);
+  buf.push_back(x[1] / kC); buf.push_back(x[3] / kC); buf.push_back(x[5] / kC);
+  buf.push_back(dxdt[1] / kC); buf.push_back(dxdt[3] / kC); buf.push_back(dxdt[5] / kC);
+}
+
+}  // namespace
+
+void Model::compute_trajectory() {
+  const Particle& P = particle;
+  if (!P.set) throw Error{OSC_ERR_RANGE, "particle not initialized.  make sure you have a particle or beam defined"};
+  if (ctstart > P.t0 || ctstop < P.t0)
+    throw Error{OSC_ERR_RANGE, "start time is greater than T0 or stop time is less than T0"};
+  if (ctstart >= ctstop)
+    throw Error{OSC_ERR_RANGE, "start time is greater than stop time.  check that set_ctstartstop is set"};
+  knots.clear();
+  ++knots_version;
+  const double dt = ((ctstop - ctstart) / kC / (npoints - 1));
+  const size_t nf = (size_t)(1 + (ctstop - P.t0) / kC / dt);
+  const size_t nb = (size_t)((P.t0 - ctstart) / kC / dt);
+
+  // The forward and backward sweeps are independent integrations from the same initial state; they
+  // run on two host threads and are stitched together afterwards (backward reversed, then forward).
+  std::vector<double> fwd, bwd;
+  fwd.reserve(10 * nf);
+  bwd.reserve(10 * nb);
+  auto forward = [&]() {
+    Integrator I{fields, P.qomg};
+    double x[6] = {P.x0.x, P.b0.x * kC, P.x0.y, P.b0.y * kC, P.x0.z, P.b0.z * kC};
+    double dxdt[6] = {0, 0, 0, 0, 0, 0};
+    I.derivs(P.t0 / kC, x, dxdt);
+    for (size_t i = 0; i != nf; ++i) {
+      const double t = P.t0 / kC + dt * i;
+      if (i == 0) I.derivs(t, x, dxdt);
+      push_point(fwd, x, dxdt, t);
+      I.derivs(t, x, dxdt);
+      I.step(x, dxdt, t, dt, x);
+    }
+  };
+  auto backward = [&]() {
+    Integrator I{fields, P.qomg};
+    double x[6] = {P.x0.x, P.b0.x * kC, P.x0.y, P.b0.y * kC, P.x0.z, P.b0.z * kC};
+    double dxdt[6] = {0, 0, 0, 0, 0, 0};
+    const double dtr = -dt;
+    for (size_t i = 0; i != nb; ++i) {
+      const double t1 = P.t0 / kC + dtr * (i);
+      const double t2 = P.t0 / kC + dtr * (i + 1);
+      I.derivs(t1, x, dxdt);
+      I.step(x, dxdt, t1, dtr, x);
+      push_point(bwd, x, dxdt, t2);
+    }
+  };
+  if (nf + nb > 4096) {
+    std::thread th(backward);
+    forward();
+    th.join();
+  } else {
+    forward();
+    backward();
+  }
+  const int64_t n = (int64_t)(nf + nb);
+  if (n < 2) throw Error{OSC_ERR_LENGTH, "Not enough points in this trajectory"};
+  if (n < 3) throw Error{OSC_ERR_LENGTH, "TSpline1D3 does not see enough points for interpolation.  Please use >= 3 points"};
+  knots.n = n;
+  knots.t.resize(n);
+  knots.y.resize(9 * n);
+  for (int64_t j = 0; j < (int64_t)nb; ++j) {  // backward points, earliest first
+    const double* r = &bwd[10 * (nb - 1 - j)];
+    knots.t[j] = r[0];
+    for (int c = 0; c < 9; ++c) knots.y[c * n + j] = r[1 + c];
+  }
+  for (int64_t j = 0; j < (int64_t)nf; ++j) {
+    const double* r = &fwd[10 * j];
+    knots.t[nb + j] = r[0];
+    for (int c = 0; c < 9; ++c) knots.y[c * n + nb + j] = r[1 + c];
+  }
+  knots.tstart = knots.t.front();
+  knots.tstop = knots.t.back();
+  spline_second_derivatives(knots);
+}
+
+void Model::ensure_trajectory() {
+  if (!particle.set) {
+    if (!has_beam) throw Error{OSC_ERR_RANGE, "no beam defined"};
+    random_particle();
+  }
+  if (knots.n == 0) compute_trajectory();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Spline (include/TOMATH.h:141-203): the diagonal recurrence depends only on the knot times, so it
+// is shared by the 9 components; each component's right-hand side sweep runs on its own.
+// ---------------------------------------------------------------------------------------------
+void spline_second_derivatives(Knots& k) {
+  const int64_t N = k.n;
+  const double* X = k.t.data();
+  k.ypp.assign(9 * N, 0.0);
+  std::vector<double> diag(N), sigv(N), pv(N);
+  diag[0] = -0.5;
+  for (int64_t i = 1; i < N - 1; ++i) {
+    const double sig = (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]);
+    const double p = sig * diag[i - 1] + 2;
+    diag[i] = (sig - 1.) / p;
+    sigv[i] = sig;
+    pv[i] = p;
+  }
+  auto component = [&](int c) {
+    const double* Y = k.y.data() + c * N;
+    double* ypp = k.ypp.data() + c * N;
+    std::vector<double> u(N);
+    const double dydx0 = (Y[1] - Y[0]) / (X[1] - X[0]);
+    u[0] = (3. / (X[1] - X[0])) * ((Y[1] - Y[0]) / (X[1] - X[0]) - dydx0);
+    for (int64_t i = 1; i < N - 1; ++i) {
+      double ui = (Y[i + 1] - Y[i]) / (X[i + 1] - X[i]) - (Y[i] - Y[i - 1]) / (X[i] - X[i - 1]);
+      u[i] = (6. * ui / (X[i + 1] - X[i - 1]) - sigv[i] * u[i - 1]) / pv[i];
+    }
+    const double qn = 0.5;
+    const double dydxN = (Y[N - 1] - Y[N - 2]) / (X[N - 1] - X[N - 2]);
+    const double un = (3. / (X[N - 1] - X[N - 2])) * (dydxN - (Y[N - 1] - Y[N - 2]) / (X[N - 1] - X[N - 2]));
+    for (int64_t i = 0; i < N - 1; ++i) ypp[i] = diag[i];
+    ypp[N - 1] = (un - qn * u[N - 2]) / (qn * diag[N - 2] + 1.);
+    for (int64_t j = N - 2; j >= 0; --j) ypp[j] = ypp[j] * ypp[j + 1] + u[j];
+  };
+  if (N > 4096) {
+    std::vector<std::thread> pool;
+    for (int c = 0; c < 9; ++c) pool.emplace_back(component, c);
+    for (auto& th : pool) th.join();
+  } else {
+    for (int c = 0; c < 9; ++c) component(c);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Rectangle surface (src/TSurfacePoints_Rectangle.cc:140-315)
+// ---------------------------------------------------------------------------------------------
+void surface_rectangle(const std::string& plane_in, int nx1, int nx2, double w1, double w2, Vec3 rot,
+                       Vec3 trans, int normal, double* xyz, double* normals, double* x1x2) {
+  std::string P = plane_in;
+  std::transform(P.begin(), P.end(), P.begin(), ::toupper);
+  const double s1 = nx1 > 1 ? w1 / (nx1 - 1) : 0;
+  const double s2 = nx2 > 1 ? w2 / (nx2 - 1) : 0;
+  // start for (both>1, both<=1, nx1<=1, nx2<=1), step vectors and normal per plane
+  struct Layout { Vec3 both, none, only2, only1, v1, v2, n; };
+  Layout L;
+  if (P == "XY") L = {v3(-w1 / 2., -w2 / 2., 0), v3(0, 0, 0), v3(0., -w2 / 2., 0), v3(-w1 / 2., 0, 0), v3(s1, 0, 0), v3(0, s2, 0), v3(0, 0, 1)};
+  else if (P == "YX") L = {v3(-w2 / 2., -w1 / 2., 0), v3(0, 0, 0), v3(-w2 / 2., 0, 0), v3(0, -w1 / 2., 0), v3(0, s1, 0), v3(s2, 0, 0), v3(0, 0, -1)};
+  else if (P == "XZ") L = {v3(-w1 / 2., 0, -w2 / 2.), v3(0, 0, 0), v3(0, 0, -w2 / 2.), v3(-w1 / 2., 0, 0), v3(s1, 0, 0), v3(0, 0, s2), v3(0, -1, 0)};
+  else if (P == "ZX") L = {v3(-w2 / 2., 0, -w1 / 2.), v3(0, 0, 0), v3(-w2 / 2., 0, 0), v3(0., 0, -w1 / 2.), v3(0, 0, s1), v3(s2, 0, 0), v3(0, 1, 0)};
+  else if (P == "YZ") L = {v3(0, -w1 / 2., -w2 / 2.), v3(0, 0, 0), v3(0, 0, -w2 / 2.), v3(0, -w1 / 2., 0), v3(0, s1, 0), v3(0, 0, s2), v3(1, 0, 0)};
+  else if (P == "ZY") L = {v3(0, -w2 / 2., -w1 / 2.), v3(0, 0, 0), v3(0, -w2 / 2., 0), v3(0, 0, -w1 / 2.), v3(0, 0, s1), v3(0, s2, 0), v3(-1, 0, 0)};
+  else throw Error{OSC_ERR_INVALID, "not a valid surface string: XY YX XZ ZX YZ ZY"};
+  Vec3 st = (nx1 > 1 && nx2 > 1) ? L.both : (nx1 <= 1 && nx2 <= 1) ? L.none : (nx1 <= 1) ? L.only2 : L.only1;
+  st = rotate_xyz(st, rot);
+  const Vec3 v1 = rotate_xyz(L.v1, rot), v2 = rotate_xyz(L.v2, rot);
+  st = st + trans;
+  Vec3 nv = rotate_xyz(L.n, rot);
+  if (normal == -1) nv = nv * -1;
+  else if (normal != 0 && normal != 1) throw Error{OSC_ERR_INVALID, "normal must be -1, 0, or 1"};
+  const double m1 = mag(v1), m2 = mag(v2);
+  const int64_t n = (int64_t)nx1 * nx2;
+  for (int64_t i = 0; i < n; ++i) {
+    const int ix1 = (int)(i / nx2), ix2 = (int)(i % nx2);
+    if (xyz) {
+      const Vec3 p = (st + v1 * (double)ix1) + v2 * (double)ix2;
+      xyz[3 * i] = p.x; xyz[3 * i + 1] = p.y; xyz[3 * i + 2] = p.z;
+    }
+    if (normals) { normals[3 * i] = nv.x; normals[3 * i + 1] = nv.y; normals[3 * i + 2] = nv.z; }
+    if (x1x2) {
+      x1x2[3 * i] = s1 * ix1 - m1 * (nx1 - 1) / 2.;
+      x1x2[3 * i + 1] = s2 * ix2 - m2 * (nx2 - 1) / 2.;
+      x1x2[3 * i + 2] = 0;
+    }
+  }
+}
+
+}  // namespace osc

@@ -1,0 +1,141 @@
+// host_core.h -- host-side model of the OSCARS radiation path: fields, beam sampling, the FP64
+// RK4 trajectory and its clamped cubic spline.  Everything here reproduces the reference's double
+// arithmetic operation for operation (built with -ffp-contract=off), so trajectories and spline
+// coefficients are bit-identical to the reference CPU build; the GPU kernels start from them.
+#pragma once
+
+#include <cstdint>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace osc {
+
+// Constants of include/TOSCARS.h:20-76 (older CODATA values, kept for parity).
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kC = 2.99792458e8;
+constexpr double kH = 6.62606876e-34;
+constexpr double kHbar = 1.054571596e-34;
+constexpr double kQe = 1.602176462e-19;
+constexpr double kMe = 9.10938356e-31;
+constexpr double kEps0 = 8.854187817E-12;
+constexpr double kMu0 = 1.2566370614E-6;
+constexpr double kSqrt2Pi = 2.5066282746310002416123552393401;
+constexpr int kMaxLevelMemory = 26;  // TParticleA::kMaxTrajectoryLevel
+
+inline double two_pi() { return 2.0 * kPi; }
+inline double four_pi() { return 4.0 * kPi; }
+inline double kg_to_gev(double m) { return 1e-9 * m * kC * kC / kQe; }
+inline double gev_to_kg(double m) { return kQe * m / (1e-9 * kC * kC); }
+inline double ev_to_omega(double e) { return e * kQe / kHbar; }
+
+struct Vec3 {
+  double x = 0, y = 0, z = 0;
+};
+inline Vec3 v3(double x, double y, double z) { return Vec3{x, y, z}; }
+inline Vec3 operator+(Vec3 a, Vec3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline Vec3 operator-(Vec3 a, Vec3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline Vec3 operator-(Vec3 a) { return {-a.x, -a.y, -a.z}; }
+inline Vec3 operator*(Vec3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline Vec3 operator/(Vec3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+inline double mag2(Vec3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+inline double mag(Vec3 a) { return __builtin_sqrt(mag2(a)); }
+inline double dot(Vec3 a, Vec3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline Vec3 cross(Vec3 a, Vec3 b) {
+  return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+inline Vec3 unit(Vec3 a) { return a / mag(a); }
+Vec3 orthogonal(Vec3 a);
+Vec3 rotate_about(Vec3 v, double angle, Vec3 axis);  // TVector3D::RotateSelf
+Vec3 rotate_xyz(Vec3 v, Vec3 r);                       // TVector3D::RotateSelfXYZ
+
+// One magnetic field source; `kind` 0 = ideal planar undulator, 1 = ideal EPU.
+struct FieldSpec {
+  int kind = 0;
+  Vec3 a, b, period, center;
+  int nperiods = 0;
+  double phase = 0, taper = 0, frequency = 0, frequency_phase = 0, time_offset = 0;
+  double period_length = 0, length = 0;
+  Vec3 period_unit;
+  void finish();  // derived quantities, TField3D_IdealUndulator::Init
+};
+
+Vec3 field_value(const FieldSpec& f, Vec3 x, double t);
+Vec3 field_sum(const std::vector<FieldSpec>& fields, Vec3 x, double t);
+
+struct Particle {
+  double q = 0, m = 0, gamma = 0, qomg = 0, current = 0;
+  Vec3 x0, b0;
+  double t0 = 0;
+  bool set = false;
+  void set_conditions(Vec3 x, Vec3 b, double t);  // TParticleA::SetInitialParticleConditions
+};
+
+struct BeamSpec {
+  double q = 0, m = 0, current = 0, e0 = 0, t0 = 0;
+  Vec3 x0, u0, hdir, vdir;
+  double sigma_e = 0;
+  double emit[2] = {0, 0}, eta[2] = {0, 0};
+  double tw_beta[2] = {0, 0}, tw_alpha[2] = {0, 0}, tw_gamma[2] = {0, 0};
+  double beta_x0[2] = {0, 0}, alpha_x0[2] = {0, 0}, gamma_x0[2] = {0, 0};
+  Vec3 lattice_ref;
+  int distribution = 1;  // 1 filament, 2 gaussian, 3 KV
+  void twiss_at_x0();
+};
+
+// libstdc++ engine and distributions, exactly as src/TRandomA.cc uses them.
+struct Rng {
+  std::mt19937 mt{5489u};
+  std::normal_distribution<double> normal{0.0, 1.0};
+  std::uniform_real_distribution<double> uniform{0.0, 1.0};
+  void seed(int s) {
+    mt = std::mt19937(s);
+    normal = std::normal_distribution<double>(0.0, 1.0);
+    uniform = std::uniform_real_distribution<double>(0.0, 1.0);
+  }
+};
+
+// RK4 knots and their spline second derivatives, SoA: t[n]; y[9][n] = x y z bx by bz ax ay az
+// (a = acceleration / c); ypp[9][n].
+struct Knots {
+  int64_t n = 0;
+  std::vector<double> t, y, ypp;
+  double tstart = 0, tstop = 0;
+  void clear() { n = 0; t.clear(); y.clear(); ypp.clear(); }
+};
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+class Model {
+ public:
+  std::vector<FieldSpec> fields;
+  BeamSpec beam;
+  bool has_beam = false;
+  Particle particle;
+  double ctstart = 0, ctstop = 0;
+  int64_t npoints = 0, npoints_per_meter = 10000;
+  Rng rng;
+  Knots knots;
+  uint64_t knots_version = 0;  // bumps whenever `knots` changes
+
+  void add_field(const FieldSpec& f);
+  void clear_fields();
+  void set_ctstartstop(double a, double b);
+  void ideal_particle();
+  void random_particle();
+  // Throws osc::Error on failure.
+  void compute_trajectory();
+  void ensure_trajectory();
+};
+
+// Spline second derivatives of the 9 components (TSpline1D3::Derivatives, include/TOMATH.h:141-203).
+void spline_second_derivatives(Knots& k);
+
+// Rectangle surface (TSurfacePoints_Rectangle).  Throws osc::Error.
+void surface_rectangle(const std::string& plane, int nx1, int nx2, double w1, double w2, Vec3 rot,
+                       Vec3 trans, int normal, double* xyz, double* normals, double* x1x2);
+
+}  // namespace osc

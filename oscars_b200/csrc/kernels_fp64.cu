@@ -1,0 +1,525 @@
+// kernels_fp64.cu -- the reference's FP64 method on sm_100a.
+//
+// Level samples (trajectory spline evaluated at the level-ladder times), the frequency-domain
+// (flux / spectrum) and time-domain (power density) sums over those samples, and the per-level
+// convergence tests.  Every operation whose rounding can move the retarded phase or the
+// 1 - n.beta denominators is written with explicit round-to-nearest intrinsics in the reference's
+// association order, so those quantities are bit-identical to the reference CPU build; only the
+// order of the final summation and the last-ulp behaviour of sin/cos/pow differ.
+//
+// Work decomposition ("waves"): every (observer, energy) entry that is still unconverged at level
+// L needs the 2^L samples of that level.  A wave launches one CTA per (128 entries x span of the
+// level); each thread owns one entry and walks the span's samples, which a single elected thread
+// stages into shared memory with 1-D TMA bulk copies (double buffered, mbarrier completion).
+// All threads read the same sample at the same time (shared-memory broadcast).  Per-span partial
+// sums go to global memory and a finalize kernel reduces them in span order, applies the
+// reference's stop rule and compacts the still-active entries for the next wave.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace osc {
+namespace dev {
+
+constexpr double kCLight = 2.99792458e8;
+constexpr double kPiD = 3.14159265358979323846;
+
+// ---------------------------------------------------------------------------------------------
+// Level samples: TParticleTrajectoryInterpolated::FillTParticleTrajectoryPointsLevel
+// (src/TParticleTrajectoryInterpolated.cc:124-158) + TSpline1D3::GetValue (include/TOMATH.h:92-121).
+// Sample i of level L lives at index 2^L + i of each of the 10 SoA arrays (index 0 unused), so the
+// union of levels 0..L is the contiguous range [1, 2^(L+1)) and every level starts 16-byte aligned.
+// ---------------------------------------------------------------------------------------------
+__global__ void k_level_fill(const double* __restrict__ knots, int64_t n, double tstart, double tstop,
+                             int64_t s_begin, int64_t s_end, double* __restrict__ lev, int64_t cap,
+                             int extended_level) {
+  const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= s_end) return;
+  const double* t = knots;
+  const double* y = knots + n;
+  const double* ypp = knots + 10 * n;
+  int L;
+  int64_t i;
+  double ts, sp;
+  if (extended_level >= 0) {  // extended level: spacing T/(2^L - 1), stored at [0, 2^L)
+    L = extended_level;
+    i = s;
+    ts = __dadd_rn(tstart, __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L + 1)));
+    sp = __ddiv_rn(__dsub_rn(tstop, tstart), __dsub_rn(ldexp(1.0, L), 1.0));
+  } else {
+    L = 63 - __clzll((unsigned long long)s);
+    i = s - ((int64_t)1 << L);
+    ts = __dadd_rn(tstart, __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L + 1)));
+    sp = __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L));
+  }
+  const double T = __dadd_rn(ts, __dmul_rn(sp, (double)i));
+  // Interval search: same result as the reference's bisection (largest klo in [0, n-2] with
+  // t[klo] <= T), started from the uniform-spacing estimate and corrected by local steps.
+  int64_t k = (int64_t)((T - t[0]) / (t[n - 1] - t[0]) * (double)(n - 1));
+  k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+  while (k > 0 && t[k] > T) --k;
+  while (k < n - 2 && t[k + 1] <= T) ++k;
+  const int64_t klo = k, khi = k + 1;
+  const double h = __dsub_rn(t[khi], t[klo]);
+  const double a = __ddiv_rn(__dsub_rn(t[khi], T), h);
+  const double b = __ddiv_rn(__dsub_rn(T, t[klo]), h);
+  const double ca = __dsub_rn(__dmul_rn(__dmul_rn(a, a), a), a);
+  const double cb = __dsub_rn(__dmul_rn(__dmul_rn(b, b), b), b);
+  const double hh = __dmul_rn(h, h);
+  lev[s] = T;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    const double* Y = y + c * n;
+    const double* P = ypp + c * n;
+    const double lin = __dadd_rn(__dmul_rn(a, Y[klo]), __dmul_rn(b, Y[khi]));
+    const double cur = __ddiv_rn(__dmul_rn(__dadd_rn(__dmul_rn(ca, P[klo]), __dmul_rn(cb, P[khi])), hh), 6.0);
+    lev[(1 + c) * cap + s] = __dadd_rn(lin, cur);
+  }
+}
+
+// Per-level max |beta_i - beta_{i-1}| over i >= 1 (the power-density stop rule, src/OSCARSSR.cc:
+// 2887-2891).  Positive doubles order like their bit patterns, so atomicMax on the bits is exact.
+__global__ void k_level_betadiff(const double* __restrict__ lev, int64_t cap, int64_t s_begin, int64_t s_end,
+                                 unsigned long long* __restrict__ bdmax_bits, int extended_level) {
+  const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= s_end) return;
+  int L;
+  int64_t i;
+  if (extended_level >= 0) { L = extended_level; i = s; }
+  else { L = 63 - __clzll((unsigned long long)s); i = s - ((int64_t)1 << L); }
+  if (i == 0) return;
+  const double* bx = lev + 4 * cap;
+  const double* by = lev + 5 * cap;
+  const double* bz = lev + 6 * cap;
+  const double dx = __dsub_rn(bx[s], bx[s - 1]), dy = __dsub_rn(by[s], by[s - 1]), dz = __dsub_rn(bz[s], bz[s - 1]);
+  const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+  atomicMax(&bdmax_bits[L], (unsigned long long)__double_as_longlong(d));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Shared-memory staging of sample ranges.
+// ---------------------------------------------------------------------------------------------
+template <int NARR, int CH>
+struct Stage {
+  // CH + 2 slots so that a range whose start is rounded down to an even index still fits.
+  double v[2][NARR][CH + 2];
+  uint64_t bar[2];
+};
+
+// Issue the bulk copies of samples [lo_al, hi_al) of the NARR arrays into buffer `b`.
+template <int NARR, int CH>
+__device__ __forceinline__ void stage_issue(Stage<NARR, CH>& st, int b, const double* lev, int64_t cap,
+                                            int64_t lo_al, int64_t hi_al) {
+  const uint32_t bytes = (uint32_t)((hi_al - lo_al) * sizeof(double));
+  mbar_arrive_expect_tx(&st.bar[b], bytes * NARR);
+#pragma unroll
+  for (int k = 0; k < NARR; ++k) tma_load_1d(&st.v[b][k][0], lev + k * cap + lo_al, bytes, &st.bar[b]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Frequency-domain wave (flux / spectrum).  Integrand: src/OSCARSSR.cc:4202-4220 (flux) and
+// :1976-1989 (spectrum), both
+//   [ (1-b^2)(n-b) / (D^2 (1-n.b)^2) + n x ((n-b) x a/c) / (D (1-n.b)^2) ] exp(-i w (t + D/c)).
+// ---------------------------------------------------------------------------------------------
+constexpr int kFdThreads = 128;
+constexpr int kFdChunk = 128;
+
+__global__ void __launch_bounds__(kFdThreads) k_fd_wave_fp64(FdWaveArgs A) {
+  __shared__ __align__(16) Stage<10, kFdChunk> st;
+  const int tid = threadIdx.x;
+  const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
+  const int64_t slot = (int64_t)blockIdx.x * kFdThreads + tid;
+  if ((int64_t)blockIdx.x * kFdThreads >= n_act) return;  // whole CTA idle
+  const bool live = slot < n_act;
+  const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+  const int64_t io = item / A.n_e, ie = item % A.n_e;
+  const double Ox = A.obs[3 * io], Oy = A.obs[3 * io + 1], Oz = A.obs[3 * io + 2];
+  const double omega = A.omega[ie];
+  const double mw = -omega;
+  const int span = blockIdx.y;
+
+  if (tid == 0) {
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint32_t phase_bits = 0;  // parity of the next completion expected on each buffer
+
+  for (int g = 0; g < A.nseg; ++g) {
+    const int64_t b0 = A.seg_b[g] + (int64_t)span * A.span_len[g];
+    const int64_t b1 = min(A.seg_e[g], b0 + A.span_len[g]);
+    double sxr = 0, sxi = 0, syr = 0, syi = 0, szr = 0, szi = 0;
+    double first_phase = 0, last_phase = 0, dmax = 0;
+    bool have = false;
+    const int64_t nchunks = b1 > b0 ? (b1 - b0 + kFdChunk - 1) / kFdChunk : 0;
+    if (tid == 0 && nchunks > 0) {
+      const int64_t lo = b0, hi = min(b1, b0 + kFdChunk);
+      stage_issue<10, kFdChunk>(st, 0, A.lev, A.cap, lo & ~(int64_t)1, (hi + 1) & ~(int64_t)1);
+    }
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const int buf = (int)(c & 1);
+      const int64_t lo = b0 + c * kFdChunk, hi = min(b1, lo + kFdChunk);
+      if (tid == 0 && c + 1 < nchunks) {  // prefetch the next chunk into the other buffer
+        const int64_t lo2 = lo + kFdChunk, hi2 = min(b1, lo2 + kFdChunk);
+        stage_issue<10, kFdChunk>(st, buf ^ 1, A.lev, A.cap, lo2 & ~(int64_t)1, (hi2 + 1) & ~(int64_t)1);
+      }
+      if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+        if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+        return;
+      }
+      phase_bits ^= 1u << buf;
+      const int64_t lo_al = lo & ~(int64_t)1;
+      const double* sT = st.v[buf][0];
+      const double* sX = st.v[buf][1];
+      const double* sY = st.v[buf][2];
+      const double* sZ = st.v[buf][3];
+      const double* sBx = st.v[buf][4];
+      const double* sBy = st.v[buf][5];
+      const double* sBz = st.v[buf][6];
+      const double* sAx = st.v[buf][7];
+      const double* sAy = st.v[buf][8];
+      const double* sAz = st.v[buf][9];
+      const int j0 = (int)(max(lo, (int64_t)1) - lo_al);  // sample 0 is the unused slot
+      const int j1 = (int)(hi - lo_al);
+      if (live) {
+        for (int j = j0; j < j1; ++j) {
+          const double T = sT[j];
+          const double Rx = __dsub_rn(Ox, sX[j]), Ry = __dsub_rn(Oy, sY[j]), Rz = __dsub_rn(Oz, sZ[j]);
+          const double D = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz)));
+          const double ph = __dmul_rn(mw, __dadd_rn(T, __ddiv_rn(D, kCLight)));
+          if (have) {
+            const double dp = fabs(__dsub_rn(ph, last_phase));
+            dmax = dp > dmax ? dp : dmax;
+          } else {
+            first_phase = ph;
+            have = true;
+          }
+          last_phase = ph;
+          const double bx = sBx[j], by = sBy[j], bz = sBz[j];
+          const double nx = __ddiv_rn(Rx, D), ny = __ddiv_rn(Ry, D), nz = __ddiv_rn(Rz, D);
+          const double b2 = __dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz));
+          const double ndb = __dadd_rn(__dadd_rn(__dmul_rn(nx, bx), __dmul_rn(ny, by)), __dmul_rn(nz, bz));
+          const double om = __dsub_rn(1.0, ndb);
+          const double p2 = __dmul_rn(om, om);
+          const double den1 = __dmul_rn(__dmul_rn(D, D), p2);
+          const double den2 = __dmul_rn(D, p2);
+          const double ob2 = __dsub_rn(1.0, b2);
+          const double ux = __dsub_rn(nx, bx), uy = __dsub_rn(ny, by), uz = __dsub_rn(nz, bz);
+          const double ax = sAx[j], ay = sAy[j], az = sAz[j];
+          const double wx = __dsub_rn(__dmul_rn(uy, az), __dmul_rn(ay, uz));
+          const double wy = __dsub_rn(__dmul_rn(uz, ax), __dmul_rn(az, ux));
+          const double wz = __dsub_rn(__dmul_rn(ux, ay), __dmul_rn(ax, uy));
+          const double vx = __dsub_rn(__dmul_rn(ny, wz), __dmul_rn(wy, nz));
+          const double vy = __dsub_rn(__dmul_rn(nz, wx), __dmul_rn(wz, nx));
+          const double vz = __dsub_rn(__dmul_rn(nx, wy), __dmul_rn(wx, ny));
+          const double ex = __dadd_rn(__ddiv_rn(__dmul_rn(ux, ob2), den1), __ddiv_rn(vx, den2));
+          const double ey = __dadd_rn(__ddiv_rn(__dmul_rn(uy, ob2), den1), __ddiv_rn(vy, den2));
+          const double ez = __dadd_rn(__ddiv_rn(__dmul_rn(uz, ob2), den1), __ddiv_rn(vz, den2));
+          double sn, cs;
+          sincos(reduce_2pi(ph), &sn, &cs);
+          sxr = fma(ex, cs, sxr); sxi = fma(ex, sn, sxi);
+          syr = fma(ey, cs, syr); syi = fma(ey, sn, syi);
+          szr = fma(ez, cs, szr); szi = fma(ez, sn, szi);
+        }
+      }
+      __syncthreads();  // everyone is done with `buf` before it is refilled
+    }
+    if (live) {
+      const int64_t ps = A.part_stride;
+      double* p = A.part + ((int64_t)(g * gridDim.y + span) * kFdPartials) * ps + slot;
+      p[0 * ps] = sxr; p[1 * ps] = sxi; p[2 * ps] = syr; p[3 * ps] = syi; p[4 * ps] = szr; p[5 * ps] = szi;
+      p[6 * ps] = have ? first_phase : 0.0;
+      p[7 * ps] = have ? last_phase : 0.0;
+      p[8 * ps] = have ? dmax : -1.0;  // -1 marks an empty span
+    }
+  }
+}
+
+struct C3 { double xr, xi, yr, yi, zr, zi; };
+
+__device__ __forceinline__ C3 c3_scale(C3 a, double s) {
+  return {a.xr * s, a.xi * s, a.yr * s, a.yi * s, a.zr * s, a.zi * s};
+}
+// (E . P) P with the complex (unconjugated) dot product of TVector3DC::Dot.
+__device__ __forceinline__ C3 c3_project(C3 e, const double* P) {
+  const double cr = (e.xr * P[0] - e.xi * P[1]) + (e.yr * P[2] - e.yi * P[3]) + (e.zr * P[4] - e.zi * P[5]);
+  const double ci = (e.xr * P[1] + e.xi * P[0]) + (e.yr * P[3] + e.yi * P[2]) + (e.zr * P[5] + e.zi * P[4]);
+  return {P[0] * cr - P[1] * ci, P[0] * ci + P[1] * cr, P[2] * cr - P[3] * ci,
+          P[2] * ci + P[3] * cr, P[4] * cr - P[5] * ci, P[4] * ci + P[5] * cr};
+}
+__device__ __forceinline__ double c3_mag2(C3 a) {
+  return (a.xr * a.xr + a.xi * a.xi) + (a.yr * a.yr + a.yi * a.yi) + (a.zr * a.zr + a.zi * a.zi);
+}
+
+// Reduce the span partials of the wave, apply the stop rule of src/OSCARSSR.cc:4222-4238, finish
+// converged / last-level entries (:4246-4267) and append the others to the next active list.
+__global__ void k_fd_finalize(FdFinalArgs A) {
+  const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
+  const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= n_act) return;
+  const int64_t item = A.act ? (int64_t)A.act[slot] : slot;
+  const int64_t ps = A.part_stride;
+  auto seg_sum = [&](int g, C3& s, double& dmax) {
+    double prev_last = 0;
+    bool prev_have = false;
+    for (int sp = 0; sp < A.spans; ++sp) {
+      const double* p = A.part + ((int64_t)(g * A.spans + sp) * kFdPartials) * ps + slot;
+      s.xr += p[0]; s.xi += p[ps]; s.yr += p[2 * ps]; s.yi += p[3 * ps]; s.zr += p[4 * ps]; s.zi += p[5 * ps];
+      const double dm = p[8 * ps];
+      if (dm >= 0) {  // non-empty span
+        if (prev_have) {
+          const double d = fabs(__dsub_rn(p[6 * ps], prev_last));
+          dmax = d > dmax ? d : dmax;
+        }
+        dmax = dm > dmax ? dm : dmax;
+        prev_last = p[7 * ps];
+        prev_have = true;
+      }
+    }
+  };
+  const int64_t N = A.n_items;
+  C3 S;
+  double last_mag;
+  double dmax = 0;
+  if (A.first) {
+    S = {0, 0, 0, 0, 0, 0};
+    double unused = 0;
+    last_mag = -1;
+    if (A.nseg == 2) {
+      seg_sum(0, S, unused);
+      C3 t = c3_scale(S, A.dt_prev);
+      if (A.project) t = c3_project(t, A.pol);
+      last_mag = c3_mag2(t);
+    }
+    seg_sum(A.nseg - 1, S, dmax);
+  } else {
+    S = {A.state[item], A.state[N + item], A.state[2 * N + item], A.state[3 * N + item], A.state[4 * N + item], A.state[5 * N + item]};
+    last_mag = A.state[6 * N + item];
+    seg_sum(0, S, dmax);
+  }
+  C3 t = c3_scale(S, A.dt_level);
+  if (A.project) t = c3_project(t, A.pol);
+  const double this_mag = c3_mag2(t);
+  const double prec = fabs(this_mag - last_mag) / last_mag;
+  const int L = A.level;
+  const bool stop = (L > 8 && prec < A.precision && dmax < kPiD) || (L > 8 && dmax < kPiD && this_mag == last_mag);
+  if (stop || L >= A.max_level) {
+    const int result_level = stop ? L : -1;
+    C3 E = c3_scale(S, A.c0 * A.dt_level);
+    if (A.project) E = c3_project(E, A.pol);
+    double v;
+    if (A.quantity == 1) v = prec * A.weight;
+    else if (A.quantity == 2) v = (double)result_level * A.weight;
+    else v = A.c2 * c3_mag2(E) * A.weight;
+    A.out[item] = v;
+    if (A.level_out) A.level_out[item] = result_level;
+    if (!stop) atomicAdd(A.not_converged, 1ull);
+    atomicAdd(A.samples, (unsigned long long)((2ll << L) - 1));
+  } else {
+    A.state[item] = S.xr; A.state[N + item] = S.xi; A.state[2 * N + item] = S.yr;
+    A.state[3 * N + item] = S.yi; A.state[4 * N + item] = S.zr; A.state[5 * N + item] = S.zi;
+    A.state[6 * N + item] = this_mag;
+    const unsigned int k = atomicAdd(A.n_next, 1u);
+    A.act_next[k] = (int)item;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Power density (src/OSCARSSR.cc:2869-2922):
+//   sum += [(N1 x ((N1 - b) x a/c)) . Nk]^2 / (1 - b.N1)^5 / |O - X|^2 * (N1 . normal),  k = 2, 3
+// ---------------------------------------------------------------------------------------------
+constexpr int kPdThreads = 128;
+constexpr int kPdChunk = 128;
+
+__device__ __forceinline__ void unit3(double x, double y, double z, double& ux, double& uy, double& uz) {
+  const double m = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+  ux = __ddiv_rn(x, m); uy = __ddiv_rn(y, m); uz = __ddiv_rn(z, m);
+}
+
+__global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
+  __shared__ __align__(16) Stage<10, kPdChunk> st;
+  const int tid = threadIdx.x;
+  const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
+  const int64_t slot = (int64_t)blockIdx.x * kPdThreads + tid;
+  if ((int64_t)blockIdx.x * kPdThreads >= n_act) return;
+  const bool live = slot < n_act;
+  const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+  const double Ox = A.obs[3 * item], Oy = A.obs[3 * item + 1], Oz = A.obs[3 * item + 2];
+  const double Nx = A.normals[3 * item], Ny = A.normals[3 * item + 1], Nz = A.normals[3 * item + 2];
+  const int span = blockIdx.y;
+  if (tid == 0) {
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint32_t phase_bits = 0;
+  for (int g = 0; g < A.nseg; ++g) {
+    const int64_t b0 = A.seg_b[g] + (int64_t)span * A.span_len[g];
+    const int64_t b1 = min(A.seg_e[g], b0 + A.span_len[g]);
+    double sum = 0;
+    const int64_t nchunks = b1 > b0 ? (b1 - b0 + kPdChunk - 1) / kPdChunk : 0;
+    if (tid == 0 && nchunks > 0) {
+      const int64_t lo = b0, hi = min(b1, b0 + kPdChunk);
+      stage_issue<10, kPdChunk>(st, 0, A.lev, A.cap, lo & ~(int64_t)1, (hi + 1) & ~(int64_t)1);
+    }
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const int buf = (int)(c & 1);
+      const int64_t lo = b0 + c * kPdChunk, hi = min(b1, lo + kPdChunk);
+      if (tid == 0 && c + 1 < nchunks) {
+        const int64_t lo2 = lo + kPdChunk, hi2 = min(b1, lo2 + kPdChunk);
+        stage_issue<10, kPdChunk>(st, buf ^ 1, A.lev, A.cap, lo2 & ~(int64_t)1, (hi2 + 1) & ~(int64_t)1);
+      }
+      if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+        if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+        return;
+      }
+      phase_bits ^= 1u << buf;
+      const int64_t lo_al = lo & ~(int64_t)1;
+      const int j0 = (int)(max(lo, (int64_t)1) - lo_al), j1 = (int)(hi - lo_al);
+      if (live) {
+        for (int j = j0; j < j1; ++j) {
+          const double Rx = __dsub_rn(Ox, st.v[buf][1][j]), Ry = __dsub_rn(Oy, st.v[buf][2][j]), Rz = __dsub_rn(Oz, st.v[buf][3][j]);
+          double n1x, n1y, n1z;
+          unit3(Rx, Ry, Rz, n1x, n1y, n1z);
+          // Orthogonal() (include/TVector3D.h:132-142), then unit; N3 = unit(N1 x N2)
+          const double xx = fabs(n1x), yy = fabs(n1y), zz = fabs(n1z);
+          double ox, oy, oz;
+          if (xx < yy) {
+            if (xx < zz) { ox = 0; oy = n1z; oz = -n1y; } else { ox = n1y; oy = -n1x; oz = 0; }
+          } else {
+            if (yy < zz) { ox = -n1z; oy = 0; oz = n1x; } else { ox = n1y; oy = -n1x; oz = 0; }
+          }
+          double n2x, n2y, n2z, n3x, n3y, n3z;
+          unit3(ox, oy, oz, n2x, n2y, n2z);
+          unit3(__dsub_rn(__dmul_rn(n1y, n2z), __dmul_rn(n2y, n1z)), __dsub_rn(__dmul_rn(n1z, n2x), __dmul_rn(n2z, n1x)),
+                __dsub_rn(__dmul_rn(n1x, n2y), __dmul_rn(n2x, n1y)), n3x, n3y, n3z);
+          const double n1dn = A.has_normal
+                                  ? __dadd_rn(__dadd_rn(__dmul_rn(n1x, Nx), __dmul_rn(n1y, Ny)), __dmul_rn(n1z, Nz))
+                                  : 1.0;
+          if (A.directional && n1dn <= 0) continue;
+          const double bx = st.v[buf][4][j], by = st.v[buf][5][j], bz = st.v[buf][6][j];
+          const double ax = st.v[buf][7][j], ay = st.v[buf][8][j], az = st.v[buf][9][j];
+          const double ux = __dsub_rn(n1x, bx), uy = __dsub_rn(n1y, by), uz = __dsub_rn(n1z, bz);
+          const double wx = __dsub_rn(__dmul_rn(uy, az), __dmul_rn(ay, uz));
+          const double wy = __dsub_rn(__dmul_rn(uz, ax), __dmul_rn(az, ux));
+          const double wz = __dsub_rn(__dmul_rn(ux, ay), __dmul_rn(ax, uy));
+          const double mx = __dsub_rn(__dmul_rn(n1y, wz), __dmul_rn(wy, n1z));
+          const double my = __dsub_rn(__dmul_rn(n1z, wx), __dmul_rn(wz, n1x));
+          const double mz = __dsub_rn(__dmul_rn(n1x, wy), __dmul_rn(wx, n1y));
+          const double bdn = __dadd_rn(__dadd_rn(__dmul_rn(bx, n1x), __dmul_rn(by, n1y)), __dmul_rn(bz, n1z));
+          const double den = pow(__dsub_rn(1.0, bdn), 5.0);
+          const double m2 = __dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz));
+          const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n2x), __dmul_rn(my, n2y)), __dmul_rn(mz, n2z));
+          const double d3 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n3x), __dmul_rn(my, n3y)), __dmul_rn(mz, n3z));
+          sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d2, d2), den), m2), n1dn);
+          sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d3, d3), den), m2), n1dn);
+        }
+      }
+      __syncthreads();
+    }
+    if (live) A.part[(int64_t)(g * gridDim.y + span) * A.part_stride + slot] = sum;
+  }
+}
+
+// src/OSCARSSR.cc:2924-2968
+__global__ void k_pd_finalize(PdFinalArgs A) {
+  const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
+  const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= n_act) return;
+  const int64_t item = A.act ? (int64_t)A.act[slot] : slot;
+  const int64_t N = A.n_items;
+  double sum, last_sum;
+  if (A.first) {
+    sum = 0;
+    last_sum = -1;
+    if (A.nseg == 2) {
+      for (int sp = 0; sp < A.spans; ++sp) sum += A.part[(int64_t)sp * A.part_stride + slot];
+      last_sum = sum * A.dt_prev;
+    }
+    for (int sp = 0; sp < A.spans; ++sp) sum += A.part[(int64_t)((A.nseg - 1) * A.spans + sp) * A.part_stride + slot];
+  } else {
+    sum = A.state[item];
+    last_sum = A.state[N + item];
+    for (int sp = 0; sp < A.spans; ++sp) sum += A.part[(int64_t)sp * A.part_stride + slot];
+  }
+  const int L = A.level;
+  const double this_sum = sum * A.dt_level;
+  double prec = fabs(this_sum - last_sum) / last_sum;
+  const double bd = A.bdmax;
+  int result_level = -1;
+  bool stop = false;
+  if ((L > 8 && prec < A.precision && bd < A.two_over_gamma) || (L > 8 && bd < A.two_over_gamma && this_sum == last_sum)) {
+    stop = true;
+    result_level = L;
+  } else if (L > 8 && this_sum == last_sum) {
+    stop = true;
+    result_level = L;
+    prec = 0;
+  }
+  if (stop || L >= A.max_level) {
+    double s = sum * (A.scale * A.dt_level);
+    s /= 1e6;
+    if (!A.directional && s < 0) s *= -1;
+    double v;
+    if (A.quantity == 1) v = prec * A.weight;
+    else if (A.quantity == 2) v = (double)result_level * A.weight;
+    else v = s * A.weight;
+    A.out[item] = v;
+    if (A.level_out) A.level_out[item] = result_level;
+    if (!stop) atomicAdd(A.not_converged, 1ull);
+    atomicAdd(A.samples, (unsigned long long)((2ll << L) - 1));
+  } else {
+    A.state[item] = sum;
+    A.state[N + item] = this_sum;
+    const unsigned int k = atomicAdd(A.n_next, 1u);
+    A.act_next[k] = (int)item;
+  }
+}
+
+}  // namespace dev
+
+// ---- launch wrappers ------------------------------------------------------------------------
+cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
+                              int64_t s_end, double* lev, int64_t cap, int extended_level,
+                              unsigned long long* bdmax_bits, cudaStream_t st) {
+  if (s_end <= s_begin) return cudaSuccess;
+  const int T = 256;
+  const int64_t nblk = (s_end - s_begin + T - 1) / T;
+  dev::k_level_fill<<<(unsigned)nblk, T, 0, st>>>(knots, n, tstart, tstop, s_begin, s_end, lev, cap, extended_level);
+  dev::k_level_betadiff<<<(unsigned)nblk, T, 0, st>>>(lev, cap, s_begin, s_end, bdmax_bits, extended_level);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int64_t n_act_bound, int spans, cudaStream_t st) {
+  const int64_t tiles = (n_act_bound + dev::kFdThreads - 1) / dev::kFdThreads;
+  if (tiles == 0) return cudaSuccess;
+  dev::k_fd_wave_fp64<<<dim3((unsigned)tiles, (unsigned)spans), dev::kFdThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fd_finalize(const FdFinalArgs& a, int64_t n_act_bound, cudaStream_t st) {
+  if (n_act_bound == 0) return cudaSuccess;
+  const int T = 256;
+  dev::k_fd_finalize<<<(unsigned)((n_act_bound + T - 1) / T), T, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pd_wave_fp64(const PdWaveArgs& a, int64_t n_act_bound, int spans, cudaStream_t st) {
+  const int64_t tiles = (n_act_bound + dev::kPdThreads - 1) / dev::kPdThreads;
+  if (tiles == 0) return cudaSuccess;
+  dev::k_pd_wave_fp64<<<dim3((unsigned)tiles, (unsigned)spans), dev::kPdThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pd_finalize(const PdFinalArgs& a, int64_t n_act_bound, cudaStream_t st) {
+  if (n_act_bound == 0) return cudaSuccess;
+  const int T = 256;
+  dev::k_pd_finalize<<<(unsigned)((n_act_bound + T - 1) / T), T, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace osc

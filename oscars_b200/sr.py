@@ -1,0 +1,465 @@
+"""``oscars_b200.sr`` -- drop-in for the ``oscars.sr`` calls of the radiation hot path.
+
+Same method names, keyword names, defaults, return shapes and ValueError messages as the reference
+CPython extension (src/OSCARSSR_Python.cc); the arithmetic runs in liboscars_b200.so: the FP64 RK4
+trajectory and spline on the host (bit-identical to the reference), the level-ladder radiation sums
+on the B200.  Argument preprocessing that the reference binding does in its own layer (rotations of
+field vectors, the default horizontal direction, polarization strings, energy grids) is restated
+here with the binding's file:line.
+
+Extensions, all keyword-only and off by default:
+  ``compute='fp64'|'mixed'``   arithmetic of the radiation sums (see include/oscars_b200.h)
+  ``return_numpy=True``        return (positions, values) arrays instead of nested lists
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import sys
+
+import numpy as np
+
+from . import _lib
+from ._lib import BeamDesc, Context, FieldDesc, RadOpts, dptr, i32ptr
+
+_ANGLE_UNSET = 112188979912321.0  # binding sentinel for "angle not given" (:5662)
+_PARTICLES = {"electron": 0, "anti-positron": 0, "positron": 1, "anti-electron": 1, "muon": 2,
+              "anti-muon": 3, "proton": 4, "anti-proton": 5, "pi+": 6, "pi-": 7, "custom": 8}
+_NOT_CONVERGED = "Not all points converged to desired precision.  Can try increasing 'max_level_extended'\n"
+
+
+def _vec3(v, name):
+    try:
+        v = [float(x) for x in v]
+    except TypeError:
+        raise ValueError("Incorrect format in '%s'" % name)
+    if len(v) != 3:
+        raise ValueError("Incorrect format in '%s'" % name)
+    return v
+
+
+def _vec2(v, name):
+    v = [float(x) for x in v]
+    if len(v) != 2:
+        raise ValueError("Incorrect format in '%s'" % name)
+    return v
+
+
+def _rotate_xyz(v, r):
+    """TVector3D::RotateSelfXYZ (src/TVector3D.cc): about X, then Y, then Z."""
+    x, y, z = v
+    s, c = math.sin(r[0]), math.cos(r[0])
+    y, z = c * y - s * z, s * y + c * z
+    s, c = math.sin(r[1]), math.cos(r[1])
+    z, x = c * z - s * x, s * z + c * x
+    s, c = math.sin(r[2]), math.cos(r[2])
+    x, y = c * x - s * y, s * x + c * y
+    return [x, y, z]
+
+
+def _polarization(polarization, angle):
+    """Binding defaults (src/OSCARSSR_Python.cc:5889-5899) and the string match of
+    src/OSCARSSR.cc:4129-4150."""
+    if polarization == "all" and angle != _ANGLE_UNSET:
+        raise ValueError("cannot specify 'all' and 'angle'.  This is to save you")
+    pol = polarization if len(polarization) else ("linear" if angle != _ANGLE_UNSET else "all")
+    p = pol.lower().replace(" ", "-")
+    if "all" in p:
+        return 0
+    if "linear-horizontal" in p or "lh" in p:
+        return 1
+    if "linear-vertical" in p or "lv" in p:
+        return 2
+    if p == "linear":
+        return 3
+    if "circular-left" in p or "cl" in p:
+        return 4
+    if "circular-right" in p or "cr" in p:
+        return 5
+    raise ValueError("Polarization requested not recognized")
+
+
+def _quantity(q, pd=False):
+    Q = q.upper()
+    if (pd and Q in ("POWER DENSITY", "POWERDENSITY")) or (not pd and Q == "FLUX"):
+        return 0
+    if Q == "PRECISION":
+        return 1
+    if Q == "LEVEL":
+        return 2
+    raise ValueError("'quantity' must be: 'flux', 'precision', 'level', or blank")
+
+
+def _compute_mode(compute):
+    if compute in ("fp64", "plain", 0):
+        return 0
+    if compute in ("mixed", 1):
+        return 1
+    raise ValueError("'compute' must be 'fp64' or 'mixed'")
+
+
+class sr:
+    """GPU implementation of the ``oscars.sr.sr`` radiation calls."""
+
+    def __init__(self, nthreads=0, gpu=0, device=None):
+        if gpu not in (0, 1):
+            raise ValueError("global gpu settign must be 0 or 1")
+        ndev = _lib.device_count()
+        self._dev = device if device is not None else (0 if ndev > 0 else -1)
+        self._ctx = Context(self._dev)
+        self._gpu_global = 1
+        self._nthreads_global = nthreads if nthreads > 0 else 2
+        self._nbeams = 0
+
+    # ---- global settings ------------------------------------------------------------------------
+    def set_gpu_global(self, gpu):
+        if gpu not in (0, 1):
+            raise ValueError("global gpu settign must be 0 or 1")
+        self._gpu_global = 1  # every radiation call of this build runs on the GPU
+
+    def check_gpu(self):
+        return _lib.device_count()
+
+    def set_nthreads_global(self, n):
+        self._nthreads_global = int(n)
+
+    def set_seed(self, seed):
+        self._ctx.call("osc_set_seed", int(float(seed)))
+
+    def version(self):
+        return _lib.lib().osc_version().decode()
+
+    # ---- fields (src/OSCARSSR_Python.cc:1309-1420, 1479-1630) ------------------------------------
+    def clear_bfields(self):
+        self._ctx.call("osc_clear_fields")
+
+    def add_bfield_undulator(self, bfield, period, nperiods, phase=0, rotations=[], translation=[], taper=0,
+                             frequency=0, frequency_phase=0, time_offset=0, name=""):
+        f = _vec3(bfield, "bfield")
+        p = _vec3(period, "period")
+        r = _vec3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        t = _vec3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
+        if len(name) > 0 and name[0] == "_":
+            raise ValueError("'name' cannot begin with '_'.  This is reserved for internal use.  Please pick a different name")
+        d = FieldDesc(kind=0, nperiods=int(nperiods), phase=float(phase), taper=float(taper),
+                      frequency=float(frequency), frequency_phase=float(frequency_phase),
+                      time_offset=float(time_offset))
+        d.bfield[:] = _rotate_xyz(f, r)
+        d.period[:] = _rotate_xyz(p, r)
+        d.center[:] = t
+        self._ctx.call("osc_add_field", ctypes.byref(d))
+
+    def add_bfield_epu(self, period, nperiods, bfieldA=[], bfieldB=[], phase=0, rotations=[], translation=[],
+                       taper=0, frequency=0, frequency_phase=0, time_offset=0, name=""):
+        if len(bfieldA) == 0 and len(bfieldB) == 0:
+            raise ValueError("Must define at least one of 'bfieldA', 'bfieldB'")
+        fa = _vec3(bfieldA, "bfieldA") if len(bfieldA) else [0.0, 0.0, 0.0]
+        fb = _vec3(bfieldB, "bfieldB") if len(bfieldB) else [0.0, 0.0, 0.0]
+        p = _vec3(period, "period")
+        r = _vec3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        t = _vec3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
+        d = FieldDesc(kind=1, nperiods=int(nperiods), phase=float(phase), taper=float(taper),
+                      frequency=float(frequency), frequency_phase=float(frequency_phase),
+                      time_offset=float(time_offset))
+        d.bfield[:] = _rotate_xyz(fa, r)
+        d.bfield_b[:] = _rotate_xyz(fb, r)
+        d.period[:] = _rotate_xyz(p, r)
+        d.center[:] = t
+        self._ctx.call("osc_add_field", ctypes.byref(d))
+
+    def get_bfield(self, x, t=0, name=""):
+        X = np.array(_vec3(x, "x"))
+        out = np.zeros(3)
+        self._ctx.call("osc_get_bfield", dptr(X), float(t), dptr(out))
+        return list(map(float, out))
+
+    # ---- beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) --------------------------------------
+    def clear_particle_beams(self):
+        self._nbeams = 0
+
+    def set_particle_beam(self, **kw):
+        self._nbeams = 0
+        self.add_particle_beam(**kw)
+
+    def add_particle_beam(self, type="electron", name="", energy_GeV=-1, d0=None, x0=None, beam="",
+                          sigma_energy_GeV=0, t0=0, current=0, weight=1, rotations=None, translation=None,
+                          horizontal_direction=None, beta=None, alpha=None, gamma=None, emittance=None, eta=None,
+                          lattice_reference=None, mass=0, charge=0, ctstartstop=None, distribution=""):
+        if beam:
+            raise ValueError("predefined beams are not part of this GPU build's drop-in surface")
+        if self._nbeams >= 1:
+            raise ValueError("this GPU build holds one beam; call set_particle_beam to replace it")
+        if gamma is not None or lattice_reference is not None:
+            raise ValueError("'gamma' and 'lattice_reference' are not part of this GPU build's drop-in surface")
+        if type not in _PARTICLES:
+            raise ValueError("invalid argument in adding particle beam.  possibly 'name' already exists")
+        pos = _vec3(x0, "x0") if x0 is not None else [0.0, 0.0, 0.0]
+        if energy_GeV != -1 and energy_GeV < 0:
+            raise ValueError("We do not currently support negative energy beams.  Please change 'energy_GeV' to >= 0")
+        dr = _vec3(d0, "d0") if d0 is not None else [0.0, 0.0, 1.0]
+        rot = _vec3(rotations, "rotations") if rotations is not None else [0.0, 0.0, 0.0]
+        tr = _vec3(translation, "translation") if translation is not None else [0.0, 0.0, 0.0]
+        if horizontal_direction is not None:
+            hd = _vec3(horizontal_direction, "horizontal_direction")
+        else:  # -Direction.Orthogonal() of the un-rotated direction (include/TVector3D.h:132-142)
+            ax, ay, az = (-v if v < 0.0 else v for v in dr)
+            if ax < ay:
+                o = [0.0, dr[2], -dr[1]] if ax < az else [dr[1], -dr[0], 0.0]
+            else:
+                o = [-dr[2], 0.0, dr[0]] if ay < az else [dr[1], -dr[0], 0.0]
+            hd = [-o[0], -o[1], -o[2]]
+        pos = _rotate_xyz(pos, rot)
+        dr = _rotate_xyz(dr, rot)
+        pos = [pos[0] + tr[0], pos[1] + tr[1], pos[2] + tr[2]]
+        if type == "custom" and (mass == 0 or charge == 0):
+            raise ValueError("'mass' or 'charge' is zero")
+        d = BeamDesc(particle=_PARTICLES[type], charge=float(charge), mass=float(mass), energy_GeV=float(energy_GeV),
+                     t0=float(t0), current=float(current), sigma_energy_GeV=float(sigma_energy_GeV))
+        d.x0[:] = pos
+        d.d0[:] = dr
+        d.horizontal[:] = hd
+        if emittance is not None:
+            d.emittance[:] = _vec2(emittance, "emittance")
+            d.has_emittance = 1
+        if beta is not None:
+            d.beta[:] = _vec2(beta, "beta")
+            d.has_beta = 1
+        if alpha is not None:
+            d.alpha[:] = _vec2(alpha, "alpha")
+            d.has_alpha = 1
+        if eta is not None:
+            d.eta[:] = _vec2(eta, "gamma")
+        dist = {"": -1, "filament": 1, "gaussian": 2, "kv": 3}
+        if distribution.lower() not in dist:
+            raise ValueError("Unknown beam distribution name: " + distribution)
+        d.distribution = dist[distribution.lower()]
+        if ctstartstop is not None:
+            d.ctstartstop[:] = _vec2(ctstartstop, "ctstartstop")
+            d.has_ctstartstop = 1
+        self._ctx.call("osc_set_beam", ctypes.byref(d))
+        self._nbeams = 1
+
+    def set_new_particle(self, beam="", particle=""):
+        self._ctx.call("osc_set_new_particle", int(particle.lower() == "ideal"))
+
+    def _particle(self):
+        x0, b0 = np.zeros(3), np.zeros(3)
+        t0, g = ctypes.c_double(), ctypes.c_double()
+        self._ctx.call("osc_get_particle", dptr(x0), dptr(b0), ctypes.byref(t0), ctypes.byref(g))
+        return x0, b0, t0.value, g.value
+
+    def get_particle_x0(self):
+        return list(map(float, self._particle()[0]))
+
+    def get_particle_beta0(self):
+        return list(map(float, self._particle()[1]))
+
+    # ---- trajectory ------------------------------------------------------------------------------
+    def set_ctstartstop(self, start, stop):
+        self._ctx.call("osc_set_ctstartstop", float(start), float(stop))
+
+    def _ctss(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._ctx.call("osc_get_ctstartstop", ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def get_ctstart(self):
+        return self._ctss()[0]
+
+    def get_ctstop(self):
+        return self._ctss()[1]
+
+    def set_npoints_trajectory(self, npoints):
+        self._ctx.call("osc_set_npoints_trajectory", int(npoints))
+
+    def get_npoints_trajectory(self):
+        n = ctypes.c_longlong()
+        self._ctx.call("osc_get_npoints_trajectory", ctypes.byref(n))
+        return n.value
+
+    def trajectory_array(self):
+        """(10, n) array: t, x, y, z, beta_x, beta_y, beta_z, a_x/c, a_y/c, a_z/c."""
+        n = ctypes.c_longlong()
+        self._ctx.call("osc_get_trajectory", None, 0, ctypes.byref(n))
+        out = np.zeros(10 * n.value)
+        self._ctx.call("osc_get_trajectory", dptr(out), out.size, ctypes.byref(n))
+        return out.reshape(10, n.value)
+
+    def get_trajectory(self):
+        a = self.trajectory_array()
+        return [[float(a[0, i]), a[1:4, i].tolist(), a[4:7, i].tolist(), a[7:10, i].tolist()] for i in range(a.shape[1])]
+
+    def calculate_trajectory(self, ofile="", bofile="", oformat=""):
+        if ofile or bofile:
+            raise ValueError("trajectory file output is not part of this GPU build's drop-in surface")
+        self._ctx.call("osc_calculate_trajectory")
+        return self.get_trajectory()
+
+    # ---- radiation -------------------------------------------------------------------------------
+    def _check_gpu(self, gpu, nthreads):
+        if gpu not in (0, 1, -1):
+            raise ValueError("'gpu' must be 0 or 1")
+        if nthreads < 0:
+            raise ValueError("'nthreads' must be > 0")
+        if nthreads > 0 and gpu == 1:
+            raise ValueError("gpu is 1 and nthreads > 0.  Both are not currently allowed.")
+        if gpu == 0:
+            raise ValueError("gpu=0 selects the reference's CPU path; this build computes on the GPU only")
+
+    def _opts(self, polarization, angle, horizontal_direction, propogation_direction, precision, max_level,
+              max_level_extended, nparticles, quantity, compute):
+        o = RadOpts()
+        o.polarization = _polarization(polarization, angle)
+        o.angle = float(angle)
+        o.horizontal[:] = _vec3(horizontal_direction, "translation") if horizontal_direction else [1.0, 0.0, 0.0]
+        o.propagation[:] = _vec3(propogation_direction, "translation") if propogation_direction else [0.0, 0.0, 1.0]
+        o.precision = float(precision)
+        o.max_level = int(max_level)
+        o.max_level_extended = int(max_level_extended)
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        o.nparticles = int(nparticles)
+        o.quantity = quantity
+        o.precision_mode = _compute_mode(compute)
+        return o
+
+    def _report(self, nnc):
+        if nnc.value > 0:
+            sys.stderr.write(_NOT_CONVERGED)
+
+    @staticmethod
+    def _energies(npoints, energy_range_eV, energy_points_eV):
+        """TSpectrumContainer::Init (src/TSpectrumContainer.cc:57-112) and the binding's default
+        point count (src/OSCARSSR_Python.cc:5817-5822)."""
+        if energy_points_eV is not None:
+            if len(energy_points_eV) == 0:
+                raise ValueError("Number of points to calculate is zero.  Check input.")
+            return np.array([float(e) for e in energy_points_eV])
+        e0 = e1 = 0.0
+        if energy_range_eV is not None:
+            if len(energy_range_eV) != 2:
+                raise ValueError("'energy_range_eV' must be a list of length 2")
+            e0, e1 = float(energy_range_eV[0]), float(energy_range_eV[1])
+        if npoints < 1:
+            npoints = abs(int(e1 - e0) + 1) if abs(e1 - e0) + 1 > 100 else 100
+        if npoints == 1:
+            return np.array([e0])
+        return np.array([e0 + (e1 - e0) / (npoints - 1) * float(i) for i in range(npoints)])
+
+    def calculate_spectrum(self, obs, npoints=0, energy_range_eV=None, energy_points_eV=None, points_eV=None,
+                           polarization="", angle=_ANGLE_UNSET, horizontal_direction=None, propogation_direction=None,
+                           precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, nthreads=0, gpu=-1,
+                           ngpu=None, quantity="flux", ofile="", bofile="", *, compute="fp64", return_numpy=False):
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        if points_eV is not None:
+            energy_points_eV = points_eV
+        E = self._energies(npoints, energy_range_eV, energy_points_eV)
+        O = np.array(_vec3(obs, "obs"))
+        self._check_gpu(gpu, nthreads)
+        q = _quantity(quantity)
+        o = self._opts(polarization, angle, horizontal_direction, propogation_direction, precision, max_level,
+                       max_level_extended, nparticles, q, compute)
+        out = np.zeros(E.size)
+        lv = np.zeros(E.size, dtype=np.int32)
+        nnc = ctypes.c_longlong()
+        self._ctx.call("osc_spectrum", dptr(O), dptr(E), E.size, ctypes.byref(o), dptr(out), i32ptr(lv), ctypes.byref(nnc))
+        self.last_levels = lv
+        self._report(nnc)
+        if ofile or bofile:
+            raise ValueError("spectrum file output is not part of this GPU build's drop-in surface")
+        if return_numpy:
+            return E, out
+        return [[float(E[i]), float(out[i])] for i in range(E.size)]
+
+    def _rectangle(self, npoints, plane, width, x0x1x2, rotations, translation, normal, pd):
+        if len(npoints) != 2:
+            raise ValueError("'npoints' must be [int, int]")
+        nx1, nx2 = int(npoints[0]), int(npoints[1])
+        if nx1 <= 0 or nx2 <= 0:
+            raise ValueError("an entry in 'npoints' is <= 0")
+        r = np.array(_vec3(rotations, "rotations") if rotations else [0.0, 0.0, 0.0])
+        t = np.array(_vec3(translation, "translation") if translation else [0.0, 0.0, 0.0])
+        w1, w2 = (0.010, 0.010) if pd else (0.0, 0.0)
+        if width is not None and len(width) == 2:
+            w1, w2 = float(width[0]), float(width[1])
+        if abs(normal) > 1:
+            raise ValueError("'normal' must be -1, 0, or 1")
+        if x0x1x2 is not None:
+            raise ValueError("'x0x1x2' surfaces are not part of this GPU build's drop-in surface")
+        if w1 <= 0 or w2 <= 0:
+            raise ValueError("'width' must be > 0" if pd else "'width' must be given as [w1, w2] with both > 0")
+        n = nx1 * nx2
+        xyz, nrm, x12 = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
+        rc = _lib.lib().osc_surface_rectangle(plane.encode(), nx1, nx2, w1, w2, dptr(r), dptr(t), int(normal),
+                                              dptr(xyz), dptr(nrm), dptr(x12))
+        if rc != 0:
+            raise ValueError(_lib.lib().osc_last_error(None).decode())
+        return xyz, nrm, x12
+
+    @staticmethod
+    def _points_result(pos, out, return_numpy):
+        pos = pos.reshape(-1, 3)
+        if return_numpy:
+            return pos, out
+        return [[pos[i].tolist(), float(out[i])] for i in range(out.size)]
+
+    def calculate_flux_rectangle(self, energy_eV, npoints=[51, 51], plane="XY", normal=0, dim=2, width=None,
+                                 rotations=None, translation=None, x0x1x2=None, polarization="", angle=_ANGLE_UNSET,
+                                 horizontal_direction=None, propogation_direction=None, nparticles=0, nthreads=0,
+                                 gpu=-1, ngpu=None, precision=0.01, max_level=-2, max_level_extended=0,
+                                 quantity="flux", ofile="", bofile="", *, compute="fp64", return_numpy=False):
+        if self._nbeams < 1:
+            raise ValueError("No particle beam defined")
+        if dim not in (2, 3):
+            raise ValueError("'dim' must be 2 or 3")
+        xyz, nrm, x12 = self._rectangle(npoints, plane, width, x0x1x2, rotations, translation, normal, False)
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        self._check_gpu(gpu, nthreads)
+        q = _quantity(quantity)
+        o = self._opts(polarization, angle, horizontal_direction, propogation_direction, precision, max_level,
+                       max_level_extended, nparticles, q, compute)
+        n = xyz.size // 3
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        nnc = ctypes.c_longlong()
+        self._ctx.call("osc_flux", dptr(xyz), n, float(energy_eV), ctypes.byref(o), dptr(out), i32ptr(lv), ctypes.byref(nnc))
+        self.last_levels = lv
+        self._report(nnc)
+        if ofile or bofile:
+            raise ValueError("flux file output is not part of this GPU build's drop-in surface")
+        return self._points_result(xyz if dim == 3 else x12, out, return_numpy)
+
+    def calculate_power_density_rectangle(self, npoints=[51, 51], plane="XY", width=None, x0x1x2=None,
+                                          rotations=None, translation=None, ofile="", bofile="", normal=0,
+                                          nparticles=0, gpu=-1, ngpu=None, nthreads=0, precision=0.01, max_level=-2,
+                                          max_level_extended=0, dim=2, quantity="power density", *, compute="fp64",
+                                          return_numpy=False):
+        if self._nbeams < 1:
+            raise ValueError("No particle beam defined")
+        if dim not in (2, 3):
+            raise ValueError("'dim' must be 2 or 3")
+        xyz, nrm, x12 = self._rectangle(npoints, plane, width, x0x1x2, rotations, translation, normal, True)
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        self._check_gpu(gpu, nthreads)
+        q = _quantity(quantity, pd=True)
+        o = self._opts("", _ANGLE_UNSET, None, None, precision, max_level, max_level_extended, nparticles, q, compute)
+        n = xyz.size // 3
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        nnc = ctypes.c_longlong()
+        self._ctx.call("osc_power_density", dptr(xyz), dptr(nrm), n, int(normal != 0), ctypes.byref(o), dptr(out),
+                       i32ptr(lv), ctypes.byref(nnc))
+        self.last_levels = lv
+        self._report(nnc)
+        if ofile or bofile:
+            raise ValueError("power density file output is not part of this GPU build's drop-in surface")
+        return self._points_result(xyz if dim == 3 else x12, out, return_numpy)
+
+    def last_stats(self):
+        """(samples integrated, kernel launches) of the last radiation call."""
+        s, l = ctypes.c_longlong(), ctypes.c_longlong()
+        self._ctx.call("osc_last_stats", ctypes.byref(s), ctypes.byref(l))
+        return s.value, l.value

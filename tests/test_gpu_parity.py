@@ -1,0 +1,94 @@
+"""GPU parity of the plain FP64 path against the reference.
+
+Every golden case (values computed by the reference's own CPU build) is replayed through
+``oscars_b200.sr`` on the GPU.  Tolerance for values: relative error <= 1e-9, measured against the
+case's peak (max_i |F_i - F_ref_i| / max_i |F_ref_i|); stop levels must be identical.  At the full
+201 x 201 flux / power-density grid the comparison is against the CPU oracle (itself pinned bit for
+bit to the reference by test_oracle_pin.py).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from cases import CASES, E1_U, UND_SETUP, run_case
+from oracle.oracle import OracleSR
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-9
+
+pytestmark = pytest.mark.gpu
+
+
+def _sr():
+    from oscars_b200.sr import sr
+    return sr(gpu=1)
+
+
+def _flat(res):
+    return (np.array([r[0] for r in res], dtype=np.float64), np.array([r[1] for r in res], dtype=np.float64))
+
+
+def _peak_rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+RADIATION_CASES = sorted(k for k, v in CASES.items() if v[-1][0] != "calculate_trajectory")
+
+
+@pytest.mark.parametrize("name", RADIATION_CASES)
+def test_golden_case_on_gpu(name):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    s = _sr()
+    calls = list(CASES[name])
+    last, kw = calls[-1]
+    pos, val = _flat(run_case(s, calls[:-1] + [(last, dict(kw, gpu=1))]))
+    assert np.array_equal(pos, g["pos"])
+    err = _peak_rel(val, g["val"])
+    if kw.get("quantity") == "level":
+        assert np.array_equal(val, g["val"])
+    else:
+        assert err <= TOL, "%s: peak-normalised error %.3e" % (name, err)
+    if "level" in g.files:
+        s2 = _sr()
+        _, lev = _flat(run_case(s2, calls[:-1] + [(last, dict(kw, gpu=1, quantity="level"))]))
+        assert np.array_equal(lev, g["level"]), "stop levels differ at %d entries" % int(np.sum(lev != g["level"]))
+
+
+def _cfg1(obj, what):
+    run_case(obj, UND_SETUP)
+    if what == "flux":
+        return obj.calculate_flux_rectangle(energy_eV=E1_U, npoints=[201, 201], width=[0.01, 0.01], translation=[0, 0, 30])
+    return obj.calculate_power_density_rectangle(npoints=[201, 201], width=[0.01, 0.01], translation=[0, 0, 30])
+
+
+@pytest.mark.parametrize("what", ["flux", "pd"])
+def test_full_201x201_grid_against_oracle(what):
+    _, ref = _flat(_cfg1(OracleSR(), what))
+    s = _sr()
+    _, val = _flat(_cfg1(s, what))
+    err = _peak_rel(val, ref)
+    assert err <= TOL, "peak-normalised error %.3e" % err
+    # per-entry relative error where the value is not vanishingly small
+    big = np.abs(ref) > 1e-6 * np.max(np.abs(ref))
+    assert np.max(np.abs(val[big] - ref[big]) / np.abs(ref[big])) <= 1e-7
+
+
+def test_device_entry_point_matches_host_entry_point():
+    import ctypes
+    import torch
+    from oscars_b200._lib import RadOpts
+    s = _sr()
+    run_case(s, UND_SETUP)
+    pos, host = _flat(s.calculate_flux_rectangle(energy_eV=E1_U, npoints=[31, 31], width=[0.01, 0.01],
+                                                 translation=[0, 0, 30], dim=3))
+    obs = torch.tensor(pos, dtype=torch.float64, device="cuda")
+    out = torch.zeros(pos.shape[0], dtype=torch.float64, device="cuda")
+    lvl = torch.zeros(pos.shape[0], dtype=torch.int32, device="cuda")
+    o = RadOpts(precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, quantity=0, precision_mode=0)
+    o.horizontal[:] = [1, 0, 0]
+    o.propagation[:] = [0, 0, 1]
+    s._ctx.call("osc_flux_device", ctypes.c_void_p(obs.data_ptr()), pos.shape[0], E1_U, ctypes.byref(o),
+                ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(lvl.data_ptr()), None)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), host)
