@@ -52,44 +52,49 @@ def setup(o):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clocks and clock-event (throttle) reasons read through NVML every 20 ms while the timed
+    region runs (the same counters `nvidia-smi --query-gpu=clocks.sm,clocks_event_reasons.*`
+    reports).  Read-only: no setting of the GPU is touched."""
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.out = None
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thr = None
+        self.error = None
+
+    def _run(self):
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                self.samples.append((N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM),
+                                     N.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                time.sleep(0.02)
+        except Exception as e:  # no NVML: report it, the number itself is unaffected
+            self.error = repr(e)
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+        self._thr = threading.Thread(target=self._run, daemon=True)
+        self._thr.start()
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                self.out = ""
+        self._stop.set()
+        self._thr.join(timeout=5)
 
     def summary(self):
-        if not self.out:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = [r for r in csv.reader(io.StringIO(self.out)) if len(r) >= 9]
-        sm = sorted(float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit())
-        mx = max((float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()), default=None)
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no NVML samples: %s" % self.error]}
+        sm = sorted(c for c, _ in self.samples)
+        reasons = sorted({name for _, r in self.samples for bit, name in self.REASONS.items() if r & bit})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples)}
 
 
 def _quiet_import_reference():
@@ -251,6 +256,13 @@ def product_arm(args):
         ms_max, samples_all = ms, float(samples)
     value = samples_all / (ms_max * 1e-3) / 1e9
 
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": value, "unit": "Gsamples/s", "ms_per_step": ms_max / args.steps,
+                              "kernel_ms": kms.value, "kernel_launches": kl.value}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     # e2e: host buffers through the C ABI, new trajectory every step (host RK4 + spline included)
     out_h = np.zeros(n)
     lvl_h = np.zeros(n, dtype=np.int32)
@@ -266,7 +278,7 @@ def product_arm(args):
     torch.cuda.synchronize()
     e2e_times = []
     e2e_samples = 0
-    for i in range(max(1, args.steps)):
+    for i in range(max(1, min(args.steps, 20))):
         t0 = time.perf_counter()
         e2e_step()
         e2e_times.append(time.perf_counter() - t0)
@@ -319,10 +331,11 @@ def product_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--compute", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--quick", action="store_true", help="device-resident timing only (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
