@@ -86,6 +86,7 @@ void Engine::upload_trajectory() {
   tstop_ = k.tstop;
   knots_version_ = model.knots_version;
   lev_filled_ = -1;
+  mrec_filled_ = -1;
   bdmax_valid_ = false;
   check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), stream), "memset");
 }
@@ -124,6 +125,55 @@ void Engine::ensure_levels(int L) {
   last_launches += 2;
   lev_filled_ = L;
   bdmax_valid_ = false;
+}
+
+// Frame of the mixed path (kernels_mixed.cu): origin at the particle start, e3 along its initial
+// velocity, e1 = unit(Orthogonal(e3)), e2 = e3 x e1; trajectory extent measured on the knots.
+void Engine::compute_frame() {
+  const Particle& P = model.particle;
+  const Vec3 e3 = unit(P.b0);
+  const Vec3 e1 = unit(orthogonal(e3));
+  const Vec3 e2 = cross(e3, e1);
+  const Vec3 rows[3] = {e1, e2, e3};
+  for (int r = 0; r < 3; ++r) {
+    frame_.rot[3 * r] = rows[r].x;
+    frame_.rot[3 * r + 1] = rows[r].y;
+    frame_.rot[3 * r + 2] = rows[r].z;
+  }
+  frame_.x0[0] = P.x0.x; frame_.x0[1] = P.x0.y; frame_.x0[2] = P.x0.z;
+  frame_.t_ref = P.t0 / kC;
+  const Knots& k = model.knots;
+  double xp = 0, zm = -1e300;
+  for (int64_t i = 0; i < k.n; ++i) {
+    const Vec3 d = v3(k.y[i] - P.x0.x, k.y[k.n + i] - P.x0.y, k.y[2 * k.n + i] - P.x0.z);
+    const double a = dot(d, e1), b = dot(d, e2), c = dot(d, e3);
+    xp = std::max(xp, std::sqrt(a * a + b * b));
+    zm = std::max(zm, c);
+  }
+  frame_.xperp_max = xp;
+  frame_.z_max = zm;
+}
+
+void Engine::ensure_mixed(int L) {
+  ensure_levels(L);
+  if (mrec_version_ != knots_version_) {
+    compute_frame();
+    mrec_version_ = knots_version_;
+    mrec_filled_ = -1;
+  }
+  if (L <= mrec_filled_) return;
+  if (mrec_cap_ < lev_cap_) {
+    mrec_.release();
+    mrec_.reserve(sizeof(float4) * 3 * lev_cap_);
+    mrec_cap_ = lev_cap_;
+    mrec_filled_ = -1;
+  }
+  const int64_t s_begin = mrec_filled_ < 0 ? 1 : ((int64_t)2 << mrec_filled_);
+  const int64_t s_end = (int64_t)2 << L;
+  check(launch_mixed_records(lev_.as<double>(), lev_cap_, s_begin, s_end, frame_, mrec_.as<float4>(), stream),
+        "mixed records");
+  ++last_launches;
+  mrec_filled_ = L;
 }
 
 void Engine::refresh_bdmax() {
@@ -176,12 +226,13 @@ static void polarization_vector(const osc_rad_opts& o, double P[6], bool& projec
   project = o.polarization != OSC_POL_ALL && m2 > 0.001;
 }
 
-// Spans per wave: enough CTAs to fill the machine, each span at least one staged chunk.
+// Spans per wave: split each level into spans so that a wave launch is >= 4 full waves of CTAs
+// (148 SMs x ~7 resident CTAs); a span keeps >= 32 samples.
 static int choose_spans(int64_t n_act, int64_t level_len) {
   const int64_t tiles = (n_act + 127) / 128;
-  const int64_t target = 148 * 6;
+  const int64_t target = 148 * 7 * 4;
   int64_t spans = 1;
-  while (tiles * spans < target && level_len / (spans * 2) >= 128) spans *= 2;
+  while (tiles * spans < target && level_len / (spans * 2) >= 32) spans *= 2;
   return (int)spans;
 }
 
@@ -195,7 +246,11 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
   const Particle& P = model.particle;
   const int Lfirst = std::min(9, lstop);
-  ensure_levels(std::min(lstop, std::max(Lfirst, 12)));
+  const bool mixed = o.precision_mode == OSC_MIXED;
+  if (mixed && rq.power_density)
+    throw Error{OSC_ERR_INVALID, "compute='mixed' applies to flux and spectrum; power density runs in FP64"};
+  if (mixed) ensure_mixed(std::min(lstop, std::max(Lfirst, 12)));
+  else ensure_levels(std::min(lstop, std::max(Lfirst, 12)));
   if (rq.power_density) refresh_bdmax();
 
   unsigned* cnt = cnt_.as<unsigned>();  // [0] n_act A, [1] n_act B, [2] err
@@ -233,7 +288,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       cur_list ^= 1;
       check(cudaMemsetAsync(cnt + (cur_list ^ 1), 0, sizeof(unsigned), st), "memset");
       n_act = nn;
-      ensure_levels(L);
+      if (mixed) ensure_mixed(L);
+      else ensure_levels(L);
       if (rq.power_density) refresh_bdmax();
     }
     const int nseg = first && L >= 1 ? 2 : 1;
@@ -244,7 +300,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     } else {
       sb[0] = (int64_t)1 << L; se[0] = (int64_t)2 << L;
     }
-    const int spans = choose_spans(n_act, (int64_t)1 << L);
+    const int spans = choose_spans(mixed ? (n_act + mixed_ept - 1) / mixed_ept : n_act, (int64_t)1 << L);
     int64_t sl[2] = {0, 0};
     for (int g = 0; g < nseg; ++g) {
       const int64_t len = se[g] - (sb[g] & ~(int64_t)1);
@@ -256,12 +312,17 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     if (!rq.power_density) {
       part_.reserve(sizeof(double) * (size_t)nseg * spans * kFdPartials * part_stride);
       FdWaveArgs w{};
-      w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
+      w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
+      w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in; w.nseg = nseg;
       for (int g = 0; g < nseg; ++g) { w.seg_b[g] = sb[g] & ~(int64_t)1; w.seg_e[g] = se[g]; w.span_len[g] = sl[g]; }
       w.part = part_.as<double>(); w.part_stride = part_stride; w.err = cnt + 2;
+      if (mixed) {  // the mixed records need no even-index alignment
+        for (int g = 0; g < nseg; ++g) w.seg_b[g] = sb[g] == 1 ? 0 : sb[g];
+      }
       auto ev = timed_begin(st);
-      check(launch_fd_wave_fp64(w, n_act, spans, st), "flux wave");
+      if (mixed) check(launch_fd_wave_mixed(w, frame_, n_act, spans, mixed_ept, st), "flux wave (mixed)");
+      else check(launch_fd_wave_fp64(w, n_act, spans, st), "flux wave");
       timed_end(ev, st);
       FdFinalArgs f{};
       f.part = part_.as<double>(); f.part_stride = part_stride; f.spans = spans; f.nseg = nseg; f.first = first;
@@ -269,6 +330,12 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
       f.precision = o.precision; f.c0 = c0; f.c2 = c2; f.weight = weight;
       for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
+      if (mixed) {  // project in the frame: P' = R P (R orthogonal, so E'.P' = E.P)
+        const double* R = frame_.rot;
+        for (int ri = 0; ri < 2; ++ri)
+          for (int r = 0; r < 3; ++r)
+            f.pol[2 * r + ri] = R[3 * r] * pol[ri] + R[3 * r + 1] * pol[2 + ri] + R[3 * r + 2] * pol[4 + ri];
+      }
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = cnt + (cur_list ^ 1);
       f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1;
@@ -301,7 +368,10 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   check(cudaMemcpyAsync(h64, c64, sizeof h64, cudaMemcpyDeviceToHost, st), "stats");
   check(cudaMemcpyAsync(&err, cnt + 2, sizeof err, cudaMemcpyDeviceToHost, st), "stats");
   check(cudaStreamSynchronize(st), "radiation");
-  if (err) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+  if (err & 1u) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+  if (err & 2u)
+    throw Error{OSC_ERR_INVALID, "compute='mixed' needs observers near the beam axis (angle < 1e-2 and a correction phase "
+                                 "below 3e4 rad); use compute='fp64' for this geometry"};
   last_not_converged += (long long)h64[0];
   last_samples += (long long)h64[1];
   if (profiling) {

@@ -9,6 +9,7 @@
 
 #include "../../include/oscars_b200.h"
 #include "host_core.h"
+#include "kernels.h"
 
 namespace osc {
 
@@ -82,6 +83,17 @@ class Engine {
   // request scratch
   DevBuf obs_, nrm_, omega_, out_, lvl_, state_, part_, act_[2], cnt_;
   DevBuf acc_, acc_comp_;          // multi-particle compensated accumulation
+  // mixed-precision records (3 x float4 per sample, same indexing as the level cache)
+  DevBuf mrec_;
+  int64_t mrec_cap_ = 0;
+  int mrec_filled_ = -1;
+  uint64_t mrec_version_ = ~0ull;
+  MixedFrame frame_{};
+  void ensure_mixed(int L);
+  void compute_frame();
+ public:
+  int mixed_ept = 2;               // entries per thread of the mixed wave kernel
+ private:
 
   void upload_trajectory();
   void ensure_levels(int L);

@@ -78,6 +78,21 @@ struct PdFinalArgs {
   unsigned long long* samples;
 };
 
+// Frame of the mixed-precision path: origin x0 (particle start), rows of rot = e1, e2, e3 with e3 the
+// initial direction; xperp_max / z_max bound the trajectory in that frame; t_ref = t0 / c.
+struct MixedFrame {
+  double rot[9];
+  double x0[3];
+  double t_ref;
+  double xperp_max, z_max;
+};
+
+cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin, int64_t s_end, const MixedFrame& F,
+                                 float4* rec, cudaStream_t st);
+cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int64_t n_act_bound, int spans, int ept,
+                                 cudaStream_t st);
+int mixed_entries_per_cta(int ept);
+
 cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
                               int64_t s_end, double* lev, int64_t cap, int extended_level,
                               unsigned long long* bdmax_bits, cudaStream_t st);

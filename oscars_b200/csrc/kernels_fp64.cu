@@ -215,9 +215,12 @@ __global__ void __launch_bounds__(kFdThreads) k_fd_wave_fp64(FdWaveArgs A) {
           const double vx = __dsub_rn(__dmul_rn(ny, wz), __dmul_rn(wy, nz));
           const double vy = __dsub_rn(__dmul_rn(nz, wx), __dmul_rn(wz, nx));
           const double vz = __dsub_rn(__dmul_rn(nx, wy), __dmul_rn(wx, ny));
-          const double ex = __dadd_rn(__ddiv_rn(__dmul_rn(ux, ob2), den1), __ddiv_rn(vx, den2));
-          const double ey = __dadd_rn(__ddiv_rn(__dmul_rn(uy, ob2), den1), __ddiv_rn(vy, den2));
-          const double ez = __dadd_rn(__ddiv_rn(__dmul_rn(uz, ob2), den1), __ddiv_rn(vz, den2));
+          // The two amplitude terms need only relative accuracy: one quotient per term, then
+          // multiplications (the reference divides each component; the difference is ~1 ulp).
+          const double f1 = ob2 / den1, f2 = 1.0 / den2;
+          const double ex = fma(ux, f1, vx * f2);
+          const double ey = fma(uy, f1, vy * f2);
+          const double ez = fma(uz, f1, vz * f2);
           double sn, cs;
           sincos(reduce_2pi(ph), &sn, &cs);
           sxr = fma(ex, cs, sxr); sxi = fma(ex, sn, sxi);

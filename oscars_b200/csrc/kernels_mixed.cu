@@ -1,2 +1,240 @@
-// kernels_mixed.cu -- mixed-precision kernels (FP64 trajectory and retarded phase, FP32 amplitudes).
+// kernels_mixed.cu -- mixed-precision frequency-domain sum (FP64 trajectory and retarded-time
+// offsets, FP32 amplitudes, sincos and per-chunk sums folded into FP64).
+//
+// Frame: every trajectory is expressed in a frame whose origin is the particle's initial position
+// X0 and whose third axis e3 is its initial direction, so observers downstream sit near the axis.
+// With R = O - X = (Rx, Ry, Rz) in that frame and rho^2 = Rx^2 + Ry^2,
+//     D = |R| = Rz + corr,   corr = rho^2 / (Rz + D)                       (no cancellation)
+//     w (t + D/c) = w (t - z/c) + w Oz/c + (w/c) corr
+// The middle term is a constant phase per (observer, energy) entry; it multiplies the whole sum by a
+// unit complex number and drops out of |E|^2, of the polarization projection and of the phase
+// differences of the stop rule, so it is not computed.  tau_s = t - z/c (a few 1e-16 s) is formed in
+// FP64 per sample and stored as float; (w/c) corr is a few 1e3 rad, so the phase carries
+// ~1e-4..1e-3 rad of rounding per sample, which averages down as 1/sqrt(samples) in the sum.
+//
+// Amplitude (src/OSCARSSR.cc:4219), with u = n - b, om = 1 - n.b and |n| = 1:
+//     (1-b^2) u / (D^2 om^2) + n x (u x a) / (D om^2)
+//   = u (1/(D om^2)) ((1-b^2)/D + n.a) - a / (D om)        [n x (u x a) = u (n.a) - a (n.u), n.u = om]
+// with the small differences formed without cancellation from per-sample FP64-exact inputs:
+//     1 - n_z = corr / D,  u_z = (1 - b_z) - (1 - n_z),
+//     om = (1-n_z) + (1-b_z) - (1-n_z)(1-b_z) - n_x b_x - n_y b_y.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
 #include "kernels.h"
+
+namespace osc {
+namespace dev {
+
+constexpr double kCl = 2.99792458e8;
+
+// Per-sample record, 3 x float4 = 48 bytes: (x, y, z, tau_s) (bx, by, 1-bz, 1-b^2) (ax, ay, az, 0)
+__global__ void k_mixed_records(const double* __restrict__ lev, int64_t cap, int64_t s_begin, int64_t s_end,
+                                MixedFrame F, float4* __restrict__ rec) {
+  const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= s_end) return;
+  const double t = lev[s];
+  const double dx = lev[cap + s] - F.x0[0], dy = lev[2 * cap + s] - F.x0[1], dz = lev[3 * cap + s] - F.x0[2];
+  const double bx = lev[4 * cap + s], by = lev[5 * cap + s], bz = lev[6 * cap + s];
+  const double ax = lev[7 * cap + s], ay = lev[8 * cap + s], az = lev[9 * cap + s];
+  const double* R = F.rot;  // rows: e1, e2, e3
+  const double x = R[0] * dx + R[1] * dy + R[2] * dz;
+  const double y = R[3] * dx + R[4] * dy + R[5] * dz;
+  const double z = R[6] * dx + R[7] * dy + R[8] * dz;
+  const double px = R[0] * bx + R[1] * by + R[2] * bz;
+  const double py = R[3] * bx + R[4] * by + R[5] * bz;
+  const double pz = R[6] * bx + R[7] * by + R[8] * bz;
+  const double qx = R[0] * ax + R[1] * ay + R[2] * az;
+  const double qy = R[3] * ax + R[4] * ay + R[5] * az;
+  const double qz = R[6] * ax + R[7] * ay + R[8] * az;
+  const double g2 = 1.0 - (px * px + py * py + pz * pz);       // 1 - b^2, ~1/gamma^2
+  const double ebz = (g2 + px * px + py * py) / (1.0 + pz);     // 1 - b_z without cancellation
+  const double taus = (t - F.t_ref) - z / kCl;
+  rec[3 * s] = make_float4((float)x, (float)y, (float)z, (float)taus);
+  rec[3 * s + 1] = make_float4((float)px, (float)py, (float)ebz, (float)g2);
+  rec[3 * s + 2] = make_float4((float)qx, (float)qy, (float)qz, 0.f);
+}
+
+constexpr int kMxThreads = 128;
+constexpr int kMxChunk = 256;
+constexpr int kMxFold = 32;  // FP32 partial sums are folded into FP64 every kMxFold samples
+
+struct MixedStage {
+  float4 v[2][kMxChunk * 3];
+  uint64_t bar[2];
+};
+
+constexpr float kTwoPiHiF = 6.28318548202514648f;     // RN_f(2 pi)
+constexpr float kTwoPiLoF = -1.7484556e-07f;         // RN_f(2 pi - kTwoPiHiF)
+constexpr float kInvTwoPiF = 0.159154943f;
+
+template <int EPT>
+__global__ void __launch_bounds__(kMxThreads) k_fd_wave_mixed(FdWaveArgs A, MixedFrame F) {
+  __shared__ __align__(16) MixedStage st;
+  const int tid = threadIdx.x;
+  const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
+  const int64_t tile0 = (int64_t)blockIdx.x * kMxThreads * EPT;
+  if (tile0 >= n_act) return;
+  const float4* rec = reinterpret_cast<const float4*>(A.lev);
+  // entry constants
+  float Ox[EPT], Oy[EPT], Oz[EPT], w[EPT], wc[EPT];
+  bool live[EPT];
+  int64_t slot[EPT];
+#pragma unroll
+  for (int e = 0; e < EPT; ++e) {
+    slot[e] = tile0 + (int64_t)e * kMxThreads + tid;
+    live[e] = slot[e] < n_act;
+    const int64_t item = live[e] ? (A.act ? (int64_t)A.act[slot[e]] : slot[e]) : 0;
+    const int64_t io = item / A.n_e, ie = item % A.n_e;
+    const double* R = F.rot;
+    const double ox = A.obs[3 * io] - F.x0[0], oy = A.obs[3 * io + 1] - F.x0[1], oz = A.obs[3 * io + 2] - F.x0[2];
+    const double fx = R[0] * ox + R[1] * oy + R[2] * oz;
+    const double fy = R[3] * ox + R[4] * oy + R[5] * oz;
+    const double fz = R[6] * ox + R[7] * oy + R[8] * oz;
+    Ox[e] = (float)fx; Oy[e] = (float)fy; Oz[e] = (float)fz;
+    const double om = A.omega[ie];
+    w[e] = (float)om;
+    wc[e] = (float)(om / kCl);
+    // validity of the near-axis phase form: small angle from the frame axis and a bounded
+    // correction phase (see the file comment); otherwise the caller must use the FP64 path
+    const double rho = sqrt(fx * fx + fy * fy) + F.xperp_max;
+    const double rz = fz - F.z_max;
+    if (live[e] && !(rz > 0 && rho < 1e-2 * rz && (om / kCl) * rho * rho / (2 * rz) < 3e4)) atomicOr(A.err, kErrBadArgs);
+  }
+  const int span = blockIdx.y;
+  if (tid == 0) {
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  uint32_t phase_bits = 0;
+  for (int g = 0; g < A.nseg; ++g) {
+    const int64_t b0 = A.seg_b[g] + (int64_t)span * A.span_len[g];
+    const int64_t b1 = min(A.seg_e[g], b0 + A.span_len[g]);
+    double S[EPT][6];
+    float first[EPT], last[EPT], dmax[EPT];
+    bool have[EPT];
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) S[e][k] = 0.0;
+      first[e] = last[e] = 0.f;
+      dmax[e] = 0.f;
+      have[e] = false;
+    }
+    const int64_t nchunks = b1 > b0 ? (b1 - b0 + kMxChunk - 1) / kMxChunk : 0;
+    if (tid == 0 && nchunks > 0) {
+      const int64_t hi = min(b1, b0 + kMxChunk);
+      mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - b0) * 48));
+      tma_load_1d(&st.v[0][0], rec + 3 * b0, (uint32_t)((hi - b0) * 48), &st.bar[0]);
+    }
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const int buf = (int)(c & 1);
+      const int64_t lo = b0 + c * kMxChunk, hi = min(b1, lo + kMxChunk);
+      if (tid == 0 && c + 1 < nchunks) {
+        const int64_t lo2 = lo + kMxChunk, hi2 = min(b1, lo2 + kMxChunk);
+        mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * 48));
+        tma_load_1d(&st.v[buf ^ 1][0], rec + 3 * lo2, (uint32_t)((hi2 - lo2) * 48), &st.bar[buf ^ 1]);
+      }
+      if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+        if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+        return;
+      }
+      phase_bits ^= 1u << buf;
+      const float4* sv = st.v[buf];
+      const int j0 = lo == 0 ? 1 : 0;  // sample 0 is the unused slot
+      const int n = (int)(hi - lo);
+      for (int jb = j0; jb < n; jb += kMxFold) {
+        const int je = min(n, jb + kMxFold);
+        float s32[EPT][6];
+#pragma unroll
+        for (int e = 0; e < EPT; ++e)
+#pragma unroll
+          for (int k = 0; k < 6; ++k) s32[e][k] = 0.f;
+        for (int j = jb; j < je; ++j) {
+          const float4 r0 = sv[3 * j], r1 = sv[3 * j + 1], r2 = sv[3 * j + 2];
+#pragma unroll
+          for (int e = 0; e < EPT; ++e) {
+            const float rx = Ox[e] - r0.x, ry = Oy[e] - r0.y, rz = Oz[e] - r0.z;
+            const float rho2 = fmaf(rx, rx, ry * ry);
+            const float d2 = fmaf(rz, rz, rho2);
+            const float iD = rsqrtf(d2);
+            const float q = rho2 * iD * iD;                                  // (rho/D)^2
+            const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);           // rho^2/(Rz+D), |rho/D| < 1e-2
+            const float ph = fmaf(wc[e], corr, w[e] * r0.w);
+            if (have[e]) {
+              const float dp = fabsf(ph - last[e]);
+              dmax[e] = fmaxf(dmax[e], dp);
+            } else {
+              first[e] = ph;
+              have[e] = true;
+            }
+            last[e] = ph;
+            const float k = rintf(ph * kInvTwoPiF);
+            const float rr = fmaf(-k, kTwoPiLoF, fmaf(-k, kTwoPiHiF, ph));
+            float sn, cs;
+            __sincosf(rr, &sn, &cs);
+            const float nx = rx * iD, ny = ry * iD;
+            const float en = corr * iD;                                      // 1 - n_z
+            const float ux = nx - r1.x, uy = ny - r1.y, uz = r1.z - en;
+            const float om = fmaf(-nx, r1.x, fmaf(-ny, r1.y, fmaf(-en, r1.z, en + r1.z)));
+            const float io = __frcp_rn(om);
+            const float na = fmaf(nx, r2.x, fmaf(ny, r2.y, (1.f - en) * r2.z));
+            const float k1 = io * io * iD * fmaf(r1.w, iD, na);
+            const float k2 = io * iD;
+            const float ex = fmaf(k1, ux, -k2 * r2.x);
+            const float ey = fmaf(k1, uy, -k2 * r2.y);
+            const float ez = fmaf(k1, uz, -k2 * r2.z);
+            s32[e][0] = fmaf(ex, cs, s32[e][0]); s32[e][1] = fmaf(ex, sn, s32[e][1]);
+            s32[e][2] = fmaf(ey, cs, s32[e][2]); s32[e][3] = fmaf(ey, sn, s32[e][3]);
+            s32[e][4] = fmaf(ez, cs, s32[e][4]); s32[e][5] = fmaf(ez, sn, s32[e][5]);
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < EPT; ++e)
+#pragma unroll
+          for (int k = 0; k < 6; ++k) S[e][k] += (double)s32[e][k];
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      if (!live[e]) continue;
+      const int64_t ps = A.part_stride;
+      double* p = A.part + ((int64_t)(g * gridDim.y + span) * kFdPartials) * ps + slot[e];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) p[k * ps] = S[e][k];
+      p[6 * ps] = have[e] ? (double)first[e] : 0.0;
+      p[7 * ps] = have[e] ? (double)last[e] : 0.0;
+      p[8 * ps] = have[e] ? (double)dmax[e] : -1.0;
+    }
+  }
+}
+
+}  // namespace dev
+
+cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin, int64_t s_end, const MixedFrame& F,
+                                 float4* rec, cudaStream_t st) {
+  if (s_end <= s_begin) return cudaSuccess;
+  const int T = 256;
+  dev::k_mixed_records<<<(unsigned)((s_end - s_begin + T - 1) / T), T, 0, st>>>(lev, cap, s_begin, s_end, F, rec);
+  return cudaGetLastError();
+}
+
+int mixed_entries_per_cta(int ept) { return dev::kMxThreads * ept; }
+
+cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int64_t n_act_bound, int spans, int ept,
+                                 cudaStream_t st) {
+  const int64_t per = (int64_t)dev::kMxThreads * ept;
+  const int64_t tiles = (n_act_bound + per - 1) / per;
+  if (tiles == 0) return cudaSuccess;
+  const dim3 grid((unsigned)tiles, (unsigned)spans);
+  if (ept == 1) dev::k_fd_wave_mixed<1><<<grid, dev::kMxThreads, 0, st>>>(a, F);
+  else if (ept == 2) dev::k_fd_wave_mixed<2><<<grid, dev::kMxThreads, 0, st>>>(a, F);
+  else dev::k_fd_wave_mixed<4><<<grid, dev::kMxThreads, 0, st>>>(a, F);
+  return cudaGetLastError();
+}
+
+}  // namespace osc

@@ -1,0 +1,99 @@
+"""Mixed-precision path (compute='mixed') against the plain FP64 GPU path.
+
+Tolerance: peak-normalised relative error max_i |F_i - F64_i| / max_i |F64_i| <= 1e-4, at a fixed
+level (precision=0, max_level=L) so that both paths integrate exactly the same samples.  The FP64
+path itself matches the reference to <= 1e-9 (test_gpu_parity.py).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from cases import E1_EPU, E1_U, EPU_SETUP, UND_SETUP, run_case
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def _sr():
+    from oscars_b200.sr import sr
+    return sr(gpu=1)
+
+
+def _vals(res):
+    return np.array([r[1] for r in res], dtype=np.float64)
+
+
+def _pair(setup, call, kw):
+    out = []
+    for compute in ("fp64", "mixed"):
+        s = _sr()
+        run_case(s, setup)
+        out.append(_vals(getattr(s, call)(**dict(kw, compute=compute))))
+    return out
+
+
+def _err(a, ref):
+    return float(np.max(np.abs(a - ref)) / np.max(np.abs(ref)))
+
+
+def test_flux_201x201_fixed_level_12():
+    f64, mx = _pair(UND_SETUP, "calculate_flux_rectangle",
+                    dict(energy_eV=E1_U, npoints=[201, 201], width=[0.01, 0.01], translation=[0, 0, 30],
+                         precision=0, max_level=12))
+    e = _err(mx, f64)
+    print("flux 201x201 L=12 mixed vs fp64: %.3e" % e)
+    assert e <= TOL
+
+
+def test_spectrum_2000_fixed_level_13():
+    f64, mx = _pair(UND_SETUP, "calculate_spectrum",
+                    dict(obs=[0, 0, 30], energy_range_eV=[100, 3000], npoints=2000, precision=0, max_level=13))
+    e = _err(mx, f64)
+    print("spectrum 2000 L=13 mixed vs fp64: %.3e" % e)
+    assert e <= TOL
+
+
+@pytest.mark.parametrize("pol", ["lh", "lv", "cl", "cr"])
+def test_polarized_flux_epu(pol):
+    f64, mx = _pair(EPU_SETUP, "calculate_flux_rectangle",
+                    dict(energy_eV=E1_EPU, npoints=[41, 41], width=[0.008, 0.008], translation=[0, 0, 30],
+                         precision=0, max_level=11, polarization=pol))
+    assert _err(mx, f64) <= TOL
+
+
+def test_off_axis_beam_frame():
+    """Tilted, displaced beam: the mixed path works in the particle's own frame."""
+    setup = [("add_bfield_undulator", dict(bfield=[0, 0.5, 0], period=[0, 0.0, 0.05], nperiods=21, phase=-math.pi / 2,
+                                           translation=[0.001, 0, 0])),
+             ("set_particle_beam", dict(type="electron", energy_GeV=3, x0=[0.001, -0.0005, -1.2], d0=[0.0003, 0.0001, 1],
+                                        current=0.5)),
+             ("set_ctstartstop", dict(start=-0.2, stop=2.4)), ("set_npoints_trajectory", dict(n=12001))]
+    f64, mx = _pair(setup, "calculate_flux_rectangle",
+                    dict(energy_eV=2 * E1_U, npoints=[31, 31], width=[0.006, 0.006], translation=[0.01, 0.003, 30],
+                         precision=0, max_level=11))
+    assert _err(mx, f64) <= TOL
+
+
+def test_adaptive_mode_close_to_fp64():
+    """Adaptive stop levels may differ where a level's relative change sits at the threshold."""
+    out, lev = [], []
+    for compute in ("fp64", "mixed"):
+        s = _sr()
+        run_case(s, UND_SETUP)
+        out.append(_vals(s.calculate_flux_rectangle(energy_eV=E1_U, npoints=[101, 101], width=[0.01, 0.01],
+                                                    translation=[0, 0, 30], compute=compute)))
+        lev.append(s.last_levels.copy())
+    frac = float(np.mean(lev[0] != lev[1]))
+    print("adaptive: %.4f of entries stop at another level; error %.3e" % (frac, _err(out[1], out[0])))
+    assert frac <= 0.01
+    assert _err(out[1], out[0]) <= 5e-3
+
+
+def test_far_off_axis_observer_is_rejected():
+    s = _sr()
+    run_case(s, UND_SETUP)
+    with pytest.raises(ValueError, match="compute='mixed' needs observers near the beam axis"):
+        s.calculate_spectrum(obs=[3, 0, 30], energy_range_eV=[100, 200], npoints=3, compute="mixed")
+    with pytest.raises(ValueError, match="power density runs in FP64"):
+        s.calculate_power_density_rectangle(npoints=[3, 3], width=[0.01, 0.01], translation=[0, 0, 30], compute="mixed")
