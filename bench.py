@@ -219,25 +219,25 @@ def product_arm(args):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    sm, ln = ctypes.c_longlong(), ctypes.c_longlong()
+    ctx.call("osc_last_stats", ctypes.byref(sm), ctypes.byref(ln))  # the job is identical every step
+    samples_per_step, launches_per_step = sm.value, ln.value
     ctx.call("osc_set_profiling", 1)
     ctx.call("osc_get_profile", None, None, None, 1)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    samples = 0
-    launches = 0
     with ClockSampler(local) as clk:
+        time.sleep(0.1)
         for i in range(args.steps):
             flush.zero_()
             evs[i][0].record(stream)
             step()
             evs[i][1].record(stream)
-            sm, ln = ctypes.c_longlong(), ctypes.c_longlong()
-            ctx.call("osc_last_stats", ctypes.byref(sm), ctypes.byref(ln))
-            samples += sm.value
-            launches += ln.value
         torch.cuda.synchronize()
+    samples = samples_per_step * args.steps
+    launches = launches_per_step * args.steps
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -258,8 +258,12 @@ def product_arm(args):
 
     if args.quick:
         if rank == 0:
-            print(json.dumps({"quick": True, "value": value, "unit": "Gsamples/s", "ms_per_step": ms_max / args.steps,
-                              "kernel_ms": kms.value, "kernel_launches": kl.value}), flush=True)
+            v, nv = ctypes.c_int(), ctypes.c_int()
+            ctx.call("osc_get_variant", 2 if args.compute == "mixed" else 0, ctypes.byref(v), ctypes.byref(nv))
+            print(json.dumps({"quick": True, "compute": args.compute, "value": value, "unit": "Gsamples/s",
+                              "ms_per_step": ms_max / args.steps, "kernel_ms_per_step": kms.value / args.steps,
+                              "kernel_launches": kl.value, "variant": v.value, "samples_per_step": samples_per_step,
+                              "clocks": clk.summary()}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return

@@ -187,6 +187,12 @@ OSC_API int osc_last_stats(osc_ctx* ctx, long long* samples, long long* launches
 OSC_API int osc_set_profiling(osc_ctx* ctx, int enable);
 OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches, long long* samples,
                             int reset);
+/* Kernel variants of the sample sums.  kind 0 = FP64 flux/spectrum, 2 = mixed flux/spectrum.
+ * variant >= 0 forces a compiled variant; -1 (default) lets the context autotune: the first call
+ * of each request shape times every variant and keeps the fastest.  osc_get_variant reports the
+ * variant the last request of that kind used and the number of compiled variants. */
+OSC_API int osc_set_variant(osc_ctx* ctx, int kind, int variant);
+OSC_API int osc_get_variant(osc_ctx* ctx, int kind, int* variant, int* n_variants);
 /* Drop the device-side level-sample cache (it is rebuilt by the next radiation call). */
 OSC_API int osc_drop_level_cache(osc_ctx* ctx);
 /* Measured arithmetic peak of this GPU: an FMA-throughput loop in FP64 (kind 0) or FP32 (kind 1),

@@ -72,6 +72,8 @@ SIGNATURES = {
     "osc_last_stats": (I, [VP, LLP, LLP]),
     "osc_set_profiling": (I, [VP, I]),
     "osc_get_profile": (I, [VP, DP, LLP, LLP, I]),
+    "osc_set_variant": (I, [VP, I, I]),
+    "osc_get_variant": (I, [VP, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
     "osc_drop_level_cache": (I, [VP]),
     "osc_measure_fma_peak": (I, [VP, I, DP]),
 }

@@ -400,6 +400,7 @@ OSC_API int osc_power_density_device(osc_ctx* ctx, const double* d_obs_xyz, cons
 
 OSC_API int osc_last_stats(osc_ctx* ctx, long long* samples, long long* launches) {
   return guarded(ctx, [&] {
+    ctx->eng->collect();
     if (samples) *samples = ctx->eng->last_samples;
     if (launches) *launches = ctx->eng->last_launches;
   });
@@ -412,10 +413,28 @@ OSC_API int osc_set_profiling(osc_ctx* ctx, int enable) {
 OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches, long long* samples, int reset) {
   return guarded(ctx, [&] {
     osc::Engine& E = *ctx->eng;
+    E.collect();
     if (kernel_ms) *kernel_ms = E.prof_ms;
     if (launches) *launches = E.prof_launches;
     if (samples) *samples = E.prof_samples;
     if (reset) { E.prof_ms = 0; E.prof_launches = 0; E.prof_samples = 0; }
+  });
+}
+
+OSC_API int osc_set_variant(osc_ctx* ctx, int kind, int variant) {
+  return guarded(ctx, [&] {
+    if (kind != 0 && kind != 2) throw osc::Error{OSC_ERR_INVALID, "kind must be 0 (fp64) or 2 (mixed)"};
+    const int n = kind == 2 ? osc::kMixedVariants : osc::kFp64Variants;
+    if (variant < -1 || variant >= n) throw osc::Error{OSC_ERR_RANGE, "variant out of range"};
+    ctx->eng->forced_variant[kind] = variant;
+  });
+}
+
+OSC_API int osc_get_variant(osc_ctx* ctx, int kind, int* variant, int* n_variants) {
+  return guarded(ctx, [&] {
+    if (kind != 0 && kind != 2) throw osc::Error{OSC_ERR_INVALID, "kind must be 0 (fp64) or 2 (mixed)"};
+    if (variant) *variant = ctx->eng->variant_in_use(kind);
+    if (n_variants) *n_variants = kind == 2 ? osc::kMixedVariants : osc::kFp64Variants;
   });
 }
 

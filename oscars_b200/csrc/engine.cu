@@ -52,6 +52,13 @@ Engine::Engine(int dev) : device(dev) {
   check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
   bd_bits_.reserve(32 * sizeof(unsigned long long));
   cnt_.reserve(64);
+  check(cudaMemset(cnt_.p, 0, 64), "memset");
+  check(cudaHostAlloc(reinterpret_cast<void**>(&stats_host_), 8 * sizeof(unsigned long long), cudaHostAllocDefault),
+        "cudaHostAlloc");
+  check(cudaHostAlloc(reinterpret_cast<void**>(&stage_host_), kStageDoubles * sizeof(double), cudaHostAllocDefault),
+        "cudaHostAlloc");
+  for (int i = 0; i < 2; ++i) check(cudaEventCreateWithFlags(&stats_ev_[i], cudaEventDisableTiming), "event");
+  check(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming), "event");
 }
 
 Engine::~Engine() {
@@ -60,6 +67,10 @@ Engine::~Engine() {
   if (stream) cudaStreamSynchronize(stream);
   for (auto& e : ev_pending_) { ev_pool_.push_back(e.first); ev_pool_.push_back(e.second); }
   for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
+  for (int i = 0; i < 2; ++i) if (stats_ev_[i]) cudaEventDestroy(stats_ev_[i]);
+  if (stage_ev_) cudaEventDestroy(stage_ev_);
+  if (stats_host_) cudaFreeHost(stats_host_);
+  if (stage_host_) cudaFreeHost(stage_host_);
   for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
                     &act_[1], &cnt_, &acc_, &acc_comp_})
     b->release();
@@ -176,20 +187,6 @@ void Engine::ensure_mixed(int L) {
   mrec_filled_ = L;
 }
 
-void Engine::refresh_bdmax() {
-  if (bdmax_valid_) return;
-  unsigned long long bits[32];
-  check(cudaMemcpyAsync(bits, bd_bits_.p, sizeof(bits), cudaMemcpyDeviceToHost, stream), "bdmax");
-  check(cudaStreamSynchronize(stream), "bdmax");
-  bdmax_.assign(32, -1.0);
-  for (int L = 1; L < 32; ++L) {
-    double d;
-    std::memcpy(&d, &bits[L], sizeof d);
-    bdmax_[L] = d;
-  }
-  bdmax_valid_ = true;
-}
-
 static double dt_inclusive(double tstart, double tstop, int L) {  // :224-237
   return (tstop - tstart) / (std::pow(2., L + 1) - 1);
 }
@@ -226,14 +223,64 @@ static void polarization_vector(const osc_rad_opts& o, double P[6], bool& projec
   project = o.polarization != OSC_POL_ALL && m2 > 0.001;
 }
 
-// Spans per wave: split each level into spans so that a wave launch is >= 4 full waves of CTAs
-// (148 SMs x ~7 resident CTAs); a span keeps >= 32 samples.
-static int choose_spans(int64_t n_act, int64_t level_len) {
-  const int64_t tiles = (n_act + 127) / 128;
-  const int64_t target = 148 * 7 * 4;
-  int64_t spans = 1;
-  while (tiles * spans < target && level_len / (spans * 2) >= 32) spans *= 2;
-  return (int)spans;
+// Levels resident before a request starts: every wave up to this level is enqueued without any
+// host round trip; entries still unconverged after it make the host extend the cache.
+constexpr int kPrefillLevel = 14;
+constexpr int kMinSpan = 32;
+
+int Engine::wave_grid(int kind, int variant) {
+  if (wave_grid_[kind][variant] == 0) {
+    int sms = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
+    const int per = kind == 2 ? mixed_blocks_per_sm(variant) : fp64_blocks_per_sm(kind == 1, variant);
+    wave_grid_[kind][variant] = sms * per;
+  }
+  return wave_grid_[kind][variant];
+}
+
+// Autotuner: the first request of a given shape (kind, size class, level range) runs the waves
+// with every compiled variant of the sample-sum kernel into scratch outputs, times them with CUDA
+// events, and keeps the fastest for that shape.  FP64 variants differ only in their register cap,
+// so they give bit-identical sums; mixed variants also change entries per thread.
+int Engine::pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out,
+                         int32_t* d_lvl, cudaStream_t st) {
+  if (forced_variant[kind] >= 0) return forced_variant[kind];
+  if (!autotune || tuning_ || kind == 1) return current_variant_[kind];
+  int lg = 0;
+  while (((int64_t)1 << (lg + 1)) <= n_items) ++lg;
+  const auto key = std::make_tuple(kind, lg, Lfirst, lstop);
+  auto it = tuned_.find(key);
+  if (it != tuned_.end()) return it->second;
+  const int nvar = kind == 2 ? kMixedVariants : kFp64Variants;
+  const bool prof = profiling;
+  profiling = false;
+  tuning_ = true;
+  cudaEvent_t a, b;
+  check(cudaEventCreate(&a), "event");
+  check(cudaEventCreate(&b), "event");
+  int best = current_variant_[kind];
+  float best_ms = 1e30f;
+  const long long saved_launches = last_launches;
+  for (int v = 0; v < nvar; ++v) {
+    current_variant_[kind] = v;
+    run_single(rq, n_items, 1.0, d_out, d_lvl, st);  // warm (loads the module, fills caches)
+    check(cudaEventRecord(a, st), "event");
+    run_single(rq, n_items, 1.0, d_out, d_lvl, st);
+    check(cudaEventRecord(b, st), "event");
+    check(cudaEventSynchronize(b), "event");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, a, b), "event");
+    if (ms < best_ms) { best_ms = ms; best = v; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  pending_.clear();  // the statistics of the timing runs are not the request's
+  last_launches = saved_launches;
+  tuning_ = false;
+  profiling = prof;
+  current_variant_[kind] = best;
+  tuned_[key] = best;
+  return best;
 }
 
 void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,
@@ -245,21 +292,42 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
   if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
   const Particle& P = model.particle;
-  const int Lfirst = std::min(9, lstop);
   const bool mixed = o.precision_mode == OSC_MIXED;
   if (mixed && rq.power_density)
     throw Error{OSC_ERR_INVALID, "compute='mixed' applies to flux and spectrum; power density runs in FP64"};
-  if (mixed) ensure_mixed(std::min(lstop, std::max(Lfirst, 12)));
-  else ensure_levels(std::min(lstop, std::max(Lfirst, 12)));
-  if (rq.power_density) refresh_bdmax();
+  const int Lfirst = std::min(9, lstop);
+  const int Lpre = std::min(lstop, std::max(Lfirst, kPrefillLevel));
+  if (mixed) ensure_mixed(Lpre);
+  else ensure_levels(Lpre);
 
-  unsigned* cnt = cnt_.as<unsigned>();  // [0] n_act A, [1] n_act B, [2] err
-  unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);  // [0] not conv, [1] samples
-  check(cudaMemsetAsync(cnt, 0, 64, st), "memset");
+  const int kind = rq.power_density ? 1 : (mixed ? 2 : 0);
+  const int variant = tuning_ ? current_variant_[kind]
+                              : pick_variant(kind, const_cast<RadRequest&>(rq), n_items, Lfirst, lstop, d_out, d_lvl, st);
+  const int grid = wave_grid(kind, variant);
+  const int tile = mixed ? mixed_entries_per_cta(variant) : 128;
+  const int64_t target = 8 * (int64_t)grid;
   const int64_t N = n_items;
+  // partial-sum buffer: the largest plan over every possible active count of every level
+  size_t part_doubles = 0;
+  const int per = rq.power_density ? 1 : kFdPartials;
+  for (int L = Lfirst; L <= lstop; ++L) {
+    for (int64_t t = 1; t <= (N + tile - 1) / tile; t = t < 64 ? t + 1 : t * 2) {
+      const int64_t n = std::min(N, t * tile);
+      const WavePlan pl = wave_plan(L == Lfirst, L, n, tile, target, kMinSpan);
+      part_doubles = std::max(part_doubles, (size_t)pl.nseg * pl.spans * per * n);
+    }
+    const WavePlan pl = wave_plan(L == Lfirst, L, N, tile, target, kMinSpan);
+    part_doubles = std::max(part_doubles, (size_t)pl.nseg * pl.spans * per * N);
+  }
+  part_.reserve(sizeof(double) * part_doubles);
   act_[0].reserve(sizeof(int) * N);
   act_[1].reserve(sizeof(int) * N);
   state_.reserve(sizeof(double) * 7 * N);
+
+  unsigned* cnt = cnt_.as<unsigned>();  // [0], [1] list counts, [2] sticky error word
+  unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);  // [0] not converged, [1] samples
+  check(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), st), "memset");
+  check(cudaMemsetAsync(c64, 0, 2 * sizeof(unsigned long long), st), "memset");
 
   const double* d_obs = obs_.as<double>();
   const double* d_nrm = rq.normals ? nrm_.as<double>() : nullptr;
@@ -271,112 +339,174 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     c0 = P.q / (four_pi() * kC * kEps0 * kSqrt2Pi);                                       // :4106
     const double cur = rq.spectrum_current_abs ? std::fabs(P.current) : P.current;
     c2 = four_pi() * cur / (kH * std::fabs(P.q) * kMu0 * kC) * 1e-6 * 0.001;              // :4109
+    if (mixed) {  // project in the frame: P' = R P (R orthogonal, so E'.P' = E.P)
+      double pr[6];
+      const double* R = frame_.rot;
+      for (int ri = 0; ri < 2; ++ri)
+        for (int r = 0; r < 3; ++r)
+          pr[2 * r + ri] = R[3 * r] * pol[ri] + R[3 * r + 1] * pol[2 + ri] + R[3 * r + 2] * pol[4 + ri];
+      for (int i = 0; i < 6; ++i) pol[i] = pr[i];
+    }
   } else {
     scale = std::fabs(P.q * P.current) / (16 * (kPi * kPi) * kEps0 * kC);                 // :2945
   }
 
   int cur_list = 0;
-  int64_t n_act = N;  // host bound on the current list size
-  for (int L = Lfirst; L <= lstop; ++L) {
+  auto launch_wave = [&](int L) {
     const bool first = L == Lfirst;
-    if (!first) {
-      // the finalize of the previous wave appended the survivors to list (cur_list ^ 1)
-      unsigned nn = 0;
-      check(cudaMemcpyAsync(&nn, cnt + (cur_list ^ 1), sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
-      check(cudaStreamSynchronize(st), "count");
-      if (nn == 0) break;
-      cur_list ^= 1;
-      check(cudaMemsetAsync(cnt + (cur_list ^ 1), 0, sizeof(unsigned), st), "memset");
-      n_act = nn;
-      if (mixed) ensure_mixed(L);
-      else ensure_levels(L);
-      if (rq.power_density) refresh_bdmax();
-    }
-    const int nseg = first && L >= 1 ? 2 : 1;
-    int64_t sb[2], se[2];
-    if (first) {
-      if (nseg == 2) { sb[0] = 1; se[0] = (int64_t)1 << L; sb[1] = (int64_t)1 << L; se[1] = (int64_t)2 << L; }
-      else { sb[0] = 1; se[0] = 2; }
-    } else {
-      sb[0] = (int64_t)1 << L; se[0] = (int64_t)2 << L;
-    }
-    const int spans = choose_spans(mixed ? (n_act + mixed_ept - 1) / mixed_ept : n_act, (int64_t)1 << L);
-    int64_t sl[2] = {0, 0};
-    for (int g = 0; g < nseg; ++g) {
-      const int64_t len = se[g] - (sb[g] & ~(int64_t)1);
-      sl[g] = ((len + spans - 1) / spans + 1) & ~(int64_t)1;
-    }
-    const int64_t part_stride = n_act;
     const int* act_in = first ? nullptr : act_[cur_list].as<int>();
     const unsigned* nact_in = first ? nullptr : cnt + cur_list;
+    unsigned* n_next = cnt + (cur_list ^ 1);
+    check(cudaMemsetAsync(n_next, 0, sizeof(unsigned), st), "memset");
     if (!rq.power_density) {
-      part_.reserve(sizeof(double) * (size_t)nseg * spans * kFdPartials * part_stride);
       FdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
       w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
-      w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in; w.nseg = nseg;
-      for (int g = 0; g < nseg; ++g) { w.seg_b[g] = sb[g] & ~(int64_t)1; w.seg_e[g] = se[g]; w.span_len[g] = sl[g]; }
-      w.part = part_.as<double>(); w.part_stride = part_stride; w.err = cnt + 2;
-      if (mixed) {  // the mixed records need no even-index alignment
-        for (int g = 0; g < nseg; ++g) w.seg_b[g] = sb[g] == 1 ? 0 : sb[g];
-      }
+      w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
+      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
+      w.part = part_.as<double>(); w.err = cnt + 2;
       auto ev = timed_begin(st);
-      if (mixed) check(launch_fd_wave_mixed(w, frame_, n_act, spans, mixed_ept, st), "flux wave (mixed)");
-      else check(launch_fd_wave_fp64(w, n_act, spans, st), "flux wave");
+      if (mixed) check(launch_fd_wave_mixed(w, frame_, grid, variant, st), "flux wave (mixed)");
+      else check(launch_fd_wave_fp64(w, grid, variant, st), "flux wave");
       timed_end(ev, st);
       FdFinalArgs f{};
-      f.part = part_.as<double>(); f.part_stride = part_stride; f.spans = spans; f.nseg = nseg; f.first = first;
-      f.level = L; f.max_level = lstop; f.quantity = o.quantity; f.project = project;
+      f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
+      f.project = project; f.tile_entries = tile; f.min_span = kMinSpan; f.target_units = target;
       f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
       f.precision = o.precision; f.c0 = c0; f.c2 = c2; f.weight = weight;
       for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
-      if (mixed) {  // project in the frame: P' = R P (R orthogonal, so E'.P' = E.P)
-        const double* R = frame_.rot;
-        for (int ri = 0; ri < 2; ++ri)
-          for (int r = 0; r < 3; ++r)
-            f.pol[2 * r + ri] = R[3 * r] * pol[ri] + R[3 * r + 1] * pol[2 + ri] + R[3 * r + 2] * pol[4 + ri];
-      }
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
-      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = cnt + (cur_list ^ 1);
+      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
       f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1;
-      check(launch_fd_finalize(f, n_act, st), "flux finalize");
+      check(launch_fd_finalize(f, N, st), "flux finalize");
     } else {
-      part_.reserve(sizeof(double) * (size_t)nseg * spans * part_stride);
       PdWaveArgs w{};
       w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
-      w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in; w.nseg = nseg;
-      for (int g = 0; g < nseg; ++g) { w.seg_b[g] = sb[g] & ~(int64_t)1; w.seg_e[g] = se[g]; w.span_len[g] = sl[g]; }
-      w.part = part_.as<double>(); w.part_stride = part_stride; w.err = cnt + 2;
+      w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
+      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
+      w.part = part_.as<double>(); w.err = cnt + 2;
       auto ev = timed_begin(st);
-      check(launch_pd_wave_fp64(w, n_act, spans, st), "power density wave");
+      check(launch_pd_wave_fp64(w, grid, st), "power density wave");
       timed_end(ev, st);
       PdFinalArgs f{};
-      f.part = part_.as<double>(); f.part_stride = part_stride; f.spans = spans; f.nseg = nseg; f.first = first;
-      f.level = L; f.max_level = lstop; f.quantity = o.quantity; f.directional = rq.directional;
+      f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
+      f.directional = rq.directional; f.tile_entries = tile; f.min_span = kMinSpan; f.target_units = target;
       f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
-      f.precision = o.precision; f.scale = scale; f.weight = weight; f.bdmax = bdmax_[L];
-      f.two_over_gamma = 2. / P.gamma;
+      f.precision = o.precision; f.scale = scale; f.weight = weight; f.two_over_gamma = 2. / P.gamma;
+      f.bdmax_levels = reinterpret_cast<const double*>(bd_bits_.p);
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
-      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = cnt + (cur_list ^ 1);
+      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
       f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1;
-      check(launch_pd_finalize(f, n_act, st), "power density finalize");
+      check(launch_pd_finalize(f, N, st), "power density finalize");
     }
     last_launches += 2;
+    cur_list ^= 1;
+  };
+  for (int L = Lfirst; L <= Lpre; ++L) launch_wave(L);
+  for (int L = Lpre + 1; L <= lstop; ++L) {  // beyond the prefilled levels the host decides
+    unsigned nn = 0;
+    check(cudaMemcpyAsync(&nn, cnt + cur_list, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
+    check(cudaStreamSynchronize(st), "count");
+    if (nn == 0) break;
+    if (mixed) ensure_mixed(L);
+    else ensure_levels(L);
+    launch_wave(L);
   }
-  unsigned long long h64[2];
+  // statistics of this particle go to pinned memory; collect() reads them after the request
+  const int slot = stats_slot_++ & 1;
+  check(cudaMemcpyAsync(stats_host_ + 4 * slot, c64, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
+        "stats");
+  check(cudaEventRecord(stats_ev_[slot], st), "event");
+  pending_.push_back(slot);
+}
+
+// Wait for the statistics of the enqueued particles of the last request and report device errors.
+void Engine::collect() {
+  if (device < 0) return;
+  for (int slot : pending_) {
+    check(cudaEventSynchronize(stats_ev_[slot]), "radiation");
+    last_not_converged += (long long)stats_host_[4 * slot];
+    last_samples += (long long)stats_host_[4 * slot + 1];
+    if (profiling) prof_samples += (long long)stats_host_[4 * slot + 1];
+  }
+  pending_.clear();
+  if (profiling) collect_timings();
   unsigned err = 0;
-  check(cudaMemcpyAsync(h64, c64, sizeof h64, cudaMemcpyDeviceToHost, st), "stats");
-  check(cudaMemcpyAsync(&err, cnt + 2, sizeof err, cudaMemcpyDeviceToHost, st), "stats");
-  check(cudaStreamSynchronize(st), "radiation");
-  if (err & 1u) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
-  if (err & 2u)
-    throw Error{OSC_ERR_INVALID, "compute='mixed' needs observers near the beam axis (angle < 1e-2 and a correction phase "
-                                 "below 3e4 rad); use compute='fp64' for this geometry"};
-  last_not_converged += (long long)h64[0];
-  last_samples += (long long)h64[1];
-  if (profiling) {
-    collect_timings();
-    prof_samples += (long long)h64[1];
+  check(cudaMemcpy(&err, cnt_.as<unsigned>() + 2, sizeof err, cudaMemcpyDeviceToHost), "error word");
+  if (err) {
+    check(cudaMemset(cnt_.as<unsigned>() + 2, 0, sizeof(unsigned)), "error word");
+    if (err & 1u) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+    throw Error{OSC_ERR_INVALID, "compute='mixed' needs observers near the beam axis (angle < 1e-2 and a correction "
+                                 "phase below 3e4 rad); use compute='fp64' for this geometry"};
+  }
+}
+
+void Engine::radiation(RadRequest& rq) {
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  check(cudaSetDevice(device), "cudaSetDevice");
+  collect();  // the previous request's statistics and deferred errors
+  last_samples = last_launches = last_not_converged = 0;
+  cudaStream_t st = rq.stream ? rq.stream : stream;
+  const int64_t n_e = rq.power_density ? 1 : (int64_t)rq.omega.size();
+  const int64_t N = rq.n_obs * n_e;
+  if (N <= 0) return;
+  if (N > 2147483647ll) throw Error{OSC_ERR_LENGTH, "more than 2^31-1 (observer, energy) entries in one call"};
+  // inputs
+  const cudaMemcpyKind in_kind = rq.obs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  obs_.reserve(sizeof(double) * 3 * rq.n_obs);
+  check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, in_kind, st), "obs");
+  if (rq.normals) {
+    nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
+    check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, in_kind, st), "normals");
+  }
+  if (!rq.power_density) {
+    omega_.reserve(sizeof(double) * n_e);
+    if (n_e <= kStageDoubles) {  // small vectors go through pinned memory so the copy stays asynchronous
+      check(cudaEventSynchronize(stage_ev_), "stage");
+      std::memcpy(stage_host_, rq.omega.data(), sizeof(double) * n_e);
+      check(cudaMemcpyAsync(omega_.p, stage_host_, sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
+      check(cudaEventRecord(stage_ev_, st), "event");
+    } else {
+      check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
+    }
+  }
+  out_.reserve(sizeof(double) * N);
+  lvl_.reserve(sizeof(int32_t) * N);
+  double* d_out = rq.out_on_device ? rq.out : out_.as<double>();
+  int32_t* d_lvl = rq.out_on_device ? rq.level_out : lvl_.as<int32_t>();
+  if (!d_lvl) d_lvl = lvl_.as<int32_t>();
+
+  const int np = rq.opts.nparticles;
+  if (np <= 0) {
+    model.ensure_trajectory();
+    upload_trajectory();
+    run_single(rq, N, 1.0, d_out, d_lvl, st);
+  } else {
+    // src/OSCARSSR.cc:4026-4062: new random particle, its trajectory, weight 1/N, compensated sum
+    const double weight = 1.0 / (double)np;
+    acc_.reserve(sizeof(double) * N);
+    acc_comp_.reserve(sizeof(double) * N);
+    check(cudaMemsetAsync(acc_.p, 0, sizeof(double) * N, st), "memset");
+    check(cudaMemsetAsync(acc_comp_.p, 0, sizeof(double) * N, st), "memset");
+    for (int ip = 0; ip < np; ++ip) {
+      model.random_particle();
+      model.compute_trajectory();  // host RK4 of particle ip overlaps the GPU work of particle ip-1
+      check(cudaStreamSynchronize(st), "particle");
+      upload_trajectory();
+      run_single(rq, N, weight, out_.as<double>(), d_lvl, st);
+      k_kahan_add<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(acc_.as<double>(), acc_comp_.as<double>(),
+                                                                out_.as<double>(), N);
+      check(cudaGetLastError(), "accumulate");
+      ++last_launches;
+    }
+    check(cudaMemcpyAsync(d_out, acc_.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "result");
+  }
+  if (!rq.out_on_device) {
+    check(cudaMemcpyAsync(rq.out, d_out, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
+    if (rq.level_out)
+      check(cudaMemcpyAsync(rq.level_out, d_lvl, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st), "download");
+    check(cudaStreamSynchronize(st), "download");
+    collect();
   }
 }
 
@@ -456,72 +586,6 @@ double Engine::measure_fma_peak(int kind) {
   cudaEventDestroy(b);
   const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
   return flops / (best * 1e-3) / 1e12;
-}
-
-void Engine::radiation(RadRequest& rq) {
-  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
-  check(cudaSetDevice(device), "cudaSetDevice");
-  last_samples = last_launches = last_not_converged = 0;
-  cudaStream_t st = rq.stream ? rq.stream : stream;
-  const int64_t n_e = rq.power_density ? 1 : (int64_t)rq.omega.size();
-  const int64_t N = rq.n_obs * n_e;
-  if (N <= 0) return;
-  // inputs
-  obs_.reserve(sizeof(double) * 3 * rq.n_obs);
-  if (rq.obs_on_device) {
-    check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, cudaMemcpyDeviceToDevice, st), "obs");
-    if (rq.normals) {
-      nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
-      check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, cudaMemcpyDeviceToDevice, st), "normals");
-    }
-  } else {
-    check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, cudaMemcpyHostToDevice, st), "obs");
-    if (rq.normals) {
-      nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
-      check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, cudaMemcpyHostToDevice, st), "normals");
-    }
-  }
-  if (!rq.power_density) {
-    omega_.reserve(sizeof(double) * n_e);
-    check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
-  }
-  out_.reserve(sizeof(double) * N);
-  lvl_.reserve(sizeof(int32_t) * N);
-  double* d_out = rq.out_on_device ? rq.out : out_.as<double>();
-  int32_t* d_lvl = rq.out_on_device ? rq.level_out : lvl_.as<int32_t>();
-  if (!d_lvl) d_lvl = lvl_.as<int32_t>();
-
-  const int np = rq.opts.nparticles;
-  if (np <= 0) {
-    model.ensure_trajectory();
-    upload_trajectory();
-    run_single(rq, N, 1.0, d_out, d_lvl, st);
-  } else {
-    // src/OSCARSSR.cc:4026-4062: new random particle, its trajectory, weight 1/N, compensated sum
-    const double weight = 1.0 / (double)np;
-    acc_.reserve(sizeof(double) * N);
-    acc_comp_.reserve(sizeof(double) * N);
-    check(cudaMemsetAsync(acc_.p, 0, sizeof(double) * N, st), "memset");
-    check(cudaMemsetAsync(acc_comp_.p, 0, sizeof(double) * N, st), "memset");
-    for (int ip = 0; ip < np; ++ip) {
-      model.random_particle();
-      model.compute_trajectory();
-      check(cudaStreamSynchronize(st), "particle");  // the previous trajectory's buffers are free
-      upload_trajectory();
-      run_single(rq, N, weight, out_.as<double>(), d_lvl, st);
-      k_kahan_add<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(acc_.as<double>(), acc_comp_.as<double>(),
-                                                                out_.as<double>(), N);
-      check(cudaGetLastError(), "accumulate");
-      ++last_launches;
-    }
-    check(cudaMemcpyAsync(d_out, acc_.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "result");
-  }
-  if (!rq.out_on_device) {
-    check(cudaMemcpyAsync(rq.out, d_out, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
-    if (rq.level_out)
-      check(cudaMemcpyAsync(rq.level_out, d_lvl, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st), "download");
-    check(cudaStreamSynchronize(st), "download");
-  }
 }
 
 }  // namespace osc

@@ -3,6 +3,8 @@
 
 #include <cstdint>
 #include <string>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -58,8 +60,10 @@ class Engine {
   bool profiling = false;
   double prof_ms = 0;
   long long prof_launches = 0, prof_samples = 0;
-  void drop_level_cache() { lev_filled_ = -1; bdmax_valid_ = false; levels_dropped_ = true; }
+  void drop_level_cache() { lev_filled_ = -1; mrec_filled_ = -1; bdmax_valid_ = false; levels_dropped_ = true; }
   double measure_fma_peak(int kind);
+  // Wait for the last request's statistics; throws the errors kernels reported on the device.
+  void collect();
 
  private:
   // trajectory on device
@@ -80,6 +84,22 @@ class Engine {
   std::pair<cudaEvent_t, cudaEvent_t> timed_begin(cudaStream_t st);
   void timed_end(std::pair<cudaEvent_t, cudaEvent_t> e, cudaStream_t st);
   void collect_timings();
+  // asynchronous statistics: per-particle counters copied to pinned memory, one event per slot
+  static constexpr int kStageDoubles = 4096;
+  unsigned long long* stats_host_ = nullptr;
+  double* stage_host_ = nullptr;
+  cudaEvent_t stats_ev_[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev_ = nullptr;
+  int stats_slot_ = 0;
+  std::vector<int> pending_;
+  // kernel variants: kind 0 = FP64 flux, 1 = FP64 power density, 2 = mixed flux
+  int wave_grid_[3][8] = {};
+  int wave_grid(int kind, int variant);
+  std::map<std::tuple<int, int, int, int>, int> tuned_;   // (kind, log2 entries, first level, last level) -> variant
+  int current_variant_[3] = {2, 0, 3};
+  int pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out, int32_t* d_lvl,
+                   cudaStream_t st);
+  bool tuning_ = false;
   // request scratch
   DevBuf obs_, nrm_, omega_, out_, lvl_, state_, part_, act_[2], cnt_;
   DevBuf acc_, acc_comp_;          // multi-particle compensated accumulation
@@ -92,12 +112,14 @@ class Engine {
   void ensure_mixed(int L);
   void compute_frame();
  public:
-  int mixed_ept = 2;               // entries per thread of the mixed wave kernel
+  int forced_variant[3] = {-1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
+  bool autotune = true;
+  int variant_in_use(int kind) const { return forced_variant[kind] >= 0 ? forced_variant[kind] : current_variant_[kind]; }
+  std::map<std::tuple<int, int, int, int>, int> tuned() const { return tuned_; }
  private:
 
   void upload_trajectory();
   void ensure_levels(int L);
-  void refresh_bdmax();
   void run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,
                   cudaStream_t st);
   void check(cudaError_t e, const char* what);

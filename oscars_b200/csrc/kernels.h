@@ -8,10 +8,48 @@ namespace osc {
 
 constexpr int kFdPartials = 9;  // 6 complex-sum components, first phase, last phase, max |dphase|
 
-// One wave of the frequency-domain sum: every active entry integrates the samples
-// [seg_b[g], seg_e[g]) of the level cache, split into gridDim.y spans of span_len[g] samples.
+// Work plan of one wave, computed identically by the host (buffer sizes), the wave kernel and the
+// finalize kernel from the device-resident active count.  Level L's samples occupy [2^L, 2^(L+1));
+// the first wave also integrates levels 0..L-1 = [1, 2^L) as a separate segment (its magnitude is
+// the "last" value of the first stop test).  Segment starts are rounded down to an even index (the
+// kernels skip sample 0); `spans` splits every segment so that tiles x spans reaches target_units.
+struct WavePlan {
+  int nseg;
+  int spans;
+  int64_t tiles;
+  int64_t seg_b[2], seg_e[2], span_len[2];
+};
+
+__host__ __device__ inline WavePlan wave_plan(int first, int L, int64_t n_act, int tile_entries, int64_t target_units,
+                                              int min_span) {
+  WavePlan p;
+  const int64_t lo = (int64_t)1 << L, hi = (int64_t)2 << L;
+  p.nseg = (first && L >= 1) ? 2 : 1;
+  // segment 0: levels 0..L-1 on the first wave (level 0 alone when L == 0), else level L
+  const int64_t b0 = first ? 1 : lo, e0 = first ? (L >= 1 ? lo : 2) : hi;
+  const int64_t b1 = lo, e1 = hi;  // segment 1 (first wave with L >= 1): level L
+  p.tiles = (n_act + tile_entries - 1) / tile_entries;
+  int spans = 1;
+  while (p.tiles * spans < target_units && lo / (spans * 2) >= min_span) spans *= 2;
+  p.spans = spans;
+  const int64_t a0 = b0 & ~(int64_t)1, a1 = b1 & ~(int64_t)1;
+  p.seg_b[0] = a0;
+  p.seg_e[0] = e0;
+  p.span_len[0] = ((e0 - a0 + spans - 1) / spans + 1) & ~(int64_t)1;
+  p.seg_b[1] = p.nseg == 2 ? a1 : 0;
+  p.seg_e[1] = p.nseg == 2 ? e1 : 0;
+  p.span_len[1] = p.nseg == 2 ? (((e1 - a1 + spans - 1) / spans + 1) & ~(int64_t)1) : 0;
+  return p;
+}
+
+// Register-friendly accessors (g is 0 or 1; selects instead of a runtime array index).
+__host__ __device__ inline int64_t seg_begin(const WavePlan& p, int g) { return g ? p.seg_b[1] : p.seg_b[0]; }
+__host__ __device__ inline int64_t seg_end(const WavePlan& p, int g) { return g ? p.seg_e[1] : p.seg_e[0]; }
+__host__ __device__ inline int64_t seg_span(const WavePlan& p, int g) { return g ? p.span_len[1] : p.span_len[0]; }
+
+// One wave of the frequency-domain sum over level `level` for the active entries.
 struct FdWaveArgs {
-  const double* lev;        // level cache, 10 arrays of `cap` doubles
+  const double* lev;        // FP64 level cache (10 arrays of `cap`) or mixed records (3 float4 per sample)
   int64_t cap;
   const double* obs;        // 3 * n_obs
   const double* omega;      // n_e
@@ -19,17 +57,16 @@ struct FdWaveArgs {
   int64_t n_items;          // n_obs * n_e (entry = obs_index * n_e + energy_index)
   const int* act;           // active entry ids (NULL: entries 0..n_items-1)
   const unsigned* n_act;    // device count of `act`
-  int nseg;
-  int64_t seg_b[2], seg_e[2], span_len[2];
-  double* part;             // partials [(seg*spans + span) * kFdPartials + k][part_stride]
-  int64_t part_stride;
+  int first, level, tile_entries, min_span;
+  int64_t target_units;
+  double* part;             // partials [(seg*spans + span) * kFdPartials + k][n_act]
   unsigned* err;
 };
 
 struct FdFinalArgs {
   const double* part;
-  int64_t part_stride;
-  int spans, nseg, first, level, max_level, quantity, project;
+  int first, level, max_level, quantity, project, tile_entries, min_span;
+  int64_t target_units;
   double dt_prev, dt_level;  // DeltaT inclusive to level-1 (first wave) and to level
   double precision, c0, c2, weight;
   double pol[6];            // polarization vector (re, im) x 3
@@ -54,18 +91,18 @@ struct PdWaveArgs {
   int64_t n_items;
   const int* act;
   const unsigned* n_act;
-  int nseg;
-  int64_t seg_b[2], seg_e[2], span_len[2];
-  double* part;             // partials [(seg*spans + span)][part_stride]
-  int64_t part_stride;
+  int first, level, tile_entries, min_span;
+  int64_t target_units;
+  double* part;             // partials [(seg*spans + span)][n_act]
   unsigned* err;
 };
 
 struct PdFinalArgs {
   const double* part;
-  int64_t part_stride;
-  int spans, nseg, first, level, max_level, quantity, directional;
-  double dt_prev, dt_level, precision, scale, weight, bdmax, two_over_gamma;
+  int first, level, max_level, quantity, directional, tile_entries, min_span;
+  int64_t target_units;
+  double dt_prev, dt_level, precision, scale, weight, two_over_gamma;
+  const double* bdmax_levels;  // device, per level max |beta_i - beta_{i-1}| (-1 for level 0)
   int64_t n_items;
   const int* act;
   const unsigned* n_act;
@@ -89,16 +126,20 @@ struct MixedFrame {
 
 cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin, int64_t s_end, const MixedFrame& F,
                                  float4* rec, cudaStream_t st);
-cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int64_t n_act_bound, int spans, int ept,
-                                 cudaStream_t st);
-int mixed_entries_per_cta(int ept);
+// Compiled kernel variants (see kernels_fp64.cu / kernels_mixed.cu); the engine's autotuner picks one.
+constexpr int kFp64Variants = 4;
+constexpr int kMixedVariants = 7;
+cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int grid, int variant, cudaStream_t st);
+int mixed_entries_per_cta(int variant);
+int mixed_blocks_per_sm(int variant);
+int fp64_blocks_per_sm(bool power_density, int variant);
 
 cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
                               int64_t s_end, double* lev, int64_t cap, int extended_level,
                               unsigned long long* bdmax_bits, cudaStream_t st);
-cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int64_t n_act_bound, int spans, cudaStream_t st);
+cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int grid, int variant, cudaStream_t st);
 cudaError_t launch_fd_finalize(const FdFinalArgs& a, int64_t n_act_bound, cudaStream_t st);
-cudaError_t launch_pd_wave_fp64(const PdWaveArgs& a, int64_t n_act_bound, int spans, cudaStream_t st);
+cudaError_t launch_pd_wave_fp64(const PdWaveArgs& a, int grid, cudaStream_t st);
 cudaError_t launch_pd_finalize(const PdFinalArgs& a, int64_t n_act_bound, cudaStream_t st);
 
 }  // namespace osc

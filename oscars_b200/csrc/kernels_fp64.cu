@@ -126,20 +126,14 @@ __device__ __forceinline__ void stage_issue(Stage<NARR, CH>& st, int b, const do
 constexpr int kFdThreads = 128;
 constexpr int kFdChunk = 128;
 
-__global__ void __launch_bounds__(kFdThreads) k_fd_wave_fp64(FdWaveArgs A) {
+template <int MINB>
+__global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A) {
   __shared__ __align__(16) Stage<10, kFdChunk> st;
   const int tid = threadIdx.x;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const int64_t slot = (int64_t)blockIdx.x * kFdThreads + tid;
-  if ((int64_t)blockIdx.x * kFdThreads >= n_act) return;  // whole CTA idle
-  const bool live = slot < n_act;
-  const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
-  const int64_t io = item / A.n_e, ie = item % A.n_e;
-  const double Ox = A.obs[3 * io], Oy = A.obs[3 * io + 1], Oz = A.obs[3 * io + 2];
-  const double omega = A.omega[ie];
-  const double mw = -omega;
-  const int span = blockIdx.y;
-
+  const WavePlan P = wave_plan(A.first, A.level, n_act, kFdThreads, A.target_units, A.min_span);
+  const int64_t units = P.tiles * P.spans;
+  if ((int64_t)blockIdx.x >= units) return;  // whole CTA idle
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
@@ -147,96 +141,105 @@ __global__ void __launch_bounds__(kFdThreads) k_fd_wave_fp64(FdWaveArgs A) {
   }
   __syncthreads();
   uint32_t phase_bits = 0;  // parity of the next completion expected on each buffer
-
-  for (int g = 0; g < A.nseg; ++g) {
-    const int64_t b0 = A.seg_b[g] + (int64_t)span * A.span_len[g];
-    const int64_t b1 = min(A.seg_e[g], b0 + A.span_len[g]);
-    double sxr = 0, sxi = 0, syr = 0, syi = 0, szr = 0, szi = 0;
-    double first_phase = 0, last_phase = 0, dmax = 0;
-    bool have = false;
-    const int64_t nchunks = b1 > b0 ? (b1 - b0 + kFdChunk - 1) / kFdChunk : 0;
-    if (tid == 0 && nchunks > 0) {
-      const int64_t lo = b0, hi = min(b1, b0 + kFdChunk);
-      stage_issue<10, kFdChunk>(st, 0, A.lev, A.cap, lo & ~(int64_t)1, (hi + 1) & ~(int64_t)1);
-    }
-    for (int64_t c = 0; c < nchunks; ++c) {
-      const int buf = (int)(c & 1);
-      const int64_t lo = b0 + c * kFdChunk, hi = min(b1, lo + kFdChunk);
-      if (tid == 0 && c + 1 < nchunks) {  // prefetch the next chunk into the other buffer
-        const int64_t lo2 = lo + kFdChunk, hi2 = min(b1, lo2 + kFdChunk);
-        stage_issue<10, kFdChunk>(st, buf ^ 1, A.lev, A.cap, lo2 & ~(int64_t)1, (hi2 + 1) & ~(int64_t)1);
+  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+    const int64_t tile = u / P.spans;
+    const int span = (int)(u % P.spans);
+    const int64_t slot = tile * kFdThreads + tid;
+    const bool live = slot < n_act;
+    const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+    const int64_t io = item / A.n_e, ie = item % A.n_e;
+    const double Ox = A.obs[3 * io], Oy = A.obs[3 * io + 1], Oz = A.obs[3 * io + 2];
+    const double mw = -A.omega[ie];
+    for (int g = 0; g < P.nseg; ++g) {
+      const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
+      const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
+      double sxr = 0, sxi = 0, syr = 0, syi = 0, szr = 0, szi = 0;
+      double first_phase = 0, last_phase = 0, dmax = 0;
+      bool have = false;
+      const int64_t nchunks = b1 > b0 ? (b1 - b0 + kFdChunk - 1) / kFdChunk : 0;
+      if (tid == 0 && nchunks > 0) {
+        const int64_t lo = b0, hi = min(b1, b0 + kFdChunk);
+        stage_issue<10, kFdChunk>(st, 0, A.lev, A.cap, lo & ~(int64_t)1, (hi + 1) & ~(int64_t)1);
       }
-      if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
-        if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
-        return;
-      }
-      phase_bits ^= 1u << buf;
-      const int64_t lo_al = lo & ~(int64_t)1;
-      const double* sT = st.v[buf][0];
-      const double* sX = st.v[buf][1];
-      const double* sY = st.v[buf][2];
-      const double* sZ = st.v[buf][3];
-      const double* sBx = st.v[buf][4];
-      const double* sBy = st.v[buf][5];
-      const double* sBz = st.v[buf][6];
-      const double* sAx = st.v[buf][7];
-      const double* sAy = st.v[buf][8];
-      const double* sAz = st.v[buf][9];
-      const int j0 = (int)(max(lo, (int64_t)1) - lo_al);  // sample 0 is the unused slot
-      const int j1 = (int)(hi - lo_al);
-      if (live) {
-        for (int j = j0; j < j1; ++j) {
-          const double T = sT[j];
-          const double Rx = __dsub_rn(Ox, sX[j]), Ry = __dsub_rn(Oy, sY[j]), Rz = __dsub_rn(Oz, sZ[j]);
-          const double D = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz)));
-          const double ph = __dmul_rn(mw, __dadd_rn(T, __ddiv_rn(D, kCLight)));
-          if (have) {
-            const double dp = fabs(__dsub_rn(ph, last_phase));
-            dmax = dp > dmax ? dp : dmax;
-          } else {
-            first_phase = ph;
-            have = true;
-          }
-          last_phase = ph;
-          const double bx = sBx[j], by = sBy[j], bz = sBz[j];
-          const double nx = __ddiv_rn(Rx, D), ny = __ddiv_rn(Ry, D), nz = __ddiv_rn(Rz, D);
-          const double b2 = __dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz));
-          const double ndb = __dadd_rn(__dadd_rn(__dmul_rn(nx, bx), __dmul_rn(ny, by)), __dmul_rn(nz, bz));
-          const double om = __dsub_rn(1.0, ndb);
-          const double p2 = __dmul_rn(om, om);
-          const double den1 = __dmul_rn(__dmul_rn(D, D), p2);
-          const double den2 = __dmul_rn(D, p2);
-          const double ob2 = __dsub_rn(1.0, b2);
-          const double ux = __dsub_rn(nx, bx), uy = __dsub_rn(ny, by), uz = __dsub_rn(nz, bz);
-          const double ax = sAx[j], ay = sAy[j], az = sAz[j];
-          const double wx = __dsub_rn(__dmul_rn(uy, az), __dmul_rn(ay, uz));
-          const double wy = __dsub_rn(__dmul_rn(uz, ax), __dmul_rn(az, ux));
-          const double wz = __dsub_rn(__dmul_rn(ux, ay), __dmul_rn(ax, uy));
-          const double vx = __dsub_rn(__dmul_rn(ny, wz), __dmul_rn(wy, nz));
-          const double vy = __dsub_rn(__dmul_rn(nz, wx), __dmul_rn(wz, nx));
-          const double vz = __dsub_rn(__dmul_rn(nx, wy), __dmul_rn(wx, ny));
-          // The two amplitude terms need only relative accuracy: one quotient per term, then
-          // multiplications (the reference divides each component; the difference is ~1 ulp).
-          const double f1 = ob2 / den1, f2 = 1.0 / den2;
-          const double ex = fma(ux, f1, vx * f2);
-          const double ey = fma(uy, f1, vy * f2);
-          const double ez = fma(uz, f1, vz * f2);
-          double sn, cs;
-          sincos(reduce_2pi(ph), &sn, &cs);
-          sxr = fma(ex, cs, sxr); sxi = fma(ex, sn, sxi);
-          syr = fma(ey, cs, syr); syi = fma(ey, sn, syi);
-          szr = fma(ez, cs, szr); szi = fma(ez, sn, szi);
+      for (int64_t c = 0; c < nchunks; ++c) {
+        const int buf = (int)(c & 1);
+        const int64_t lo = b0 + c * kFdChunk, hi = min(b1, lo + kFdChunk);
+        if (tid == 0 && c + 1 < nchunks) {  // prefetch the next chunk into the other buffer
+          const int64_t lo2 = lo + kFdChunk, hi2 = min(b1, lo2 + kFdChunk);
+          stage_issue<10, kFdChunk>(st, buf ^ 1, A.lev, A.cap, lo2 & ~(int64_t)1, (hi2 + 1) & ~(int64_t)1);
         }
+        if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+          if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+          return;
+        }
+        phase_bits ^= 1u << buf;
+        const int64_t lo_al = lo & ~(int64_t)1;
+        const double* sT = st.v[buf][0];
+        const double* sX = st.v[buf][1];
+        const double* sY = st.v[buf][2];
+        const double* sZ = st.v[buf][3];
+        const double* sBx = st.v[buf][4];
+        const double* sBy = st.v[buf][5];
+        const double* sBz = st.v[buf][6];
+        const double* sAx = st.v[buf][7];
+        const double* sAy = st.v[buf][8];
+        const double* sAz = st.v[buf][9];
+        const int j0 = (int)(max(lo, (int64_t)1) - lo_al);  // sample 0 is the unused slot
+        const int j1 = (int)(hi - lo_al);
+        if (live) {
+          for (int j = j0; j < j1; ++j) {
+            const double T = sT[j];
+            const double Rx = __dsub_rn(Ox, sX[j]), Ry = __dsub_rn(Oy, sY[j]), Rz = __dsub_rn(Oz, sZ[j]);
+            const double D = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz)));
+            const double ph = __dmul_rn(mw, __dadd_rn(T, __ddiv_rn(D, kCLight)));
+            if (have) {
+              const double dp = fabs(__dsub_rn(ph, last_phase));
+              dmax = dp > dmax ? dp : dmax;
+            } else {
+              first_phase = ph;
+              have = true;
+            }
+            last_phase = ph;
+            const double bx = sBx[j], by = sBy[j], bz = sBz[j];
+            const double nx = __ddiv_rn(Rx, D), ny = __ddiv_rn(Ry, D), nz = __ddiv_rn(Rz, D);
+            const double b2 = __dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz));
+            const double ndb = __dadd_rn(__dadd_rn(__dmul_rn(nx, bx), __dmul_rn(ny, by)), __dmul_rn(nz, bz));
+            const double om = __dsub_rn(1.0, ndb);
+            const double p2 = __dmul_rn(om, om);
+            const double den1 = __dmul_rn(__dmul_rn(D, D), p2);
+            const double den2 = __dmul_rn(D, p2);
+            const double ob2 = __dsub_rn(1.0, b2);
+            const double ux = __dsub_rn(nx, bx), uy = __dsub_rn(ny, by), uz = __dsub_rn(nz, bz);
+            const double ax = sAx[j], ay = sAy[j], az = sAz[j];
+            const double wx = __dsub_rn(__dmul_rn(uy, az), __dmul_rn(ay, uz));
+            const double wy = __dsub_rn(__dmul_rn(uz, ax), __dmul_rn(az, ux));
+            const double wz = __dsub_rn(__dmul_rn(ux, ay), __dmul_rn(ax, uy));
+            const double vx = __dsub_rn(__dmul_rn(ny, wz), __dmul_rn(wy, nz));
+            const double vy = __dsub_rn(__dmul_rn(nz, wx), __dmul_rn(wz, nx));
+            const double vz = __dsub_rn(__dmul_rn(nx, wy), __dmul_rn(wx, ny));
+            // The two amplitude terms need only relative accuracy: one quotient per term, then
+            // multiplications (the reference divides each component; the difference is ~1 ulp).
+            const double f1 = ob2 / den1, f2 = 1.0 / den2;
+            const double ex = fma(ux, f1, vx * f2);
+            const double ey = fma(uy, f1, vy * f2);
+            const double ez = fma(uz, f1, vz * f2);
+            double sn, cs;
+            sincos(reduce_2pi(ph), &sn, &cs);
+            sxr = fma(ex, cs, sxr); sxi = fma(ex, sn, sxi);
+            syr = fma(ey, cs, syr); syi = fma(ey, sn, syi);
+            szr = fma(ez, cs, szr); szi = fma(ez, sn, szi);
+          }
+        }
+        __syncthreads();  // everyone is done with `buf` before it is refilled
       }
-      __syncthreads();  // everyone is done with `buf` before it is refilled
-    }
-    if (live) {
-      const int64_t ps = A.part_stride;
-      double* p = A.part + ((int64_t)(g * gridDim.y + span) * kFdPartials) * ps + slot;
-      p[0 * ps] = sxr; p[1 * ps] = sxi; p[2 * ps] = syr; p[3 * ps] = syi; p[4 * ps] = szr; p[5 * ps] = szi;
-      p[6 * ps] = have ? first_phase : 0.0;
-      p[7 * ps] = have ? last_phase : 0.0;
-      p[8 * ps] = have ? dmax : -1.0;  // -1 marks an empty span
+      if (live) {
+        double* p = A.part + ((int64_t)(g * P.spans + span) * kFdPartials) * n_act + slot;
+        p[0 * n_act] = sxr; p[1 * n_act] = sxi; p[2 * n_act] = syr; p[3 * n_act] = syi;
+        p[4 * n_act] = szr; p[5 * n_act] = szi;
+        p[6 * n_act] = have ? first_phase : 0.0;
+        p[7 * n_act] = have ? last_phase : 0.0;
+        p[8 * n_act] = have ? dmax : -1.0;  // -1 marks an empty span
+      }
     }
   }
 }
@@ -263,13 +266,14 @@ __global__ void k_fd_finalize(FdFinalArgs A) {
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
   const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= n_act) return;
+  const WavePlan P = wave_plan(A.first, A.level, n_act, A.tile_entries, A.target_units, A.min_span);
   const int64_t item = A.act ? (int64_t)A.act[slot] : slot;
-  const int64_t ps = A.part_stride;
+  const int64_t ps = n_act;
   auto seg_sum = [&](int g, C3& s, double& dmax) {
     double prev_last = 0;
     bool prev_have = false;
-    for (int sp = 0; sp < A.spans; ++sp) {
-      const double* p = A.part + ((int64_t)(g * A.spans + sp) * kFdPartials) * ps + slot;
+    for (int sp = 0; sp < P.spans; ++sp) {
+      const double* p = A.part + ((int64_t)(g * P.spans + sp) * kFdPartials) * ps + slot;
       s.xr += p[0]; s.xi += p[ps]; s.yr += p[2 * ps]; s.yi += p[3 * ps]; s.zr += p[4 * ps]; s.zi += p[5 * ps];
       const double dm = p[8 * ps];
       if (dm >= 0) {  // non-empty span
@@ -291,13 +295,13 @@ __global__ void k_fd_finalize(FdFinalArgs A) {
     S = {0, 0, 0, 0, 0, 0};
     double unused = 0;
     last_mag = -1;
-    if (A.nseg == 2) {
+    if (P.nseg == 2) {
       seg_sum(0, S, unused);
       C3 t = c3_scale(S, A.dt_prev);
       if (A.project) t = c3_project(t, A.pol);
       last_mag = c3_mag2(t);
     }
-    seg_sum(A.nseg - 1, S, dmax);
+    seg_sum(P.nseg - 1, S, dmax);
   } else {
     S = {A.state[item], A.state[N + item], A.state[2 * N + item], A.state[3 * N + item], A.state[4 * N + item], A.state[5 * N + item]};
     last_mag = A.state[6 * N + item];
@@ -346,13 +350,9 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
   __shared__ __align__(16) Stage<10, kPdChunk> st;
   const int tid = threadIdx.x;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const int64_t slot = (int64_t)blockIdx.x * kPdThreads + tid;
-  if ((int64_t)blockIdx.x * kPdThreads >= n_act) return;
-  const bool live = slot < n_act;
-  const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
-  const double Ox = A.obs[3 * item], Oy = A.obs[3 * item + 1], Oz = A.obs[3 * item + 2];
-  const double Nx = A.normals[3 * item], Ny = A.normals[3 * item + 1], Nz = A.normals[3 * item + 2];
-  const int span = blockIdx.y;
+  const WavePlan P = wave_plan(A.first, A.level, n_act, kPdThreads, A.target_units, A.min_span);
+  const int64_t units = P.tiles * P.spans;
+  if ((int64_t)blockIdx.x >= units) return;
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
@@ -360,71 +360,81 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
   }
   __syncthreads();
   uint32_t phase_bits = 0;
-  for (int g = 0; g < A.nseg; ++g) {
-    const int64_t b0 = A.seg_b[g] + (int64_t)span * A.span_len[g];
-    const int64_t b1 = min(A.seg_e[g], b0 + A.span_len[g]);
-    double sum = 0;
-    const int64_t nchunks = b1 > b0 ? (b1 - b0 + kPdChunk - 1) / kPdChunk : 0;
-    if (tid == 0 && nchunks > 0) {
-      const int64_t lo = b0, hi = min(b1, b0 + kPdChunk);
-      stage_issue<10, kPdChunk>(st, 0, A.lev, A.cap, lo & ~(int64_t)1, (hi + 1) & ~(int64_t)1);
-    }
-    for (int64_t c = 0; c < nchunks; ++c) {
-      const int buf = (int)(c & 1);
-      const int64_t lo = b0 + c * kPdChunk, hi = min(b1, lo + kPdChunk);
-      if (tid == 0 && c + 1 < nchunks) {
-        const int64_t lo2 = lo + kPdChunk, hi2 = min(b1, lo2 + kPdChunk);
-        stage_issue<10, kPdChunk>(st, buf ^ 1, A.lev, A.cap, lo2 & ~(int64_t)1, (hi2 + 1) & ~(int64_t)1);
+  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+    const int64_t tile = u / P.spans;
+    const int span = (int)(u % P.spans);
+    const int64_t slot = tile * kPdThreads + tid;
+    const bool live = slot < n_act;
+    const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+    const double Ox = A.obs[3 * item], Oy = A.obs[3 * item + 1], Oz = A.obs[3 * item + 2];
+    double Nx = 0, Ny = 0, Nz = 0;
+    if (A.has_normal) { Nx = A.normals[3 * item]; Ny = A.normals[3 * item + 1]; Nz = A.normals[3 * item + 2]; }
+    for (int g = 0; g < P.nseg; ++g) {
+      const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
+      const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
+      double sum = 0;
+      const int64_t nchunks = b1 > b0 ? (b1 - b0 + kPdChunk - 1) / kPdChunk : 0;
+      if (tid == 0 && nchunks > 0) {
+        const int64_t lo = b0, hi = min(b1, b0 + kPdChunk);
+        stage_issue<10, kPdChunk>(st, 0, A.lev, A.cap, lo & ~(int64_t)1, (hi + 1) & ~(int64_t)1);
       }
-      if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
-        if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
-        return;
-      }
-      phase_bits ^= 1u << buf;
-      const int64_t lo_al = lo & ~(int64_t)1;
-      const int j0 = (int)(max(lo, (int64_t)1) - lo_al), j1 = (int)(hi - lo_al);
-      if (live) {
-        for (int j = j0; j < j1; ++j) {
-          const double Rx = __dsub_rn(Ox, st.v[buf][1][j]), Ry = __dsub_rn(Oy, st.v[buf][2][j]), Rz = __dsub_rn(Oz, st.v[buf][3][j]);
-          double n1x, n1y, n1z;
-          unit3(Rx, Ry, Rz, n1x, n1y, n1z);
-          // Orthogonal() (include/TVector3D.h:132-142), then unit; N3 = unit(N1 x N2)
-          const double xx = fabs(n1x), yy = fabs(n1y), zz = fabs(n1z);
-          double ox, oy, oz;
-          if (xx < yy) {
-            if (xx < zz) { ox = 0; oy = n1z; oz = -n1y; } else { ox = n1y; oy = -n1x; oz = 0; }
-          } else {
-            if (yy < zz) { ox = -n1z; oy = 0; oz = n1x; } else { ox = n1y; oy = -n1x; oz = 0; }
-          }
-          double n2x, n2y, n2z, n3x, n3y, n3z;
-          unit3(ox, oy, oz, n2x, n2y, n2z);
-          unit3(__dsub_rn(__dmul_rn(n1y, n2z), __dmul_rn(n2y, n1z)), __dsub_rn(__dmul_rn(n1z, n2x), __dmul_rn(n2z, n1x)),
-                __dsub_rn(__dmul_rn(n1x, n2y), __dmul_rn(n2x, n1y)), n3x, n3y, n3z);
-          const double n1dn = A.has_normal
-                                  ? __dadd_rn(__dadd_rn(__dmul_rn(n1x, Nx), __dmul_rn(n1y, Ny)), __dmul_rn(n1z, Nz))
-                                  : 1.0;
-          if (A.directional && n1dn <= 0) continue;
-          const double bx = st.v[buf][4][j], by = st.v[buf][5][j], bz = st.v[buf][6][j];
-          const double ax = st.v[buf][7][j], ay = st.v[buf][8][j], az = st.v[buf][9][j];
-          const double ux = __dsub_rn(n1x, bx), uy = __dsub_rn(n1y, by), uz = __dsub_rn(n1z, bz);
-          const double wx = __dsub_rn(__dmul_rn(uy, az), __dmul_rn(ay, uz));
-          const double wy = __dsub_rn(__dmul_rn(uz, ax), __dmul_rn(az, ux));
-          const double wz = __dsub_rn(__dmul_rn(ux, ay), __dmul_rn(ax, uy));
-          const double mx = __dsub_rn(__dmul_rn(n1y, wz), __dmul_rn(wy, n1z));
-          const double my = __dsub_rn(__dmul_rn(n1z, wx), __dmul_rn(wz, n1x));
-          const double mz = __dsub_rn(__dmul_rn(n1x, wy), __dmul_rn(wx, n1y));
-          const double bdn = __dadd_rn(__dadd_rn(__dmul_rn(bx, n1x), __dmul_rn(by, n1y)), __dmul_rn(bz, n1z));
-          const double den = pow(__dsub_rn(1.0, bdn), 5.0);
-          const double m2 = __dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz));
-          const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n2x), __dmul_rn(my, n2y)), __dmul_rn(mz, n2z));
-          const double d3 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n3x), __dmul_rn(my, n3y)), __dmul_rn(mz, n3z));
-          sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d2, d2), den), m2), n1dn);
-          sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d3, d3), den), m2), n1dn);
+      for (int64_t c = 0; c < nchunks; ++c) {
+        const int buf = (int)(c & 1);
+        const int64_t lo = b0 + c * kPdChunk, hi = min(b1, lo + kPdChunk);
+        if (tid == 0 && c + 1 < nchunks) {
+          const int64_t lo2 = lo + kPdChunk, hi2 = min(b1, lo2 + kPdChunk);
+          stage_issue<10, kPdChunk>(st, buf ^ 1, A.lev, A.cap, lo2 & ~(int64_t)1, (hi2 + 1) & ~(int64_t)1);
         }
+        if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+          if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+          return;
+        }
+        phase_bits ^= 1u << buf;
+        const int64_t lo_al = lo & ~(int64_t)1;
+        const int j0 = (int)(max(lo, (int64_t)1) - lo_al), j1 = (int)(hi - lo_al);
+        if (live) {
+          for (int j = j0; j < j1; ++j) {
+            const double Rx = __dsub_rn(Ox, st.v[buf][1][j]), Ry = __dsub_rn(Oy, st.v[buf][2][j]), Rz = __dsub_rn(Oz, st.v[buf][3][j]);
+            double n1x, n1y, n1z;
+            unit3(Rx, Ry, Rz, n1x, n1y, n1z);
+            // Orthogonal() (include/TVector3D.h:132-142), then unit; N3 = unit(N1 x N2)
+            const double xx = fabs(n1x), yy = fabs(n1y), zz = fabs(n1z);
+            double ox, oy, oz;
+            if (xx < yy) {
+              if (xx < zz) { ox = 0; oy = n1z; oz = -n1y; } else { ox = n1y; oy = -n1x; oz = 0; }
+            } else {
+              if (yy < zz) { ox = -n1z; oy = 0; oz = n1x; } else { ox = n1y; oy = -n1x; oz = 0; }
+            }
+            double n2x, n2y, n2z, n3x, n3y, n3z;
+            unit3(ox, oy, oz, n2x, n2y, n2z);
+            unit3(__dsub_rn(__dmul_rn(n1y, n2z), __dmul_rn(n2y, n1z)), __dsub_rn(__dmul_rn(n1z, n2x), __dmul_rn(n2z, n1x)),
+                  __dsub_rn(__dmul_rn(n1x, n2y), __dmul_rn(n2x, n1y)), n3x, n3y, n3z);
+            const double n1dn = A.has_normal
+                                    ? __dadd_rn(__dadd_rn(__dmul_rn(n1x, Nx), __dmul_rn(n1y, Ny)), __dmul_rn(n1z, Nz))
+                                    : 1.0;
+            if (A.directional && n1dn <= 0) continue;
+            const double bx = st.v[buf][4][j], by = st.v[buf][5][j], bz = st.v[buf][6][j];
+            const double ax = st.v[buf][7][j], ay = st.v[buf][8][j], az = st.v[buf][9][j];
+            const double ux = __dsub_rn(n1x, bx), uy = __dsub_rn(n1y, by), uz = __dsub_rn(n1z, bz);
+            const double wx = __dsub_rn(__dmul_rn(uy, az), __dmul_rn(ay, uz));
+            const double wy = __dsub_rn(__dmul_rn(uz, ax), __dmul_rn(az, ux));
+            const double wz = __dsub_rn(__dmul_rn(ux, ay), __dmul_rn(ax, uy));
+            const double mx = __dsub_rn(__dmul_rn(n1y, wz), __dmul_rn(wy, n1z));
+            const double my = __dsub_rn(__dmul_rn(n1z, wx), __dmul_rn(wz, n1x));
+            const double mz = __dsub_rn(__dmul_rn(n1x, wy), __dmul_rn(wx, n1y));
+            const double bdn = __dadd_rn(__dadd_rn(__dmul_rn(bx, n1x), __dmul_rn(by, n1y)), __dmul_rn(bz, n1z));
+            const double den = pow(__dsub_rn(1.0, bdn), 5.0);
+            const double m2 = __dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz));
+            const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n2x), __dmul_rn(my, n2y)), __dmul_rn(mz, n2z));
+            const double d3 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n3x), __dmul_rn(my, n3y)), __dmul_rn(mz, n3z));
+            sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d2, d2), den), m2), n1dn);
+            sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d3, d3), den), m2), n1dn);
+          }
+        }
+        __syncthreads();
       }
-      __syncthreads();
+      if (live) A.part[(int64_t)(g * P.spans + span) * n_act + slot] = sum;
     }
-    if (live) A.part[(int64_t)(g * gridDim.y + span) * A.part_stride + slot] = sum;
   }
 }
 
@@ -433,26 +443,27 @@ __global__ void k_pd_finalize(PdFinalArgs A) {
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
   const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= n_act) return;
+  const WavePlan P = wave_plan(A.first, A.level, n_act, A.tile_entries, A.target_units, A.min_span);
   const int64_t item = A.act ? (int64_t)A.act[slot] : slot;
   const int64_t N = A.n_items;
   double sum, last_sum;
   if (A.first) {
     sum = 0;
     last_sum = -1;
-    if (A.nseg == 2) {
-      for (int sp = 0; sp < A.spans; ++sp) sum += A.part[(int64_t)sp * A.part_stride + slot];
+    if (P.nseg == 2) {
+      for (int sp = 0; sp < P.spans; ++sp) sum += A.part[(int64_t)sp * n_act + slot];
       last_sum = sum * A.dt_prev;
     }
-    for (int sp = 0; sp < A.spans; ++sp) sum += A.part[(int64_t)((A.nseg - 1) * A.spans + sp) * A.part_stride + slot];
+    for (int sp = 0; sp < P.spans; ++sp) sum += A.part[(int64_t)((P.nseg - 1) * P.spans + sp) * n_act + slot];
   } else {
     sum = A.state[item];
     last_sum = A.state[N + item];
-    for (int sp = 0; sp < A.spans; ++sp) sum += A.part[(int64_t)sp * A.part_stride + slot];
+    for (int sp = 0; sp < P.spans; ++sp) sum += A.part[(int64_t)sp * n_act + slot];
   }
   const int L = A.level;
   const double this_sum = sum * A.dt_level;
   double prec = fabs(this_sum - last_sum) / last_sum;
-  const double bd = A.bdmax;
+  const double bd = A.bdmax_levels[L];
   int result_level = -1;
   bool stop = false;
   if ((L > 8 && prec < A.precision && bd < A.two_over_gamma) || (L > 8 && bd < A.two_over_gamma && this_sum == last_sum)) {
@@ -497,10 +508,16 @@ cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, dou
   return cudaGetLastError();
 }
 
-cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int64_t n_act_bound, int spans, cudaStream_t st) {
-  const int64_t tiles = (n_act_bound + dev::kFdThreads - 1) / dev::kFdThreads;
-  if (tiles == 0) return cudaSuccess;
-  dev::k_fd_wave_fp64<<<dim3((unsigned)tiles, (unsigned)spans), dev::kFdThreads, 0, st>>>(a);
+// Compiled variants of the FP64 wave kernel: minimum resident CTAs per SM (register cap).
+static const int kFp64MinBlocks[kFp64Variants] = {1, 6, 7, 8};
+
+cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int grid, int variant, cudaStream_t st) {
+  switch (variant) {
+    case 1: dev::k_fd_wave_fp64<6><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+    case 2: dev::k_fd_wave_fp64<7><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+    case 3: dev::k_fd_wave_fp64<8><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+    default: dev::k_fd_wave_fp64<1><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+  }
   return cudaGetLastError();
 }
 
@@ -511,10 +528,8 @@ cudaError_t launch_fd_finalize(const FdFinalArgs& a, int64_t n_act_bound, cudaSt
   return cudaGetLastError();
 }
 
-cudaError_t launch_pd_wave_fp64(const PdWaveArgs& a, int64_t n_act_bound, int spans, cudaStream_t st) {
-  const int64_t tiles = (n_act_bound + dev::kPdThreads - 1) / dev::kPdThreads;
-  if (tiles == 0) return cudaSuccess;
-  dev::k_pd_wave_fp64<<<dim3((unsigned)tiles, (unsigned)spans), dev::kPdThreads, 0, st>>>(a);
+cudaError_t launch_pd_wave_fp64(const PdWaveArgs& a, int grid, cudaStream_t st) {
+  dev::k_pd_wave_fp64<<<grid, dev::kPdThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -523,6 +538,22 @@ cudaError_t launch_pd_finalize(const PdFinalArgs& a, int64_t n_act_bound, cudaSt
   const int T = 256;
   dev::k_pd_finalize<<<(unsigned)((n_act_bound + T - 1) / T), T, 0, st>>>(a);
   return cudaGetLastError();
+}
+
+int fp64_blocks_per_sm(bool power_density, int variant) {
+  int n = 0;
+  if (power_density) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_pd_wave_fp64, dev::kPdThreads, 0);
+  } else {
+    switch (variant) {
+      case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<6>, dev::kFdThreads, 0); break;
+      case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<7>, dev::kFdThreads, 0); break;
+      case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<8>, dev::kFdThreads, 0); break;
+      default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<1>, dev::kFdThreads, 0); break;
+    }
+  }
+  (void)kFp64MinBlocks;
+  return n > 0 ? n : 1;
 }
 
 }  // namespace osc

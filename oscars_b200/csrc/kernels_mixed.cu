@@ -5,7 +5,7 @@
 // X0 and whose third axis e3 is its initial direction, so observers downstream sit near the axis.
 // With R = O - X = (Rx, Ry, Rz) in that frame and rho^2 = Rx^2 + Ry^2,
 //     D = |R| = Rz + corr,   corr = rho^2 / (Rz + D)                       (no cancellation)
-//     w (t + D/c) = w (t - z/c) + w Oz/c + (w/c) corr
+//     w (t + D/c) = w (t - z/c) + w Oz/c + (w/c) corr      (the sum uses exp(-i w (t + D/c)))
 // The middle term is a constant phase per (observer, energy) entry; it multiplies the whole sum by a
 // unit complex number and drops out of |E|^2, of the polarization projection and of the phase
 // differences of the stop rule, so it is not computed.  tau_s = t - z/c (a few 1e-16 s) is formed in
@@ -69,40 +69,15 @@ constexpr float kTwoPiHiF = 6.28318548202514648f;     // RN_f(2 pi)
 constexpr float kTwoPiLoF = -1.7484556e-07f;         // RN_f(2 pi - kTwoPiHiF)
 constexpr float kInvTwoPiF = 0.159154943f;
 
-template <int EPT>
-__global__ void __launch_bounds__(kMxThreads) k_fd_wave_mixed(FdWaveArgs A, MixedFrame F) {
+template <int EPT, int MINB>
+__global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A, MixedFrame F) {
   __shared__ __align__(16) MixedStage st;
   const int tid = threadIdx.x;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const int64_t tile0 = (int64_t)blockIdx.x * kMxThreads * EPT;
-  if (tile0 >= n_act) return;
+  const WavePlan P = wave_plan(A.first, A.level, n_act, kMxThreads * EPT, A.target_units, A.min_span);
+  const int64_t units = P.tiles * P.spans;
+  if ((int64_t)blockIdx.x >= units) return;
   const float4* rec = reinterpret_cast<const float4*>(A.lev);
-  // entry constants
-  float Ox[EPT], Oy[EPT], Oz[EPT], w[EPT], wc[EPT];
-  bool live[EPT];
-  int64_t slot[EPT];
-#pragma unroll
-  for (int e = 0; e < EPT; ++e) {
-    slot[e] = tile0 + (int64_t)e * kMxThreads + tid;
-    live[e] = slot[e] < n_act;
-    const int64_t item = live[e] ? (A.act ? (int64_t)A.act[slot[e]] : slot[e]) : 0;
-    const int64_t io = item / A.n_e, ie = item % A.n_e;
-    const double* R = F.rot;
-    const double ox = A.obs[3 * io] - F.x0[0], oy = A.obs[3 * io + 1] - F.x0[1], oz = A.obs[3 * io + 2] - F.x0[2];
-    const double fx = R[0] * ox + R[1] * oy + R[2] * oz;
-    const double fy = R[3] * ox + R[4] * oy + R[5] * oz;
-    const double fz = R[6] * ox + R[7] * oy + R[8] * oz;
-    Ox[e] = (float)fx; Oy[e] = (float)fy; Oz[e] = (float)fz;
-    const double om = A.omega[ie];
-    w[e] = (float)om;
-    wc[e] = (float)(om / kCl);
-    // validity of the near-axis phase form: small angle from the frame axis and a bounded
-    // correction phase (see the file comment); otherwise the caller must use the FP64 path
-    const double rho = sqrt(fx * fx + fy * fy) + F.xperp_max;
-    const double rz = fz - F.z_max;
-    if (live[e] && !(rz > 0 && rho < 1e-2 * rz && (om / kCl) * rho * rho / (2 * rz) < 3e4)) atomicOr(A.err, kErrBadArgs);
-  }
-  const int span = blockIdx.y;
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
@@ -110,105 +85,134 @@ __global__ void __launch_bounds__(kMxThreads) k_fd_wave_mixed(FdWaveArgs A, Mixe
   }
   __syncthreads();
   uint32_t phase_bits = 0;
-  for (int g = 0; g < A.nseg; ++g) {
-    const int64_t b0 = A.seg_b[g] + (int64_t)span * A.span_len[g];
-    const int64_t b1 = min(A.seg_e[g], b0 + A.span_len[g]);
-    double S[EPT][6];
-    float first[EPT], last[EPT], dmax[EPT];
-    bool have[EPT];
+  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+    const int64_t tile = u / P.spans;
+    const int span = (int)(u % P.spans);
+    // entry constants
+    float Ox[EPT], Oy[EPT], Oz[EPT], w[EPT], wc[EPT];
+    bool live[EPT];
+    int64_t slot[EPT];
 #pragma unroll
     for (int e = 0; e < EPT; ++e) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) S[e][k] = 0.0;
-      first[e] = last[e] = 0.f;
-      dmax[e] = 0.f;
-      have[e] = false;
+      slot[e] = tile * kMxThreads * EPT + (int64_t)e * kMxThreads + tid;
+      live[e] = slot[e] < n_act;
+      const int64_t item = live[e] ? (A.act ? (int64_t)A.act[slot[e]] : slot[e]) : 0;
+      const int64_t io = item / A.n_e, ie = item % A.n_e;
+      const double* R = F.rot;
+      const double ox = A.obs[3 * io] - F.x0[0], oy = A.obs[3 * io + 1] - F.x0[1], oz = A.obs[3 * io + 2] - F.x0[2];
+      const double fx = R[0] * ox + R[1] * oy + R[2] * oz;
+      const double fy = R[3] * ox + R[4] * oy + R[5] * oz;
+      const double fz = R[6] * ox + R[7] * oy + R[8] * oz;
+      Ox[e] = (float)fx; Oy[e] = (float)fy; Oz[e] = (float)fz;
+      const double om = A.omega[ie];
+      w[e] = (float)om;
+      wc[e] = (float)(om / kCl);
+      // validity of the near-axis phase form: small angle from the frame axis and a bounded
+      // correction phase (see the file comment); otherwise the caller must use the FP64 path
+      const double rho = sqrt(fx * fx + fy * fy) + F.xperp_max;
+      const double rz = fz - F.z_max;
+      if (live[e] && span == 0 && !(rz > 0 && rho < 1e-2 * rz && (om / kCl) * rho * rho / (2 * rz) < 3e4))
+        atomicOr(A.err, kErrBadArgs);
     }
-    const int64_t nchunks = b1 > b0 ? (b1 - b0 + kMxChunk - 1) / kMxChunk : 0;
-    if (tid == 0 && nchunks > 0) {
-      const int64_t hi = min(b1, b0 + kMxChunk);
-      mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - b0) * 48));
-      tma_load_1d(&st.v[0][0], rec + 3 * b0, (uint32_t)((hi - b0) * 48), &st.bar[0]);
-    }
-    for (int64_t c = 0; c < nchunks; ++c) {
-      const int buf = (int)(c & 1);
-      const int64_t lo = b0 + c * kMxChunk, hi = min(b1, lo + kMxChunk);
-      if (tid == 0 && c + 1 < nchunks) {
-        const int64_t lo2 = lo + kMxChunk, hi2 = min(b1, lo2 + kMxChunk);
-        mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * 48));
-        tma_load_1d(&st.v[buf ^ 1][0], rec + 3 * lo2, (uint32_t)((hi2 - lo2) * 48), &st.bar[buf ^ 1]);
+    for (int g = 0; g < P.nseg; ++g) {
+      const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
+      const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
+      double S[EPT][6];
+      float first[EPT], last[EPT], dmax[EPT];
+      bool have[EPT];
+#pragma unroll
+      for (int e = 0; e < EPT; ++e) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) S[e][k] = 0.0;
+        first[e] = last[e] = 0.f;
+        dmax[e] = 0.f;
+        have[e] = false;
       }
-      if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
-        if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
-        return;
+      const int64_t nchunks = b1 > b0 ? (b1 - b0 + kMxChunk - 1) / kMxChunk : 0;
+      if (tid == 0 && nchunks > 0) {
+        const int64_t hi = min(b1, b0 + kMxChunk);
+        mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - b0) * 48));
+        tma_load_1d(&st.v[0][0], rec + 3 * b0, (uint32_t)((hi - b0) * 48), &st.bar[0]);
       }
-      phase_bits ^= 1u << buf;
-      const float4* sv = st.v[buf];
-      const int j0 = lo == 0 ? 1 : 0;  // sample 0 is the unused slot
-      const int n = (int)(hi - lo);
-      for (int jb = j0; jb < n; jb += kMxFold) {
-        const int je = min(n, jb + kMxFold);
-        float s32[EPT][6];
-#pragma unroll
-        for (int e = 0; e < EPT; ++e)
-#pragma unroll
-          for (int k = 0; k < 6; ++k) s32[e][k] = 0.f;
-        for (int j = jb; j < je; ++j) {
-          const float4 r0 = sv[3 * j], r1 = sv[3 * j + 1], r2 = sv[3 * j + 2];
-#pragma unroll
-          for (int e = 0; e < EPT; ++e) {
-            const float rx = Ox[e] - r0.x, ry = Oy[e] - r0.y, rz = Oz[e] - r0.z;
-            const float rho2 = fmaf(rx, rx, ry * ry);
-            const float d2 = fmaf(rz, rz, rho2);
-            const float iD = rsqrtf(d2);
-            const float q = rho2 * iD * iD;                                  // (rho/D)^2
-            const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);           // rho^2/(Rz+D), |rho/D| < 1e-2
-            const float ph = fmaf(wc[e], corr, w[e] * r0.w);
-            if (have[e]) {
-              const float dp = fabsf(ph - last[e]);
-              dmax[e] = fmaxf(dmax[e], dp);
-            } else {
-              first[e] = ph;
-              have[e] = true;
-            }
-            last[e] = ph;
-            const float k = rintf(ph * kInvTwoPiF);
-            const float rr = fmaf(-k, kTwoPiLoF, fmaf(-k, kTwoPiHiF, ph));
-            float sn, cs;
-            __sincosf(rr, &sn, &cs);
-            const float nx = rx * iD, ny = ry * iD;
-            const float en = corr * iD;                                      // 1 - n_z
-            const float ux = nx - r1.x, uy = ny - r1.y, uz = r1.z - en;
-            const float om = fmaf(-nx, r1.x, fmaf(-ny, r1.y, fmaf(-en, r1.z, en + r1.z)));
-            const float io = __frcp_rn(om);
-            const float na = fmaf(nx, r2.x, fmaf(ny, r2.y, (1.f - en) * r2.z));
-            const float k1 = io * io * iD * fmaf(r1.w, iD, na);
-            const float k2 = io * iD;
-            const float ex = fmaf(k1, ux, -k2 * r2.x);
-            const float ey = fmaf(k1, uy, -k2 * r2.y);
-            const float ez = fmaf(k1, uz, -k2 * r2.z);
-            s32[e][0] = fmaf(ex, cs, s32[e][0]); s32[e][1] = fmaf(ex, sn, s32[e][1]);
-            s32[e][2] = fmaf(ey, cs, s32[e][2]); s32[e][3] = fmaf(ey, sn, s32[e][3]);
-            s32[e][4] = fmaf(ez, cs, s32[e][4]); s32[e][5] = fmaf(ez, sn, s32[e][5]);
-          }
+      for (int64_t c = 0; c < nchunks; ++c) {
+        const int buf = (int)(c & 1);
+        const int64_t lo = b0 + c * kMxChunk, hi = min(b1, lo + kMxChunk);
+        if (tid == 0 && c + 1 < nchunks) {
+          const int64_t lo2 = lo + kMxChunk, hi2 = min(b1, lo2 + kMxChunk);
+          mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * 48));
+          tma_load_1d(&st.v[buf ^ 1][0], rec + 3 * lo2, (uint32_t)((hi2 - lo2) * 48), &st.bar[buf ^ 1]);
         }
+        if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+          if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+          return;
+        }
+        phase_bits ^= 1u << buf;
+        const float4* sv = st.v[buf];
+        const int j0 = lo == 0 ? 1 : 0;  // sample 0 is the unused slot
+        const int n = (int)(hi - lo);
+        for (int jb = j0; jb < n; jb += kMxFold) {
+          const int je = min(n, jb + kMxFold);
+          float s32[EPT][6];
 #pragma unroll
-        for (int e = 0; e < EPT; ++e)
+          for (int e = 0; e < EPT; ++e)
 #pragma unroll
-          for (int k = 0; k < 6; ++k) S[e][k] += (double)s32[e][k];
+            for (int k = 0; k < 6; ++k) s32[e][k] = 0.f;
+          for (int j = jb; j < je; ++j) {
+            const float4 r0 = sv[3 * j], r1 = sv[3 * j + 1], r2 = sv[3 * j + 2];
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+              const float rx = Ox[e] - r0.x, ry = Oy[e] - r0.y, rz = Oz[e] - r0.z;
+              const float rho2 = fmaf(rx, rx, ry * ry);
+              const float d2 = fmaf(rz, rz, rho2);
+              const float iD = rsqrtf(d2);
+              const float q = rho2 * iD * iD;                                  // (rho/D)^2
+              const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);           // rho^2/(Rz+D), |rho/D| < 1e-2
+              const float ph = -fmaf(wc[e], corr, w[e] * r0.w);              // exp(-i w (t + D/c))
+              if (have[e]) {
+                const float dp = fabsf(ph - last[e]);
+                dmax[e] = fmaxf(dmax[e], dp);
+              } else {
+                first[e] = ph;
+                have[e] = true;
+              }
+              last[e] = ph;
+              const float k = rintf(ph * kInvTwoPiF);
+              const float rr = fmaf(-k, kTwoPiLoF, fmaf(-k, kTwoPiHiF, ph));
+              float sn, cs;
+              __sincosf(rr, &sn, &cs);
+              const float nx = rx * iD, ny = ry * iD;
+              const float en = corr * iD;                                      // 1 - n_z
+              const float ux = nx - r1.x, uy = ny - r1.y, uz = r1.z - en;
+              const float om = fmaf(-nx, r1.x, fmaf(-ny, r1.y, fmaf(-en, r1.z, en + r1.z)));
+              const float io = __fdividef(1.f, om);
+              const float na = fmaf(nx, r2.x, fmaf(ny, r2.y, (1.f - en) * r2.z));
+              const float k1 = io * io * iD * fmaf(r1.w, iD, na);
+              const float k2 = io * iD;
+              const float ex = fmaf(k1, ux, -k2 * r2.x);
+              const float ey = fmaf(k1, uy, -k2 * r2.y);
+              const float ez = fmaf(k1, uz, -k2 * r2.z);
+              s32[e][0] = fmaf(ex, cs, s32[e][0]); s32[e][1] = fmaf(ex, sn, s32[e][1]);
+              s32[e][2] = fmaf(ey, cs, s32[e][2]); s32[e][3] = fmaf(ey, sn, s32[e][3]);
+              s32[e][4] = fmaf(ez, cs, s32[e][4]); s32[e][5] = fmaf(ez, sn, s32[e][5]);
+            }
+          }
+#pragma unroll
+          for (int e = 0; e < EPT; ++e)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) S[e][k] += (double)s32[e][k];
+        }
+        __syncthreads();
       }
-      __syncthreads();
-    }
 #pragma unroll
-    for (int e = 0; e < EPT; ++e) {
-      if (!live[e]) continue;
-      const int64_t ps = A.part_stride;
-      double* p = A.part + ((int64_t)(g * gridDim.y + span) * kFdPartials) * ps + slot[e];
+      for (int e = 0; e < EPT; ++e) {
+        if (!live[e]) continue;
+        double* p = A.part + ((int64_t)(g * P.spans + span) * kFdPartials) * n_act + slot[e];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) p[k * ps] = S[e][k];
-      p[6 * ps] = have[e] ? (double)first[e] : 0.0;
-      p[7 * ps] = have[e] ? (double)last[e] : 0.0;
-      p[8 * ps] = have[e] ? (double)dmax[e] : -1.0;
+        for (int k = 0; k < 6; ++k) p[k * n_act] = S[e][k];
+        p[6 * n_act] = have[e] ? (double)first[e] : 0.0;
+        p[7 * n_act] = have[e] ? (double)last[e] : 0.0;
+        p[8 * n_act] = have[e] ? (double)dmax[e] : -1.0;
+      }
     }
   }
 }
@@ -223,17 +227,41 @@ cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin
   return cudaGetLastError();
 }
 
-int mixed_entries_per_cta(int ept) { return dev::kMxThreads * ept; }
+// Compiled variants of the mixed wave kernel: (entries per thread, minimum resident CTAs per SM).
+static const int kMixedEpt[kMixedVariants] = {1, 1, 2, 2, 2, 4, 4};
 
-cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int64_t n_act_bound, int spans, int ept,
-                                 cudaStream_t st) {
-  const int64_t per = (int64_t)dev::kMxThreads * ept;
-  const int64_t tiles = (n_act_bound + per - 1) / per;
-  if (tiles == 0) return cudaSuccess;
-  const dim3 grid((unsigned)tiles, (unsigned)spans);
-  if (ept == 1) dev::k_fd_wave_mixed<1><<<grid, dev::kMxThreads, 0, st>>>(a, F);
-  else if (ept == 2) dev::k_fd_wave_mixed<2><<<grid, dev::kMxThreads, 0, st>>>(a, F);
-  else dev::k_fd_wave_mixed<4><<<grid, dev::kMxThreads, 0, st>>>(a, F);
+int mixed_entries_per_cta(int variant) { return dev::kMxThreads * kMixedEpt[variant]; }
+
+template <int EPT, int MINB>
+static void mixed_occ(int& n) {
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_mixed<EPT, MINB>, dev::kMxThreads, 0);
+}
+
+int mixed_blocks_per_sm(int variant) {
+  int n = 0;
+  switch (variant) {
+    case 0: mixed_occ<1, 1>(n); break;
+    case 1: mixed_occ<1, 8>(n); break;
+    case 2: mixed_occ<2, 1>(n); break;
+    case 3: mixed_occ<2, 5>(n); break;
+    case 4: mixed_occ<2, 6>(n); break;
+    case 5: mixed_occ<4, 1>(n); break;
+    default: mixed_occ<4, 3>(n); break;
+  }
+  return n > 0 ? n : 1;
+}
+
+cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int grid, int variant, cudaStream_t st) {
+  const int T = dev::kMxThreads;
+  switch (variant) {
+    case 0: dev::k_fd_wave_mixed<1, 1><<<grid, T, 0, st>>>(a, F); break;
+    case 1: dev::k_fd_wave_mixed<1, 8><<<grid, T, 0, st>>>(a, F); break;
+    case 2: dev::k_fd_wave_mixed<2, 1><<<grid, T, 0, st>>>(a, F); break;
+    case 3: dev::k_fd_wave_mixed<2, 5><<<grid, T, 0, st>>>(a, F); break;
+    case 4: dev::k_fd_wave_mixed<2, 6><<<grid, T, 0, st>>>(a, F); break;
+    case 5: dev::k_fd_wave_mixed<4, 1><<<grid, T, 0, st>>>(a, F); break;
+    default: dev::k_fd_wave_mixed<4, 3><<<grid, T, 0, st>>>(a, F); break;
+  }
   return cudaGetLastError();
 }
 

@@ -86,8 +86,9 @@ def test_adaptive_mode_close_to_fp64():
         lev.append(s.last_levels.copy())
     frac = float(np.mean(lev[0] != lev[1]))
     print("adaptive: %.4f of entries stop at another level; error %.3e" % (frac, _err(out[1], out[0])))
-    assert frac <= 0.01
-    assert _err(out[1], out[0]) <= 5e-3
+    # flips happen at low-flux entries where |E| << sum |terms|, so the peak-normalised error stays small
+    assert frac <= 0.03
+    assert _err(out[1], out[0]) <= 1e-4
 
 
 def test_far_off_axis_observer_is_rejected():
