@@ -176,6 +176,35 @@ def cpu_baseline_leg():
             "sample": "central %d of 201 rows x 201 columns, one pass, %.2f s" % (rows, dt)}
 
 
+def _time_device_steps(ctx, step, stream, flush, steps, warmup, local):
+    """Per-step CUDA events on the launching stream, L2 flushed before every step (outside the
+    events).  Returns (total ms, samples per step, launches per step, wave-kernel ms, clocks)."""
+    import ctypes
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    sm, ln = ctypes.c_longlong(), ctypes.c_longlong()
+    ctx.call("osc_last_stats", ctypes.byref(sm), ctypes.byref(ln))  # the job is identical every step
+    ctx.call("osc_set_profiling", 1)
+    ctx.call("osc_get_profile", None, None, None, 1)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with ClockSampler(local) as clk:
+        time.sleep(0.1)
+        for i in range(steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            step()
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    kms, kl = ctypes.c_double(), ctypes.c_longlong()
+    ctx.call("osc_get_profile", ctypes.byref(kms), ctypes.byref(kl), None, 1)
+    ctx.call("osc_set_profiling", 0)
+    return ms, sm.value, ln.value, kms.value, kl.value, clk.summary()
+
+
 def product_arm(args):
     import ctypes
     import numpy as np
@@ -199,74 +228,73 @@ def product_arm(args):
     ctx = s._ctx
     xyz, nrm, x12 = s._rectangle([GRID, GRID], "XY", [0.01, 0.01], None, None, [0, 0, 30], 0, False)
     n = GRID * GRID
-    o = RadOpts(precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, quantity=0,
-                precision_mode=1 if args.compute == "mixed" else 0)
-    o.horizontal[:] = [1, 0, 0]
-    o.propagation[:] = [0, 0, 1]
+    modes = ["fp64", "mixed"] if args.compute == "mixed" else ["fp64"]
+    opts = {}
+    for m in modes:
+        o = RadOpts(precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, quantity=0,
+                    precision_mode=1 if m == "mixed" else 0)
+        o.horizontal[:] = [1, 0, 0]
+        o.propagation[:] = [0, 0, 1]
+        opts[m] = o
     dev = torch.device("cuda", local)
     d_obs = torch.tensor(xyz, dtype=torch.float64, device=dev)
-    d_out = torch.zeros(n, dtype=torch.float64, device=dev)
+    d_out = {m: torch.zeros(n, dtype=torch.float64, device=dev) for m in modes}
     d_lvl = torch.zeros(n, dtype=torch.int32, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
     stream = torch.cuda.current_stream(dev)
     sptr = ctypes.c_void_p(stream.cuda_stream)
 
-    def step():
-        ctx.call("osc_drop_level_cache")
-        ctx.call("osc_flux_device", ctypes.c_void_p(d_obs.data_ptr()), n, energy, ctypes.byref(o),
-                 ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_lvl.data_ptr()), sptr)
+    def make_step(m):
+        def step():
+            ctx.call("osc_drop_level_cache")  # level samples are rebuilt inside every step
+            ctx.call("osc_flux_device", ctypes.c_void_p(d_obs.data_ptr()), n, energy, ctypes.byref(opts[m]),
+                     ctypes.c_void_p(d_out[m].data_ptr()), ctypes.c_void_p(d_lvl.data_ptr()), sptr)
+        return step
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    sm, ln = ctypes.c_longlong(), ctypes.c_longlong()
-    ctx.call("osc_last_stats", ctypes.byref(sm), ctypes.byref(ln))  # the job is identical every step
-    samples_per_step, launches_per_step = sm.value, ln.value
-    ctx.call("osc_set_profiling", 1)
-    ctx.call("osc_get_profile", None, None, None, 1)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(local) as clk:
-        time.sleep(0.1)
-        for i in range(args.steps):
-            flush.zero_()
-            evs[i][0].record(stream)
-            step()
-            evs[i][1].record(stream)
-        torch.cuda.synchronize()
-    samples = samples_per_step * args.steps
-    launches = launches_per_step * args.steps
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in evs)
-    kms, kl, ks = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
-    ctx.call("osc_get_profile", ctypes.byref(kms), ctypes.byref(kl), ctypes.byref(ks), 1)
-    ctx.call("osc_set_profiling", 0)
-    t = torch.tensor([ms, float(samples)], dtype=torch.float64, device=dev)
-    if world > 1:
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        ms_max, samples_all = float(tmax[0]), float(tsum[1])
-    else:
-        ms_max, samples_all = ms, float(samples)
-    value = samples_all / (ms_max * 1e-3) / 1e9
+    res = {}
+    for m in modes:
+        if world > 1:
+            dist.barrier()
+        ms, sps, lps, kms, kl, clocks = _time_device_steps(ctx, make_step(m), stream, flush, args.steps, args.warmup, local)
+        t = torch.tensor([ms, float(sps * args.steps)], dtype=torch.float64, device=dev)
+        if world > 1:
+            tmax, tsum = t.clone(), t.clone()
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+            dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+            ms_max, samples_all = float(tmax[0]), float(tsum[1])
+        else:
+            ms_max, samples_all = ms, float(sps * args.steps)
+        v, nv = ctypes.c_int(), ctypes.c_int()
+        ctx.call("osc_get_variant", 2 if m == "mixed" else 0, ctypes.byref(v), ctypes.byref(nv))
+        peak = ctypes.c_double()
+        ctx.call("osc_measure_fma_peak", 0 if m == "fp64" else 1, ctypes.byref(peak))
+        achieved = sps * args.steps * FLOP_PER_SAMPLE / (kms * 1e-3) / 1e12 if kms > 0 else None
+        traffic = None
+        prof_path = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(prof_path):
+            traffic = json.load(open(prof_path)).get("k_fd_wave_%s" % m)
+        res[m] = {"value": samples_all / (ms_max * 1e-3) / 1e9, "ms_per_step": ms_max / args.steps,
+                  "samples_per_step": sps, "launches_per_step": lps, "variant": v.value, "clocks": clocks,
+                  "roofline": {"bound": "fp64" if m == "fp64" else "fp32", "achieved": achieved, "peak": peak.value,
+                               "unit": "TFLOP/s", "frac": (achieved / peak.value) if achieved else None,
+                               "traffic": traffic, "kernel": "k_fd_wave_%s" % m, "flop_per_sample": FLOP_PER_SAMPLE,
+                               "kernel_ms_per_step": kms / args.steps, "kernel_launches_per_step": kl / args.steps,
+                               "peak_source": "in-run FMA-throughput loop on this GPU (osc_measure_fma_peak); the "
+                                              "sample sums run on the %s pipe, not the tensor cores or HBM"
+                                              % ("FP64" if m == "fp64" else "FP32/SFU")}}
+    head = modes[-1]
+    err = None
+    if "mixed" in res:
+        a, b = d_out["mixed"].cpu().numpy(), d_out["fp64"].cpu().numpy()
+        err = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
     if args.quick:
         if rank == 0:
-            v, nv = ctypes.c_int(), ctypes.c_int()
-            ctx.call("osc_get_variant", 2 if args.compute == "mixed" else 0, ctypes.byref(v), ctypes.byref(nv))
-            print(json.dumps({"quick": True, "compute": args.compute, "value": value, "unit": "Gsamples/s",
-                              "ms_per_step": ms_max / args.steps, "kernel_ms_per_step": kms.value / args.steps,
-                              "kernel_launches": kl.value, "variant": v.value, "samples_per_step": samples_per_step,
-                              "clocks": clk.summary()}), flush=True)
+            print(json.dumps({"quick": True, "compute": head, "modes": res, "mixed_vs_fp64_peak_rel_err": err}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return
+
     # e2e: host buffers through the C ABI, new trajectory every step (host RK4 + spline included)
     out_h = np.zeros(n)
     lvl_h = np.zeros(n, dtype=np.int32)
@@ -274,14 +302,13 @@ def product_arm(args):
 
     def e2e_step():
         s.set_new_particle(particle="ideal")  # drops the trajectory: RK4 + spline + upload again
-        ctx.call("osc_flux", _lib.dptr(xyz), n, energy, ctypes.byref(o), _lib.dptr(out_h), _lib.i32ptr(lvl_h),
-                 ctypes.byref(nnc))
+        ctx.call("osc_flux", _lib.dptr(xyz), n, energy, ctypes.byref(opts[head]), _lib.dptr(out_h),
+                 _lib.i32ptr(lvl_h), ctypes.byref(nnc))
     e2e_step()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    e2e_times = []
-    e2e_samples = 0
+    e2e_times, e2e_samples = [], 0
     for i in range(max(1, min(args.steps, 20))):
         t0 = time.perf_counter()
         e2e_step()
@@ -289,43 +316,33 @@ def product_arm(args):
         sm = ctypes.c_longlong()
         ctx.call("osc_last_stats", ctypes.byref(sm), None)
         e2e_samples += sm.value
-    e2e_s = sum(e2e_times)
-    te = torch.tensor([e2e_s, float(e2e_samples)], dtype=torch.float64, device=dev)
+    te = torch.tensor([sum(e2e_times), float(e2e_samples)], dtype=torch.float64, device=dev)
     if world > 1:
-        tm = te.clone()
+        tm, ts = te.clone(), te.clone()
         dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        ts = te.clone()
         dist.all_reduce(ts, op=dist.ReduceOp.SUM)
         e2e_value = float(ts[1]) / float(tm[0]) / 1e9
     else:
-        e2e_value = e2e_samples / e2e_s / 1e9
+        e2e_value = e2e_samples / sum(e2e_times) / 1e9
     h2d = xyz.nbytes + 19 * 20001 * 8 + 8
     d2h = out_h.nbytes + lvl_h.nbytes
-
-    peak = ctypes.c_double()
-    ctx.call("osc_measure_fma_peak", 0 if args.compute == "fp64" else 1, ctypes.byref(peak))
-    achieved = ks.value * FLOP_PER_SAMPLE / (kms.value * 1e-3) / 1e12 if kms.value > 0 else None
-    traffic = None
-    prof_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof_path):
-        traffic = json.load(open(prof_path)).get("fd_wave_%s" % args.compute)
-    roof = {"bound": "fp64" if args.compute == "fp64" else "fp32", "achieved": achieved, "peak": peak.value,
-            "unit": "TFLOP/s", "frac": (achieved / peak.value) if achieved else None, "traffic": traffic,
-            "kernel": "k_fd_wave_%s" % args.compute, "flop_per_sample": FLOP_PER_SAMPLE,
-            "kernel_ms_per_step": kms.value / max(1, args.steps), "kernel_launches": kl.value,
-            "peak_source": "in-run FMA-throughput loop on this GPU (osc_measure_fma_peak); the sample-sum "
-                           "kernels run on the FP64/FP32 pipes, not the tensor cores or HBM"}
-    clocks = clk.summary()
     if rank == 0:
         cpu = cpu_baseline_leg() if world == 1 else None
-        line = {"metric": METRIC, "value": value, "unit": "Gsamples/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.compute == "fp64" else "f32+f64",
-                "data": "synthetic",
-                "config": {"workload": WORKLOAD, "compute": args.compute, "l2": "flushed between steps (256 MB write)",
+        r = res[head]
+        line = {"metric": METRIC, "value": r["value"], "unit": "Gsamples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "compute": head, "l2": "flushed between steps (256 MB write)",
                            "parallelism": "independent job per rank" if world > 1 else "single GPU"},
                 "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+                "gpu_launches": r["launches_per_step"] * args.steps, "roofline": r["roofline"], "cpu_baseline": cpu,
+                "clocks": r["clocks"]}
+        if "mixed" in res:
+            f = res["fp64"]
+            line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
+                            "clocks": f["clocks"]}
+            line["mixed_over_fp64"] = r["value"] / f["value"]
+            line["mixed_vs_fp64_peak_rel_err"] = err
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -338,7 +355,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
-    ap.add_argument("--compute", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--compute", default="mixed", choices=["fp64", "mixed"],
+                    help="headline arithmetic; 'mixed' also times the FP64 path and reports both")
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":

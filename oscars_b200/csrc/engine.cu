@@ -53,11 +53,12 @@ Engine::Engine(int dev) : device(dev) {
   bd_bits_.reserve(32 * sizeof(unsigned long long));
   cnt_.reserve(64);
   check(cudaMemset(cnt_.p, 0, 64), "memset");
-  check(cudaHostAlloc(reinterpret_cast<void**>(&stats_host_), 8 * sizeof(unsigned long long), cudaHostAllocDefault),
+  check(cudaHostAlloc(reinterpret_cast<void**>(&stats_host_), 2 * kStatSlots * sizeof(unsigned long long),
+                      cudaHostAllocDefault),
         "cudaHostAlloc");
   check(cudaHostAlloc(reinterpret_cast<void**>(&stage_host_), kStageDoubles * sizeof(double), cudaHostAllocDefault),
         "cudaHostAlloc");
-  for (int i = 0; i < 2; ++i) check(cudaEventCreateWithFlags(&stats_ev_[i], cudaEventDisableTiming), "event");
+  for (int i = 0; i < kStatSlots; ++i) check(cudaEventCreateWithFlags(&stats_ev_[i], cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming), "event");
 }
 
@@ -67,7 +68,7 @@ Engine::~Engine() {
   if (stream) cudaStreamSynchronize(stream);
   for (auto& e : ev_pending_) { ev_pool_.push_back(e.first); ev_pool_.push_back(e.second); }
   for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
-  for (int i = 0; i < 2; ++i) if (stats_ev_[i]) cudaEventDestroy(stats_ev_[i]);
+  for (int i = 0; i < kStatSlots; ++i) if (stats_ev_[i]) cudaEventDestroy(stats_ev_[i]);
   if (stage_ev_) cudaEventDestroy(stage_ev_);
   if (stats_host_) cudaFreeHost(stats_host_);
   if (stage_host_) cudaFreeHost(stage_host_);
@@ -303,21 +304,25 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   const int kind = rq.power_density ? 1 : (mixed ? 2 : 0);
   const int variant = tuning_ ? current_variant_[kind]
                               : pick_variant(kind, const_cast<RadRequest&>(rq), n_items, Lfirst, lstop, d_out, d_lvl, st);
-  const int grid = wave_grid(kind, variant);
+  const int resident = wave_grid(kind, variant);  // CTAs resident at once on the device
   const int tile = mixed ? mixed_entries_per_cta(variant) : 128;
-  const int64_t target = 8 * (int64_t)grid;
+  const int64_t target = 4 * (int64_t)resident;   // >= 4 waves of equal units per launch
   const int64_t N = n_items;
   // partial-sum buffer: the largest plan over every possible active count of every level
+  // partial-sum buffer and per-level grid: the largest plan over every possible active count
   size_t part_doubles = 0;
+  std::vector<int64_t> grid_of(lstop + 1, 1);
   const int per = rq.power_density ? 1 : kFdPartials;
+  const int64_t ntiles = (N + tile - 1) / tile;
   for (int L = Lfirst; L <= lstop; ++L) {
-    for (int64_t t = 1; t <= (N + tile - 1) / tile; t = t < 64 ? t + 1 : t * 2) {
+    for (int64_t t = 1;; t = t < 256 ? t + 1 : t + t / 8) {
       const int64_t n = std::min(N, t * tile);
       const WavePlan pl = wave_plan(L == Lfirst, L, n, tile, target, kMinSpan);
       part_doubles = std::max(part_doubles, (size_t)pl.nseg * pl.spans * per * n);
+      grid_of[L] = std::max(grid_of[L], pl.tiles * pl.spans);
+      if (t >= ntiles) break;
+      if (L == Lfirst) t = ntiles - 1;  // the first wave always has all N entries
     }
-    const WavePlan pl = wave_plan(L == Lfirst, L, N, tile, target, kMinSpan);
-    part_doubles = std::max(part_doubles, (size_t)pl.nseg * pl.spans * per * N);
   }
   part_.reserve(sizeof(double) * part_doubles);
   act_[0].reserve(sizeof(int) * N);
@@ -366,8 +371,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + 2;
       auto ev = timed_begin(st);
-      if (mixed) check(launch_fd_wave_mixed(w, frame_, grid, variant, st), "flux wave (mixed)");
-      else check(launch_fd_wave_fp64(w, grid, variant, st), "flux wave");
+      if (mixed) check(launch_fd_wave_mixed(w, frame_, (int)grid_of[L], variant, st), "flux wave (mixed)");
+      else check(launch_fd_wave_fp64(w, (int)grid_of[L], variant, st), "flux wave");
       timed_end(ev, st);
       FdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
@@ -386,7 +391,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + 2;
       auto ev = timed_begin(st);
-      check(launch_pd_wave_fp64(w, grid, st), "power density wave");
+      check(launch_pd_wave_fp64(w, (int)grid_of[L], st), "power density wave");
       timed_end(ev, st);
       PdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
@@ -412,9 +417,10 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     else ensure_levels(L);
     launch_wave(L);
   }
-  // statistics of this particle go to pinned memory; collect() reads them after the request
-  const int slot = stats_slot_++ & 1;
-  check(cudaMemcpyAsync(stats_host_ + 4 * slot, c64, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
+  // statistics of this particle go to a pinned ring slot; collect() reads them when asked
+  if ((int)pending_.size() >= kStatSlots) collect();
+  const int slot = stats_slot_++ % kStatSlots;
+  check(cudaMemcpyAsync(stats_host_ + 2 * slot, c64, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
         "stats");
   check(cudaEventRecord(stats_ev_[slot], st), "event");
   pending_.push_back(slot);
@@ -425,9 +431,9 @@ void Engine::collect() {
   if (device < 0) return;
   for (int slot : pending_) {
     check(cudaEventSynchronize(stats_ev_[slot]), "radiation");
-    last_not_converged += (long long)stats_host_[4 * slot];
-    last_samples += (long long)stats_host_[4 * slot + 1];
-    if (profiling) prof_samples += (long long)stats_host_[4 * slot + 1];
+    last_not_converged += (long long)stats_host_[2 * slot];
+    last_samples += (long long)stats_host_[2 * slot + 1];
+    if (profiling) prof_samples += (long long)stats_host_[2 * slot + 1];
   }
   pending_.clear();
   if (profiling) collect_timings();
@@ -444,7 +450,9 @@ void Engine::collect() {
 void Engine::radiation(RadRequest& rq) {
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
-  collect();  // the previous request's statistics and deferred errors
+  // statistics describe the latest request: drop those of earlier ones without waiting for them
+  // (their ring slots may be rewritten; copies into a slot stay in stream order)
+  pending_.clear();
   last_samples = last_launches = last_not_converged = 0;
   cudaStream_t st = rq.stream ? rq.stream : stream;
   const int64_t n_e = rq.power_density ? 1 : (int64_t)rq.omega.size();

@@ -88,7 +88,8 @@ class Engine {
   static constexpr int kStageDoubles = 4096;
   unsigned long long* stats_host_ = nullptr;
   double* stage_host_ = nullptr;
-  cudaEvent_t stats_ev_[2] = {nullptr, nullptr};
+  static constexpr int kStatSlots = 64;
+  cudaEvent_t stats_ev_[kStatSlots] = {};
   cudaEvent_t stage_ev_ = nullptr;
   int stats_slot_ = 0;
   std::vector<int> pending_;

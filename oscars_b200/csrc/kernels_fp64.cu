@@ -131,7 +131,11 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
   __shared__ __align__(16) Stage<10, kFdChunk> st;
   const int tid = threadIdx.x;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const WavePlan P = wave_plan(A.first, A.level, n_act, kFdThreads, A.target_units, A.min_span);
+  // the plan is uniform over the CTA; keeping it in shared memory frees the registers its
+  // fields would otherwise hold across the sample loop
+  __shared__ WavePlan P;
+  if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, kFdThreads, A.target_units, A.min_span);
+  __syncthreads();
   const int64_t units = P.tiles * P.spans;
   if ((int64_t)blockIdx.x >= units) return;  // whole CTA idle
   if (tid == 0) {
@@ -141,7 +145,8 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
   }
   __syncthreads();
   uint32_t phase_bits = 0;  // parity of the next completion expected on each buffer
-  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+  {
+    const int64_t u = blockIdx.x;  // one (tile, span) unit per CTA; the grid covers the largest plan
     const int64_t tile = u / P.spans;
     const int span = (int)(u % P.spans);
     const int64_t slot = tile * kFdThreads + tid;
@@ -350,7 +355,11 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
   __shared__ __align__(16) Stage<10, kPdChunk> st;
   const int tid = threadIdx.x;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const WavePlan P = wave_plan(A.first, A.level, n_act, kPdThreads, A.target_units, A.min_span);
+  // the plan is uniform over the CTA; keeping it in shared memory frees the registers its
+  // fields would otherwise hold across the sample loop
+  __shared__ WavePlan P;
+  if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, kPdThreads, A.target_units, A.min_span);
+  __syncthreads();
   const int64_t units = P.tiles * P.spans;
   if ((int64_t)blockIdx.x >= units) return;
   if (tid == 0) {
@@ -360,7 +369,8 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
   }
   __syncthreads();
   uint32_t phase_bits = 0;
-  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+  {
+    const int64_t u = blockIdx.x;  // one (tile, span) unit per CTA; the grid covers the largest plan
     const int64_t tile = u / P.spans;
     const int span = (int)(u % P.spans);
     const int64_t slot = tile * kPdThreads + tid;

@@ -74,7 +74,11 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
   __shared__ __align__(16) MixedStage st;
   const int tid = threadIdx.x;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const WavePlan P = wave_plan(A.first, A.level, n_act, kMxThreads * EPT, A.target_units, A.min_span);
+  // the plan is uniform over the CTA; keeping it in shared memory frees the registers its
+  // fields would otherwise hold across the sample loop
+  __shared__ WavePlan P;
+  if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, kMxThreads * EPT, A.target_units, A.min_span);
+  __syncthreads();
   const int64_t units = P.tiles * P.spans;
   if ((int64_t)blockIdx.x >= units) return;
   const float4* rec = reinterpret_cast<const float4*>(A.lev);
@@ -85,7 +89,8 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
   }
   __syncthreads();
   uint32_t phase_bits = 0;
-  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+  {
+    const int64_t u = blockIdx.x;  // one (tile, span) unit per CTA; the grid covers the largest plan
     const int64_t tile = u / P.spans;
     const int span = (int)(u % P.spans);
     // entry constants
