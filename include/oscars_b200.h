@@ -199,6 +199,27 @@ OSC_API int osc_drop_level_cache(osc_ctx* ctx);
  * returned in TFLOP/s counting one FMA as two floating-point operations. */
 OSC_API int osc_measure_fma_peak(osc_ctx* ctx, int kind, double* tflops);
 
+/* ---- allocation-free entry point --------------------------------------------------------------
+ * No counterpart in the reference (its GPU path allocates device and pinned memory on every call).
+ * For callers that cannot allocate on the call path -- a plugin running inside a host application
+ * that owns all device memory, or a real-time loop that must not enter the allocator after start-up
+ * -- this computes the FP64 flux at one fixed level (every observer sums exactly the samples of
+ * levels 0..level, no adaptive stop) without allocating anything: no cudaMalloc/cudaFree, no host
+ * heap.  Its scratch is a 16 MiB static device array held by every GPU that loads the library until
+ * the process exits; a request must fit in it (224 B per trajectory point + 80 B x 2^(level+1) +
+ * 176 B per observer, alignment aside) or the call returns OSC_ERR_LENGTH with the reason in
+ * `message`.  The first call on a device looks up the array's device address, so make it before any
+ * stream capture.  Calls are synchronous; they all share the one array, so calls whose GPU work
+ * overlaps race.  trajectory: host, 10 x n SoA as osc_get_trajectory returns it; obs_xyz: host,
+ * 3 x n_obs; polarization: host, 6 doubles (re, im of x, y, z) or NULL for none; charge [C] and
+ * current [A] of the particle; out: host, n_obs values in the units of osc_flux; message: optional
+ * buffer for a NUL-terminated reason. */
+OSC_API int osc_flux_fixed_level_noalloc(int device, const double* trajectory, long long n_points,
+                                         const double* obs_xyz, long long n_obs, double energy_eV,
+                                         int level, double charge, double current,
+                                         const double polarization[6], double* out, char* message,
+                                         long long message_capacity);
+
 #ifdef __cplusplus
 }
 #endif

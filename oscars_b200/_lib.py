@@ -76,6 +76,7 @@ SIGNATURES = {
     "osc_get_variant": (I, [VP, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
     "osc_drop_level_cache": (I, [VP]),
     "osc_measure_fma_peak": (I, [VP, I, DP]),
+    "osc_flux_fixed_level_noalloc": (I, [I, DP, LL, DP, LL, D, I, D, D, DP, DP, ctypes.c_char_p, LL]),
 }
 
 _lib = None

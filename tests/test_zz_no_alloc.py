@@ -1,0 +1,70 @@
+"""The allocation-free flux entry point (osc_flux_fixed_level_noalloc).
+
+It exists for callers that must not allocate on the call path (a plugin inside a host application
+that owns all device memory, a real-time loop past start-up); its scratch is a static device array.
+Here it is called through the C ABI twice in a row on the same inputs, and each result is checked
+against the regular entry point (osc_flux through oscars_b200.sr, fixed level: precision=0,
+max_level=L) within the parity tolerance of the other GPU tests: 1e-9 peak-normalised.  Requests
+beyond the static scratch must be refused with a message.  This file is named to be collected last.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from cases import E1_U, UND_SETUP, run_case
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-9
+QE = 1.602176462e-19
+
+
+def _setup():
+    from oscars_b200.sr import sr
+    s = sr(gpu=1)
+    run_case(s, UND_SETUP)
+    s.calculate_trajectory()
+    return s
+
+
+def _noalloc(traj, obs, level, pol=None):
+    from oscars_b200 import _lib
+    L = _lib.lib()
+    n = traj.shape[1]
+    out = np.zeros(obs.shape[0])
+    msg = ctypes.create_string_buffer(512)
+    p = None if pol is None else _lib.dptr(np.ascontiguousarray(pol, dtype=np.float64))
+    rc = L.osc_flux_fixed_level_noalloc(0, _lib.dptr(np.ascontiguousarray(traj)), n, _lib.dptr(np.ascontiguousarray(obs)),
+                                        obs.shape[0], E1_U, level, -QE, 0.5, p, _lib.dptr(out), msg, len(msg))
+    return rc, out, msg.value.decode()
+
+
+@pytest.mark.parametrize("pol", [None, "lh"])
+def test_noalloc_matches_regular_entry_point_twice(pol):
+    s = _setup()
+    traj = s.trajectory_array()
+    level = 11
+    kw = dict(energy_eV=E1_U, npoints=[41, 41], width=[0.01, 0.01], translation=[0, 0, 30], precision=0,
+              max_level=level, dim=3)
+    if pol:
+        kw["polarization"] = pol
+    res = s.calculate_flux_rectangle(**kw)
+    obs = np.array([r[0] for r in res])
+    ref = np.array([r[1] for r in res])
+    pvec = None if pol is None else np.array([1.0, 0, 0, 0, 0, 0])
+    for call in range(2):
+        rc, out, msg = _noalloc(traj, obs, level, pvec)
+        assert rc == 0, msg
+        err = float(np.max(np.abs(out - ref)) / np.max(np.abs(ref)))
+        assert err <= TOL, "call %d: peak-normalised error %.3e" % (call, err)
+
+
+def test_noalloc_refuses_requests_beyond_its_scratch():
+    s = _setup()
+    traj = s.trajectory_array()
+    obs = np.zeros((5, 3))
+    obs[:, 2] = 30.0
+    rc, out, msg = _noalloc(traj, obs, 20)
+    assert rc == 3 and "16 MiB" in msg
+    rc, out, msg = _noalloc(traj, np.tile(obs, (20000, 1)), 10)
+    assert rc == 3 and "scratch" in msg
