@@ -330,9 +330,10 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   state_.reserve(sizeof(double) * 7 * N);
 
   unsigned* cnt = cnt_.as<unsigned>();  // [0], [1] list counts, [2] sticky error word
-  unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);  // [0] not converged, [1] samples
+  // [0] not converged, [1] samples, [2] unit counter of the running wave
+  unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);
   check(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), st), "memset");
-  check(cudaMemsetAsync(c64, 0, 2 * sizeof(unsigned long long), st), "memset");
+  check(cudaMemsetAsync(c64, 0, 3 * sizeof(unsigned long long), st), "memset");
 
   const double* d_obs = obs_.as<double>();
   const double* d_nrm = rq.normals ? nrm_.as<double>() : nullptr;
@@ -369,10 +370,11 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
-      w.part = part_.as<double>(); w.err = cnt + 2;
+      w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
       auto ev = timed_begin(st);
-      if (mixed) check(launch_fd_wave_mixed(w, frame_, (int)grid_of[L], variant, st), "flux wave (mixed)");
-      else check(launch_fd_wave_fp64(w, (int)grid_of[L], variant, st), "flux wave");
+      const int g = (int)std::min<int64_t>(grid_of[L], resident);
+      if (mixed) check(launch_fd_wave_mixed(w, frame_, g, variant, st), "flux wave (mixed)");
+      else check(launch_fd_wave_fp64(w, g, variant, st), "flux wave");
       timed_end(ev, st);
       FdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
@@ -382,16 +384,16 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
-      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1;
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = c64 + 2;
       check(launch_fd_finalize(f, N, st), "flux finalize");
     } else {
       PdWaveArgs w{};
       w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
-      w.part = part_.as<double>(); w.err = cnt + 2;
+      w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
       auto ev = timed_begin(st);
-      check(launch_pd_wave_fp64(w, (int)grid_of[L], st), "power density wave");
+      check(launch_pd_wave_fp64(w, (int)std::min<int64_t>(grid_of[L], resident), st), "power density wave");
       timed_end(ev, st);
       PdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
@@ -401,7 +403,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       f.bdmax_levels = reinterpret_cast<const double*>(bd_bits_.p);
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
-      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1;
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = c64 + 2;
       check(launch_pd_finalize(f, N, st), "power density finalize");
     }
     last_launches += 2;

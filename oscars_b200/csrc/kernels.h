@@ -59,8 +59,9 @@ struct FdWaveArgs {
   const unsigned* n_act;    // device count of `act`
   int first, level, tile_entries, min_span;
   int64_t target_units;
-  double* part;             // partials [(seg*spans + span) * kFdPartials + k][n_act]
+  double* part;             // partials, entry-major: [slot][seg][span][kFdPartials]
   unsigned* err;
+  unsigned long long* work;  // next unit to take (zero at launch; the finalize resets it)
 };
 
 struct FdFinalArgs {
@@ -80,6 +81,7 @@ struct FdFinalArgs {
   int* level_out;
   unsigned long long* not_converged;
   unsigned long long* samples;
+  unsigned long long* work_reset;  // the wave's unit counter, zeroed for the next wave
 };
 
 struct PdWaveArgs {
@@ -93,8 +95,9 @@ struct PdWaveArgs {
   const unsigned* n_act;
   int first, level, tile_entries, min_span;
   int64_t target_units;
-  double* part;             // partials [(seg*spans + span)][n_act]
+  double* part;             // partials, entry-major: [slot][seg][span]
   unsigned* err;
+  unsigned long long* work;
 };
 
 struct PdFinalArgs {
@@ -113,6 +116,7 @@ struct PdFinalArgs {
   int* level_out;
   unsigned long long* not_converged;
   unsigned long long* samples;
+  unsigned long long* work_reset;
 };
 
 // Frame of the mixed-precision path: origin x0 (particle start), rows of rot = e1, e2, e3 with e3 the

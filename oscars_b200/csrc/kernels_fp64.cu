@@ -83,19 +83,26 @@ __global__ void k_level_fill(const double* __restrict__ knots, int64_t n, double
 // 2887-2891).  Positive doubles order like their bit patterns, so atomicMax on the bits is exact.
 __global__ void k_level_betadiff(const double* __restrict__ lev, int64_t cap, int64_t s_begin, int64_t s_end,
                                  unsigned long long* __restrict__ bdmax_bits, int extended_level) {
+  __shared__ unsigned long long blk[32];  // per-level maxima of this block, merged into global at the end
+  if (threadIdx.x < 32) blk[threadIdx.x] = 0;
+  __syncthreads();
   const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= s_end) return;
-  int L;
-  int64_t i;
-  if (extended_level >= 0) { L = extended_level; i = s; }
-  else { L = 63 - __clzll((unsigned long long)s); i = s - ((int64_t)1 << L); }
-  if (i == 0) return;
-  const double* bx = lev + 4 * cap;
-  const double* by = lev + 5 * cap;
-  const double* bz = lev + 6 * cap;
-  const double dx = __dsub_rn(bx[s], bx[s - 1]), dy = __dsub_rn(by[s], by[s - 1]), dz = __dsub_rn(bz[s], bz[s - 1]);
-  const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-  atomicMax(&bdmax_bits[L], (unsigned long long)__double_as_longlong(d));
+  if (s < s_end) {
+    int L;
+    int64_t i;
+    if (extended_level >= 0) { L = extended_level; i = s; }
+    else { L = 63 - __clzll((unsigned long long)s); i = s - ((int64_t)1 << L); }
+    if (i > 0) {
+      const double* bx = lev + 4 * cap;
+      const double* by = lev + 5 * cap;
+      const double* bz = lev + 6 * cap;
+      const double dx = __dsub_rn(bx[s], bx[s - 1]), dy = __dsub_rn(by[s], by[s - 1]), dz = __dsub_rn(bz[s], bz[s - 1]);
+      const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+      atomicMax(&blk[L & 31], (unsigned long long)__double_as_longlong(d));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 32 && blk[threadIdx.x]) atomicMax(&bdmax_bits[threadIdx.x], blk[threadIdx.x]);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -137,7 +144,6 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
   if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, kFdThreads, A.target_units, A.min_span);
   __syncthreads();
   const int64_t units = P.tiles * P.spans;
-  if ((int64_t)blockIdx.x >= units) return;  // whole CTA idle
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
@@ -145,8 +151,13 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
   }
   __syncthreads();
   uint32_t phase_bits = 0;  // parity of the next completion expected on each buffer
-  {
-    const int64_t u = blockIdx.x;  // one (tile, span) unit per CTA; the grid covers the largest plan
+  __shared__ int64_t next_unit;
+  for (;;) {  // CTAs take (tile, span) units from a shared counter until the wave's units run out
+    if (tid == 0) next_unit = (int64_t)atomicAdd(A.work, 1ull);
+    __syncthreads();
+    const int64_t u = next_unit;
+    __syncthreads();
+    if (u >= units) break;
     const int64_t tile = u / P.spans;
     const int span = (int)(u % P.spans);
     const int64_t slot = tile * kFdThreads + tid;
@@ -237,13 +248,12 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
         }
         __syncthreads();  // everyone is done with `buf` before it is refilled
       }
-      if (live) {
-        double* p = A.part + ((int64_t)(g * P.spans + span) * kFdPartials) * n_act + slot;
-        p[0 * n_act] = sxr; p[1 * n_act] = sxi; p[2 * n_act] = syr; p[3 * n_act] = syi;
-        p[4 * n_act] = szr; p[5 * n_act] = szi;
-        p[6 * n_act] = have ? first_phase : 0.0;
-        p[7 * n_act] = have ? last_phase : 0.0;
-        p[8 * n_act] = have ? dmax : -1.0;  // -1 marks an empty span
+      if (live) {  // entry-major: the finalize reads an entry's spans contiguously
+        double* p = A.part + (slot * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
+        p[0] = sxr; p[1] = sxi; p[2] = syr; p[3] = syi; p[4] = szr; p[5] = szi;
+        p[6] = have ? first_phase : 0.0;
+        p[7] = have ? last_phase : 0.0;
+        p[8] = have ? dmax : -1.0;  // -1 marks an empty span
       }
     }
   }
@@ -267,39 +277,76 @@ __device__ __forceinline__ double c3_mag2(C3 a) {
 
 // Reduce the span partials of the wave, apply the stop rule of src/OSCARSSR.cc:4222-4238, finish
 // converged / last-level entries (:4246-4267) and append the others to the next active list.
+// Span partials of one entry are reduced by a group of kFinLanes lanes: lane l sums the spans
+// l, l + kFinLanes, ... in order, then a fixed shuffle tree combines the lanes (deterministic).
+constexpr int kFinLanes = 8;
+
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = kFinLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, kFinLanes);
+  return v;
+}
+__device__ __forceinline__ double group_max(double v) {
+#pragma unroll
+  for (int o = kFinLanes / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o, kFinLanes));
+  return v;
+}
+
+// Warp-aggregated bookkeeping of the finalize kernels: one atomic per warp for the survivor list and
+// one per warp for each statistics counter, instead of one per entry on a single address.
+__device__ __forceinline__ void finalize_bookkeeping(bool finished, bool unconverged, bool survive, int64_t item,
+                                                     int L, int* act_next, unsigned* n_next,
+                                                     unsigned long long* not_converged, unsigned long long* samples) {
+  const unsigned full = 0xffffffffu;
+  const int lane32 = threadIdx.x & 31;
+  const unsigned fin = __ballot_sync(full, finished);
+  const unsigned unc = __ballot_sync(full, unconverged);
+  const unsigned sur = __ballot_sync(full, survive);
+  const int leader = 0;
+  if (lane32 == leader) {
+    if (fin) atomicAdd(samples, (unsigned long long)__popc(fin) * (unsigned long long)((2ll << L) - 1));
+    if (unc) atomicAdd(not_converged, (unsigned long long)__popc(unc));
+  }
+  unsigned base = 0;
+  if (sur && lane32 == __ffs(sur) - 1) base = atomicAdd(n_next, (unsigned)__popc(sur));
+  base = __shfl_sync(full, base, sur ? __ffs(sur) - 1 : 0);
+  if (survive) act_next[base + __popc(sur & ((1u << lane32) - 1u))] = (int)item;
+}
+
 __global__ void k_fd_finalize(FdFinalArgs A) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.work_reset) *A.work_reset = 0;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= n_act) return;
+  const int lane = threadIdx.x % kFinLanes;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kFinLanes;
+  if ((int64_t)blockIdx.x * blockDim.x / kFinLanes >= n_act) return;  // whole block idle
+  const bool live = slot < n_act;
   const WavePlan P = wave_plan(A.first, A.level, n_act, A.tile_entries, A.target_units, A.min_span);
-  const int64_t item = A.act ? (int64_t)A.act[slot] : slot;
-  const int64_t ps = n_act;
+  const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+  // sums and max phase step of segment g over this lane's spans, then over the group
   auto seg_sum = [&](int g, C3& s, double& dmax) {
-    double prev_last = 0;
-    bool prev_have = false;
-    for (int sp = 0; sp < P.spans; ++sp) {
-      const double* p = A.part + ((int64_t)(g * P.spans + sp) * kFdPartials) * ps + slot;
-      s.xr += p[0]; s.xi += p[ps]; s.yr += p[2 * ps]; s.yi += p[3 * ps]; s.zr += p[4 * ps]; s.zi += p[5 * ps];
-      const double dm = p[8 * ps];
-      if (dm >= 0) {  // non-empty span
-        if (prev_have) {
-          const double d = fabs(__dsub_rn(p[6 * ps], prev_last));
-          dmax = d > dmax ? d : dmax;
+    C3 t = {0, 0, 0, 0, 0, 0};
+    double dm = 0;
+    if (live) {
+      const double* base = A.part + (slot * P.nseg * P.spans + g * P.spans) * kFdPartials;
+      for (int sp = lane; sp < P.spans; sp += kFinLanes) {
+        const double* p = base + sp * kFdPartials;
+        t.xr += p[0]; t.xi += p[1]; t.yr += p[2]; t.yi += p[3]; t.zr += p[4]; t.zi += p[5];
+        if (p[8] >= 0) {  // non-empty span (empty spans only trail the segment)
+          dm = fmax(dm, p[8]);
+          if (sp > 0) dm = fmax(dm, fabs(__dsub_rn(p[6], p[-kFdPartials + 7])));
         }
-        dmax = dm > dmax ? dm : dmax;
-        prev_last = p[7 * ps];
-        prev_have = true;
       }
     }
+    s.xr += group_sum(t.xr); s.xi += group_sum(t.xi); s.yr += group_sum(t.yr);
+    s.yi += group_sum(t.yi); s.zr += group_sum(t.zr); s.zi += group_sum(t.zi);
+    dmax = fmax(dmax, group_max(dm));
   };
   const int64_t N = A.n_items;
-  C3 S;
-  double last_mag;
+  C3 S = {0, 0, 0, 0, 0, 0};
+  double last_mag = -1;
   double dmax = 0;
   if (A.first) {
-    S = {0, 0, 0, 0, 0, 0};
     double unused = 0;
-    last_mag = -1;
     if (P.nseg == 2) {
       seg_sum(0, S, unused);
       C3 t = c3_scale(S, A.dt_prev);
@@ -308,35 +355,42 @@ __global__ void k_fd_finalize(FdFinalArgs A) {
     }
     seg_sum(P.nseg - 1, S, dmax);
   } else {
-    S = {A.state[item], A.state[N + item], A.state[2 * N + item], A.state[3 * N + item], A.state[4 * N + item], A.state[5 * N + item]};
-    last_mag = A.state[6 * N + item];
+    if (live) {
+      S = {A.state[item], A.state[N + item], A.state[2 * N + item], A.state[3 * N + item], A.state[4 * N + item],
+           A.state[5 * N + item]};
+      last_mag = A.state[6 * N + item];
+    }
     seg_sum(0, S, dmax);
   }
-  C3 t = c3_scale(S, A.dt_level);
-  if (A.project) t = c3_project(t, A.pol);
-  const double this_mag = c3_mag2(t);
-  const double prec = fabs(this_mag - last_mag) / last_mag;
-  const int L = A.level;
-  const bool stop = (L > 8 && prec < A.precision && dmax < kPiD) || (L > 8 && dmax < kPiD && this_mag == last_mag);
-  if (stop || L >= A.max_level) {
-    const int result_level = stop ? L : -1;
-    C3 E = c3_scale(S, A.c0 * A.dt_level);
-    if (A.project) E = c3_project(E, A.pol);
-    double v;
-    if (A.quantity == 1) v = prec * A.weight;
-    else if (A.quantity == 2) v = (double)result_level * A.weight;
-    else v = A.c2 * c3_mag2(E) * A.weight;
-    A.out[item] = v;
-    if (A.level_out) A.level_out[item] = result_level;
-    if (!stop) atomicAdd(A.not_converged, 1ull);
-    atomicAdd(A.samples, (unsigned long long)((2ll << L) - 1));
-  } else {
-    A.state[item] = S.xr; A.state[N + item] = S.xi; A.state[2 * N + item] = S.yr;
-    A.state[3 * N + item] = S.yi; A.state[4 * N + item] = S.zr; A.state[5 * N + item] = S.zi;
-    A.state[6 * N + item] = this_mag;
-    const unsigned int k = atomicAdd(A.n_next, 1u);
-    A.act_next[k] = (int)item;
+  bool finished = false, unconverged = false, survive = false;
+  if (live && lane == 0) {
+    C3 t = c3_scale(S, A.dt_level);
+    if (A.project) t = c3_project(t, A.pol);
+    const double this_mag = c3_mag2(t);
+    const double prec = fabs(this_mag - last_mag) / last_mag;
+    const int L = A.level;
+    const bool stop = (L > 8 && prec < A.precision && dmax < kPiD) || (L > 8 && dmax < kPiD && this_mag == last_mag);
+    if (stop || L >= A.max_level) {
+      const int result_level = stop ? L : -1;
+      C3 E = c3_scale(S, A.c0 * A.dt_level);
+      if (A.project) E = c3_project(E, A.pol);
+      double v;
+      if (A.quantity == 1) v = prec * A.weight;
+      else if (A.quantity == 2) v = (double)result_level * A.weight;
+      else v = A.c2 * c3_mag2(E) * A.weight;
+      A.out[item] = v;
+      if (A.level_out) A.level_out[item] = result_level;
+      finished = true;
+      unconverged = !stop;
+    } else {
+      const int64_t N = A.n_items;
+      A.state[item] = S.xr; A.state[N + item] = S.xi; A.state[2 * N + item] = S.yr;
+      A.state[3 * N + item] = S.yi; A.state[4 * N + item] = S.zr; A.state[5 * N + item] = S.zi;
+      A.state[6 * N + item] = this_mag;
+      survive = true;
+    }
   }
+  finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -361,7 +415,6 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
   if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, kPdThreads, A.target_units, A.min_span);
   __syncthreads();
   const int64_t units = P.tiles * P.spans;
-  if ((int64_t)blockIdx.x >= units) return;
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
@@ -369,8 +422,13 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
   }
   __syncthreads();
   uint32_t phase_bits = 0;
-  {
-    const int64_t u = blockIdx.x;  // one (tile, span) unit per CTA; the grid covers the largest plan
+  __shared__ int64_t next_unit;
+  for (;;) {  // CTAs take (tile, span) units from a shared counter until the wave's units run out
+    if (tid == 0) next_unit = (int64_t)atomicAdd(A.work, 1ull);
+    __syncthreads();
+    const int64_t u = next_unit;
+    __syncthreads();
+    if (u >= units) break;
     const int64_t tile = u / P.spans;
     const int span = (int)(u % P.spans);
     const int64_t slot = tile * kPdThreads + tid;
@@ -443,65 +501,77 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
         }
         __syncthreads();
       }
-      if (live) A.part[(int64_t)(g * P.spans + span) * n_act + slot] = sum;
+      if (live) A.part[slot * P.nseg * P.spans + g * P.spans + span] = sum;
     }
   }
 }
 
 // src/OSCARSSR.cc:2924-2968
 __global__ void k_pd_finalize(PdFinalArgs A) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && A.work_reset) *A.work_reset = 0;
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
-  const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= n_act) return;
+  const int lane = threadIdx.x % kFinLanes;
+  const int64_t slot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kFinLanes;
+  if ((int64_t)blockIdx.x * blockDim.x / kFinLanes >= n_act) return;
+  const bool live = slot < n_act;
   const WavePlan P = wave_plan(A.first, A.level, n_act, A.tile_entries, A.target_units, A.min_span);
-  const int64_t item = A.act ? (int64_t)A.act[slot] : slot;
+  const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
   const int64_t N = A.n_items;
-  double sum, last_sum;
+  auto seg_sum = [&](int g) {
+    double t = 0;
+    if (live)
+      for (int sp = lane; sp < P.spans; sp += kFinLanes) t += A.part[slot * P.nseg * P.spans + g * P.spans + sp];
+    return group_sum(t);
+  };
+  double sum = 0, last_sum = -1;
   if (A.first) {
-    sum = 0;
-    last_sum = -1;
     if (P.nseg == 2) {
-      for (int sp = 0; sp < P.spans; ++sp) sum += A.part[(int64_t)sp * n_act + slot];
+      sum += seg_sum(0);
       last_sum = sum * A.dt_prev;
     }
-    for (int sp = 0; sp < P.spans; ++sp) sum += A.part[(int64_t)((P.nseg - 1) * P.spans + sp) * n_act + slot];
+    sum += seg_sum(P.nseg - 1);
   } else {
-    sum = A.state[item];
-    last_sum = A.state[N + item];
-    for (int sp = 0; sp < P.spans; ++sp) sum += A.part[(int64_t)sp * n_act + slot];
+    if (live) {
+      sum = A.state[item];
+      last_sum = A.state[N + item];
+    }
+    sum += seg_sum(0);
   }
-  const int L = A.level;
-  const double this_sum = sum * A.dt_level;
-  double prec = fabs(this_sum - last_sum) / last_sum;
-  const double bd = A.bdmax_levels[L];
-  int result_level = -1;
-  bool stop = false;
-  if ((L > 8 && prec < A.precision && bd < A.two_over_gamma) || (L > 8 && bd < A.two_over_gamma && this_sum == last_sum)) {
-    stop = true;
-    result_level = L;
-  } else if (L > 8 && this_sum == last_sum) {
-    stop = true;
-    result_level = L;
-    prec = 0;
+  bool finished = false, unconverged = false, survive = false;
+  if (live && lane == 0) {
+    const int L = A.level;
+    const double this_sum = sum * A.dt_level;
+    double prec = fabs(this_sum - last_sum) / last_sum;
+    const double bd = A.bdmax_levels[L];
+    int result_level = -1;
+    bool stop = false;
+    if ((L > 8 && prec < A.precision && bd < A.two_over_gamma) || (L > 8 && bd < A.two_over_gamma && this_sum == last_sum)) {
+      stop = true;
+      result_level = L;
+    } else if (L > 8 && this_sum == last_sum) {
+      stop = true;
+      result_level = L;
+      prec = 0;
+    }
+    if (stop || L >= A.max_level) {
+      double sv = sum * (A.scale * A.dt_level);
+      sv /= 1e6;
+      if (!A.directional && sv < 0) sv *= -1;
+      double v;
+      if (A.quantity == 1) v = prec * A.weight;
+      else if (A.quantity == 2) v = (double)result_level * A.weight;
+      else v = sv * A.weight;
+      A.out[item] = v;
+      if (A.level_out) A.level_out[item] = result_level;
+      finished = true;
+      unconverged = !stop;
+    } else {
+      A.state[item] = sum;
+      A.state[N + item] = this_sum;
+      survive = true;
+    }
   }
-  if (stop || L >= A.max_level) {
-    double s = sum * (A.scale * A.dt_level);
-    s /= 1e6;
-    if (!A.directional && s < 0) s *= -1;
-    double v;
-    if (A.quantity == 1) v = prec * A.weight;
-    else if (A.quantity == 2) v = (double)result_level * A.weight;
-    else v = s * A.weight;
-    A.out[item] = v;
-    if (A.level_out) A.level_out[item] = result_level;
-    if (!stop) atomicAdd(A.not_converged, 1ull);
-    atomicAdd(A.samples, (unsigned long long)((2ll << L) - 1));
-  } else {
-    A.state[item] = sum;
-    A.state[N + item] = this_sum;
-    const unsigned int k = atomicAdd(A.n_next, 1u);
-    A.act_next[k] = (int)item;
-  }
+  finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples);
 }
 
 }  // namespace dev
@@ -534,7 +604,8 @@ cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int grid, int variant, cuda
 cudaError_t launch_fd_finalize(const FdFinalArgs& a, int64_t n_act_bound, cudaStream_t st) {
   if (n_act_bound == 0) return cudaSuccess;
   const int T = 256;
-  dev::k_fd_finalize<<<(unsigned)((n_act_bound + T - 1) / T), T, 0, st>>>(a);
+  const int64_t threads = n_act_bound * dev::kFinLanes;
+  dev::k_fd_finalize<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -546,7 +617,8 @@ cudaError_t launch_pd_wave_fp64(const PdWaveArgs& a, int grid, cudaStream_t st) 
 cudaError_t launch_pd_finalize(const PdFinalArgs& a, int64_t n_act_bound, cudaStream_t st) {
   if (n_act_bound == 0) return cudaSuccess;
   const int T = 256;
-  dev::k_pd_finalize<<<(unsigned)((n_act_bound + T - 1) / T), T, 0, st>>>(a);
+  const int64_t threads = n_act_bound * dev::kFinLanes;
+  dev::k_pd_finalize<<<(unsigned)((threads + T - 1) / T), T, 0, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -80,7 +80,6 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
   if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, kMxThreads * EPT, A.target_units, A.min_span);
   __syncthreads();
   const int64_t units = P.tiles * P.spans;
-  if ((int64_t)blockIdx.x >= units) return;
   const float4* rec = reinterpret_cast<const float4*>(A.lev);
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
@@ -89,8 +88,13 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
   }
   __syncthreads();
   uint32_t phase_bits = 0;
-  {
-    const int64_t u = blockIdx.x;  // one (tile, span) unit per CTA; the grid covers the largest plan
+  __shared__ int64_t next_unit;
+  for (;;) {  // CTAs take (tile, span) units from a shared counter until the wave's units run out
+    if (tid == 0) next_unit = (int64_t)atomicAdd(A.work, 1ull);
+    __syncthreads();
+    const int64_t u = next_unit;
+    __syncthreads();
+    if (u >= units) break;
     const int64_t tile = u / P.spans;
     const int span = (int)(u % P.spans);
     // entry constants
@@ -211,12 +215,12 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
 #pragma unroll
       for (int e = 0; e < EPT; ++e) {
         if (!live[e]) continue;
-        double* p = A.part + ((int64_t)(g * P.spans + span) * kFdPartials) * n_act + slot[e];
+        double* p = A.part + (slot[e] * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) p[k * n_act] = S[e][k];
-        p[6 * n_act] = have[e] ? (double)first[e] : 0.0;
-        p[7 * n_act] = have[e] ? (double)last[e] : 0.0;
-        p[8 * n_act] = have[e] ? (double)dmax[e] : -1.0;
+        for (int k = 0; k < 6; ++k) p[k] = S[e][k];
+        p[6] = have[e] ? (double)first[e] : 0.0;
+        p[7] = have[e] ? (double)last[e] : 0.0;
+        p[8] = have[e] ? (double)dmax[e] : -1.0;
       }
     }
   }

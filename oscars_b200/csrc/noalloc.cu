@@ -151,7 +151,7 @@ extern "C" OSC_API int osc_flux_fixed_level_noalloc(int device, const double* tr
     FdWaveArgs a{};
     a.lev = lev; a.cap = cap; a.obs = obs; a.omega = omega; a.n_e = 1; a.n_items = n_obs;
     a.act = nullptr; a.n_act = nullptr; a.first = 1; a.level = level; a.tile_entries = 128; a.min_span = 32;
-    a.target_units = 1; a.part = part; a.err = cnt + 2;
+    a.target_units = 1; a.part = part; a.err = cnt + 2; a.work = c64 + 2;  // zeroed with the counters
     e = launch_fd_wave_fp64(a, (int)(plan.tiles * plan.spans), 0, st);
   }
   if (e == cudaSuccess) {
@@ -163,7 +163,7 @@ extern "C" OSC_API int osc_flux_fixed_level_noalloc(int device, const double* tr
     for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
     f.n_items = n_obs; f.act = nullptr; f.n_act = nullptr; f.state = u;  // never written at the last level
     f.act_next = reinterpret_cast<int*>(u); f.n_next = cnt + 1;
-    f.out = res; f.level_out = nullptr; f.not_converged = c64; f.samples = c64 + 1;
+    f.out = res; f.level_out = nullptr; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = c64 + 2;
     e = launch_fd_finalize(f, n_obs, st);
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, res, sizeof(double) * n_obs, cudaMemcpyDeviceToHost);
