@@ -166,6 +166,41 @@ OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double*
                               long long n_obs, int directional, const osc_rad_opts* opts,
                               double* out, int32_t* level_out, long long* n_not_converged);
 
+/* ---- batches of independent jobs (no reference counterpart: the reference integrates one
+ *      particle through one field container per call).  Job k is the ideal particle of a beam of
+ *      `particle` at energy_GeV, starting at x0 along d0 at t0, through fields
+ *      [field_begin, field_begin + field_count) of `fields`, tracked over [ctstart, ctstop] with
+ *      npoints RK4 points, and observed at observers [obs_begin, obs_begin + n_obs) of obs_xyz and
+ *      energies [energy_begin, energy_begin + n_energies) of energies_eV. */
+typedef struct {
+  int field_begin, field_count;
+  int particle;             /* osc_particle_type */
+  double charge, mass;      /* [C], [kg]; custom particles only */
+  double energy_GeV;
+  double x0[3];             /* [m] */
+  double d0[3];             /* direction */
+  double t0;                /* [m] */
+  double current;           /* [A]; 0 = the particle charge */
+  double ctstart, ctstop;   /* [m] */
+  long long npoints;
+  long long obs_begin, n_obs;
+  long long energy_begin, n_energies;
+  int spectrum;             /* 1: normalised like osc_spectrum (|current|), 0: like osc_flux */
+} osc_job_desc;
+
+/* opts->precision_mode OSC_MIXED integrates all jobs in shared launches (trajectories, splines
+ * and level samples on the device; the waves up to level 13 replayed from a CUDA graph once a
+ * shape is known); OSC_FP64 runs the jobs one after another through osc_flux's FP64 path.
+ * opts->nparticles must be 0.  out: with average == 0, every job's n_obs x n_energies values in
+ * job order (observer-major, energy fastest); with average != 0, the jobs (which must then share
+ * observers and energies) are averaged with weight 1/n_jobs in job order -- a multi-particle beam.
+ * level_out (may be NULL) has the same layout (the last job's levels when averaging). */
+OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fields,
+                           const osc_job_desc* jobs, int n_jobs, const double* obs_xyz,
+                           long long n_obs, const double* energies_eV, long long n_energies,
+                           const osc_rad_opts* opts, int average, double* out,
+                           int32_t* level_out, long long* n_not_converged);
+
 /* ---- device-resident variants: same arithmetic, pointers are device memory on the context's
  *      device, work is queued on `stream` (a cudaStream_t, NULL = the context's stream) and the
  *      call returns without synchronising.  Single particle (opts->nparticles must be 0). */
@@ -187,7 +222,8 @@ OSC_API int osc_last_stats(osc_ctx* ctx, long long* samples, long long* launches
 OSC_API int osc_set_profiling(osc_ctx* ctx, int enable);
 OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches, long long* samples,
                             int reset);
-/* Kernel variants of the sample sums.  kind 0 = FP64 flux/spectrum, 2 = mixed flux/spectrum.
+/* Kernel variants of the sample sums.  kind 0 = FP64 flux/spectrum, 2 = mixed flux/spectrum,
+ * 3 = batched mixed (osc_batch_flux and multi-particle mixed requests; tuned on the first wave).
  * variant >= 0 forces a compiled variant; -1 (default) lets the context autotune: the first call
  * of each request shape times every variant and keeps the fastest.  osc_get_variant reports the
  * variant the last request of that kind used and the number of compiled variants. */

@@ -43,6 +43,13 @@ class RadOpts(ctypes.Structure):
                 ("quantity", I), ("precision_mode", I)]
 
 
+class JobDesc(ctypes.Structure):
+    _fields_ = [("field_begin", I), ("field_count", I), ("particle", I), ("charge", D), ("mass", D),
+                ("energy_GeV", D), ("x0", D * 3), ("d0", D * 3), ("t0", D), ("current", D), ("ctstart", D),
+                ("ctstop", D), ("npoints", LL), ("obs_begin", LL), ("n_obs", LL), ("energy_begin", LL),
+                ("n_energies", LL), ("spectrum", I)]
+
+
 # name -> (restype, argtypes); this table is also the list of exported symbols the tests check
 SIGNATURES = {
     "osc_get_device_count": (I, [ctypes.POINTER(I)]),
@@ -69,6 +76,8 @@ SIGNATURES = {
     "osc_power_density": (I, [VP, DP, DP, LL, I, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
     "osc_flux_device": (I, [VP, VP, LL, D, ctypes.POINTER(RadOpts), VP, VP, VP]),
     "osc_power_density_device": (I, [VP, VP, VP, LL, I, ctypes.POINTER(RadOpts), VP, VP, VP]),
+    "osc_batch_flux": (I, [VP, ctypes.POINTER(FieldDesc), I, ctypes.POINTER(JobDesc), I, DP, LL, DP, LL,
+                           ctypes.POINTER(RadOpts), I, DP, I32P, LLP]),
     "osc_last_stats": (I, [VP, LLP, LLP]),
     "osc_set_profiling": (I, [VP, I]),
     "osc_get_profile": (I, [VP, DP, LLP, LLP, I]),

@@ -1,0 +1,1015 @@
+// batch.cu -- many radiation jobs integrated in the same launches (mixed precision).
+//
+// A job is one particle through its own field set and trajectory range, observed on its own
+// observer list at its own energies.  A multi-particle beam is a batch of jobs that share fields,
+// observers and energies and whose results are averaged (src/OSCARSSR.cc:4026-4062); a set of
+// uneven undulator jobs is a batch of unrelated jobs.  Per chunk of jobs every stage runs once over
+// all of them:
+//   k_batch_rk4       FP64 RK4, one thread per (job, direction)           src/OSCARSSR.cc:910-1009
+//   k_batch_extent    trajectory extent in the job frame (validity bound of the mixed phase form)
+//   k_batch_spline    clamped cubic spline, one thread per (job, component) include/TOMATH.h:141-203
+//   k_batch_fill      level samples written straight as 48-byte mixed records, one thread per sample
+//   k_batch_plan      per-job tiles, units, partial offsets and active offsets of a wave (one block)
+//   k_batch_wave      the mixed sample sum; persistent CTAs take (job, tile, span) units from a counter
+//   k_batch_finalize  span reduction and the stop rule of src/OSCARSSR.cc:4222-4238 per entry
+//   k_batch_average   compensated mean over the jobs of a beam, in particle order
+// The launches of a chunk up to the prefilled level are captured once into a CUDA graph and
+// replayed; only waves beyond that level need the host (to size the next level's records).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "device_common.cuh"
+#include "engine.h"
+#include "fd_common.cuh"
+#include "kernels.h"
+
+namespace osc {
+namespace dev {
+
+// ---------------------------------------------------------------------------------------------
+// Fields and RK4 on the device.  Same operations as the host model (TField3D_IdealUndulator /
+// TField3D_IdealEPU and TParticleA::RK4); sin and cos are CUDA's, so a trajectory agrees with the
+// host's to rounding, not bit for bit -- this path is the mixed-precision one.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void pole_block_d(const DevField& f, const double* amp, double d, double shift, double tc,
+                                             double* F) {
+  const double L = f.length, lam = f.period_length;
+  if (d > L / 2. + shift || d < -L / 2. + shift) return;
+  const double s = sin(2.0 * kPiD * (d - shift) / lam);
+  double k = 1.0;  // 1/4 and 3/4 end poles (src/TField3D_IdealUndulator.cc:125-142)
+  if (d < -L / 2. + shift + lam || d > L / 2. + shift - lam)
+    k = (d < -L / 2. + shift + lam / 2. || d > L / 2. + shift - lam / 2.) ? 0.25 : 0.75;
+  F[0] += amp[0] * k * s * tc;
+  F[1] += amp[1] * k * s * tc;
+  F[2] += amp[2] * k * s * tc;
+}
+
+__device__ void field_sum_d(const DevField* __restrict__ fs, int nf, double x, double y, double z, double t,
+                            double* B) {
+  B[0] = B[1] = B[2] = 0;
+  for (int i = 0; i < nf; ++i) {
+    const DevField& f = fs[i];
+    const double d = (x - f.center[0]) * f.period_unit[0] + (y - f.center[1]) * f.period_unit[1] +
+                     (z - f.center[2]) * f.period_unit[2];
+    const double tc = 1 + d * f.taper;
+    double F[3] = {0, 0, 0};
+    if (f.kind == 0) {
+      pole_block_d(f, f.a, d, f.phase * f.period_mag / (2.0 * kPiD), tc, F);
+    } else {  // EPU: A shifted by +phase/2, B by -phase/2 (src/TField3D_IdealEPU.cc:127-165)
+      pole_block_d(f, f.a, d, f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
+      pole_block_d(f, f.b, d, -f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
+    }
+    const double w = f.frequency == 0 ? 1.0 : cos(2.0 * kPiD * f.frequency * (t + f.time_offset) + f.frequency_phase);
+    B[0] += F[0] * w;
+    B[1] += F[1] * w;
+    B[2] += F[2] * w;
+  }
+}
+
+struct Rk4Ctx {
+  const DevField* fs;
+  int nf;
+  double qomg;
+  bool superluminal;
+};
+
+__device__ __forceinline__ void derivs_d(Rk4Ctx& c, double t, const double* x, double* dxdt) {
+  const double one_minus = 1. - (x[1] * x[1] + x[3] * x[3] + x[5] * x[5]) / (kCLight * kCLight);
+  if (one_minus <= 0) {  // a state at or above c: reported to the host, dxdt left as it was
+    c.superluminal = true;
+    return;
+  }
+  double B[3];
+  field_sum_d(c.fs, c.nf, x[0], x[2], x[4], t, B);
+  dxdt[0] = x[1];
+  dxdt[1] = c.qomg * (-x[5] * B[1] + x[3] * B[2]);
+  dxdt[2] = x[3];
+  dxdt[3] = c.qomg * (x[5] * B[0] - x[1] * B[2]);
+  dxdt[4] = x[5];
+  dxdt[5] = c.qomg * (x[1] * B[1] - x[3] * B[0]);
+}
+
+__device__ __forceinline__ void rk4_step_d(Rk4Ctx& c, double* y, const double* dydx, double x, double h) {
+  double dym[6], dyt[6], yt[6];
+  const double hh = h * 0.5, h6 = h / 6.0, xh = x + hh;
+  for (int i = 0; i < 6; ++i) yt[i] = y[i] + hh * dydx[i];
+  derivs_d(c, xh, yt, dyt);
+  for (int i = 0; i < 6; ++i) yt[i] = y[i] + hh * dyt[i];
+  derivs_d(c, xh, yt, dym);
+  for (int i = 0; i < 6; ++i) {
+    yt[i] = y[i] + h * dym[i];
+    dym[i] += dyt[i];
+  }
+  derivs_d(c, x + h, yt, dyt);
+  for (int i = 0; i < 6; ++i) y[i] = y[i] + h6 * (dydx[i] + dyt[i] + 2.0 * dym[i]);
+}
+
+// One thread per (job, direction).  Forward points land at [nb, nb + nf), backward points at
+// [0, nb) in time order; each point carries the acceleration of the state before it, as the
+// reference's integrator stores it (src/OSCARSSR.cc:930-1004).
+__global__ void k_batch_rk4(const DevJob* __restrict__ jobs, int njobs, const DevField* __restrict__ fields,
+                            double* __restrict__ arena, unsigned* __restrict__ err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * njobs) return;
+  const DevJob& J = jobs[t >> 1];
+  const bool fwd = (t & 1) == 0;
+  const int64_t n = (int64_t)J.nf + J.nb;
+  double* K = arena + J.knots;
+  Rk4Ctx c{fields + J.field_begin, J.field_count, J.qomg, false};
+  const double* x0 = J.frame.x0;
+  double x[6] = {x0[0], J.b0[0] * kCLight, x0[1], J.b0[1] * kCLight, x0[2], J.b0[2] * kCLight};
+  double dxdt[6] = {0, 0, 0, 0, 0, 0};
+  const double t0 = J.frame.t_ref;
+  auto store = [&](int64_t i, double tt) {
+    K[i] = tt;
+    K[n + i] = x[0];
+    K[2 * n + i] = x[2];
+    K[3 * n + i] = x[4];
+    K[4 * n + i] = x[1] / kCLight;
+    K[5 * n + i] = x[3] / kCLight;
+    K[6 * n + i] = x[5] / kCLight;
+    K[7 * n + i] = dxdt[1] / kCLight;
+    K[8 * n + i] = dxdt[3] / kCLight;
+    K[9 * n + i] = dxdt[5] / kCLight;
+  };
+  if (fwd) {
+    derivs_d(c, t0, x, dxdt);
+    for (int i = 0; i < J.nf; ++i) {
+      const double tt = t0 + J.dt * i;
+      store(J.nb + i, tt);
+      derivs_d(c, tt, x, dxdt);
+      rk4_step_d(c, x, dxdt, tt, J.dt);
+    }
+  } else {
+    const double dtr = -J.dt;
+    for (int i = 0; i < J.nb; ++i) {
+      const double t1 = t0 + dtr * i;
+      derivs_d(c, t1, x, dxdt);
+      rk4_step_d(c, x, dxdt, t1, dtr);
+      store(J.nb - 1 - i, t0 + dtr * (i + 1));
+    }
+  }
+  if (c.superluminal) atomicOr(err, kErrSuperluminal);
+}
+
+// Trajectory extent in the job frame: max transverse distance from the axis and max longitudinal
+// coordinate (one block of 256 threads per job).
+__global__ void k_batch_extent(DevJob* __restrict__ jobs, const double* __restrict__ arena) {
+  __shared__ double sx[256], sz[256];
+  DevJob& J = jobs[blockIdx.x];
+  const int64_t n = (int64_t)J.nf + J.nb;
+  const double* K = arena + J.knots;
+  const double* R = J.frame.rot;
+  const double* x0 = J.frame.x0;
+  double xp = 0, zm = -1e300;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double dx = K[n + i] - x0[0], dy = K[2 * n + i] - x0[1], dz = K[3 * n + i] - x0[2];
+    const double a = R[0] * dx + R[1] * dy + R[2] * dz;
+    const double b = R[3] * dx + R[4] * dy + R[5] * dz;
+    const double c = R[6] * dx + R[7] * dy + R[8] * dz;
+    xp = fmax(xp, sqrt(a * a + b * b));
+    zm = fmax(zm, c);
+  }
+  sx[threadIdx.x] = xp;
+  sz[threadIdx.x] = zm;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      sx[threadIdx.x] = fmax(sx[threadIdx.x], sx[threadIdx.x + o]);
+      sz[threadIdx.x] = fmax(sz[threadIdx.x], sz[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    J.frame.xperp_max = sx[0];
+    J.frame.z_max = sz[0];
+  }
+}
+
+// Clamped spline second derivatives (end slopes from the end differences, as TSpline1D3 sets
+// them), one thread per (job, component); `work` holds the forward-sweep terms.
+__global__ void k_batch_spline(const DevJob* __restrict__ jobs, int njobs, double* __restrict__ arena,
+                               double* __restrict__ work) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 9 * njobs) return;
+  const DevJob& J = jobs[t / 9];
+  const int c = t % 9;
+  const int64_t n = (int64_t)J.nf + J.nb;
+  const double* X = arena + J.knots;
+  const double* Y = X + (1 + c) * n;
+  double* ypp = arena + J.knots + (10 + c) * n;
+  double* u = work + J.u_off + c * n;
+  const double dydx0 = __ddiv_rn(__dsub_rn(Y[1], Y[0]), __dsub_rn(X[1], X[0]));
+  ypp[0] = -0.5;
+  u[0] = __dmul_rn(__ddiv_rn(3., __dsub_rn(X[1], X[0])),
+                   __dsub_rn(__ddiv_rn(__dsub_rn(Y[1], Y[0]), __dsub_rn(X[1], X[0])), dydx0));
+  for (int64_t i = 1; i < n - 1; ++i) {
+    const double sig = __ddiv_rn(__dsub_rn(X[i], X[i - 1]), __dsub_rn(X[i + 1], X[i - 1]));
+    const double p = __dadd_rn(__dmul_rn(sig, ypp[i - 1]), 2.0);
+    ypp[i] = __ddiv_rn(__dsub_rn(sig, 1.), p);
+    const double ui = __dsub_rn(__ddiv_rn(__dsub_rn(Y[i + 1], Y[i]), __dsub_rn(X[i + 1], X[i])),
+                                __ddiv_rn(__dsub_rn(Y[i], Y[i - 1]), __dsub_rn(X[i], X[i - 1])));
+    u[i] = __ddiv_rn(__dsub_rn(__ddiv_rn(__dmul_rn(6., ui), __dsub_rn(X[i + 1], X[i - 1])), __dmul_rn(sig, u[i - 1])), p);
+  }
+  const double dydxn = __ddiv_rn(__dsub_rn(Y[n - 1], Y[n - 2]), __dsub_rn(X[n - 1], X[n - 2]));
+  const double un = __dmul_rn(__ddiv_rn(3., __dsub_rn(X[n - 1], X[n - 2])),
+                              __dsub_rn(dydxn, __ddiv_rn(__dsub_rn(Y[n - 1], Y[n - 2]), __dsub_rn(X[n - 1], X[n - 2]))));
+  ypp[n - 1] = __ddiv_rn(__dsub_rn(un, __dmul_rn(0.5, u[n - 2])), __dadd_rn(__dmul_rn(0.5, ypp[n - 2]), 1.));
+  for (int64_t k = n - 2; k >= 0; --k) ypp[k] = __dadd_rn(__dmul_rn(ypp[k], ypp[k + 1]), u[k]);
+}
+
+// Level samples [s_begin, s_end) of every job whose active count is non-zero (all jobs when `cnt` is
+// NULL), evaluated from its spline and written as mixed records (fd_common.cuh) at
+// rec[3 * (j * stride + s - s_off)]; one thread per (job, sample).
+__global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const double* __restrict__ arena,
+                             const unsigned* __restrict__ cnt, float4* __restrict__ rec, int64_t stride,
+                             int64_t s_off, int64_t s_begin, int64_t s_end) {
+  const int64_t per = s_end - s_begin;
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= per * njobs) return;
+  const int j = (int)(g / per);
+  if (cnt && cnt[j] == 0) return;
+  const DevJob& J = jobs[j];
+  const int64_t s = s_begin + g % per;
+  const int64_t n = (int64_t)J.nf + J.nb;
+  const double T = level_time(J.tstart, J.tstop, s);
+  double v[9];
+  spline_eval9(arena + J.knots, n, T, v);
+  const MixedFrame& F = J.frame;
+  const double* R = F.rot;
+  const double dx = v[0] - F.x0[0], dy = v[1] - F.x0[1], dz = v[2] - F.x0[2];
+  const double x = R[0] * dx + R[1] * dy + R[2] * dz;
+  const double y = R[3] * dx + R[4] * dy + R[5] * dz;
+  const double z = R[6] * dx + R[7] * dy + R[8] * dz;
+  const double px = R[0] * v[3] + R[1] * v[4] + R[2] * v[5];
+  const double py = R[3] * v[3] + R[4] * v[4] + R[5] * v[5];
+  const double pz = R[6] * v[3] + R[7] * v[4] + R[8] * v[5];
+  const double qx = R[0] * v[6] + R[1] * v[7] + R[2] * v[8];
+  const double qy = R[3] * v[6] + R[4] * v[7] + R[5] * v[8];
+  const double qz = R[6] * v[6] + R[7] * v[7] + R[8] * v[8];
+  const double g2 = 1.0 - (px * px + py * py + pz * pz);       // 1 - b^2
+  const double ebz = (g2 + px * px + py * py) / (1.0 + pz);     // 1 - b_z without cancellation
+  const double taus = (T - F.t_ref) - z / kCLight;
+  float4* r = rec + 3 * (j * stride + s - s_off);
+  r[0] = make_float4((float)x, (float)y, (float)z, (float)taus);
+  r[1] = make_float4((float)px, (float)py, (float)ebz, (float)g2);
+  r[2] = make_float4((float)qx, (float)qy, (float)qz, 0.f);
+}
+
+// Offsets of one wave over the chunk (one block of 1024 threads): per job the active count n_j (all
+// entries on the first wave), units = ceil(n_j / tile) x spans, partial doubles
+// n_j x nseg x spans x kFdPartials, and exclusive prefix sums of the three.  `spans` is common to
+// the wave: the smallest power of two giving at least target_units units in total (wave_spans).
+__global__ void __launch_bounds__(1024) k_batch_plan(const DevJob* __restrict__ jobs, int njobs,
+                                                     const unsigned* __restrict__ cnt, int first, int L, int tile,
+                                                     int64_t target, int min_span, BatchPlan P) {
+  constexpr int T = 1024;
+  __shared__ int64_t red[3][T];
+  __shared__ int64_t carry[3];
+  __shared__ int spans_s;
+  const int tid = threadIdx.x;
+  int64_t tiles = 0;
+  for (int j = tid; j < njobs; j += T) {
+    const int64_t na = first ? jobs[j].n_obs * jobs[j].n_e : (int64_t)cnt[j];
+    tiles += (na + tile - 1) / tile;
+  }
+  red[0][tid] = tiles;
+  __syncthreads();
+  for (int o = T / 2; o > 0; o >>= 1) {
+    if (tid < o) red[0][tid] += red[0][tid + o];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    spans_s = wave_spans(L, red[0][0], target, min_span);
+    *P.spans = spans_s;
+    carry[0] = carry[1] = carry[2] = 0;
+  }
+  __syncthreads();
+  const int spans = spans_s;
+  const int nseg = (first && L >= 1) ? 2 : 1;
+  for (int base = 0; base < njobs; base += T) {
+    const int j = base + tid;
+    int64_t v[3] = {0, 0, 0};
+    if (j < njobs) {
+      const int64_t na = first ? jobs[j].n_obs * jobs[j].n_e : (int64_t)cnt[j];
+      v[0] = (na + tile - 1) / tile * spans;
+      v[1] = na * nseg * spans * kFdPartials;
+      v[2] = na;
+    }
+    for (int q = 0; q < 3; ++q) red[q][tid] = v[q];
+    __syncthreads();
+    for (int o = 1; o < T; o <<= 1) {  // inclusive scans (Hillis-Steele)
+      int64_t w[3];
+      for (int q = 0; q < 3; ++q) w[q] = tid >= o ? red[q][tid - o] : 0;
+      __syncthreads();
+      for (int q = 0; q < 3; ++q) red[q][tid] += w[q];
+      __syncthreads();
+    }
+    if (j < njobs) {
+      P.unit_start[j] = carry[0] + red[0][tid] - v[0];
+      P.part_start[j] = carry[1] + red[1][tid] - v[1];
+      P.act_start[j] = carry[2] + red[2][tid] - v[2];
+    }
+    __syncthreads();
+    if (tid == T - 1)
+      for (int q = 0; q < 3; ++q) carry[q] += red[q][T - 1];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    P.unit_start[njobs] = carry[0];
+    P.part_start[njobs] = carry[1];
+    P.act_start[njobs] = carry[2];
+  }
+}
+
+// Last j with starts[j] <= x (starts non-decreasing, starts[0] = 0 <= x).
+__device__ __forceinline__ int find_job(const int64_t* __restrict__ starts, int njobs, int64_t x) {
+  int lo = 0, hi = njobs;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (starts[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+constexpr int kBThreads = 128;
+constexpr int kBChunk = 256;
+constexpr int kBFold = 32;  // FP32 partial sums are folded into FP64 every kBFold samples
+
+struct BatchStage {
+  float4 v[2][kBChunk * 3];
+  uint64_t bar[2];
+};
+
+template <int EPT, int MINB>
+__global__ void __launch_bounds__(kBThreads, MINB) k_batch_wave(BatchWaveArgs A) {
+  __shared__ __align__(16) BatchStage st;
+  __shared__ WavePlan P;
+  __shared__ int64_t next_unit;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    P = wave_plan_spans(A.first, A.level, *A.plan.spans);
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int64_t units = A.plan.unit_start[A.njobs];
+  uint32_t phase_bits = 0;
+  for (;;) {  // CTAs take (job, tile, span) units from a shared counter until the wave's units run out
+    if (tid == 0) next_unit = (int64_t)atomicAdd(A.work, 1ull);
+    __syncthreads();
+    const int64_t u = next_unit;
+    __syncthreads();
+    if (u >= units) break;
+    const int j = find_job(A.plan.unit_start, A.njobs, u);
+    const DevJob& J = A.jobs[j];
+    const int64_t local = u - A.plan.unit_start[j];
+    const int64_t tile = local / P.spans;
+    const int span = (int)(local % P.spans);
+    const int64_t n_act = A.first ? J.n_obs * J.n_e : (int64_t)A.cnt[j];
+    float Ox[EPT], Oy[EPT], Oz[EPT], w[EPT], wc[EPT];
+    bool live[EPT];
+    int64_t slot[EPT];
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      slot[e] = tile * kBThreads * EPT + (int64_t)e * kBThreads + tid;
+      live[e] = slot[e] < n_act;
+      const int64_t item = live[e] ? (A.first ? slot[e] : (int64_t)A.act[J.entry_begin + slot[e]]) : 0;
+      const int64_t io = J.obs_begin + item / J.n_e, ie = J.omega_begin + item % J.n_e;
+      const double* R = J.frame.rot;
+      const double ox = A.obs[3 * io] - J.frame.x0[0], oy = A.obs[3 * io + 1] - J.frame.x0[1];
+      const double oz = A.obs[3 * io + 2] - J.frame.x0[2];
+      const double fx = R[0] * ox + R[1] * oy + R[2] * oz;
+      const double fy = R[3] * ox + R[4] * oy + R[5] * oz;
+      const double fz = R[6] * ox + R[7] * oy + R[8] * oz;
+      Ox[e] = (float)fx; Oy[e] = (float)fy; Oz[e] = (float)fz;
+      const double om = A.omega[ie];
+      w[e] = (float)om;
+      wc[e] = (float)(om / kCLight);
+      if (live[e] && span == 0 && !mixed_geometry_ok(fx, fy, fz, om, J.frame.xperp_max, J.frame.z_max))
+        atomicOr(A.err, kErrBadArgs);
+    }
+    // records of job j: sample s at rec_j[3 * (s - s_off)]
+    const float4* rec_j = A.rec + 3 * (int64_t)j * A.stride;
+    for (int g = 0; g < P.nseg; ++g) {
+      const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
+      const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
+      double S[EPT][6];
+      float first[EPT], last[EPT], dmax[EPT];
+      bool have[EPT];
+#pragma unroll
+      for (int e = 0; e < EPT; ++e) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) S[e][k] = 0.0;
+        first[e] = last[e] = 0.f;
+        dmax[e] = 0.f;
+        have[e] = false;
+      }
+      const int64_t nchunks = b1 > b0 ? (b1 - b0 + kBChunk - 1) / kBChunk : 0;
+      if (tid == 0 && nchunks > 0) {
+        const int64_t hi = min(b1, b0 + kBChunk);
+        mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - b0) * 48));
+        tma_load_1d(&st.v[0][0], rec_j + 3 * (b0 - A.s_off), (uint32_t)((hi - b0) * 48), &st.bar[0]);
+      }
+      for (int64_t c = 0; c < nchunks; ++c) {
+        const int buf = (int)(c & 1);
+        const int64_t lo = b0 + c * kBChunk, hi = min(b1, lo + kBChunk);
+        if (tid == 0 && c + 1 < nchunks) {  // prefetch the next chunk into the other buffer
+          const int64_t lo2 = lo + kBChunk, hi2 = min(b1, lo2 + kBChunk);
+          mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * 48));
+          tma_load_1d(&st.v[buf ^ 1][0], rec_j + 3 * (lo2 - A.s_off), (uint32_t)((hi2 - lo2) * 48), &st.bar[buf ^ 1]);
+        }
+        if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+          if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+          return;
+        }
+        phase_bits ^= 1u << buf;
+        const float4* sv = st.v[buf];
+        const int j0 = lo == 0 ? 1 : 0;  // sample 0 is the unused slot
+        const int n = (int)(hi - lo);
+        for (int jb = j0; jb < n; jb += kBFold) {
+          const int je = min(n, jb + kBFold);
+          float s32[EPT][6];
+#pragma unroll
+          for (int e = 0; e < EPT; ++e)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) s32[e][k] = 0.f;
+          for (int jj = jb; jj < je; ++jj) {
+            const float4 r0 = sv[3 * jj], r1 = sv[3 * jj + 1], r2 = sv[3 * jj + 2];
+#pragma unroll
+            for (int e = 0; e < EPT; ++e) {
+              const float ph = mixed_sample(r0, r1, r2, Ox[e], Oy[e], Oz[e], w[e], wc[e], s32[e]);
+              if (have[e]) {
+                dmax[e] = fmaxf(dmax[e], fabsf(ph - last[e]));
+              } else {
+                first[e] = ph;
+                have[e] = true;
+              }
+              last[e] = ph;
+            }
+          }
+#pragma unroll
+          for (int e = 0; e < EPT; ++e)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) S[e][k] += (double)s32[e][k];
+        }
+        __syncthreads();  // everyone is done with `buf` before it is refilled
+      }
+#pragma unroll
+      for (int e = 0; e < EPT; ++e) {
+        if (!live[e]) continue;
+        double* p = A.part + A.plan.part_start[j] + (slot[e] * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) p[k] = S[e][k];
+        p[6] = have[e] ? (double)first[e] : 0.0;
+        p[7] = have[e] ? (double)last[e] : 0.0;
+        p[8] = have[e] ? (double)dmax[e] : -1.0;  // -1 marks an empty span
+      }
+    }
+  }
+}
+
+// Groups of kFinLanes lanes take the active entries of all jobs in act_start order (grid-stride;
+// the loop bound is block-uniform so every warp stays converged for its shuffles and ballots).
+__global__ void __launch_bounds__(256) k_batch_finalize(BatchFinalArgs A) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *A.work_reset = 0;
+  const int64_t total = A.plan.act_start[A.njobs];
+  const int spans = *A.plan.spans;
+  const int L = A.level;
+  const int nseg = (A.first && L >= 1) ? 2 : 1;
+  const int lane = threadIdx.x % kFinLanes;
+  const unsigned full = 0xffffffffu;
+  const int lane32 = threadIdx.x & 31;
+  const int64_t per_pass = (int64_t)gridDim.x * blockDim.x / kFinLanes;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x / kFinLanes; base < total; base += per_pass) {
+    const int64_t gidx = base + threadIdx.x / kFinLanes;
+    const bool live = gidx < total;
+    const int j = live ? find_job(A.plan.act_start, A.njobs, gidx) : 0;
+    const DevJob& J = A.jobs[j];
+    const int64_t slot = live ? gidx - A.plan.act_start[j] : 0;
+    const int64_t item = live ? (A.first ? slot : (int64_t)A.act[J.entry_begin + slot]) : 0;
+    const int64_t e = J.entry_begin + item;
+    const double* pbase = A.part + A.plan.part_start[j] + slot * nseg * spans * kFdPartials;
+    auto seg_sum = [&](int g, C3& s, double& dmax) {
+      C3 t = {0, 0, 0, 0, 0, 0};
+      double dm = 0;
+      if (live) {
+        for (int sp = lane; sp < spans; sp += kFinLanes) {
+          const double* p = pbase + (g * spans + sp) * kFdPartials;
+          t.xr += p[0]; t.xi += p[1]; t.yr += p[2]; t.yi += p[3]; t.zr += p[4]; t.zi += p[5];
+          if (p[8] >= 0) {  // non-empty span (empty spans only trail the segment)
+            dm = fmax(dm, p[8]);
+            if (sp > 0) dm = fmax(dm, fabs(p[6] - p[-kFdPartials + 7]));
+          }
+        }
+      }
+      s.xr += group_sum(t.xr); s.xi += group_sum(t.xi); s.yr += group_sum(t.yr);
+      s.yi += group_sum(t.yi); s.zr += group_sum(t.zr); s.zi += group_sum(t.zi);
+      dmax = fmax(dmax, group_max(dm));
+    };
+    auto mag = [&](C3 v, double scale) {
+      C3 t = c3_scale(v, scale);
+      if (A.project) t = c3_project(t, J.pol);
+      return c3_mag2(t);
+    };
+    const double T = J.tstop - J.tstart;
+    C3 S = {0, 0, 0, 0, 0, 0};
+    double last_mag = -1, dmax = 0;
+    if (A.first) {
+      double unused = 0;
+      if (nseg == 2) {
+        seg_sum(0, S, unused);
+        last_mag = mag(S, T / (ldexp(1.0, L) - 1));  // DeltaT inclusive to level L-1
+      }
+      seg_sum(nseg - 1, S, dmax);
+    } else {
+      if (live) {
+        const int64_t N = A.n_entries;
+        S = {A.state[e], A.state[N + e], A.state[2 * N + e], A.state[3 * N + e], A.state[4 * N + e],
+             A.state[5 * N + e]};
+        last_mag = A.state[6 * N + e];
+      }
+      seg_sum(0, S, dmax);
+    }
+    bool finished = false, unconverged = false, survive = false;
+    if (live && lane == 0) {
+      const double dtl = T / (ldexp(1.0, L + 1) - 1);  // DeltaT inclusive to level L
+      const double this_mag = mag(S, dtl);
+      const double prec = fabs(this_mag - last_mag) / last_mag;
+      const bool stop = (L > 8 && prec < A.precision && dmax < kPiD) || (L > 8 && dmax < kPiD && this_mag == last_mag);
+      if (stop || L >= A.max_level) {
+        const int result_level = stop ? L : -1;
+        double v;
+        if (A.quantity == 1) v = prec;
+        else if (A.quantity == 2) v = (double)result_level;
+        else v = J.c2 * mag(S, J.c0 * dtl);
+        A.out[e] = v;
+        if (A.level_out) A.level_out[e] = result_level;
+        finished = true;
+        unconverged = !stop;
+      } else {
+        const int64_t N = A.n_entries;
+        A.state[e] = S.xr; A.state[N + e] = S.xi; A.state[2 * N + e] = S.yr;
+        A.state[3 * N + e] = S.yi; A.state[4 * N + e] = S.zr; A.state[5 * N + e] = S.zi;
+        A.state[6 * N + e] = this_mag;
+        survive = true;
+      }
+    }
+    const unsigned fin = __ballot_sync(full, finished), unc = __ballot_sync(full, unconverged);
+    if (lane32 == 0) {
+      if (fin) atomicAdd(A.samples, (unsigned long long)__popc(fin) * (unsigned long long)((2ll << L) - 1));
+      if (unc) atomicAdd(A.not_converged, (unsigned long long)__popc(unc));
+    }
+    // survivors join their job's next list; one atomic per (warp, job)
+    const unsigned sur_all = __ballot_sync(full, survive);
+    const unsigned peers = __match_any_sync(full, survive ? j : -1) & sur_all;
+    const int leader = survive ? __ffs(peers) - 1 : lane32;
+    unsigned pos = 0;
+    if (survive && lane32 == leader) pos = atomicAdd(&A.cnt_next[j], (unsigned)__popc(peers));
+    pos = __shfl_sync(full, pos, leader);
+    if (survive) A.act_next[J.entry_begin + pos + __popc(peers & ((1u << lane32) - 1u))] = (int)item;
+  }
+}
+
+// acc[m] += weight x value of entry m of every job of the chunk, in job order, compensated
+// (T3DScalarContainer::AddToPoint over particles).
+__global__ void k_batch_average(const double* __restrict__ vals, const DevJob* __restrict__ jobs, int njobs,
+                                int64_t m_count, double weight, double* __restrict__ acc, double* __restrict__ comp) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= m_count) return;
+  double S = acc[m], c = comp[m];
+  for (int j = 0; j < njobs; ++j) {
+    const double v = __dmul_rn(vals[jobs[j].entry_begin + m], weight);
+    const double y = __dsub_rn(v, c);
+    const double t = __dadd_rn(S, y);
+    c = __dsub_rn(__dsub_rn(t, S), y);
+    S = t;
+  }
+  acc[m] = S;
+  comp[m] = c;
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------------------------
+// Variants of the batched wave kernel: (entries per thread, minimum resident CTAs per SM).
+// ---------------------------------------------------------------------------------------------
+static const int kBatchEpt[kBatchVariants] = {1, 1, 2, 2, 2, 4, 4};
+
+template <int EPT, int MINB>
+static int batch_occ() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_batch_wave<EPT, MINB>, dev::kBThreads, 0);
+  return n > 0 ? n : 1;
+}
+
+static int batch_blocks_per_sm(int variant) {
+  switch (variant) {
+    case 0: return batch_occ<1, 1>();
+    case 1: return batch_occ<1, 8>();
+    case 2: return batch_occ<2, 1>();
+    case 3: return batch_occ<2, 5>();
+    case 4: return batch_occ<2, 6>();
+    case 5: return batch_occ<4, 1>();
+    default: return batch_occ<4, 3>();
+  }
+}
+
+static cudaError_t launch_batch_wave(const BatchWaveArgs& a, int grid, int variant, cudaStream_t st) {
+  const int T = dev::kBThreads;
+  switch (variant) {
+    case 0: dev::k_batch_wave<1, 1><<<grid, T, 0, st>>>(a); break;
+    case 1: dev::k_batch_wave<1, 8><<<grid, T, 0, st>>>(a); break;
+    case 2: dev::k_batch_wave<2, 1><<<grid, T, 0, st>>>(a); break;
+    case 3: dev::k_batch_wave<2, 5><<<grid, T, 0, st>>>(a); break;
+    case 4: dev::k_batch_wave<2, 6><<<grid, T, 0, st>>>(a); break;
+    case 5: dev::k_batch_wave<4, 1><<<grid, T, 0, st>>>(a); break;
+    default: dev::k_batch_wave<4, 3><<<grid, T, 0, st>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host orchestration
+// ---------------------------------------------------------------------------------------------
+namespace {
+constexpr int kBatchPrefill = 13;        // levels enqueued without the host (records kept resident)
+constexpr int kBatchMinSpan = 32;
+constexpr int kBatchMaxJobsPerChunk = 4096;
+
+DevField to_dev_field(FieldSpec f) {
+  f.finish();
+  DevField d;
+  std::memset(&d, 0, sizeof d);
+  d.kind = f.kind;
+  d.nperiods = f.nperiods;
+  const Vec3 a = f.a, b = f.b, c = f.center, u = f.period_unit;
+  d.a[0] = a.x; d.a[1] = a.y; d.a[2] = a.z;
+  d.b[0] = b.x; d.b[1] = b.y; d.b[2] = b.z;
+  d.center[0] = c.x; d.center[1] = c.y; d.center[2] = c.z;
+  d.period_unit[0] = u.x; d.period_unit[1] = u.y; d.period_unit[2] = u.z;
+  d.phase = f.phase; d.taper = f.taper; d.frequency = f.frequency; d.frequency_phase = f.frequency_phase;
+  d.time_offset = f.time_offset; d.period_length = f.period_length; d.period_mag = mag(f.period);
+  d.length = f.length;
+  return d;
+}
+}  // namespace
+
+int Engine::batch_resident(int v) {
+  if (wave_grid_[3][v] == 0) {
+    int sms = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
+    wave_grid_[3][v] = sms * batch_blocks_per_sm(v);
+  }
+  return wave_grid_[3][v];
+}
+
+void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
+                   int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
+                   bool average, double* out, int32_t* level_out) {
+  pending_.clear();
+  last_samples = last_launches = last_not_converged = 0;
+  if (jobs.empty()) return;
+  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
+  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
+  if (lstop > kMaxLevelMemory)
+    throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
+  if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
+  const int Lfirst = std::min(9, lstop);
+  const int Lpre = std::min(lstop, std::max(Lfirst, kBatchPrefill));
+  double pol[6];
+  bool project = false;
+  polarization_vector(o, pol, project);
+
+  // ---- job descriptors, validated like Model::compute_trajectory ----
+  std::vector<DevJob> dj(jobs.size());
+  const int64_t m_avg = average ? jobs[0].n_obs * jobs[0].n_e : 0;
+  for (size_t k = 0; k < jobs.size(); ++k) {
+    const BatchJob& S = jobs[k];
+    const Particle& P = S.particle;
+    if (S.field_begin < 0 || S.field_count < 0 || (size_t)S.field_begin + S.field_count > fields.size())
+      throw Error{OSC_ERR_RANGE, "job field range outside the field array"};
+    if (S.obs_begin < 0 || S.n_obs < 1 || S.obs_begin + S.n_obs > n_obs_total)
+      throw Error{OSC_ERR_RANGE, "job observer range outside the observer array"};
+    if (S.omega_begin < 0 || S.n_e < 1 || S.omega_begin + S.n_e > n_omega_total)
+      throw Error{OSC_ERR_RANGE, "job energy range outside the energy array"};
+    if (S.n_obs * S.n_e > 2147483647ll) throw Error{OSC_ERR_LENGTH, "more than 2^31-1 entries in one job"};
+    if (average && (S.obs_begin != jobs[0].obs_begin || S.n_obs != jobs[0].n_obs ||
+                    S.omega_begin != jobs[0].omega_begin || S.n_e != jobs[0].n_e))
+      throw Error{OSC_ERR_INVALID, "averaged jobs must share their observers and energies"};
+    if (!P.set) throw Error{OSC_ERR_RANGE, "particle not initialized.  make sure you have a particle or beam defined"};
+    if (S.ctstart > P.t0 || S.ctstop < P.t0)
+      throw Error{OSC_ERR_RANGE, "start time is greater than T0 or stop time is less than T0"};
+    if (S.ctstart >= S.ctstop)
+      throw Error{OSC_ERR_RANGE, "start time is greater than stop time.  check that set_ctstartstop is set"};
+    if (S.npoints < 2) throw Error{OSC_ERR_LENGTH, "Not enough points in this trajectory"};
+    const double dt = ((S.ctstop - S.ctstart) / kC / (S.npoints - 1));
+    const int64_t nf = (int64_t)(1 + (S.ctstop - P.t0) / kC / dt);
+    const int64_t nb = (int64_t)((P.t0 - S.ctstart) / kC / dt);
+    if (nf + nb < 3)
+      throw Error{OSC_ERR_LENGTH, "TSpline1D3 does not see enough points for interpolation.  Please use >= 3 points"};
+    if (nf + nb > 2147483647ll) throw Error{OSC_ERR_LENGTH, "trajectory too long"};
+    DevJob& d = dj[k];
+    std::memset(&d, 0, sizeof d);
+    const Vec3 e3 = unit(P.b0);
+    const Vec3 e1 = unit(orthogonal(e3));
+    const Vec3 e2 = cross(e3, e1);
+    const Vec3 rows[3] = {e1, e2, e3};
+    for (int r = 0; r < 3; ++r) {
+      d.frame.rot[3 * r] = rows[r].x;
+      d.frame.rot[3 * r + 1] = rows[r].y;
+      d.frame.rot[3 * r + 2] = rows[r].z;
+    }
+    d.frame.x0[0] = P.x0.x; d.frame.x0[1] = P.x0.y; d.frame.x0[2] = P.x0.z;
+    d.frame.t_ref = P.t0 / kC;
+    d.b0[0] = P.b0.x; d.b0[1] = P.b0.y; d.b0[2] = P.b0.z;
+    d.qomg = P.qomg;
+    d.dt = dt;
+    d.tstart = P.t0 / kC + (-dt) * (double)nb;
+    d.tstop = P.t0 / kC + dt * (double)(nf - 1);
+    d.c0 = P.q / (four_pi() * kC * kEps0 * kSqrt2Pi);                                           // :4106
+    const double cur = S.current_abs ? std::fabs(P.current) : P.current;
+    d.c2 = four_pi() * cur / (kH * std::fabs(P.q) * kMu0 * kC) * 1e-6 * 0.001;                  // :4109
+    for (int ri = 0; ri < 2; ++ri)  // P' = R P in the job frame (R orthogonal: E'.P' = E.P)
+      for (int r = 0; r < 3; ++r)
+        d.pol[2 * r + ri] = d.frame.rot[3 * r] * pol[ri] + d.frame.rot[3 * r + 1] * pol[2 + ri] +
+                            d.frame.rot[3 * r + 2] * pol[4 + ri];
+    d.nf = (int)nf;
+    d.nb = (int)nb;
+    d.field_begin = S.field_begin;
+    d.field_count = S.field_count;
+    d.obs_begin = S.obs_begin; d.omega_begin = S.omega_begin; d.n_obs = S.n_obs; d.n_e = S.n_e;
+  }
+
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  check(cudaSetDevice(device), "cudaSetDevice");
+  cudaStream_t st = stream;
+  std::vector<DevField> df;
+  for (const FieldSpec& f : fields) df.push_back(to_dev_field(f));
+  if (df.empty()) df.push_back(DevField{});
+  b_fields_.reserve(sizeof(DevField) * df.size());
+  b_obs_.reserve(sizeof(double) * 3 * n_obs_total);
+  b_omega_.reserve(sizeof(double) * n_omega_total);
+  // stream-ordered copies (pageable sources are staged before the calls return)
+  check(cudaMemcpyAsync(b_fields_.p, df.data(), sizeof(DevField) * df.size(), cudaMemcpyHostToDevice, st), "fields");
+  check(cudaMemcpyAsync(b_obs_.p, obs, sizeof(double) * 3 * n_obs_total, cudaMemcpyHostToDevice, st), "observers");
+  check(cudaMemcpyAsync(b_omega_.p, omega, sizeof(double) * n_omega_total, cudaMemcpyHostToDevice, st), "energies");
+  if (average) {
+    b_acc_.reserve(sizeof(double) * 2 * m_avg);
+    check(cudaMemsetAsync(b_acc_.p, 0, sizeof(double) * 2 * m_avg, st), "memset");
+  }
+
+  int sms = 0;
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
+  int max_resident = 0, max_tile = 0;
+  for (int v = 0; v < kBatchVariants; ++v) {
+    max_resident = std::max(max_resident, batch_resident(v));
+    max_tile = std::max(max_tile, dev::kBThreads * kBatchEpt[v]);
+  }
+  const int64_t target = 4 * (int64_t)max_resident;  // >= 4 units per resident CTA when work allows
+
+  // ---- chunks of jobs sized to the free device memory ----
+  size_t free_b = 0, total_b = 0;
+  check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  const size_t budget = std::min<size_t>(free_b / 2, (size_t)64 << 30);
+  const int64_t rec_per_job = (int64_t)2 << Lpre;  // levels 0..Lpre, sample s at index s
+  size_t done_entries = 0;
+  size_t j0 = 0;
+  while (j0 < dj.size()) {
+    size_t j1 = j0, bytes = 0;
+    while (j1 < dj.size() && j1 - j0 < (size_t)kBatchMaxJobsPerChunk) {
+      const DevJob& d = dj[j1];
+      const size_t need = sizeof(double) * 28 * ((size_t)d.nf + d.nb) + 48 * (size_t)rec_per_job +
+                          (size_t)(d.n_obs * d.n_e) * (56 + 8 + 4 + 8 + 16 * kFdPartials);
+      if (j1 > j0 && bytes + need > budget) break;
+      bytes += need;
+      ++j1;
+    }
+    const int nj = (int)(j1 - j0);
+    int64_t knots = 0, work = 0, N = 0;
+    for (int k = 0; k < nj; ++k) {
+      DevJob& d = dj[j0 + k];
+      const int64_t n = (int64_t)d.nf + d.nb;
+      d.knots = knots;
+      knots += 19 * n;
+      d.u_off = work;
+      work += 9 * n;
+      d.entry_begin = N;
+      N += d.n_obs * d.n_e;
+    }
+    // partial sums: spans = 1 gives 2 segments x N entries; a wave split into more spans has fewer
+    // than 2 x target units of at most max_tile entries each (wave_spans)
+    const size_t part_doubles = (size_t)std::max<int64_t>(2 * N, 4 * target * max_tile) * kFdPartials;
+    b_jobs_.reserve(sizeof(DevJob) * nj);
+    b_knots_.reserve(sizeof(double) * knots);
+    b_work_.reserve(sizeof(double) * work);
+    b_rec_.reserve(sizeof(float4) * 3 * rec_per_job * nj);
+    b_state_.reserve(sizeof(double) * 7 * N);
+    b_out_.reserve(sizeof(double) * N);
+    b_lvl_.reserve(sizeof(int32_t) * N);
+    b_act_[0].reserve(sizeof(int) * N);
+    b_act_[1].reserve(sizeof(int) * N);
+    b_part_.reserve(sizeof(double) * part_doubles);
+    b_plan_.reserve(sizeof(int64_t) * 3 * (nj + 1) + 64);
+    b_cnt_.reserve(sizeof(unsigned) * 2 * nj + 256);
+    check(cudaMemcpyAsync(b_jobs_.p, dj.data() + j0, sizeof(DevJob) * nj, cudaMemcpyHostToDevice, st), "jobs");
+    DevJob* d_jobs = b_jobs_.as<DevJob>();
+    unsigned* cnt0 = b_cnt_.as<unsigned>();
+    unsigned* cnts[2] = {cnt0, cnt0 + nj};
+    // after the two count arrays: [0] error word, [2..] 3 x u64 (not converged, samples, unit counter)
+    unsigned* misc = cnt0 + ((2 * nj + 7) & ~7);
+    unsigned long long* m64 = reinterpret_cast<unsigned long long*>(misc + 2);
+    BatchPlan plan;
+    plan.unit_start = b_plan_.as<int64_t>();
+    plan.part_start = plan.unit_start + (nj + 1);
+    plan.act_start = plan.part_start + (nj + 1);
+    plan.spans = reinterpret_cast<int*>(plan.act_start + (nj + 1));
+
+    int cur = 0;  // active list / count array of the next wave
+    auto wave = [&](int L, int v, int64_t stride, int64_t s_off, const float4* rec) {
+      const bool first = L == Lfirst;
+      unsigned* cin = cnts[cur];
+      unsigned* cout = cnts[cur ^ 1];
+      check(cudaMemsetAsync(cout, 0, sizeof(unsigned) * nj, st), "memset");
+      const int tile = dev::kBThreads * kBatchEpt[v];
+      dev::k_batch_plan<<<1, 1024, 0, st>>>(d_jobs, nj, cin, first, L, tile, target, kBatchMinSpan, plan);
+      BatchWaveArgs w{};
+      w.jobs = d_jobs; w.njobs = nj; w.rec = rec; w.stride = stride; w.s_off = s_off;
+      w.obs = b_obs_.as<double>(); w.omega = b_omega_.as<double>(); w.act = b_act_[cur].as<int>(); w.cnt = cin;
+      w.plan = plan; w.first = first; w.level = L; w.part = b_part_.as<double>(); w.err = misc; w.work = m64 + 2;
+      check(launch_batch_wave(w, batch_resident(v), v, st), "batch wave");
+      BatchFinalArgs f{};
+      f.jobs = d_jobs; f.njobs = nj; f.act = w.act; f.cnt = cin; f.plan = plan; f.part = w.part;
+      f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity; f.project = project;
+      f.precision = o.precision; f.n_entries = N; f.state = b_state_.as<double>();
+      f.act_next = b_act_[cur ^ 1].as<int>(); f.cnt_next = cout; f.out = b_out_.as<double>();
+      f.level_out = b_lvl_.as<int32_t>(); f.not_converged = m64; f.samples = m64 + 1; f.work_reset = m64 + 2;
+      dev::k_batch_finalize<<<sms * 8, 256, 0, st>>>(f);
+      check(cudaGetLastError(), "batch finalize");
+      last_launches += 3;
+      cur ^= 1;
+    };
+    // trajectories, splines, the resident levels' records and the waves up to Lpre: no host sync
+    auto front = [&](int v, bool tune) {
+      check(cudaMemsetAsync(misc, 0, 64, st), "memset");
+      dev::k_batch_rk4<<<(2 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_fields_.as<DevField>(),
+                                                          b_knots_.as<double>(), misc);
+      dev::k_batch_extent<<<nj, 256, 0, st>>>(d_jobs, b_knots_.as<double>());
+      dev::k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_knots_.as<double>(), b_work_.as<double>());
+      const int64_t fill_n = (rec_per_job - 1) * nj;
+      dev::k_batch_fill<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(
+          d_jobs, nj, b_knots_.as<double>(), nullptr, b_rec_.as<float4>(), rec_per_job, 0, 1, rec_per_job);
+      check(cudaGetLastError(), "batch trajectories");
+      last_launches += 4;
+      if (tune) v = tune_batch(nj, Lfirst, target, d_jobs, plan, misc, m64, rec_per_job);
+      for (int L = Lfirst; L <= Lpre; ++L) wave(L, v, rec_per_job, 0, b_rec_.as<float4>());
+      return v;
+    };
+    // a new shape is tuned and run eagerly; a known shape is captured and replayed as a graph
+    const auto key = std::make_tuple(nj, N, Lfirst, Lpre);
+    int v = forced_variant[3] >= 0 ? forced_variant[3] : current_variant_[3];
+    const bool need_tune = forced_variant[3] < 0 && autotune && tuned_batch_.find(key) == tuned_batch_.end();
+    if (forced_variant[3] < 0 && autotune && !need_tune) v = tuned_batch_[key];
+    if (need_tune || !use_graphs) {
+      v = front(v, need_tune);
+      if (need_tune) {
+        tuned_batch_[key] = v;
+        current_variant_[3] = v;
+      }
+    } else {
+      cudaGraph_t g = nullptr;
+      check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
+      try {
+        front(v, false);
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+      }
+      check(cudaStreamEndCapture(st, &g), "capture");
+      bool updated = false;
+      if (graph_exec_) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(graph_exec_, g, &info) == cudaSuccess;
+        if (!updated) {
+          cudaGetLastError();
+          cudaGraphExecDestroy(graph_exec_);
+          graph_exec_ = nullptr;
+        }
+      }
+      if (!updated) {
+        const cudaError_t e = cudaGraphInstantiate(&graph_exec_, g, 0);
+        if (e != cudaSuccess) {
+          cudaGraphDestroy(g);
+          graph_exec_ = nullptr;
+          check(e, "graph instantiate");
+        }
+      }
+      cudaGraphDestroy(g);
+      check(cudaGraphLaunch(graph_exec_, st), "graph launch");
+      ++graph_launches_;
+    }
+    // levels beyond the resident ones: records of one level at a time, for the jobs still active
+    for (int L = Lpre + 1; L <= lstop; ++L) {
+      std::vector<unsigned> c(nj);
+      check(cudaMemcpyAsync(c.data(), cnts[cur], sizeof(unsigned) * nj, cudaMemcpyDeviceToHost, st), "counts");
+      check(cudaStreamSynchronize(st), "counts");
+      bool any = false;
+      for (unsigned x : c) any = any || x > 0;
+      if (!any) break;
+      const int64_t len = (int64_t)1 << L;
+      b_rec_ext_.reserve(sizeof(float4) * 3 * len * nj);
+      const int64_t fill_n = len * nj;
+      dev::k_batch_fill<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(
+          d_jobs, nj, b_knots_.as<double>(), cnts[cur], b_rec_ext_.as<float4>(), len, len, len, 2 * len);
+      check(cudaGetLastError(), "batch fill");
+      ++last_launches;
+      wave(L, v, len, len, b_rec_ext_.as<float4>());
+    }
+    // results of the chunk
+    if (average) {
+      dev::k_batch_average<<<(unsigned)((m_avg + 255) / 256), 256, 0, st>>>(
+          b_out_.as<double>(), d_jobs, nj, m_avg, 1.0 / (double)jobs.size(), b_acc_.as<double>(),
+          b_acc_.as<double>() + m_avg);
+      check(cudaGetLastError(), "batch average");
+      ++last_launches;
+      if (level_out && j1 == dj.size())  // levels of the last particle, as the reference leaves them
+        check(cudaMemcpyAsync(level_out, b_lvl_.as<int32_t>() + dj[j1 - 1].entry_begin, sizeof(int32_t) * m_avg,
+                              cudaMemcpyDeviceToHost, st), "levels");
+    } else {
+      check(cudaMemcpyAsync(out + done_entries, b_out_.p, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
+      if (level_out)
+        check(cudaMemcpyAsync(level_out + done_entries, b_lvl_.p, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st),
+              "download");
+    }
+    unsigned long long h64[2] = {0, 0};
+    unsigned err = 0;
+    check(cudaMemcpyAsync(h64, m64, sizeof h64, cudaMemcpyDeviceToHost, st), "stats");
+    check(cudaMemcpyAsync(&err, misc, sizeof err, cudaMemcpyDeviceToHost, st), "stats");
+    check(cudaStreamSynchronize(st), "batch");
+    if (err & dev::kErrTmaTimeout)
+      throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+    if (err & dev::kErrSuperluminal)
+      throw Error{OSC_ERR_RANGE, "a trajectory reached the speed of light (check the fields)"};
+    if (err & dev::kErrBadArgs)
+      throw Error{OSC_ERR_INVALID, "compute='mixed' needs observers near the beam axis (angle < 1e-2 and a correction "
+                                   "phase below 3e4 rad); use compute='fp64' for this geometry"};
+    last_not_converged += (long long)h64[0];
+    last_samples += (long long)h64[1];
+    if (profiling) prof_samples += (long long)h64[1];
+    done_entries += (size_t)N;
+    j0 = j1;
+  }
+  if (average) {
+    check(cudaMemcpyAsync(out, b_acc_.p, sizeof(double) * m_avg, cudaMemcpyDeviceToHost, st), "download");
+    check(cudaStreamSynchronize(st), "download");
+  }
+}
+
+// Autotuner of the batched wave: times the first wave of the chunk with every compiled variant
+// (each run rewrites only the partial sums, so the runs are interchangeable) and keeps the fastest.
+int Engine::tune_batch(int nj, int Lfirst, int64_t target, const DevJob* d_jobs, const BatchPlan& plan,
+                       unsigned* misc, unsigned long long* m64, int64_t rec_stride) {
+  cudaStream_t st = stream;
+  cudaEvent_t a, b;
+  check(cudaEventCreate(&a), "event");
+  check(cudaEventCreate(&b), "event");
+  int best = current_variant_[3];
+  float best_ms = 1e30f;
+  for (int v = 0; v < kBatchVariants; ++v) {
+    const int tile = dev::kBThreads * kBatchEpt[v];
+    dev::k_batch_plan<<<1, 1024, 0, st>>>(d_jobs, nj, nullptr, 1, Lfirst, tile, target, kBatchMinSpan, plan);
+    BatchWaveArgs w{};
+    w.jobs = d_jobs; w.njobs = nj; w.rec = b_rec_.as<float4>(); w.stride = rec_stride; w.s_off = 0;
+    w.obs = b_obs_.as<double>(); w.omega = b_omega_.as<double>(); w.act = nullptr; w.cnt = nullptr;
+    w.plan = plan; w.first = 1; w.level = Lfirst; w.part = b_part_.as<double>(); w.err = misc; w.work = m64 + 2;
+    float ms_v = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      check(cudaMemsetAsync(m64 + 2, 0, sizeof(unsigned long long), st), "memset");
+      check(cudaEventRecord(a, st), "event");
+      check(launch_batch_wave(w, batch_resident(v), v, st), "batch wave");
+      check(cudaEventRecord(b, st), "event");
+      check(cudaEventSynchronize(b), "event");
+      float ms = 0;
+      check(cudaEventElapsedTime(&ms, a, b), "event");
+      ms_v = std::min(ms_v, ms);
+    }
+    if (ms_v < best_ms) {
+      best_ms = ms_v;
+      best = v;
+    }
+  }
+  check(cudaMemsetAsync(m64 + 2, 0, sizeof(unsigned long long), st), "memset");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
+}  // namespace osc

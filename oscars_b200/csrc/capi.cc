@@ -141,24 +141,26 @@ OSC_API int osc_clear_fields(osc_ctx* ctx) {
   return guarded(ctx, [&] { ctx->eng->model.clear_fields(); });
 }
 
+osc::FieldSpec field_from_desc(const osc_field_desc* f) {
+  if (!f) throw osc::Error{OSC_ERR_INVALID, "field descriptor is NULL"};
+  if (f->kind != OSC_FIELD_UNDULATOR && f->kind != OSC_FIELD_EPU) throw osc::Error{OSC_ERR_INVALID, "unknown field kind"};
+  osc::FieldSpec s;
+  s.kind = f->kind;
+  s.a = V3(f->bfield);
+  s.b = V3(f->bfield_b);
+  s.period = V3(f->period);
+  s.nperiods = f->nperiods;
+  s.center = V3(f->center);
+  s.phase = f->phase;
+  s.taper = f->taper;
+  s.frequency = f->frequency;
+  s.frequency_phase = f->frequency_phase;
+  s.time_offset = f->time_offset;
+  return s;
+}
+
 OSC_API int osc_add_field(osc_ctx* ctx, const osc_field_desc* f) {
-  return guarded(ctx, [&] {
-    if (!f) throw osc::Error{OSC_ERR_INVALID, "field descriptor is NULL"};
-    if (f->kind != OSC_FIELD_UNDULATOR && f->kind != OSC_FIELD_EPU) throw osc::Error{OSC_ERR_INVALID, "unknown field kind"};
-    osc::FieldSpec s;
-    s.kind = f->kind;
-    s.a = V3(f->bfield);
-    s.b = V3(f->bfield_b);
-    s.period = V3(f->period);
-    s.nperiods = f->nperiods;
-    s.center = V3(f->center);
-    s.phase = f->phase;
-    s.taper = f->taper;
-    s.frequency = f->frequency;
-    s.frequency_phase = f->frequency_phase;
-    s.time_offset = f->time_offset;
-    ctx->eng->model.add_field(s);
-  });
+  return guarded(ctx, [&] { ctx->eng->model.add_field(field_from_desc(f)); });
 }
 
 OSC_API int osc_get_bfield(osc_ctx* ctx, const double x[3], double t, double out[3]) {
@@ -337,6 +339,69 @@ OSC_API int osc_spectrum(osc_ctx* ctx, const double obs[3], const double* energi
   });
 }
 
+// A batch of independent jobs (no reference counterpart: the reference runs one particle and one
+// field container per call).  Mixed precision runs all jobs in shared launches; FP64 runs them one
+// after another through the single-trajectory path.
+OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fields, const osc_job_desc* jobs,
+                           int n_jobs, const double* obs_xyz, long long n_obs, const double* energies_eV,
+                           long long n_energies, const osc_rad_opts* opts, int average, double* out,
+                           int32_t* level_out, long long* n_not_converged) {
+  return guarded(ctx, [&] {
+    using namespace osc;
+    check_opts(opts);
+    if (opts->nparticles != 0) throw Error{OSC_ERR_INVALID, "batch jobs are single particles: nparticles must be 0"};
+    if (n_fields < 0 || n_jobs < 0 || n_obs < 0 || n_energies < 0) throw Error{OSC_ERR_INVALID, "negative count"};
+    if ((n_fields > 0 && !fields) || (n_jobs > 0 && (!jobs || !out)) || (n_obs > 0 && !obs_xyz) ||
+        (n_energies > 0 && !energies_eV))
+      throw Error{OSC_ERR_INVALID, "bad buffers"};
+    std::vector<FieldSpec> fs;
+    for (int i = 0; i < n_fields; ++i) {
+      FieldSpec f = field_from_desc(fields + i);
+      f.finish();
+      fs.push_back(f);
+    }
+    std::vector<double> omega(n_energies);
+    for (long long i = 0; i < n_energies; ++i) omega[i] = ev_to_omega(energies_eV[i]);
+    std::vector<BatchJob> bj(n_jobs);
+    for (int k = 0; k < n_jobs; ++k) {
+      const osc_job_desc& d = jobs[k];
+      BatchJob& J = bj[k];
+      double q = 0, m = 0;
+      if (particle_qm(d.particle, d.charge, d.mass, q, m)) throw Error{OSC_ERR_INVALID, "unknown particle type"};
+      if (d.particle == OSC_PARTICLE_CUSTOM && (d.mass == 0 || d.charge == 0))
+        throw Error{OSC_ERR_INVALID, "'mass' or 'charge' is zero"};
+      if (d.energy_GeV < 0) throw Error{OSC_ERR_INVALID, "job energy_GeV must be >= 0"};
+      // the ideal particle of a beam with this energy and direction (TParticleBeam::GetNewParticle)
+      const Vec3 dir = V3(d.d0);
+      const Vec3 u0 = mag2(dir) > 0 ? unit(dir) : Vec3{};
+      const double e0 = d.energy_GeV < kg_to_gev(m) ? m : d.energy_GeV;
+      const double g = e0 / kg_to_gev(m) < 1 ? 1 : e0 / kg_to_gev(m);
+      const double b = g != 1 ? std::sqrt(1.0 - 1.0 / (g * g)) : 0;
+      J.particle.q = q;
+      J.particle.m = m;
+      J.particle.current = d.current != 0 ? d.current : q;
+      J.particle.set_conditions(V3(d.x0), u0 * b, d.t0);
+      J.field_begin = d.field_begin;
+      J.field_count = d.field_count;
+      J.ctstart = d.ctstart;
+      J.ctstop = d.ctstop;
+      J.npoints = d.npoints;
+      J.obs_begin = d.obs_begin;
+      J.n_obs = d.n_obs;
+      J.omega_begin = d.energy_begin;
+      J.n_e = d.n_energies;
+      J.current_abs = d.spectrum != 0;
+    }
+    Engine& E = *ctx->eng;
+    if (opts->precision_mode == OSC_MIXED) {
+      E.batch(fs, bj, obs_xyz, n_obs, omega.data(), n_energies, *opts, average != 0, out, level_out);
+    } else {
+      E.batch_fp64(fs, bj, obs_xyz, n_obs, omega.data(), n_energies, *opts, average != 0, out, level_out);
+    }
+    if (n_not_converged) *n_not_converged = E.last_not_converged;
+  });
+}
+
 OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double* normals, long long n_obs,
                               int directional, const osc_rad_opts* opts, double* out, int32_t* level_out,
                               long long* n_not_converged) {
@@ -421,20 +486,25 @@ OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches
   });
 }
 
+static int n_variants_of(int kind) {
+  return kind == 3 ? osc::kBatchVariants : kind == 2 ? osc::kMixedVariants : osc::kFp64Variants;
+}
+
 OSC_API int osc_set_variant(osc_ctx* ctx, int kind, int variant) {
   return guarded(ctx, [&] {
-    if (kind != 0 && kind != 2) throw osc::Error{OSC_ERR_INVALID, "kind must be 0 (fp64) or 2 (mixed)"};
-    const int n = kind == 2 ? osc::kMixedVariants : osc::kFp64Variants;
-    if (variant < -1 || variant >= n) throw osc::Error{OSC_ERR_RANGE, "variant out of range"};
+    if (kind != 0 && kind != 2 && kind != 3)
+      throw osc::Error{OSC_ERR_INVALID, "kind must be 0 (fp64), 2 (mixed) or 3 (batched mixed)"};
+    if (variant < -1 || variant >= n_variants_of(kind)) throw osc::Error{OSC_ERR_RANGE, "variant out of range"};
     ctx->eng->forced_variant[kind] = variant;
   });
 }
 
 OSC_API int osc_get_variant(osc_ctx* ctx, int kind, int* variant, int* n_variants) {
   return guarded(ctx, [&] {
-    if (kind != 0 && kind != 2) throw osc::Error{OSC_ERR_INVALID, "kind must be 0 (fp64) or 2 (mixed)"};
+    if (kind != 0 && kind != 2 && kind != 3)
+      throw osc::Error{OSC_ERR_INVALID, "kind must be 0 (fp64), 2 (mixed) or 3 (batched mixed)"};
     if (variant) *variant = ctx->eng->variant_in_use(kind);
-    if (n_variants) *n_variants = kind == 2 ? osc::kMixedVariants : osc::kFp64Variants;
+    if (n_variants) *n_variants = n_variants_of(kind);
   });
 }
 

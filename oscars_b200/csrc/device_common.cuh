@@ -14,7 +14,7 @@ namespace osc {
 namespace dev {
 
 // Error flags written by kernels (bit mask, OR-ed into a device word read back by the host).
-enum : unsigned { kErrTmaTimeout = 1u, kErrBadArgs = 2u };
+enum : unsigned { kErrTmaTimeout = 1u, kErrBadArgs = 2u, kErrSuperluminal = 4u };
 
 // Polls of an mbarrier before a wait is declared stuck (each poll is a try_wait that itself may
 // suspend the thread for a hardware-defined interval), i.e. far beyond any legitimate latency.

@@ -72,8 +72,11 @@ Engine::~Engine() {
   if (stage_ev_) cudaEventDestroy(stage_ev_);
   if (stats_host_) cudaFreeHost(stats_host_);
   if (stage_host_) cudaFreeHost(stage_host_);
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
-                    &act_[1], &cnt_, &acc_, &acc_comp_})
+                    &act_[1], &cnt_, &acc_, &acc_comp_, &mrec_, &b_fields_, &b_obs_, &b_omega_, &b_acc_, &b_jobs_,
+                    &b_knots_, &b_work_, &b_rec_, &b_rec_ext_, &b_state_, &b_out_, &b_lvl_, &b_act_[0], &b_act_[1],
+                    &b_part_, &b_plan_, &b_cnt_})
     b->release();
   if (stream) cudaStreamDestroy(stream);
 }
@@ -188,12 +191,12 @@ void Engine::ensure_mixed(int L) {
   mrec_filled_ = L;
 }
 
-static double dt_inclusive(double tstart, double tstop, int L) {  // :224-237
+double dt_inclusive(double tstart, double tstop, int L) {  // :224-237
   return (tstop - tstart) / (std::pow(2., L + 1) - 1);
 }
 
 // Polarization vector of src/OSCARSSR.cc:4116-4150 (host double arithmetic, reference order).
-static void polarization_vector(const osc_rad_opts& o, double P[6], bool& project) {
+void polarization_vector(const osc_rad_opts& o, double P[6], bool& project) {
   const Vec3 hor = v3(o.horizontal[0], o.horizontal[1], o.horizontal[2]);
   const Vec3 prop = v3(o.propagation[0], o.propagation[1], o.propagation[2]);
   const Vec3 vert = unit(cross(prop, hor));
@@ -487,6 +490,10 @@ void Engine::radiation(RadRequest& rq) {
   if (!d_lvl) d_lvl = lvl_.as<int32_t>();
 
   const int np = rq.opts.nparticles;
+  if (np > 0 && rq.opts.precision_mode == OSC_MIXED && !rq.power_density) {
+    radiation_beam_mixed(rq, N);
+    return;
+  }
   if (np <= 0) {
     model.ensure_trajectory();
     upload_trajectory();
@@ -518,6 +525,132 @@ void Engine::radiation(RadRequest& rq) {
     check(cudaStreamSynchronize(st), "download");
     collect();
   }
+}
+
+// Multi-particle flux / spectrum in mixed precision: the particles are drawn on the host in the
+// reference's order (src/OSCARSSR.cc:4026-4062) and integrated as one batch whose results are
+// averaged with weight 1/N in particle order.
+void Engine::radiation_beam_mixed(RadRequest& rq, int64_t N) {
+  const int np = rq.opts.nparticles;
+  const int64_t n_e = (int64_t)rq.omega.size();
+  std::vector<double> obs_h;
+  const double* obs = rq.obs;
+  if (rq.obs_on_device) {
+    obs_h.resize(3 * rq.n_obs);
+    check(cudaMemcpy(obs_h.data(), rq.obs, sizeof(double) * 3 * rq.n_obs, cudaMemcpyDeviceToHost), "observers");
+    obs = obs_h.data();
+  }
+  std::vector<BatchJob> jobs(np);
+  for (int ip = 0; ip < np; ++ip) {
+    model.random_particle();
+    BatchJob& J = jobs[ip];
+    J.field_begin = 0;
+    J.field_count = (int)model.fields.size();
+    J.particle = model.particle;
+    J.ctstart = model.ctstart;
+    J.ctstop = model.ctstop;
+    J.npoints = model.npoints;
+    J.obs_begin = 0;
+    J.n_obs = rq.n_obs;
+    J.omega_begin = 0;
+    J.n_e = n_e;
+    J.current_abs = rq.spectrum_current_abs;
+  }
+  // the host trajectory now belongs to an earlier particle: recompute it on demand
+  model.knots.clear();
+  ++model.knots_version;
+  std::vector<double> out_h, lvl_unused;
+  std::vector<int32_t> lvl_h;
+  double* out = rq.out;
+  int32_t* lvl = rq.level_out;
+  if (rq.out_on_device) {
+    out_h.resize(N);
+    lvl_h.resize(N);
+    out = out_h.data();
+    lvl = lvl_h.data();
+  }
+  batch(model.fields, jobs, obs, rq.n_obs, rq.omega.data(), n_e, rq.opts, true, out, lvl);
+  if (rq.out_on_device) {
+    check(cudaMemcpy(rq.out, out_h.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "result");
+    if (rq.level_out)
+      check(cudaMemcpy(rq.level_out, lvl_h.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice), "result");
+  }
+}
+
+void Engine::batch_fp64(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
+                        int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
+                        bool average, double* out, int32_t* level_out) {
+  const int64_t m_avg = jobs.empty() ? 0 : jobs[0].n_obs * jobs[0].n_e;
+  for (const BatchJob& J : jobs) {
+    if (J.field_begin < 0 || J.field_count < 0 || (size_t)J.field_begin + J.field_count > fields.size())
+      throw Error{OSC_ERR_RANGE, "job field range outside the field array"};
+    if (J.obs_begin < 0 || J.n_obs < 1 || J.obs_begin + J.n_obs > n_obs_total)
+      throw Error{OSC_ERR_RANGE, "job observer range outside the observer array"};
+    if (J.omega_begin < 0 || J.n_e < 1 || J.omega_begin + J.n_e > n_omega_total)
+      throw Error{OSC_ERR_RANGE, "job energy range outside the energy array"};
+    if (average && (J.obs_begin != jobs[0].obs_begin || J.n_obs != jobs[0].n_obs ||
+                    J.omega_begin != jobs[0].omega_begin || J.n_e != jobs[0].n_e))
+      throw Error{OSC_ERR_INVALID, "averaged jobs must share their observers and energies"};
+  }
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  // the context's own model is set aside and restored; its trajectory is uploaded again afterwards
+  Model saved = model;
+  long long samples = 0, launches = 0, nnc = 0;
+  std::vector<double> val, acc(average ? m_avg : 0, 0.0), comp(average ? m_avg : 0, 0.0);
+  int64_t done = 0;
+  try {
+    for (size_t k = 0; k < jobs.size(); ++k) {
+      const BatchJob& J = jobs[k];
+      model.fields.assign(fields.begin() + J.field_begin, fields.begin() + J.field_begin + J.field_count);
+      model.particle = J.particle;
+      model.ctstart = J.ctstart;
+      model.ctstop = J.ctstop;
+      model.npoints = J.npoints;
+      model.compute_trajectory();
+      RadRequest rq;
+      rq.obs = obs + 3 * J.obs_begin;
+      rq.n_obs = J.n_obs;
+      rq.omega.assign(omega + J.omega_begin, omega + J.omega_begin + J.n_e);
+      rq.opts = o;
+      rq.opts.nparticles = 0;
+      rq.spectrum_current_abs = J.current_abs;
+      const int64_t m = J.n_obs * J.n_e;
+      if (average) {
+        val.resize(m);
+        rq.out = val.data();
+        rq.level_out = (level_out && k + 1 == jobs.size()) ? level_out : nullptr;
+      } else {
+        rq.out = out + done;
+        rq.level_out = level_out ? level_out + done : nullptr;
+      }
+      radiation(rq);
+      samples += last_samples;
+      launches += last_launches;
+      nnc += last_not_converged;
+      if (average) {  // compensated sum with weight 1/N in job order (T3DScalarContainer::AddToPoint)
+        const double w = 1.0 / (double)jobs.size();
+        for (int64_t i = 0; i < m; ++i) {
+          const double y = val[i] * w - comp[i];
+          const double t = acc[i] + y;
+          comp[i] = (t - acc[i]) - y;
+          acc[i] = t;
+        }
+      }
+      done += m;
+    }
+  } catch (...) {
+    const uint64_t v = model.knots_version;
+    model = saved;
+    model.knots_version = v + 1;
+    throw;
+  }
+  const uint64_t v = model.knots_version;
+  model = saved;
+  model.knots_version = v + 1;  // a version no cached upload has seen
+  if (average) std::copy(acc.begin(), acc.end(), out);
+  last_samples = samples;
+  last_launches = launches;
+  last_not_converged = nnc;
 }
 
 std::pair<cudaEvent_t, cudaEvent_t> Engine::timed_begin(cudaStream_t st) {

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/oscars_b200.h"
+#include "batch.h"
 #include "host_core.h"
 #include "kernels.h"
 
@@ -41,6 +42,21 @@ struct RadRequest {
   cudaStream_t stream = nullptr;
 };
 
+// One job of a batch (host side): a particle with its trajectory range through fields
+// [field_begin, field_begin + field_count) of the batch, observed at observers
+// [obs_begin, obs_begin + n_obs) and energies [omega_begin, omega_begin + n_e) of the batch.
+struct BatchJob {
+  int field_begin = 0, field_count = 0;
+  Particle particle;
+  double ctstart = 0, ctstop = 0;
+  int64_t npoints = 0;
+  int64_t obs_begin = 0, n_obs = 0, omega_begin = 0, n_e = 0;
+  bool current_abs = false;  // spectrum: |I| in the flux constant (src/OSCARSSR.cc:1888)
+};
+
+double dt_inclusive(double tstart, double tstop, int L);
+void polarization_vector(const osc_rad_opts& o, double P[6], bool& project);
+
 class Engine {
  public:
   explicit Engine(int device);
@@ -55,6 +71,19 @@ class Engine {
 
   // Run one radiation request for the current model state (single or multi particle).
   void radiation(RadRequest& rq);
+  // Mixed-precision flux / spectrum of a batch of jobs in shared launches.  `out` (host) receives
+  // every job's entries in job order, or with `average` the mean over the jobs (which must then
+  // share observers and energies); `level_out` (host, optional) the stop levels (of the last job
+  // when averaging).
+  void batch(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
+             int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o, bool average,
+             double* out, int32_t* level_out);
+  // The same jobs one after another through the single-trajectory FP64 path (host RK4).
+  void batch_fp64(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
+                  int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
+                  bool average, double* out, int32_t* level_out);
+  bool use_graphs = true;            // replay the batched front of a known shape as a CUDA graph
+  long long graph_launches() const { return graph_launches_; }
 
   // profiling of the sample-integration kernels
   bool profiling = false;
@@ -93,11 +122,11 @@ class Engine {
   cudaEvent_t stage_ev_ = nullptr;
   int stats_slot_ = 0;
   std::vector<int> pending_;
-  // kernel variants: kind 0 = FP64 flux, 1 = FP64 power density, 2 = mixed flux
-  int wave_grid_[3][8] = {};
+  // kernel variants: kind 0 = FP64 flux, 1 = FP64 power density, 2 = mixed flux, 3 = batched mixed
+  int wave_grid_[4][8] = {};
   int wave_grid(int kind, int variant);
   std::map<std::tuple<int, int, int, int>, int> tuned_;   // (kind, log2 entries, first level, last level) -> variant
-  int current_variant_[3] = {2, 0, 3};
+  int current_variant_[4] = {2, 0, 3, 3};
   int pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out, int32_t* d_lvl,
                    cudaStream_t st);
   bool tuning_ = false;
@@ -113,11 +142,22 @@ class Engine {
   void ensure_mixed(int L);
   void compute_frame();
  public:
-  int forced_variant[3] = {-1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
+  int forced_variant[4] = {-1, -1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
   bool autotune = true;
   int variant_in_use(int kind) const { return forced_variant[kind] >= 0 ? forced_variant[kind] : current_variant_[kind]; }
   std::map<std::tuple<int, int, int, int>, int> tuned() const { return tuned_; }
  private:
+
+  // batched path
+  DevBuf b_fields_, b_obs_, b_omega_, b_acc_, b_jobs_, b_knots_, b_work_, b_rec_, b_rec_ext_, b_state_, b_out_,
+      b_lvl_, b_act_[2], b_part_, b_plan_, b_cnt_;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  long long graph_launches_ = 0;
+  std::map<std::tuple<int, int64_t, int, int>, int> tuned_batch_;  // (jobs, entries, first, prefill level)
+  int batch_resident(int variant);
+  int tune_batch(int nj, int Lfirst, int64_t target, const DevJob* d_jobs, const BatchPlan& plan, unsigned* misc,
+                 unsigned long long* m64, int64_t rec_stride);
+  void radiation_beam_mixed(RadRequest& rq, int64_t N);
 
   void upload_trajectory();
   void ensure_levels(int L);

@@ -20,17 +20,15 @@ struct WavePlan {
   int64_t seg_b[2], seg_e[2], span_len[2];
 };
 
-__host__ __device__ inline WavePlan wave_plan(int first, int L, int64_t n_act, int tile_entries, int64_t target_units,
-                                              int min_span) {
+// Segments of a wave with a given span count (tiles left to the caller).
+__host__ __device__ inline WavePlan wave_plan_spans(int first, int L, int spans) {
   WavePlan p;
   const int64_t lo = (int64_t)1 << L, hi = (int64_t)2 << L;
   p.nseg = (first && L >= 1) ? 2 : 1;
   // segment 0: levels 0..L-1 on the first wave (level 0 alone when L == 0), else level L
   const int64_t b0 = first ? 1 : lo, e0 = first ? (L >= 1 ? lo : 2) : hi;
   const int64_t b1 = lo, e1 = hi;  // segment 1 (first wave with L >= 1): level L
-  p.tiles = (n_act + tile_entries - 1) / tile_entries;
-  int spans = 1;
-  while (p.tiles * spans < target_units && lo / (spans * 2) >= min_span) spans *= 2;
+  p.tiles = 0;
   p.spans = spans;
   const int64_t a0 = b0 & ~(int64_t)1, a1 = b1 & ~(int64_t)1;
   p.seg_b[0] = a0;
@@ -39,6 +37,23 @@ __host__ __device__ inline WavePlan wave_plan(int first, int L, int64_t n_act, i
   p.seg_b[1] = p.nseg == 2 ? a1 : 0;
   p.seg_e[1] = p.nseg == 2 ? e1 : 0;
   p.span_len[1] = p.nseg == 2 ? (((e1 - a1 + spans - 1) / spans + 1) & ~(int64_t)1) : 0;
+  return p;
+}
+
+// Smallest power-of-two span count with tiles x spans >= target_units, keeping spans of at least
+// min_span samples of level L.
+__host__ __device__ inline int wave_spans(int L, int64_t tiles, int64_t target_units, int min_span) {
+  const int64_t lo = (int64_t)1 << L;
+  int spans = 1;
+  while (tiles * spans < target_units && lo / (spans * 2) >= min_span) spans *= 2;
+  return spans;
+}
+
+__host__ __device__ inline WavePlan wave_plan(int first, int L, int64_t n_act, int tile_entries, int64_t target_units,
+                                              int min_span) {
+  const int64_t tiles = (n_act + tile_entries - 1) / tile_entries;
+  WavePlan p = wave_plan_spans(first, L, wave_spans(L, tiles, target_units, min_span));
+  p.tiles = tiles;
   return p;
 }
 

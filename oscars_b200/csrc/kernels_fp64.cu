@@ -18,13 +18,11 @@
 #include <cuda_runtime.h>
 
 #include "device_common.cuh"
+#include "fd_common.cuh"
 #include "kernels.h"
 
 namespace osc {
 namespace dev {
-
-constexpr double kCLight = 2.99792458e8;
-constexpr double kPiD = 3.14159265358979323846;
 
 // ---------------------------------------------------------------------------------------------
 // Level samples: TParticleTrajectoryInterpolated::FillTParticleTrajectoryPointsLevel
@@ -37,9 +35,6 @@ __global__ void k_level_fill(const double* __restrict__ knots, int64_t n, double
                              int extended_level) {
   const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= s_end) return;
-  const double* t = knots;
-  const double* y = knots + n;
-  const double* ypp = knots + 10 * n;
   int L;
   int64_t i;
   double ts, sp;
@@ -55,28 +50,11 @@ __global__ void k_level_fill(const double* __restrict__ knots, int64_t n, double
     sp = __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L));
   }
   const double T = __dadd_rn(ts, __dmul_rn(sp, (double)i));
-  // Interval search: same result as the reference's bisection (largest klo in [0, n-2] with
-  // t[klo] <= T), started from the uniform-spacing estimate and corrected by local steps.
-  int64_t k = (int64_t)((T - t[0]) / (t[n - 1] - t[0]) * (double)(n - 1));
-  k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
-  while (k > 0 && t[k] > T) --k;
-  while (k < n - 2 && t[k + 1] <= T) ++k;
-  const int64_t klo = k, khi = k + 1;
-  const double h = __dsub_rn(t[khi], t[klo]);
-  const double a = __ddiv_rn(__dsub_rn(t[khi], T), h);
-  const double b = __ddiv_rn(__dsub_rn(T, t[klo]), h);
-  const double ca = __dsub_rn(__dmul_rn(__dmul_rn(a, a), a), a);
-  const double cb = __dsub_rn(__dmul_rn(__dmul_rn(b, b), b), b);
-  const double hh = __dmul_rn(h, h);
+  double v[9];
+  spline_eval9(knots, n, T, v);
   lev[s] = T;
 #pragma unroll
-  for (int c = 0; c < 9; ++c) {
-    const double* Y = y + c * n;
-    const double* P = ypp + c * n;
-    const double lin = __dadd_rn(__dmul_rn(a, Y[klo]), __dmul_rn(b, Y[khi]));
-    const double cur = __ddiv_rn(__dmul_rn(__dadd_rn(__dmul_rn(ca, P[klo]), __dmul_rn(cb, P[khi])), hh), 6.0);
-    lev[(1 + c) * cap + s] = __dadd_rn(lin, cur);
-  }
+  for (int c = 0; c < 9; ++c) lev[(1 + c) * cap + s] = v[c];
 }
 
 // Per-level max |beta_i - beta_{i-1}| over i >= 1 (the power-density stop rule, src/OSCARSSR.cc:
@@ -259,38 +237,9 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
   }
 }
 
-struct C3 { double xr, xi, yr, yi, zr, zi; };
-
-__device__ __forceinline__ C3 c3_scale(C3 a, double s) {
-  return {a.xr * s, a.xi * s, a.yr * s, a.yi * s, a.zr * s, a.zi * s};
-}
-// (E . P) P with the complex (unconjugated) dot product of TVector3DC::Dot.
-__device__ __forceinline__ C3 c3_project(C3 e, const double* P) {
-  const double cr = (e.xr * P[0] - e.xi * P[1]) + (e.yr * P[2] - e.yi * P[3]) + (e.zr * P[4] - e.zi * P[5]);
-  const double ci = (e.xr * P[1] + e.xi * P[0]) + (e.yr * P[3] + e.yi * P[2]) + (e.zr * P[5] + e.zi * P[4]);
-  return {P[0] * cr - P[1] * ci, P[0] * ci + P[1] * cr, P[2] * cr - P[3] * ci,
-          P[2] * ci + P[3] * cr, P[4] * cr - P[5] * ci, P[4] * ci + P[5] * cr};
-}
-__device__ __forceinline__ double c3_mag2(C3 a) {
-  return (a.xr * a.xr + a.xi * a.xi) + (a.yr * a.yr + a.yi * a.yi) + (a.zr * a.zr + a.zi * a.zi);
-}
-
 // Reduce the span partials of the wave, apply the stop rule of src/OSCARSSR.cc:4222-4238, finish
-// converged / last-level entries (:4246-4267) and append the others to the next active list.
-// Span partials of one entry are reduced by a group of kFinLanes lanes: lane l sums the spans
-// l, l + kFinLanes, ... in order, then a fixed shuffle tree combines the lanes (deterministic).
-constexpr int kFinLanes = 8;
-
-__device__ __forceinline__ double group_sum(double v) {
-#pragma unroll
-  for (int o = kFinLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, kFinLanes);
-  return v;
-}
-__device__ __forceinline__ double group_max(double v) {
-#pragma unroll
-  for (int o = kFinLanes / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o, kFinLanes));
-  return v;
-}
+// converged / last-level entries (:4246-4267) and append the others to the next active list
+// (span partials reduced by kFinLanes-lane groups, fd_common.cuh).
 
 // Warp-aggregated bookkeeping of the finalize kernels: one atomic per warp for the survivor list and
 // one per warp for each statistics counter, instead of one per entry on a single address.

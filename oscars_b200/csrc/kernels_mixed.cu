@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "device_common.cuh"
+#include "fd_common.cuh"
 #include "kernels.h"
 
 namespace osc {
@@ -64,10 +65,6 @@ struct MixedStage {
   float4 v[2][kMxChunk * 3];
   uint64_t bar[2];
 };
-
-constexpr float kTwoPiHiF = 6.28318548202514648f;     // RN_f(2 pi)
-constexpr float kTwoPiLoF = -1.7484556e-07f;         // RN_f(2 pi - kTwoPiHiF)
-constexpr float kInvTwoPiF = 0.159154943f;
 
 template <int EPT, int MINB>
 __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A, MixedFrame F) {
@@ -118,10 +115,7 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
       wc[e] = (float)(om / kCl);
       // validity of the near-axis phase form: small angle from the frame axis and a bounded
       // correction phase (see the file comment); otherwise the caller must use the FP64 path
-      const double rho = sqrt(fx * fx + fy * fy) + F.xperp_max;
-      const double rz = fz - F.z_max;
-      if (live[e] && span == 0 && !(rz > 0 && rho < 1e-2 * rz && (om / kCl) * rho * rho / (2 * rz) < 3e4))
-        atomicOr(A.err, kErrBadArgs);
+      if (live[e] && span == 0 && !mixed_geometry_ok(fx, fy, fz, om, F.xperp_max, F.z_max)) atomicOr(A.err, kErrBadArgs);
     }
     for (int g = 0; g < P.nseg; ++g) {
       const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
@@ -170,13 +164,7 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
             const float4 r0 = sv[3 * j], r1 = sv[3 * j + 1], r2 = sv[3 * j + 2];
 #pragma unroll
             for (int e = 0; e < EPT; ++e) {
-              const float rx = Ox[e] - r0.x, ry = Oy[e] - r0.y, rz = Oz[e] - r0.z;
-              const float rho2 = fmaf(rx, rx, ry * ry);
-              const float d2 = fmaf(rz, rz, rho2);
-              const float iD = rsqrtf(d2);
-              const float q = rho2 * iD * iD;                                  // (rho/D)^2
-              const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);           // rho^2/(Rz+D), |rho/D| < 1e-2
-              const float ph = -fmaf(wc[e], corr, w[e] * r0.w);              // exp(-i w (t + D/c))
+              const float ph = mixed_sample(r0, r1, r2, Ox[e], Oy[e], Oz[e], w[e], wc[e], s32[e]);
               if (have[e]) {
                 const float dp = fabsf(ph - last[e]);
                 dmax[e] = fmaxf(dmax[e], dp);
@@ -185,24 +173,6 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
                 have[e] = true;
               }
               last[e] = ph;
-              const float k = rintf(ph * kInvTwoPiF);
-              const float rr = fmaf(-k, kTwoPiLoF, fmaf(-k, kTwoPiHiF, ph));
-              float sn, cs;
-              __sincosf(rr, &sn, &cs);
-              const float nx = rx * iD, ny = ry * iD;
-              const float en = corr * iD;                                      // 1 - n_z
-              const float ux = nx - r1.x, uy = ny - r1.y, uz = r1.z - en;
-              const float om = fmaf(-nx, r1.x, fmaf(-ny, r1.y, fmaf(-en, r1.z, en + r1.z)));
-              const float io = __fdividef(1.f, om);
-              const float na = fmaf(nx, r2.x, fmaf(ny, r2.y, (1.f - en) * r2.z));
-              const float k1 = io * io * iD * fmaf(r1.w, iD, na);
-              const float k2 = io * iD;
-              const float ex = fmaf(k1, ux, -k2 * r2.x);
-              const float ey = fmaf(k1, uy, -k2 * r2.y);
-              const float ez = fmaf(k1, uz, -k2 * r2.z);
-              s32[e][0] = fmaf(ex, cs, s32[e][0]); s32[e][1] = fmaf(ex, sn, s32[e][1]);
-              s32[e][2] = fmaf(ey, cs, s32[e][2]); s32[e][3] = fmaf(ey, sn, s32[e][3]);
-              s32[e][4] = fmaf(ez, cs, s32[e][4]); s32[e][5] = fmaf(ez, sn, s32[e][5]);
             }
           }
 #pragma unroll
