@@ -16,6 +16,12 @@ sample = one (observer, energy, trajectory point) term of the radiation sum, cou
 Under torchrun each rank runs its own job (energy E1 * (1 + 1e-3 rank)): no collective on the data
 path, weak scaling; the reported time is the max over ranks.
 
+``batched`` (single GPU) adds the two batched workloads: a 10k-particle EPU beam (101 x 101 flux)
+and 512 uneven undulator jobs, each timed on the device (every chunk of jobs from its first to its
+last kernel, device RK4 and splines included) and end to end through the public API, beside the
+FP64 reference method on a subset of the same particles / jobs and the mixed-vs-FP64 error at a
+fixed level.  ``--only beam|uneven`` runs one of them alone.
+
 ``--impl reference`` times the reference's own CPU implementation (oracle/_ref, built from the
 reference sources by oracle/Makefile; the CPU restatement in oracle/ when that build is absent)
 on all host cores, on the same workload and metric.
@@ -343,10 +349,181 @@ def product_arm(args):
                             "clocks": f["clocks"]}
             line["mixed_over_fp64"] = r["value"] / f["value"]
             line["mixed_vs_fp64_peak_rel_err"] = err
+        if world == 1 and args.batched_steps > 0:
+            bw = max(3, args.warmup)
+            line["batched"] = {"note": "inputs far larger than L2 (GBs of level records); device time = each "
+                                       "chunk of jobs from first to last kernel, trajectories included",
+                               "epu_beam_10k": beam_leg(args.batched_steps, bw, local),
+                               "uneven_512": uneven_leg(args.batched_steps, bw, local)}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# Batched workloads (mixed precision through the batch path, FP64 through the single-trajectory
+# path on a subset of the same particles / jobs)
+# ---------------------------------------------------------------------------------------------
+E1_EPU = 179.2558
+BEAM_PARTICLES = 10000
+BEAM_WORKLOAD = ("EPU beam: By=0.6T cos + Bx=0.4T sin, lambda=57mm, 30 periods; 3 GeV electrons, sigma_E=3 MeV, "
+                 "emittance (0.9 nm, 8 pm), beta (1.5, 0.8) m, alpha 0; %d particles (seed 1), 16001-point RK4 each; "
+                 "flux 101x101 on 8mm x 8mm at z=30m at E1=179.2558 eV; adaptive levels" % BEAM_PARTICLES)
+UNEVEN_JOBS = 512
+UNEVEN_WORKLOAD = ("%d uneven jobs (seed 2024): planar undulators lambda~U[15,100]mm, B0~U[0.2,1.2]T, N~U{10..200}, "
+                   "4k-64k RK4 points; 1-4096 observers (rectangles, z~U[20,40]m) x 1-256 energies within E1 +-5%%; "
+                   "adaptive levels" % UNEVEN_JOBS)
+
+
+def setup_epu_beam(o, seed=1):
+    o.add_bfield_undulator(bfield=[0, 0.6, 0], period=[0, 0, 0.057], nperiods=30, phase=-math.pi / 2)
+    o.add_bfield_undulator(bfield=[0.4, 0, 0], period=[0, 0, 0.057], nperiods=30, phase=0)
+    o.set_particle_beam(type="electron", energy_GeV=3, x0=[0, 0, 0], d0=[0, 0, 1], current=0.5,
+                        sigma_energy_GeV=0.003, beta=[1.5, 0.8], alpha=[0, 0], emittance=[0.9e-9, 8e-12])
+    o.set_ctstartstop(-1.5, 1.5)
+    o.set_npoints_trajectory(16001)
+    o.set_seed(seed)
+
+
+def _e1_eV(bfield, period, energy_GeV=3.0):
+    lam_cm = period * 100
+    K = 0.9337 * bfield * lam_cm
+    return 1000 * 0.9496 * energy_GeV ** 2 / (lam_cm * (1 + K * K / 2))
+
+
+def uneven_jobs(seed=2024, n=UNEVEN_JOBS):
+    import numpy as np
+    from oscars_b200.batch import Job, undulator
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(n):
+        lam = rng.uniform(0.015, 0.10)
+        B = rng.uniform(0.2, 1.2)
+        N = int(rng.integers(10, 201))
+        half = lam * (N + 2) / 2 + 0.2
+        npts = int(np.clip(240 * (N + 2 + 0.4 / lam), 4096, 65536))  # ~240 points per period plus drifts
+        nx, ny = int(rng.integers(1, 65)), int(rng.integers(1, 65))
+        wx, wy = rng.uniform(0.001, 0.006, 2)
+        z = rng.uniform(20, 40)
+        xs = np.linspace(-wx / 2, wx / 2, nx) if nx > 1 else np.zeros(1)
+        ys = np.linspace(-wy / 2, wy / 2, ny) if ny > 1 else np.zeros(1)
+        X, Y = np.meshgrid(xs, ys, indexing="ij")
+        obs = np.stack([X.ravel(), Y.ravel(), np.full(X.size, z)], 1)
+        ne = int(rng.integers(1, 257))
+        e1 = _e1_eV(B, lam)
+        jobs.append(Job(fields=[undulator([0, B, 0], [0, 0, lam], N, phase=-math.pi / 2)], energy_GeV=3.0,
+                        ctstartstop=(-half, half), npoints=npts, obs=obs,
+                        energies_eV=np.linspace(0.95 * e1, 1.05 * e1, ne), current=0.5))
+    return jobs
+
+
+def _profiled(ctx, fn):
+    """fn() with device profiling on: (result, device ms, samples, launches, wall s)."""
+    import ctypes
+    ctx.call("osc_set_profiling", 1)
+    ctx.call("osc_get_profile", None, None, None, 1)
+    t0 = time.perf_counter()
+    r = fn()
+    wall = time.perf_counter() - t0
+    ms, ns = ctypes.c_double(), ctypes.c_longlong()
+    ctx.call("osc_get_profile", ctypes.byref(ms), None, ctypes.byref(ns), 1)
+    ctx.call("osc_set_profiling", 0)
+    sm, ln = ctypes.c_longlong(), ctypes.c_longlong()
+    ctx.call("osc_last_stats", ctypes.byref(sm), ctypes.byref(ln))
+    return r, ms.value, sm.value, ln.value, wall
+
+
+def _peak_err(a, b):
+    import numpy as np
+    a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, check_level=12):
+    """EPU beam, 10k particles: mixed (batched) timed on the device and end to end; FP64 (reference
+    path, host RK4 per particle) end to end on the first `fp64_particles`; mixed vs FP64 error at a
+    fixed level on `check_particles`."""
+    import numpy as np
+    from oscars_b200.sr import sr
+    s = sr(gpu=1, device=local)
+    setup_epu_beam(s)
+    kw = dict(energy_eV=E1_EPU, npoints=[101, 101], width=[0.008, 0.008], translation=[0, 0, 30], return_numpy=True)
+
+    def run(np_, compute, **extra):
+        s.set_seed(1)
+        return s.calculate_flux_rectangle(nparticles=np_, compute=compute, **dict(kw, **extra))
+    for _ in range(warmup):
+        run(BEAM_PARTICLES, "mixed")
+    dev_ms = wall = 0.0
+    samples = launches = 0
+    with ClockSampler(local) as clk:
+        for _ in range(steps):
+            _, ms, sm, ln, w = _profiled(s._ctx, lambda: run(BEAM_PARTICLES, "mixed"))
+            dev_ms += ms
+            wall += w
+            samples += sm
+            launches += ln
+    run(fp64_particles, "fp64")
+    _, _, sm64, _, w64 = _profiled(s._ctx, lambda: run(fp64_particles, "fp64"))
+    a = run(check_particles, "mixed", precision=0, max_level=check_level)[1]
+    b = run(check_particles, "fp64", precision=0, max_level=check_level)[1]
+    mixed_e2e = samples / wall / 1e9
+    fp64_e2e = sm64 / w64 / 1e9
+    return {"workload": BEAM_WORKLOAD, "steps": steps, "warmup": warmup,
+            "value": samples / (dev_ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": dev_ms / steps,
+            "samples_per_step": samples // steps, "gpu_launches_per_step": launches // steps,
+            "e2e": {"value": mixed_e2e, "unit": "Gsamples/s", "wall_s_per_step": wall / steps,
+                    "path": "sr.calculate_flux_rectangle(nparticles=10000, compute='mixed', return_numpy=True)"},
+            "fp64": {"e2e": fp64_e2e, "unit": "Gsamples/s", "particles": fp64_particles,
+                     "path": "sr.calculate_flux_rectangle(nparticles=%d, compute='fp64') (reference method: host RK4 "
+                             "per particle, FP64 sums)" % fp64_particles},
+            "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
+            "mixed_vs_fp64_peak_rel_err": {"value": _peak_err(a, b), "particles": check_particles,
+                                           "fixed_level": check_level},
+            "clocks": clk.summary()}
+
+
+def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12):
+    """512 uneven jobs through osc_batch_flux: mixed timed on the device and end to end; FP64 (jobs
+    one after another through the FP64 path) end to end on the first `fp64_jobs`; mixed vs FP64 error
+    at a fixed level on those jobs."""
+    from oscars_b200.batch import BatchRunner
+    jobs = uneven_jobs()
+    r = BatchRunner(local)
+    for _ in range(warmup):
+        r.flux(jobs, compute="mixed")
+    dev_ms = wall = 0.0
+    samples = launches = 0
+    with ClockSampler(local) as clk:
+        for _ in range(steps):
+            _, ms, sm, ln, w = _profiled(r.ctx, lambda: r.flux(jobs, compute="mixed"))
+            dev_ms += ms
+            wall += w
+            samples += sm
+            launches += ln
+    variant = r.variant()[0]
+    sub = jobs[:fp64_jobs]
+    r.ctx.call("osc_set_variant", 0, 2)  # FP64 variant fixed: no per-shape tuning runs inside the timing
+    r.flux(sub, compute="fp64")
+    _, _, sm64, _, w64 = _profiled(r.ctx, lambda: r.flux(sub, compute="fp64"))
+    a = r.flux(sub, compute="mixed", precision=0, max_level=check_level)
+    b = r.flux(sub, compute="fp64", precision=0, max_level=check_level)
+    err = max(_peak_err(x, y) for x, y in zip(a, b))
+    mixed_e2e = samples / wall / 1e9
+    fp64_e2e = sm64 / w64 / 1e9
+    return {"workload": UNEVEN_WORKLOAD, "steps": steps, "warmup": warmup,
+            "value": samples / (dev_ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": dev_ms / steps,
+            "samples_per_step": samples // steps, "gpu_launches_per_step": launches // steps, "variant": variant,
+            "e2e": {"value": mixed_e2e, "unit": "Gsamples/s", "wall_s_per_step": wall / steps,
+                    "path": "oscars_b200.batch.BatchRunner.flux(jobs, compute='mixed')"},
+            "fp64": {"e2e": fp64_e2e, "unit": "Gsamples/s", "jobs": fp64_jobs,
+                     "path": "BatchRunner.flux(jobs[:%d], compute='fp64') (jobs one after another, host RK4)"
+                             % fp64_jobs},
+            "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
+            "mixed_vs_fp64_peak_rel_err": {"value": err, "jobs": fp64_jobs, "fixed_level": check_level,
+                                           "norm": "per job, max over jobs"},
+            "clocks": clk.summary()}
 
 
 def main():
@@ -358,9 +535,18 @@ def main():
     ap.add_argument("--compute", default="mixed", choices=["fp64", "mixed"],
                     help="headline arithmetic; 'mixed' also times the FP64 path and reports both")
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (for profiler runs)")
+    ap.add_argument("--batched-steps", type=int, default=3,
+                    help="timed steps of the batched workloads (EPU beam, uneven jobs); 0 skips them")
+    ap.add_argument("--only", default="", choices=["", "beam", "uneven"],
+                    help="run one batched workload alone and print its JSON object (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.only:
+        import torch
+        torch.cuda.set_device(0)
+        leg = beam_leg if args.only == "beam" else uneven_leg
+        print(json.dumps(leg(args.batched_steps, args.warmup)), flush=True)
     else:
         product_arm(args)
 

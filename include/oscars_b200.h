@@ -217,8 +217,10 @@ OSC_API int osc_power_density_device(osc_ctx* ctx, const double* d_obs_xyz,
 OSC_API int osc_last_stats(osc_ctx* ctx, long long* samples, long long* launches);
 
 /* Profiling: when enabled, every sample-integration kernel launch is bracketed by CUDA events on
- * its stream; osc_get_profile returns the summed device time [ms] of those launches since the last
- * reset, their number, and the samples they integrated (reset = 1 clears the counters). */
+ * its stream (for batches -- osc_batch_flux and multi-particle mixed requests -- each chunk of jobs
+ * from its first kernel to its last, trajectories included); osc_get_profile returns the summed
+ * device time [ms] of those intervals since the last reset, their number, and the samples they
+ * integrated (reset = 1 clears the counters). */
 OSC_API int osc_set_profiling(osc_ctx* ctx, int enable);
 OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches, long long* samples,
                             int reset);

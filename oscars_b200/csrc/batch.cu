@@ -873,6 +873,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     };
     // a new shape is tuned and run eagerly; a known shape is captured and replayed as a graph
     const auto key = std::make_tuple(nj, N, Lfirst, Lpre);
+    const auto chunk_ev = timed_begin(st);  // with profiling on: device time of the whole chunk
     int v = forced_variant[3] >= 0 ? forced_variant[3] : current_variant_[3];
     const bool need_tune = forced_variant[3] < 0 && autotune && tuned_batch_.find(key) == tuned_batch_.end();
     if (forced_variant[3] < 0 && autotune && !need_tune) v = tuned_batch_[key];
@@ -949,6 +950,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
         check(cudaMemcpyAsync(level_out + done_entries, b_lvl_.p, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st),
               "download");
     }
+    timed_end(chunk_ev, st);
     unsigned long long h64[2] = {0, 0};
     unsigned err = 0;
     check(cudaMemcpyAsync(h64, m64, sizeof h64, cudaMemcpyDeviceToHost, st), "stats");
@@ -963,7 +965,10 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
                                    "phase below 3e4 rad); use compute='fp64' for this geometry"};
     last_not_converged += (long long)h64[0];
     last_samples += (long long)h64[1];
-    if (profiling) prof_samples += (long long)h64[1];
+    if (profiling) {
+      prof_samples += (long long)h64[1];
+      collect_timings();
+    }
     done_entries += (size_t)N;
     j0 = j1;
   }
