@@ -38,7 +38,7 @@ enum osc_status {
   OSC_ERR_TIMEOUT = 8       /* a bounded device-side wait gave up */
 };
 
-enum osc_field_kind { OSC_FIELD_UNDULATOR = 0, OSC_FIELD_EPU = 1 };
+enum osc_field_kind { OSC_FIELD_UNDULATOR = 0, OSC_FIELD_EPU = 1, OSC_FIELD_GRID = 2 };
 
 /* Particle types of TParticleA::SetParticleType (src/TParticleA.cc:78-121). */
 enum osc_particle_type {
@@ -77,6 +77,20 @@ typedef struct {
   double frequency;         /* [Hz], 0 = static */
   double frequency_phase;   /* [rad] */
   double time_offset;       /* [s] */
+  /* OSC_FIELD_UNDULATOR, optional: amplitude factor of each of the 2 * nperiods half-periods of the
+   * full-strength region between the end poles (NULL / 0 = all 1). */
+  const double* half_period_scale;
+  int n_half_periods;
+  /* OSC_FIELD_GRID (TField3D_Grid, src/TField3D_Grid.cc:153-283): grid_n points per axis from
+   * grid_start in steps grid_step; grid_values holds 3 field components per point at index
+   * ix * ny * nz + iy * nz + iz; `rotations` rotate the values on load and the evaluation point
+   * before `center` (the translation) is subtracted; time factor
+   * cos(2 pi frequency (t + time_offset) + frequency_phase). */
+  long long grid_n[3];
+  double grid_start[3];
+  double grid_step[3];
+  const double* grid_values;
+  double rotations[3];
 } osc_field_desc;
 
 typedef struct {
@@ -127,6 +141,12 @@ OSC_API const char* osc_version(void);
 OSC_API int osc_clear_fields(osc_ctx* ctx);
 OSC_API int osc_add_field(osc_ctx* ctx, const osc_field_desc* field);
 OSC_API int osc_get_bfield(osc_ctx* ctx, const double x[3], double t, double out[3]);
+/* add_bfield_file: OSCARSSR::AddMagneticField(FileName, Format, ...) (src/OSCARSSR.cc:70-103) with
+ * the TField3D_Grid readers for the 'OSCARS' (src/TField3D_Grid.cc:365-530) and 'OSCARS1D ...'
+ * (:572-870) text formats; scaling may be NULL (n_scaling 0). */
+OSC_API int osc_add_field_file(osc_ctx* ctx, const char* path, const char* format, const double rotations[3],
+                               const double translation[3], const double* scaling, int n_scaling,
+                               double frequency, double frequency_phase, double time_offset);
 
 /* ---- beam: set_particle_beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) ------------------ */
 OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* beam);

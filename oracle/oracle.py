@@ -57,6 +57,8 @@ def load():
     lib.orc_add_undulator.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_int, dp, D, D, D, D, D]
     lib.orc_add_epu.argtypes = [ctypes.c_void_p, dp, dp, dp, ctypes.c_int, dp, D, D, D, D, D]
     lib.orc_get_bfield.argtypes = [ctypes.c_void_p, dp, D, dp]
+    lib.orc_set_half_period_scale.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
+    lib.orc_add_grid.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), dp, dp, dp, dp, dp, dp, D, D, D]
     lib.orc_set_beam.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D, D, dp, dp, D, D, dp,
                                  ctypes.c_int, D, dp, ctypes.c_int, dp, dp, ctypes.c_int,
                                  ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int]
@@ -179,6 +181,141 @@ def rectangle(plane, nx1, nx2, w1, w2, rotations, translation, normal):
     return xyz, normals, x1x2
 
 
+# ---- grid field files (restating src/TField3D_Grid.cc:365-530 and :572-870) -------------------
+def _first_number(line):
+    """TField3D_Grid::GetHeaderValue: the first number on the line (0 when there is none)."""
+    tok = line.split()
+    try:
+        return float(tok[0]) if tok else 0.0
+    except ValueError:
+        return 0.0
+
+
+def read_oscars_grid(path, rotations, scaling):
+    """'OSCARS' format: comment line, 9 header lines (start, step, n for x, y, z), then
+    nx*ny*nz lines 'Fx Fy Fz' with x slowest.  Returns (n, start, step, stop, values)."""
+    with open(path) as fi:
+        lines = fi.read().split("\n")
+    hv = [_first_number(lines[1 + i]) if 1 + i < len(lines) else 0.0 for i in range(9)]
+    xs, xst, nx, ys, yst, ny, zs, zst, nz = hv
+    NX, NY, NZ = int(nx), int(ny), int(nz)
+    sc = list(scaling)
+    XStep = xst * sc[0] if len(sc) > 0 else xst
+    YStep = yst * sc[1] if len(sc) > 1 else yst
+    ZStep = zst * sc[2] if len(sc) > 2 else zst
+    fsx = sc[3] if len(sc) > 3 else 1
+    fsy = sc[4] if len(sc) > 4 else 1
+    fsz = sc[5] if len(sc) > 5 else 1
+    XStart = (xs + xst * (NX - 1) / 2.) - XStep * (NX - 1) / 2.
+    YStart = (ys + yst * (NY - 1) / 2.) - YStep * (NY - 1) / 2.
+    ZStart = (zs + zst * (NZ - 1) / 2.) - ZStep * (NZ - 1) / 2.
+    if NX < 1 or NY < 1 or NZ < 1:
+        raise ValueError("invalid number of points in at least one dimension")
+    n = [NX, NY, NZ]
+    start = [XStart, YStart, ZStart]
+    step = [XStep, YStep, ZStep]
+    stop = [start[a] + (n[a] - 1) * step[a] for a in range(3)]
+    vals = np.empty((NX * NY * NZ, 3))
+    k = 0
+    for i in range(NX * NY * NZ):
+        li = 10 + i
+        if li >= len(lines) - 1:  # getline reached the end of the file (the reference checks eof())
+            raise ValueError("error reading file.  Check format")
+        tok = lines[li].split()
+        try:
+            fx, fy, fz = float(tok[0]), float(tok[1]), float(tok[2])
+        except (IndexError, ValueError):
+            raise ValueError("error reading file.  Check format")
+        if fsx != 1:
+            fx *= fsx
+        if fsy != 1:
+            fy *= fsy
+        if fsz != 1:
+            fz *= fsz
+        vals[k] = rotate_xyz([fx, fy, fz], rotations)
+        k += 1
+    return n, start, step, stop, vals
+
+
+def read_oscars1d_grid(path, fmt, rotations, scaling, comment="#"):
+    """'OSCARS1D <columns>': irregular samples along one axis, sorted, resampled at 10000 points
+    per metre by linear interpolation.  Returns (n, start, step, stop, values)."""
+    order = [-1, -1, -1, -1]
+    has = [False] * 4
+    axis = ""
+    index = xdim = fdim = 0
+    for c in fmt[8:].split():
+        if index > 3:
+            raise ValueError("spatial or B-field dimensions are too large(index>3)")
+        if c in ("X", "Y", "Z"):
+            axis = c
+            xdim += 1
+            order[index] = 0
+        elif c in ("Bx", "Ex", "Fx"):
+            has[1] = True
+            fdim += 1
+            order[index] = 1
+        elif c in ("By", "Ey", "Fy"):
+            has[2] = True
+            fdim += 1
+            order[index] = 2
+        elif c in ("Bz", "Ez", "Fz"):
+            has[3] = True
+            fdim += 1
+            order[index] = 3
+        else:
+            raise ValueError("only excepts X Y Z Bx By Bz")
+        index += 1
+    count = xdim + fdim
+    if xdim != 1:
+        raise ValueError("spatial or B-field dimensions are too large")
+    with open(path) as fi:
+        lines = fi.read().split("\n")
+    if lines and lines[-1] == "":
+        lines = lines[:-1]
+    data = []
+    for L in lines[1:]:
+        stripped = L.lstrip(" \t")
+        if stripped == "" or stripped[0] == comment:
+            continue
+        tok = L.replace(",", " ").split()
+        val = [0.0, 0.0, 0.0, 0.0]
+        for i in range(count):
+            try:
+                val[order[i]] = float(tok[i])
+            except (IndexError, ValueError):
+                raise ValueError("something is incorrect with data format or iformat string")
+        for i in range(min(len(scaling), 4)):
+            if order[i] < 0:
+                continue
+            val[order[i]] *= scaling[i]
+        data.append(val)
+    data.sort(key=lambda a: a[0])
+    if len(data) < 2:
+        raise ValueError("not enough data points")
+    first, last = data[0][0], data[-1][0]
+    npts = int((last - first) * 10000)
+    step = (last - first) / float(npts - 1)
+    ax = {"X": 0, "Y": 1, "Z": 2}[axis]
+    n, start, stp, stop = [1, 1, 1], [0.0] * 3, [0.0] * 3, [0.0] * 3
+    n[ax], start[ax], stp[ax], stop[ax] = npts, first, step, last
+    vals = np.empty((npts, 3))
+    min_bin = after = before = 0
+    for i in range(npts):
+        z = i * step + first
+        for j in range(min_bin + 1, len(data)):
+            if data[j][0] > z:
+                after, before, min_bin = j, j - 1, j - 1
+                break
+        nb = [0.0, 0.0, 0.0]
+        for k in range(3):
+            if has[k + 1]:
+                slope = (data[after][k + 1] - data[before][k + 1]) / (data[after][0] - data[before][0])
+                nb[k] = data[before][k + 1] + (z - data[before][0]) * slope
+        vals[i] = rotate_xyz(nb, rotations)
+    return n, start, stp, stop, vals
+
+
 def polarization_code(polarization, angle):
     """Binding default (src/OSCARSSR_Python.cc:5889-5899) + string match (src/OSCARSSR.cc:4129-4150)."""
     if polarization == "all" and angle != _ANGLE_UNSET:
@@ -260,7 +397,8 @@ class OracleSR:
         self._lib.orc_clear_fields(self._h)
 
     def add_bfield_undulator(self, bfield, period, nperiods, phase=0, rotations=[], translation=[],
-                             taper=0, frequency=0, frequency_phase=0, time_offset=0, name=""):
+                             taper=0, frequency=0, frequency_phase=0, time_offset=0, name="",
+                             half_period_scale=None):
         f = _v3(bfield, "bfield")
         p = _v3(period, "period")
         r = _v3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
@@ -272,6 +410,43 @@ class OracleSR:
         self._check(self._lib.orc_add_undulator(self._h, _dp(F), _dp(Pp), int(nperiods), _dp(T),
                                                 float(phase), float(taper), float(frequency),
                                                 float(frequency_phase), float(time_offset)))
+        if half_period_scale is not None:
+            hs = np.ascontiguousarray(np.asarray(half_period_scale, dtype=np.float64))
+            self._check(self._lib.orc_set_half_period_scale(self._h, _dp(hs), int(hs.size)))
+
+    def _add_grid(self, n, start, step, stop, vals, rotations, translation, frequency, frequency_phase,
+                  time_offset):
+        N = (ctypes.c_long * 3)(*n)
+        a = lambda v: np.ascontiguousarray(np.array(v, dtype=np.float64))
+        S, St, Sp, V, R, T = a(start), a(step), a(stop), a(vals), a(rotations), a(translation)
+        self._check(self._lib.orc_add_grid(self._h, N, _dp(S), _dp(St), _dp(Sp), _dp(V), _dp(R), _dp(T),
+                                           float(frequency), float(frequency_phase), float(time_offset)))
+
+    def add_bfield_file(self, ifile="", iformat="", rotations=[], translation=[], scale=[], frequency=0,
+                        frequency_phase=0, time_offset=0, name=""):
+        r = _v3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        t = _v3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
+        F = iformat.upper()
+        if F == "OSCARS":
+            n, start, step, stop, vals = read_oscars_grid(ifile, r, list(scale))
+        elif len(F) > 8 and F[:8] == "OSCARS1D":
+            n, start, step, stop, vals = read_oscars1d_grid(ifile, iformat, r, list(scale))
+        else:
+            raise ValueError("format not restated by the oracle: %s" % iformat)
+        self._add_grid(n, start, step, stop, vals, r, t, frequency, frequency_phase, time_offset)
+
+    def add_bfield_grid(self, values, npoints, start, step, rotations=[], translation=[], frequency=0,
+                        frequency_phase=0, time_offset=0, name=""):
+        r = _v3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        t = _v3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
+        n = [int(v) for v in npoints]
+        st = [float(v) for v in step]
+        st = [st[a] if n[a] > 1 else 0.0 for a in range(3)]
+        start = [float(v) for v in start]
+        stop = [start[a] + (n[a] - 1) * st[a] for a in range(3)]
+        v = np.asarray(values, dtype=np.float64).reshape(-1, 3)
+        vals = np.array([rotate_xyz(list(x), r) for x in v])
+        self._add_grid(n, start, st, stop, vals, r, t, frequency, frequency_phase, time_offset)
 
     def add_bfield_epu(self, period, nperiods, bfieldA=[], bfieldB=[], phase=0, rotations=[],
                        translation=[], taper=0, frequency=0, frequency_phase=0, time_offset=0, name=""):

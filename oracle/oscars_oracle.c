@@ -149,13 +149,37 @@ static double rng_normal(orc_rng* r) {
  * (src/TField3D_IdealEPU.cc:116-170), summed by TFieldContainer::GetF (src/TFieldContainer.cc:85-104)
  * ------------------------------------------------------------------------------------------- */
 typedef struct {
-  int kind; /* 0 undulator, 1 EPU */
+  int kind; /* 0 undulator, 1 EPU, 2 grid */
   v3 field, field_b, period, center;
   int nperiods;
   double phase, taper, frequency, frequency_phase, time_offset;
   double period_length, und_length;
   v3 period_unit;
+  double* half_scale; /* undulator: per half-period factors of the full-strength region, or NULL */
+  int n_half;
+  /* grid (TField3D_Grid): n, start, step, stop per axis, dimension code, values (3 per point) */
+  long gn[3];
+  double gstart[3], gstep[3], gstop[3];
+  int gdim;
+  double* gval;
+  v3 grot;
 } orc_field;
+
+enum { GD_X = 0, GD_Y, GD_Z, GD_XY, GD_XZ, GD_YZ, GD_XYZ };
+
+/* TVector3D::RotateSelfXYZ: about x, then y, then z. */
+static v3 vrotxyz(v3 v, v3 r) {
+  double s = sin(r.x), c = cos(r.x), t = v.y;
+  v.y = c * t - s * v.z;
+  v.z = s * t + c * v.z;
+  s = sin(r.y); c = cos(r.y); t = v.z;
+  v.z = c * t - s * v.x;
+  v.x = s * t + c * v.x;
+  s = sin(r.z); c = cos(r.z); t = v.x;
+  v.x = c * t - s * v.y;
+  v.y = s * t + c * v.y;
+  return v;
+}
 
 /* One sinusoidal block with the 1/4 and 3/4 end poles, as in IdealUndulator::GetF. */
 static v3 und_block(const orc_field* f, v3 amp, double d, double phase_shift, double taper_corr) {
@@ -170,11 +194,78 @@ static v3 und_block(const orc_field* f, v3 amp, double d, double phase_shift, do
       F = vmul(vmul(vmul(amp, 0.75), s), taper_corr);
   } else {
     F = vmul(vmul(amp, s), taper_corr);
+    if (f->half_scale) { /* half-period k of the full-strength region, counted from its start */
+      long k = (long)((d - (-L / 2. + phase_shift + lam)) / (lam / 2.));
+      k = k < 0 ? 0 : (k >= f->n_half ? f->n_half - 1 : k);
+      F = vmul(F, f->half_scale[k]);
+    }
   }
   return F;
 }
 
+/* Grid field, src/TField3D_Grid.cc:153-283. */
+static v3 gval(const orc_field* f, long i) { return V(f->gval[3 * i], f->gval[3 * i + 1], f->gval[3 * i + 2]); }
+static v3 glerp(v3 a, v3 b, double d, double step) { return vadd(a, vdiv(vmul(vsub(b, a), d), step)); }
+
+static v3 grid_eval(const orc_field* f, v3 XIN, double T) {
+  v3 X = vsub(vrotxyz(XIN, f->grot), f->center);
+  double p[3] = {X.x, X.y, X.z};
+  long ni[3] = {0, 0, 0};
+  double di[3] = {0, 0, 0};
+  for (int a = 0; a < 3; ++a) {
+    if (f->gn[a] > 1 && (p[a] <= f->gstart[a] || p[a] >= f->gstop[a])) return V(0, 0, 0);
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (f->gn[a] > 1) {
+      ni[a] = (long)((p[a] - f->gstart[a]) / f->gstep[a]);
+      di[a] = (p[a] - f->gstart[a]) - ni[a] * f->gstep[a];
+      if (ni[a] > f->gn[a] - 2) ni[a] = f->gn[a] - 2;
+    }
+  }
+  long NY = f->gn[1], NZ = f->gn[2];
+#define GI(ix, iy, iz) ((ix) * NY * NZ + (iy) * NZ + (iz))
+  long nx = ni[0], ny = ni[1], nz = ni[2];
+  double dx = di[0], dy = di[1], dz = di[2];
+  v3 F;
+  switch (f->gdim) {
+    case GD_XYZ: {
+      v3 v00 = glerp(gval(f, GI(nx, ny, nz)), gval(f, GI(nx + 1, ny, nz)), dx, f->gstep[0]);
+      v3 v10 = glerp(gval(f, GI(nx, ny + 1, nz)), gval(f, GI(nx + 1, ny + 1, nz)), dx, f->gstep[0]);
+      v3 v01 = glerp(gval(f, GI(nx, ny, nz + 1)), gval(f, GI(nx + 1, ny, nz + 1)), dx, f->gstep[0]);
+      v3 v11 = glerp(gval(f, GI(nx, ny + 1, nz + 1)), gval(f, GI(nx + 1, ny + 1, nz + 1)), dx, f->gstep[0]);
+      v3 v0 = glerp(v00, v10, dy, f->gstep[1]);
+      v3 v1 = glerp(v01, v11, dy, f->gstep[1]);
+      F = glerp(v0, v1, dz, f->gstep[2]);
+      break;
+    }
+    case GD_X: F = glerp(gval(f, nx), gval(f, nx + 1), dx, f->gstep[0]); break;
+    case GD_Y: F = glerp(gval(f, ny), gval(f, ny + 1), dy, f->gstep[1]); break;
+    case GD_Z: F = glerp(gval(f, nz), gval(f, nz + 1), dz, f->gstep[2]); break;
+    case GD_XY: {
+      v3 v0 = glerp(gval(f, GI(nx, ny, 0)), gval(f, GI(nx + 1, ny, 0)), dx, f->gstep[0]);
+      v3 v1 = glerp(gval(f, GI(nx, ny + 1, 0)), gval(f, GI(nx + 1, ny + 1, 0)), dx, f->gstep[0]);
+      F = glerp(v0, v1, dy, f->gstep[1]);
+      break;
+    }
+    case GD_XZ: {
+      v3 v0 = glerp(gval(f, GI(nx, 0, nz)), gval(f, GI(nx + 1, 0, nz)), dx, f->gstep[0]);
+      v3 v1 = glerp(gval(f, GI(nx, 0, nz + 1)), gval(f, GI(nx + 1, 0, nz + 1)), dx, f->gstep[0]);
+      F = glerp(v0, v1, dz, f->gstep[2]);
+      break;
+    }
+    default: {
+      v3 v0 = glerp(gval(f, GI(0, ny, nz)), gval(f, GI(0, ny + 1, nz)), dy, f->gstep[1]);
+      v3 v1 = glerp(gval(f, GI(0, ny, nz + 1)), gval(f, GI(0, ny + 1, nz + 1)), dy, f->gstep[1]);
+      F = glerp(v0, v1, dz, f->gstep[2]);
+      break;
+    }
+  }
+#undef GI
+  return vmul(F, cos(twopi() * f->frequency * (T + f->time_offset) + f->frequency_phase));
+}
+
 static v3 field_eval(const orc_field* f, v3 X, double T) {
+  if (f->kind == 2) return grid_eval(f, X, T);
   double d = vdot(vsub(X, f->center), f->period_unit);
   double taper_corr = 1 + d * f->taper;
   v3 F;
@@ -256,14 +347,24 @@ orc_sim* orc_new(void) {
   rng_seed(&s->rng, 5489u);
   return s;
 }
+static void fields_free(orc_sim* s) {
+  for (int i = 0; i < s->nfields; ++i) {
+    free(s->fields[i].half_scale);
+    free(s->fields[i].gval);
+    s->fields[i].half_scale = NULL;
+    s->fields[i].gval = NULL;
+  }
+  s->nfields = 0;
+}
 void orc_free(orc_sim* s) {
   if (!s) return;
   traj_clear(&s->tr);
+  fields_free(s);
   free(s);
 }
 const char* orc_last_error(const orc_sim* s) { return s->err; }
 
-int orc_clear_fields(orc_sim* s) { s->nfields = 0; traj_clear(&s->tr); return ORC_OK; }
+int orc_clear_fields(orc_sim* s) { fields_free(s); traj_clear(&s->tr); return ORC_OK; }
 
 static int add_field(orc_sim* s, int kind, const double* fa, const double* fb, const double* period,
                      int nperiods, const double* center, double phase, double taper, double freq,
@@ -296,6 +397,46 @@ int orc_add_epu(orc_sim* s, const double field_a[3], const double field_b[3], co
                 double frequency_phase, double time_offset) {
   return add_field(s, 1, field_a, field_b, period, nperiods, center, phase, taper, frequency,
                    frequency_phase, time_offset);
+}
+
+int orc_set_half_period_scale(orc_sim* s, const double* scale, int n) {
+  if (s->nfields < 1 || s->fields[s->nfields - 1].kind != 0) return fail(s, ORC_ERR_STATE, "last field is not an undulator");
+  orc_field* f = &s->fields[s->nfields - 1];
+  if (n != 2 * f->nperiods) return fail(s, ORC_ERR_RANGE, "n_half_periods must be 2 * nperiods");
+  free(f->half_scale);
+  f->half_scale = (double*)malloc(sizeof(double) * n);
+  if (!f->half_scale) return fail(s, ORC_ERR_ALLOC, "allocation failed");
+  memcpy(f->half_scale, scale, sizeof(double) * n);
+  f->n_half = n;
+  traj_clear(&s->tr);
+  return ORC_OK;
+}
+
+int orc_add_grid(orc_sim* s, const long n[3], const double start[3], const double step[3], const double stop[3],
+                 const double* values, const double rotations[3], const double translation[3], double frequency,
+                 double frequency_phase, double time_offset) {
+  if (s->nfields >= 64) return fail(s, ORC_ERR_RANGE, "too many fields");
+  int hx = n[0] > 1, hy = n[1] > 1, hz = n[2] > 1;
+  int dim = hx && hy && hz ? GD_XYZ : hx && hy ? GD_XY : hx && hz ? GD_XZ : hy && hz ? GD_YZ : hx ? GD_X : hy ? GD_Y
+          : hz ? GD_Z : -1;
+  if (dim < 0) return fail(s, ORC_ERR_RANGE, "invalid dimensions");
+  long N = n[0] * n[1] * n[2];
+  orc_field* f = &s->fields[s->nfields];
+  memset(f, 0, sizeof *f);
+  f->gval = (double*)malloc(sizeof(double) * 3 * N);
+  if (!f->gval) return fail(s, ORC_ERR_ALLOC, "allocation failed");
+  memcpy(f->gval, values, sizeof(double) * 3 * N);
+  ++s->nfields;
+  f->kind = 2;
+  for (int a = 0; a < 3; ++a) {
+    f->gn[a] = n[a]; f->gstart[a] = start[a]; f->gstep[a] = step[a]; f->gstop[a] = stop[a];
+  }
+  f->gdim = dim;
+  f->grot = V(rotations[0], rotations[1], rotations[2]);
+  f->center = V(translation[0], translation[1], translation[2]);
+  f->frequency = frequency; f->frequency_phase = frequency_phase; f->time_offset = time_offset;
+  traj_clear(&s->tr);
+  return ORC_OK;
 }
 
 static v3 field_sum(const orc_sim* s, v3 X, double T) {

@@ -41,6 +41,14 @@ int orc_add_epu(orc_sim*, const double field_a[3], const double field_b[3], cons
                 int nperiods, const double center[3], double phase, double taper, double frequency,
                 double frequency_phase, double time_offset);
 int orc_get_bfield(const orc_sim*, const double x[3], double t, double out[3]);
+/* Amplitude factors of the 2 * nperiods half-periods of the last added undulator's full-strength
+ * region (between its end poles). */
+int orc_set_half_period_scale(orc_sim*, const double* scale, int n);
+/* Regular grid field (TField3D_Grid, src/TField3D_Grid.cc:153-283): values (3 per point, already
+ * rotated, index ix*ny*nz + iy*nz + iz); the file readers are restated in oracle.py. */
+int orc_add_grid(orc_sim*, const long n[3], const double start[3], const double step[3], const double stop[3],
+                 const double* values, const double rotations[3], const double translation[3], double frequency,
+                 double frequency_phase, double time_offset);
 
 /* set_particle_beam: charge [C], mass [kg] (0,0 selects by type code 0=electron,1=positron). */
 int orc_set_beam(orc_sim*, int type_code, double charge, double mass, double energy_GeV,

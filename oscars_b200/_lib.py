@@ -27,7 +27,8 @@ LLP = ctypes.POINTER(LL)
 class FieldDesc(ctypes.Structure):
     _fields_ = [("kind", I), ("bfield", D * 3), ("bfield_b", D * 3), ("period", D * 3), ("nperiods", I),
                 ("center", D * 3), ("phase", D), ("taper", D), ("frequency", D), ("frequency_phase", D),
-                ("time_offset", D)]
+                ("time_offset", D), ("half_period_scale", DP), ("n_half_periods", I), ("grid_n", LL * 3),
+                ("grid_start", D * 3), ("grid_step", D * 3), ("grid_values", DP), ("rotations", D * 3)]
 
 
 class BeamDesc(ctypes.Structure):
@@ -60,6 +61,7 @@ SIGNATURES = {
     "osc_clear_fields": (I, [VP]),
     "osc_add_field": (I, [VP, ctypes.POINTER(FieldDesc)]),
     "osc_get_bfield": (I, [VP, DP, D, DP]),
+    "osc_add_field_file": (I, [VP, ctypes.c_char_p, ctypes.c_char_p, DP, DP, DP, I, D, D, D]),
     "osc_set_beam": (I, [VP, ctypes.POINTER(BeamDesc)]),
     "osc_set_seed": (I, [VP, I]),
     "osc_set_new_particle": (I, [VP, I]),

@@ -26,15 +26,25 @@ import numpy as np
 from . import _lib
 from .sr import _PARTICLES, _ANGLE_UNSET, _compute_mode, _polarization
 
-__all__ = ["Job", "undulator", "epu", "BatchRunner", "flux_batch"]
+__all__ = ["Job", "undulator", "epu", "grid", "BatchRunner", "flux_batch"]
 
 
 def undulator(bfield, period, nperiods, translation=(0, 0, 0), phase=0.0, taper=0.0, frequency=0.0,
-              frequency_phase=0.0, time_offset=0.0):
-    """An ideal planar undulator, with the arguments of sr.add_bfield_undulator."""
+              frequency_phase=0.0, time_offset=0.0, half_period_scale=None):
+    """An ideal planar undulator, with the arguments of sr.add_bfield_undulator (optionally with
+    2 * nperiods half-period amplitude factors)."""
     return dict(kind=0, bfield=list(bfield), bfield_b=[0, 0, 0], period=list(period), nperiods=int(nperiods),
                 center=list(translation), phase=phase, taper=taper, frequency=frequency,
-                frequency_phase=frequency_phase, time_offset=time_offset)
+                frequency_phase=frequency_phase, time_offset=time_offset, half_period_scale=half_period_scale)
+
+
+def grid(values, npoints, start, step, rotations=(0, 0, 0), translation=(0, 0, 0), frequency=0.0,
+         frequency_phase=0.0, time_offset=0.0):
+    """A regular-grid field, as sr.add_bfield_grid."""
+    return dict(kind=2, values=np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1, 3)),
+                npoints=[int(v) for v in npoints], start=list(start), step=list(step), rotations=list(rotations),
+                center=list(translation), frequency=frequency, frequency_phase=frequency_phase,
+                time_offset=time_offset)
 
 
 def epu(bfield, bfield_b, period, nperiods, translation=(0, 0, 0), phase=0.0, taper=0.0):
@@ -78,19 +88,33 @@ class BatchRunner:
         if not jobs:
             return []
         fdescs, jdescs, obs_all, e_all = [], [], [], []
+        keep = []  # arrays the descriptors point into, alive until the call returns
         n_obs = n_e = 0
         for jb in jobs:
             fb = len(fdescs)
             for f in jb.fields:
                 d = _lib.FieldDesc()
                 d.kind = f["kind"]
-                d.bfield[:] = f["bfield"]
-                d.bfield_b[:] = f["bfield_b"]
-                d.period[:] = f["period"]
-                d.nperiods = f["nperiods"]
                 d.center[:] = f["center"]
-                d.phase, d.taper = f["phase"], f["taper"]
                 d.frequency, d.frequency_phase, d.time_offset = f["frequency"], f["frequency_phase"], f["time_offset"]
+                if f["kind"] == 2:
+                    keep.append(f["values"])
+                    d.grid_n[:] = f["npoints"]
+                    d.grid_start[:] = f["start"]
+                    d.grid_step[:] = f["step"]
+                    d.grid_values = _lib.dptr(f["values"])
+                    d.rotations[:] = f["rotations"]
+                else:
+                    d.bfield[:] = f["bfield"]
+                    d.bfield_b[:] = f["bfield_b"]
+                    d.period[:] = f["period"]
+                    d.nperiods = f["nperiods"]
+                    d.phase, d.taper = f["phase"], f["taper"]
+                    if f.get("half_period_scale") is not None:
+                        hs = np.ascontiguousarray(np.asarray(f["half_period_scale"], dtype=np.float64).ravel())
+                        keep.append(hs)
+                        d.half_period_scale = _lib.dptr(hs)
+                        d.n_half_periods = int(hs.size)
                 fdescs.append(d)
             o = np.ascontiguousarray(np.asarray(jb.obs, dtype=np.float64).reshape(-1, 3))
             e = np.ascontiguousarray(np.asarray(jb.energies_eV, dtype=np.float64).reshape(-1))

@@ -35,33 +35,117 @@ namespace dev {
 // TField3D_IdealEPU and TParticleA::RK4); sin and cos are CUDA's, so a trajectory agrees with the
 // host's to rounding, not bit for bit -- this path is the mixed-precision one.
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void pole_block_d(const DevField& f, const double* amp, double d, double shift, double tc,
-                                             double* F) {
+__device__ __forceinline__ void pole_block_d(const DevField& f, const double* __restrict__ vals, const double* amp,
+                                             double d, double shift, double tc, double* F) {
   const double L = f.length, lam = f.period_length;
   if (d > L / 2. + shift || d < -L / 2. + shift) return;
   const double s = sin(2.0 * kPiD * (d - shift) / lam);
-  double k = 1.0;  // 1/4 and 3/4 end poles (src/TField3D_IdealUndulator.cc:125-142)
-  if (d < -L / 2. + shift + lam || d > L / 2. + shift - lam)
-    k = (d < -L / 2. + shift + lam / 2. || d > L / 2. + shift - lam / 2.) ? 0.25 : 0.75;
-  F[0] += amp[0] * k * s * tc;
-  F[1] += amp[1] * k * s * tc;
-  F[2] += amp[2] * k * s * tc;
+  if (d < -L / 2. + shift + lam || d > L / 2. + shift - lam) {  // 1/4 and 3/4 end poles
+    const double k = (d < -L / 2. + shift + lam / 2. || d > L / 2. + shift - lam / 2.) ? 0.25 : 0.75;
+    F[0] += amp[0] * k * s * tc;
+    F[1] += amp[1] * k * s * tc;
+    F[2] += amp[2] * k * s * tc;
+    return;
+  }
+  double h = 1.0;
+  if (f.n_half > 0) {  // half-period k of the full-strength region
+    int64_t k = (int64_t)((d - (-L / 2. + shift + lam)) / (lam / 2.));
+    k = k < 0 ? 0 : (k >= f.n_half ? f.n_half - 1 : k);
+    h = vals[f.half_off + k];
+  }
+  F[0] += amp[0] * s * tc * h;
+  F[1] += amp[1] * s * tc * h;
+  F[2] += amp[2] * s * tc * h;
 }
 
-__device__ void field_sum_d(const DevField* __restrict__ fs, int nf, double x, double y, double z, double t,
-                            double* B) {
+// Grid field (src/TField3D_Grid.cc:153-283), the host model's operations.
+__device__ void grid_field_d(const DevField& f, const double* __restrict__ vals, double x, double y, double z,
+                             double t, double* B) {
+  // TVector3D::RotateSelfXYZ with the host's sin / cos of the angles, then the translation
+  double vx = x, vy = y, vz = z, tt;
+  tt = vy; vy = f.rot_cos[0] * tt - f.rot_sin[0] * vz; vz = f.rot_sin[0] * tt + f.rot_cos[0] * vz;
+  tt = vz; vz = f.rot_cos[1] * tt - f.rot_sin[1] * vx; vx = f.rot_sin[1] * tt + f.rot_cos[1] * vx;
+  tt = vx; vx = f.rot_cos[2] * tt - f.rot_sin[2] * vy; vy = f.rot_sin[2] * tt + f.rot_cos[2] * vy;
+  const double p[3] = {vx - f.center[0], vy - f.center[1], vz - f.center[2]};
+  int64_t ni[3] = {0, 0, 0};
+  double di[3] = {0, 0, 0};
+  for (int a = 0; a < 3; ++a) {
+    if (f.grid_n[a] > 1) {
+      if (p[a] <= f.grid_start[a] || p[a] >= f.grid_stop[a]) return;
+      ni[a] = (int64_t)((p[a] - f.grid_start[a]) / f.grid_step[a]);
+      di[a] = (p[a] - f.grid_start[a]) - ni[a] * f.grid_step[a];
+      if (ni[a] > f.grid_n[a] - 2) ni[a] = f.grid_n[a] - 2;
+    }
+  }
+  const double* V = vals + f.grid_off;
+  const int64_t NY = f.grid_n[1], NZ = f.grid_n[2];
+  auto lerp = [&](const double* a0, const double* a1, double d, double step, double* o) {
+    for (int c = 0; c < 3; ++c) o[c] = a0[c] + (a1[c] - a0[c]) * d / step;
+  };
+  auto at = [&](int64_t ix, int64_t iy, int64_t iz) { return V + 3 * (ix * NY * NZ + iy * NZ + iz); };
+  const int64_t nx = ni[0], ny = ni[1], nz = ni[2];
+  double F[3];
+  switch (f.grid_dim) {
+    case kGridXYZ: {
+      double v00[3], v10[3], v01[3], v11[3], v0[3], v1[3];
+      lerp(at(nx, ny, nz), at(nx + 1, ny, nz), di[0], f.grid_step[0], v00);
+      lerp(at(nx, ny + 1, nz), at(nx + 1, ny + 1, nz), di[0], f.grid_step[0], v10);
+      lerp(at(nx, ny, nz + 1), at(nx + 1, ny, nz + 1), di[0], f.grid_step[0], v01);
+      lerp(at(nx, ny + 1, nz + 1), at(nx + 1, ny + 1, nz + 1), di[0], f.grid_step[0], v11);
+      lerp(v00, v10, di[1], f.grid_step[1], v0);
+      lerp(v01, v11, di[1], f.grid_step[1], v1);
+      lerp(v0, v1, di[2], f.grid_step[2], F);
+      break;
+    }
+    case kGridX: lerp(V + 3 * nx, V + 3 * (nx + 1), di[0], f.grid_step[0], F); break;
+    case kGridY: lerp(V + 3 * ny, V + 3 * (ny + 1), di[1], f.grid_step[1], F); break;
+    case kGridZ: lerp(V + 3 * nz, V + 3 * (nz + 1), di[2], f.grid_step[2], F); break;
+    case kGridXY: {
+      double v0[3], v1[3];
+      lerp(at(nx, ny, 0), at(nx + 1, ny, 0), di[0], f.grid_step[0], v0);
+      lerp(at(nx, ny + 1, 0), at(nx + 1, ny + 1, 0), di[0], f.grid_step[0], v1);
+      lerp(v0, v1, di[1], f.grid_step[1], F);
+      break;
+    }
+    case kGridXZ: {
+      double v0[3], v1[3];
+      lerp(at(nx, 0, nz), at(nx + 1, 0, nz), di[0], f.grid_step[0], v0);
+      lerp(at(nx, 0, nz + 1), at(nx + 1, 0, nz + 1), di[0], f.grid_step[0], v1);
+      lerp(v0, v1, di[2], f.grid_step[2], F);
+      break;
+    }
+    default: {
+      double v0[3], v1[3];
+      lerp(at(0, ny, nz), at(0, ny + 1, nz), di[1], f.grid_step[1], v0);
+      lerp(at(0, ny, nz + 1), at(0, ny + 1, nz + 1), di[1], f.grid_step[1], v1);
+      lerp(v0, v1, di[2], f.grid_step[2], F);
+      break;
+    }
+  }
+  const double w = cos(2.0 * kPiD * f.frequency * (t + f.time_offset) + f.frequency_phase);
+  B[0] += F[0] * w;
+  B[1] += F[1] * w;
+  B[2] += F[2] * w;
+}
+
+__device__ void field_sum_d(const DevField* __restrict__ fs, int nf, const double* __restrict__ vals, double x,
+                            double y, double z, double t, double* B) {
   B[0] = B[1] = B[2] = 0;
   for (int i = 0; i < nf; ++i) {
     const DevField& f = fs[i];
+    if (f.kind == 2) {
+      grid_field_d(f, vals, x, y, z, t, B);
+      continue;
+    }
     const double d = (x - f.center[0]) * f.period_unit[0] + (y - f.center[1]) * f.period_unit[1] +
                      (z - f.center[2]) * f.period_unit[2];
     const double tc = 1 + d * f.taper;
     double F[3] = {0, 0, 0};
     if (f.kind == 0) {
-      pole_block_d(f, f.a, d, f.phase * f.period_mag / (2.0 * kPiD), tc, F);
+      pole_block_d(f, vals, f.a, d, f.phase * f.period_mag / (2.0 * kPiD), tc, F);
     } else {  // EPU: A shifted by +phase/2, B by -phase/2 (src/TField3D_IdealEPU.cc:127-165)
-      pole_block_d(f, f.a, d, f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
-      pole_block_d(f, f.b, d, -f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
+      pole_block_d(f, vals, f.a, d, f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
+      pole_block_d(f, vals, f.b, d, -f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
     }
     const double w = f.frequency == 0 ? 1.0 : cos(2.0 * kPiD * f.frequency * (t + f.time_offset) + f.frequency_phase);
     B[0] += F[0] * w;
@@ -73,6 +157,7 @@ __device__ void field_sum_d(const DevField* __restrict__ fs, int nf, double x, d
 struct Rk4Ctx {
   const DevField* fs;
   int nf;
+  const double* vals;
   double qomg;
   bool superluminal;
 };
@@ -84,7 +169,7 @@ __device__ __forceinline__ void derivs_d(Rk4Ctx& c, double t, const double* x, d
     return;
   }
   double B[3];
-  field_sum_d(c.fs, c.nf, x[0], x[2], x[4], t, B);
+  field_sum_d(c.fs, c.nf, c.vals, x[0], x[2], x[4], t, B);
   dxdt[0] = x[1];
   dxdt[1] = c.qomg * (-x[5] * B[1] + x[3] * B[2]);
   dxdt[2] = x[3];
@@ -112,14 +197,15 @@ __device__ __forceinline__ void rk4_step_d(Rk4Ctx& c, double* y, const double* d
 // [0, nb) in time order; each point carries the acceleration of the state before it, as the
 // reference's integrator stores it (src/OSCARSSR.cc:930-1004).
 __global__ void k_batch_rk4(const DevJob* __restrict__ jobs, int njobs, const DevField* __restrict__ fields,
-                            double* __restrict__ arena, unsigned* __restrict__ err) {
+                            const double* __restrict__ field_vals, double* __restrict__ arena,
+                            unsigned* __restrict__ err) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 2 * njobs) return;
   const DevJob& J = jobs[t >> 1];
   const bool fwd = (t & 1) == 0;
   const int64_t n = (int64_t)J.nf + J.nb;
   double* K = arena + J.knots;
-  Rk4Ctx c{fields + J.field_begin, J.field_count, J.qomg, false};
+  Rk4Ctx c{fields + J.field_begin, J.field_count, field_vals, J.qomg, false};
   const double* x0 = J.frame.x0;
   double x[6] = {x0[0], J.b0[0] * kCLight, x0[1], J.b0[1] * kCLight, x0[2], J.b0[2] * kCLight};
   double dxdt[6] = {0, 0, 0, 0, 0, 0};
@@ -643,10 +729,36 @@ constexpr int kBatchPrefill = 13;        // levels enqueued without the host (re
 constexpr int kBatchMinSpan = 32;
 constexpr int kBatchMaxJobsPerChunk = 4096;
 
-DevField to_dev_field(FieldSpec f) {
+DevField to_dev_field(FieldSpec f, std::vector<double>& vals) {
   f.finish();
   DevField d;
   std::memset(&d, 0, sizeof d);
+  if (f.kind == 2) {
+    const GridData& g = *f.grid;
+    d.kind = 2;
+    d.grid_dim = g.dimx;
+    for (int a = 0; a < 3; ++a) {
+      d.grid_n[a] = g.n[a];
+      d.grid_start[a] = g.start[a];
+      d.grid_step[a] = g.step[a];
+      d.grid_stop[a] = g.stop[a];
+    }
+    d.grid_off = (int64_t)vals.size();
+    vals.insert(vals.end(), g.v.begin(), g.v.end());
+    const double r[3] = {f.rotations.x, f.rotations.y, f.rotations.z};
+    for (int a = 0; a < 3; ++a) {
+      d.rot_sin[a] = std::sin(r[a]);
+      d.rot_cos[a] = std::cos(r[a]);
+    }
+    d.center[0] = f.center.x; d.center[1] = f.center.y; d.center[2] = f.center.z;
+    d.frequency = f.frequency; d.frequency_phase = f.frequency_phase; d.time_offset = f.time_offset;
+    return d;
+  }
+  if (!f.half_scale.empty()) {
+    d.half_off = (int64_t)vals.size();
+    d.n_half = (int)f.half_scale.size();
+    vals.insert(vals.end(), f.half_scale.begin(), f.half_scale.end());
+  }
   d.kind = f.kind;
   d.nperiods = f.nperiods;
   const Vec3 a = f.a, b = f.b, c = f.center, u = f.period_unit;
@@ -751,9 +863,14 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
   check(cudaSetDevice(device), "cudaSetDevice");
   cudaStream_t st = stream;
   std::vector<DevField> df;
-  for (const FieldSpec& f : fields) df.push_back(to_dev_field(f));
+  std::vector<double> fvals;
+  for (const FieldSpec& f : fields) df.push_back(to_dev_field(f, fvals));
   if (df.empty()) df.push_back(DevField{});
+  if (fvals.empty()) fvals.push_back(0.0);
   b_fields_.reserve(sizeof(DevField) * df.size());
+  b_fvals_.reserve(sizeof(double) * fvals.size());
+  check(cudaMemcpyAsync(b_fvals_.p, fvals.data(), sizeof(double) * fvals.size(), cudaMemcpyHostToDevice, st),
+        "field values");
   b_obs_.reserve(sizeof(double) * 3 * n_obs_total);
   b_omega_.reserve(sizeof(double) * n_omega_total);
   // stream-ordered copies (pageable sources are staged before the calls return)
@@ -859,7 +976,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     auto front = [&](int v, bool tune) {
       check(cudaMemsetAsync(misc, 0, 64, st), "memset");
       dev::k_batch_rk4<<<(2 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_fields_.as<DevField>(),
-                                                          b_knots_.as<double>(), misc);
+                                                          b_fvals_.as<double>(), b_knots_.as<double>(), misc);
       dev::k_batch_extent<<<nj, 256, 0, st>>>(d_jobs, b_knots_.as<double>());
       dev::k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_knots_.as<double>(), b_work_.as<double>());
       const int64_t fill_n = (rec_per_job - 1) * nj;

@@ -10,13 +10,23 @@
 
 namespace osc {
 
-// Ideal undulator / EPU on the device (FieldSpec after finish()).
+// A field source on the device (FieldSpec after finish()).
 struct DevField {
-  int kind;                 // 0 undulator, 1 EPU
+  int kind;                 // 0 undulator, 1 EPU, 2 grid
   int nperiods;
   double a[3], b[3], center[3], period_unit[3];
   double phase, taper, frequency, frequency_phase, time_offset;
   double period_length, period_mag, length;
+  // undulator half-period factors: n_half values at half_off of the batch's value array (0: none)
+  int64_t half_off;
+  int n_half;
+  // grid: points, start / step / stop per axis, dimension code, values (3 per point) at grid_off,
+  // sin and cos of the rotation angles (computed on the host, as the host model computes them)
+  int grid_dim;
+  int64_t grid_n[3];
+  double grid_start[3], grid_step[3], grid_stop[3];
+  int64_t grid_off;
+  double rot_sin[3], rot_cos[3];
 };
 
 struct DevJob {

@@ -143,6 +143,12 @@ OSC_API int osc_clear_fields(osc_ctx* ctx) {
 
 osc::FieldSpec field_from_desc(const osc_field_desc* f) {
   if (!f) throw osc::Error{OSC_ERR_INVALID, "field descriptor is NULL"};
+  if (f->kind == OSC_FIELD_GRID) {
+    if (!f->grid_values) throw osc::Error{OSC_ERR_INVALID, "grid field without values"};
+    const int64_t n[3] = {f->grid_n[0], f->grid_n[1], f->grid_n[2]};
+    return osc::grid_from_values(n, f->grid_start, f->grid_step, f->grid_values, V3(f->rotations), V3(f->center),
+                                 f->frequency, f->frequency_phase, f->time_offset);
+  }
   if (f->kind != OSC_FIELD_UNDULATOR && f->kind != OSC_FIELD_EPU) throw osc::Error{OSC_ERR_INVALID, "unknown field kind"};
   osc::FieldSpec s;
   s.kind = f->kind;
@@ -156,11 +162,29 @@ osc::FieldSpec field_from_desc(const osc_field_desc* f) {
   s.frequency = f->frequency;
   s.frequency_phase = f->frequency_phase;
   s.time_offset = f->time_offset;
+  if (f->half_period_scale && f->n_half_periods > 0) {
+    if (f->kind != OSC_FIELD_UNDULATOR) throw osc::Error{OSC_ERR_INVALID, "half-period factors apply to undulators"};
+    if (f->n_half_periods != 2 * f->nperiods)
+      throw osc::Error{OSC_ERR_LENGTH, "n_half_periods must be 2 * nperiods"};
+    s.half_scale.assign(f->half_period_scale, f->half_period_scale + f->n_half_periods);
+  }
   return s;
 }
 
 OSC_API int osc_add_field(osc_ctx* ctx, const osc_field_desc* f) {
   return guarded(ctx, [&] { ctx->eng->model.add_field(field_from_desc(f)); });
+}
+
+OSC_API int osc_add_field_file(osc_ctx* ctx, const char* path, const char* format, const double rotations[3],
+                               const double translation[3], const double* scaling, int n_scaling, double frequency,
+                               double frequency_phase, double time_offset) {
+  return guarded(ctx, [&] {
+    if (!path || !format) throw osc::Error{OSC_ERR_INVALID, "path and format are required"};
+    if (n_scaling < 0 || (n_scaling > 0 && !scaling)) throw osc::Error{OSC_ERR_INVALID, "bad scaling"};
+    std::vector<double> sc(scaling, scaling + n_scaling);
+    ctx->eng->model.add_field(osc::grid_from_file(path, format, V3(rotations), V3(translation), sc, frequency,
+                                                  frequency_phase, time_offset));
+  });
 }
 
 OSC_API int osc_get_bfield(osc_ctx* ctx, const double x[3], double t, double out[3]) {

@@ -149,7 +149,7 @@ class Engine {
  private:
 
   // batched path
-  DevBuf b_fields_, b_obs_, b_omega_, b_acc_, b_jobs_, b_knots_, b_work_, b_rec_, b_rec_ext_, b_state_, b_out_,
+  DevBuf b_fields_, b_fvals_, b_obs_, b_omega_, b_acc_, b_jobs_, b_knots_, b_work_, b_rec_, b_rec_ext_, b_state_, b_out_,
       b_lvl_, b_act_[2], b_part_, b_plan_, b_cnt_;
   cudaGraphExec_t graph_exec_ = nullptr;
   long long graph_launches_ = 0;

@@ -3,8 +3,11 @@
 #include "host_core.h"
 
 #include <algorithm>
+#include <array>
 #include <cctype>
 #include <cmath>
+#include <fstream>
+#include <sstream>
 #include <thread>
 
 #include "../../include/oscars_b200.h"
@@ -48,12 +51,15 @@ Vec3 rotate_xyz(Vec3 v, Vec3 r) {  // TVector3D::RotateSelfX, Y, Z in that order
 // Fields
 // ---------------------------------------------------------------------------------------------
 void FieldSpec::finish() {  // TField3D_IdealUndulator::Init :94-98
+  if (kind == 2) return;
   period_length = mag(period);
   period_unit = unit(period);
   length = mag(period) * (nperiods + 2);
 }
 
-// One sinusoidal block with 1/4 and 3/4 end poles (src/TField3D_IdealUndulator.cc:125-142).
+// One sinusoidal block with 1/4 and 3/4 end poles (src/TField3D_IdealUndulator.cc:125-142).  With
+// half-period factors, the full-strength region [-L/2 + shift + lam, L/2 + shift - lam] (2 N
+// half-periods between zeros of the sine) is scaled per half-period.
 static Vec3 pole_block(const FieldSpec& f, Vec3 amp, double d, double shift, double taper_corr) {
   const double L = f.length, lam = f.period_length;
   if (d > L / 2. + shift || d < -L / 2. + shift) return Vec3{};
@@ -63,10 +69,79 @@ static Vec3 pole_block(const FieldSpec& f, Vec3 amp, double d, double shift, dou
       return amp * 0.25 * s * taper_corr;
     return amp * 0.75 * s * taper_corr;
   }
-  return amp * s * taper_corr;
+  if (f.half_scale.empty()) return amp * s * taper_corr;
+  const int64_t nh = (int64_t)f.half_scale.size();
+  int64_t k = (int64_t)((d - (-L / 2. + shift + lam)) / (lam / 2.));
+  k = k < 0 ? 0 : (k >= nh ? nh - 1 : k);
+  return amp * s * taper_corr * f.half_scale[k];
+}
+
+// Grid interpolation (src/TField3D_Grid.cc:153-283): rotate, translate, zero outside the grid,
+// multilinear interpolation v0 + d (v1 - v0) / step per axis, times the time factor.
+static inline Vec3 grid_at(const GridData& g, int64_t i) { return v3(g.v[3 * i], g.v[3 * i + 1], g.v[3 * i + 2]); }
+static inline Vec3 lerp_step(Vec3 v0, Vec3 v1, double d, double step) { return v0 + (v1 - v0) * d / step; }
+
+static Vec3 grid_value(const FieldSpec& f, Vec3 xin, double t) {
+  const GridData& g = *f.grid;
+  Vec3 X = rotate_xyz(xin, f.rotations);
+  X = X - f.center;
+  const double p[3] = {X.x, X.y, X.z};
+  int64_t ni[3] = {0, 0, 0};
+  double di[3] = {0, 0, 0};
+  for (int a = 0; a < 3; ++a) {
+    if (g.n[a] > 1) {
+      if (p[a] <= g.start[a] || p[a] >= g.stop[a]) return Vec3{};
+      ni[a] = (int64_t)((p[a] - g.start[a]) / g.step[a]);
+      di[a] = (p[a] - g.start[a]) - ni[a] * g.step[a];
+      // the reference would read one past its data if rounding put a point just below the stop
+      // into the last cell; clamp to the last cell instead
+      if (ni[a] > g.n[a] - 2) ni[a] = g.n[a] - 2;
+    }
+  }
+  const int64_t NY = g.n[1], NZ = g.n[2];
+  auto idx = [&](int64_t ix, int64_t iy, int64_t iz) { return ix * NY * NZ + iy * NZ + iz; };
+  const int64_t nx = ni[0], ny = ni[1], nz = ni[2];
+  const double dx = di[0], dy = di[1], dz = di[2];
+  Vec3 F;
+  switch (g.dimx) {
+    case kGridXYZ: {
+      const Vec3 v00 = lerp_step(grid_at(g, idx(nx, ny, nz)), grid_at(g, idx(nx + 1, ny, nz)), dx, g.step[0]);
+      const Vec3 v10 = lerp_step(grid_at(g, idx(nx, ny + 1, nz)), grid_at(g, idx(nx + 1, ny + 1, nz)), dx, g.step[0]);
+      const Vec3 v01 = lerp_step(grid_at(g, idx(nx, ny, nz + 1)), grid_at(g, idx(nx + 1, ny, nz + 1)), dx, g.step[0]);
+      const Vec3 v11 = lerp_step(grid_at(g, idx(nx, ny + 1, nz + 1)), grid_at(g, idx(nx + 1, ny + 1, nz + 1)), dx,
+                                 g.step[0]);
+      const Vec3 v0 = lerp_step(v00, v10, dy, g.step[1]);
+      const Vec3 v1 = lerp_step(v01, v11, dy, g.step[1]);
+      F = lerp_step(v0, v1, dz, g.step[2]);
+      break;
+    }
+    case kGridX: F = lerp_step(grid_at(g, nx), grid_at(g, nx + 1), dx, g.step[0]); break;
+    case kGridY: F = lerp_step(grid_at(g, ny), grid_at(g, ny + 1), dy, g.step[1]); break;
+    case kGridZ: F = lerp_step(grid_at(g, nz), grid_at(g, nz + 1), dz, g.step[2]); break;
+    case kGridXY: {
+      const Vec3 v0 = lerp_step(grid_at(g, idx(nx, ny, 0)), grid_at(g, idx(nx + 1, ny, 0)), dx, g.step[0]);
+      const Vec3 v1 = lerp_step(grid_at(g, idx(nx, ny + 1, 0)), grid_at(g, idx(nx + 1, ny + 1, 0)), dx, g.step[0]);
+      F = lerp_step(v0, v1, dy, g.step[1]);
+      break;
+    }
+    case kGridXZ: {
+      const Vec3 v0 = lerp_step(grid_at(g, idx(nx, 0, nz)), grid_at(g, idx(nx + 1, 0, nz)), dx, g.step[0]);
+      const Vec3 v1 = lerp_step(grid_at(g, idx(nx, 0, nz + 1)), grid_at(g, idx(nx + 1, 0, nz + 1)), dx, g.step[0]);
+      F = lerp_step(v0, v1, dz, g.step[2]);
+      break;
+    }
+    default: {  // kGridYZ
+      const Vec3 v0 = lerp_step(grid_at(g, idx(0, ny, nz)), grid_at(g, idx(0, ny + 1, nz)), dy, g.step[1]);
+      const Vec3 v1 = lerp_step(grid_at(g, idx(0, ny, nz + 1)), grid_at(g, idx(0, ny + 1, nz + 1)), dy, g.step[1]);
+      F = lerp_step(v0, v1, dz, g.step[2]);
+      break;
+    }
+  }
+  return F * std::cos(two_pi() * f.frequency * (t + f.time_offset) + f.frequency_phase);
 }
 
 Vec3 field_value(const FieldSpec& f, Vec3 x, double t) {
+  if (f.kind == 2) return grid_value(f, x, t);
   const double d = dot(x - f.center, f.period_unit);
   const double taper_corr = 1 + d * f.taper;
   Vec3 F;
@@ -78,6 +153,218 @@ Vec3 field_value(const FieldSpec& f, Vec3 x, double t) {
   }
   if (f.frequency == 0) return F;
   return F * std::cos(two_pi() * f.frequency * (t + f.time_offset) + f.frequency_phase);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Grid fields from files (src/TField3D_Grid.cc:365-530 OSCARS, :572-870 OSCARS1D)
+// ---------------------------------------------------------------------------------------------
+static int grid_dimx(const GridData& g) {
+  const bool hx = g.n[0] > 1, hy = g.n[1] > 1, hz = g.n[2] > 1;
+  if (hx && hy && hz) return kGridXYZ;
+  if (hx && hy) return kGridXY;
+  if (hx && hz) return kGridXZ;
+  if (hy && hz) return kGridYZ;
+  if (hx) return kGridX;
+  if (hy) return kGridY;
+  if (hz) return kGridZ;
+  throw Error{OSC_ERR_RANGE, "invalid dimensions"};
+}
+
+static FieldSpec grid_spec(std::shared_ptr<GridData> g, Vec3 rotations, Vec3 translation, double frequency,
+                           double frequency_phase, double time_offset) {
+  FieldSpec f;
+  f.kind = 2;
+  f.rotations = rotations;
+  f.center = translation;
+  f.frequency = frequency;
+  f.frequency_phase = frequency_phase;
+  f.time_offset = time_offset;
+  f.grid = std::move(g);
+  return f;
+}
+
+static double header_value(const std::string& line) {  // GetHeaderValue: first number on the line
+  std::istringstream S(line);
+  double v = 0;
+  S >> v;
+  if (S.bad()) throw Error{OSC_ERR_INVALID, "cannot read header value"};
+  return v;
+}
+
+static FieldSpec read_oscars_grid(const std::string& path, Vec3 rot, Vec3 trans, const std::vector<double>& sc,
+                                  double fr, double fp, double to) {
+  std::ifstream fi(path);
+  if (!fi) throw Error{OSC_ERR_INVALID, "cannot open file for reading"};
+  std::string L;
+  std::getline(fi, L);  // comment
+  double hv[9];
+  for (int i = 0; i < 9; ++i) {
+    std::getline(fi, L);
+    hv[i] = header_value(L);
+  }
+  const double xs_in = hv[0], xst_in = hv[1], ys_in = hv[3], yst_in = hv[4], zs_in = hv[6], zst_in = hv[7];
+  const int NX = (int)hv[2], NY = (int)hv[5], NZ = (int)hv[8];
+  const double XStep = sc.size() > 0 ? xst_in * sc[0] : xst_in;
+  const double YStep = sc.size() > 1 ? yst_in * sc[1] : yst_in;
+  const double ZStep = sc.size() > 2 ? zst_in * sc[2] : zst_in;
+  const double FxS = sc.size() > 3 ? sc[3] : 1, FyS = sc.size() > 4 ? sc[4] : 1, FzS = sc.size() > 5 ? sc[5] : 1;
+  const double MiddleX = xs_in + xst_in * (NX - 1) / 2., XStart = MiddleX - XStep * (NX - 1) / 2.;
+  const double MiddleY = ys_in + yst_in * (NY - 1) / 2., YStart = MiddleY - YStep * (NY - 1) / 2.;
+  const double MiddleZ = zs_in + zst_in * (NZ - 1) / 2., ZStart = MiddleZ - ZStep * (NZ - 1) / 2.;
+  if (NX < 1 || NY < 1 || NZ < 1) throw Error{OSC_ERR_RANGE, "invalid number of points in at least one dimension"};
+  auto g = std::make_shared<GridData>();
+  g->n[0] = NX; g->n[1] = NY; g->n[2] = NZ;
+  g->start[0] = XStart; g->start[1] = YStart; g->start[2] = ZStart;
+  g->step[0] = XStep; g->step[1] = YStep; g->step[2] = ZStep;
+  for (int a = 0; a < 3; ++a) g->stop[a] = g->start[a] + (g->n[a] - 1) * g->step[a];
+  g->dimx = grid_dimx(*g);
+  g->v.reserve(3 * (size_t)NX * NY * NZ);
+  std::istringstream S;
+  for (int ix = 0; ix != NX; ++ix)
+    for (int iy = 0; iy != NY; ++iy)
+      for (int iz = 0; iz != NZ; ++iz) {
+        std::getline(fi, L);
+        if (fi.eof()) throw Error{OSC_ERR_INVALID, "error reading file.  Check format"};
+        double fx, fy, fz;
+        S.clear();
+        S.str(L);
+        S >> fx >> fy >> fz;
+        if (FxS != 1) fx *= FxS;
+        if (FyS != 1) fy *= FyS;
+        if (FzS != 1) fz *= FzS;
+        if (S.fail()) throw Error{OSC_ERR_INVALID, "error reading file.  Check format"};
+        const Vec3 F = rotate_xyz(v3(fx, fy, fz), rot);
+        g->v.push_back(F.x);
+        g->v.push_back(F.y);
+        g->v.push_back(F.z);
+      }
+  return grid_spec(g, rot, trans, fr, fp, to);
+}
+
+static FieldSpec read_oscars1d_grid(const std::string& path, const std::string& format, Vec3 rot, Vec3 trans,
+                                    const std::vector<double>& sc, double fr, double fp, double to, char comment) {
+  std::ifstream fi(path);
+  if (!fi) throw Error{OSC_ERR_INVALID, "cannot open file for reading"};
+  int order[4] = {-1, -1, -1, -1};
+  std::istringstream fs(std::string(format.begin() + 8, format.end()));
+  std::string c, axis;
+  int index = 0, xdim = 0, fdim = 0;
+  bool has[4] = {false, false, false, false};
+  while (fs >> c) {
+    if (index > 3) throw Error{OSC_ERR_RANGE, "spatial or B-field dimensions are too large(index>3)"};
+    if (c == "X" || c == "Y" || c == "Z") {
+      axis = c;
+      ++xdim;
+      order[index++] = 0;
+    } else if (c == "Bx" || c == "Ex" || c == "Fx") {
+      has[1] = true; ++fdim; order[index++] = 1;
+    } else if (c == "By" || c == "Ey" || c == "Fy") {
+      has[2] = true; ++fdim; order[index++] = 2;
+    } else if (c == "Bz" || c == "Ez" || c == "Fz") {
+      has[3] = true; ++fdim; order[index++] = 3;
+    } else {
+      throw Error{OSC_ERR_INVALID, "only excepts X Y Z Bx By Bz"};
+    }
+  }
+  const int count = xdim + fdim;
+  if (xdim != 1) throw Error{OSC_ERR_RANGE, "spatial or B-field dimensions are too large"};
+  std::string L;
+  std::getline(fi, L);  // comment line
+  std::vector<std::array<double, 4>> in;
+  std::istringstream S;
+  while (std::getline(fi, L)) {
+    const size_t first = L.find_first_not_of(" \t");
+    if (first == std::string::npos || L[first] == comment) continue;
+    std::replace(L.begin(), L.end(), ',', ' ');
+    S.clear();
+    S.str(L);
+    double val[4] = {0, 0, 0, 0};
+    for (int i = 0; i < count; ++i) {
+      S >> val[order[i]];
+      if (S.fail()) throw Error{OSC_ERR_LENGTH, "something is incorrect with data format or iformat string"};
+    }
+    for (size_t i = 0; i != sc.size() && i < 4; ++i) {
+      if (order[i] < 0) continue;
+      val[order[i]] *= sc[i];
+    }
+    in.push_back({val[0], val[1], val[2], val[3]});
+  }
+  std::sort(in.begin(), in.end(), [](const std::array<double, 4>& A, const std::array<double, 4>& B) { return A[0] < B[0]; });
+  if (in.size() < 2) throw Error{OSC_ERR_LENGTH, "not enough data points"};
+  const double First = in.front()[0], Last = in.back()[0];
+  const size_t kPointsPerMeter = 10000;
+  const size_t NPoints = (size_t)((Last - First) * kPointsPerMeter);
+  const double Step = (Last - First) / (double)(NPoints - 1);
+  auto g = std::make_shared<GridData>();
+  const int ax = axis == "X" ? 0 : axis == "Y" ? 1 : 2;
+  g->n[ax] = (int64_t)NPoints;
+  g->start[ax] = First;
+  g->stop[ax] = Last;
+  g->step[ax] = Step;
+  g->dimx = grid_dimx(*g);
+  g->v.reserve(3 * NPoints);
+  size_t min_bin = 0, after = 0, before = 0;
+  for (size_t i = 0; i != NPoints; ++i) {
+    const double z = i * Step + First;
+    for (size_t j = min_bin + 1; j != in.size(); ++j) {
+      if (in[j][0] > z) {
+        after = j;
+        before = j - 1;
+        min_bin = j - 1;
+        break;
+      }
+    }
+    double nb[3];
+    for (int k = 0; k < 3; ++k) {
+      const double slope = !has[k + 1] ? 0 : (in[after][k + 1] - in[before][k + 1]) / (in[after][0] - in[before][0]);
+      nb[k] = !has[k + 1] ? 0 : in[before][k + 1] + (z - in[before][0]) * slope;
+    }
+    const Vec3 F = rotate_xyz(v3(nb[0], nb[1], nb[2]), rot);
+    g->v.push_back(F.x);
+    g->v.push_back(F.y);
+    g->v.push_back(F.z);
+  }
+  return grid_spec(g, rot, trans, fr, fp, to);
+}
+
+FieldSpec grid_from_file(const std::string& path, const std::string& format, Vec3 rotations, Vec3 translation,
+                         const std::vector<double>& scaling, double frequency, double frequency_phase,
+                         double time_offset, char comment) {
+  std::string F = format;
+  std::transform(F.begin(), F.end(), F.begin(), ::toupper);
+  // OSCARSSR::AddMagneticField (src/OSCARSSR.cc:70-103) accepts these format names
+  const bool is1d = F.size() > 8 && F.compare(0, 8, "OSCARS1D") == 0;
+  if (!(F == "OSCARS" || F == "SRW" || F == "SPECTRA" || F == "BINARY" || is1d))
+    throw Error{OSC_ERR_INVALID, "Incorrect format in format string"};
+  if (F == "OSCARS") return read_oscars_grid(path, rotations, translation, scaling, frequency, frequency_phase, time_offset);
+  if (is1d)
+    return read_oscars1d_grid(path, format, rotations, translation, scaling, frequency, frequency_phase, time_offset,
+                              comment);
+  throw Error{OSC_ERR_INVALID, "grid file format " + F + " is not supported by this build (OSCARS and OSCARS1D are)"};
+}
+
+FieldSpec grid_from_values(const int64_t n[3], const double start[3], const double step[3], const double* values,
+                           Vec3 rotations, Vec3 translation, double frequency, double frequency_phase,
+                           double time_offset) {
+  auto g = std::make_shared<GridData>();
+  for (int a = 0; a < 3; ++a) {
+    if (n[a] < 1) throw Error{OSC_ERR_RANGE, "invalid number of points in at least one dimension"};
+    if (n[a] > 1 && !(step[a] > 0)) throw Error{OSC_ERR_RANGE, "grid steps must be positive"};
+    g->n[a] = n[a];
+    g->start[a] = start[a];
+    g->step[a] = n[a] > 1 ? step[a] : 0;
+    g->stop[a] = g->start[a] + (g->n[a] - 1) * g->step[a];
+  }
+  g->dimx = grid_dimx(*g);
+  const int64_t N = n[0] * n[1] * n[2];
+  g->v.resize(3 * N);
+  for (int64_t i = 0; i < N; ++i) {
+    const Vec3 F = rotate_xyz(v3(values[3 * i], values[3 * i + 1], values[3 * i + 2]), rotations);
+    g->v[3 * i] = F.x;
+    g->v[3 * i + 1] = F.y;
+    g->v[3 * i + 2] = F.z;
+  }
+  return grid_spec(g, rotations, translation, frequency, frequency_phase, time_offset);
 }
 
 Vec3 field_sum(const std::vector<FieldSpec>& fields, Vec3 x, double t) {  // TFieldContainer::GetF

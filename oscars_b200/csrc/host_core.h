@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <random>
 #include <string>
 #include <vector>
@@ -49,16 +50,42 @@ Vec3 orthogonal(Vec3 a);
 Vec3 rotate_about(Vec3 v, double angle, Vec3 axis);  // TVector3D::RotateSelf
 Vec3 rotate_xyz(Vec3 v, Vec3 r);                       // TVector3D::RotateSelfXYZ
 
-// One magnetic field source; `kind` 0 = ideal planar undulator, 1 = ideal EPU.
+// Field values on a regular 1-3D grid (TField3D_Grid): n[a] points along axis a from start[a] in
+// steps step[a] up to stop[a]; v holds the (already rotated) field vectors, 3 doubles per point, at
+// index ix * n[1] * n[2] + iy * n[2] + iz.  dimx: which axes have more than one point.
+enum GridDim { kGridX = 0, kGridY, kGridZ, kGridXY, kGridXZ, kGridYZ, kGridXYZ };
+struct GridData {
+  int64_t n[3] = {1, 1, 1};
+  double start[3] = {0, 0, 0}, step[3] = {0, 0, 0}, stop[3] = {0, 0, 0};
+  int dimx = kGridZ;
+  std::vector<double> v;
+};
+
+// One magnetic field source; `kind` 0 = ideal planar undulator, 1 = ideal EPU, 2 = grid.
 struct FieldSpec {
   int kind = 0;
-  Vec3 a, b, period, center;
+  Vec3 a, b, period, center;   // center: the translation (grid: subtracted after the rotation)
   int nperiods = 0;
   double phase = 0, taper = 0, frequency = 0, frequency_phase = 0, time_offset = 0;
   double period_length = 0, length = 0;
   Vec3 period_unit;
+  // undulator only, optional: amplitude factor of each of the 2 * nperiods half-periods of the
+  // full-strength region (between the end poles); empty = all 1
+  std::vector<double> half_scale;
+  // grid only
+  Vec3 rotations;
+  std::shared_ptr<const GridData> grid;
   void finish();  // derived quantities, TField3D_IdealUndulator::Init
 };
+
+// Grid fields from the reference's text formats (TField3D_Grid::ReadFile, ReadFile_OSCARS1D) and
+// from memory.  Throw osc::Error.
+FieldSpec grid_from_file(const std::string& path, const std::string& format, Vec3 rotations, Vec3 translation,
+                         const std::vector<double>& scaling, double frequency, double frequency_phase,
+                         double time_offset, char comment = '#');
+FieldSpec grid_from_values(const int64_t n[3], const double start[3], const double step[3], const double* values,
+                           Vec3 rotations, Vec3 translation, double frequency, double frequency_phase,
+                           double time_offset);
 
 Vec3 field_value(const FieldSpec& f, Vec3 x, double t);
 Vec3 field_sum(const std::vector<FieldSpec>& fields, Vec3 x, double t);

@@ -134,7 +134,9 @@ class sr:
         self._ctx.call("osc_clear_fields")
 
     def add_bfield_undulator(self, bfield, period, nperiods, phase=0, rotations=[], translation=[], taper=0,
-                             frequency=0, frequency_phase=0, time_offset=0, name=""):
+                             frequency=0, frequency_phase=0, time_offset=0, name="", *, half_period_scale=None):
+        """``half_period_scale`` (this build's extension): 2 * nperiods amplitude factors, one per
+        half-period of the full-strength region between the end poles."""
         f = _vec3(bfield, "bfield")
         p = _vec3(period, "period")
         r = _vec3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
@@ -147,6 +149,59 @@ class sr:
         d.bfield[:] = _rotate_xyz(f, r)
         d.period[:] = _rotate_xyz(p, r)
         d.center[:] = t
+        if half_period_scale is not None:
+            hs = np.ascontiguousarray(np.asarray(half_period_scale, dtype=np.float64).ravel())
+            d.half_period_scale = dptr(hs)
+            d.n_half_periods = int(hs.size)
+        self._ctx.call("osc_add_field", ctypes.byref(d))
+
+    def add_bfield_file(self, ifile="", bifile="", iformat="", rotations=[], translation=[], scale=[], frequency=0,
+                        frequency_phase=0, time_offset=0, name=""):
+        """Grid field from a file (src/OSCARSSR_Python.cc:526-625); formats 'OSCARS' and
+        'OSCARS1D <columns>' (e.g. 'OSCARS1D Z Bx By Bz')."""
+        if len(ifile) and len(bifile):
+            raise ValueError("cannot specify both 'ifile' and 'bifile'")
+        if len(ifile) and not len(iformat):
+            raise ValueError("'iformat' is blank")
+        try:
+            r = _vec3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        except ValueError:
+            raise ValueError("Incorrect format in 'rotations'")
+        try:
+            t = _vec3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
+        except ValueError:
+            raise ValueError("Incorrect format in 'translation'")
+        if len(name) > 0 and name[0] == "_":
+            raise ValueError("'name' cannot begin with '_'.  This is reserved for internal use.  Please pick a different name")
+        path, fmt = (bifile, "BINARY") if len(bifile) else (ifile, iformat)
+        sc = np.ascontiguousarray(np.asarray(list(scale), dtype=np.float64))
+        R, T = np.array(r), np.array(t)
+        try:
+            self._ctx.call("osc_add_field_file", path.encode(), fmt.encode(), dptr(R), dptr(T),
+                           dptr(sc) if sc.size else None, int(sc.size), float(frequency), float(frequency_phase),
+                           float(time_offset))
+        except ValueError as e:
+            raise ValueError("Could not import magnetic field.  Check 'ifile' and 'iformat' are correct (%s)" % e)
+
+    def add_bfield_grid(self, values, npoints, start, step, rotations=[], translation=[], frequency=0,
+                        frequency_phase=0, time_offset=0, name=""):
+        """Grid field from memory (this build's extension): ``values`` has shape
+        (nx, ny, nz, 3) or (nx * ny * nz, 3) in the reference's order (x slowest, z fastest);
+        interpolation and conventions as add_bfield_file."""
+        n = [int(v) for v in npoints]
+        if len(n) != 3:
+            raise ValueError("'npoints' must have 3 entries [nx, ny, nz]")
+        v = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1, 3))
+        if v.shape[0] != n[0] * n[1] * n[2]:
+            raise ValueError("'values' must hold nx * ny * nz field vectors")
+        d = FieldDesc(kind=2, frequency=float(frequency), frequency_phase=float(frequency_phase),
+                      time_offset=float(time_offset))
+        d.grid_n[:] = n
+        d.grid_start[:] = _vec3(start, "start")
+        d.grid_step[:] = _vec3(step, "step")
+        d.grid_values = dptr(v)
+        d.rotations[:] = _vec3(rotations, "rotations") if len(rotations) else [0.0, 0.0, 0.0]
+        d.center[:] = _vec3(translation, "translation") if len(translation) else [0.0, 0.0, 0.0]
         self._ctx.call("osc_add_field", ctypes.byref(d))
 
     def add_bfield_epu(self, period, nperiods, bfieldA=[], bfieldB=[], phase=0, rotations=[], translation=[],

@@ -7,6 +7,10 @@ a 41-period planar undulator (B0 = 0.5 T, 50 mm period) and a 30-period elliptic
 (By = 0.6 T cos, Bx = 0.4 T sin, 57 mm period), both with a 3 GeV electron beam.
 """
 import math
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIELDS = os.path.join(HERE, "fields")
 
 E1_U = 458.9458        # first harmonic of the planar undulator [eV]
 E1_EPU = 179.2558      # first harmonic of the elliptical configuration [eV]
@@ -26,6 +30,86 @@ def traj(n=20001, a=-1.5, b=1.5):
 
 UND_SETUP = [UND, BEAM] + traj()
 EPU_SETUP = [EPU_Y, EPU_X, BEAM] + traj(16001)
+
+
+# ---- grid fields and per-half-period undulator amplitudes --------------------------------------
+def write_field_files():
+    """Write the field files under fields/ (deterministic; the committed copies are what the tests
+    and fixtures read).  und1d.txt: 'OSCARS1D Z By Bx' samples on an irregular z grid; grid3d.txt:
+    an 'OSCARS' 3 x 3 x 241 grid; halfscale_41.txt: 82 half-period amplitude factors 1 + delta,
+    delta ~ N(0, 0.005)."""
+    import numpy as np
+    os.makedirs(FIELDS, exist_ok=True)
+    rng = np.random.default_rng(20240607)
+    n = 1001
+    z = -1.2 + 2.4 * np.arange(n) / (n - 1)
+    z[1:-1] += rng.uniform(-0.3, 0.3, n - 2) * 2.4 / (n - 1)
+    env = 0.5 * (np.tanh((z + 1.05) / 0.02) - np.tanh((z - 1.05) / 0.02))
+    by = 0.5 * np.cos(2 * np.pi * z / 0.05) * env
+    bx = 0.04 * np.sin(2 * np.pi * z / 0.05) * env
+    with open(os.path.join(FIELDS, "und1d.txt"), "w") as f:
+        f.write("# OSCARS1D Z By Bx test field (irregular z, tanh ends)\n")
+        for i in rng.permutation(n):  # unsorted on purpose: the reader sorts
+            f.write("%.15g, %.15g %.15g\n" % (z[i], by[i], bx[i]))
+    nx, ny, nz = 3, 3, 241
+    with open(os.path.join(FIELDS, "grid3d.txt"), "w") as f:
+        f.write("# OSCARS 3D grid test field\n-0.002\n0.002\n%d\n-0.002\n0.002\n%d\n-0.96\n0.008\n%d\n" % (nx, ny, nz))
+        for ix in range(nx):
+            for iy in range(ny):
+                for iz in range(nz):
+                    zz = -0.96 + 0.008 * iz
+                    env = 0.5 * (1 - math.cos(math.pi * iz / (nz - 1)))
+                    f.write("%.10g %.10g %.10g\n" % (0.01 * (ix - 1) * env, 0.4 * math.cos(2 * math.pi * zz / 0.05)
+                                                      * (1 + 0.05 * (iy - 1)) * env, 0.002 * (iz - 120) / 120))
+    d = rng.normal(0.0, 0.005, 82)
+    with open(os.path.join(FIELDS, "halfscale_41.txt"), "w") as f:
+        for v in 1 + d:
+            f.write("%.17g\n" % v)
+
+
+def field_file(name):
+    return os.path.join(FIELDS, name)
+
+
+def halfscale_41():
+    with open(field_file("halfscale_41.txt")) as f:
+        return [float(v) for v in f.read().split()]
+
+
+def halfscale_function(bfield, period, nperiods, phase, half_period_scale):
+    """An undulator with per-half-period amplitude factors as a Python field function (for the
+    reference's add_bfield_function): TField3D_IdealUndulator::GetF's operations in the same order
+    (src/TField3D_IdealUndulator.cc:113-152), the full-strength region's half-period k scaled by
+    half_period_scale[k].  No rotation, translation, taper or time dependence."""
+    mag = math.sqrt(period[0] * period[0] + period[1] * period[1] + period[2] * period[2])
+    pu = [period[0] / mag, period[1] / mag, period[2] / mag]
+    lam = mag
+    L = mag * (nperiods + 2)
+    shift = phase * mag / (2.0 * math.pi)
+    two_pi = 2.0 * math.pi
+    hs = list(half_period_scale)
+    amp = [float(v) for v in bfield]
+
+    def field(x, y, z, t):
+        d = (x - 0.0) * pu[0] + (y - 0.0) * pu[1] + (z - 0.0) * pu[2]
+        tc = 1 + d * 0.0
+        if d > L / 2. + shift or d < -L / 2. + shift:
+            return [0.0, 0.0, 0.0]
+        s = math.sin(two_pi * (d - shift) / lam)
+        if d < -L / 2. + shift + lam or d > L / 2. + shift - lam:
+            k = 0.25 if (d < -L / 2. + shift + lam / 2. or d > L / 2. + shift - lam / 2.) else 0.75
+            return [a * k * s * tc for a in amp]
+        i = int((d - (-L / 2. + shift + lam)) / (lam / 2.))
+        i = 0 if i < 0 else (len(hs) - 1 if i >= len(hs) else i)
+        return [a * s * tc * hs[i] for a in amp]
+    return field
+
+
+GRID1D = ("add_bfield_file", dict(ifile="und1d.txt", iformat="OSCARS1D Z By Bx", translation=[0, 0, 0.01],
+                                  scale=[1, 1.02, 1]))
+GRID3D = ("add_bfield_file", dict(ifile="grid3d.txt", iformat="OSCARS", rotations=[0, 0, 0.002],
+                                  translation=[0.0001, 0, 0], scale=[1, 1, 1, 1, 1.1, 1]))
+HALFSCALE = ("add_bfield_halfscale", dict(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, phase=-math.pi / 2))
 
 CASES = {
     # trajectory of the planar undulator (checked through a subsample plus whole-array sums)
@@ -64,6 +148,16 @@ CASES = {
                         ] + traj(8001, -1.0, 1.2) + [("calculate_spectrum", dict(obs=[0.002, 0.001, 25], energy_range_eV=[50, 1500], npoints=64))],
     "epu_field_spec": [("add_bfield_epu", dict(period=[0, 0, 0.04], nperiods=25, bfieldA=[0, 0.5, 0], bfieldB=[0.5, 0, 0], phase=1.2)), BEAM] + traj(12001, -1.0, 1.0)
                       + [("calculate_spectrum", dict(obs=[0, 0, 20], energy_range_eV=[200, 2000], npoints=60, polarization="cr"))],
+    # grid fields from the reference's text formats (TField3D_Grid)
+    "grid1d_traj": [GRID1D, BEAM] + traj(16001) + [("calculate_trajectory", {})],
+    "grid1d_flux": [GRID1D, BEAM] + traj(16001) + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[11, 11], width=[0.008, 0.008], translation=[0, 0, 30], precision=0, max_level=11))],
+    "grid1d_spec": [GRID1D, BEAM] + traj(16001) + [("calculate_spectrum", dict(obs=[0.0005, 0, 30], energy_range_eV=[300, 600], npoints=40))],
+    "grid3d_traj": [GRID3D, BEAM] + traj(12001, -1.2, 1.2) + [("calculate_trajectory", {})],
+    "grid3d_flux": [GRID3D, BEAM] + traj(12001, -1.2, 1.2) + [("calculate_flux_rectangle", dict(energy_eV=516.0, npoints=[9, 9], width=[0.006, 0.006], translation=[0, 0, 30]))],
+    "grid3d_pd": [GRID3D, BEAM] + traj(12001, -1.2, 1.2) + [("calculate_power_density_rectangle", dict(npoints=[9, 9], width=[0.01, 0.01], translation=[0, 0, 30]))],
+    # 41-period undulator with 82 half-period amplitude factors (the field-tuning configuration)
+    "halfscale_traj": [HALFSCALE, BEAM] + traj() + [("calculate_trajectory", {})],
+    "halfscale_flux": [HALFSCALE, BEAM] + traj() + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[11, 11], width=[0.002, 0.002], translation=[0, 0, 30], precision=0, max_level=11))],
 }
 
 
@@ -77,6 +171,16 @@ def run_case(obj, calls):
             out = obj.set_npoints_trajectory(kw["n"])
         elif name == "set_seed":
             out = obj.set_seed(kw["seed"])
+        elif name == "add_bfield_file":
+            kw = dict(kw, ifile=field_file(kw["ifile"]))
+            out = obj.add_bfield_file(**kw)
+        elif name == "add_bfield_halfscale":
+            hs = halfscale_41()
+            if hasattr(obj, "add_bfield_function"):  # the reference: the same field as a Python function
+                out = obj.add_bfield_function(halfscale_function(kw["bfield"], kw["period"], kw["nperiods"],
+                                                                 kw["phase"], hs))
+            else:
+                out = obj.add_bfield_undulator(half_period_scale=hs, **kw)
         else:
             out = getattr(obj, name)(**kw)
     return out

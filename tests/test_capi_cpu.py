@@ -38,10 +38,13 @@ def test_library_exports_every_declared_symbol():
     assert declared == set(_lib.SIGNATURES), declared ^ set(_lib.SIGNATURES)
 
 
-def test_trajectory_bit_exact_with_reference():
-    g = np.load(os.path.join(GOLDEN, "traj_und.npz"))
+@pytest.mark.parametrize("name", sorted(k for k, v in CASES.items() if v[-1][0] == "calculate_trajectory"))
+def test_trajectory_bit_exact_with_reference(name):
+    """Ideal undulator, grid fields from both text formats, and the half-period-scaled undulator
+    (given to the reference as a Python field function)."""
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
     s = host_sr()
-    run_case(s, CASES["traj_und"])
+    run_case(s, CASES[name])
     a = s.trajectory_array()
     assert a.shape[1] == int(g["n"])
     assert np.array_equal(a[:, g["idx"]], g["sub"])
@@ -101,6 +104,35 @@ def test_spectrum_energy_grid_matches_golden():
     g = np.load(os.path.join(GOLDEN, "spec_und_2000.npz"))
     E = SR._energies(2000, [100, 3000], None)
     assert np.array_equal(E, g["pos"])
+
+
+def test_grid_file_errors():
+    s = host_sr()
+    with pytest.raises(ValueError, match="cannot specify both 'ifile' and 'bifile'"):
+        s.add_bfield_file(ifile="a", bifile="b")
+    with pytest.raises(ValueError, match="'iformat' is blank"):
+        s.add_bfield_file(ifile="a")
+    with pytest.raises(ValueError, match="Could not import magnetic field"):
+        s.add_bfield_file(ifile="/nonexistent/file.txt", iformat="OSCARS")
+    with pytest.raises(ValueError, match="Could not import magnetic field"):
+        s.add_bfield_file(ifile=os.path.join(GOLDEN, "fields", "und1d.txt"), iformat="OSCARS1D Z Q")
+    with pytest.raises(ValueError, match="Could not import magnetic field"):
+        s.add_bfield_file(ifile=os.path.join(GOLDEN, "fields", "und1d.txt"), iformat="TEXT")
+    with pytest.raises(ValueError, match="2 \\* nperiods"):
+        s.add_bfield_undulator(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, half_period_scale=[1.0] * 80)
+
+
+def test_grid_from_memory_matches_file_grid():
+    """add_bfield_grid with the values of an 'OSCARS' file gives the file's field."""
+    from oracle.oracle import read_oscars_grid
+    path = os.path.join(GOLDEN, "fields", "grid3d.txt")
+    n, start, step, stop, vals = read_oscars_grid(path, [0.0, 0.0, 0.0], [])
+    a, b = host_sr(), host_sr()
+    a.add_bfield_file(ifile=path, iformat="OSCARS", translation=[0.0001, 0, 0])
+    b.add_bfield_grid(vals, n, start, step, translation=[0.0001, 0, 0])
+    pts = [[-0.0015 + 1.5e-5 * i, 0.0012 - 1.2e-5 * i, -1.0 + 0.01 * i] for i in range(201)]
+    fa = np.array([a.get_bfield(p) for p in pts])
+    assert np.array_equal(fa, np.array([b.get_bfield(p) for p in pts])) and np.abs(fa).max() > 0.1
 
 
 def test_errors_are_value_errors():

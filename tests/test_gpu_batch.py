@@ -161,3 +161,26 @@ def test_batch_rejects_far_off_axis_observers():
     jobs[1].obs = np.array([[2.0, 0.0, 30.0]])
     with pytest.raises(ValueError, match="compute='fp64'"):
         BatchRunner(0).flux(jobs, compute="mixed", precision=0, max_level=10)
+
+
+def test_batch_grid_and_halfscale_fields_match_fp64():
+    """Device RK4 through a grid field (both text formats) and a half-period-scaled undulator."""
+    from oscars_b200.batch import BatchRunner, Job, grid, undulator
+    from cases import field_file, halfscale_41
+    from oracle.oracle import read_oscars1d_grid, read_oscars_grid
+    n1, s1, st1, _, v1 = read_oscars1d_grid(field_file("und1d.txt"), "OSCARS1D Z By Bx", [0.0, 0.0, 0.0], [1, 1.02, 1])
+    n3, s3, st3, _, v3 = read_oscars_grid(field_file("grid3d.txt"), [0.0, 0.0, 0.0], [1, 1, 1, 1, 1.1, 1])
+    obs = _grid(5, 5, 0.004, 30.0)
+    jobs = [Job(fields=[grid(v1, n1, s1, st1, translation=(0, 0, 0.01))], energy_GeV=3, ctstartstop=(-1.5, 1.5),
+                npoints=16001, obs=obs, energies_eV=[440.0, 459.0]),
+            Job(fields=[grid(v3, n3, s3, st3, rotations=(0, 0, 0.002), translation=(0.0001, 0, 0))], energy_GeV=3,
+                ctstartstop=(-1.2, 1.2), npoints=12001, obs=obs, energies_eV=[516.0]),
+            Job(fields=[undulator([0, 0.5, 0], [0, 0, 0.05], 41, phase=-math.pi / 2, half_period_scale=halfscale_41())],
+                energy_GeV=3, ctstartstop=(-1.5, 1.5), npoints=20001, obs=obs, energies_eV=[458.9458])]
+    r = BatchRunner(0)
+    mx = r.flux(jobs, compute="mixed", precision=0, max_level=11)
+    f64 = r.flux(jobs, compute="fp64", precision=0, max_level=11)
+    for a, b in zip(mx, f64):
+        e = _err(a, b)
+        print("grid/halfscale job: mixed vs fp64 %.3e" % e)
+        assert e <= TOL
