@@ -221,6 +221,29 @@ OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fie
                            const osc_rad_opts* opts, int average, double* out,
                            int32_t* level_out, long long* n_not_converged);
 
+/* ---- differentiation (no reference counterpart: the reference has no gradients) ------------
+ * osc_set_half_period_scale replaces the half-period amplitude factors of field `field_index`
+ * (an undulator added with them; -1 = the one field that has them) and drops the trajectory.
+ * osc_flux_vjp computes, at the fixed level `level` (all samples of levels 0..level, no stop rule),
+ * the flux F of every (observer, energy) entry -- the value osc_flux / osc_spectrum return with
+ * precision 0 and max_level = level -- and grad_half_scale = (dF/ds)^T grad_flux, the gradient of any
+ * loss with dLoss/dF = grad_flux with respect to those factors, by reverse mode through the
+ * radiation sum, the trajectory spline and the RK4 steps (FP64, checkpoints every 256 steps).
+ * Entries are observer-major with energies fastest; spectrum = 1 normalises like osc_spectrum.
+ * grad_knots (may be NULL) receives the gradient with respect to the trajectory knots (9 x n_points,
+ * the layout of osc_trajectory_vjp's knot_grad).
+ * Polarization 'all' only; ideal undulator / EPU fields only; opts->nparticles must be 0. */
+OSC_API int osc_set_half_period_scale(osc_ctx* ctx, int field_index, const double* scale, long long n);
+/* Gradient of sum_j knot_grad . knot_j (knot_grad: 9 x n_points, the layout of osc_get_trajectory
+ * without its time row) with respect to the half-period factors: the trajectory part of the adjoint
+ * on its own (reverse mode through the RK4 steps). */
+OSC_API int osc_trajectory_vjp(osc_ctx* ctx, const double* knot_grad, long long n_points,
+                               double* grad_half_scale, long long n_half);
+OSC_API int osc_flux_vjp(osc_ctx* ctx, const double* obs_xyz, long long n_obs, const double* energies_eV,
+                         long long n_energies, int level, const osc_rad_opts* opts, int spectrum,
+                         const double* grad_flux, double* flux_out, double* grad_half_scale,
+                         long long n_half, double* grad_knots);
+
 /* ---- device-resident variants: same arithmetic, pointers are device memory on the context's
  *      device, work is queued on `stream` (a cudaStream_t, NULL = the context's stream) and the
  *      call returns without synchronising.  Single particle (opts->nparticles must be 0). */

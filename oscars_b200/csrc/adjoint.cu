@@ -1,0 +1,571 @@
+// adjoint.cu -- gradient of a fixed-level flux with respect to the per-half-period amplitude factors
+// of an undulator (reverse mode, FP64).
+//
+// Forward (what is differentiated): the RK4 trajectory through the fields (src/OSCARSSR.cc:910-1009),
+// its clamped spline (include/TOMATH.h:141-203), the level samples s = 1 .. 2^(L+1)-1 of the fixed
+// level L (src/TParticleTrajectoryInterpolated.cc:124-158), and per (observer, energy) entry the
+// complex sum S = sum_s A_s exp(-i w (t_s + D_s/c)), F = C2 |C0 dT_L S|^2 (src/OSCARSSR.cc:4179-4268).
+// Given dLoss/dF per entry, the reverse sweep is:
+//   k_adj_weights      W = 2 C2 (C0 dT)^2 dLoss/dF conj(S) per entry (and F itself)
+//   k_adj_samples      per level sample, sum over entries of d Re(W . A e^{i phi}) / d(X, beta, a/c);
+//                      one thread per sample, entries staged through shared memory
+//   k_adj_spline_eval  sample -> knot values and second derivatives (transpose of the evaluation)
+//   k_adj_spline_solve second derivatives -> knot values (transpose of the tridiagonal sweeps)
+//   k_adj_rk4          knots -> RK4 states -> field amplitudes: one thread per integration direction,
+//                      states recomputed from checkpoints every 256 steps, each step's stages
+//                      recomputed and differentiated in reverse.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "device_common.cuh"
+#include "engine.h"
+#include "fd_common.cuh"
+#include "kernels.h"
+
+namespace osc {
+namespace dev {
+
+constexpr int kCkptStride = 256;
+
+// ---- 1. entry weights ----------------------------------------------------------------------
+// part: first-wave partials of level L with one span ([entry][segment][kFdPartials]).
+__global__ void k_adj_weights(const double* __restrict__ part, int64_t n, const double* __restrict__ grad_flux,
+                              double c0dt, double c2, double* __restrict__ W, double* __restrict__ flux) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double S[6];
+  for (int k = 0; k < 6; ++k) S[k] = part[e * 2 * kFdPartials + k] + part[e * 2 * kFdPartials + kFdPartials + k];
+  double m = 0;
+  for (int k = 0; k < 6; ++k) m += (c0dt * S[k]) * (c0dt * S[k]);
+  flux[e] = c2 * m;
+  const double w = 2.0 * c2 * c0dt * c0dt * grad_flux[e];
+  for (int k = 0; k < 3; ++k) {
+    W[6 * e + 2 * k] = w * S[2 * k];           // Re conj(S)
+    W[6 * e + 2 * k + 1] = -w * S[2 * k + 1];  // Im conj(S)
+  }
+}
+
+// ---- 2. per-sample gradients --------------------------------------------------------------
+constexpr int kAdjThreads = 128;
+constexpr int kAdjStage = 128;
+
+struct AdjEntry {
+  double o[3], w, wr[3], wi[3];
+};
+
+// Reverse mode of A = u k1 - a k2 (u = n - b, k2 = 1/(D om), k1 = k2 / om (g/D + n.a), om = 1 - n.b,
+// g = 1 - b.b, n = R / D, R = O - X) and phi = -w (t + D/c), for J = Re(sum_c W_c A_c e^{i phi}).
+__global__ void __launch_bounds__(kAdjThreads) k_adj_samples(const double* __restrict__ lev, int64_t cap,
+                                                               int64_t s_end, const double* __restrict__ obs,
+                                                               const double* __restrict__ omega, int64_t n_e,
+                                                               const double* __restrict__ W, int64_t n_entries,
+                                                               int64_t entries_per_cta, double* __restrict__ gs) {
+  __shared__ AdjEntry se[kAdjStage];
+  const int64_t s = 1 + (int64_t)blockIdx.x * kAdjThreads + threadIdx.x;
+  const bool live = s < s_end;
+  const int64_t si = live ? s : 1;
+  const double T = lev[si];
+  const double X = lev[cap + si], Y = lev[2 * cap + si], Z = lev[3 * cap + si];
+  const double bx = lev[4 * cap + si], by = lev[5 * cap + si], bz = lev[6 * cap + si];
+  const double ax = lev[7 * cap + si], ay = lev[8 * cap + si], az = lev[9 * cap + si];
+  const double g = 1.0 - (bx * bx + by * by + bz * bz);
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const int64_t e0 = (int64_t)blockIdx.y * entries_per_cta;
+  const int64_t e1 = min(n_entries, e0 + entries_per_cta);
+  for (int64_t base = e0; base < e1; base += kAdjStage) {
+    const int64_t e = base + threadIdx.x;
+    if (threadIdx.x < kAdjStage && e < e1) {
+      const int64_t io = e / n_e, ie = e % n_e;
+      AdjEntry& E = se[threadIdx.x];
+      E.o[0] = obs[3 * io]; E.o[1] = obs[3 * io + 1]; E.o[2] = obs[3 * io + 2];
+      E.w = omega[ie];
+      for (int k = 0; k < 3; ++k) { E.wr[k] = W[6 * e + 2 * k]; E.wi[k] = W[6 * e + 2 * k + 1]; }
+    }
+    __syncthreads();
+    const int cnt = (int)min((int64_t)kAdjStage, e1 - base);
+    if (live) {
+      for (int j = 0; j < cnt; ++j) {
+        const AdjEntry& E = se[j];
+        const double Rx = E.o[0] - X, Ry = E.o[1] - Y, Rz = E.o[2] - Z;
+        const double D = sqrt(Rx * Rx + Ry * Ry + Rz * Rz);
+        const double iD = 1.0 / D;
+        const double nx = Rx * iD, ny = Ry * iD, nz = Rz * iD;
+        const double ux = nx - bx, uy = ny - by, uz = nz - bz;
+        const double om = 1.0 - (nx * bx + ny * by + nz * bz);
+        const double iom = 1.0 / om;
+        const double na = nx * ax + ny * ay + nz * az;
+        const double k2 = iD * iom;
+        const double h = g * iD + na;
+        const double k1 = k2 * iom * h;
+        const double Ax = ux * k1 - ax * k2, Ay = uy * k1 - ay * k2, Az = uz * k1 - az * k2;
+        double sn, cs;
+        sincos(reduce_2pi(-E.w * (T + D / kCLight)), &sn, &cs);
+        const double Px = E.wr[0] * cs - E.wi[0] * sn, Py = E.wr[1] * cs - E.wi[1] * sn, Pz = E.wr[2] * cs - E.wi[2] * sn;
+        const double Qx = E.wr[0] * sn + E.wi[0] * cs, Qy = E.wr[1] * sn + E.wi[1] * cs, Qz = E.wr[2] * sn + E.wi[2] * cs;
+        // reverse sweep
+        const double phb = -(Qx * Ax + Qy * Ay + Qz * Az);
+        double Db = -(E.w / kCLight) * phb;
+        const double ubx = Px * k1, uby = Py * k1, ubz = Pz * k1;
+        const double k1b = Px * ux + Py * uy + Pz * uz;
+        double abx = -Px * k2, aby = -Py * k2, abz = -Pz * k2;
+        double k2b = -(Px * ax + Py * ay + Pz * az);
+        k2b += k1b * iom * h;
+        double iomb = k1b * k2 * h;
+        const double hb = k1b * k2 * iom;
+        const double gb = hb * iD;
+        double iDb = hb * g;
+        const double nab = hb;
+        iDb += k2b * iom;
+        iomb += k2b * iD;
+        const double omb = -iomb * iom * iom;
+        Db += -iDb * iD * iD;
+        double bbx = -2.0 * gb * bx, bby = -2.0 * gb * by, bbz = -2.0 * gb * bz;
+        double nbx = nab * ax, nby = nab * ay, nbz = nab * az;
+        abx += nab * nx; aby += nab * ny; abz += nab * nz;
+        nbx += -omb * bx; nby += -omb * by; nbz += -omb * bz;
+        bbx += -omb * nx; bby += -omb * ny; bbz += -omb * nz;
+        nbx += ubx; nby += uby; nbz += ubz;
+        bbx -= ubx; bby -= uby; bbz -= ubz;
+        const double nbn = nbx * nx + nby * ny + nbz * nz;
+        Db += -nbn * iD;
+        const double Rbx = nbx * iD + Db * nx, Rby = nby * iD + Db * ny, Rbz = nbz * iD + Db * nz;
+        acc[0] -= Rbx; acc[1] -= Rby; acc[2] -= Rbz;
+        acc[3] += bbx; acc[4] += bby; acc[5] += bbz;
+        acc[6] += abx; acc[7] += aby; acc[8] += abz;
+      }
+    }
+    __syncthreads();
+  }
+  if (live)
+    for (int c = 0; c < 9; ++c) atomicAdd(&gs[c * cap + s], acc[c]);
+}
+
+// ---- 3. sample -> knots ---------------------------------------------------------------------
+__global__ void k_adj_spline_eval(const double* __restrict__ knots, int64_t n, double tstart, double tstop,
+                                  int64_t s_end, const double* __restrict__ gs, int64_t cap,
+                                  double* __restrict__ ybar, double* __restrict__ pbar) {
+  const int64_t s = 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= s_end) return;
+  const double* t = knots;
+  const double T = level_time(tstart, tstop, s);
+  int64_t k = (int64_t)((T - t[0]) / (t[n - 1] - t[0]) * (double)(n - 1));
+  k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+  while (k > 0 && t[k] > T) --k;
+  while (k < n - 2 && t[k + 1] <= T) ++k;
+  const double h = t[k + 1] - t[k];
+  const double a = (t[k + 1] - T) / h, b = (T - t[k]) / h;
+  const double ca = (a * a * a - a) * (h * h) / 6.0, cb = (b * b * b - b) * (h * h) / 6.0;
+  for (int c = 0; c < 9; ++c) {
+    const double v = gs[c * cap + s];
+    if (v == 0) continue;
+    atomicAdd(&ybar[c * n + k], a * v);
+    atomicAdd(&ybar[c * n + k + 1], b * v);
+    atomicAdd(&pbar[c * n + k], ca * v);
+    atomicAdd(&pbar[c * n + k + 1], cb * v);
+  }
+}
+
+// ---- 4. second derivatives -> knot values (one thread per component) --------------------------
+// Forward (linear in y): u_0 = 0, u_i = (6 ud_i / (X_{i+1} - X_{i-1}) - sig_i u_{i-1}) / p_i,
+// ypp_{n-1} = -0.5 u_{n-2} / (0.5 diag_{n-2} + 1), ypp_k = diag_k ypp_{k+1} + u_k.
+__global__ void k_adj_spline_solve(const double* __restrict__ knots, int64_t n, double* __restrict__ ybar,
+                                   double* __restrict__ pbar, double* __restrict__ diag_work) {
+  const int c = threadIdx.x;
+  if (c >= 9) return;
+  const double* X = knots;
+  double* diag = diag_work + c * n;
+  double* B = pbar + c * n;  // becomes the adjoint of u in place
+  double* Yb = ybar + c * n;
+  diag[0] = -0.5;
+  for (int64_t i = 1; i < n - 1; ++i) {
+    const double sig = (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]);
+    diag[i] = (sig - 1.) / (sig * diag[i - 1] + 2.0);
+  }
+  for (int64_t k = 0; k <= n - 2; ++k) B[k + 1] += diag[k] * B[k];
+  B[n - 2] += -0.5 / (0.5 * diag[n - 2] + 1.) * B[n - 1];
+  for (int64_t i = n - 2; i >= 1; --i) {
+    const double sig = (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]);
+    const double p = sig * diag[i - 1] + 2.0;
+    const double udb = B[i] * 6.0 / ((X[i + 1] - X[i - 1]) * p);
+    B[i - 1] += -sig / p * B[i];
+    const double hi = X[i + 1] - X[i], hm = X[i] - X[i - 1];
+    Yb[i + 1] += udb / hi;
+    Yb[i] += -udb / hi - udb / hm;
+    Yb[i - 1] += udb / hm;
+  }
+}
+
+// ---- 5. RK4 adjoint ---------------------------------------------------------------------------
+struct AdjFields {
+  const DevField* fs;
+  int nf;
+  const double* vals;
+  int param_field;   // index of the field whose half-period factors are the parameters
+  double qomg;
+  double* pbar;      // gradient of the parameters (n_half of the parameter field)
+};
+
+// Field value at a point, and, when Bb != nullptr, the vector-Jacobian products of B with respect to
+// the position (added to posb) and to the parameter field's half-period factors (added to pbar).
+__device__ void field_vjp(const AdjFields& F, double x, double y, double z, double t, double* B, const double* Bb,
+                          double* posb) {
+  B[0] = B[1] = B[2] = 0;
+  for (int i = 0; i < F.nf; ++i) {
+    const DevField& f = F.fs[i];
+    const double d = (x - f.center[0]) * f.period_unit[0] + (y - f.center[1]) * f.period_unit[1] +
+                     (z - f.center[2]) * f.period_unit[2];
+    const double tc = 1 + d * f.taper;
+    const double w = f.frequency == 0 ? 1.0 : cos(2.0 * kPiD * f.frequency * (t + f.time_offset) + f.frequency_phase);
+    const int nblk = f.kind == 1 ? 2 : 1;
+    for (int blk = 0; blk < nblk; ++blk) {
+      const double* amp = blk == 0 ? f.a : f.b;
+      const double shift = f.kind == 0 ? f.phase * f.period_mag / (2.0 * kPiD)
+                                       : (blk == 0 ? 1.0 : -1.0) * f.phase / 2. * f.period_mag / (2.0 * kPiD);
+      const double L = f.length, lam = f.period_length;
+      if (d > L / 2. + shift || d < -L / 2. + shift) continue;
+      const double th = 2.0 * kPiD * (d - shift) / lam;
+      const double s = sin(th), c = cos(th);
+      double kf = 1.0;
+      int64_t hk = -1;
+      if (d < -L / 2. + shift + lam || d > L / 2. + shift - lam) {
+        kf = (d < -L / 2. + shift + lam / 2. || d > L / 2. + shift - lam / 2.) ? 0.25 : 0.75;
+      } else if (f.n_half > 0) {
+        hk = (int64_t)((d - (-L / 2. + shift + lam)) / (lam / 2.));
+        hk = hk < 0 ? 0 : (hk >= f.n_half ? f.n_half - 1 : hk);
+        kf = F.vals[f.half_off + hk];
+      }
+      const double phi = kf * s * tc;
+      B[0] += amp[0] * phi * w;
+      B[1] += amp[1] * phi * w;
+      B[2] += amp[2] * phi * w;
+      if (Bb) {
+        const double gA = (Bb[0] * amp[0] + Bb[1] * amp[1] + Bb[2] * amp[2]) * w;
+        const double dphi = kf * (c * (2.0 * kPiD / lam) * tc + s * f.taper);
+        posb[0] += gA * dphi * f.period_unit[0];
+        posb[1] += gA * dphi * f.period_unit[1];
+        posb[2] += gA * dphi * f.period_unit[2];
+        if (hk >= 0 && i == F.param_field) atomicAdd(&F.pbar[hk], gA * s * tc);
+      }
+    }
+  }
+}
+
+__device__ void f_eval(const AdjFields& F, double t, const double* y, double* dy) {
+  double B[3];
+  field_vjp(F, y[0], y[2], y[4], t, B, nullptr, nullptr);
+  dy[0] = y[1];
+  dy[1] = F.qomg * (-y[5] * B[1] + y[3] * B[2]);
+  dy[2] = y[3];
+  dy[3] = F.qomg * (y[5] * B[0] - y[1] * B[2]);
+  dy[4] = y[5];
+  dy[5] = F.qomg * (y[1] * B[1] - y[3] * B[0]);
+}
+
+// yb += (df/dy)^T fb at (t, y); parameter gradient accumulated by field_vjp.
+__device__ void f_vjp(const AdjFields& F, double t, const double* y, const double* fb, double* yb) {
+  const double vx = y[1], vy = y[3], vz = y[5];
+  double B[3];
+  const double Bb[3] = {F.qomg * (fb[3] * vz - fb[5] * vy), F.qomg * (-fb[1] * vz + fb[5] * vx),
+                        F.qomg * (fb[1] * vy - fb[3] * vx)};
+  double posb[3] = {0, 0, 0};
+  field_vjp(F, y[0], y[2], y[4], t, B, Bb, posb);
+  yb[0] += posb[0];
+  yb[2] += posb[1];
+  yb[4] += posb[2];
+  yb[1] += fb[0] + F.qomg * (-fb[3] * B[2] + fb[5] * B[1]);
+  yb[3] += fb[2] + F.qomg * (fb[1] * B[2] - fb[5] * B[0]);
+  yb[5] += fb[4] + F.qomg * (-fb[1] * B[1] + fb[3] * B[0]);
+}
+
+__device__ void rk4_step(const AdjFields& F, double* y, double t, double h) {
+  double k1[6], k2[6], k3[6], k4[6], yt[6];
+  f_eval(F, t, y, k1);
+  for (int i = 0; i < 6; ++i) yt[i] = y[i] + h * 0.5 * k1[i];
+  f_eval(F, t + h * 0.5, yt, k2);
+  for (int i = 0; i < 6; ++i) yt[i] = y[i] + h * 0.5 * k2[i];
+  f_eval(F, t + h * 0.5, yt, k3);
+  for (int i = 0; i < 6; ++i) yt[i] = y[i] + h * k3[i];
+  f_eval(F, t + h, yt, k4);
+  for (int i = 0; i < 6; ++i) y[i] = y[i] + h / 6.0 * (k1[i] + k4[i] + 2.0 * (k2[i] + k3[i]));
+}
+
+// lam (adjoint of the step's output) -> adjoint of its input y (returned in lam).
+__device__ void rk4_vjp(const AdjFields& F, const double* y, double t, double h, double* lam) {
+  double k1[6], k2[6], k3[6], y2[6], y3[6], y4[6];
+  f_eval(F, t, y, k1);
+  for (int i = 0; i < 6; ++i) y2[i] = y[i] + h * 0.5 * k1[i];
+  f_eval(F, t + h * 0.5, y2, k2);
+  for (int i = 0; i < 6; ++i) y3[i] = y[i] + h * 0.5 * k2[i];
+  f_eval(F, t + h * 0.5, y3, k3);
+  for (int i = 0; i < 6; ++i) y4[i] = y[i] + h * k3[i];
+  double yb[6], k1b[6], k2b[6], k3b[6], k4b[6], tmp[6];
+  for (int i = 0; i < 6; ++i) {
+    yb[i] = lam[i];
+    k1b[i] = h / 6.0 * lam[i];
+    k2b[i] = h / 3.0 * lam[i];
+    k3b[i] = h / 3.0 * lam[i];
+    k4b[i] = h / 6.0 * lam[i];
+  }
+  for (int i = 0; i < 6; ++i) tmp[i] = 0;
+  f_vjp(F, t + h, y4, k4b, tmp);
+  for (int i = 0; i < 6; ++i) { yb[i] += tmp[i]; k3b[i] += h * tmp[i]; tmp[i] = 0; }
+  f_vjp(F, t + h * 0.5, y3, k3b, tmp);
+  for (int i = 0; i < 6; ++i) { yb[i] += tmp[i]; k2b[i] += h * 0.5 * tmp[i]; tmp[i] = 0; }
+  f_vjp(F, t + h * 0.5, y2, k2b, tmp);
+  for (int i = 0; i < 6; ++i) { yb[i] += tmp[i]; k1b[i] += h * 0.5 * tmp[i]; tmp[i] = 0; }
+  f_vjp(F, t, y, k1b, tmp);
+  for (int i = 0; i < 6; ++i) lam[i] = yb[i] + tmp[i];
+}
+
+struct AdjChain {
+  double x0[6];     // initial state (x, vx, y, vy, z, vz)
+  double t0, dt;    // [s]
+  int nf, nb;       // knots forward / backward of t0
+  const double* kb; // knot adjoints, 9 x n (x y z bx by bz ax ay az); n = nf + nb
+  double* ckpt;     // per direction: (states / kCkptStride + 2) x 6
+  double* seg;      // per direction: (kCkptStride + 1) x 6
+  int64_t ckpt_stride_dir, seg_stride_dir;
+};
+
+// Knot state / acceleration adjoints in the RK4 state layout.
+__device__ __forceinline__ void knot_state_adj(const double* kb, int64_t n, int64_t j, double* lam) {
+  lam[0] += kb[j]; lam[2] += kb[n + j]; lam[4] += kb[2 * n + j];
+  lam[1] += kb[3 * n + j] / kCLight; lam[3] += kb[4 * n + j] / kCLight; lam[5] += kb[5 * n + j] / kCLight;
+}
+__device__ __forceinline__ void knot_accel_adj(const double* kb, int64_t n, int64_t j, double* fb) {
+  fb[0] = 0; fb[2] = 0; fb[4] = 0;
+  fb[1] = kb[6 * n + j] / kCLight; fb[3] = kb[7 * n + j] / kCLight; fb[5] = kb[8 * n + j] / kCLight;
+}
+
+// Thread 0: the forward chain (states z_i at t0 + i dt, i = 0 .. nf-1, at knots nb + i; knot nb + i + 1
+// holds f(t_i, z_i), knot nb also f(t_0, z_0)).  Thread 1: the backward chain (z_i at t0 - i dt,
+// i = 0 .. nb, z_i at knot nb - i for i >= 1; knot nb - 1 - i holds f(t_i, z_i)).
+__global__ void k_adj_rk4(AdjFields F, AdjChain C) {
+  const int dir = threadIdx.x;
+  if (dir > 1) return;
+  const int64_t n = (int64_t)C.nf + C.nb;
+  const double h = dir == 0 ? C.dt : -C.dt;
+  const int64_t M = dir == 0 ? (int64_t)C.nf - 1 : (int64_t)C.nb;  // last state used
+  if (M < 0) return;
+  double* ck = C.ckpt + dir * C.ckpt_stride_dir;
+  double* sg = C.seg + dir * C.seg_stride_dir;
+  // checkpoints z_{m * stride}
+  double y[6];
+  for (int i = 0; i < 6; ++i) y[i] = C.x0[i];
+  for (int64_t i = 0; i <= M; ++i) {
+    if (i % kCkptStride == 0)
+      for (int k = 0; k < 6; ++k) ck[(i / kCkptStride) * 6 + k] = y[k];
+    if (i < M) rk4_step(F, y, C.t0 + h * (double)i, h);
+  }
+  auto state_knot = [&](int64_t i) -> int64_t {
+    if (dir == 0) return C.nb + i;
+    return i >= 1 ? C.nb - i : -1;
+  };
+  auto accel_knot = [&](int64_t i) -> int64_t {
+    if (dir == 0) return i + 1 <= (int64_t)C.nf - 1 ? C.nb + i + 1 : -1;
+    return i <= (int64_t)C.nb - 1 ? C.nb - 1 - i : -1;
+  };
+  double lam[6] = {0, 0, 0, 0, 0, 0};
+  const int64_t nseg = (M + kCkptStride - 1) / kCkptStride;  // segments (s0, s1]
+  for (int64_t m = (nseg > 0 ? nseg - 1 : 0); m >= 0; --m) {
+    const int64_t s0 = m * kCkptStride, s1 = min(M, s0 + kCkptStride);
+    for (int k = 0; k < 6; ++k) y[k] = ck[m * 6 + k];
+    for (int64_t i = s0; i <= s1; ++i) {
+      for (int k = 0; k < 6; ++k) sg[(i - s0) * 6 + k] = y[k];
+      if (i < s1) rk4_step(F, y, C.t0 + h * (double)i, h);
+    }
+    const int64_t lo = m == 0 ? 0 : s0 + 1;
+    for (int64_t i = s1; i >= lo; --i) {
+      const double* zi = sg + (i - s0) * 6;
+      const int64_t sk = state_knot(i);
+      if (sk >= 0) knot_state_adj(C.kb, n, sk, lam);
+      const int64_t ak = accel_knot(i);
+      double fb[6];
+      if (ak >= 0) {
+        knot_accel_adj(C.kb, n, ak, fb);
+        f_vjp(F, C.t0 + h * (double)i, zi, fb, lam);
+      }
+      if (dir == 0 && i == 0) {  // knot nb also holds f(t_0, z_0)
+        knot_accel_adj(C.kb, n, C.nb, fb);
+        f_vjp(F, C.t0, zi, fb, lam);
+      }
+      if (i > 0) rk4_vjp(F, sg + (i - 1 - s0) * 6, C.t0 + h * (double)(i - 1), h, lam);
+    }
+    if (m == 0) break;
+  }
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------------------------
+// Host orchestration
+// ---------------------------------------------------------------------------------------------
+// Knot adjoints (9 x n on the device, layout of the knot values) -> gradient of the half-period
+// factors of field `param_field` (device pointer, n_params values; valid after the stream
+// completes).
+double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_params, cudaStream_t st) {
+  const Particle& P = model.particle;
+  const int64_t n = nknots_;
+  std::vector<double> fvals;
+  std::vector<DevField> df;
+  for (const FieldSpec& f : model.fields) df.push_back(to_dev_field(f, fvals));
+  if (fvals.empty()) fvals.push_back(0.0);
+  const double dt = ((model.ctstop - model.ctstart) / kC / (model.npoints - 1));
+  const int64_t nf = (int64_t)(1 + (model.ctstop - P.t0) / kC / dt);
+  const int64_t nb = (int64_t)((P.t0 - model.ctstart) / kC / dt);
+  if (nf + nb != n) throw Error{OSC_ERR_STATE, "trajectory and its knots disagree"};
+  const int64_t ck_dir = (std::max(nf, nb) / dev::kCkptStride + 2) * 6;
+  const int64_t seg_dir = (dev::kCkptStride + 1) * 6;
+  adj_r_.reserve(sizeof(DevField) * df.size() + sizeof(double) * (fvals.size() + n_params + 2 * ck_dir + 2 * seg_dir) + 256);
+  char* base = adj_r_.as<char>();
+  DevField* d_fields = reinterpret_cast<DevField*>(base);
+  double* d_vals = reinterpret_cast<double*>(base + ((sizeof(DevField) * df.size() + 255) & ~(size_t)255));
+  double* d_pgrad = d_vals + fvals.size();
+  double* d_ck = d_pgrad + n_params;
+  double* d_seg = d_ck + 2 * ck_dir;
+  check(cudaMemcpyAsync(d_fields, df.data(), sizeof(DevField) * df.size(), cudaMemcpyHostToDevice, st), "fields");
+  check(cudaMemcpyAsync(d_vals, fvals.data(), sizeof(double) * fvals.size(), cudaMemcpyHostToDevice, st), "fields");
+  check(cudaMemsetAsync(d_pgrad, 0, sizeof(double) * n_params, st), "memset");
+  dev::AdjFields AF{d_fields, (int)df.size(), d_vals, param_field, P.qomg, d_pgrad};
+  dev::AdjChain AC{};
+  const double x0[6] = {P.x0.x, P.b0.x * kC, P.x0.y, P.b0.y * kC, P.x0.z, P.b0.z * kC};
+  for (int i = 0; i < 6; ++i) AC.x0[i] = x0[i];
+  AC.t0 = P.t0 / kC;
+  AC.dt = dt;
+  AC.nf = (int)nf;
+  AC.nb = (int)nb;
+  AC.kb = d_kb;
+  AC.ckpt = d_ck;
+  AC.seg = d_seg;
+  AC.ckpt_stride_dir = ck_dir;
+  AC.seg_stride_dir = seg_dir;
+  dev::k_adj_rk4<<<1, 32, 0, st>>>(AF, AC);
+  check(cudaGetLastError(), "trajectory adjoint");
+  ++last_launches;
+  return d_pgrad;
+}
+
+static int param_field_of(const Model& model, int64_t n_params) {
+  int param_field = -1;
+  for (size_t i = 0; i < model.fields.size(); ++i) {
+    const FieldSpec& f = model.fields[i];
+    if (f.kind == 2) throw Error{OSC_ERR_INVALID, "the adjoint supports ideal undulator and EPU fields"};
+    if (!f.half_scale.empty()) {
+      if (param_field >= 0) throw Error{OSC_ERR_INVALID, "more than one field has half-period factors"};
+      param_field = (int)i;
+    }
+  }
+  if (param_field < 0) throw Error{OSC_ERR_STATE, "no field has half-period factors to differentiate"};
+  if ((int64_t)model.fields[param_field].half_scale.size() != n_params)
+    throw Error{OSC_ERR_LENGTH, "gradient length must equal the number of half-period factors"};
+  return param_field;
+}
+
+void Engine::trajectory_vjp(const double* knot_grad, double* grad_params, int64_t n_params) {
+  const int param_field = param_field_of(model, n_params);
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  check(cudaSetDevice(device), "cudaSetDevice");
+  cudaStream_t st = stream;
+  model.ensure_trajectory();
+  upload_trajectory();
+  const int64_t n = nknots_;
+  adj_.reserve(sizeof(double) * 9 * n);
+  check(cudaMemcpyAsync(adj_.p, knot_grad, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, st), "knot gradient");
+  double* d_pgrad = rk4_adjoint(adj_.as<double>(), param_field, n_params, st);
+  check(cudaMemcpyAsync(grad_params, d_pgrad, sizeof(double) * n_params, cudaMemcpyDeviceToHost, st), "download");
+  check(cudaStreamSynchronize(st), "trajectory adjoint");
+}
+
+void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double>& omega, int level,
+                      const osc_rad_opts& o, bool current_abs, const double* grad_flux, double* flux_out,
+                      double* grad_params, int64_t n_params, double* grad_knots) {
+  if (level < 1 || level > 20) throw Error{OSC_ERR_RANGE, "adjoint level must be in [1, 20]"};
+  const int param_field = param_field_of(model, n_params);
+  double pol[6];
+  bool project = false;
+  polarization_vector(o, pol, project);
+  if (project) throw Error{OSC_ERR_INVALID, "the adjoint supports polarization 'all'"};
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  check(cudaSetDevice(device), "cudaSetDevice");
+  pending_.clear();
+  last_samples = last_launches = last_not_converged = 0;
+  cudaStream_t st = stream;
+  const int64_t n_e = (int64_t)omega.size();
+  const int64_t N = n_obs * n_e;
+  if (N <= 0) return;
+
+  model.ensure_trajectory();
+  upload_trajectory();
+  ensure_levels(level);
+  const Particle& P = model.particle;
+  // inputs
+  obs_.reserve(sizeof(double) * 3 * n_obs);
+  omega_.reserve(sizeof(double) * n_e);
+  adj_.reserve(sizeof(double) * (N /*grad*/ + N /*flux*/ + 6 * N /*W*/));
+  check(cudaMemcpyAsync(obs_.p, obs, sizeof(double) * 3 * n_obs, cudaMemcpyHostToDevice, st), "obs");
+  check(cudaMemcpyAsync(omega_.p, omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
+  double* d_grad = adj_.as<double>();
+  double* d_flux = d_grad + N;
+  double* d_W = d_flux + N;
+  check(cudaMemcpyAsync(d_grad, grad_flux, sizeof(double) * N, cudaMemcpyHostToDevice, st), "grad");
+  // forward sums at level L: the first-wave kernel with one span per segment
+  part_.reserve(sizeof(double) * 2 * kFdPartials * N);
+  cnt_.reserve(64);
+  unsigned* cnt = cnt_.as<unsigned>();
+  unsigned long long* work = reinterpret_cast<unsigned long long*>(cnt + 4) + 2;
+  check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");
+  FdWaveArgs w{};
+  w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = obs_.as<double>(); w.omega = omega_.as<double>();
+  w.n_e = n_e; w.n_items = N; w.act = nullptr; w.n_act = nullptr; w.first = 1; w.level = level;
+  w.tile_entries = 128; w.min_span = 32; w.target_units = 1; w.part = part_.as<double>(); w.err = cnt + 2;
+  w.work = work;
+  const int fv = forced_variant[0] >= 0 ? forced_variant[0] : current_variant_[0];
+  check(launch_fd_wave_fp64(w, (int)std::min<int64_t>((N + 127) / 128, wave_grid(0, fv)), fv, st), "adjoint forward");
+  check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");  // counters start at zero
+  const double dtL = dt_inclusive(tstart_, tstop_, level);
+  const double c0 = P.q / (four_pi() * kC * kEps0 * kSqrt2Pi);
+  const double cur = current_abs ? std::fabs(P.current) : P.current;
+  const double c2 = four_pi() * cur / (kH * std::fabs(P.q) * kMu0 * kC) * 1e-6 * 0.001;
+  dev::k_adj_weights<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(part_.as<double>(), N, d_grad, c0 * dtL, c2, d_W,
+                                                                  d_flux);
+  // per-sample gradients
+  const int64_t s_end = (int64_t)2 << level;
+  const int64_t n = nknots_;
+  adj_s_.reserve(sizeof(double) * (9 * lev_cap_ + 2 * 9 * n + 9 * n));
+  double* d_gs = adj_s_.as<double>();
+  double* d_yb = d_gs + 9 * lev_cap_;
+  double* d_pb = d_yb + 9 * n;
+  double* d_diag = d_pb + 9 * n;
+  check(cudaMemsetAsync(d_gs, 0, sizeof(double) * (9 * lev_cap_ + 2 * 9 * n), st), "memset");
+  int sms = 0;
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
+  const int64_t gx = (s_end - 1 + dev::kAdjThreads - 1) / dev::kAdjThreads;
+  const int64_t want = 16 * (int64_t)sms;  // CTAs in flight
+  int64_t gy = std::max<int64_t>(1, std::min<int64_t>((want + gx - 1) / gx, (N + dev::kAdjStage - 1) / dev::kAdjStage));
+  const int64_t per = ((N + gy - 1) / gy + dev::kAdjStage - 1) / dev::kAdjStage * dev::kAdjStage;
+  gy = (N + per - 1) / per;
+  dev::k_adj_samples<<<dim3((unsigned)gx, (unsigned)gy), dev::kAdjThreads, 0, st>>>(
+      lev_.as<double>(), lev_cap_, s_end, obs_.as<double>(), omega_.as<double>(), n_e, d_W, N, per, d_gs);
+  dev::k_adj_spline_eval<<<(unsigned)((s_end - 1 + 255) / 256), 256, 0, st>>>(knots_.as<double>(), n, tstart_, tstop_,
+                                                                             s_end, d_gs, lev_cap_, d_yb, d_pb);
+  dev::k_adj_spline_solve<<<1, 32, 0, st>>>(knots_.as<double>(), n, d_yb, d_pb, d_diag);
+  // RK4 adjoint
+  double* d_pgrad = rk4_adjoint(d_yb, param_field, n_params, st);
+  if (grad_knots) check(cudaMemcpyAsync(grad_knots, d_yb, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, st), "download");
+  if (flux_out) check(cudaMemcpyAsync(flux_out, d_flux, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
+  check(cudaMemcpyAsync(grad_params, d_pgrad, sizeof(double) * n_params, cudaMemcpyDeviceToHost, st), "download");
+  unsigned err = 0;
+  check(cudaMemcpyAsync(&err, cnt + 2, sizeof err, cudaMemcpyDeviceToHost, st), "error word");
+  check(cudaStreamSynchronize(st), "adjoint");
+  if (err & dev::kErrTmaTimeout) {
+    check(cudaMemset(cnt + 2, 0, sizeof(unsigned)), "error word");
+    throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+  }
+  last_samples = N * (s_end - 1);
+}
+
+}  // namespace osc

@@ -728,6 +728,7 @@ namespace {
 constexpr int kBatchPrefill = 13;        // levels enqueued without the host (records kept resident)
 constexpr int kBatchMinSpan = 32;
 constexpr int kBatchMaxJobsPerChunk = 4096;
+}  // namespace
 
 DevField to_dev_field(FieldSpec f, std::vector<double>& vals) {
   f.finish();
@@ -771,7 +772,6 @@ DevField to_dev_field(FieldSpec f, std::vector<double>& vals) {
   d.length = f.length;
   return d;
 }
-}  // namespace
 
 int Engine::batch_resident(int v) {
   if (wave_grid_[3][v] == 0) {

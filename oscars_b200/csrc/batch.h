@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -88,6 +89,10 @@ struct BatchFinalArgs {
   unsigned long long* samples;
   unsigned long long* work_reset;
 };
+
+struct FieldSpec;
+// Device form of a field; grid values and half-period factors are appended to `vals`.
+DevField to_dev_field(FieldSpec f, std::vector<double>& vals);
 
 // Compiled variants of the batched wave kernel (entries per thread, minimum CTAs per SM).
 constexpr int kBatchVariants = 7;

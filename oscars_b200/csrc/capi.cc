@@ -426,6 +426,51 @@ OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fie
   });
 }
 
+OSC_API int osc_set_half_period_scale(osc_ctx* ctx, int field_index, const double* scale, long long n) {
+  return guarded(ctx, [&] {
+    osc::Model& M = ctx->eng->model;
+    int idx = field_index;
+    if (idx < 0) {
+      for (size_t i = 0; i < M.fields.size(); ++i)
+        if (!M.fields[i].half_scale.empty()) idx = (int)i;
+    }
+    if (idx < 0 || idx >= (int)M.fields.size()) throw osc::Error{OSC_ERR_RANGE, "no such field"};
+    osc::FieldSpec& f = M.fields[idx];
+    if (f.kind != OSC_FIELD_UNDULATOR) throw osc::Error{OSC_ERR_INVALID, "half-period factors apply to undulators"};
+    if (!scale || n != 2 * (long long)f.nperiods) throw osc::Error{OSC_ERR_LENGTH, "n must be 2 * nperiods"};
+    f.half_scale.assign(scale, scale + n);
+    M.knots.clear();
+    ++M.knots_version;
+  });
+}
+
+OSC_API int osc_trajectory_vjp(osc_ctx* ctx, const double* knot_grad, long long n_points, double* grad_half_scale,
+                               long long n_half) {
+  return guarded(ctx, [&] {
+    if (!knot_grad || !grad_half_scale) throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    osc::Model& M = ctx->eng->model;
+    M.ensure_trajectory();
+    if (n_points != M.knots.n) throw osc::Error{OSC_ERR_LENGTH, "n_points differs from the trajectory's"};
+    ctx->eng->trajectory_vjp(knot_grad, grad_half_scale, n_half);
+  });
+}
+
+OSC_API int osc_flux_vjp(osc_ctx* ctx, const double* obs_xyz, long long n_obs, const double* energies_eV,
+                         long long n_energies, int level, const osc_rad_opts* opts, int spectrum,
+                         const double* grad_flux, double* flux_out, double* grad_half_scale, long long n_half,
+                         double* grad_knots) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (opts->nparticles != 0) throw osc::Error{OSC_ERR_INVALID, "the adjoint is for one particle: nparticles must be 0"};
+    if (n_obs < 1 || n_energies < 1 || !obs_xyz || !energies_eV || !grad_flux || !grad_half_scale)
+      throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    std::vector<double> omega(n_energies);
+    for (long long i = 0; i < n_energies; ++i) omega[i] = osc::ev_to_omega(energies_eV[i]);
+    ctx->eng->flux_vjp(obs_xyz, n_obs, omega, level, *opts, spectrum != 0, grad_flux, flux_out, grad_half_scale,
+                       n_half, grad_knots);
+  });
+}
+
 OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double* normals, long long n_obs,
                               int directional, const osc_rad_opts* opts, double* out, int32_t* level_out,
                               long long* n_not_converged) {

@@ -82,6 +82,14 @@ class Engine {
   void batch_fp64(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
                   int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
                   bool average, double* out, int32_t* level_out);
+  // Fixed-level flux and its vector-Jacobian product with respect to the half-period factors of the
+  // (single) undulator that has them: grad_params = (dF/ds)^T grad_flux.  Host buffers; FP64.
+  void flux_vjp(const double* obs, int64_t n_obs, const std::vector<double>& omega, int level,
+                const osc_rad_opts& o, bool current_abs, const double* grad_flux, double* flux_out,
+                double* grad_params, int64_t n_params, double* grad_knots = nullptr);
+  // Gradient of <knot_grad, knots> (knot_grad: host, 9 x n in the knot layout x y z bx by bz ax ay az)
+  // with respect to the half-period factors: reverse mode through the RK4 steps.
+  void trajectory_vjp(const double* knot_grad, double* grad_params, int64_t n_params);
   bool use_graphs = true;            // replay the batched front of a known shape as a CUDA graph
   long long graph_launches() const { return graph_launches_; }
 
@@ -151,6 +159,7 @@ class Engine {
   // batched path
   DevBuf b_fields_, b_fvals_, b_obs_, b_omega_, b_acc_, b_jobs_, b_knots_, b_work_, b_rec_, b_rec_ext_, b_state_, b_out_,
       b_lvl_, b_act_[2], b_part_, b_plan_, b_cnt_;
+  DevBuf adj_, adj_s_, adj_r_;      // adjoint scratch
   cudaGraphExec_t graph_exec_ = nullptr;
   long long graph_launches_ = 0;
   std::map<std::tuple<int, int64_t, int, int>, int> tuned_batch_;  // (jobs, entries, first, prefill level)
@@ -158,6 +167,7 @@ class Engine {
   int tune_batch(int nj, int Lfirst, int64_t target, const DevJob* d_jobs, const BatchPlan& plan, unsigned* misc,
                  unsigned long long* m64, int64_t rec_stride);
   void radiation_beam_mixed(RadRequest& rq, int64_t N);
+  double* rk4_adjoint(const double* d_kb, int param_field, int64_t n_params, cudaStream_t st);
 
   void upload_trajectory();
   void ensure_levels(int L);

@@ -184,3 +184,25 @@ def run_case(obj, calls):
         else:
             out = getattr(obj, name)(**kw)
     return out
+
+
+# ---- differentiable tuning: the small configuration of the gradient fixtures -------------------
+ADJ_LEVEL = 10
+ADJ_FD_STEPS = (1e-6, 1e-3, 3e-3)   # central-difference steps of the gradient fixture
+
+
+def richardson(fd_h, fd_rh, r):
+    """Extrapolate central differences at steps h and r h to remove the O(h^2) term."""
+    return (r * r * fd_h - fd_rh) / (r * r - 1)
+
+
+def adjoint_config():
+    """41-period undulator (B0 = 0.5 T, 50 mm) with 82 half-period factors; 5 x 5 observers over
+    1 mm x 1 mm at z = 30 m; 8 energies over E1 +- 5 %; fixed level 10.  Loss = sum (F(s) - F(1))^2
+    at s = the factors of halfscale_41.txt."""
+    import numpy as np
+    from oracle.oracle import rectangle
+    obs, _, _ = rectangle("XY", 5, 5, 0.001, 0.001, [0.0, 0.0, 0.0], [0.0, 0.0, 30.0], 0)
+    energies = np.linspace(0.95 * E1_U, 1.05 * E1_U, 8)
+    return obs, energies, ADJ_LEVEL
+

@@ -71,8 +71,51 @@ def make(name, S):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), pos=pos, val=val, **extra)
 
 
+def make_adjoint(S):
+    """Central finite differences of loss = sum (F(s) - F(1))^2 over the adjoint configuration, every
+    one of the 82 half-period factors, with the reference's CPU path (the scaled undulator given to it
+    as a Python field function), at the steps ADJ_FD_STEPS -> adjoint_fd.npz (grad_h<i> per step).
+    The FP64 retarded phase (~7e10 rad here) carries ~1e-5 rad of rounding, so differences with
+    h = 1e-6 are dominated by rounding; the tests extrapolate the larger steps (Richardson)."""
+    import math
+    from cases import ADJ_FD_STEPS, BEAM, adjoint_config, halfscale_41, halfscale_function
+    obs, energies, level = adjoint_config()
+    s0 = np.array(halfscale_41())
+
+    def flux(s):
+        o = S.sr(nthreads=1, gpu=0)
+        o.add_bfield_function(halfscale_function([0, 0.5, 0], [0, 0, 0.05], 41, -math.pi / 2, list(s)))
+        o.set_particle_beam(**BEAM[1])
+        o.set_ctstartstop(-1.5, 1.5)
+        o.set_npoints_trajectory(20001)
+        F = np.zeros((obs.shape[0], energies.size))
+        for j, e in enumerate(energies):
+            res = o.calculate_flux_rectangle(energy_eV=float(e), npoints=[5, 5], width=[0.001, 0.001],
+                                             translation=[0, 0, 30], precision=0, max_level=level, nthreads=1,
+                                             dim=3)
+            assert np.array_equal(np.array([r[0] for r in res]), obs)
+            F[:, j] = [r[1] for r in res]
+        return F
+    F1 = flux(np.ones(82))
+    F = flux(s0)
+    loss = lambda s: float(np.sum((flux(s) - F1) ** 2))
+    out = dict(s=s0, F=F, F1=F1, h=np.array(ADJ_FD_STEPS), level=level)
+    for i, h in enumerate(ADJ_FD_STEPS):
+        g = np.zeros(82)
+        for k in range(82):
+            e = np.zeros(82)
+            e[k] = h
+            g[k] = (loss(s0 + e) - loss(s0 - e)) / (2 * h)
+        out["grad_h%d" % i] = g
+    np.savez_compressed(os.path.join(HERE, "adjoint_fd.npz"), **out)
+
+
 def main(argv):
     S = reference()
+    if argv[1:] == ["adjoint_fd"]:
+        make_adjoint(S)
+        print("wrote adjoint_fd")
+        return
     names = argv[1:] or sorted(CASES)
     for n in names:
         make(n, S)
