@@ -228,7 +228,8 @@ OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fie
  * the flux F of every (observer, energy) entry -- the value osc_flux / osc_spectrum return with
  * precision 0 and max_level = level -- and grad_half_scale = (dF/ds)^T grad_flux, the gradient of any
  * loss with dLoss/dF = grad_flux with respect to those factors, by reverse mode through the
- * radiation sum, the trajectory spline and the RK4 steps (FP64, checkpoints every 256 steps).
+ * radiation sum, the trajectory spline and the RK4 steps (FP64; the RK4 part runs parallel in time
+ * over 64-step segments joined by their 6 x 6 Jacobians).
  * Entries are observer-major with energies fastest; spectrum = 1 normalises like osc_spectrum.
  * grad_knots (may be NULL) receives the gradient with respect to the trajectory knots (9 x n_points,
  * the layout of osc_trajectory_vjp's knot_grad).

@@ -11,9 +11,11 @@
 //                      one thread per sample, entries staged through shared memory
 //   k_adj_spline_eval  sample -> knot values and second derivatives (transpose of the evaluation)
 //   k_adj_spline_solve second derivatives -> knot values (transpose of the tridiagonal sweeps)
-//   k_adj_rk4          knots -> RK4 states -> field amplitudes: one thread per integration direction,
-//                      states recomputed from checkpoints every 256 steps, each step's stages
-//                      recomputed and differentiated in reverse.
+//   k_adj_rk4_segments knots -> RK4 states -> field amplitudes, parallel in time: every 64-step
+//                      segment of both integration chains runs its reverse pass at once (states read
+//                      back from the knots, each step's stages recomputed and differentiated), once
+//                      with the knot adjoints and once per unit adjoint entering it;
+//   k_adj_rk4_combine  a sequential sweep of the 6 x 6 segment Jacobians joins the segments.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -28,8 +30,6 @@
 
 namespace osc {
 namespace dev {
-
-constexpr int kCkptStride = 256;
 
 // ---- 1. entry weights ----------------------------------------------------------------------
 // part: first-wave partials of level L with one span ([entry][segment][kFdPartials]).
@@ -169,33 +169,93 @@ __global__ void k_adj_spline_eval(const double* __restrict__ knots, int64_t n, d
   }
 }
 
-// ---- 4. second derivatives -> knot values (one thread per component) --------------------------
+// ---- 4. second derivatives -> knot values --------------------------------------------------
 // Forward (linear in y): u_0 = 0, u_i = (6 ud_i / (X_{i+1} - X_{i-1}) - sig_i u_{i-1}) / p_i,
-// ypp_{n-1} = -0.5 u_{n-2} / (0.5 diag_{n-2} + 1), ypp_k = diag_k ypp_{k+1} + u_k.
-__global__ void k_adj_spline_solve(const double* __restrict__ knots, int64_t n, double* __restrict__ ybar,
-                                   double* __restrict__ pbar, double* __restrict__ diag_work) {
-  const int c = threadIdx.x;
-  if (c >= 9) return;
-  const double* X = knots;
-  double* diag = diag_work + c * n;
-  double* B = pbar + c * n;  // becomes the adjoint of u in place
-  double* Yb = ybar + c * n;
-  diag[0] = -0.5;
-  for (int64_t i = 1; i < n - 1; ++i) {
-    const double sig = (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]);
-    diag[i] = (sig - 1.) / (sig * diag[i - 1] + 2.0);
+// ypp_{n-1} = -0.5 u_{n-2} / (0.5 diag_{n-2} + 1), ypp_k = diag_k ypp_{k+1} + u_k, with
+// sig_i = (X_i - X_{i-1}) / (X_{i+1} - X_{i-1}), p_i = sig_i diag_{i-1} + 2.  Its transpose is two
+// first-order linear recurrences, each evaluated as a block-wide scan of affine maps x -> a x + b
+// (one block of kScanThreads per component), then a three-point gather.
+constexpr int kScanThreads = 1024;
+
+struct Affine { double a, b; };  // x -> a x + b
+__device__ __forceinline__ Affine compose(Affine first, Affine then) {  // then(first(x))
+  return {then.a * first.a, then.a * first.b + then.b};
+}
+
+// x_k = A(k) x_{k-1} + B(k) for k = 0 .. m-1 (x_{-1} = 0), in index order k or (reverse) m-1-k;
+// A(k), B(k) are callables of the recurrence index, `out(k, x)` receives every x_k.
+template <class FA, class FB, class FO>
+__device__ void block_linear_scan(int64_t m, FA A, FB B, FO out) {
+  __shared__ double sa[kScanThreads], sb[kScanThreads];
+  const int t = threadIdx.x;
+  const int64_t chunk = (m + kScanThreads - 1) / kScanThreads;
+  const int64_t k0 = t * chunk, k1 = min(m, k0 + chunk);
+  Affine f{1.0, 0.0};
+  for (int64_t k = k0; k < k1; ++k) f = compose(f, Affine{A(k), B(k)});
+  sa[t] = f.a;
+  sb[t] = f.b;
+  __syncthreads();
+  for (int o = 1; o < kScanThreads; o <<= 1) {  // inclusive scan of the chunk maps
+    Affine prev{1.0, 0.0};
+    if (t >= o) prev = Affine{sa[t - o], sb[t - o]};
+    __syncthreads();
+    if (t >= o) {
+      const Affine cur = compose(prev, Affine{sa[t], sb[t]});
+      sa[t] = cur.a;
+      sb[t] = cur.b;
+    }
+    __syncthreads();
   }
-  for (int64_t k = 0; k <= n - 2; ++k) B[k + 1] += diag[k] * B[k];
-  B[n - 2] += -0.5 / (0.5 * diag[n - 2] + 1.) * B[n - 1];
-  for (int64_t i = n - 2; i >= 1; --i) {
-    const double sig = (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]);
-    const double p = sig * diag[i - 1] + 2.0;
-    const double udb = B[i] * 6.0 / ((X[i + 1] - X[i - 1]) * p);
-    B[i - 1] += -sig / p * B[i];
-    const double hi = X[i + 1] - X[i], hm = X[i] - X[i - 1];
-    Yb[i + 1] += udb / hi;
-    Yb[i] += -udb / hi - udb / hm;
-    Yb[i - 1] += udb / hm;
+  double x = t > 0 ? sb[t - 1] : 0.0;  // value entering this chunk (x_{-1} = 0)
+  __syncthreads();
+  for (int64_t k = k0; k < k1; ++k) {
+    x = A(k) * x + B(k);
+    out(k, x);
+  }
+  __syncthreads();
+}
+
+// One block per component; pbar (adjoint of ypp) is overwritten, ybar accumulates; work: n doubles
+// per component.
+__global__ void __launch_bounds__(kScanThreads) k_adj_spline_solve(const double* __restrict__ knots, int64_t n,
+                                                                     double* __restrict__ ybar,
+                                                                     double* __restrict__ pbar,
+                                                                     double* __restrict__ work) {
+  const int c = blockIdx.x;
+  const double* X = knots;
+  const double* diag = knots + 19 * n;
+  double* B = pbar + c * n;
+  double* U = work + c * n;
+  double* Yb = ybar + c * n;
+  auto sig = [&](int64_t i) { return (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]); };
+  // (1) B'_0 = B_0, B'_k = B_k + diag_{k-1} B'_{k-1}
+  block_linear_scan(n, [&](int64_t k) { return k > 0 ? diag[k - 1] : 0.0; }, [&](int64_t k) { return B[k]; },
+                    [&](int64_t k, double x) { U[k] = x; });
+  // (2) u_{n-2} also feeds ypp_{n-1}
+  if (threadIdx.x == 0) U[n - 2] += -0.5 / (0.5 * diag[n - 2] + 1.) * U[n - 1];
+  __syncthreads();
+  // (3) V_{n-2} = U_{n-2}, V_{j} = U_j + (-sig_{j+1} / p_{j+1}) V_{j+1}, j = n-3 .. 1 (written into B)
+  const int64_t m = n - 2;  // j = n-2 .. 1 -> k = 0 .. m-1
+  block_linear_scan(m,
+                    [&](int64_t k) {
+                      const int64_t j = n - 2 - k;
+                      if (j == n - 2) return 0.0;
+                      const double sg = sig(j + 1);
+                      return -sg / (sg * diag[j] + 2.0);
+                    },
+                    [&](int64_t k) { return U[n - 2 - k]; }, [&](int64_t k, double x) { B[n - 2 - k] = x; });
+  // (4) udb_i = V_i 6 / ((X_{i+1} - X_{i-1}) p_i), i = 1 .. n-2 (into U), then the three-point gather
+  for (int64_t i = 1 + threadIdx.x; i <= n - 2; i += blockDim.x) {
+    const double sg = sig(i);
+    U[i] = B[i] * 6.0 / ((X[i + 1] - X[i - 1]) * (sg * diag[i - 1] + 2.0));
+  }
+  __syncthreads();
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+    double acc = 0;
+    if (j - 1 >= 1 && j - 1 <= n - 2) acc += U[j - 1] / (X[j] - X[j - 1]);
+    if (j >= 1 && j <= n - 2) acc += -U[j] / (X[j + 1] - X[j]) - U[j] / (X[j] - X[j - 1]);
+    if (j + 1 >= 1 && j + 1 <= n - 2) acc += U[j + 1] / (X[j + 1] - X[j]);
+    Yb[j] += acc;
   }
 }
 
@@ -321,15 +381,36 @@ __device__ void rk4_vjp(const AdjFields& F, const double* y, double t, double h,
   for (int i = 0; i < 6; ++i) lam[i] = yb[i] + tmp[i];
 }
 
-struct AdjChain {
-  double x0[6];     // initial state (x, vx, y, vy, z, vz)
-  double t0, dt;    // [s]
-  int nf, nb;       // knots forward / backward of t0
-  const double* kb; // knot adjoints, 9 x n (x y z bx by bz ax ay az); n = nf + nb
-  double* ckpt;     // per direction: (states / kCkptStride + 2) x 6
-  double* seg;      // per direction: (kCkptStride + 1) x 6
-  int64_t ckpt_stride_dir, seg_stride_dir;
+// The two integration chains: z_0 = initial state; the forward chain has z_i at t0 + i dt at knot
+// nb + i (i = 0 .. nf-1, knot nb + i + 1 holds f(t_i, z_i), knot nb also f(t_0, z_0)); the backward
+// chain has z_i at t0 - i dt at knot nb - i (i = 0 .. nb; knot nb - 1 - i holds f(t_i, z_i)).  States
+// are read back from the knots.  Each chain is cut into segments (s0, s1] of kSegSteps steps.
+constexpr int kSegSteps = 64;
+
+struct AdjSegs {
+  double t0, dt;
+  int nf, nb;
+  const double* knots;  // t | y[9] | ... (n each)
+  const double* kb;     // knot adjoints, 9 x n
+  int64_t nseg[2];      // segments of the forward and backward chains
+  int64_t base[2];      // index of each chain's first segment
+  double* lam_loc;      // per segment: adjoint leaving it with zero adjoint entering (6)
+  double* jt;           // per segment: J^T e_r for r = 0..5 (6 x 6)
+  double* pseg;         // per segment: parameter gradient of the pass with e_r entering (6 x n_params)
+  int n_params;
 };
+
+__device__ __forceinline__ void chain_state(const AdjSegs& S, int dir, int64_t i, double* z) {
+  const int64_t n = (int64_t)S.nf + S.nb;
+  const int64_t j = dir == 0 ? S.nb + i : S.nb - i;
+  const double* y = S.knots + n;
+  z[0] = y[j];
+  z[1] = y[3 * n + j] * kCLight;
+  z[2] = y[n + j];
+  z[3] = y[4 * n + j] * kCLight;
+  z[4] = y[2 * n + j];
+  z[5] = y[5 * n + j] * kCLight;
+}
 
 // Knot state / acceleration adjoints in the RK4 state layout.
 __device__ __forceinline__ void knot_state_adj(const double* kb, int64_t n, int64_t j, double* lam) {
@@ -341,61 +422,74 @@ __device__ __forceinline__ void knot_accel_adj(const double* kb, int64_t n, int6
   fb[1] = kb[6 * n + j] / kCLight; fb[3] = kb[7 * n + j] / kCLight; fb[5] = kb[8 * n + j] / kCLight;
 }
 
-// Thread 0: the forward chain (states z_i at t0 + i dt, i = 0 .. nf-1, at knots nb + i; knot nb + i + 1
-// holds f(t_i, z_i), knot nb also f(t_0, z_0)).  Thread 1: the backward chain (z_i at t0 - i dt,
-// i = 0 .. nb, z_i at knot nb - i for i >= 1; knot nb - 1 - i holds f(t_i, z_i)).
-__global__ void k_adj_rk4(AdjFields F, AdjChain C) {
-  const int dir = threadIdx.x;
-  if (dir > 1) return;
-  const int64_t n = (int64_t)C.nf + C.nb;
-  const double h = dir == 0 ? C.dt : -C.dt;
-  const int64_t M = dir == 0 ? (int64_t)C.nf - 1 : (int64_t)C.nb;  // last state used
-  if (M < 0) return;
-  double* ck = C.ckpt + dir * C.ckpt_stride_dir;
-  double* sg = C.seg + dir * C.seg_stride_dir;
-  // checkpoints z_{m * stride}
-  double y[6];
-  for (int i = 0; i < 6; ++i) y[i] = C.x0[i];
-  for (int64_t i = 0; i <= M; ++i) {
-    if (i % kCkptStride == 0)
-      for (int k = 0; k < 6; ++k) ck[(i / kCkptStride) * 6 + k] = y[k];
-    if (i < M) rk4_step(F, y, C.t0 + h * (double)i, h);
-  }
-  auto state_knot = [&](int64_t i) -> int64_t {
-    if (dir == 0) return C.nb + i;
-    return i >= 1 ? C.nb - i : -1;
-  };
-  auto accel_knot = [&](int64_t i) -> int64_t {
-    if (dir == 0) return i + 1 <= (int64_t)C.nf - 1 ? C.nb + i + 1 : -1;
-    return i <= (int64_t)C.nb - 1 ? C.nb - 1 - i : -1;
-  };
+// One block per segment; thread 0 runs the segment's reverse pass with the knot adjoints and zero
+// adjoint entering (its parameter gradient goes straight to the result), threads 1..6 run it with the
+// unit adjoint e_{r-1} entering and no knot adjoints (the columns of the segment's transposed
+// Jacobian and parameter sensitivities, combined by k_adj_rk4_combine).
+__global__ void __launch_bounds__(32) k_adj_rk4_segments(AdjFields F, AdjSegs S) {
+  const int r = threadIdx.x;
+  if (r > 6) return;
+  const int64_t g = blockIdx.x;
+  const int dir = g < S.base[1] ? 0 : 1;
+  const int64_t m = g - S.base[dir];
+  const int64_t n = (int64_t)S.nf + S.nb;
+  const double h = dir == 0 ? S.dt : -S.dt;
+  const int64_t M = dir == 0 ? (int64_t)S.nf - 1 : (int64_t)S.nb;
+  const int64_t s0 = m * kSegSteps, s1 = min(M, s0 + kSegSteps);
+  const int64_t lo = m == 0 ? 0 : s0 + 1;
+  AdjFields Fr = F;
+  if (r > 0) Fr.pbar = S.pseg + (g * 6 + (r - 1)) * S.n_params;
   double lam[6] = {0, 0, 0, 0, 0, 0};
-  const int64_t nseg = (M + kCkptStride - 1) / kCkptStride;  // segments (s0, s1]
-  for (int64_t m = (nseg > 0 ? nseg - 1 : 0); m >= 0; --m) {
-    const int64_t s0 = m * kCkptStride, s1 = min(M, s0 + kCkptStride);
-    for (int k = 0; k < 6; ++k) y[k] = ck[m * 6 + k];
-    for (int64_t i = s0; i <= s1; ++i) {
-      for (int k = 0; k < 6; ++k) sg[(i - s0) * 6 + k] = y[k];
-      if (i < s1) rk4_step(F, y, C.t0 + h * (double)i, h);
-    }
-    const int64_t lo = m == 0 ? 0 : s0 + 1;
-    for (int64_t i = s1; i >= lo; --i) {
-      const double* zi = sg + (i - s0) * 6;
-      const int64_t sk = state_knot(i);
-      if (sk >= 0) knot_state_adj(C.kb, n, sk, lam);
-      const int64_t ak = accel_knot(i);
+  if (r > 0) lam[r - 1] = 1.0;
+  double zi[6], zp[6];
+  for (int64_t i = s1; i >= lo; --i) {
+    chain_state(S, dir, i, zi);
+    if (r == 0) {
+      const int64_t sk = dir == 0 ? S.nb + i : (i >= 1 ? S.nb - i : -1);
+      if (sk >= 0) knot_state_adj(S.kb, n, sk, lam);
+      const int64_t ak = dir == 0 ? (i + 1 <= (int64_t)S.nf - 1 ? S.nb + i + 1 : -1)
+                                  : (i <= (int64_t)S.nb - 1 ? S.nb - 1 - i : -1);
       double fb[6];
       if (ak >= 0) {
-        knot_accel_adj(C.kb, n, ak, fb);
-        f_vjp(F, C.t0 + h * (double)i, zi, fb, lam);
+        knot_accel_adj(S.kb, n, ak, fb);
+        f_vjp(Fr, S.t0 + h * (double)i, zi, fb, lam);
       }
       if (dir == 0 && i == 0) {  // knot nb also holds f(t_0, z_0)
-        knot_accel_adj(C.kb, n, C.nb, fb);
-        f_vjp(F, C.t0, zi, fb, lam);
+        knot_accel_adj(S.kb, n, S.nb, fb);
+        f_vjp(Fr, S.t0, zi, fb, lam);
       }
-      if (i > 0) rk4_vjp(F, sg + (i - 1 - s0) * 6, C.t0 + h * (double)(i - 1), h, lam);
     }
-    if (m == 0) break;
+    if (i > 0) {
+      chain_state(S, dir, i - 1, zp);
+      rk4_vjp(Fr, zp, S.t0 + h * (double)(i - 1), h, lam);
+    }
+  }
+  if (r == 0) {
+    for (int k = 0; k < 6; ++k) S.lam_loc[g * 6 + k] = lam[k];
+  } else {
+    for (int k = 0; k < 6; ++k) S.jt[(g * 6 + (r - 1)) * 6 + k] = lam[k];
+  }
+}
+
+// Sequential sweep over the segments of each chain (warp 0: forward chain, warp 1: backward chain):
+// the adjoint entering segment m is the one leaving segment m + 1.
+__global__ void __launch_bounds__(64) k_adj_rk4_combine(AdjSegs S, double* __restrict__ pbar) {
+  const int d = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double lam[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t m = S.nseg[d] - 1; m >= 0; --m) {
+    const int64_t g = S.base[d] + m;
+    for (int k = lane; k < S.n_params; k += 32) {
+      double acc = 0;
+      for (int r = 0; r < 6; ++r) acc += lam[r] * S.pseg[(g * 6 + r) * S.n_params + k];
+      if (acc != 0) atomicAdd(&pbar[k], acc);
+    }
+    double nl[6];
+    for (int j = 0; j < 6; ++j) {
+      double v = S.lam_loc[g * 6 + j];
+      for (int r = 0; r < 6; ++r) v += S.jt[(g * 6 + r) * 6 + j] * lam[r];
+      nl[j] = v;
+    }
+    for (int j = 0; j < 6; ++j) lam[j] = nl[j];
   }
 }
 
@@ -418,34 +512,43 @@ double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_param
   const int64_t nf = (int64_t)(1 + (model.ctstop - P.t0) / kC / dt);
   const int64_t nb = (int64_t)((P.t0 - model.ctstart) / kC / dt);
   if (nf + nb != n) throw Error{OSC_ERR_STATE, "trajectory and its knots disagree"};
-  const int64_t ck_dir = (std::max(nf, nb) / dev::kCkptStride + 2) * 6;
-  const int64_t seg_dir = (dev::kCkptStride + 1) * 6;
-  adj_r_.reserve(sizeof(DevField) * df.size() + sizeof(double) * (fvals.size() + n_params + 2 * ck_dir + 2 * seg_dir) + 256);
+  auto segs = [](int64_t M) -> int64_t { return M < 0 ? 0 : (M == 0 ? 1 : (M + dev::kSegSteps - 1) / dev::kSegSteps); };
+  const int64_t ns0 = segs(nf - 1), ns1 = segs(nb), nseg = ns0 + ns1;
+  const size_t field_bytes = (sizeof(DevField) * df.size() + 255) & ~(size_t)255;
+  adj_r_.reserve(field_bytes + sizeof(double) * (fvals.size() + n_params + nseg * (6 + 36 + 6 * n_params)));
   char* base = adj_r_.as<char>();
   DevField* d_fields = reinterpret_cast<DevField*>(base);
-  double* d_vals = reinterpret_cast<double*>(base + ((sizeof(DevField) * df.size() + 255) & ~(size_t)255));
+  double* d_vals = reinterpret_cast<double*>(base + field_bytes);
   double* d_pgrad = d_vals + fvals.size();
-  double* d_ck = d_pgrad + n_params;
-  double* d_seg = d_ck + 2 * ck_dir;
+  double* d_lam = d_pgrad + n_params;
+  double* d_jt = d_lam + 6 * nseg;
+  double* d_pseg = d_jt + 36 * nseg;
   check(cudaMemcpyAsync(d_fields, df.data(), sizeof(DevField) * df.size(), cudaMemcpyHostToDevice, st), "fields");
   check(cudaMemcpyAsync(d_vals, fvals.data(), sizeof(double) * fvals.size(), cudaMemcpyHostToDevice, st), "fields");
   check(cudaMemsetAsync(d_pgrad, 0, sizeof(double) * n_params, st), "memset");
+  check(cudaMemsetAsync(d_pseg, 0, sizeof(double) * 6 * n_params * nseg, st), "memset");
   dev::AdjFields AF{d_fields, (int)df.size(), d_vals, param_field, P.qomg, d_pgrad};
-  dev::AdjChain AC{};
-  const double x0[6] = {P.x0.x, P.b0.x * kC, P.x0.y, P.b0.y * kC, P.x0.z, P.b0.z * kC};
-  for (int i = 0; i < 6; ++i) AC.x0[i] = x0[i];
-  AC.t0 = P.t0 / kC;
-  AC.dt = dt;
-  AC.nf = (int)nf;
-  AC.nb = (int)nb;
-  AC.kb = d_kb;
-  AC.ckpt = d_ck;
-  AC.seg = d_seg;
-  AC.ckpt_stride_dir = ck_dir;
-  AC.seg_stride_dir = seg_dir;
-  dev::k_adj_rk4<<<1, 32, 0, st>>>(AF, AC);
+  dev::AdjSegs S{};
+  S.t0 = P.t0 / kC;
+  S.dt = dt;
+  S.nf = (int)nf;
+  S.nb = (int)nb;
+  S.knots = knots_.as<double>();
+  S.kb = d_kb;
+  S.nseg[0] = ns0;
+  S.nseg[1] = ns1;
+  S.base[0] = 0;
+  S.base[1] = ns0;
+  S.lam_loc = d_lam;
+  S.jt = d_jt;
+  S.pseg = d_pseg;
+  S.n_params = (int)n_params;
+  if (nseg > 0) {
+    dev::k_adj_rk4_segments<<<(unsigned)nseg, 32, 0, st>>>(AF, S);
+    dev::k_adj_rk4_combine<<<1, 64, 0, st>>>(S, d_pgrad);
+  }
   check(cudaGetLastError(), "trajectory adjoint");
-  ++last_launches;
+  last_launches += 2;
   return d_pgrad;
 }
 
@@ -552,7 +655,7 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
       lev_.as<double>(), lev_cap_, s_end, obs_.as<double>(), omega_.as<double>(), n_e, d_W, N, per, d_gs);
   dev::k_adj_spline_eval<<<(unsigned)((s_end - 1 + 255) / 256), 256, 0, st>>>(knots_.as<double>(), n, tstart_, tstop_,
                                                                              s_end, d_gs, lev_cap_, d_yb, d_pb);
-  dev::k_adj_spline_solve<<<1, 32, 0, st>>>(knots_.as<double>(), n, d_yb, d_pb, d_diag);
+  dev::k_adj_spline_solve<<<9, dev::kScanThreads, 0, st>>>(knots_.as<double>(), n, d_yb, d_pb, d_diag);
   // RK4 adjoint
   double* d_pgrad = rk4_adjoint(d_yb, param_field, n_params, st);
   if (grad_knots) check(cudaMemcpyAsync(grad_knots, d_yb, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, st), "download");

@@ -90,12 +90,15 @@ void Engine::upload_trajectory() {
   if (knots_version_ == model.knots_version && nknots_ == k.n) return;
   levels_dropped_ = false;
   const int64_t n = k.n;
-  knots_.reserve(sizeof(double) * 19 * n);
+  knots_.reserve(sizeof(double) * 20 * n);
   double* d = knots_.as<double>();
   check(cudaMemcpyAsync(d, k.t.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload t");
   check(cudaMemcpyAsync(d + n, k.y.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, stream), "upload y");
   check(cudaMemcpyAsync(d + 10 * n, k.ypp.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, stream),
         "upload ypp");
+  if ((int64_t)k.diag.size() == n)
+    check(cudaMemcpyAsync(d + 19 * n, k.diag.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream),
+          "upload diag");
   nknots_ = n;
   tstart_ = k.tstart;
   tstop_ = k.tstop;

@@ -649,7 +649,9 @@ void spline_second_derivatives(Knots& k) {
   const int64_t N = k.n;
   const double* X = k.t.data();
   k.ypp.assign(9 * N, 0.0);
-  std::vector<double> diag(N), sigv(N), pv(N);
+  std::vector<double>& diag = k.diag;
+  diag.assign(N, 0.0);
+  std::vector<double> sigv(N), pv(N);
   diag[0] = -0.5;
   for (int64_t i = 1; i < N - 1; ++i) {
     const double sig = (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]);

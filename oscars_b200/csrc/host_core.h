@@ -127,8 +127,9 @@ struct Rng {
 struct Knots {
   int64_t n = 0;
   std::vector<double> t, y, ypp;
+  std::vector<double> diag;  // factored diagonal of the spline system (depends on t only)
   double tstart = 0, tstop = 0;
-  void clear() { n = 0; t.clear(); y.clear(); ypp.clear(); }
+  void clear() { n = 0; t.clear(); y.clear(); ypp.clear(); diag.clear(); }
 };
 
 struct Error {

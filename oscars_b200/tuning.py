@@ -5,7 +5,9 @@ between the end poles) has one amplitude factor s_k per half-period (``add_bfiel
 half_period_scale=s)``).  ``UndulatorFlux.apply(s, problem)`` returns the fixed-level flux of every
 (observer, energy) entry as a torch tensor; its backward pass is the hand-written adjoint
 (``osc_flux_vjp``: reverse mode through the radiation sum, the trajectory spline and the RK4 steps,
-FP64, RK4 states recomputed from checkpoints every 256 steps).  PyTorch only carries the tensors.
+FP64; the RK4 part runs parallel in time over 64-step segments, each step's stages recomputed from
+the stored states, joined by a sweep of the segments' 6 x 6 Jacobians).  PyTorch only carries the
+tensors.
 
     problem = TuningProblem(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41,
                             obs=obs_xyz, energies_eV=E, level=12)
