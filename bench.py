@@ -20,7 +20,9 @@ path, weak scaling; the reported time is the max over ranks.
 and 512 uneven undulator jobs, each timed on the device (every chunk of jobs from its first to its
 last kernel, device RK4 and splines included) and end to end through the public API, beside the
 FP64 reference method on a subset of the same particles / jobs and the mixed-vs-FP64 error at a
-fixed level.  ``--only beam|uneven`` runs one of them alone.
+fixed level.  ``tuning`` adds the differentiable field-tuning workload (gradient of a flux loss with
+respect to 82 half-period undulator amplitudes) in grad/s.  ``--only beam|uneven|tuning`` runs one
+of them alone.
 
 ``--impl reference`` times the reference's own CPU implementation (oracle/_ref, built from the
 reference sources by oracle/Makefile; the CPU restatement in oracle/ when that build is absent)
@@ -355,6 +357,7 @@ def product_arm(args):
                                        "chunk of jobs from first to last kernel, trajectories included",
                                "epu_beam_10k": beam_leg(args.batched_steps, bw, local),
                                "uneven_512": uneven_leg(args.batched_steps, bw, local)}
+            line["tuning"] = tuning_leg(max(5, args.batched_steps), bw, local)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -526,6 +529,59 @@ def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12):
             "clocks": clk.summary()}
 
 
+# ---------------------------------------------------------------------------------------------
+# Differentiable field tuning: gradient of a flux loss with respect to 82 half-period amplitudes
+# ---------------------------------------------------------------------------------------------
+TUNING_WORKLOAD = ("41-period undulator B0=0.5T lambda=50mm with 82 half-period factors 1+delta, delta~N(0,0.005) "
+                   "(seed 82); 3 GeV; 20001-point RK4; loss=sum (F-F_ideal)^2 over 21x21 observers (2mm x 2mm at "
+                   "z=30m) x 256 energies over E1 +-5%; fixed level 12; FP64 forward and adjoint")
+
+
+def tuning_leg(steps, warmup, local=0, check_params=(3, 20, 41, 70)):
+    """One step = the forward flux and its adjoint gradient (osc_flux_multi + osc_flux_vjp); grad/s
+    with Richardson central differences (h = 1e-3, 3e-3) on a few factors as a check."""
+    import numpy as np
+    from oscars_b200.tuning import TuningProblem
+    xs = np.linspace(-0.001, 0.001, 21)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    obs = np.stack([X.ravel(), Y.ravel(), np.full(X.size, 30.0)], 1)
+    energies = np.linspace(0.95 * E1, 1.05 * E1, 256)
+    p = TuningProblem(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, obs=obs, energies_eV=energies,
+                      level=12, gpu=local)
+    s = 1 + np.random.default_rng(82).normal(0.0, 0.005, 82)
+    F_ideal = p.flux(np.ones(82))
+
+    def step():
+        F = p.flux(s)
+        return p.vjp(s, 2 * (F - F_ideal))[1]
+    for _ in range(warmup):
+        step()
+    t_fwd = t_all = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            F = p.flux(s)
+            t1 = time.perf_counter()
+            g = p.vjp(s, 2 * (F - F_ideal))[1]
+            t2 = time.perf_counter()
+            t_fwd += t1 - t0
+            t_all += t2 - t0
+    loss = lambda v: float(np.sum((p.flux(v) - F_ideal) ** 2))
+
+    def central(k, h):
+        e = np.zeros(82)
+        e[k] = h
+        return (loss(s + e) - loss(s - e)) / (2 * h)
+    fd = np.array([(9 * central(k, 1e-3) - central(k, 3e-3)) / 8 for k in check_params])
+    err = float(np.max(np.abs(g[list(check_params)] - fd)) / np.max(np.abs(fd)))
+    return {"workload": TUNING_WORKLOAD, "steps": steps, "warmup": warmup, "value": steps / t_all,
+            "unit": "grad/s", "ms_per_step": 1e3 * t_all / steps, "forward_ms": 1e3 * t_fwd / steps,
+            "adjoint_ms": 1e3 * (t_all - t_fwd) / steps,
+            "grad_vs_richardson_fd": {"value": err, "params": list(check_params), "steps": [1e-3, 3e-3]},
+            "path": "oscars_b200.tuning.TuningProblem.flux + vjp (osc_flux_multi, osc_flux_vjp); wall clock, "
+                    "host buffers", "clocks": clk.summary()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -537,7 +593,7 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (for profiler runs)")
     ap.add_argument("--batched-steps", type=int, default=3,
                     help="timed steps of the batched workloads (EPU beam, uneven jobs); 0 skips them")
-    ap.add_argument("--only", default="", choices=["", "beam", "uneven"],
+    ap.add_argument("--only", default="", choices=["", "beam", "uneven", "tuning"],
                     help="run one batched workload alone and print its JSON object (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -545,7 +601,7 @@ def main():
     elif args.only:
         import torch
         torch.cuda.set_device(0)
-        leg = beam_leg if args.only == "beam" else uneven_leg
+        leg = {"beam": beam_leg, "uneven": uneven_leg, "tuning": tuning_leg}[args.only]
         print(json.dumps(leg(args.batched_steps, args.warmup)), flush=True)
     else:
         product_arm(args)

@@ -182,6 +182,13 @@ OSC_API int osc_flux(osc_ctx* ctx, const double* obs_xyz, long long n_obs, doubl
 OSC_API int osc_spectrum(osc_ctx* ctx, const double obs[3], const double* energies_eV,
                          long long n_energies, const osc_rad_opts* opts, double* out,
                          int32_t* level_out, long long* n_not_converged);
+/* Flux of every (observer, energy) pair in one request (no reference counterpart: the reference
+ * computes one energy per calculate_flux call or one observer per calculate_spectrum call).  out has
+ * n_obs x n_energies values, observer-major with energies fastest; spectrum = 1 normalises like
+ * osc_spectrum (|current|), 0 like osc_flux. */
+OSC_API int osc_flux_multi(osc_ctx* ctx, const double* obs_xyz, long long n_obs, const double* energies_eV,
+                           long long n_energies, const osc_rad_opts* opts, int spectrum, double* out,
+                           int32_t* level_out, long long* n_not_converged);
 OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double* normals,
                               long long n_obs, int directional, const osc_rad_opts* opts,
                               double* out, int32_t* level_out, long long* n_not_converged);

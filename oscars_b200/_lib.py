@@ -75,6 +75,7 @@ SIGNATURES = {
     "osc_surface_rectangle": (I, [ctypes.c_char_p, I, I, D, D, DP, DP, I, DP, DP, DP]),
     "osc_flux": (I, [VP, DP, LL, D, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
     "osc_spectrum": (I, [VP, DP, DP, LL, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
+    "osc_flux_multi": (I, [VP, DP, LL, DP, LL, ctypes.POINTER(RadOpts), I, DP, I32P, LLP]),
     "osc_power_density": (I, [VP, DP, DP, LL, I, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
     "osc_flux_device": (I, [VP, VP, LL, D, ctypes.POINTER(RadOpts), VP, VP, VP]),
     "osc_power_density_device": (I, [VP, VP, VP, LL, I, ctypes.POINTER(RadOpts), VP, VP, VP]),

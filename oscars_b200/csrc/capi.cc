@@ -471,6 +471,27 @@ OSC_API int osc_flux_vjp(osc_ctx* ctx, const double* obs_xyz, long long n_obs, c
   });
 }
 
+OSC_API int osc_flux_multi(osc_ctx* ctx, const double* obs_xyz, long long n_obs, const double* energies_eV,
+                           long long n_energies, const osc_rad_opts* opts, int spectrum, double* out,
+                           int32_t* level_out, long long* n_not_converged) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (n_obs < 0 || n_energies < 0 || (n_obs > 0 && n_energies > 0 && (!obs_xyz || !energies_eV || !out)))
+      throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    osc::RadRequest rq;
+    rq.obs = obs_xyz;
+    rq.n_obs = n_obs;
+    rq.omega.resize(n_energies);
+    for (long long i = 0; i < n_energies; ++i) rq.omega[i] = osc::ev_to_omega(energies_eV[i]);
+    rq.opts = *opts;
+    rq.spectrum_current_abs = spectrum != 0;
+    rq.out = out;
+    rq.level_out = level_out;
+    ctx->eng->radiation(rq);
+    if (n_not_converged) *n_not_converged = ctx->eng->last_not_converged;
+  });
+}
+
 OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double* normals, long long n_obs,
                               int directional, const osc_rad_opts* opts, double* out, int32_t* level_out,
                               long long* n_not_converged) {

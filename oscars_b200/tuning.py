@@ -63,18 +63,8 @@ class TuningProblem:
         self.set_scale(s)
         n_o, n_e = self.shape
         out = np.zeros(n_o * n_e)
-        lv = np.zeros(n_o * n_e, dtype=np.int32)
-        if self.spectrum or n_o == 1:
-            if n_o != 1:
-                raise ValueError("spectrum problems have one observer")
-            self.sr._ctx.call("osc_spectrum", _lib.dptr(self.obs[0].copy()), _lib.dptr(self.energies), n_e,
-                              ctypes.byref(self._opts), _lib.dptr(out), _lib.i32ptr(lv), None)
-        else:
-            for j, e in enumerate(self.energies):
-                col = np.zeros(n_o)
-                self.sr._ctx.call("osc_flux", _lib.dptr(self.obs), n_o, float(e), ctypes.byref(self._opts),
-                                  _lib.dptr(col), _lib.i32ptr(lv[:n_o].copy()), None)
-                out[j::n_e] = col
+        self.sr._ctx.call("osc_flux_multi", _lib.dptr(self.obs), n_o, _lib.dptr(self.energies), n_e,
+                          ctypes.byref(self._opts), 1 if self.spectrum else 0, _lib.dptr(out), None, None)
         return out.reshape(n_o, n_e)
 
     def vjp(self, s, grad_flux, knots=False):

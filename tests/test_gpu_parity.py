@@ -92,3 +92,34 @@ def test_device_entry_point_matches_host_entry_point():
                 ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(lvl.data_ptr()), None)
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), host)
+
+
+def test_flux_multi_matches_single_energy_calls():
+    """osc_flux_multi (all observers x energies in one request) against osc_flux per energy and
+    osc_spectrum, FP64, fixed level."""
+    import ctypes
+    from oscars_b200 import _lib
+    from oscars_b200._lib import RadOpts
+    s = _sr()
+    run_case(s, UND_SETUP)
+    xyz, _, _ = s._rectangle([7, 5], "XY", [0.004, 0.004], None, None, [0, 0, 30], 0, False)
+    xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    E = np.array([440.0, 458.9458, 470.0])
+    o = RadOpts(precision=0.0, max_level=11, max_level_extended=0, nparticles=0, quantity=0, precision_mode=0)
+    o.horizontal[:] = [1, 0, 0]
+    o.propagation[:] = [0, 0, 1]
+    n = xyz.shape[0]
+    multi = np.zeros(n * E.size)
+    s._ctx.call("osc_flux_multi", _lib.dptr(xyz), n, _lib.dptr(E), E.size, ctypes.byref(o), 0, _lib.dptr(multi),
+                None, None)
+    for j, e in enumerate(E):
+        one = np.zeros(n)
+        s._ctx.call("osc_flux", _lib.dptr(xyz), n, float(e), ctypes.byref(o), _lib.dptr(one), None, None)
+        assert _peak_rel(multi[j::E.size], one) <= 1e-12
+    spec = np.zeros(E.size)
+    s._ctx.call("osc_spectrum", _lib.dptr(xyz[3].copy()), _lib.dptr(E), E.size, ctypes.byref(o), _lib.dptr(spec),
+                None, None)
+    one_obs = np.zeros(E.size)
+    s._ctx.call("osc_flux_multi", _lib.dptr(xyz[3].copy()), 1, _lib.dptr(E), E.size, ctypes.byref(o), 1,
+                _lib.dptr(one_obs), None, None)
+    assert _peak_rel(one_obs, spec) <= 1e-12
