@@ -14,7 +14,9 @@ sample = one (observer, energy, trajectory point) term of the radiation sum, cou
 ``e2e``    the same job through the C ABI with host buffers: host RK4 + spline, host->device
            copies, kernels, device->host copy of the results, every step.
 Under torchrun each rank runs its own job (energy E1 * (1 + 1e-3 rank)): no collective on the data
-path, weak scaling; the reported time is the max over ranks.
+path, weak scaling; the reported time is the max over ranks.  The 10k-particle EPU beam is then run
+split over the ranks (``epu_beam_10k_sharded``: particles round-robin, one NCCL all_reduce of the
+partial fluxes, strong scaling).
 
 ``batched`` (single GPU) adds the two batched workloads: a 10k-particle EPU beam (101 x 101 flux)
 and 512 uneven undulator jobs, each timed on the device (every chunk of jobs from its first to its
@@ -334,6 +336,12 @@ def product_arm(args):
         e2e_value = e2e_samples / sum(e2e_times) / 1e9
     h2d = xyz.nbytes + 19 * 20001 * 8 + 8
     d2h = out_h.nbytes + lvl_h.nbytes
+    sharded = None
+    if world > 1 and args.batched_steps > 0:  # every rank takes part in its collectives
+        try:
+            sharded = sharded_beam_leg(args.batched_steps, max(3, args.warmup), local, rank, world)
+        except Exception as e:  # reported in the line; the headline stands
+            sharded = {"error": "%s: %s" % (type(e).__name__, e)}
     if rank == 0:
         cpu = cpu_baseline_leg() if world == 1 else None
         r = res[head]
@@ -358,6 +366,8 @@ def product_arm(args):
                                "epu_beam_10k": beam_leg(args.batched_steps, bw, local),
                                "uneven_512": uneven_leg(args.batched_steps, bw, local)}
             line["tuning"] = tuning_leg(max(5, args.batched_steps), bw, local)
+        if sharded is not None:
+            line["epu_beam_10k_sharded"] = sharded
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -529,6 +539,51 @@ def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12):
             "clocks": clk.summary()}
 
 
+def sharded_beam_leg(steps, warmup, local, rank, world):
+    """The EPU beam split over the ranks (torchrun): every rank draws the same 10k particles,
+    integrates particles rank, rank + W, ... (shard option, weight 1/N) and one NCCL all_reduce sums
+    the 101 x 101 partial fluxes.  Device time per rank (profiled chunks + the all_reduce on the
+    current stream), max over ranks; samples summed over ranks."""
+    import ctypes
+    import torch
+    import torch.distributed as dist
+    from oscars_b200.shard import allreduce_sum
+    from oscars_b200.sr import sr
+    s = sr(gpu=1, device=local)
+    setup_epu_beam(s)
+    kw = dict(energy_eV=E1_EPU, npoints=[101, 101], width=[0.008, 0.008], translation=[0, 0, 30], return_numpy=True,
+              nparticles=BEAM_PARTICLES, compute="mixed", shard=(rank, world))
+
+    def run():
+        s.set_seed(1)
+        return allreduce_sum(s.calculate_flux_rectangle(**kw)[1])
+    for _ in range(warmup):
+        run()
+    dev_ms = 0.0
+    samples = 0
+    stream = torch.cuda.current_stream()
+    dist.barrier()
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        _, ms, sm, _, _ = _profiled(s._ctx, lambda: s.calculate_flux_rectangle(**kw))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        part = torch.zeros(101 * 101, dtype=torch.float64, device="cuda")
+        a.record(stream)
+        dist.all_reduce(part)
+        b.record(stream)
+        torch.cuda.synchronize()
+        dev_ms += ms + a.elapsed_time(b)
+        samples += sm
+    t = torch.tensor([dev_ms, float(samples)], dtype=torch.float64, device="cuda")
+    tmax, tsum = t.clone(), t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return {"workload": BEAM_WORKLOAD + "; particles round-robin over %d ranks, one NCCL all_reduce" % world,
+            "steps": steps, "warmup": warmup, "value": float(tsum[1]) / (float(tmax[0]) * 1e-3) / 1e9,
+            "unit": "Gsamples/s", "ms_per_step": float(tmax[0]) / steps, "scaling": "strong",
+            "timing": "device time per rank (batch chunks + all_reduce), max over ranks"}
+
+
 # ---------------------------------------------------------------------------------------------
 # Differentiable field tuning: gradient of a flux loss with respect to 82 half-period amplitudes
 # ---------------------------------------------------------------------------------------------
@@ -582,6 +637,13 @@ def tuning_leg(steps, warmup, local=0, check_params=(3, 20, 41, 70)):
                     "host buffers", "clocks": clk.summary()}
 
 
+def _free_port():
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -593,11 +655,26 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (for profiler runs)")
     ap.add_argument("--batched-steps", type=int, default=3,
                     help="timed steps of the batched workloads (EPU beam, uneven jobs); 0 skips them")
-    ap.add_argument("--only", default="", choices=["", "beam", "uneven", "tuning"],
+    ap.add_argument("--only", default="", choices=["", "beam", "uneven", "tuning", "sharded"],
                     help="run one batched workload alone and print its JSON object (for profiler runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.only == "sharded":  # the split beam on the ranks of torchrun (or a 1-rank group)
+        import torch
+        import torch.distributed as dist
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        if world > 1:
+            dist.init_process_group("nccl")
+        else:
+            dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % _free_port(), rank=0, world_size=1)
+        r = sharded_beam_leg(args.batched_steps, args.warmup, local, rank, world)
+        if rank == 0:
+            print(json.dumps(r), flush=True)
+        dist.destroy_process_group()
     elif args.only:
         import torch
         torch.cuda.set_device(0)

@@ -124,6 +124,12 @@ typedef struct {
   int nparticles;           /* 0 = the current particle; N = N random particles, weight 1/N */
   int quantity;             /* osc_quantity */
   int precision_mode;       /* osc_precision_mode */
+  /* Multi-particle requests split over processes (no reference counterpart): with shard_count > 1
+   * all N particles are still drawn in order, but only those with index % shard_count == shard_rank
+   * are integrated, each with weight 1/N, so the shards' outputs add up to the whole request (one
+   * all-reduce).  0 / 0 (or 0 / 1) = the whole request. */
+  int shard_rank;
+  int shard_count;
 } osc_rad_opts;
 
 /* ---- device / context ---------------------------------------------------------------------- */
@@ -153,6 +159,12 @@ OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* beam);
 OSC_API int osc_set_seed(osc_ctx* ctx, int seed);                  /* TRandomA::SetSeed */
 OSC_API int osc_set_new_particle(osc_ctx* ctx, int ideal);         /* OSCARSSR::SetNewParticle */
 OSC_API int osc_get_particle(osc_ctx* ctx, double x0[3], double beta0[3], double* t0, double* gamma);
+/* Draw n particles from the beam exactly as a request with nparticles = n does (advancing the
+ * context's random sequence the same way) and return those of shard shard_rank of shard_count
+ * (index % shard_count == shard_rank): 6 doubles each (x0[3] [m], beta0[3]) in out, their number in
+ * *n_out (out must hold 6 * ceil(n / shard_count) doubles).  Works on host-only contexts. */
+OSC_API int osc_beam_particles(osc_ctx* ctx, long long n, int shard_rank, int shard_count, double* out,
+                               long long* n_out);
 OSC_API int osc_set_ctstartstop(osc_ctx* ctx, double start, double stop);       /* :637-647 */
 OSC_API int osc_get_ctstartstop(osc_ctx* ctx, double* start, double* stop);
 OSC_API int osc_set_npoints_trajectory(osc_ctx* ctx, long long n);

@@ -73,6 +73,7 @@ def load():
     lib.orc_normal.restype = D
     lib.orc_set_new_particle.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.orc_get_particle.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp]
+    lib.orc_set_particle.argtypes = [ctypes.c_void_p, dp, dp, D]
     lib.orc_calculate_trajectory.argtypes = [ctypes.c_void_p]
     lib.orc_trajectory_npoints.argtypes = [ctypes.c_void_p]
     lib.orc_trajectory_npoints.restype = ctypes.c_long
@@ -462,6 +463,11 @@ class OracleSR:
         self._check(self._lib.orc_add_epu(self._h, _dp(A), _dp(B), _dp(Pp), int(nperiods), _dp(T),
                                           float(phase), float(taper), float(frequency),
                                           float(frequency_phase), float(time_offset)))
+
+    def set_particle(self, x0, beta0, t0=0.0):
+        """Use a particle of the beam's species with these initial conditions."""
+        a = lambda v: np.ascontiguousarray(np.array(v, dtype=np.float64))
+        self._check(self._lib.orc_set_particle(self._h, _dp(a(x0)), _dp(a(beta0)), float(t0)))
 
     def get_bfield(self, x, t=0):
         X = np.array(_v3(x), dtype=np.float64)

@@ -646,6 +646,17 @@ int orc_set_new_particle(orc_sim* s, int ideal) {
   return ORC_OK;
 }
 
+int orc_set_particle(orc_sim* s, const double x0[3], const double b0[3], double t0) {
+  if (!s->has_beam) return fail(s, ORC_ERR_STATE, "no beam defined");
+  orc_particle p;
+  memset(&p, 0, sizeof p);
+  p.q = s->beam.q; p.m = s->beam.m; p.current = s->beam.current;
+  particle_set_conditions(&p, V(x0[0], x0[1], x0[2]), V(b0[0], b0[1], b0[2]), t0);
+  s->p = p;
+  traj_clear(&s->tr);
+  return ORC_OK;
+}
+
 int orc_get_particle(const orc_sim* s, double x0[3], double b0[3], double* t0, double* gamma,
                      double* q, double* m, double* current) {
   x0[0] = s->p.x0.x; x0[1] = s->p.x0.y; x0[2] = s->p.x0.z;

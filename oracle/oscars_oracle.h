@@ -64,6 +64,8 @@ int orc_set_seed(orc_sim*, int seed);
 double orc_uniform(orc_sim*);
 double orc_normal(orc_sim*);
 int orc_set_new_particle(orc_sim*, int ideal);
+/* A particle of the beam's species at the given initial conditions (as a drawn particle would be). */
+int orc_set_particle(orc_sim*, const double x0[3], const double b0[3], double t0);
 int orc_get_particle(const orc_sim*, double x0[3], double b0[3], double* t0, double* gamma,
                      double* q, double* m, double* current);
 

@@ -41,7 +41,7 @@ class BeamDesc(ctypes.Structure):
 class RadOpts(ctypes.Structure):
     _fields_ = [("polarization", I), ("angle", D), ("horizontal", D * 3), ("propagation", D * 3),
                 ("precision", D), ("max_level", I), ("max_level_extended", I), ("nparticles", I),
-                ("quantity", I), ("precision_mode", I)]
+                ("quantity", I), ("precision_mode", I), ("shard_rank", I), ("shard_count", I)]
 
 
 class JobDesc(ctypes.Structure):
@@ -66,6 +66,7 @@ SIGNATURES = {
     "osc_set_seed": (I, [VP, I]),
     "osc_set_new_particle": (I, [VP, I]),
     "osc_get_particle": (I, [VP, DP, DP, DP, DP]),
+    "osc_beam_particles": (I, [VP, LL, I, I, DP, LLP]),
     "osc_set_ctstartstop": (I, [VP, D, D]),
     "osc_get_ctstartstop": (I, [VP, DP, DP]),
     "osc_set_npoints_trajectory": (I, [VP, LL]),

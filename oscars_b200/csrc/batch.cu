@@ -784,7 +784,7 @@ int Engine::batch_resident(int v) {
 
 void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
                    int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
-                   bool average, double* out, int32_t* level_out) {
+                   bool average, double* out, int32_t* level_out, double average_weight) {
   pending_.clear();
   last_samples = last_launches = last_not_converged = 0;
   if (jobs.empty()) return;
@@ -1054,7 +1054,8 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     // results of the chunk
     if (average) {
       dev::k_batch_average<<<(unsigned)((m_avg + 255) / 256), 256, 0, st>>>(
-          b_out_.as<double>(), d_jobs, nj, m_avg, 1.0 / (double)jobs.size(), b_acc_.as<double>(),
+          b_out_.as<double>(), d_jobs, nj, m_avg, average_weight > 0 ? average_weight : 1.0 / (double)jobs.size(),
+          b_acc_.as<double>(),
           b_acc_.as<double>() + m_avg);
       check(cudaGetLastError(), "batch average");
       ++last_launches;

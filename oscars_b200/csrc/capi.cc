@@ -66,6 +66,8 @@ void check_opts(const osc_rad_opts* o) {
     throw osc::Error{OSC_ERR_INVALID, "'quantity' must be: 'flux', 'precision', 'level', or blank"};
   if (o->precision_mode != OSC_FP64 && o->precision_mode != OSC_MIXED)
     throw osc::Error{OSC_ERR_INVALID, "unknown precision mode"};
+  if (o->shard_count < 0 || (o->shard_count > 1 && (o->shard_rank < 0 || o->shard_rank >= o->shard_count)))
+    throw osc::Error{OSC_ERR_RANGE, "shard_rank must be in [0, shard_count)"};
 }
 
 }  // namespace
@@ -256,6 +258,27 @@ OSC_API int osc_set_new_particle(osc_ctx* ctx, int ideal) {
     if (!M.has_beam) throw osc::Error{OSC_ERR_RANGE, "no beam defined"};
     if (ideal) M.ideal_particle();
     else M.random_particle();
+  });
+}
+
+OSC_API int osc_beam_particles(osc_ctx* ctx, long long n, int shard_rank, int shard_count, double* out,
+                               long long* n_out) {
+  return guarded(ctx, [&] {
+    osc::Model& M = ctx->eng->model;
+    if (!M.has_beam) throw osc::Error{OSC_ERR_RANGE, "no beam defined"};
+    if (n < 0 || !out) throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    const int cnt = shard_count > 1 ? shard_count : 1;
+    if (shard_rank < 0 || shard_rank >= cnt) throw osc::Error{OSC_ERR_RANGE, "shard_rank must be in [0, shard_count)"};
+    long long k = 0;
+    for (long long ip = 0; ip < n; ++ip) {
+      M.random_particle();
+      if (ip % cnt != shard_rank) continue;
+      const osc::Particle& p = M.particle;
+      const double v[6] = {p.x0.x, p.x0.y, p.x0.z, p.b0.x, p.b0.y, p.b0.z};
+      for (int i = 0; i < 6; ++i) out[6 * k + i] = v[i];
+      ++k;
+    }
+    if (n_out) *n_out = k;
   });
 }
 

@@ -508,8 +508,10 @@ void Engine::radiation(RadRequest& rq) {
     acc_comp_.reserve(sizeof(double) * N);
     check(cudaMemsetAsync(acc_.p, 0, sizeof(double) * N, st), "memset");
     check(cudaMemsetAsync(acc_comp_.p, 0, sizeof(double) * N, st), "memset");
+    const int shards = rq.opts.shard_count > 1 ? rq.opts.shard_count : 1;
     for (int ip = 0; ip < np; ++ip) {
       model.random_particle();
+      if (ip % shards != rq.opts.shard_rank % shards) continue;  // another process's particle
       model.compute_trajectory();  // host RK4 of particle ip overlaps the GPU work of particle ip-1
       check(cudaStreamSynchronize(st), "particle");
       upload_trajectory();
@@ -543,10 +545,14 @@ void Engine::radiation_beam_mixed(RadRequest& rq, int64_t N) {
     check(cudaMemcpy(obs_h.data(), rq.obs, sizeof(double) * 3 * rq.n_obs, cudaMemcpyDeviceToHost), "observers");
     obs = obs_h.data();
   }
-  std::vector<BatchJob> jobs(np);
+  const int shards = rq.opts.shard_count > 1 ? rq.opts.shard_count : 1;
+  std::vector<BatchJob> jobs;
+  jobs.reserve(np / shards + 1);
   for (int ip = 0; ip < np; ++ip) {
     model.random_particle();
-    BatchJob& J = jobs[ip];
+    if (ip % shards != rq.opts.shard_rank % shards) continue;  // another process's particle
+    jobs.emplace_back();
+    BatchJob& J = jobs.back();
     J.field_begin = 0;
     J.field_count = (int)model.fields.size();
     J.particle = model.particle;
@@ -572,7 +578,12 @@ void Engine::radiation_beam_mixed(RadRequest& rq, int64_t N) {
     out = out_h.data();
     lvl = lvl_h.data();
   }
-  batch(model.fields, jobs, obs, rq.n_obs, rq.omega.data(), n_e, rq.opts, true, out, lvl);
+  if (jobs.empty()) {  // this shard has no particle: its share of the sum is zero
+    std::fill(out, out + N, 0.0);
+    if (lvl) std::fill(lvl, lvl + N, -1);
+  } else {
+    batch(model.fields, jobs, obs, rq.n_obs, rq.omega.data(), n_e, rq.opts, true, out, lvl, 1.0 / (double)np);
+  }
   if (rq.out_on_device) {
     check(cudaMemcpy(rq.out, out_h.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "result");
     if (rq.level_out)

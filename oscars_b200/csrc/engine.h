@@ -77,7 +77,7 @@ class Engine {
   // when averaging).
   void batch(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
              int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o, bool average,
-             double* out, int32_t* level_out);
+             double* out, int32_t* level_out, double average_weight = 0.0);  // 0: 1 / jobs
   // The same jobs one after another through the single-trajectory FP64 path (host RK4).
   void batch_fp64(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
                   int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,

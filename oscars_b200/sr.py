@@ -10,6 +10,10 @@ here with the binding's file:line.
 Extensions, all keyword-only and off by default:
   ``compute='fp64'|'mixed'``   arithmetic of the radiation sums (see include/oscars_b200.h)
   ``return_numpy=True``        return (positions, values) arrays instead of nested lists
+  ``shard=(rank, count)``      this process's share of a multi-particle request (particles with
+                               index % count == rank, weight 1/N): the shares add up to the whole
+  ``half_period_scale=...``    (add_bfield_undulator) per-half-period amplitude factors
+  ``add_bfield_grid(...)``     a grid field from memory (the file readers are add_bfield_file)
 """
 from __future__ import annotations
 
@@ -303,6 +307,15 @@ class sr:
         self._ctx.call("osc_get_particle", dptr(x0), dptr(b0), ctypes.byref(t0), ctypes.byref(g))
         return x0, b0, t0.value, g.value
 
+    def beam_particles(self, n, shard=(0, 1)):
+        """The particles a request with nparticles = n draws (same random sequence), restricted to
+        shard (rank, count): array (k, 6) of x0 [m] and beta0."""
+        rank, count = int(shard[0]), int(shard[1])
+        out = np.zeros(6 * ((int(n) + count - 1) // count + 1))
+        k = ctypes.c_longlong()
+        self._ctx.call("osc_beam_particles", int(n), rank, count, dptr(out), ctypes.byref(k))
+        return out[:6 * k.value].reshape(k.value, 6)
+
     def get_particle_x0(self):
         return list(map(float, self._particle()[0]))
 
@@ -362,8 +375,13 @@ class sr:
             raise ValueError("gpu=0 selects the reference's CPU path; this build computes on the GPU only")
 
     def _opts(self, polarization, angle, horizontal_direction, propogation_direction, precision, max_level,
-              max_level_extended, nparticles, quantity, compute):
+              max_level_extended, nparticles, quantity, compute, shard=None):
         o = RadOpts()
+        if shard is not None:  # (rank, count): this process's share of a multi-particle request
+            rank, count = int(shard[0]), int(shard[1])
+            if count < 1 or not 0 <= rank < count:
+                raise ValueError("'shard' must be (rank, count) with 0 <= rank < count")
+            o.shard_rank, o.shard_count = rank, count
         o.polarization = _polarization(polarization, angle)
         o.angle = float(angle)
         o.horizontal[:] = _vec3(horizontal_direction, "translation") if horizontal_direction else [1.0, 0.0, 0.0]
@@ -404,7 +422,8 @@ class sr:
     def calculate_spectrum(self, obs, npoints=0, energy_range_eV=None, energy_points_eV=None, points_eV=None,
                            polarization="", angle=_ANGLE_UNSET, horizontal_direction=None, propogation_direction=None,
                            precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, nthreads=0, gpu=-1,
-                           ngpu=None, quantity="flux", ofile="", bofile="", *, compute="fp64", return_numpy=False):
+                           ngpu=None, quantity="flux", ofile="", bofile="", *, compute="fp64", return_numpy=False,
+                           shard=None):
         if nparticles < 0:
             raise ValueError("'nparticles' must be >= 1 (sort of)")
         if points_eV is not None:
@@ -414,7 +433,7 @@ class sr:
         self._check_gpu(gpu, nthreads)
         q = _quantity(quantity)
         o = self._opts(polarization, angle, horizontal_direction, propogation_direction, precision, max_level,
-                       max_level_extended, nparticles, q, compute)
+                       max_level_extended, nparticles, q, compute, shard)
         out = np.zeros(E.size)
         lv = np.zeros(E.size, dtype=np.int32)
         nnc = ctypes.c_longlong()
@@ -463,7 +482,8 @@ class sr:
                                  rotations=None, translation=None, x0x1x2=None, polarization="", angle=_ANGLE_UNSET,
                                  horizontal_direction=None, propogation_direction=None, nparticles=0, nthreads=0,
                                  gpu=-1, ngpu=None, precision=0.01, max_level=-2, max_level_extended=0,
-                                 quantity="flux", ofile="", bofile="", *, compute="fp64", return_numpy=False):
+                                 quantity="flux", ofile="", bofile="", *, compute="fp64", return_numpy=False,
+                                 shard=None):
         if self._nbeams < 1:
             raise ValueError("No particle beam defined")
         if dim not in (2, 3):
@@ -474,7 +494,7 @@ class sr:
         self._check_gpu(gpu, nthreads)
         q = _quantity(quantity)
         o = self._opts(polarization, angle, horizontal_direction, propogation_direction, precision, max_level,
-                       max_level_extended, nparticles, q, compute)
+                       max_level_extended, nparticles, q, compute, shard)
         n = xyz.size // 3
         out = np.zeros(n)
         lv = np.zeros(n, dtype=np.int32)
@@ -490,7 +510,7 @@ class sr:
                                           rotations=None, translation=None, ofile="", bofile="", normal=0,
                                           nparticles=0, gpu=-1, ngpu=None, nthreads=0, precision=0.01, max_level=-2,
                                           max_level_extended=0, dim=2, quantity="power density", *, compute="fp64",
-                                          return_numpy=False):
+                                          return_numpy=False, shard=None):
         if self._nbeams < 1:
             raise ValueError("No particle beam defined")
         if dim not in (2, 3):
@@ -500,7 +520,8 @@ class sr:
             raise ValueError("'nparticles' must be >= 1 (sort of)")
         self._check_gpu(gpu, nthreads)
         q = _quantity(quantity, pd=True)
-        o = self._opts("", _ANGLE_UNSET, None, None, precision, max_level, max_level_extended, nparticles, q, compute)
+        o = self._opts("", _ANGLE_UNSET, None, None, precision, max_level, max_level_extended, nparticles, q, compute,
+                       shard)
         n = xyz.size // 3
         out = np.zeros(n)
         lv = np.zeros(n, dtype=np.int32)

@@ -184,3 +184,21 @@ def test_batch_grid_and_halfscale_fields_match_fp64():
         e = _err(a, b)
         print("grid/halfscale job: mixed vs fp64 %.3e" % e)
         assert e <= TOL
+
+
+@pytest.mark.parametrize("compute,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
+def test_particle_shards_add_up_to_the_whole_request(compute, tol):
+    """shard=(rank, count): each share integrates particles rank, rank + count, ... with weight 1/N."""
+    from oscars_b200.sr import sr
+    setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=5))]
+    kw = dict(energy_eV=E1_EPU, npoints=[9, 9], width=[0.006, 0.006], translation=[0, 0, 30], nparticles=7,
+              precision=0, max_level=10, compute=compute, return_numpy=True)
+    s = sr(gpu=1)
+    run_case(s, setup)
+    whole = s.calculate_flux_rectangle(**kw)[1]
+    total = np.zeros_like(whole)
+    for r in range(3):
+        t = sr(gpu=1)
+        run_case(t, setup)
+        total += t.calculate_flux_rectangle(shard=(r, 3), **kw)[1]
+    assert _err(total, whole) <= tol
