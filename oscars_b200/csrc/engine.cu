@@ -76,7 +76,7 @@ Engine::~Engine() {
   for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
                     &act_[1], &cnt_, &acc_, &acc_comp_, &mrec_, &b_fields_, &b_fvals_, &b_obs_, &b_omega_, &b_acc_, &b_jobs_,
                     &b_knots_, &b_work_, &b_rec_, &b_rec_ext_, &b_state_, &b_out_, &b_lvl_, &b_act_[0], &b_act_[1],
-                    &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_})
+                    &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_, &fused_})
     b->release();
   if (stream) cudaStreamDestroy(stream);
 }
@@ -314,17 +314,18 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   const int tile = mixed ? mixed_entries_per_cta(variant) : 128;
   const int64_t target = 4 * (int64_t)resident;   // >= 4 waves of equal units per launch
   const int64_t N = n_items;
-  // partial-sum buffer: the largest plan over every possible active count of every level
-  // partial-sum buffer and per-level grid: the largest plan over every possible active count
-  size_t part_doubles = 0;
-  std::vector<int64_t> grid_of(lstop + 1, 1);
+  // Partial-sum buffer: a wave has tiles x spans units with spans the smallest power of two reaching
+  // the target (wave_spans), so tiles x spans < max(tiles, 2 x target) whatever the active count;
+  // every unit stores 2 segments x `per` values for each of its `tile` entry slots.
   const int per = rq.power_density ? 1 : kFdPartials;
   const int64_t ntiles = (N + tile - 1) / tile;
+  const size_t part_doubles = (size_t)2 * per * tile * std::max<int64_t>(ntiles, 2 * target);
+  // per-level grid: the largest unit count over the active counts the level can have
+  std::vector<int64_t> grid_of(lstop + 1, 1);
   for (int L = Lfirst; L <= lstop; ++L) {
     for (int64_t t = 1;; t = t < 256 ? t + 1 : t + t / 8) {
       const int64_t n = std::min(N, t * tile);
       const WavePlan pl = wave_plan(L == Lfirst, L, n, tile, target, kMinSpan);
-      part_doubles = std::max(part_doubles, (size_t)pl.nseg * pl.spans * per * n);
       grid_of[L] = std::max(grid_of[L], pl.tiles * pl.spans);
       if (t >= ntiles) break;
       if (L == Lfirst) t = ntiles - 1;  // the first wave always has all N entries
@@ -340,6 +341,18 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);
   check(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), st), "memset");
   check(cudaMemsetAsync(c64, 0, 3 * sizeof(unsigned long long), st), "memset");
+  // Flux / spectrum waves finalize their own tiles (one launch per level).  Wave w reads its active
+  // count from fz3[w % 3], appends survivors to fz3[(w + 1) % 3] and zeroes fz3[(w + 2) % 3] for the
+  // wave after; it takes units from fw[w % 2] and zeroes fw[(w + 1) % 2].
+  const bool fused = !rq.power_density;
+  unsigned* fz3 = nullptr;
+  unsigned long long* fw = nullptr;
+  if (fused) {
+    fused_.reserve(64 + sizeof(unsigned) * (size_t)(ntiles + 1));
+    fz3 = fused_.as<unsigned>();
+    fw = reinterpret_cast<unsigned long long*>(fz3 + 4);
+    check(cudaMemsetAsync(fused_.p, 0, 64 + sizeof(unsigned) * (size_t)(ntiles + 1), st), "memset");
+  }
 
   const double* d_obs = obs_.as<double>();
   const double* d_nrm = rq.normals ? nrm_.as<double>() : nullptr;
@@ -366,10 +379,41 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   int cur_list = 0;
   auto launch_wave = [&](int L) {
     const bool first = L == Lfirst;
+    const int wv = L - Lfirst;
     const int* act_in = first ? nullptr : act_[cur_list].as<int>();
-    const unsigned* nact_in = first ? nullptr : cnt + cur_list;
-    unsigned* n_next = cnt + (cur_list ^ 1);
-    check(cudaMemsetAsync(n_next, 0, sizeof(unsigned), st), "memset");
+    const unsigned* nact_in = first ? nullptr : (fused ? fz3 + wv % 3 : cnt + cur_list);
+    unsigned* n_next = fused ? fz3 + (wv + 1) % 3 : cnt + (cur_list ^ 1);
+    if (!fused) check(cudaMemsetAsync(n_next, 0, sizeof(unsigned), st), "memset");
+    if (fused) {
+      FdWaveArgs w{};
+      w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
+      w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
+      w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
+      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
+      w.part = part_.as<double>(); w.err = cnt + 2; w.work = fw + wv % 2;
+      w.fused = 1;
+      w.tile_done = fz3 + 16;
+      w.zero_u32 = fz3 + (wv + 2) % 3;
+      w.zero_u64 = fw + (wv + 1) % 2;
+      FdFinalArgs& f = w.fin;
+      f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
+      f.project = project; f.tile_entries = tile; f.min_span = kMinSpan; f.target_units = target;
+      f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
+      f.precision = o.precision; f.c0 = c0; f.c2 = c2; f.weight = weight;
+      for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
+      f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
+      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = nullptr;
+      f.dmax_spans_joined = mixed && mixed_variant_is_split(variant);
+      auto ev = timed_begin(st);
+      const int g = (int)std::min<int64_t>(grid_of[L], resident);
+      if (mixed) check(launch_fd_wave_mixed(w, frame_, g, variant, st), "flux wave (mixed)");
+      else check(launch_fd_wave_fp64(w, g, variant, st), "flux wave");
+      timed_end(ev, st);
+      last_launches += 1;
+      cur_list ^= 1;
+      return;
+    }
     if (!rq.power_density) {
       FdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
@@ -418,7 +462,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   for (int L = Lfirst; L <= Lpre; ++L) launch_wave(L);
   for (int L = Lpre + 1; L <= lstop; ++L) {  // beyond the prefilled levels the host decides
     unsigned nn = 0;
-    check(cudaMemcpyAsync(&nn, cnt + cur_list, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
+    const unsigned* active = fused ? fz3 + (L - Lfirst) % 3 : cnt + cur_list;
+    check(cudaMemcpyAsync(&nn, active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
     check(cudaStreamSynchronize(st), "count");
     if (nn == 0) break;
     if (mixed) ensure_mixed(L);

@@ -131,7 +131,7 @@ class Engine {
   int stats_slot_ = 0;
   std::vector<int> pending_;
   // kernel variants: kind 0 = FP64 flux, 1 = FP64 power density, 2 = mixed flux, 3 = batched mixed
-  int wave_grid_[4][8] = {};
+  int wave_grid_[4][16] = {};
   int wave_grid(int kind, int variant);
   std::map<std::tuple<int, int, int, int>, int> tuned_;   // (kind, log2 entries, first level, last level) -> variant
   int current_variant_[4] = {2, 0, 3, 3};
@@ -140,6 +140,7 @@ class Engine {
   bool tuning_ = false;
   // request scratch
   DevBuf obs_, nrm_, omega_, out_, lvl_, state_, part_, act_[2], cnt_;
+  DevBuf fused_;                   // fused waves: rotating counts, unit counters, per-tile counters
   DevBuf acc_, acc_comp_;          // multi-particle compensated accumulation
   // mixed-precision records (3 x float4 per sample, same indexing as the level cache)
   DevBuf mrec_;

@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "kernels.h"
+
 namespace osc {
 namespace dev {
 
@@ -98,6 +100,17 @@ __device__ __forceinline__ float mixed_sample(const float4 r0, const float4 r1, 
   return ph;
 }
 
+// The phase alone, with the operations of mixed_sample (same value).
+__device__ __forceinline__ float mixed_phase(const float4 r0, float Ox, float Oy, float Oz, float w, float wc) {
+  const float rx = Ox - r0.x, ry = Oy - r0.y, rz = Oz - r0.z;
+  const float rho2 = fmaf(rx, rx, ry * ry);
+  const float d2 = fmaf(rz, rz, rho2);
+  const float iD = rsqrtf(d2);
+  const float q = rho2 * iD * iD;
+  const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);
+  return -fmaf(wc, corr, w * r0.w);
+}
+
 // Validity of the near-axis phase form for an observer at (fx, fy, fz) in the particle frame: small
 // angle from the frame axis and a bounded correction phase; otherwise the FP64 path must be used.
 __device__ __forceinline__ bool mixed_geometry_ok(double fx, double fy, double fz, double om, double xperp_max,
@@ -139,6 +152,138 @@ __device__ __forceinline__ double group_max(double v) {
 #pragma unroll
   for (int o = kFinLanes / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o, kFinLanes));
   return v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Finalize of the frequency-domain waves: span reduction, the stop rule of
+// src/OSCARSSR.cc:4222-4238, finished entries' outputs (:4246-4267) and the survivor list.
+// ---------------------------------------------------------------------------------------------
+// Warp-aggregated bookkeeping: one atomic per warp for the survivor list and for each statistics
+// counter, instead of one per entry on a single address.
+__device__ __forceinline__ void finalize_bookkeeping(bool finished, bool unconverged, bool survive, int64_t item,
+                                                     int L, int* act_next, unsigned* n_next,
+                                                     unsigned long long* not_converged, unsigned long long* samples) {
+  const unsigned full = 0xffffffffu;
+  const int lane32 = threadIdx.x & 31;
+  const unsigned fin = __ballot_sync(full, finished);
+  const unsigned unc = __ballot_sync(full, unconverged);
+  const unsigned sur = __ballot_sync(full, survive);
+  if (lane32 == 0) {
+    if (fin) atomicAdd(samples, (unsigned long long)__popc(fin) * (unsigned long long)((2ll << L) - 1));
+    if (unc) atomicAdd(not_converged, (unsigned long long)__popc(unc));
+  }
+  unsigned base = 0;
+  if (sur && lane32 == __ffs(sur) - 1) base = atomicAdd(n_next, (unsigned)__popc(sur));
+  base = __shfl_sync(full, base, sur ? __ffs(sur) - 1 : 0);
+  if (survive) act_next[base + __popc(sur & ((1u << lane32) - 1u))] = (int)item;
+}
+
+// One entry after its sum S up to level L: finish it (converged or last level) or keep its state.
+__device__ __forceinline__ void fd_entry_decide(const FdFinalArgs& A, int64_t item, const C3& S, double last_mag,
+                                                double dmax, bool& finished, bool& unconverged, bool& survive) {
+  C3 t = c3_scale(S, A.dt_level);
+  if (A.project) t = c3_project(t, A.pol);
+  const double this_mag = c3_mag2(t);
+  const double prec = fabs(this_mag - last_mag) / last_mag;
+  const int L = A.level;
+  const bool stop = (L > 8 && prec < A.precision && dmax < kPiD) || (L > 8 && dmax < kPiD && this_mag == last_mag);
+  if (stop || L >= A.max_level) {
+    const int result_level = stop ? L : -1;
+    C3 E = c3_scale(S, A.c0 * A.dt_level);
+    if (A.project) E = c3_project(E, A.pol);
+    double v;
+    if (A.quantity == 1) v = prec * A.weight;
+    else if (A.quantity == 2) v = (double)result_level * A.weight;
+    else v = A.c2 * c3_mag2(E) * A.weight;
+    A.out[item] = v;
+    if (A.level_out) A.level_out[item] = result_level;
+    finished = true;
+    unconverged = !stop;
+  } else {
+    const int64_t N = A.n_items;
+    A.state[item] = S.xr; A.state[N + item] = S.xi; A.state[2 * N + item] = S.yr;
+    A.state[3 * N + item] = S.yi; A.state[4 * N + item] = S.zr; A.state[5 * N + item] = S.zi;
+    A.state[6 * N + item] = this_mag;
+    survive = true;
+  }
+}
+
+// Index of partial component k of (tile, segment g, span sp, entry q of the tile) in the fused,
+// tile-major layout.
+__device__ __forceinline__ int64_t fused_part_index(const WavePlan& P, int64_t tile, int g, int sp, int k, int q,
+                                                    int tile_entries) {
+  return ((((tile * P.nseg + g) * P.spans + sp) * kFdPartials) + k) * (int64_t)tile_entries + q;
+}
+
+// Fused finalize of one tile by all threads of the CTA that finished its last span; entry q of the
+// tile is (e * THREADS + threadIdx.x) for q < TE.  Partials are read through L2 (other CTAs wrote
+// them).  With A.dmax_spans_joined the stored maxima already include the step into each span.
+template <int EPT, int THREADS>
+__device__ void fd_tile_finalize(const FdFinalArgs& A, const WavePlan& P, int64_t tile, int64_t n_act, int TE) {
+  for (int e = 0; e < EPT; ++e) {
+    const int q = e * THREADS + (int)threadIdx.x;
+    const int64_t slot = tile * TE + q;
+    const bool live = q < TE && slot < n_act;
+    const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+    auto seg_sum = [&](int g, C3& s, double& dmax) {
+      for (int sp = 0; sp < P.spans; ++sp) {
+        const double* p = A.part + fused_part_index(P, tile, g, sp, 0, q, TE);
+        s.xr += __ldcg(p); s.xi += __ldcg(p + TE); s.yr += __ldcg(p + 2 * TE);
+        s.yi += __ldcg(p + 3 * TE); s.zr += __ldcg(p + 4 * TE); s.zi += __ldcg(p + 5 * TE);
+        const double dm = __ldcg(p + 8 * TE);
+        if (dm >= 0) {  // non-empty span (empty spans only trail the segment)
+          dmax = fmax(dmax, dm);
+          if (sp > 0 && !A.dmax_spans_joined) {
+            const double* pp = A.part + fused_part_index(P, tile, g, sp - 1, 0, q, TE);
+            dmax = fmax(dmax, fabs(__dsub_rn(__ldcg(p + 6 * TE), __ldcg(pp + 7 * TE))));
+          }
+        }
+      }
+    };
+    bool finished = false, unconverged = false, survive = false;
+    if (live) {
+      C3 S = {0, 0, 0, 0, 0, 0};
+      double last_mag = -1, dmax = 0;
+      if (A.first) {
+        double unused = 0;
+        if (P.nseg == 2) {
+          seg_sum(0, S, unused);
+          C3 t = c3_scale(S, A.dt_prev);
+          if (A.project) t = c3_project(t, A.pol);
+          last_mag = c3_mag2(t);
+        }
+        seg_sum(P.nseg - 1, S, dmax);
+      } else {
+        const int64_t N = A.n_items;
+        S = {A.state[item], A.state[N + item], A.state[2 * N + item], A.state[3 * N + item], A.state[4 * N + item],
+             A.state[5 * N + item]};
+        last_mag = A.state[6 * N + item];
+        seg_sum(0, S, dmax);
+      }
+      fd_entry_decide(A, item, S, last_mag, dmax, finished, unconverged, survive);
+    }
+    finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged,
+                         A.samples);
+  }
+}
+
+// End of a unit in a fused wave: publish this CTA's partials, count the tile's finished spans, and
+// let the CTA that finished the last one finalize the tile.
+template <int EPT, int THREADS>
+__device__ __forceinline__ void fused_unit_done(const FdWaveArgs& A, const WavePlan& P, int64_t tile,
+                                                int64_t n_act, int* s_last, int TE = EPT * THREADS) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned done = atomicAdd(&A.tile_done[tile], 1u);
+    *s_last = done == (unsigned)(P.spans - 1);
+    if (*s_last) __threadfence();
+  }
+  __syncthreads();
+  if (*s_last) {
+    fd_tile_finalize<EPT, THREADS>(A.fin, P, tile, n_act, TE);
+    if (threadIdx.x == 0) A.tile_done[tile] = 0;
+  }
 }
 
 }  // namespace dev

@@ -62,23 +62,6 @@ __host__ __device__ inline int64_t seg_begin(const WavePlan& p, int g) { return 
 __host__ __device__ inline int64_t seg_end(const WavePlan& p, int g) { return g ? p.seg_e[1] : p.seg_e[0]; }
 __host__ __device__ inline int64_t seg_span(const WavePlan& p, int g) { return g ? p.span_len[1] : p.span_len[0]; }
 
-// One wave of the frequency-domain sum over level `level` for the active entries.
-struct FdWaveArgs {
-  const double* lev;        // FP64 level cache (10 arrays of `cap`) or mixed records (3 float4 per sample)
-  int64_t cap;
-  const double* obs;        // 3 * n_obs
-  const double* omega;      // n_e
-  int64_t n_e;
-  int64_t n_items;          // n_obs * n_e (entry = obs_index * n_e + energy_index)
-  const int* act;           // active entry ids (NULL: entries 0..n_items-1)
-  const unsigned* n_act;    // device count of `act`
-  int first, level, tile_entries, min_span;
-  int64_t target_units;
-  double* part;             // partials, entry-major: [slot][seg][span][kFdPartials]
-  unsigned* err;
-  unsigned long long* work;  // next unit to take (zero at launch; the finalize resets it)
-};
-
 struct FdFinalArgs {
   const double* part;
   int first, level, max_level, quantity, project, tile_entries, min_span;
@@ -97,6 +80,33 @@ struct FdFinalArgs {
   unsigned long long* not_converged;
   unsigned long long* samples;
   unsigned long long* work_reset;  // the wave's unit counter, zeroed for the next wave
+  int dmax_spans_joined;    // the span maxima include the step from the previous span's last sample
+};
+
+// One wave of the frequency-domain sum over level `level` for the active entries.
+struct FdWaveArgs {
+  const double* lev;        // FP64 level cache (10 arrays of `cap`) or mixed records (3 float4 per sample)
+  int64_t cap;
+  const double* obs;        // 3 * n_obs
+  const double* omega;      // n_e
+  int64_t n_e;
+  int64_t n_items;          // n_obs * n_e (entry = obs_index * n_e + energy_index)
+  const int* act;           // active entry ids (NULL: entries 0..n_items-1)
+  const unsigned* n_act;    // device count of `act`
+  int first, level, tile_entries, min_span;
+  int64_t target_units;
+  double* part;             // partials, entry-major: [slot][seg][span][kFdPartials]; fused: see below
+  unsigned* err;
+  unsigned long long* work;  // next unit to take (zero at launch; the finalize resets it)
+  // Fused finalize: the last CTA to finish a tile's spans reduces them, applies the stop rule and
+  // appends survivors (no finalize launch).  Partials are then tile-major,
+  // [tile][seg][span][kFdPartials][entry in tile], so writes and the finalizer's reads coalesce.
+  // zero_u32 / zero_u64 are the counters of the following wave, zeroed by block 0 at start.
+  int fused;
+  unsigned* tile_done;      // per tile: spans finished (the finalizer resets it to 0)
+  unsigned* zero_u32;
+  unsigned long long* zero_u64;
+  FdFinalArgs fin;
 };
 
 struct PdWaveArgs {
@@ -147,9 +157,10 @@ cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin
                                  float4* rec, cudaStream_t st);
 // Compiled kernel variants (see kernels_fp64.cu / kernels_mixed.cu); the engine's autotuner picks one.
 constexpr int kFp64Variants = 4;
-constexpr int kMixedVariants = 7;
+constexpr int kMixedVariants = 10;
 cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int grid, int variant, cudaStream_t st);
 int mixed_entries_per_cta(int variant);
+bool mixed_variant_is_split(int variant);  // sample-split variants: fused finalize only
 int mixed_blocks_per_sm(int variant);
 int fp64_blocks_per_sm(bool power_density, int variant);
 

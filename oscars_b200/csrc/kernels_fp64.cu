@@ -114,7 +114,12 @@ constexpr int kFdChunk = 128;
 template <int MINB>
 __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A) {
   __shared__ __align__(16) Stage<10, kFdChunk> st;
+  __shared__ int s_last;
   const int tid = threadIdx.x;
+  if (A.fused && blockIdx.x == 0 && tid == 0) {  // counters of the following wave
+    if (A.zero_u32) *A.zero_u32 = 0;
+    if (A.zero_u64) *A.zero_u64 = 0;
+  }
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
   // the plan is uniform over the CTA; keeping it in shared memory frees the registers its
   // fields would otherwise hold across the sample loop
@@ -226,41 +231,24 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
         }
         __syncthreads();  // everyone is done with `buf` before it is refilled
       }
-      if (live) {  // entry-major: the finalize reads an entry's spans contiguously
-        double* p = A.part + (slot * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
-        p[0] = sxr; p[1] = sxi; p[2] = syr; p[3] = syi; p[4] = szr; p[5] = szi;
-        p[6] = have ? first_phase : 0.0;
-        p[7] = have ? last_phase : 0.0;
-        p[8] = have ? dmax : -1.0;  // -1 marks an empty span
+      if (live) {
+        // entry-major for the finalize kernel (an entry's spans contiguous); tile-major when fused
+        double* p = A.fused ? A.part + fused_part_index(P, tile, g, span, 0, tid, kFdThreads)
+                            : A.part + (slot * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
+        const int64_t cs = A.fused ? kFdThreads : 1;  // stride between components
+        p[0] = sxr; p[cs] = sxi; p[2 * cs] = syr; p[3 * cs] = syi; p[4 * cs] = szr; p[5 * cs] = szi;
+        p[6 * cs] = have ? first_phase : 0.0;
+        p[7 * cs] = have ? last_phase : 0.0;
+        p[8 * cs] = have ? dmax : -1.0;  // -1 marks an empty span
       }
     }
+    if (A.fused) fused_unit_done<1, kFdThreads>(A, P, tile, n_act, &s_last);
   }
 }
 
 // Reduce the span partials of the wave, apply the stop rule of src/OSCARSSR.cc:4222-4238, finish
 // converged / last-level entries (:4246-4267) and append the others to the next active list
 // (span partials reduced by kFinLanes-lane groups, fd_common.cuh).
-
-// Warp-aggregated bookkeeping of the finalize kernels: one atomic per warp for the survivor list and
-// one per warp for each statistics counter, instead of one per entry on a single address.
-__device__ __forceinline__ void finalize_bookkeeping(bool finished, bool unconverged, bool survive, int64_t item,
-                                                     int L, int* act_next, unsigned* n_next,
-                                                     unsigned long long* not_converged, unsigned long long* samples) {
-  const unsigned full = 0xffffffffu;
-  const int lane32 = threadIdx.x & 31;
-  const unsigned fin = __ballot_sync(full, finished);
-  const unsigned unc = __ballot_sync(full, unconverged);
-  const unsigned sur = __ballot_sync(full, survive);
-  const int leader = 0;
-  if (lane32 == leader) {
-    if (fin) atomicAdd(samples, (unsigned long long)__popc(fin) * (unsigned long long)((2ll << L) - 1));
-    if (unc) atomicAdd(not_converged, (unsigned long long)__popc(unc));
-  }
-  unsigned base = 0;
-  if (sur && lane32 == __ffs(sur) - 1) base = atomicAdd(n_next, (unsigned)__popc(sur));
-  base = __shfl_sync(full, base, sur ? __ffs(sur) - 1 : 0);
-  if (survive) act_next[base + __popc(sur & ((1u << lane32) - 1u))] = (int)item;
-}
 
 __global__ void k_fd_finalize(FdFinalArgs A) {
   if (blockIdx.x == 0 && threadIdx.x == 0 && A.work_reset) *A.work_reset = 0;
@@ -312,33 +300,7 @@ __global__ void k_fd_finalize(FdFinalArgs A) {
     seg_sum(0, S, dmax);
   }
   bool finished = false, unconverged = false, survive = false;
-  if (live && lane == 0) {
-    C3 t = c3_scale(S, A.dt_level);
-    if (A.project) t = c3_project(t, A.pol);
-    const double this_mag = c3_mag2(t);
-    const double prec = fabs(this_mag - last_mag) / last_mag;
-    const int L = A.level;
-    const bool stop = (L > 8 && prec < A.precision && dmax < kPiD) || (L > 8 && dmax < kPiD && this_mag == last_mag);
-    if (stop || L >= A.max_level) {
-      const int result_level = stop ? L : -1;
-      C3 E = c3_scale(S, A.c0 * A.dt_level);
-      if (A.project) E = c3_project(E, A.pol);
-      double v;
-      if (A.quantity == 1) v = prec * A.weight;
-      else if (A.quantity == 2) v = (double)result_level * A.weight;
-      else v = A.c2 * c3_mag2(E) * A.weight;
-      A.out[item] = v;
-      if (A.level_out) A.level_out[item] = result_level;
-      finished = true;
-      unconverged = !stop;
-    } else {
-      const int64_t N = A.n_items;
-      A.state[item] = S.xr; A.state[N + item] = S.xi; A.state[2 * N + item] = S.yr;
-      A.state[3 * N + item] = S.yi; A.state[4 * N + item] = S.zr; A.state[5 * N + item] = S.zi;
-      A.state[6 * N + item] = this_mag;
-      survive = true;
-    }
-  }
+  if (live && lane == 0) fd_entry_decide(A, item, S, last_mag, dmax, finished, unconverged, survive);
   finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples);
 }
 

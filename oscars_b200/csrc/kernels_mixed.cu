@@ -69,7 +69,12 @@ struct MixedStage {
 template <int EPT, int MINB>
 __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A, MixedFrame F) {
   __shared__ __align__(16) MixedStage st;
+  __shared__ int s_last;
   const int tid = threadIdx.x;
+  if (A.fused && blockIdx.x == 0 && tid == 0) {  // counters of the following wave
+    if (A.zero_u32) *A.zero_u32 = 0;
+    if (A.zero_u64) *A.zero_u64 = 0;
+  }
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
   // the plan is uniform over the CTA; keeping it in shared memory frees the registers its
   // fields would otherwise hold across the sample loop
@@ -185,14 +190,178 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
 #pragma unroll
       for (int e = 0; e < EPT; ++e) {
         if (!live[e]) continue;
-        double* p = A.part + (slot[e] * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
+        // entry-major for the finalize kernel; tile-major when fused
+        double* p = A.fused ? A.part + fused_part_index(P, tile, g, span, 0, e * kMxThreads + tid, kMxThreads * EPT)
+                            : A.part + (slot[e] * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
+        const int64_t cs = A.fused ? kMxThreads * EPT : 1;  // stride between components
 #pragma unroll
-        for (int k = 0; k < 6; ++k) p[k] = S[e][k];
-        p[6] = have[e] ? (double)first[e] : 0.0;
-        p[7] = have[e] ? (double)last[e] : 0.0;
-        p[8] = have[e] ? (double)dmax[e] : -1.0;
+        for (int k = 0; k < 6; ++k) p[k * cs] = S[e][k];
+        p[6 * cs] = have[e] ? (double)first[e] : 0.0;
+        p[7 * cs] = have[e] ? (double)last[e] : 0.0;
+        p[8 * cs] = have[e] ? (double)dmax[e] : -1.0;
       }
     }
+    if (A.fused) fused_unit_done<EPT, kMxThreads>(A, P, tile, n_act, &s_last);
+  }
+}
+
+// Sample-split variant: the CTA's 128 threads form SUB groups of TE = 128 / SUB threads; group s
+// handles, for the same TE entries, the s-th of SUB equal parts of every staged chunk.  Each part
+// starts from the phase of the sample before it, so the largest phase step needs no exchange
+// between groups or spans (dmax_spans_joined); the groups' sums are reduced in shared memory and
+// one partial per entry and span is stored.  Smaller tiles mean fewer spans per entry.
+template <int SUB, int MINB>
+__global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_split(FdWaveArgs A, MixedFrame F) {
+  constexpr int TE = kMxThreads / SUB;
+  constexpr int PART = kMxChunk / SUB;
+  __shared__ __align__(16) MixedStage st;
+  __shared__ __align__(16) float4 prev_rec[3];
+  __shared__ int prev_valid;
+  __shared__ double red[SUB > 1 ? SUB - 1 : 1][7][TE];
+  __shared__ int s_last;
+  __shared__ WavePlan P;
+  __shared__ int64_t next_unit;
+  const int tid = threadIdx.x;
+  const int grp = tid / TE, q = tid % TE;
+  if (A.fused && blockIdx.x == 0 && tid == 0) {  // counters of the following wave
+    if (A.zero_u32) *A.zero_u32 = 0;
+    if (A.zero_u64) *A.zero_u64 = 0;
+  }
+  const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
+  if (tid == 0) {
+    P = wave_plan(A.first, A.level, n_act, TE, A.target_units, A.min_span);
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int64_t units = P.tiles * P.spans;
+  const float4* rec = reinterpret_cast<const float4*>(A.lev);
+  uint32_t phase_bits = 0;
+  for (;;) {
+    if (tid == 0) next_unit = (int64_t)atomicAdd(A.work, 1ull);
+    __syncthreads();
+    const int64_t u = next_unit;
+    __syncthreads();
+    if (u >= units) break;
+    const int64_t tile = u / P.spans;
+    const int span = (int)(u % P.spans);
+    const int64_t slot = tile * TE + q;
+    const bool live = slot < n_act;
+    const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+    const int64_t io = item / A.n_e, ie = item % A.n_e;
+    float Ox, Oy, Oz, w, wc;
+    {
+      const double* R = F.rot;
+      const double ox = A.obs[3 * io] - F.x0[0], oy = A.obs[3 * io + 1] - F.x0[1], oz = A.obs[3 * io + 2] - F.x0[2];
+      const double fx = R[0] * ox + R[1] * oy + R[2] * oz;
+      const double fy = R[3] * ox + R[4] * oy + R[5] * oz;
+      const double fz = R[6] * ox + R[7] * oy + R[8] * oz;
+      Ox = (float)fx; Oy = (float)fy; Oz = (float)fz;
+      const double om = A.omega[ie];
+      w = (float)om;
+      wc = (float)(om / kCl);
+      if (live && grp == 0 && span == 0 && !mixed_geometry_ok(fx, fy, fz, om, F.xperp_max, F.z_max))
+        atomicOr(A.err, kErrBadArgs);
+    }
+    for (int g = 0; g < P.nseg; ++g) {
+      const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
+      const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
+      double S[6] = {0, 0, 0, 0, 0, 0};
+      float dmax = 0.f;
+      bool any = false;
+      const int64_t nchunks = b1 > b0 ? (b1 - b0 + kMxChunk - 1) / kMxChunk : 0;
+      if (tid == 0) {
+        // the sample before the span, if it belongs to the same segment (span > 0)
+        prev_valid = span > 0 && b0 < b1;
+        if (prev_valid) {
+          prev_rec[0] = rec[3 * (b0 - 1)];
+          prev_rec[1] = rec[3 * (b0 - 1) + 1];
+          prev_rec[2] = rec[3 * (b0 - 1) + 2];
+        }
+        if (nchunks > 0) {
+          const int64_t hi = min(b1, b0 + kMxChunk);
+          mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - b0) * 48));
+          tma_load_1d(&st.v[0][0], rec + 3 * b0, (uint32_t)((hi - b0) * 48), &st.bar[0]);
+        }
+      }
+      __syncthreads();
+      for (int64_t c = 0; c < nchunks; ++c) {
+        const int buf = (int)(c & 1);
+        const int64_t lo = b0 + c * kMxChunk, hi = min(b1, lo + kMxChunk);
+        if (tid == 0 && c + 1 < nchunks) {
+          const int64_t lo2 = lo + kMxChunk, hi2 = min(b1, lo2 + kMxChunk);
+          mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * 48));
+          tma_load_1d(&st.v[buf ^ 1][0], rec + 3 * lo2, (uint32_t)((hi2 - lo2) * 48), &st.bar[buf ^ 1]);
+        }
+        if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+          if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+          return;
+        }
+        phase_bits ^= 1u << buf;
+        const float4* sv = st.v[buf];
+        const int n = (int)(hi - lo);
+        int j0 = grp * PART;
+        const int j1 = min(n, (grp + 1) * PART);
+        if (live && j0 < j1) {
+          float last = __int_as_float(0x7fc00000);  // NaN: no step into the first sample
+          if (lo + j0 == 0) {
+            j0 = 1;  // sample 0 is the unused slot and has no successor step
+          } else if (j0 > 0) {
+            last = mixed_phase(sv[3 * (j0 - 1)], Ox, Oy, Oz, w, wc);
+          } else if (prev_valid) {
+            last = mixed_phase(prev_rec[0], Ox, Oy, Oz, w, wc);
+          }
+          for (int jb = j0; jb < j1; jb += kMxFold) {
+            const int je = min(j1, jb + kMxFold);
+            float s32[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int j = jb; j < je; ++j) {
+              const float ph = mixed_sample(sv[3 * j], sv[3 * j + 1], sv[3 * j + 2], Ox, Oy, Oz, w, wc, s32);
+              dmax = fmaxf(dmax, fabsf(ph - last));
+              last = ph;
+            }
+#pragma unroll
+            for (int k = 0; k < 6; ++k) S[k] += (double)s32[k];
+          }
+          any = any || j0 < j1;
+        }
+        __syncthreads();  // everyone is done with `buf` (and prev_rec) before they are refilled
+        if (tid == 0 && c + 1 < nchunks) {
+          prev_rec[0] = sv[3 * (n - 1)];
+          prev_rec[1] = sv[3 * (n - 1) + 1];
+          prev_rec[2] = sv[3 * (n - 1) + 2];
+          prev_valid = 1;
+        }
+        __syncthreads();
+      }
+      // reduce the groups' sums in group order; group 0 stores the span's partial
+      if (SUB > 1) {
+        if (grp > 0) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) red[grp - 1][k][q] = S[k];
+          red[grp - 1][6][q] = any ? (double)dmax : -1.0;
+        }
+        __syncthreads();
+        if (grp == 0) {
+          double dm = any ? (double)dmax : -1.0;
+          for (int o = 0; o < SUB - 1; ++o) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) S[k] += red[o][k][q];
+            dm = fmax(dm, red[o][6][q]);
+          }
+          if (live) {
+            double* p = A.part + fused_part_index(P, tile, g, span, 0, q, TE);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) p[k * TE] = S[k];
+            p[6 * TE] = 0.0;
+            p[7 * TE] = 0.0;
+            p[8 * TE] = dm;  // -1: empty span
+          }
+        }
+        __syncthreads();
+      }
+    }
+    fused_unit_done<1, kMxThreads>(A, P, tile, n_act, &s_last, TE);
   }
 }
 
@@ -207,9 +376,15 @@ cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin
 }
 
 // Compiled variants of the mixed wave kernel: (entries per thread, minimum resident CTAs per SM).
-static const int kMixedEpt[kMixedVariants] = {1, 1, 2, 2, 2, 4, 4};
+// Variants 0-6: (entries per thread, minimum CTAs per SM); 7-9: sample-split (groups, minimum CTAs),
+// which need the fused finalize.
+static const int kMixedEpt[kMixedVariants] = {1, 1, 2, 2, 2, 4, 4, 0, 0, 0};
+static const int kMixedSub[kMixedVariants] = {0, 0, 0, 0, 0, 0, 0, 4, 4, 2};
 
-int mixed_entries_per_cta(int variant) { return dev::kMxThreads * kMixedEpt[variant]; }
+int mixed_entries_per_cta(int variant) {
+  return kMixedSub[variant] ? dev::kMxThreads / kMixedSub[variant] : dev::kMxThreads * kMixedEpt[variant];
+}
+bool mixed_variant_is_split(int variant) { return kMixedSub[variant] != 0; }
 
 template <int EPT, int MINB>
 static void mixed_occ(int& n) {
@@ -225,7 +400,10 @@ int mixed_blocks_per_sm(int variant) {
     case 3: mixed_occ<2, 5>(n); break;
     case 4: mixed_occ<2, 6>(n); break;
     case 5: mixed_occ<4, 1>(n); break;
-    default: mixed_occ<4, 3>(n); break;
+    case 6: mixed_occ<4, 3>(n); break;
+    case 7: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_mixed_split<4, 1>, dev::kMxThreads, 0); break;
+    case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_mixed_split<4, 6>, dev::kMxThreads, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_mixed_split<2, 4>, dev::kMxThreads, 0); break;
   }
   return n > 0 ? n : 1;
 }
@@ -239,7 +417,10 @@ cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int g
     case 3: dev::k_fd_wave_mixed<2, 5><<<grid, T, 0, st>>>(a, F); break;
     case 4: dev::k_fd_wave_mixed<2, 6><<<grid, T, 0, st>>>(a, F); break;
     case 5: dev::k_fd_wave_mixed<4, 1><<<grid, T, 0, st>>>(a, F); break;
-    default: dev::k_fd_wave_mixed<4, 3><<<grid, T, 0, st>>>(a, F); break;
+    case 6: dev::k_fd_wave_mixed<4, 3><<<grid, T, 0, st>>>(a, F); break;
+    case 7: dev::k_fd_wave_mixed_split<4, 1><<<grid, T, 0, st>>>(a, F); break;
+    case 8: dev::k_fd_wave_mixed_split<4, 6><<<grid, T, 0, st>>>(a, F); break;
+    default: dev::k_fd_wave_mixed_split<2, 4><<<grid, T, 0, st>>>(a, F); break;
   }
   return cudaGetLastError();
 }
