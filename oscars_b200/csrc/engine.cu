@@ -172,11 +172,15 @@ void Engine::compute_frame() {
   frame_.z_max = zm;
 }
 
-void Engine::ensure_mixed(int L) {
+void Engine::ensure_mixed(int L, int layout) {
   ensure_levels(L);
   if (mrec_version_ != knots_version_) {
     compute_frame();
     mrec_version_ = knots_version_;
+    mrec_filled_ = -1;
+  }
+  if (layout != mrec_layout_) {
+    mrec_layout_ = layout;
     mrec_filled_ = -1;
   }
   if (L <= mrec_filled_) return;
@@ -188,7 +192,7 @@ void Engine::ensure_mixed(int L) {
   }
   const int64_t s_begin = mrec_filled_ < 0 ? 1 : ((int64_t)2 << mrec_filled_);
   const int64_t s_end = (int64_t)2 << L;
-  check(launch_mixed_records(lev_.as<double>(), lev_cap_, s_begin, s_end, frame_, mrec_.as<float4>(), stream),
+  check(launch_mixed_records(lev_.as<double>(), lev_cap_, s_begin, s_end, frame_, mrec_.as<float4>(), layout, stream),
         "mixed records");
   ++last_launches;
   mrec_filled_ = L;
@@ -304,12 +308,12 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     throw Error{OSC_ERR_INVALID, "compute='mixed' applies to flux and spectrum; power density runs in FP64"};
   const int Lfirst = std::min(9, lstop);
   const int Lpre = std::min(lstop, std::max(Lfirst, kPrefillLevel));
-  if (mixed) ensure_mixed(Lpre);
-  else ensure_levels(Lpre);
-
   const int kind = rq.power_density ? 1 : (mixed ? 2 : 0);
   const int variant = tuning_ ? current_variant_[kind]
                               : pick_variant(kind, const_cast<RadRequest&>(rq), n_items, Lfirst, lstop, d_out, d_lvl, st);
+  const int layout = mixed ? mixed_variant_layout(variant) : 0;
+  if (mixed) ensure_mixed(Lpre, layout);
+  else ensure_levels(Lpre);
   const int resident = wave_grid(kind, variant);  // CTAs resident at once on the device
   const int tile = mixed ? mixed_entries_per_cta(variant) : 128;
   const int64_t target = 4 * (int64_t)resident;   // >= 4 waves of equal units per launch
@@ -320,17 +324,17 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   const int per = rq.power_density ? 1 : kFdPartials;
   const int64_t ntiles = (N + tile - 1) / tile;
   const size_t part_doubles = (size_t)2 * per * tile * std::max<int64_t>(ntiles, 2 * target);
-  // per-level grid: the largest unit count over the active counts the level can have
-  std::vector<int64_t> grid_of(lstop + 1, 1);
-  for (int L = Lfirst; L <= lstop; ++L) {
-    for (int64_t t = 1;; t = t < 256 ? t + 1 : t + t / 8) {
-      const int64_t n = std::min(N, t * tile);
-      const WavePlan pl = wave_plan(L == Lfirst, L, n, tile, target, kMinSpan);
-      grid_of[L] = std::max(grid_of[L], pl.tiles * pl.spans);
-      if (t >= ntiles) break;
-      if (L == Lfirst) t = ntiles - 1;  // the first wave always has all N entries
+  // Per-level grid: the largest unit count over the active counts the level can have, capped at the
+  // resident CTAs.  The first wave has all N entries; a later wave with t tiles has t x spans units,
+  // which reaches the target (> resident) once t x (largest span count of the level) does.
+  auto grid_for = [&](int L) -> int {
+    if (L == Lfirst) {
+      const WavePlan pl = wave_plan(1, L, N, tile, target, kMinSpan);
+      return (int)std::min<int64_t>(pl.tiles * pl.spans, resident);
     }
-  }
+    const int64_t span_max = wave_spans(L, 1, INT64_MAX, kMinSpan);
+    return (int)std::min<int64_t>(ntiles * span_max, resident);
+  };
   part_.reserve(sizeof(double) * part_doubles);
   act_[0].reserve(sizeof(int) * N);
   act_[1].reserve(sizeof(int) * N);
@@ -406,7 +410,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = nullptr;
       f.dmax_spans_joined = mixed && mixed_variant_is_split(variant);
       auto ev = timed_begin(st);
-      const int g = (int)std::min<int64_t>(grid_of[L], resident);
+      const int g = grid_for(L);
       if (mixed) check(launch_fd_wave_mixed(w, frame_, g, variant, st), "flux wave (mixed)");
       else check(launch_fd_wave_fp64(w, g, variant, st), "flux wave");
       timed_end(ev, st);
@@ -422,7 +426,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
       auto ev = timed_begin(st);
-      const int g = (int)std::min<int64_t>(grid_of[L], resident);
+      const int g = grid_for(L);
       if (mixed) check(launch_fd_wave_mixed(w, frame_, g, variant, st), "flux wave (mixed)");
       else check(launch_fd_wave_fp64(w, g, variant, st), "flux wave");
       timed_end(ev, st);
@@ -443,7 +447,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
       auto ev = timed_begin(st);
-      check(launch_pd_wave_fp64(w, (int)std::min<int64_t>(grid_of[L], resident), st), "power density wave");
+      check(launch_pd_wave_fp64(w, grid_for(L), st), "power density wave");
       timed_end(ev, st);
       PdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
@@ -466,7 +470,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     check(cudaMemcpyAsync(&nn, active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
     check(cudaStreamSynchronize(st), "count");
     if (nn == 0) break;
-    if (mixed) ensure_mixed(L);
+    if (mixed) ensure_mixed(L, layout);
     else ensure_levels(L);
     launch_wave(L);
   }

@@ -146,9 +146,10 @@ class Engine {
   DevBuf mrec_;
   int64_t mrec_cap_ = 0;
   int mrec_filled_ = -1;
+  int mrec_layout_ = 0;
   uint64_t mrec_version_ = ~0ull;
   MixedFrame frame_{};
-  void ensure_mixed(int L);
+  void ensure_mixed(int L, int layout);  // layout: mixed_variant_layout of the kernel variant
   void compute_frame();
  public:
   int forced_variant[4] = {-1, -1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape

@@ -66,6 +66,25 @@ __device__ __forceinline__ double level_time(double tstart, double tstop, int64_
 //   u (1/(D om^2)) ((1-b^2)/D + n.a) - a / (D om).
 // Adds the term times exp(i phase) to s[6] (x re, x im, y re, y im, z re, z im); returns the phase.
 // ---------------------------------------------------------------------------------------------
+// Hardware approximations (MUFU) with denormals flushed: the mixed-precision terms never see
+// denormal operands (distances ~1..100 m, 1 - n.b ~ 1e-9..1e-6, reduced phases in [-pi, pi]), so
+// the flush-to-zero forms give the same values as rsqrtf / __fdividef(1, x) / __sincosf on every
+// input they receive, without the extra instructions that handle denormal inputs.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ void sincos_ftz(float x, float* s, float* c) {
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(*s) : "f"(x));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*c) : "f"(x));
+}
+
 constexpr float kTwoPiHiF = 6.28318548202514648f;     // RN_f(2 pi)
 constexpr float kTwoPiLoF = -1.7484556e-07f;         // RN_f(2 pi - kTwoPiHiF)
 constexpr float kInvTwoPiF = 0.159154943f;
@@ -75,19 +94,19 @@ __device__ __forceinline__ float mixed_sample(const float4 r0, const float4 r1, 
   const float rx = Ox - r0.x, ry = Oy - r0.y, rz = Oz - r0.z;
   const float rho2 = fmaf(rx, rx, ry * ry);
   const float d2 = fmaf(rz, rz, rho2);
-  const float iD = rsqrtf(d2);
+  const float iD = rsqrt_ftz(d2);
   const float q = rho2 * iD * iD;                                  // (rho/D)^2
   const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);           // rho^2/(Rz+D), |rho/D| < 1e-2
   const float ph = -fmaf(wc, corr, w * r0.w);                      // exp(-i w (t + D/c))
   const float k = rintf(ph * kInvTwoPiF);
   const float rr = fmaf(-k, kTwoPiLoF, fmaf(-k, kTwoPiHiF, ph));  // Cody-Waite reduction to [-pi, pi]
   float sn, cs;
-  __sincosf(rr, &sn, &cs);
+  sincos_ftz(rr, &sn, &cs);
   const float nx = rx * iD, ny = ry * iD;
   const float en = corr * iD;                                      // 1 - n_z
   const float ux = nx - r1.x, uy = ny - r1.y, uz = r1.z - en;
   const float om = fmaf(-nx, r1.x, fmaf(-ny, r1.y, fmaf(-en, r1.z, en + r1.z)));
-  const float io = __fdividef(1.f, om);
+  const float io = rcp_ftz(om);
   const float na = fmaf(nx, r2.x, fmaf(ny, r2.y, (1.f - en) * r2.z));
   const float k1 = io * io * iD * fmaf(r1.w, iD, na);
   const float k2 = io * iD;
@@ -105,7 +124,7 @@ __device__ __forceinline__ float mixed_phase(const float4 r0, float Ox, float Oy
   const float rx = Ox - r0.x, ry = Oy - r0.y, rz = Oz - r0.z;
   const float rho2 = fmaf(rx, rx, ry * ry);
   const float d2 = fmaf(rz, rz, rho2);
-  const float iD = rsqrtf(d2);
+  const float iD = rsqrt_ftz(d2);
   const float q = rho2 * iD * iD;
   const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);
   return -fmaf(wc, corr, w * r0.w);

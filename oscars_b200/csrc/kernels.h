@@ -153,14 +153,17 @@ struct MixedFrame {
   double xperp_max, z_max;
 };
 
+// Mixed records of samples [s_begin, s_end): layout 0 = 3 float4 per sample, 1 = pair records
+// (6 float4 per two samples, see kernels_mixed.cu).
 cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin, int64_t s_end, const MixedFrame& F,
-                                 float4* rec, cudaStream_t st);
+                                 float4* rec, int layout, cudaStream_t st);
 // Compiled kernel variants (see kernels_fp64.cu / kernels_mixed.cu); the engine's autotuner picks one.
 constexpr int kFp64Variants = 4;
-constexpr int kMixedVariants = 10;
+constexpr int kMixedVariants = 13;
 cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int grid, int variant, cudaStream_t st);
 int mixed_entries_per_cta(int variant);
 bool mixed_variant_is_split(int variant);  // sample-split variants: fused finalize only
+int mixed_variant_layout(int variant);     // records layout the variant reads
 int mixed_blocks_per_sm(int variant);
 int fp64_blocks_per_sm(bool power_density, int variant);
 

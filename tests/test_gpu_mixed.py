@@ -98,3 +98,33 @@ def test_far_off_axis_observer_is_rejected():
         s.calculate_spectrum(obs=[3, 0, 30], energy_range_eV=[100, 200], npoints=3, compute="mixed")
     with pytest.raises(ValueError, match="power density runs in FP64"):
         s.calculate_power_density_rectangle(npoints=[3, 3], width=[0.01, 0.01], translation=[0, 0, 30], compute="mixed")
+
+
+def _variants(kind):
+    import ctypes
+    s = _sr()
+    v, n = ctypes.c_int(), ctypes.c_int()
+    s._ctx.call("osc_get_variant", kind, ctypes.byref(v), ctypes.byref(n))
+    return n.value
+
+
+@pytest.mark.parametrize("variant", range(13))
+def test_every_mixed_variant_matches_fp64(variant):
+    """Each compiled mixed kernel (sample records, sample-split, packed pair records) on a flux grid
+    with many spans per entry (level 13, fixed) and on a spectrum past the prefilled levels."""
+    if variant >= _variants(2):
+        pytest.skip("variant not compiled")
+    flux = dict(energy_eV=E1_U, npoints=[41, 41], width=[0.008, 0.008], translation=[0, 0, 30], precision=0,
+                max_level=13)
+    spec = dict(obs=[0.0005, 0.0002, 30], energy_range_eV=[100, 3000], npoints=300, precision=0, max_level=16)
+    for call, kw in (("calculate_flux_rectangle", flux), ("calculate_spectrum", spec)):
+        out = {}
+        for compute in ("fp64", "mixed"):
+            s = _sr()
+            if compute == "mixed":
+                s._ctx.call("osc_set_variant", 2, variant)
+            run_case(s, UND_SETUP)
+            out[compute] = _vals(getattr(s, call)(**dict(kw, compute=compute)))
+        e = _err(out["mixed"], out["fp64"])
+        print("variant %d %s: mixed vs fp64 %.3e" % (variant, call, e))
+        assert e <= TOL
