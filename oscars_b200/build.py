@@ -24,7 +24,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-HOST_FLAGS = ["-O2", "-fPIC", "-ffp-contract=off", "-fvisibility=hidden", "-pthread"]
+HOST_FLAGS = ["-O3", "-fPIC", "-ffp-contract=off", "-fvisibility=hidden", "-pthread"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xptxas=-v"] + \
     sum([["-Xcompiler", f] for f in HOST_FLAGS], [])
 

@@ -14,7 +14,9 @@ namespace osc {
 namespace dev {
 
 // Error flags written by kernels (bit mask, OR-ed into a device word read back by the host).
-enum : unsigned { kErrTmaTimeout = 1u, kErrBadArgs = 2u, kErrSuperluminal = 4u };
+// kErrPlan: a kernel was launched with a tile size other than the one it was compiled for (the
+// host sized its partial sums for that tile); the kernel returns before touching memory.
+enum : unsigned { kErrTmaTimeout = 1u, kErrBadArgs = 2u, kErrSuperluminal = 4u, kErrPlan = 8u };
 
 // Polls of an mbarrier before a wait is declared stuck (each poll is a try_wait that itself may
 // suspend the thread for a hardware-defined interval), i.e. far beyond any legitimate latency.

@@ -499,6 +499,7 @@ void Engine::collect() {
   if (err) {
     check(cudaMemset(cnt_.as<unsigned>() + 2, 0, sizeof(unsigned)), "error word");
     if (err & 1u) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+    if (err & 8u) throw Error{OSC_ERR_STATE, "a sample-sum kernel variant was planned with another tile size"};
     throw Error{OSC_ERR_INVALID, "compute='mixed' needs observers near the beam axis (angle < 1e-2 and a correction "
                                  "phase below 3e4 rad); use compute='fp64' for this geometry"};
   }

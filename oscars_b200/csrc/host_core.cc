@@ -4,15 +4,112 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cctype>
 #include <cmath>
+#include <condition_variable>
+#include <exception>
 #include <fstream>
+#include <mutex>
 #include <sstream>
 #include <thread>
 
 #include "../../include/oscars_b200.h"
 
 namespace osc {
+
+// ---------------------------------------------------------------------------------------------
+// Persistent host threads for the independent parts of a trajectory (the two integration sweeps,
+// the 9 spline components): created once, woken per call, so a trajectory costs no thread starts.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+class TaskPool {
+ public:
+  ~TaskPool() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+
+  void run(int n, const std::function<void(int)>& fn) {
+    std::lock_guard<std::mutex> call(call_m_);
+    if (threads_.empty()) {
+      const unsigned hw = std::thread::hardware_concurrency();
+      const int w = (int)std::min(8u, hw > 1 ? hw - 1 : 1u);
+      for (int i = 0; i < w; ++i) threads_.emplace_back([this] { worker(); });
+    }
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      fn_ = &fn;
+      n_ = n;
+      next_.store(0);
+      error_ = nullptr;
+      ++gen_;
+    }
+    cv_.notify_all();
+    drain();
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return active_ == 0; });
+    fn_ = nullptr;
+    if (error_) std::rethrow_exception(error_);
+  }
+
+ private:
+  void drain() {
+    for (int i; (i = next_.fetch_add(1)) < n_;) {
+      try {
+        (*fn_)(i);
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(m_);
+        if (!error_) error_ = std::current_exception();
+      }
+    }
+  }
+  void worker() {
+    uint64_t seen = 0;
+    std::unique_lock<std::mutex> lk(m_);
+    for (;;) {
+      cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+      if (stop_) return;
+      seen = gen_;
+      if (!fn_) continue;  // woke after that call had finished
+      ++active_;
+      lk.unlock();
+      drain();
+      lk.lock();
+      if (--active_ == 0) done_.notify_all();
+    }
+  }
+
+  std::mutex call_m_, m_;
+  std::condition_variable cv_, done_;
+  std::vector<std::thread> threads_;
+  const std::function<void(int)>* fn_ = nullptr;
+  int n_ = 0, active_ = 0;
+  std::atomic<int> next_{0};
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+  std::exception_ptr error_;
+};
+
+TaskPool& task_pool() {
+  static TaskPool pool;
+  return pool;
+}
+
+}  // namespace
+
+void parallel_tasks(int n, const std::function<void(int)>& fn) {
+  if (n <= 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  task_pool().run(n, fn);
+}
 
 Vec3 orthogonal(Vec3 a) {  // include/TVector3D.h:132-142
   double xx = a.x < 0.0 ? -a.x : a.x;
@@ -146,10 +243,10 @@ Vec3 field_value(const FieldSpec& f, Vec3 x, double t) {
   const double taper_corr = 1 + d * f.taper;
   Vec3 F;
   if (f.kind == 0) {
-    F = pole_block(f, f.a, d, f.phase * mag(f.period) / two_pi(), taper_corr);
+    F = pole_block(f, f.a, d, f.phase * f.period_length / two_pi(), taper_corr);
   } else {  // src/TField3D_IdealEPU.cc:127-165: A shifted by +phase/2, B by -phase/2
-    F = pole_block(f, f.a, d, f.phase / 2. * mag(f.period) / two_pi(), taper_corr);
-    F = F + pole_block(f, f.b, d, -f.phase / 2. * mag(f.period) / two_pi(), taper_corr);
+    F = pole_block(f, f.a, d, f.phase / 2. * f.period_length / two_pi(), taper_corr);
+    F = F + pole_block(f, f.b, d, -f.phase / 2. * f.period_length / two_pi(), taper_corr);
   }
   if (f.frequency == 0) return F;
   return F * std::cos(two_pi() * f.frequency * (t + f.time_offset) + f.frequency_phase);
@@ -575,7 +672,10 @@ void Model::compute_trajectory() {
 
   // The forward and backward sweeps are independent integrations from the same initial state; they
   // run on two host threads and are stitched together afterwards (backward reversed, then forward).
-  std::vector<double> fwd, bwd;
+  std::vector<double>& fwd = sweep[0];
+  std::vector<double>& bwd = sweep[1];
+  fwd.clear();
+  bwd.clear();
   fwd.reserve(10 * nf);
   bwd.reserve(10 * nb);
   auto forward = [&]() {
@@ -605,9 +705,10 @@ void Model::compute_trajectory() {
     }
   };
   if (nf + nb > 4096) {
-    std::thread th(backward);
-    forward();
-    th.join();
+    parallel_tasks(2, [&](int i) {
+      if (i == 0) forward();
+      else backward();
+    });
   } else {
     forward();
     backward();
@@ -651,7 +752,9 @@ void spline_second_derivatives(Knots& k) {
   k.ypp.assign(9 * N, 0.0);
   std::vector<double>& diag = k.diag;
   diag.assign(N, 0.0);
-  std::vector<double> sigv(N), pv(N);
+  if (k.work.size() < (size_t)(11 * N)) k.work.resize(11 * N);
+  double* sigv = k.work.data();
+  double* pv = sigv + N;
   diag[0] = -0.5;
   for (int64_t i = 1; i < N - 1; ++i) {
     const double sig = (X[i] - X[i - 1]) / (X[i + 1] - X[i - 1]);
@@ -663,7 +766,7 @@ void spline_second_derivatives(Knots& k) {
   auto component = [&](int c) {
     const double* Y = k.y.data() + c * N;
     double* ypp = k.ypp.data() + c * N;
-    std::vector<double> u(N);
+    double* u = k.work.data() + (2 + c) * N;
     const double dydx0 = (Y[1] - Y[0]) / (X[1] - X[0]);
     u[0] = (3. / (X[1] - X[0])) * ((Y[1] - Y[0]) / (X[1] - X[0]) - dydx0);
     for (int64_t i = 1; i < N - 1; ++i) {
@@ -678,9 +781,7 @@ void spline_second_derivatives(Knots& k) {
     for (int64_t j = N - 2; j >= 0; --j) ypp[j] = ypp[j] * ypp[j + 1] + u[j];
   };
   if (N > 4096) {
-    std::vector<std::thread> pool;
-    for (int c = 0; c < 9; ++c) pool.emplace_back(component, c);
-    for (auto& th : pool) th.join();
+    parallel_tasks(9, component);
   } else {
     for (int c = 0; c < 9; ++c) component(c);
   }

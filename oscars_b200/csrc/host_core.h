@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <random>
 #include <string>
@@ -128,6 +129,7 @@ struct Knots {
   int64_t n = 0;
   std::vector<double> t, y, ypp;
   std::vector<double> diag;  // factored diagonal of the spline system (depends on t only)
+  std::vector<double> work;  // spline scratch (sigma, p, 9 right-hand sides), kept between calls
   double tstart = 0, tstop = 0;
   void clear() { n = 0; t.clear(); y.clear(); ypp.clear(); diag.clear(); }
 };
@@ -148,6 +150,7 @@ class Model {
   Rng rng;
   Knots knots;
   uint64_t knots_version = 0;  // bumps whenever `knots` changes
+  std::vector<double> sweep[2];  // forward / backward integration points, kept between calls
 
   void add_field(const FieldSpec& f);
   void clear_fields();
@@ -161,6 +164,11 @@ class Model {
 
 // Spline second derivatives of the 9 components (TSpline1D3::Derivatives, include/TOMATH.h:141-203).
 void spline_second_derivatives(Knots& k);
+
+// Runs fn(0) .. fn(n - 1) on a process-wide set of persistent host threads (the caller works too)
+// and returns when all have finished; the first exception a task throws is rethrown here.  Calls
+// from several threads are served one after another.
+void parallel_tasks(int n, const std::function<void(int)>& fn);
 
 // Rectangle surface (TSurfacePoints_Rectangle).  Throws osc::Error.
 void surface_rectangle(const std::string& plane, int nx1, int nx2, double w1, double w2, Vec3 rot,

@@ -68,6 +68,10 @@ struct MixedStage {
 
 template <int EPT, int MINB>
 __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A, MixedFrame F) {
+  if (A.tile_entries != kMxThreads * EPT) {  // the host sized the partials for another tile
+    if (threadIdx.x == 0) atomicOr(A.err, kErrPlan);
+    return;
+  }
   __shared__ __align__(16) MixedStage st;
   __shared__ int s_last;
   const int tid = threadIdx.x;
@@ -213,6 +217,10 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed(FdWaveArgs A
 template <int SUB, int MINB>
 __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_split(FdWaveArgs A, MixedFrame F) {
   constexpr int TE = kMxThreads / SUB;
+  if (A.tile_entries != TE) {  // the host sized the partials for another tile
+    if (threadIdx.x == 0) atomicOr(A.err, kErrPlan);
+    return;
+  }
   constexpr int PART = kMxChunk / SUB;
   __shared__ __align__(16) MixedStage st;
   __shared__ __align__(16) float4 prev_rec[3];
@@ -445,20 +453,20 @@ __device__ __forceinline__ float2 pair_sample(const float4* __restrict__ q, cons
   const float2 nx = mul2(rx, iD), ny = mul2(ry, iD), en = mul2(corr, iD);  // en = 1 - nz
   const float2 ux = add2(nx, NBX), uy = add2(ny, NBY), uz = fma2(en, M1, EB);
   const float2 om = fma2(ny, NBY, fma2(nx, NBX, fma2(en, BZ, EB)));
-  const float2 io = make_float2(rcp_ftz(om.x), rcp_ftz(om.y));
+  // e = k2 (h u - a) with k2 = 1/(D om), h = ((1-b^2)/D + n.a)/om, formed from -1/om:
+  // v = a + (-h) u = -(h u - a), e = (-k2) v.
+  const float2 nio = make_float2(rcp_ftz(-om.x), rcp_ftz(-om.y));
   const float2 na = fma2(nx, AX, fma2(ny, AY, mul2(fma2(en, M1, f2(1.f)), AZ)));
-  const float2 k2 = mul2(io, iD);
-  const float2 k1 = mul2(mul2(io, k2), fma2(G, iD, na));
-  const float2 nk2 = mul2(k2, M1);
-  const float2 ex = fma2(k1, ux, mul2(nk2, AX));
-  const float2 ey = fma2(k1, uy, mul2(nk2, AY));
-  const float2 ez = fma2(k1, uz, mul2(nk2, AZ));
-  acc[0] = fma2(ex, cs, acc[0]);
-  acc[1] = fma2(ex, sn, acc[1]);
-  acc[2] = fma2(ey, cs, acc[2]);
-  acc[3] = fma2(ey, sn, acc[3]);
-  acc[4] = fma2(ez, cs, acc[4]);
-  acc[5] = fma2(ez, sn, acc[5]);
+  const float2 nh = mul2(nio, fma2(G, iD, na));
+  const float2 vx = fma2(nh, ux, AX), vy = fma2(nh, uy, AY), vz = fma2(nh, uz, AZ);
+  const float2 nk2 = mul2(nio, iD);
+  const float2 kc = mul2(nk2, cs), ks = mul2(nk2, sn);
+  acc[0] = fma2(vx, kc, acc[0]);
+  acc[1] = fma2(vx, ks, acc[1]);
+  acc[2] = fma2(vy, kc, acc[2]);
+  acc[3] = fma2(vy, ks, acc[3]);
+  acc[4] = fma2(vz, kc, acc[4]);
+  acc[5] = fma2(vz, ks, acc[5]);
   return P;
 }
 
@@ -506,6 +514,10 @@ __global__ void k_mixed_records_pair(const double* __restrict__ lev, int64_t cap
 template <int SUB, int MINB>
 __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveArgs A, MixedFrame F) {
   constexpr int TE = kMxThreads / SUB;
+  if (A.tile_entries != TE) {  // the host sized the partials for another tile
+    if (threadIdx.x == 0) atomicOr(A.err, kErrPlan);
+    return;
+  }
   constexpr int CP = kPrChunk / 2;  // pairs per chunk
   constexpr int PP = CP / SUB;      // pairs per group and chunk
   __shared__ __align__(16) PairStage st;
