@@ -38,6 +38,7 @@ import io
 import json
 import math
 import os
+import re
 import subprocess
 import sys
 import threading
@@ -52,6 +53,21 @@ GRID = 201
 WORKLOAD = ("flux 201x201 XY rectangle 10mm x 10mm at z=30m, E=E1=458.9458 eV; planar undulator "
             "B0=0.5T lambda=50mm 41 periods; 3 GeV electron; 20001-point RK4; adaptive levels (precision 0.01)")
 FLOP_PER_SAMPLE = 83  # algorithmic work per sample of the frequency-domain integrand
+
+
+def _profiled_traffic():
+    """DRAM bytes (read + write) per launch of each profiled kernel variant, from the ncu summaries
+    under profiles/ (lines 'traffic per launch (dram read + write), <kernel>: <bytes> B')."""
+    out = {}
+    pat = re.compile(r"^traffic per launch \(dram read \+ write\), (\S+): (\d+) B")
+    pdir = os.path.join(ROOT, "profiles")
+    for fn in sorted(os.listdir(pdir)) if os.path.isdir(pdir) else []:
+        if fn.endswith(".md"):
+            for line in open(os.path.join(pdir, fn)):
+                mt = pat.match(line.strip())
+                if mt:
+                    out[mt.group(1)] = int(mt.group(2))
+    return out
 
 
 def setup(o):
@@ -236,6 +252,8 @@ def product_arm(args):
     setup(s)
     s.calculate_trajectory()
     ctx = s._ctx
+    if args.variant >= 0:  # a fixed kernel variant (profiler runs: no autotuning under the profiler)
+        ctx.call("osc_set_variant", 2 if args.compute == "mixed" else 0, args.variant)
     xyz, nrm, x12 = s._rectangle([GRID, GRID], "XY", [0.01, 0.01], None, None, [0, 0, 30], 0, False)
     n = GRID * GRID
     modes = ["fp64", "mixed"] if args.compute == "mixed" else ["fp64"]
@@ -279,15 +297,13 @@ def product_arm(args):
         peak = ctypes.c_double()
         ctx.call("osc_measure_fma_peak", 0 if m == "fp64" else 1, ctypes.byref(peak))
         achieved = sps * args.steps * FLOP_PER_SAMPLE / (kms * 1e-3) / 1e12 if kms > 0 else None
-        traffic = None
-        prof_path = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(prof_path):
-            traffic = json.load(open(prof_path)).get("k_fd_wave_%s" % m)
+        kname = _lib.variant_name(2 if m == "mixed" else 0, v.value)
+        traffic = _profiled_traffic().get(kname)
         res[m] = {"value": samples_all / (ms_max * 1e-3) / 1e9, "ms_per_step": ms_max / args.steps,
                   "samples_per_step": sps, "launches_per_step": lps, "variant": v.value, "clocks": clocks,
                   "roofline": {"bound": "fp64" if m == "fp64" else "fp32", "achieved": achieved, "peak": peak.value,
                                "unit": "TFLOP/s", "frac": (achieved / peak.value) if achieved else None,
-                               "traffic": traffic, "kernel": "k_fd_wave_%s" % m, "flop_per_sample": FLOP_PER_SAMPLE,
+                               "traffic": traffic, "kernel": kname, "flop_per_sample": FLOP_PER_SAMPLE,
                                "kernel_ms_per_step": kms / args.steps, "kernel_launches_per_step": kl / args.steps,
                                "peak_source": "in-run FMA-throughput loop on this GPU (osc_measure_fma_peak); the "
                                               "sample sums run on the %s pipe, not the tensor cores or HBM"
@@ -653,6 +669,8 @@ def main():
     ap.add_argument("--compute", default="mixed", choices=["fp64", "mixed"],
                     help="headline arithmetic; 'mixed' also times the FP64 path and reports both")
     ap.add_argument("--quick", action="store_true", help="device-resident timing only (for profiler runs)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="force this compiled variant of the --compute kernel instead of autotuning (profiler runs)")
     ap.add_argument("--batched-steps", type=int, default=3,
                     help="timed steps of the batched workloads (EPU beam, uneven jobs); 0 skips them")
     ap.add_argument("--only", default="", choices=["", "beam", "uneven", "tuning", "sharded"],

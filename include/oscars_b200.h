@@ -294,6 +294,10 @@ OSC_API int osc_get_profile(osc_ctx* ctx, double* kernel_ms, long long* launches
  * variant the last request of that kind used and the number of compiled variants. */
 OSC_API int osc_set_variant(osc_ctx* ctx, int kind, int variant);
 OSC_API int osc_get_variant(osc_ctx* ctx, int kind, int* variant, int* n_variants);
+/* Name of compiled variant `variant` of kind 0, 2 or 3: the kernel and its template arguments
+ * (e.g. "k_fd_wave_mixed_pair<4,4>"), NUL-terminated into name[capacity].  No context; errors go
+ * to osc_last_error(NULL).  No counterpart in the reference (it has one kernel per quantity). */
+OSC_API int osc_variant_name(int kind, int variant, char* name, long long capacity);
 /* Drop the device-side level-sample cache (it is rebuilt by the next radiation call). */
 OSC_API int osc_drop_level_cache(osc_ctx* ctx);
 /* Measured arithmetic peak of this GPU: an FMA-throughput loop in FP64 (kind 0) or FP32 (kind 1),

@@ -90,6 +90,7 @@ SIGNATURES = {
     "osc_get_profile": (I, [VP, DP, LLP, LLP, I]),
     "osc_set_variant": (I, [VP, I, I]),
     "osc_get_variant": (I, [VP, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
+    "osc_variant_name": (I, [I, I, ctypes.c_char_p, ctypes.c_longlong]),
     "osc_drop_level_cache": (I, [VP]),
     "osc_measure_fma_peak": (I, [VP, I, DP]),
     "osc_flux_fixed_level_noalloc": (I, [I, DP, LL, DP, LL, D, I, D, D, DP, DP, ctypes.c_char_p, LL]),
@@ -155,6 +156,16 @@ class Context:
                 raise RuntimeError("oscars_b200 %s (%s): %s" % (name, STATUS_NAMES.get(rc, rc), msg))
             raise ValueError(msg)
         return rc
+
+
+def variant_name(kind: int, variant: int) -> str:
+    """Kernel and template arguments of compiled variant `variant` of kind 0 (FP64 flux), 2 (mixed)
+    or 3 (batched mixed)."""
+    buf = ctypes.create_string_buffer(96)
+    rc = lib().osc_variant_name(int(kind), int(variant), buf, len(buf))
+    if rc != OSC_OK:
+        raise ValueError(lib().osc_last_error(None).decode())
+    return buf.value.decode()
 
 
 def device_count() -> int:

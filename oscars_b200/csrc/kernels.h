@@ -164,6 +164,7 @@ cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int g
 int mixed_entries_per_cta(int variant);
 bool mixed_variant_is_split(int variant);  // sample-split variants: fused finalize only
 int mixed_variant_layout(int variant);     // records layout the variant reads
+const char* mixed_variant_name(int variant);  // kernel and template arguments of a variant
 int mixed_blocks_per_sm(int variant);
 int fp64_blocks_per_sm(bool power_density, int variant);
 

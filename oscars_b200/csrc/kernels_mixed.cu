@@ -682,6 +682,14 @@ int mixed_entries_per_cta(int variant) {
   return kMixedSub[variant] ? dev::kMxThreads / kMixedSub[variant] : dev::kMxThreads * kMixedEpt[variant];
 }
 bool mixed_variant_is_split(int variant) { return kMixedSub[variant] != 0; }
+const char* mixed_variant_name(int variant) {
+  static const char* const kNames[kMixedVariants] = {
+      "k_fd_wave_mixed<1,1>", "k_fd_wave_mixed<1,8>", "k_fd_wave_mixed<2,1>", "k_fd_wave_mixed<2,5>",
+      "k_fd_wave_mixed<2,6>", "k_fd_wave_mixed<4,1>", "k_fd_wave_mixed<4,3>", "k_fd_wave_mixed_split<4,1>",
+      "k_fd_wave_mixed_split<4,6>", "k_fd_wave_mixed_split<2,4>", "k_fd_wave_mixed_pair<4,4>",
+      "k_fd_wave_mixed_pair<4,1>", "k_fd_wave_mixed_pair<2,4>"};
+  return variant >= 0 && variant < kMixedVariants ? kNames[variant] : "";
+}
 int mixed_variant_layout(int variant) { return variant >= 10 ? 1 : 0; }
 
 template <int EPT, int MINB>

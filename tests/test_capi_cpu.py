@@ -162,3 +162,15 @@ def test_radiation_without_gpu_fails_loudly():
     run_case(s, CASES["traj_und"][:-1])
     with pytest.raises(RuntimeError, match="no usable GPU|without a GPU"):
         s.calculate_spectrum(obs=[0, 0, 30], energy_range_eV=[100, 200], npoints=3)
+
+
+def test_variant_names():
+    from oscars_b200 import _lib
+    for kind, n in ((0, 4), (2, 13), (3, 7)):
+        names = [_lib.variant_name(kind, v) for v in range(n)]
+        assert all(names) and len(set(names)) == n
+    assert _lib.variant_name(2, 10) == "k_fd_wave_mixed_pair<4,4>"
+    with pytest.raises(ValueError, match="out of range"):
+        _lib.variant_name(2, 13)
+    with pytest.raises(ValueError, match="kind"):
+        _lib.variant_name(1, 0)
