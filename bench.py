@@ -11,8 +11,11 @@ sample = one (observer, energy, trajectory point) term of the radiation sum, cou
 
 ``value``  flux integral with trajectory and observers resident in HBM (level samples rebuilt
            every step); CUDA events per step on the launching stream, L2 flushed between steps.
-``e2e``    the same job through the C ABI with host buffers: host RK4 + spline, host->device
-           copies, kernels, device->host copy of the results, every step.
+``e2e``    the same job through the C ABI (osc_flux) with pinned host buffers: observers copied
+           in, level samples rebuilt, kernels, flux and levels copied out, every step; the
+           trajectory is computed once before the loop, as in the reference arm's step.
+           ``e2e.with_new_trajectory`` also draws a new particle every step (host RK4 + spline +
+           trajectory upload inside the timing).
 Under torchrun each rank runs its own job (energy E1 * (1 + 1e-3 rank)): no collective on the data
 path, weak scaling; the reported time is the max over ranks.  The 10k-particle EPU beam is then run
 split over the ranks (``epu_beam_10k_sharded``: particles round-robin, one NCCL all_reduce of the
@@ -321,37 +324,48 @@ def product_arm(args):
             dist.destroy_process_group()
         return
 
-    # e2e: host buffers through the C ABI, new trajectory every step (host RK4 + spline included)
-    out_h = np.zeros(n)
-    lvl_h = np.zeros(n, dtype=np.int32)
+    # e2e: the user's call through the C ABI with host buffers in pinned memory: observers in, flux and
+    # levels out, copies inside the timed call.  Like the reference arm's step, the trajectory is the
+    # one computed before the timed loop; the level samples are rebuilt every step.  A second figure
+    # draws a new particle every step (host RK4 + spline + trajectory upload inside the timing).
+    xyz_p = torch.from_numpy(np.ascontiguousarray(xyz)).pin_memory()
+    out_p = torch.zeros(n, dtype=torch.float64).pin_memory()
+    lvl_p = torch.zeros(n, dtype=torch.int32).pin_memory()
+    xyz_h, out_h, lvl_h = xyz_p.numpy(), out_p.numpy(), lvl_p.numpy()  # numpy views of the pinned buffers
     nnc = ctypes.c_longlong()
 
-    def e2e_step():
-        s.set_new_particle(particle="ideal")  # drops the trajectory: RK4 + spline + upload again
-        ctx.call("osc_flux", _lib.dptr(xyz), n, energy, ctypes.byref(opts[head]), _lib.dptr(out_h),
-                 _lib.i32ptr(lvl_h), ctypes.byref(nnc))
-    e2e_step()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e2e_times, e2e_samples = [], 0
-    for i in range(max(1, min(args.steps, 20))):
-        t0 = time.perf_counter()
+    def e2e_run(new_particle):
+        def e2e_step():
+            if new_particle:
+                s.set_new_particle(particle="ideal")  # drops the trajectory: RK4 + spline + upload again
+            else:
+                ctx.call("osc_drop_level_cache")
+            ctx.call("osc_flux", _lib.dptr(xyz_h), n, energy, ctypes.byref(opts[head]), _lib.dptr(out_h),
+                     _lib.i32ptr(lvl_h), ctypes.byref(nnc))
         e2e_step()
-        e2e_times.append(time.perf_counter() - t0)
-        sm = ctypes.c_longlong()
-        ctx.call("osc_last_stats", ctypes.byref(sm), None)
-        e2e_samples += sm.value
-    te = torch.tensor([sum(e2e_times), float(e2e_samples)], dtype=torch.float64, device=dev)
-    if world > 1:
-        tm, ts = te.clone(), te.clone()
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
-        e2e_value = float(ts[1]) / float(tm[0]) / 1e9
-    else:
-        e2e_value = e2e_samples / sum(e2e_times) / 1e9
-    h2d = xyz.nbytes + 19 * 20001 * 8 + 8
-    d2h = out_h.nbytes + lvl_h.nbytes
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        times, samples = [], 0
+        for i in range(max(1, min(args.steps, 20))):
+            t0 = time.perf_counter()
+            e2e_step()
+            times.append(time.perf_counter() - t0)
+            sm = ctypes.c_longlong()
+            ctx.call("osc_last_stats", ctypes.byref(sm), None)
+            samples += sm.value
+        te = torch.tensor([sum(times), float(samples)], dtype=torch.float64, device=dev)
+        if world > 1:
+            tm, ts = te.clone(), te.clone()
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+            dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+            return float(ts[1]) / float(tm[0]) / 1e9
+        return samples / sum(times) / 1e9
+
+    e2e_value = e2e_run(False)
+    e2e_traj_value = e2e_run(True)
+    h2d = xyz.nbytes + 8
+    d2h = n * 8 + n * 4
     sharded = None
     if world > 1 and args.batched_steps > 0:  # every rank takes part in its collectives
         try:
@@ -366,7 +380,11 @@ def product_arm(args):
                 "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "compute": head, "l2": "flushed between steps (256 MB write)",
                            "parallelism": "independent job per rank" if world > 1 else "single GPU"},
-                "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "host_buffers": "pinned", "path": "osc_flux (C ABI), trajectory computed before the loop as in the reference arm",
+                        "with_new_trajectory": {"value": e2e_traj_value, "unit": "Gsamples/s",
+                                                "h2d_bytes_per_step": h2d + 19 * 20001 * 8,
+                                                "note": "new particle every step: host RK4 + spline + trajectory upload timed too"}},
                 "gpu_launches": r["launches_per_step"] * args.steps, "roofline": r["roofline"], "cpu_baseline": cpu,
                 "clocks": r["clocks"]}
         if "mixed" in res:
