@@ -6,16 +6,20 @@
 // them this file offers one entry point whose scratch memory is a file-scope static __device__
 // array, reserved when the library's module is loaded on a device and held until the process exits.
 //
-// The array's name is not a device address in host code.  Its address is looked up once per device
-// with cudaGetSymbolAddress (with that device current) and cached in a fixed-size table; the first
-// call on a device does that lookup, so make the first call on each device before any stream
-// capture begins.  All calls share the one array and it keeps the previous call's contents: every
-// region that must start at zero is cleared on each call, and two calls whose GPU work overlaps (from
-// different host threads, or on a device another thread is also using through this entry point)
-// race on the array.  Calls are synchronous: results are in `out` when the call returns.
+// The array's name is not a device address in host code.  Its address is looked up with
+// cudaGetSymbolAddress, with the device current, once per device and CUDA context: the lookup is
+// cached together with the context's unique ID, so a context that was destroyed and created again
+// (cudaDeviceReset in the host application) gets a fresh lookup instead of a stale address.  The
+// first call on a device (and the first after its context was re-created) does that lookup, so make
+// it before any stream capture begins.  All calls share the one array and it keeps the previous
+// call's contents: every region that must start at zero is cleared on each call, and two calls
+// whose GPU work overlaps (from different host threads, or on a device another thread is also using
+// through this entry point) race on the array.  Calls are synchronous: results are in `out` when the
+// call returns, and the caller's current device is restored before every return.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "../../include/oscars_b200.h"
@@ -28,7 +32,71 @@ constexpr size_t kScratchBytes = (size_t)16 << 20;  // 16 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices];  // per-device address of g_noalloc_scratch, null until looked up
+
+// Address of g_noalloc_scratch per device, valid for the context whose unique ID it records.
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;  // 0: not looked up
+  void* addr = nullptr;
+};
+ScratchSlot g_slots[kMaxDevices];
+std::mutex g_slots_mutex;
+
+// Driver entry points for the current context's unique ID (cuCtxGetCurrent, cuCtxGetId, CUDA 12.0),
+// resolved through the runtime so the library does not link libcuda directly.
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+std::once_flag g_driver_once;
+
+// Unique ID of the current context, 0 if the driver cannot tell (the address is then looked up on
+// every call).
+unsigned long long current_context_id() {
+  std::call_once(g_driver_once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!g_ctx_get_current || !g_ctx_get_id || g_ctx_get_current(&ctx) != 0 || !ctx || g_ctx_get_id(ctx, &id) != 0)
+    return 0;
+  return id;
+}
+
+// Device address of the scratch array on the current device (`device`), from the cache when the
+// context is the one it was looked up in.
+cudaError_t scratch_address(int device, void** out) {
+  const unsigned long long id = current_context_id();
+  std::lock_guard<std::mutex> lock(g_slots_mutex);
+  ScratchSlot& slot = g_slots[device];
+  if (id != 0 && slot.ctx_id == id && slot.addr) {
+    *out = slot.addr;
+    return cudaSuccess;
+  }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  slot.ctx_id = id;
+  slot.addr = p;
+  *out = p;
+  return cudaSuccess;
+}
+
+// Puts the caller's current device back when the entry point returns.
+struct DeviceRestore {
+  int prev = -1;
+  ~DeviceRestore() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 void set_message(char* msg, long long cap, const char* text) {
   if (msg && cap > 0) std::snprintf(msg, (size_t)cap, "%s", text);
@@ -107,14 +175,18 @@ extern "C" OSC_API int osc_flux_fixed_level_noalloc(int device, const double* tr
     set_message(message, message_capacity, text);
     return OSC_ERR_LENGTH;
   }
-  cudaError_t e = cudaSetDevice(device);
-  if (e == cudaSuccess && !g_scratch_addr[device]) e = cudaGetSymbolAddress(&g_scratch_addr[device], g_noalloc_scratch);
+  DeviceRestore restore;
+  cudaError_t e = cudaGetDevice(&restore.prev);
+  if (e != cudaSuccess) restore.prev = -1;
+  e = cudaSetDevice(device);
+  void* scratch = nullptr;
+  if (e == cudaSuccess) e = scratch_address(device, &scratch);
   if (e != cudaSuccess) {
     cudaGetLastError();
     set_message(message, message_capacity, cudaGetErrorString(e));
     return OSC_ERR_CUDA;
   }
-  unsigned char* base = static_cast<unsigned char*>(g_scratch_addr[device]);
+  unsigned char* base = static_cast<unsigned char*>(scratch);
   double* knots = reinterpret_cast<double*>(base + off_knots);
   double* u = reinterpret_cast<double*>(base + off_u);
   double* lev = reinterpret_cast<double*>(base + off_lev);
@@ -167,7 +239,7 @@ extern "C" OSC_API int osc_flux_fixed_level_noalloc(int device, const double* tr
     e = launch_fd_finalize(f, n_obs, st);
   }
   if (e == cudaSuccess) e = cudaMemcpy(out, res, sizeof(double) * n_obs, cudaMemcpyDeviceToHost);
-  static unsigned err_word;  // static storage: no allocation on this path
+  unsigned err_word = 0;
   if (e == cudaSuccess) e = cudaMemcpy(&err_word, cnt + 2, sizeof(unsigned), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) {
     cudaGetLastError();

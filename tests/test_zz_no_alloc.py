@@ -1,11 +1,14 @@
 """The allocation-free flux entry point (osc_flux_fixed_level_noalloc).
 
 It exists for callers that must not allocate on the call path (a plugin inside a host application
-that owns all device memory, a real-time loop past start-up); its scratch is a static device array.
-Here it is called through the C ABI twice in a row on the same inputs, and each result is checked
-against the regular entry point (osc_flux through oscars_b200.sr, fixed level: precision=0,
-max_level=L) within the parity tolerance of the other GPU tests: 1e-9 peak-normalised.  Requests
-beyond the static scratch must be refused with a message.  This file is named to be collected last.
+that owns all device memory, a real-time loop past start-up); its scratch is a static device array
+that every call reuses.  Here it is called through the C ABI on consecutive requests -- a larger one
+(more observers, a higher level) before a smaller one, and the same request twice -- and each result
+is checked against the regular entry point (osc_flux through oscars_b200.sr, fixed level:
+precision=0, max_level=L) within the parity tolerance of the other GPU tests: 1e-9 peak-normalised.
+That covers what a previous call leaves behind in the shared array.  A warm call must leave the
+device's free memory unchanged, and requests beyond the static scratch must be refused with a
+message.  This file is named to be collected last.
 """
 import ctypes
 
@@ -39,24 +42,49 @@ def _noalloc(traj, obs, level, pol=None):
     return rc, out, msg.value.decode()
 
 
-@pytest.mark.parametrize("pol", [None, "lh"])
-def test_noalloc_matches_regular_entry_point_twice(pol):
-    s = _setup()
-    traj = s.trajectory_array()
-    level = 11
-    kw = dict(energy_eV=E1_U, npoints=[41, 41], width=[0.01, 0.01], translation=[0, 0, 30], precision=0,
+def _regular(s, npoints, level, pol):
+    kw = dict(energy_eV=E1_U, npoints=npoints, width=[0.01, 0.01], translation=[0, 0, 30], precision=0,
               max_level=level, dim=3)
     if pol:
         kw["polarization"] = pol
     res = s.calculate_flux_rectangle(**kw)
-    obs = np.array([r[0] for r in res])
-    ref = np.array([r[1] for r in res])
+    return np.array([r[0] for r in res]), np.array([r[1] for r in res])
+
+
+@pytest.mark.parametrize("pol", [None, "lh"])
+def test_noalloc_matches_regular_entry_point_on_consecutive_requests(pol):
+    s = _setup()
+    traj = s.trajectory_array()
     pvec = None if pol is None else np.array([1.0, 0, 0, 0, 0, 0])
-    for call in range(2):
+    # larger request first (more observers, higher level), then a smaller one twice
+    for npoints, level in (([61, 61], 12), ([41, 41], 11), ([41, 41], 11)):
+        obs, ref = _regular(s, npoints, level, pol)
         rc, out, msg = _noalloc(traj, obs, level, pvec)
         assert rc == 0, msg
         err = float(np.max(np.abs(out - ref)) / np.max(np.abs(ref)))
-        assert err <= TOL, "call %d: peak-normalised error %.3e" % (call, err)
+        assert err <= TOL, "%s at level %d: peak-normalised error %.3e" % (npoints, level, err)
+
+
+def test_noalloc_warm_call_leaves_free_device_memory_unchanged():
+    import torch
+    s = _setup()
+    traj = s.trajectory_array()
+    obs, ref = _regular(s, [21, 21], 10, None)
+    rc, out, msg = _noalloc(traj, obs, 10)  # warm: module and scratch address set up
+    assert rc == 0, msg
+    same = False
+    for _ in range(3):  # another process on the device could move the figure; one exact match suffices
+        torch.cuda.synchronize(0)
+        before = torch.cuda.mem_get_info(0)[0]
+        rc, out, msg = _noalloc(traj, obs, 10)
+        torch.cuda.synchronize(0)
+        after = torch.cuda.mem_get_info(0)[0]
+        assert rc == 0, msg
+        if before == after:
+            same = True
+            break
+    assert same, "free device memory changed across an allocation-free call"
+    assert float(np.max(np.abs(out - ref)) / np.max(np.abs(ref))) <= TOL
 
 
 def test_noalloc_refuses_requests_beyond_its_scratch():
