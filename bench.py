@@ -272,7 +272,10 @@ def product_arm(args):
     d_out = {m: torch.zeros(n, dtype=torch.float64, device=dev) for m in modes}
     d_lvl = torch.zeros(n, dtype=torch.int32, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
-    stream = torch.cuda.current_stream(dev)
+    # one dedicated stream: the library's kernels, the L2 flush and the timing events all go on it
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sptr = ctypes.c_void_p(stream.cuda_stream)
 
     def make_step(m):

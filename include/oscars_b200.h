@@ -313,12 +313,16 @@ OSC_API int osc_measure_fma_peak(osc_ctx* ctx, int kind, double* tflops);
  * heap.  Its scratch is a 16 MiB static device array held by every GPU that loads the library until
  * the process exits; a request must fit in it (224 B per trajectory point + 80 B x 2^(level+1) +
  * 176 B per observer, alignment aside) or the call returns OSC_ERR_LENGTH with the reason in
- * `message`.  The first call on a device looks up the array's device address, so make it before any
- * stream capture.  Calls are synchronous; they all share the one array, so calls whose GPU work
- * overlaps race.  trajectory: host, 10 x n SoA as osc_get_trajectory returns it; obs_xyz: host,
- * 3 x n_obs; polarization: host, 6 doubles (re, im of x, y, z) or NULL for none; charge [C] and
- * current [A] of the particle; out: host, n_obs values in the units of osc_flux; message: optional
- * buffer for a NUL-terminated reason. */
+ * `message`.  The array's device address is looked up on the first call on each device (and again
+ * on the first call after that device's CUDA context was destroyed and created anew, e.g. by
+ * cudaDeviceReset), so make the first call on a device before any stream capture.  Calls are
+ * synchronous and restore the caller's current device before returning.  Every call uses the same
+ * array, which keeps the previous call's contents (what must start at zero is cleared on each call);
+ * two calls whose GPU work overlaps -- from different host threads, or alongside another thread's
+ * call on the same device -- race on it and may return wrong results.  trajectory: host, 10 x n SoA
+ * as osc_get_trajectory returns it; obs_xyz: host, 3 x n_obs; polarization: host, 6 doubles (re, im
+ * of x, y, z) or NULL for none; charge [C] and current [A] of the particle; out: host, n_obs values
+ * in the units of osc_flux; message: optional buffer for a NUL-terminated reason. */
 OSC_API int osc_flux_fixed_level_noalloc(int device, const double* trajectory, long long n_points,
                                          const double* obs_xyz, long long n_obs, double energy_eV,
                                          int level, double charge, double current,

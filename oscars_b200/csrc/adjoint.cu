@@ -572,6 +572,7 @@ void Engine::trajectory_vjp(const double* knot_grad, double* grad_params, int64_
   const int param_field = param_field_of(model, n_params);
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
+  use_stream(stream);
   cudaStream_t st = stream;
   model.ensure_trajectory();
   upload_trajectory();
@@ -594,6 +595,7 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
   if (project) throw Error{OSC_ERR_INVALID, "the adjoint supports polarization 'all'"};
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
+  use_stream(stream);
   pending_.clear();
   last_samples = last_launches = last_not_converged = 0;
   cudaStream_t st = stream;

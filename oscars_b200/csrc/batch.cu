@@ -309,10 +309,11 @@ __global__ void k_batch_spline(const DevJob* __restrict__ jobs, int njobs, doubl
 }
 
 // Level samples [s_begin, s_end) of every job whose active count is non-zero (all jobs when `cnt` is
-// NULL), evaluated from its spline and written as mixed records (fd_common.cuh) at
-// rec[3 * (j * stride + s - s_off)]; one thread per (job, sample).
+// NULL), evaluated from its spline and written as pair records (fd_common.cuh): job j's records
+// start at float kPairFloats / 2 * j * stride of `rec`, sample s at local index s - s_off (s_off
+// even); sample 0 is the zero-amplitude record.  One thread per (job, sample).
 __global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const double* __restrict__ arena,
-                             const unsigned* __restrict__ cnt, float4* __restrict__ rec, int64_t stride,
+                             const unsigned* __restrict__ cnt, float* __restrict__ rec, int64_t stride,
                              int64_t s_off, int64_t s_begin, int64_t s_end) {
   const int64_t per = s_end - s_begin;
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -322,7 +323,7 @@ __global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const d
   const DevJob& J = jobs[j];
   const int64_t s = s_begin + g % per;
   const int64_t n = (int64_t)J.nf + J.nb;
-  const double T = level_time(J.tstart, J.tstop, s);
+  const double T = level_time(J.tstart, J.tstop, s == 0 ? 1 : s);
   double v[9];
   spline_eval9(arena + J.knots, n, T, v);
   const MixedFrame& F = J.frame;
@@ -337,13 +338,9 @@ __global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const d
   const double qx = R[0] * v[6] + R[1] * v[7] + R[2] * v[8];
   const double qy = R[3] * v[6] + R[4] * v[7] + R[5] * v[8];
   const double qz = R[6] * v[6] + R[7] * v[7] + R[8] * v[8];
-  const double g2 = 1.0 - (px * px + py * py + pz * pz);       // 1 - b^2
-  const double ebz = (g2 + px * px + py * py) / (1.0 + pz);     // 1 - b_z without cancellation
   const double taus = (T - F.t_ref) - z / kCLight;
-  float4* r = rec + 3 * (j * stride + s - s_off);
-  r[0] = make_float4((float)x, (float)y, (float)z, (float)taus);
-  r[1] = make_float4((float)px, (float)py, (float)ebz, (float)g2);
-  r[2] = make_float4((float)qx, (float)qy, (float)qz, 0.f);
+  write_pair_record(rec + (kPairFloats / 2) * (int64_t)j * stride, s - s_off, s == 0, x, y, z, taus, px, py, pz, qx,
+                    qy, qz);
 }
 
 // Offsets of one wave over the chunk (one block of 1024 threads): per job the active count n_j (all
@@ -424,20 +421,30 @@ __device__ __forceinline__ int find_job(const int64_t* __restrict__ starts, int 
 }
 
 constexpr int kBThreads = 128;
-constexpr int kBChunk = 256;
-constexpr int kBFold = 32;  // FP32 partial sums are folded into FP64 every kBFold samples
+constexpr int kBChunk = 256;   // samples per staged chunk (128 pair records, 20 KB)
+constexpr int kBFold = 16;     // pairs per FP32 partial sum before it is folded into FP64
 
 struct BatchStage {
-  float4 v[2][kBChunk * 3];
+  float4 v[2][kBChunk / 2 * kPairF4];
   uint64_t bar[2];
 };
 
-template <int EPT, int MINB>
+// The mixed sample sum over all jobs of a chunk.  Persistent CTAs take (job, tile, span) units from a
+// shared counter (the job by binary search of the unit prefix); within a unit the sum is that of
+// k_fd_wave_mixed_pair: SUB groups of TE = 128 / SUB threads, one entry per thread, each group
+// taking 1/SUB of every staged chunk of pair records, the largest phase step carried across parts
+// and spans (the span maxima include the step into each span).  One partial per entry and span,
+// entry-major per job from part_start[j]; k_batch_finalize reduces them.
+template <int SUB, int MINB>
 __global__ void __launch_bounds__(kBThreads, MINB) k_batch_wave(BatchWaveArgs A) {
+  constexpr int TE = kBThreads / SUB;
+  constexpr int CP = kBChunk / 2;  // pairs per chunk
   __shared__ __align__(16) BatchStage st;
+  __shared__ double red[SUB > 1 ? SUB - 1 : 1][7][TE];
   __shared__ WavePlan P;
   __shared__ int64_t next_unit;
   const int tid = threadIdx.x;
+  const int grp = tid / TE, q = tid % TE;
   if (tid == 0) {
     P = wave_plan_spans(A.first, A.level, *A.plan.spans);
     mbar_init(&st.bar[0], 1);
@@ -459,14 +466,11 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_batch_wave(BatchWaveArgs A)
     const int64_t tile = local / P.spans;
     const int span = (int)(local % P.spans);
     const int64_t n_act = A.first ? J.n_obs * J.n_e : (int64_t)A.cnt[j];
-    float Ox[EPT], Oy[EPT], Oz[EPT], w[EPT], wc[EPT];
-    bool live[EPT];
-    int64_t slot[EPT];
-#pragma unroll
-    for (int e = 0; e < EPT; ++e) {
-      slot[e] = tile * kBThreads * EPT + (int64_t)e * kBThreads + tid;
-      live[e] = slot[e] < n_act;
-      const int64_t item = live[e] ? (A.first ? slot[e] : (int64_t)A.act[J.entry_begin + slot[e]]) : 0;
+    const int64_t slot = tile * TE + q;
+    const bool live = slot < n_act;
+    const int64_t item = live ? (A.first ? slot : (int64_t)A.act[J.entry_begin + slot]) : 0;
+    PairObs o;
+    {
       const int64_t io = J.obs_begin + item / J.n_e, ie = J.omega_begin + item % J.n_e;
       const double* R = J.frame.rot;
       const double ox = A.obs[3 * io] - J.frame.x0[0], oy = A.obs[3 * io + 1] - J.frame.x0[1];
@@ -474,42 +478,36 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_batch_wave(BatchWaveArgs A)
       const double fx = R[0] * ox + R[1] * oy + R[2] * oz;
       const double fy = R[3] * ox + R[4] * oy + R[5] * oz;
       const double fz = R[6] * ox + R[7] * oy + R[8] * oz;
-      Ox[e] = (float)fx; Oy[e] = (float)fy; Oz[e] = (float)fz;
       const double om = A.omega[ie];
-      w[e] = (float)om;
-      wc[e] = (float)(om / kCLight);
-      if (live[e] && span == 0 && !mixed_geometry_ok(fx, fy, fz, om, J.frame.xperp_max, J.frame.z_max))
-        atomicOr(A.err, kErrBadArgs);
+      o = make_pair_obs(fx, fy, fz, om);
+      if (live && grp == 0 && span == 0 && !mixed_geometry_ok(fx, fy, fz, om, J.frame)) atomicOr(A.err, kErrBadArgs);
     }
-    // records of job j: sample s at rec_j[3 * (s - s_off)]
-    const float4* rec_j = A.rec + 3 * (int64_t)j * A.stride;
+    // pair records of job j: absolute pair p at rec_j[kPairF4 * (p - s_off / 2)]
+    const float4* rec_j = A.rec + (kPairF4 / 2) * (int64_t)j * A.stride - kPairF4 * (A.s_off >> 1);
     for (int g = 0; g < P.nseg; ++g) {
       const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
       const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
-      double S[EPT][6];
-      float first[EPT], last[EPT], dmax[EPT];
-      bool have[EPT];
-#pragma unroll
-      for (int e = 0; e < EPT; ++e) {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) S[e][k] = 0.0;
-        first[e] = last[e] = 0.f;
-        dmax[e] = 0.f;
-        have[e] = false;
-      }
-      const int64_t nchunks = b1 > b0 ? (b1 - b0 + kBChunk - 1) / kBChunk : 0;
+      const int64_t p0 = b0 >> 1, p1 = b1 > b0 ? b1 >> 1 : p0;  // spans are whole pairs
+      double S[6] = {0, 0, 0, 0, 0, 0};
+      float dmax = 0.f;
+      bool any = false;
+      const int64_t nchunks = (p1 - p0 + CP - 1) / CP;
+      float carry = __int_as_float(0x7fc00000);  // NaN: no step into the segment's first sample
+      if (live && span > 0 && nchunks > 0)
+        carry = pair_phase_at(reinterpret_cast<const float*>(rec_j + kPairF4 * (p0 - 1)), 1, o);
       if (tid == 0 && nchunks > 0) {
-        const int64_t hi = min(b1, b0 + kBChunk);
-        mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - b0) * 48));
-        tma_load_1d(&st.v[0][0], rec_j + 3 * (b0 - A.s_off), (uint32_t)((hi - b0) * 48), &st.bar[0]);
+        const int64_t hi = min(p1, p0 + CP);
+        mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - p0) * (kPairFloats * 4)));
+        tma_load_1d(&st.v[0][0], rec_j + kPairF4 * p0, (uint32_t)((hi - p0) * (kPairFloats * 4)), &st.bar[0]);
       }
       for (int64_t c = 0; c < nchunks; ++c) {
         const int buf = (int)(c & 1);
-        const int64_t lo = b0 + c * kBChunk, hi = min(b1, lo + kBChunk);
+        const int64_t lo = p0 + c * CP, hi = min(p1, lo + CP);
         if (tid == 0 && c + 1 < nchunks) {  // prefetch the next chunk into the other buffer
-          const int64_t lo2 = lo + kBChunk, hi2 = min(b1, lo2 + kBChunk);
-          mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * 48));
-          tma_load_1d(&st.v[buf ^ 1][0], rec_j + 3 * (lo2 - A.s_off), (uint32_t)((hi2 - lo2) * 48), &st.bar[buf ^ 1]);
+          const int64_t lo2 = lo + CP, hi2 = min(p1, lo2 + CP);
+          mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * (kPairFloats * 4)));
+          tma_load_1d(&st.v[buf ^ 1][0], rec_j + kPairF4 * lo2, (uint32_t)((hi2 - lo2) * (kPairFloats * 4)),
+                      &st.bar[buf ^ 1]);
         }
         if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
           if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
@@ -517,46 +515,55 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_batch_wave(BatchWaveArgs A)
         }
         phase_bits ^= 1u << buf;
         const float4* sv = st.v[buf];
-        const int j0 = lo == 0 ? 1 : 0;  // sample 0 is the unused slot
         const int n = (int)(hi - lo);
-        for (int jb = j0; jb < n; jb += kBFold) {
-          const int je = min(n, jb + kBFold);
-          float s32[EPT][6];
+        const int j0 = (grp * n) / SUB, j1 = ((grp + 1) * n) / SUB;  // the chunk's pairs split evenly
+        if (live && j0 < j1) {
+          float last = j0 > 0 ? pair_phase_at(reinterpret_cast<const float*>(sv + kPairF4 * (j0 - 1)), 1, o) : carry;
+          for (int jb = j0; jb < j1; jb += kBFold) {
+            const int je = min(j1, jb + kBFold);
+            float2 acc[6];
 #pragma unroll
-          for (int e = 0; e < EPT; ++e)
+            for (int k = 0; k < 6; ++k) acc[k] = f2(0.f);
+#pragma unroll 2
+            for (int jj = jb; jj < je; ++jj) {
+              const float2 ph = pair_sample(sv + kPairF4 * jj, o, acc);
+              dmax = fmaxf(dmax, fmaxf(fabsf(ph.x - last), fabsf(ph.y - ph.x)));
+              last = ph.y;
+            }
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s32[e][k] = 0.f;
-          for (int jj = jb; jj < je; ++jj) {
-            const float4 r0 = sv[3 * jj], r1 = sv[3 * jj + 1], r2 = sv[3 * jj + 2];
-#pragma unroll
-            for (int e = 0; e < EPT; ++e) {
-              const float ph = mixed_sample(r0, r1, r2, Ox[e], Oy[e], Oz[e], w[e], wc[e], s32[e]);
-              if (have[e]) {
-                dmax[e] = fmaxf(dmax[e], fabsf(ph - last[e]));
-              } else {
-                first[e] = ph;
-                have[e] = true;
-              }
-              last[e] = ph;
+            for (int k = 0; k < 6; k += 2) {
+              S[k] += (double)acc[k].x + (double)acc[k].y;
+              S[k + 1] -= (double)acc[k + 1].x + (double)acc[k + 1].y;
             }
           }
-#pragma unroll
-          for (int e = 0; e < EPT; ++e)
-#pragma unroll
-            for (int k = 0; k < 6; ++k) S[e][k] += (double)s32[e][k];
+          any = true;
         }
+        if (live && c + 1 < nchunks)  // the chunk is full: its last sample precedes the next
+          carry = pair_phase_at(reinterpret_cast<const float*>(sv + kPairF4 * (CP - 1)), 1, o);
         __syncthreads();  // everyone is done with `buf` before it is refilled
       }
+      // reduce the groups' sums in group order; group 0 stores the span's partial
+      if (SUB > 1 && grp > 0) {
 #pragma unroll
-      for (int e = 0; e < EPT; ++e) {
-        if (!live[e]) continue;
-        double* p = A.part + A.plan.part_start[j] + (slot[e] * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) p[k] = S[e][k];
-        p[6] = have[e] ? (double)first[e] : 0.0;
-        p[7] = have[e] ? (double)last[e] : 0.0;
-        p[8] = have[e] ? (double)dmax[e] : -1.0;  // -1 marks an empty span
+        for (int k = 0; k < 6; ++k) red[grp - 1][k][q] = S[k];
+        red[grp - 1][6][q] = any ? (double)dmax : -1.0;
       }
+      if (SUB > 1) __syncthreads();
+      if (grp == 0 && live) {
+        double dm = any ? (double)dmax : -1.0;
+        for (int o2 = 0; o2 < SUB - 1; ++o2) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) S[k] += red[o2][k][q];
+          dm = fmax(dm, red[o2][6][q]);
+        }
+        double* p = A.part + A.plan.part_start[j] + (slot * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) p[k] = S[k];
+        p[6] = 0.0;
+        p[7] = 0.0;
+        p[8] = dm;  // -1 marks an empty span
+      }
+      if (SUB > 1) __syncthreads();
     }
   }
 }
@@ -589,10 +596,7 @@ __global__ void __launch_bounds__(256) k_batch_finalize(BatchFinalArgs A) {
         for (int sp = lane; sp < spans; sp += kFinLanes) {
           const double* p = pbase + (g * spans + sp) * kFdPartials;
           t.xr += p[0]; t.xi += p[1]; t.yr += p[2]; t.yi += p[3]; t.zr += p[4]; t.zi += p[5];
-          if (p[8] >= 0) {  // non-empty span (empty spans only trail the segment)
-            dm = fmax(dm, p[8]);
-            if (sp > 0) dm = fmax(dm, fabs(p[6] - p[-kFdPartials + 7]));
-          }
+          if (p[8] >= 0) dm = fmax(dm, p[8]);  // the span maxima include the step into each span
         }
       }
       s.xr += group_sum(t.xr); s.xi += group_sum(t.xi); s.yr += group_sum(t.yr);
@@ -686,37 +690,33 @@ __global__ void k_batch_average(const double* __restrict__ vals, const DevJob* _
 // ---------------------------------------------------------------------------------------------
 // Variants of the batched wave kernel: (entries per thread, minimum resident CTAs per SM).
 // ---------------------------------------------------------------------------------------------
-static const int kBatchEpt[kBatchVariants] = {1, 1, 2, 2, 2, 4, 4};
+static const int kBatchSub[kBatchVariants] = {4, 4, 2, 1};  // groups per CTA: tiles of 128 / SUB entries
 
-template <int EPT, int MINB>
+template <int SUB, int MINB>
 static int batch_occ() {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_batch_wave<EPT, MINB>, dev::kBThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_batch_wave<SUB, MINB>, dev::kBThreads, 0);
   return n > 0 ? n : 1;
 }
 
 static int batch_blocks_per_sm(int variant) {
   switch (variant) {
-    case 0: return batch_occ<1, 1>();
-    case 1: return batch_occ<1, 8>();
-    case 2: return batch_occ<2, 1>();
-    case 3: return batch_occ<2, 5>();
-    case 4: return batch_occ<2, 6>();
-    case 5: return batch_occ<4, 1>();
-    default: return batch_occ<4, 3>();
+    case 0: return batch_occ<4, 4>();
+    case 1: return batch_occ<4, 1>();
+    case 2: return batch_occ<2, 4>();
+    default: return batch_occ<1, 4>();
   }
 }
+
+static int batch_tile(int variant) { return dev::kBThreads / kBatchSub[variant]; }
 
 static cudaError_t launch_batch_wave(const BatchWaveArgs& a, int grid, int variant, cudaStream_t st) {
   const int T = dev::kBThreads;
   switch (variant) {
-    case 0: dev::k_batch_wave<1, 1><<<grid, T, 0, st>>>(a); break;
-    case 1: dev::k_batch_wave<1, 8><<<grid, T, 0, st>>>(a); break;
-    case 2: dev::k_batch_wave<2, 1><<<grid, T, 0, st>>>(a); break;
-    case 3: dev::k_batch_wave<2, 5><<<grid, T, 0, st>>>(a); break;
-    case 4: dev::k_batch_wave<2, 6><<<grid, T, 0, st>>>(a); break;
-    case 5: dev::k_batch_wave<4, 1><<<grid, T, 0, st>>>(a); break;
-    default: dev::k_batch_wave<4, 3><<<grid, T, 0, st>>>(a); break;
+    case 0: dev::k_batch_wave<4, 4><<<grid, T, 0, st>>>(a); break;
+    case 1: dev::k_batch_wave<4, 1><<<grid, T, 0, st>>>(a); break;
+    case 2: dev::k_batch_wave<2, 4><<<grid, T, 0, st>>>(a); break;
+    default: dev::k_batch_wave<1, 4><<<grid, T, 0, st>>>(a); break;
   }
   return cudaGetLastError();
 }
@@ -726,7 +726,7 @@ static cudaError_t launch_batch_wave(const BatchWaveArgs& a, int grid, int varia
 // ---------------------------------------------------------------------------------------------
 namespace {
 constexpr int kBatchPrefill = 13;        // levels enqueued without the host (records kept resident)
-constexpr int kBatchMinSpan = 32;
+constexpr int kBatchMinSpan = 128;
 constexpr int kBatchMaxJobsPerChunk = 4096;
 }  // namespace
 
@@ -840,6 +840,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     }
     d.frame.x0[0] = P.x0.x; d.frame.x0[1] = P.x0.y; d.frame.x0[2] = P.x0.z;
     d.frame.t_ref = P.t0 / kC;
+    d.frame.theta_max = mixed_theta_max(P.gamma);
     d.b0[0] = P.b0.x; d.b0[1] = P.b0.y; d.b0[2] = P.b0.z;
     d.qomg = P.qomg;
     d.dt = dt;
@@ -861,6 +862,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
 
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
+  use_stream(stream);
   cudaStream_t st = stream;
   std::vector<DevField> df;
   std::vector<double> fvals;
@@ -887,7 +889,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
   int max_resident = 0, max_tile = 0;
   for (int v = 0; v < kBatchVariants; ++v) {
     max_resident = std::max(max_resident, batch_resident(v));
-    max_tile = std::max(max_tile, dev::kBThreads * kBatchEpt[v]);
+    max_tile = std::max(max_tile, batch_tile(v));
   }
   const int64_t target = 4 * (int64_t)max_resident;  // >= 4 units per resident CTA when work allows
 
@@ -902,7 +904,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     size_t j1 = j0, bytes = 0;
     while (j1 < dj.size() && j1 - j0 < (size_t)kBatchMaxJobsPerChunk) {
       const DevJob& d = dj[j1];
-      const size_t need = sizeof(double) * 28 * ((size_t)d.nf + d.nb) + 48 * (size_t)rec_per_job +
+      const size_t need = sizeof(double) * 28 * ((size_t)d.nf + d.nb) + kMixedRecordBytesPerSample * (size_t)rec_per_job +
                           (size_t)(d.n_obs * d.n_e) * (56 + 8 + 4 + 8 + 16 * kFdPartials);
       if (j1 > j0 && bytes + need > budget) break;
       bytes += need;
@@ -926,7 +928,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     b_jobs_.reserve(sizeof(DevJob) * nj);
     b_knots_.reserve(sizeof(double) * knots);
     b_work_.reserve(sizeof(double) * work);
-    b_rec_.reserve(sizeof(float4) * 3 * rec_per_job * nj);
+    b_rec_.reserve((size_t)kMixedRecordBytesPerSample * rec_per_job * nj);
     b_state_.reserve(sizeof(double) * 7 * N);
     b_out_.reserve(sizeof(double) * N);
     b_lvl_.reserve(sizeof(int32_t) * N);
@@ -954,7 +956,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
       unsigned* cin = cnts[cur];
       unsigned* cout = cnts[cur ^ 1];
       check(cudaMemsetAsync(cout, 0, sizeof(unsigned) * nj, st), "memset");
-      const int tile = dev::kBThreads * kBatchEpt[v];
+      const int tile = batch_tile(v);
       dev::k_batch_plan<<<1, 1024, 0, st>>>(d_jobs, nj, cin, first, L, tile, target, kBatchMinSpan, plan);
       BatchWaveArgs w{};
       w.jobs = d_jobs; w.njobs = nj; w.rec = rec; w.stride = stride; w.s_off = s_off;
@@ -979,9 +981,9 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
                                                           b_fvals_.as<double>(), b_knots_.as<double>(), misc);
       dev::k_batch_extent<<<nj, 256, 0, st>>>(d_jobs, b_knots_.as<double>());
       dev::k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_knots_.as<double>(), b_work_.as<double>());
-      const int64_t fill_n = (rec_per_job - 1) * nj;
+      const int64_t fill_n = rec_per_job * nj;  // samples 0 .. 2^(Lpre+1) - 1 of every job
       dev::k_batch_fill<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(
-          d_jobs, nj, b_knots_.as<double>(), nullptr, b_rec_.as<float4>(), rec_per_job, 0, 1, rec_per_job);
+          d_jobs, nj, b_knots_.as<double>(), nullptr, b_rec_.as<float>(), rec_per_job, 0, 0, rec_per_job);
       check(cudaGetLastError(), "batch trajectories");
       last_launches += 4;
       if (tune) v = tune_batch(nj, Lfirst, target, d_jobs, plan, misc, m64, rec_per_job);
@@ -1043,10 +1045,10 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
       for (unsigned x : c) any = any || x > 0;
       if (!any) break;
       const int64_t len = (int64_t)1 << L;
-      b_rec_ext_.reserve(sizeof(float4) * 3 * len * nj);
+      b_rec_ext_.reserve((size_t)kMixedRecordBytesPerSample * len * nj);
       const int64_t fill_n = len * nj;
       dev::k_batch_fill<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(
-          d_jobs, nj, b_knots_.as<double>(), cnts[cur], b_rec_ext_.as<float4>(), len, len, len, 2 * len);
+          d_jobs, nj, b_knots_.as<double>(), cnts[cur], b_rec_ext_.as<float>(), len, len, len, 2 * len);
       check(cudaGetLastError(), "batch fill");
       ++last_launches;
       wave(L, v, len, len, b_rec_ext_.as<float4>());
@@ -1079,8 +1081,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     if (err & dev::kErrSuperluminal)
       throw Error{OSC_ERR_RANGE, "a trajectory reached the speed of light (check the fields)"};
     if (err & dev::kErrBadArgs)
-      throw Error{OSC_ERR_INVALID, "compute='mixed' needs observers near the beam axis (angle < 1e-2 and a correction "
-                                   "phase below 3e4 rad); use compute='fp64' for this geometry"};
+      throw Error{OSC_ERR_INVALID, kMixedGeometryMessage};
     last_not_converged += (long long)h64[0];
     last_samples += (long long)h64[1];
     if (profiling) {
@@ -1107,7 +1108,7 @@ int Engine::tune_batch(int nj, int Lfirst, int64_t target, const DevJob* d_jobs,
   int best = current_variant_[3];
   float best_ms = 1e30f;
   for (int v = 0; v < kBatchVariants; ++v) {
-    const int tile = dev::kBThreads * kBatchEpt[v];
+    const int tile = batch_tile(v);
     dev::k_batch_plan<<<1, 1024, 0, st>>>(d_jobs, nj, nullptr, 1, Lfirst, tile, target, kBatchMinSpan, plan);
     BatchWaveArgs w{};
     w.jobs = d_jobs; w.njobs = nj; w.rec = b_rec_.as<float4>(); w.stride = rec_stride; w.s_off = 0;

@@ -57,7 +57,7 @@ struct BatchPlan {
 struct BatchWaveArgs {
   const DevJob* jobs;
   int njobs;
-  const float4* rec;        // records: sample s of job j at rec[3 * (j * stride + s - s_off)]
+  const float4* rec;        // pair records: job j from float4 5 * j * stride, sample s at local index s - s_off
   int64_t stride, s_off;
   const double* obs;
   const double* omega;
@@ -94,7 +94,7 @@ struct FieldSpec;
 // Device form of a field; grid values and half-period factors are appended to `vals`.
 DevField to_dev_field(FieldSpec f, std::vector<double>& vals);
 
-// Compiled variants of the batched wave kernel (entries per thread, minimum CTAs per SM).
-constexpr int kBatchVariants = 7;
+// Compiled variants of the batched wave kernel (groups per CTA, minimum CTAs per SM).
+constexpr int kBatchVariants = 4;
 
 }  // namespace osc

@@ -628,9 +628,8 @@ OSC_API int osc_variant_name(int kind, int variant, char* name, long long capaci
     if (variant < 0 || variant >= n_variants_of(kind)) throw osc::Error{OSC_ERR_RANGE, "variant out of range"};
     static const char* const kFp64[] = {"k_fd_wave_fp64<1>", "k_fd_wave_fp64<6>", "k_fd_wave_fp64<7>",
                                         "k_fd_wave_fp64<8>"};
-    static const char* const kBatch[] = {"k_batch_wave<1,1>", "k_batch_wave<1,8>", "k_batch_wave<2,1>",
-                                         "k_batch_wave<2,5>", "k_batch_wave<2,6>", "k_batch_wave<4,1>",
-                                         "k_batch_wave<4,3>"};
+    static const char* const kBatch[] = {"k_batch_wave<4,4>", "k_batch_wave<4,1>", "k_batch_wave<2,4>",
+                                         "k_batch_wave<1,4>"};
     static_assert(sizeof(kFp64) / sizeof(kFp64[0]) == osc::kFp64Variants, "FP64 variant names");
     static_assert(sizeof(kBatch) / sizeof(kBatch[0]) == osc::kBatchVariants, "batch variant names");
     const char* n = kind == 0 ? kFp64[variant] : kind == 2 ? osc::mixed_variant_name(variant) : kBatch[variant];

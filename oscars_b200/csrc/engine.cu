@@ -60,6 +60,8 @@ Engine::Engine(int dev) : device(dev) {
         "cudaHostAlloc");
   for (int i = 0; i < kStatSlots; ++i) check(cudaEventCreateWithFlags(&stats_ev_[i], cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming), "event");
+  check(cudaEventCreateWithFlags(&order_ev_, cudaEventDisableTiming), "event");
+  cur_ = stream;
 }
 
 Engine::~Engine() {
@@ -70,6 +72,8 @@ Engine::~Engine() {
   for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
   for (int i = 0; i < kStatSlots; ++i) if (stats_ev_[i]) cudaEventDestroy(stats_ev_[i]);
   if (stage_ev_) cudaEventDestroy(stage_ev_);
+  if (order_ev_) cudaEventDestroy(order_ev_);
+  if (last_stream_valid_ && last_stream_ != stream) cudaStreamSynchronize(last_stream_);
   if (stats_host_) cudaFreeHost(stats_host_);
   if (stage_host_) cudaFreeHost(stage_host_);
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
@@ -92,12 +96,12 @@ void Engine::upload_trajectory() {
   const int64_t n = k.n;
   knots_.reserve(sizeof(double) * 20 * n);
   double* d = knots_.as<double>();
-  check(cudaMemcpyAsync(d, k.t.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload t");
-  check(cudaMemcpyAsync(d + n, k.y.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, stream), "upload y");
-  check(cudaMemcpyAsync(d + 10 * n, k.ypp.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, stream),
+  check(cudaMemcpyAsync(d, k.t.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cur_), "upload t");
+  check(cudaMemcpyAsync(d + n, k.y.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, cur_), "upload y");
+  check(cudaMemcpyAsync(d + 10 * n, k.ypp.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, cur_),
         "upload ypp");
   if ((int64_t)k.diag.size() == n)
-    check(cudaMemcpyAsync(d + 19 * n, k.diag.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream),
+    check(cudaMemcpyAsync(d + 19 * n, k.diag.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cur_),
           "upload diag");
   nknots_ = n;
   tstart_ = k.tstart;
@@ -106,7 +110,7 @@ void Engine::upload_trajectory() {
   lev_filled_ = -1;
   mrec_filled_ = -1;
   bdmax_valid_ = false;
-  check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), stream), "memset");
+  check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), cur_), "memset");
 }
 
 // Make levels 0..L resident.  The cache grows by doubling; growing refills from level 0.
@@ -122,9 +126,9 @@ void Engine::ensure_levels(int L) {
       const int64_t used = (int64_t)2 << lev_filled_;
       for (int a = 0; a < 10; ++a)
         check(cudaMemcpyAsync(nb.as<double>() + a * cap, lev_.as<double>() + a * lev_cap_, sizeof(double) * used,
-                              cudaMemcpyDeviceToDevice, stream),
+                              cudaMemcpyDeviceToDevice, cur_),
               "level cache grow");
-      check(cudaStreamSynchronize(stream), "level cache grow");
+      check(cudaStreamSynchronize(cur_), "level cache grow");
       lev_.release();
       lev_ = nb;
       nb.p = nullptr;
@@ -134,11 +138,11 @@ void Engine::ensure_levels(int L) {
     lev_cap_ = cap;
   }
   if (lev_filled_ < 0)
-    check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), stream), "memset");
+    check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), cur_), "memset");
   const int64_t s_begin = lev_filled_ < 0 ? 1 : ((int64_t)2 << lev_filled_);
   const int64_t s_end = (int64_t)2 << L;
   check(launch_level_fill(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, lev_.as<double>(), lev_cap_,
-                          -1, bd_bits_.as<unsigned long long>(), stream),
+                          -1, bd_bits_.as<unsigned long long>(), cur_),
         "level fill");
   last_launches += 2;
   lev_filled_ = L;
@@ -170,29 +174,28 @@ void Engine::compute_frame() {
   }
   frame_.xperp_max = xp;
   frame_.z_max = zm;
+  frame_.theta_max = mixed_theta_max(P.gamma);
 }
 
-void Engine::ensure_mixed(int L, int layout) {
-  ensure_levels(L);
+void Engine::ensure_mixed(int L) {
   if (mrec_version_ != knots_version_) {
     compute_frame();
     mrec_version_ = knots_version_;
     mrec_filled_ = -1;
   }
-  if (layout != mrec_layout_) {
-    mrec_layout_ = layout;
-    mrec_filled_ = -1;
-  }
   if (L <= mrec_filled_) return;
-  if (mrec_cap_ < lev_cap_) {
+  const int64_t need = (int64_t)2 << L;
+  if (need > mrec_cap_) {  // grows by refilling from sample 0 (one spline evaluation per sample)
+    const int64_t cap = std::max<int64_t>(need, (int64_t)2 << 14);
     mrec_.release();
-    mrec_.reserve(sizeof(float4) * 3 * lev_cap_);
-    mrec_cap_ = lev_cap_;
+    mrec_.reserve((size_t)kMixedRecordBytesPerSample * cap);
+    mrec_cap_ = cap;
     mrec_filled_ = -1;
   }
-  const int64_t s_begin = mrec_filled_ < 0 ? 1 : ((int64_t)2 << mrec_filled_);
-  const int64_t s_end = (int64_t)2 << L;
-  check(launch_mixed_records(lev_.as<double>(), lev_cap_, s_begin, s_end, frame_, mrec_.as<float4>(), layout, stream),
+  const int64_t s_begin = mrec_filled_ < 0 ? 0 : ((int64_t)2 << mrec_filled_);
+  const int64_t s_end = need;
+  check(launch_mixed_records(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, frame_, mrec_.as<float4>(),
+                             cur_),
         "mixed records");
   ++last_launches;
   mrec_filled_ = L;
@@ -238,6 +241,9 @@ void polarization_vector(const osc_rad_opts& o, double P[6], bool& project) {
 // host round trip; entries still unconverged after it make the host extend the cache.
 constexpr int kPrefillLevel = 14;
 constexpr int kMinSpan = 32;
+// Mixed waves: spans of at least one staged chunk's worth of pairs, so that a unit's fixed costs (its
+// first copy, the partial store, the tile counter) stay small beside its arithmetic.
+constexpr int kMinSpanMixed = 128;
 
 int Engine::wave_grid(int kind, int variant) {
   if (wave_grid_[kind][variant] == 0) {
@@ -307,15 +313,21 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   if (mixed && rq.power_density)
     throw Error{OSC_ERR_INVALID, "compute='mixed' applies to flux and spectrum; power density runs in FP64"};
   const int Lfirst = std::min(9, lstop);
-  const int Lpre = std::min(lstop, std::max(Lfirst, kPrefillLevel));
   const int kind = rq.power_density ? 1 : (mixed ? 2 : 0);
+  // Levels enqueued without a host round trip: up to kPrefillLevel, or, for a request shape seen
+  // before, up to the highest level its previous call needed (waves past it would find no entries;
+  // levels beyond are still added by the host loop below when entries remain).
+  const auto hist_key = std::make_tuple(kind, n_items, (int64_t)rq.omega.size(), lstop, o.precision);
+  const auto hist = prefill_hist_.find(hist_key);
+  const int Lpre_want = hist != prefill_hist_.end() ? hist->second : kPrefillLevel;
+  const int Lpre = std::min(lstop, std::max(Lfirst, Lpre_want));
   const int variant = tuning_ ? current_variant_[kind]
                               : pick_variant(kind, const_cast<RadRequest&>(rq), n_items, Lfirst, lstop, d_out, d_lvl, st);
-  const int layout = mixed ? mixed_variant_layout(variant) : 0;
-  if (mixed) ensure_mixed(Lpre, layout);
+  if (mixed) ensure_mixed(Lpre);
   else ensure_levels(Lpre);
   const int resident = wave_grid(kind, variant);  // CTAs resident at once on the device
   const int tile = mixed ? mixed_entries_per_cta(variant) : 128;
+  const int min_span = mixed ? kMinSpanMixed : kMinSpan;
   const int64_t target = 4 * (int64_t)resident;   // >= 4 waves of equal units per launch
   const int64_t N = n_items;
   // Partial-sum buffer: a wave has tiles x spans units with spans the smallest power of two reaching
@@ -329,10 +341,10 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   // which reaches the target (> resident) once t x (largest span count of the level) does.
   auto grid_for = [&](int L) -> int {
     if (L == Lfirst) {
-      const WavePlan pl = wave_plan(1, L, N, tile, target, kMinSpan);
+      const WavePlan pl = wave_plan(1, L, N, tile, target, min_span);
       return (int)std::min<int64_t>(pl.tiles * pl.spans, resident);
     }
-    const int64_t span_max = wave_spans(L, 1, INT64_MAX, kMinSpan);
+    const int64_t span_max = wave_spans(L, 1, INT64_MAX, min_span);
     return (int)std::min<int64_t>(ntiles * span_max, resident);
   };
   part_.reserve(sizeof(double) * part_doubles);
@@ -344,6 +356,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   // [0] not converged, [1] samples, [2] unit counter of the running wave
   unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);
   check(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), st), "memset");
+  unsigned* level_max = cnt + 12;  // highest level at which an entry finished
+  check(cudaMemsetAsync(level_max, 0, sizeof(unsigned), st), "memset");
   check(cudaMemsetAsync(c64, 0, 3 * sizeof(unsigned long long), st), "memset");
   // Flux / spectrum waves finalize their own tiles (one launch per level).  Wave w reads its active
   // count from fz3[w % 3], appends survivors to fz3[(w + 1) % 3] and zeroes fz3[(w + 2) % 3] for the
@@ -393,7 +407,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
       w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
-      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
+      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + 2; w.work = fw + wv % 2;
       w.fused = 1;
       w.tile_done = fz3 + 16;
@@ -401,14 +415,14 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.zero_u64 = fw + (wv + 1) % 2;
       FdFinalArgs& f = w.fin;
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
-      f.project = project; f.tile_entries = tile; f.min_span = kMinSpan; f.target_units = target;
+      f.project = project; f.tile_entries = tile; f.min_span = min_span; f.target_units = target;
       f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
       f.precision = o.precision; f.c0 = c0; f.c2 = c2; f.weight = weight;
       for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
-      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = nullptr;
-      f.dmax_spans_joined = mixed && mixed_variant_is_split(variant);
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.level_max = level_max; f.work_reset = nullptr;
+      f.dmax_spans_joined = mixed;
       auto ev = timed_begin(st);
       const int g = grid_for(L);
       if (mixed) check(launch_fd_wave_mixed(w, frame_, g, variant, st), "flux wave (mixed)");
@@ -423,7 +437,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
       w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
-      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
+      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
       auto ev = timed_begin(st);
       const int g = grid_for(L);
@@ -432,32 +446,32 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       timed_end(ev, st);
       FdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
-      f.project = project; f.tile_entries = tile; f.min_span = kMinSpan; f.target_units = target;
+      f.project = project; f.tile_entries = tile; f.min_span = min_span; f.target_units = target;
       f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
       f.precision = o.precision; f.c0 = c0; f.c2 = c2; f.weight = weight;
       for (int i = 0; i < 6; ++i) f.pol[i] = pol[i];
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
-      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = c64 + 2;
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.level_max = level_max; f.work_reset = c64 + 2;
       check(launch_fd_finalize(f, N, st), "flux finalize");
     } else {
       PdWaveArgs w{};
       w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
-      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = kMinSpan; w.target_units = target;
+      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
       auto ev = timed_begin(st);
       check(launch_pd_wave_fp64(w, grid_for(L), st), "power density wave");
       timed_end(ev, st);
       PdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
-      f.directional = rq.directional; f.tile_entries = tile; f.min_span = kMinSpan; f.target_units = target;
+      f.directional = rq.directional; f.tile_entries = tile; f.min_span = min_span; f.target_units = target;
       f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
       f.precision = o.precision; f.scale = scale; f.weight = weight; f.two_over_gamma = 2. / P.gamma;
       f.bdmax_levels = reinterpret_cast<const double*>(bd_bits_.p);
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
-      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.work_reset = c64 + 2;
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.level_max = level_max; f.work_reset = c64 + 2;
       check(launch_pd_finalize(f, N, st), "power density finalize");
     }
     last_launches += 2;
@@ -465,12 +479,16 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   };
   for (int L = Lfirst; L <= Lpre; ++L) launch_wave(L);
   for (int L = Lpre + 1; L <= lstop; ++L) {  // beyond the prefilled levels the host decides
-    unsigned nn = 0;
+    unsigned nn = 0, lmax = 0;
     const unsigned* active = fused ? fz3 + (L - Lfirst) % 3 : cnt + cur_list;
     check(cudaMemcpyAsync(&nn, active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
+    check(cudaMemcpyAsync(&lmax, level_max, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
     check(cudaStreamSynchronize(st), "count");
-    if (nn == 0) break;
-    if (mixed) ensure_mixed(L, layout);
+    if (nn == 0) {
+      if (!tuning_) prefill_hist_[hist_key] = std::max<int>(Lfirst, (int)lmax);
+      break;
+    }
+    if (mixed) ensure_mixed(L);
     else ensure_levels(L);
     launch_wave(L);
   }
@@ -500,14 +518,27 @@ void Engine::collect() {
     check(cudaMemset(cnt_.as<unsigned>() + 2, 0, sizeof(unsigned)), "error word");
     if (err & 1u) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
     if (err & 8u) throw Error{OSC_ERR_STATE, "a sample-sum kernel variant was planned with another tile size"};
-    throw Error{OSC_ERR_INVALID, "compute='mixed' needs observers near the beam axis (angle < 1e-2 and a correction "
-                                 "phase below 3e4 rad); use compute='fp64' for this geometry"};
+    throw Error{OSC_ERR_INVALID, kMixedGeometryMessage};
   }
+}
+
+// Make `s` the stream of the work that follows.  The caches (trajectory, level samples, records) and
+// the request scratch are shared by all requests of the context, so when the stream changes, `s`
+// first waits for everything enqueued on the previous one.
+void Engine::use_stream(cudaStream_t s) {
+  if (last_stream_valid_ && last_stream_ != s) {
+    check(cudaEventRecord(order_ev_, last_stream_), "event");
+    check(cudaStreamWaitEvent(s, order_ev_, 0), "stream wait");
+  }
+  last_stream_ = s;
+  last_stream_valid_ = true;
+  cur_ = s;
 }
 
 void Engine::radiation(RadRequest& rq) {
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
+  use_stream(rq.stream ? rq.stream : stream);
   // statistics describe the latest request: drop those of earlier ones without waiting for them
   // (their ring slots may be rewritten; copies into a slot stay in stream order)
   pending_.clear();

@@ -134,6 +134,8 @@ class Engine {
   int wave_grid_[4][16] = {};
   int wave_grid(int kind, int variant);
   std::map<std::tuple<int, int, int, int>, int> tuned_;   // (kind, log2 entries, first level, last level) -> variant
+  // (kind, entries, energies, last level, precision) -> highest level the last such request needed
+  std::map<std::tuple<int, int64_t, int64_t, int, double>, int> prefill_hist_;
   int current_variant_[4] = {2, 0, 3, 3};
   int pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out, int32_t* d_lvl,
                    cudaStream_t st);
@@ -142,14 +144,13 @@ class Engine {
   DevBuf obs_, nrm_, omega_, out_, lvl_, state_, part_, act_[2], cnt_;
   DevBuf fused_;                   // fused waves: rotating counts, unit counters, per-tile counters
   DevBuf acc_, acc_comp_;          // multi-particle compensated accumulation
-  // mixed-precision records (3 x float4 per sample, same indexing as the level cache)
+  // mixed-precision pair records (kMixedRecordBytesPerSample per sample, level-cache indexing)
   DevBuf mrec_;
   int64_t mrec_cap_ = 0;
   int mrec_filled_ = -1;
-  int mrec_layout_ = 0;
   uint64_t mrec_version_ = ~0ull;
   MixedFrame frame_{};
-  void ensure_mixed(int L, int layout);  // layout: mixed_variant_layout of the kernel variant
+  void ensure_mixed(int L);
   void compute_frame();
  public:
   int forced_variant[4] = {-1, -1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
@@ -171,6 +172,13 @@ class Engine {
   void radiation_beam_mixed(RadRequest& rq, int64_t N);
   double* rk4_adjoint(const double* d_kb, int param_field, int64_t n_params, cudaStream_t st);
 
+  // stream of the running request (caches and scratch are written on it), and the ordering of
+  // requests that arrive on different streams
+  cudaStream_t cur_ = nullptr;
+  cudaStream_t last_stream_ = nullptr;
+  bool last_stream_valid_ = false;
+  cudaEvent_t order_ev_ = nullptr;
+  void use_stream(cudaStream_t s);
   void upload_trajectory();
   void ensure_levels(int L);
   void run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,

@@ -57,19 +57,44 @@ __device__ __forceinline__ double level_time(double tstart, double tstop, int64_
 }
 
 // ---------------------------------------------------------------------------------------------
-// Mixed-precision per-sample term.  A sample is stored as 3 x float4 = 48 bytes in the particle
-// frame (origin X0, third axis along the initial velocity):
-//   r0 = (x, y, z, tau_s = t - t0/c - z/c)   r1 = (bx, by, 1-bz, 1-b^2)   r2 = (ax, ay, az, 0)
-// With R = O - X, rho^2 = Rx^2 + Ry^2 and D = Rz + corr, corr = rho^2/(Rz + D) (series for
-// |rho/D| < 1e-2), the retarded phase is -(w tau_s + (w/c) corr) up to the constant w Oz/c, and the
-// amplitude (src/OSCARSSR.cc:4219) with u = n - b, om = 1 - n.b is
-//   u (1/(D om^2)) ((1-b^2)/D + n.a) - a / (D om).
-// Adds the term times exp(i phase) to s[6] (x re, x im, y re, y im, z re, z im); returns the phase.
+// Mixed-precision sample term over pair records.
+//
+// Frame: origin X0 (the particle start), third axis e3 along the initial velocity, so observers
+// downstream sit near the axis.  With R = O - X = (Rx, Ry, Rz) in that frame, rho^2 = Rx^2 + Ry^2,
+//     D = |R| = Rz + corr,   corr = rho^2 / (Rz + D)                      (no cancellation)
+//     w (t + D/c) = w tau_s + (w/c) corr + w Oz/c,   tau_s = t - t0/c - z/c
+// The last term is a constant phase per (observer, energy) entry: it multiplies the whole sum by a
+// unit complex number and drops out of |E|^2, of the polarization projection and of the phase steps
+// of the stop rule, so it is not computed.
+//
+// Phase, FP64.  corr is first formed in FP32 (relative error ~1e-7 -- a few 1e-3 rad when (w/c) corr
+// reaches 1e4 rad, too much for a 1e-4 flux tolerance).  One Newton step on f(c) = c (c + 2 Rz) -
+// rho^2, whose root is D - Rz, refines it in FP64 from the FP64 sample position:
+//     c1 = c - f(c) / f'(c),   f'(c) = 2 (c + Rz) = 2 D,
+// with 1/(2D) taken from the FP32 rsqrt (its 1e-7 error multiplies a correction that is itself 1e-7
+// of c), so c1 is exact to ~1e-14 relative.  P = w tau_s + (w/c) c1 is then formed and reduced to
+// [-pi, pi] in FP64: k = rint(P / 2pi) by adding 1.5 * 2^52, then P - k 2pi.  Only the reduced
+// phase goes to FP32, for sin / cos.
+//
+// Amplitude, FP32 (src/OSCARSSR.cc:4219), with u = n - b, om = 1 - n.b and |n| = 1:
+//     (1-b^2) u / (D^2 om^2) + n x (u x a) / (D om^2)
+//   = u (1/(D om^2)) ((1-b^2)/D + n.a) - a / (D om)        [n x (u x a) = u (n.a) - a (n.u), n.u = om]
+// with the small differences formed without cancellation from per-sample FP64-exact inputs:
+//     1 - n_z = corr / D,  u_z = (1 - b_z) - (1 - n_z),  om = (1-b_z) + (1-n_z) b_z - n_x b_x - n_y b_y.
+// The FP32 phase P32 = w tau_s + (w/c) corr of the same operands gives the phase steps of the stop
+// rule (|P_j - P_{j-1}| < pi), where its ~1e-3 rad rounding is immaterial.
+//
+// Pair records: samples 2p and 2p + 1 share 40 floats (160 bytes).  Floats 0..23 hold the FP32
+// components, component c of sample 2p + b at float 4 (c / 2) + 2 (c % 2) + b, with
+//   x, y, z, tau_s | -bx, -by, 1-bz, bz | 1-b^2, az, ax, ay
+// so that every half of a loaded float4 is one component of both samples (the operand of one packed
+// f32x2 instruction); bytes 96..159 hold the FP64 x, y, z, tau_s as double2 pairs (x0 x1 | y0 y1 |
+// z0 z1 | t0 t1).  Sample 0, the unused slot of the level ladder, holds a zero-amplitude record at
+// the position and time of sample 1 (no contribution, no phase step), so every span is a whole
+// number of pairs.
 // ---------------------------------------------------------------------------------------------
-// Hardware approximations (MUFU) with denormals flushed: the mixed-precision terms never see
-// denormal operands (distances ~1..100 m, 1 - n.b ~ 1e-9..1e-6, reduced phases in [-pi, pi]), so
-// the flush-to-zero forms give the same values as rsqrtf / __fdividef(1, x) / __sincosf on every
-// input they receive, without the extra instructions that handle denormal inputs.
+// Hardware approximations (MUFU) with denormals flushed: the terms never see denormal operands
+// (distances ~1..100 m, 1 - n.b ~ 1e-9..1e-4, reduced phases in [-pi, pi]).
 __device__ __forceinline__ float rsqrt_ftz(float x) {
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -85,58 +110,175 @@ __device__ __forceinline__ void sincos_ftz(float x, float* s, float* c) {
   asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*c) : "f"(x));
 }
 
-constexpr float kTwoPiHiF = 6.28318548202514648f;     // RN_f(2 pi)
-constexpr float kTwoPiLoF = -1.7484556e-07f;         // RN_f(2 pi - kTwoPiHiF)
-constexpr float kInvTwoPiF = 0.159154943f;
+constexpr int kPairFloats = 40;                        // floats per pair record (160 bytes)
+constexpr int kPairF4 = kPairFloats / 4;               // float4 per pair record
+constexpr double kTwoPiHiD = 6.283185307179586;        // RN(2 pi)
+constexpr double kInvTwoPiD = 0.15915494309189535;     // RN(1 / (2 pi))
+constexpr double kRoundD = 6755399441055744.0;         // 1.5 * 2^52: t + kRoundD rounds t to an integer
 
-__device__ __forceinline__ float mixed_sample(const float4 r0, const float4 r1, const float4 r2, float Ox, float Oy,
-                                              float Oz, float w, float wc, float* s) {
-  const float rx = Ox - r0.x, ry = Oy - r0.y, rz = Oz - r0.z;
-  const float rho2 = fmaf(rx, rx, ry * ry);
-  const float d2 = fmaf(rz, rz, rho2);
-  const float iD = rsqrt_ftz(d2);
-  const float q = rho2 * iD * iD;                                  // (rho/D)^2
-  const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);           // rho^2/(Rz+D), |rho/D| < 1e-2
-  const float ph = -fmaf(wc, corr, w * r0.w);                      // exp(-i w (t + D/c))
-  const float k = rintf(ph * kInvTwoPiF);
-  const float rr = fmaf(-k, kTwoPiLoF, fmaf(-k, kTwoPiHiF, ph));  // Cody-Waite reduction to [-pi, pi]
-  float sn, cs;
-  sincos_ftz(rr, &sn, &cs);
-  const float nx = rx * iD, ny = ry * iD;
-  const float en = corr * iD;                                      // 1 - n_z
-  const float ux = nx - r1.x, uy = ny - r1.y, uz = r1.z - en;
-  const float om = fmaf(-nx, r1.x, fmaf(-ny, r1.y, fmaf(-en, r1.z, en + r1.z)));
-  const float io = rcp_ftz(om);
-  const float na = fmaf(nx, r2.x, fmaf(ny, r2.y, (1.f - en) * r2.z));
-  const float k1 = io * io * iD * fmaf(r1.w, iD, na);
-  const float k2 = io * iD;
-  const float ex = fmaf(k1, ux, -k2 * r2.x);
-  const float ey = fmaf(k1, uy, -k2 * r2.y);
-  const float ez = fmaf(k1, uz, -k2 * r2.z);
-  s[0] = fmaf(ex, cs, s[0]); s[1] = fmaf(ex, sn, s[1]);
-  s[2] = fmaf(ey, cs, s[2]); s[3] = fmaf(ey, sn, s[3]);
-  s[4] = fmaf(ez, cs, s[4]); s[5] = fmaf(ez, sn, s[5]);
-  return ph;
+// Record of one level sample (FP64 values in the particle frame) at sample index s of pair record
+// storage `rec` (s even-aligned with the level ladder).  zero_amplitude writes the record of sample 0
+// (the position and time of sample 1 must be passed for it).
+__device__ __forceinline__ void write_pair_record(float* __restrict__ rec, int64_t s, bool zero_amplitude, double x,
+                                                  double y, double z, double taus, double px, double py, double pz,
+                                                  double qx, double qy, double qz) {
+  const double g2 = 1.0 - (px * px + py * py + pz * pz);       // 1 - b^2, ~1/gamma^2
+  const double ebz = (g2 + px * px + py * py) / (1.0 + pz);     // 1 - b_z without cancellation
+  float v[12] = {(float)x, (float)y, (float)z, (float)taus, (float)-px, (float)-py,
+                 (float)ebz, (float)pz, (float)g2, (float)qz, (float)qx, (float)qy};
+  if (zero_amplitude) {
+    v[4] = v[5] = 0.f;
+    v[6] = 1.f;
+    v[7] = v[8] = v[9] = v[10] = v[11] = 0.f;
+  }
+  float* base = rec + kPairFloats * (s >> 1) + (s & 1);
+#pragma unroll
+  for (int c = 0; c < 12; ++c) base[4 * (c >> 1) + 2 * (c & 1)] = v[c];
+  double* d = reinterpret_cast<double*>(rec + kPairFloats * (s >> 1)) + 12 + (s & 1);
+  d[0] = x;
+  d[2] = y;
+  d[4] = z;
+  d[6] = taus;
 }
 
-// The phase alone, with the operations of mixed_sample (same value).
-__device__ __forceinline__ float mixed_phase(const float4 r0, float Ox, float Oy, float Oz, float w, float wc) {
-  const float rx = Ox - r0.x, ry = Oy - r0.y, rz = Oz - r0.z;
-  const float rho2 = fmaf(rx, rx, ry * ry);
-  const float d2 = fmaf(rz, rz, rho2);
-  const float iD = rsqrt_ftz(d2);
-  const float q = rho2 * iD * iD;
-  const float corr = rho2 * iD * fmaf(0.125f, q, 0.5f);
-  return -fmaf(wc, corr, w * r0.w);
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// Per-entry constants: observer in the particle frame, w and w/c, in FP32 (both lanes equal) and FP64.
+struct PairObs {
+  float2 ox, oy, oz, w, wc;
+  double dox, doy, doz, dw, dwc;
+};
+
+__device__ __forceinline__ PairObs make_pair_obs(double fx, double fy, double fz, double om) {
+  PairObs o;
+  o.ox = f2((float)fx);
+  o.oy = f2((float)fy);
+  o.oz = f2((float)fz);
+  o.w = f2((float)om);
+  o.wc = f2((float)(om / kCLight));
+  o.dox = fx;
+  o.doy = fy;
+  o.doz = fz;
+  o.dw = om;
+  o.dwc = om / kCLight;
+  return o;
 }
 
-// Validity of the near-axis phase form for an observer at (fx, fy, fz) in the particle frame: small
-// angle from the frame axis and a bounded correction phase; otherwise the FP64 path must be used.
-__device__ __forceinline__ bool mixed_geometry_ok(double fx, double fy, double fz, double om, double xperp_max,
-                                                  double z_max) {
-  const double rho = sqrt(fx * fx + fy * fy) + xperp_max;
-  const double rz = fz - z_max;
-  return rz > 0 && rho < 1e-2 * rz && (om / kCLight) * rho * rho / (2 * rz) < 3e4;
+// FP32 phase P32 of one sample with the per-lane operations of pair_sample (same value): the
+// quantity whose steps the stop rule bounds.
+__device__ __forceinline__ float pair_phase(float x, float y, float z, float tau, const PairObs& o) {
+  const float rx = fmaf(x, -1.f, o.ox.x), ry = fmaf(y, -1.f, o.oy.x), rz = fmaf(z, -1.f, o.oz.x);
+  const float rho2 = fmaf(rx, rx, __fmul_rn(ry, ry));
+  const float d2 = fmaf(rz, rz, rho2);
+  const float iD = rsqrt_ftz(d2);
+  const float ri = __fmul_rn(rho2, iD);
+  const float q = __fmul_rn(ri, iD);
+  const float corr = __fmul_rn(ri, fmaf(0.125f, q, 0.5f));
+  return fmaf(o.wc.x, corr, __fmul_rn(o.w.x, tau));
+}
+
+// P32 of sample b (0 or 1) of the pair record at `q` (shared or global memory).
+__device__ __forceinline__ float pair_phase_at(const float* q, int b, const PairObs& o) {
+  return pair_phase(q[b], q[2 + b], q[4 + b], q[6 + b], o);
+}
+
+// Exact float -> double of a non-negative normal float by assembling the bits on the integer pipe
+// (the F2F conversion instructions share the slow XU pipe with sin, cos, rsqrt and rcp); +0 and
+// denormals come out as ~6e-39 instead of their value, which no caller tells apart from 0.
+__device__ __forceinline__ double nonneg_float_to_double(float x) {
+  const unsigned u = __float_as_uint(x);
+  return __hiloint2double((int)((u >> 3) + 0x38000000u), (int)(u << 29));
+}
+
+constexpr double kFourPiD = 12.566370614359172;   // RN(4 pi)
+constexpr float kFourPiF = 12.566370964050293f;   // RN_f(4 pi)
+
+// A reduced phase plus 4 pi, v in [3 pi, 5 pi] (inside [8, 16), one binade), to FP32 on the integer
+// pipe: the float of the same binade takes the top 23 fraction bits of v (truncation, < 1e-6 rad),
+// and subtracting 4 pi in FP32 is exact (Sterbenz).  The offset between kFourPiD and kFourPiF is a
+// constant phase shared by every sample, so it drops out of |E|^2.
+__device__ __forceinline__ float reduced_phase_to_float(double v) {
+  const unsigned lo = (unsigned)__double2loint(v), hi = (unsigned)__double2hiint(v);
+  const unsigned m = __funnelshift_l(lo, hi, 3) & 0x007FFFFFu;
+  return __uint_as_float(m | 0x41000000u) - kFourPiF;
+}
+
+// FP64 retarded phase of one sample, reduced to [-pi, pi] (see the section comment): corr_f and
+// half_iD = 1 / (2 D) are the sample's FP32 values.  The phase is carried as P + 4 pi so that its
+// reduction lands in one binade; 2 - rint((P + 4 pi) / 2pi) multiples of 2pi are removed with the
+// leading double of 2pi only (the trailing part would move the result by < 2e-12 rad).
+__device__ __forceinline__ float fp64_phase(double x, double y, double z, double tau, float corr_f, float half_iD,
+                                            const PairObs& o) {
+  const double Rx = o.dox - x, Ry = o.doy - y, Rz = o.doz - z;
+  const double r2 = fma(Rx, Rx, Ry * Ry);
+  const double c = nonneg_float_to_double(corr_f);
+  const double f = fma(c, fma(2.0, Rz, c), -r2);
+  const double c1 = fma(-f, nonneg_float_to_double(half_iD), c);
+  const double P4 = fma(o.dwc, c1, fma(o.dw, tau, kFourPiD));
+  const double nk = (kRoundD + 2.0) - fma(P4, kInvTwoPiD, kRoundD);
+  return reduced_phase_to_float(fma(nk, kTwoPiHiD, P4));
+}
+
+// Both samples of one pair record `q` for one entry: adds e (cos P, sin P) per lane to acc (x re,
+// x im, y re, y im, z re, z im; the imaginary parts with the sign of +sin P) and returns P32 of both
+// samples.  The sum uses exp(-i P): the caller negates the imaginary parts when it folds acc.
+__device__ __forceinline__ float2 pair_sample(const float4* __restrict__ q, const PairObs& o, float2* acc) {
+  const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5];
+  const double2* dq = reinterpret_cast<const double2*>(q + 6);
+  const double2 DX = dq[0], DY = dq[1], DZ = dq[2], DT = dq[3];
+  const float2 X = make_float2(q0.x, q0.y), Y = make_float2(q0.z, q0.w);
+  const float2 Z = make_float2(q1.x, q1.y), T = make_float2(q1.z, q1.w);
+  const float2 NBX = make_float2(q2.x, q2.y), NBY = make_float2(q2.z, q2.w);
+  const float2 EB = make_float2(q3.x, q3.y), BZ = make_float2(q3.z, q3.w);
+  const float2 G = make_float2(q4.x, q4.y), AZ = make_float2(q4.z, q4.w);
+  const float2 AX = make_float2(q5.x, q5.y), AY = make_float2(q5.z, q5.w);
+  const float2 M1 = f2(-1.f);
+  const float2 rx = fma2(X, M1, o.ox), ry = fma2(Y, M1, o.oy), rz = fma2(Z, M1, o.oz);
+  const float2 rho2 = fma2(rx, rx, mul2(ry, ry));
+  const float2 d2 = fma2(rz, rz, rho2);
+  const float2 iD = make_float2(rsqrt_ftz(d2.x), rsqrt_ftz(d2.y));
+  const float2 ri = mul2(rho2, iD);
+  const float2 qq = mul2(ri, iD);
+  const float2 corr = mul2(ri, fma2(f2(0.125f), qq, f2(0.5f)));
+  const float2 P = fma2(o.wc, corr, mul2(o.w, T));
+  const float2 hD = mul2(iD, f2(0.5f));
+  const float rr0 = fp64_phase(DX.x, DY.x, DZ.x, DT.x, corr.x, hD.x, o);
+  const float rr1 = fp64_phase(DX.y, DY.y, DZ.y, DT.y, corr.y, hD.y, o);
+  float2 sn, cs;
+  sincos_ftz(rr0, &sn.x, &cs.x);
+  sincos_ftz(rr1, &sn.y, &cs.y);
+  const float2 nx = mul2(rx, iD), ny = mul2(ry, iD), en = mul2(corr, iD);  // en = 1 - nz
+  const float2 ux = add2(nx, NBX), uy = add2(ny, NBY), uz = fma2(en, M1, EB);
+  const float2 om = fma2(ny, NBY, fma2(nx, NBX, fma2(en, BZ, EB)));
+  // e = k2 (h u - a) with k2 = 1/(D om), h = ((1-b^2)/D + n.a)/om, formed from -1/om:
+  // v = a + (-h) u = -(h u - a), e = (-k2) v.
+  const float2 nio = make_float2(rcp_ftz(-om.x), rcp_ftz(-om.y));
+  const float2 na = fma2(nx, AX, fma2(ny, AY, mul2(fma2(en, M1, f2(1.f)), AZ)));
+  const float2 nh = mul2(nio, fma2(G, iD, na));
+  const float2 vx = fma2(nh, ux, AX), vy = fma2(nh, uy, AY), vz = fma2(nh, uz, AZ);
+  const float2 nk2 = mul2(nio, iD);
+  const float2 kc = mul2(nk2, cs), ks = mul2(nk2, sn);
+  acc[0] = fma2(vx, kc, acc[0]);
+  acc[1] = fma2(vx, ks, acc[1]);
+  acc[2] = fma2(vy, kc, acc[2]);
+  acc[3] = fma2(vy, ks, acc[3]);
+  acc[4] = fma2(vz, kc, acc[4]);
+  acc[5] = fma2(vz, ks, acc[5]);
+  return P;
+}
+
+// Validity of the mixed path for an observer at (fx, fy, fz) in the particle frame: within
+// F.theta_max of the frame axis (trajectory extent included), downstream of the trajectory, and a
+// correction phase (w/c) rho^2 / (2 Rz) of at most 3e4 rad.  theta_max = min(1e-2, 20 / gamma)
+// (mixed_theta_max): beyond ~20 / gamma the flux is a deep cancellation of nearly equal terms
+// (|sum| << sum |terms|) that FP32 amplitudes do not resolve to 1e-4.
+__device__ __forceinline__ bool mixed_geometry_ok(double fx, double fy, double fz, double om, const MixedFrame& F) {
+  const double rho = sqrt(fx * fx + fy * fy) + F.xperp_max;
+  const double rz = fz - F.z_max;
+  return rz > 0 && rho < F.theta_max * rz && (om / kCLight) * rho * rho / (2 * rz) < 3e4;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -179,9 +321,11 @@ __device__ __forceinline__ double group_max(double v) {
 // ---------------------------------------------------------------------------------------------
 // Warp-aggregated bookkeeping: one atomic per warp for the survivor list and for each statistics
 // counter, instead of one per entry on a single address.
+// `level_max` (may be NULL) records the highest level at which an entry finished.
 __device__ __forceinline__ void finalize_bookkeeping(bool finished, bool unconverged, bool survive, int64_t item,
                                                      int L, int* act_next, unsigned* n_next,
-                                                     unsigned long long* not_converged, unsigned long long* samples) {
+                                                     unsigned long long* not_converged, unsigned long long* samples,
+                                                     unsigned* level_max) {
   const unsigned full = 0xffffffffu;
   const int lane32 = threadIdx.x & 31;
   const unsigned fin = __ballot_sync(full, finished);
@@ -190,6 +334,7 @@ __device__ __forceinline__ void finalize_bookkeeping(bool finished, bool unconve
   if (lane32 == 0) {
     if (fin) atomicAdd(samples, (unsigned long long)__popc(fin) * (unsigned long long)((2ll << L) - 1));
     if (unc) atomicAdd(not_converged, (unsigned long long)__popc(unc));
+    if (fin && level_max) atomicMax(level_max, (unsigned)L);
   }
   unsigned base = 0;
   if (sur && lane32 == __ffs(sur) - 1) base = atomicAdd(n_next, (unsigned)__popc(sur));
@@ -282,7 +427,95 @@ __device__ void fd_tile_finalize(const FdFinalArgs& A, const WavePlan& P, int64_
       fd_entry_decide(A, item, S, last_mag, dmax, finished, unconverged, survive);
     }
     finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged,
-                         A.samples);
+                         A.samples, A.level_max);
+  }
+}
+
+// Fused finalize of one tile by all THREADS threads of the CTA, in G = THREADS / TE groups of TE
+// threads (entry q = threadIdx.x % TE): group g sums the spans g, g + G, ... of its entry in order, the
+// groups' sums are combined in group order through `red` ((G - 1) x 7 x TE doubles) and group 0
+// applies the stop rule.  The span maxima include the step into each span (the mixed kernels).
+template <int THREADS>
+__device__ void fd_tile_finalize_grouped(const FdFinalArgs& A, const WavePlan& P, int64_t tile, int64_t n_act, int TE,
+                                         double* red) {
+  const int G = THREADS / TE;
+  const int grp = (int)threadIdx.x / TE, q = (int)threadIdx.x % TE;
+  const int64_t slot = tile * TE + q;
+  const bool live = slot < n_act;
+  const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+  // sum of segment g over all spans, complete in group 0 (all threads take part: it synchronises)
+  auto seg_sum = [&](int g, C3& s, double& dmax) {
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    double dm = 0;
+    if (live) {
+      for (int sp = grp; sp < P.spans; sp += G) {
+        const double* p = A.part + fused_part_index(P, tile, g, sp, 0, q, TE);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) t[k] += __ldcg(p + k * TE);
+        const double d = __ldcg(p + 8 * TE);
+        if (d >= 0) dm = fmax(dm, d);  // -1: an empty span (they only trail the segment)
+      }
+    }
+    if (G > 1) {
+      if (grp > 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) red[((grp - 1) * 7 + k) * TE + q] = t[k];
+        red[((grp - 1) * 7 + 6) * TE + q] = dm;
+      }
+      __syncthreads();
+      if (grp == 0) {
+        for (int o = 0; o < G - 1; ++o) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) t[k] += red[(o * 7 + k) * TE + q];
+          dm = fmax(dm, red[(o * 7 + 6) * TE + q]);
+        }
+      }
+      __syncthreads();
+    }
+    s.xr += t[0]; s.xi += t[1]; s.yr += t[2]; s.yi += t[3]; s.zr += t[4]; s.zi += t[5];
+    dmax = fmax(dmax, dm);
+  };
+  C3 S = {0, 0, 0, 0, 0, 0};
+  double last_mag = -1, dmax = 0;
+  if (A.first) {
+    double unused = 0;
+    if (P.nseg == 2) {
+      seg_sum(0, S, unused);
+      C3 t = c3_scale(S, A.dt_prev);
+      if (A.project) t = c3_project(t, A.pol);
+      last_mag = c3_mag2(t);
+    }
+    seg_sum(P.nseg - 1, S, dmax);
+  } else {
+    if (live && grp == 0) {
+      const int64_t N = A.n_items;
+      S = {A.state[item], A.state[N + item], A.state[2 * N + item], A.state[3 * N + item], A.state[4 * N + item],
+           A.state[5 * N + item]};
+      last_mag = A.state[6 * N + item];
+    }
+    seg_sum(0, S, dmax);
+  }
+  bool finished = false, unconverged = false, survive = false;
+  if (live && grp == 0) fd_entry_decide(A, item, S, last_mag, dmax, finished, unconverged, survive);
+  finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged,
+                       A.samples, A.level_max);
+}
+
+// End of a unit of a fused wave with the grouped finalize (the mixed kernels): as fused_unit_done.
+template <int THREADS>
+__device__ __forceinline__ void fused_unit_done_grouped(const FdWaveArgs& A, const WavePlan& P, int64_t tile,
+                                                        int64_t n_act, int* s_last, int TE, double* red) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned done = atomicAdd(&A.tile_done[tile], 1u);
+    *s_last = done == (unsigned)(P.spans - 1);
+    if (*s_last) __threadfence();
+  }
+  __syncthreads();
+  if (*s_last) {
+    fd_tile_finalize_grouped<THREADS>(A.fin, P, tile, n_act, TE, red);
+    if (threadIdx.x == 0) A.tile_done[tile] = 0;
   }
 }
 

@@ -81,11 +81,12 @@ struct FdFinalArgs {
   unsigned long long* samples;
   unsigned long long* work_reset;  // the wave's unit counter, zeroed for the next wave
   int dmax_spans_joined;    // the span maxima include the step from the previous span's last sample
+  unsigned* level_max;      // highest level at which an entry finished (may be NULL)
 };
 
 // One wave of the frequency-domain sum over level `level` for the active entries.
 struct FdWaveArgs {
-  const double* lev;        // FP64 level cache (10 arrays of `cap`) or mixed records (3 float4 per sample)
+  const double* lev;        // FP64 level cache (10 arrays of `cap`) or mixed pair records
   int64_t cap;
   const double* obs;        // 3 * n_obs
   const double* omega;      // n_e
@@ -142,28 +143,42 @@ struct PdFinalArgs {
   unsigned long long* not_converged;
   unsigned long long* samples;
   unsigned long long* work_reset;
+  unsigned* level_max;      // highest level at which an entry finished (may be NULL)
 };
 
 // Frame of the mixed-precision path: origin x0 (particle start), rows of rot = e1, e2, e3 with e3 the
-// initial direction; xperp_max / z_max bound the trajectory in that frame; t_ref = t0 / c.
+// initial direction; xperp_max / z_max bound the trajectory in that frame; t_ref = t0 / c;
+// theta_max = the largest observer angle the path accepts (mixed_theta_max of the particle's gamma).
 struct MixedFrame {
   double rot[9];
   double x0[3];
   double t_ref;
   double xperp_max, z_max;
+  double theta_max;
 };
 
-// Mixed records of samples [s_begin, s_end): layout 0 = 3 float4 per sample, 1 = pair records
-// (6 float4 per two samples, see kernels_mixed.cu).
-cudaError_t launch_mixed_records(const double* lev, int64_t cap, int64_t s_begin, int64_t s_end, const MixedFrame& F,
-                                 float4* rec, int layout, cudaStream_t st);
+// Refusal of an observer outside the mixed path's validity region (mixed_geometry_ok).
+constexpr const char* kMixedGeometryMessage =
+    "compute='mixed' needs observers near the beam axis (angle below min(1e-2, 20/gamma) and a correction "
+    "phase below 3e4 rad); use compute='fp64' for this geometry";
+
+// Largest observer angle from the frame axis the mixed path accepts for a particle of Lorentz
+// factor gamma: min(1e-2, 20 / gamma) (see mixed_geometry_ok in fd_common.cuh).
+__host__ __device__ inline double mixed_theta_max(double gamma) {
+  const double t = 20.0 / gamma;
+  return t < 1e-2 ? t : 1e-2;
+}
+
+// Mixed pair records (fd_common.cuh, 160 bytes per two samples) of level samples [s_begin, s_end),
+// evaluated from the trajectory knots (t | y[9] | y''[9], n points).
+cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
+                                 int64_t s_end, const MixedFrame& F, float4* rec, cudaStream_t st);
+constexpr int kMixedRecordBytesPerSample = 80;
 // Compiled kernel variants (see kernels_fp64.cu / kernels_mixed.cu); the engine's autotuner picks one.
 constexpr int kFp64Variants = 4;
-constexpr int kMixedVariants = 13;
+constexpr int kMixedVariants = 4;
 cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int grid, int variant, cudaStream_t st);
 int mixed_entries_per_cta(int variant);
-bool mixed_variant_is_split(int variant);  // sample-split variants: fused finalize only
-int mixed_variant_layout(int variant);     // records layout the variant reads
 const char* mixed_variant_name(int variant);  // kernel and template arguments of a variant
 int mixed_blocks_per_sm(int variant);
 int fp64_blocks_per_sm(bool power_density, int variant);

@@ -301,7 +301,8 @@ __global__ void k_fd_finalize(FdFinalArgs A) {
   }
   bool finished = false, unconverged = false, survive = false;
   if (live && lane == 0) fd_entry_decide(A, item, S, last_mag, dmax, finished, unconverged, survive);
-  finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples);
+  finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples,
+                       A.level_max);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -482,7 +483,8 @@ __global__ void k_pd_finalize(PdFinalArgs A) {
       survive = true;
     }
   }
-  finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples);
+  finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples,
+                       A.level_max);
 }
 
 }  // namespace dev

@@ -140,6 +140,23 @@ def test_beam_mixed_matches_fp64_fixed_level(nparticles):
     assert e <= TOL
 
 
+def test_epu_beam_101x101_64_particles_fixed_level():
+    """The multi-particle EPU configuration on its full 101 x 101 grid (8 mm at 30 m, E1) with a
+    64-particle subset of the beam, device trajectories (mixed) against host RK4 (FP64)."""
+    from oscars_b200.sr import sr
+    setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=42))]
+    kw = dict(energy_eV=E1_EPU, npoints=[101, 101], width=[0.008, 0.008], translation=[0, 0, 30],
+              nparticles=64, precision=0, max_level=12)
+    out = {}
+    for compute in ("fp64", "mixed"):
+        s = sr(gpu=1)
+        run_case(s, setup)
+        out[compute] = np.array([v[1] for v in s.calculate_flux_rectangle(**dict(kw, compute=compute))])
+    e = _err(out["mixed"], out["fp64"])
+    print("beam of 64, 101x101, L=12: mixed vs fp64 %.3e" % e)
+    assert e <= TOL
+
+
 def test_beam_mixed_polarized_and_spectrum():
     from oscars_b200.sr import sr
     setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=2))]

@@ -2,7 +2,11 @@
 
 Tolerance: peak-normalised relative error max_i |F_i - F64_i| / max_i |F64_i| <= 1e-4, at a fixed
 level (precision=0, max_level=L) so that both paths integrate exactly the same samples.  The FP64
-path itself matches the reference to <= 1e-9 (test_gpu_parity.py).
+path itself matches the reference to <= 1e-9 (test_gpu_parity.py).  Each case is normalised by its
+own peak, so small grids away from the axis test the path where the flux is weak, not only near the
+on-axis maximum.  The cases span the region the mixed path accepts (mixed_geometry_ok): observer
+angles up to min(1e-2, 20/gamma), correction phases (w/c) rho^2 / (2 Rz) up to 3e4 rad, harmonics
+up to the 7th, the 2-3 keV end of the 100-3000 eV spectrum off axis; outside it the path refuses.
 """
 import math
 
@@ -91,6 +95,79 @@ def test_adaptive_mode_close_to_fp64():
     assert _err(out[1], out[0]) <= 1e-4
 
 
+HBAR_C_EVM = 1.973269804e-7  # hbar c [eV m]: w / c = E / (hbar c)
+GAMMA_3GEV = 3.0 / 0.51099895e-3
+
+
+def _setup_energy(energy_GeV):
+    und, beam = UND_SETUP[0], dict(UND_SETUP[1][1], energy_GeV=energy_GeV)
+    return [und, ("set_particle_beam", beam)] + UND_SETUP[2:]
+
+
+@pytest.mark.parametrize("theta_gamma", [2, 5])
+def test_small_off_axis_grids_at_e1(theta_gamma):
+    """3 x 3 grids 0.2 mm wide at 20 m, centred theta_gamma / gamma off axis: the flux there is a
+    fraction of the on-axis peak, and the phase correction is 3e3 .. 2e4 rad."""
+    x = theta_gamma / GAMMA_3GEV * 20
+    f64, mx = _pair(UND_SETUP, "calculate_flux_rectangle",
+                    dict(energy_eV=E1_U, npoints=[3, 3], width=[0.0002, 0.0002], translation=[x, 0, 20],
+                         precision=0, max_level=13))
+    e = _err(mx, f64)
+    print("off-axis grid theta*gamma=%d: mixed vs fp64 %.3e" % (theta_gamma, e))
+    assert e <= TOL
+
+
+@pytest.mark.parametrize("harmonic", [3, 5, 7])
+@pytest.mark.parametrize("corr_phase", [1e4, 2.7e4])
+def test_harmonics_up_to_the_correction_phase_limit(harmonic, corr_phase):
+    """15 x 15 grid at 20 m whose corner reaches the given correction phase at the h-th harmonic
+    (the guard accepts up to 3e4 rad; the trajectory ends 1.5 m downstream of the origin)."""
+    E = harmonic * E1_U
+    rho = math.sqrt(corr_phase * 2 * (20 - 1.5) / (E / HBAR_C_EVM))
+    w = 2 * rho / math.sqrt(2)
+    f64, mx = _pair(UND_SETUP, "calculate_flux_rectangle",
+                    dict(energy_eV=E, npoints=[15, 15], width=[w, w], translation=[0, 0, 20], precision=0,
+                         max_level=13))
+    e = _err(mx, f64)
+    print("harmonic %d, corner correction phase %.1e rad (grid %.1f mm): mixed vs fp64 %.3e"
+          % (harmonic, corr_phase, w * 1e3, e))
+    assert e <= TOL
+
+
+@pytest.mark.parametrize("obs", [[0.006, 0.002, 30], [0.0095, 0.0, 30]])
+def test_off_axis_spectrum_2_to_3_keV(obs):
+    """The high-energy end of the 100-3000 eV spectrum at observers 6-10 mm off axis at 30 m
+    (correction phases 1e4 and 2.4e4 rad at 3 keV)."""
+    f64, mx = _pair(UND_SETUP, "calculate_spectrum",
+                    dict(obs=obs, energy_range_eV=[2000, 3000], npoints=201, precision=0, max_level=13))
+    e = _err(mx, f64)
+    print("spectrum 2-3 keV at %s: mixed vs fp64 %.3e" % (obs, e))
+    assert e <= TOL
+
+
+@pytest.mark.parametrize("angle,energy_eV", [(0.5e-2, 12.8), (0.9e-2, 5.0)])
+def test_wide_angles_at_low_beam_energy(angle, energy_eV):
+    """A 0.5 GeV beam (gamma 978): the angle limit is 1e-2 itself.  3 x 3 grids 4 mm wide at 20 m,
+    centred at rho / Rz = 0.5e-2 and 0.9e-2, at energies that keep the correction phase near 2e4 rad."""
+    f64, mx = _pair(_setup_energy(0.5), "calculate_flux_rectangle",
+                    dict(energy_eV=energy_eV, npoints=[3, 3], width=[0.004, 0.004], translation=[angle * 20, 0, 20],
+                         precision=0, max_level=12))
+    e = _err(mx, f64)
+    print("0.5 GeV, rho/Rz = %.1e at %.1f eV: mixed vs fp64 %.3e" % (angle, energy_eV, e))
+    assert e <= TOL
+
+
+def test_angles_beyond_the_limit_are_refused():
+    """30 / gamma at 3 GeV (above 20 / gamma) and 1.2e-2 at 0.5 GeV (above 1e-2) are refused."""
+    cases = [(UND_SETUP, 30 / GAMMA_3GEV * 20, 10.0), (_setup_energy(0.5), 0.012 * 20, 2.0)]
+    for setup, x, E in cases:
+        s = _sr()
+        run_case(s, setup)
+        with pytest.raises(ValueError, match="compute='mixed' needs observers near the beam axis"):
+            s.calculate_flux_rectangle(energy_eV=E, npoints=[1, 1], width=[1e-4, 1e-4], translation=[x, 0, 20],
+                                       compute="mixed")
+
+
 def test_far_off_axis_observer_is_rejected():
     s = _sr()
     run_case(s, UND_SETUP)
@@ -108,10 +185,10 @@ def _variants(kind):
     return n.value
 
 
-@pytest.mark.parametrize("variant", range(13))
+@pytest.mark.parametrize("variant", range(4))
 def test_every_mixed_variant_matches_fp64(variant):
-    """Each compiled mixed kernel (sample records, sample-split, packed pair records) on a flux grid
-    with many spans per entry (level 13, fixed) and on a spectrum past the prefilled levels."""
+    """Each compiled mixed kernel (pair records, 1/2/4 sample groups per CTA) on a flux grid with many
+    spans per entry (level 13, fixed) and on a spectrum past the prefilled levels."""
     if variant >= _variants(2):
         pytest.skip("variant not compiled")
     flux = dict(energy_eV=E1_U, npoints=[41, 41], width=[0.008, 0.008], translation=[0, 0, 30], precision=0,
