@@ -240,6 +240,17 @@ OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fie
                            const osc_rad_opts* opts, int average, double* out,
                            int32_t* level_out, long long* n_not_converged);
 
+/* The jobs' trajectories exactly as the batched mixed path integrates them on the device (its RK4
+ * and spline kernels; no reference counterpart -- it exists to compare the device integration with
+ * the host's, which follows src/OSCARSSR.cc:910-1009 bit for bit).  Per job, in job order, 19 x n
+ * doubles: t [s]; x, y, z [m]; beta_x, beta_y, beta_z; a_x/c, a_y/c, a_z/c [1/s]; then the 9 clamped-
+ * spline second derivatives of those components (include/TOMATH.h:141-203), each a row of n values.
+ * npoints_out[k] = n of job k (npoints or npoints + 1, as the reference's step count gives it); out
+ * must hold 19 x the sum of those (19 x (npoints + 2) per job is always enough).  The jobs' observer
+ * and energy ranges are ignored. */
+OSC_API int osc_batch_trajectories(osc_ctx* ctx, const osc_field_desc* fields, int n_fields, const osc_job_desc* jobs,
+                                   int n_jobs, double* out, long long capacity, long long* npoints_out);
+
 /* ---- differentiation (no reference counterpart: the reference has no gradients) ------------
  * osc_set_half_period_scale replaces the half-period amplitude factors of field `field_index`
  * (an undulator added with them; -1 = the one field that has them) and drops the trajectory.

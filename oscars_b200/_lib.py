@@ -82,6 +82,7 @@ SIGNATURES = {
     "osc_power_density_device": (I, [VP, VP, VP, LL, I, ctypes.POINTER(RadOpts), VP, VP, VP]),
     "osc_batch_flux": (I, [VP, ctypes.POINTER(FieldDesc), I, ctypes.POINTER(JobDesc), I, DP, LL, DP, LL,
                            ctypes.POINTER(RadOpts), I, DP, I32P, LLP]),
+    "osc_batch_trajectories": (I, [VP, ctypes.POINTER(FieldDesc), I, ctypes.POINTER(JobDesc), I, DP, LL, LLP]),
     "osc_set_half_period_scale": (I, [VP, I, DP, LL]),
     "osc_trajectory_vjp": (I, [VP, DP, LL, DP, LL]),
     "osc_flux_vjp": (I, [VP, DP, LL, DP, LL, I, ctypes.POINTER(RadOpts), I, DP, DP, DP, LL, DP]),

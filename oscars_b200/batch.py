@@ -80,13 +80,10 @@ class BatchRunner:
         self.last_levels = None
         self.last_not_converged = 0
 
-    def flux(self, jobs: List[Job], compute: str = "mixed", polarization: str = "all", angle=_ANGLE_UNSET,
-             horizontal_direction=None, propogation_direction=None, precision: float = 0.01, max_level: int = -2,
-             max_level_extended: int = 0, quantity: str = "flux", average: bool = False):
-        """Flux (or spectrum) of every job; a list of (n_obs, n_energies) arrays, or one array with
-        average=True (jobs sharing observers and energies, mean with weight 1/N)."""
-        if not jobs:
-            return []
+    @staticmethod
+    def _descriptors(jobs, average=False):
+        """Field and job descriptors of a batch, the concatenated observers and energies, and the
+        arrays the descriptors point into (to keep alive until the call returns)."""
         fdescs, jdescs, obs_all, e_all = [], [], [], []
         keep = []  # arrays the descriptors point into, alive until the call returns
         n_obs = n_e = 0
@@ -145,6 +142,16 @@ class BatchRunner:
             jdescs.append(jd)
         obs = np.ascontiguousarray(np.concatenate(obs_all))
         en = np.ascontiguousarray(np.concatenate(e_all))
+        return fdescs, jdescs, obs, en, keep
+
+    def flux(self, jobs: List[Job], compute: str = "mixed", polarization: str = "all", angle=_ANGLE_UNSET,
+             horizontal_direction=None, propogation_direction=None, precision: float = 0.01, max_level: int = -2,
+             max_level_extended: int = 0, quantity: str = "flux", average: bool = False):
+        """Flux (or spectrum) of every job; a list of (n_obs, n_energies) arrays, or one array with
+        average=True (jobs sharing observers and energies, mean with weight 1/N)."""
+        if not jobs:
+            return []
+        fdescs, jdescs, obs, en, keep = self._descriptors(jobs, average)
         opts = self._opts(polarization, angle, horizontal_direction, propogation_direction, precision, max_level,
                           max_level_extended, quantity, compute)
         sizes = [jd.n_obs * jd.n_energies for jd in jdescs]
@@ -167,6 +174,28 @@ class BatchRunner:
             levels.append(lvl[k:k + m].reshape(jd.n_obs, jd.n_energies))
             k += m
         self.last_levels = levels
+        return res
+
+    def trajectories(self, jobs: List[Job]):
+        """The jobs' trajectories as the batched mixed path integrates them on the device (RK4 and
+        spline kernels): per job a (19, n) array -- t [s]; x, y, z [m]; beta_x, beta_y, beta_z;
+        a_x/c, a_y/c, a_z/c [1/s]; and the 9 spline second derivatives of those components."""
+        if not jobs:
+            return []
+        fdescs, jdescs, _, _, keep = self._descriptors(jobs)
+        cap = 0
+        for jd in jdescs:  # upper bound of the point count: npoints + 2
+            cap += 19 * (int(jd.npoints) + 2)
+        out = np.zeros(cap)
+        npts = np.zeros(len(jdescs), dtype=np.int64)
+        F = (_lib.FieldDesc * max(1, len(fdescs)))(*fdescs)
+        J = (_lib.JobDesc * len(jdescs))(*jdescs)
+        self.ctx.call("osc_batch_trajectories", F, len(fdescs), J, len(jdescs), _lib.dptr(out), cap,
+                      npts.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+        res, k = [], 0
+        for n in npts:
+            res.append(out[k:k + 19 * n].reshape(19, n).copy())
+            k += 19 * n
         return res
 
     def stats(self):

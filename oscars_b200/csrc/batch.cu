@@ -773,43 +773,20 @@ DevField to_dev_field(FieldSpec f, std::vector<double>& vals) {
   return d;
 }
 
-int Engine::batch_resident(int v) {
-  if (wave_grid_[3][v] == 0) {
-    int sms = 0;
-    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
-    wave_grid_[3][v] = sms * batch_blocks_per_sm(v);
-  }
-  return wave_grid_[3][v];
-}
-
-void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
-                   int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
-                   bool average, double* out, int32_t* level_out, double average_weight) {
-  pending_.clear();
-  last_samples = last_launches = last_not_converged = 0;
-  if (jobs.empty()) return;
-  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
-  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
-  if (lstop > kMaxLevelMemory)
-    throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
-  if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
-  const int Lfirst = std::min(9, lstop);
-  const int Lpre = std::min(lstop, std::max(Lfirst, kBatchPrefill));
-  double pol[6];
-  bool project = false;
-  polarization_vector(o, pol, project);
-
-  // ---- job descriptors, validated like Model::compute_trajectory ----
+// Device descriptors of a batch's jobs, validated like Model::compute_trajectory: frame, RK4 step and
+// point counts, flux constants, polarization vector in the job frame (pol), field and entry ranges
+// (the latter only with_entries).
+static std::vector<DevJob> build_dev_jobs(size_t n_fields, const std::vector<BatchJob>& jobs, int64_t n_obs_total,
+                                          int64_t n_omega_total, bool average, const double* pol, bool with_entries) {
   std::vector<DevJob> dj(jobs.size());
-  const int64_t m_avg = average ? jobs[0].n_obs * jobs[0].n_e : 0;
   for (size_t k = 0; k < jobs.size(); ++k) {
     const BatchJob& S = jobs[k];
     const Particle& P = S.particle;
-    if (S.field_begin < 0 || S.field_count < 0 || (size_t)S.field_begin + S.field_count > fields.size())
+    if (S.field_begin < 0 || S.field_count < 0 || (size_t)S.field_begin + S.field_count > n_fields)
       throw Error{OSC_ERR_RANGE, "job field range outside the field array"};
-    if (S.obs_begin < 0 || S.n_obs < 1 || S.obs_begin + S.n_obs > n_obs_total)
+    if (with_entries && (S.obs_begin < 0 || S.n_obs < 1 || S.obs_begin + S.n_obs > n_obs_total))
       throw Error{OSC_ERR_RANGE, "job observer range outside the observer array"};
-    if (S.omega_begin < 0 || S.n_e < 1 || S.omega_begin + S.n_e > n_omega_total)
+    if (with_entries && (S.omega_begin < 0 || S.n_e < 1 || S.omega_begin + S.n_e > n_omega_total))
       throw Error{OSC_ERR_RANGE, "job energy range outside the energy array"};
     if (S.n_obs * S.n_e > 2147483647ll) throw Error{OSC_ERR_LENGTH, "more than 2^31-1 entries in one job"};
     if (average && (S.obs_begin != jobs[0].obs_begin || S.n_obs != jobs[0].n_obs ||
@@ -859,6 +836,39 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     d.field_count = S.field_count;
     d.obs_begin = S.obs_begin; d.omega_begin = S.omega_begin; d.n_obs = S.n_obs; d.n_e = S.n_e;
   }
+
+  return dj;
+}
+
+int Engine::batch_resident(int v) {
+  if (wave_grid_[3][v] == 0) {
+    int sms = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
+    wave_grid_[3][v] = sms * batch_blocks_per_sm(v);
+  }
+  return wave_grid_[3][v];
+}
+
+void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
+                   int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
+                   bool average, double* out, int32_t* level_out, double average_weight) {
+  pending_.clear();
+  last_samples = last_launches = last_not_converged = 0;
+  if (jobs.empty()) return;
+  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
+  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
+  if (lstop > kMaxLevelMemory)
+    throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
+  if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
+  const int Lfirst = std::min(9, lstop);
+  const int Lpre = std::min(lstop, std::max(Lfirst, kBatchPrefill));
+  double pol[6];
+  bool project = false;
+  polarization_vector(o, pol, project);
+
+  // ---- job descriptors, validated like Model::compute_trajectory ----
+  std::vector<DevJob> dj = build_dev_jobs(fields.size(), jobs, n_obs_total, n_omega_total, average, pol, true);
+  const int64_t m_avg = average ? jobs[0].n_obs * jobs[0].n_e : 0;
 
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
@@ -1095,6 +1105,57 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
     check(cudaMemcpyAsync(out, b_acc_.p, sizeof(double) * m_avg, cudaMemcpyDeviceToHost, st), "download");
     check(cudaStreamSynchronize(st), "download");
   }
+}
+
+// Trajectories of the jobs as the batched path computes them (k_batch_rk4, k_batch_spline, one chunk):
+// per job 19 x n knot values in job order (t | x y z bx by bz ax/c ay/c az/c | their 9 spline second
+// derivatives), npoints[k] = n of job k.  For comparing the device integration with the host's.
+void Engine::batch_trajectories(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, double* out,
+                                int64_t capacity, int64_t* npoints) {
+  const double pol[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<DevJob> dj = build_dev_jobs(fields.size(), jobs, 0, 0, false, pol, false);
+  int64_t knots = 0, work = 0;
+  for (DevJob& d : dj) {
+    const int64_t n = (int64_t)d.nf + d.nb;
+    d.knots = knots;
+    knots += 19 * n;
+    d.u_off = work;
+    work += 9 * n;
+  }
+  if (knots > capacity) throw Error{OSC_ERR_LENGTH, "output capacity below 19 x points summed over the jobs"};
+  if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
+  if (dj.empty()) return;
+  check(cudaSetDevice(device), "cudaSetDevice");
+  use_stream(stream);
+  cudaStream_t st = stream;
+  std::vector<DevField> df;
+  std::vector<double> fvals;
+  for (const FieldSpec& f : fields) df.push_back(to_dev_field(f, fvals));
+  if (df.empty()) df.push_back(DevField{});
+  if (fvals.empty()) fvals.push_back(0.0);
+  const int nj = (int)dj.size();
+  b_fields_.reserve(sizeof(DevField) * df.size());
+  b_fvals_.reserve(sizeof(double) * fvals.size());
+  b_jobs_.reserve(sizeof(DevJob) * nj);
+  b_knots_.reserve(sizeof(double) * knots);
+  b_work_.reserve(sizeof(double) * work);
+  b_cnt_.reserve(64);
+  check(cudaMemcpyAsync(b_fvals_.p, fvals.data(), sizeof(double) * fvals.size(), cudaMemcpyHostToDevice, st), "fields");
+  check(cudaMemcpyAsync(b_fields_.p, df.data(), sizeof(DevField) * df.size(), cudaMemcpyHostToDevice, st), "fields");
+  check(cudaMemcpyAsync(b_jobs_.p, dj.data(), sizeof(DevJob) * nj, cudaMemcpyHostToDevice, st), "jobs");
+  unsigned* err = b_cnt_.as<unsigned>();
+  check(cudaMemsetAsync(err, 0, sizeof(unsigned), st), "memset");
+  dev::k_batch_rk4<<<(2 * nj + 63) / 64, 64, 0, st>>>(b_jobs_.as<DevJob>(), nj, b_fields_.as<DevField>(),
+                                                      b_fvals_.as<double>(), b_knots_.as<double>(), err);
+  dev::k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(b_jobs_.as<DevJob>(), nj, b_knots_.as<double>(),
+                                                         b_work_.as<double>());
+  check(cudaGetLastError(), "batch trajectories");
+  check(cudaMemcpyAsync(out, b_knots_.p, sizeof(double) * knots, cudaMemcpyDeviceToHost, st), "download");
+  unsigned e = 0;
+  check(cudaMemcpyAsync(&e, err, sizeof e, cudaMemcpyDeviceToHost, st), "error word");
+  check(cudaStreamSynchronize(st), "batch trajectories");
+  if (e & dev::kErrSuperluminal) throw Error{OSC_ERR_RANGE, "a trajectory reached the speed of light (check the fields)"};
+  for (int k = 0; k < nj; ++k) npoints[k] = (int64_t)dj[k].nf + dj[k].nb;
 }
 
 // Autotuner of the batched wave: times the first wave of the chunk with every compiled variant

@@ -389,6 +389,54 @@ OSC_API int osc_spectrum(osc_ctx* ctx, const double obs[3], const double* energi
 // A batch of independent jobs (no reference counterpart: the reference runs one particle and one
 // field container per call).  Mixed precision runs all jobs in shared launches; FP64 runs them one
 // after another through the single-trajectory path.
+// Fields of a batch request (FieldSpec after finish()).
+static std::vector<osc::FieldSpec> fields_from_descs(const osc_field_desc* fields, int n_fields) {
+  using namespace osc;
+  std::vector<FieldSpec> fs;
+  for (int i = 0; i < n_fields; ++i) {
+    FieldSpec f = field_from_desc(fields + i);
+    f.finish();
+    fs.push_back(f);
+  }
+  return fs;
+}
+
+// Jobs of a batch request: the ideal particle of a beam with each job's energy and direction
+// (TParticleBeam::GetNewParticle), its trajectory range and its observer / energy ranges.
+static std::vector<osc::BatchJob> jobs_from_descs(const osc_job_desc* jobs, int n_jobs) {
+  using namespace osc;
+  std::vector<BatchJob> bj(n_jobs);
+  for (int k = 0; k < n_jobs; ++k) {
+    const osc_job_desc& d = jobs[k];
+    BatchJob& J = bj[k];
+    double q = 0, m = 0;
+    if (particle_qm(d.particle, d.charge, d.mass, q, m)) throw Error{OSC_ERR_INVALID, "unknown particle type"};
+    if (d.particle == OSC_PARTICLE_CUSTOM && (d.mass == 0 || d.charge == 0))
+      throw Error{OSC_ERR_INVALID, "'mass' or 'charge' is zero"};
+    if (d.energy_GeV < 0) throw Error{OSC_ERR_INVALID, "job energy_GeV must be >= 0"};
+    const Vec3 dir = V3(d.d0);
+    const Vec3 u0 = mag2(dir) > 0 ? unit(dir) : Vec3{};
+    const double e0 = d.energy_GeV < kg_to_gev(m) ? m : d.energy_GeV;
+    const double g = e0 / kg_to_gev(m) < 1 ? 1 : e0 / kg_to_gev(m);
+    const double b = g != 1 ? std::sqrt(1.0 - 1.0 / (g * g)) : 0;
+    J.particle.q = q;
+    J.particle.m = m;
+    J.particle.current = d.current != 0 ? d.current : q;
+    J.particle.set_conditions(V3(d.x0), u0 * b, d.t0);
+    J.field_begin = d.field_begin;
+    J.field_count = d.field_count;
+    J.ctstart = d.ctstart;
+    J.ctstop = d.ctstop;
+    J.npoints = d.npoints;
+    J.obs_begin = d.obs_begin;
+    J.n_obs = d.n_obs;
+    J.omega_begin = d.energy_begin;
+    J.n_e = d.n_energies;
+    J.current_abs = d.spectrum != 0;
+  }
+  return bj;
+}
+
 OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fields, const osc_job_desc* jobs,
                            int n_jobs, const double* obs_xyz, long long n_obs, const double* energies_eV,
                            long long n_energies, const osc_rad_opts* opts, int average, double* out,
@@ -401,44 +449,10 @@ OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fie
     if ((n_fields > 0 && !fields) || (n_jobs > 0 && (!jobs || !out)) || (n_obs > 0 && !obs_xyz) ||
         (n_energies > 0 && !energies_eV))
       throw Error{OSC_ERR_INVALID, "bad buffers"};
-    std::vector<FieldSpec> fs;
-    for (int i = 0; i < n_fields; ++i) {
-      FieldSpec f = field_from_desc(fields + i);
-      f.finish();
-      fs.push_back(f);
-    }
+    std::vector<FieldSpec> fs = fields_from_descs(fields, n_fields);
     std::vector<double> omega(n_energies);
     for (long long i = 0; i < n_energies; ++i) omega[i] = ev_to_omega(energies_eV[i]);
-    std::vector<BatchJob> bj(n_jobs);
-    for (int k = 0; k < n_jobs; ++k) {
-      const osc_job_desc& d = jobs[k];
-      BatchJob& J = bj[k];
-      double q = 0, m = 0;
-      if (particle_qm(d.particle, d.charge, d.mass, q, m)) throw Error{OSC_ERR_INVALID, "unknown particle type"};
-      if (d.particle == OSC_PARTICLE_CUSTOM && (d.mass == 0 || d.charge == 0))
-        throw Error{OSC_ERR_INVALID, "'mass' or 'charge' is zero"};
-      if (d.energy_GeV < 0) throw Error{OSC_ERR_INVALID, "job energy_GeV must be >= 0"};
-      // the ideal particle of a beam with this energy and direction (TParticleBeam::GetNewParticle)
-      const Vec3 dir = V3(d.d0);
-      const Vec3 u0 = mag2(dir) > 0 ? unit(dir) : Vec3{};
-      const double e0 = d.energy_GeV < kg_to_gev(m) ? m : d.energy_GeV;
-      const double g = e0 / kg_to_gev(m) < 1 ? 1 : e0 / kg_to_gev(m);
-      const double b = g != 1 ? std::sqrt(1.0 - 1.0 / (g * g)) : 0;
-      J.particle.q = q;
-      J.particle.m = m;
-      J.particle.current = d.current != 0 ? d.current : q;
-      J.particle.set_conditions(V3(d.x0), u0 * b, d.t0);
-      J.field_begin = d.field_begin;
-      J.field_count = d.field_count;
-      J.ctstart = d.ctstart;
-      J.ctstop = d.ctstop;
-      J.npoints = d.npoints;
-      J.obs_begin = d.obs_begin;
-      J.n_obs = d.n_obs;
-      J.omega_begin = d.energy_begin;
-      J.n_e = d.n_energies;
-      J.current_abs = d.spectrum != 0;
-    }
+    std::vector<BatchJob> bj = jobs_from_descs(jobs, n_jobs);
     Engine& E = *ctx->eng;
     if (opts->precision_mode == OSC_MIXED) {
       E.batch(fs, bj, obs_xyz, n_obs, omega.data(), n_energies, *opts, average != 0, out, level_out);
@@ -446,6 +460,21 @@ OSC_API int osc_batch_flux(osc_ctx* ctx, const osc_field_desc* fields, int n_fie
       E.batch_fp64(fs, bj, obs_xyz, n_obs, omega.data(), n_energies, *opts, average != 0, out, level_out);
     }
     if (n_not_converged) *n_not_converged = E.last_not_converged;
+  });
+}
+
+OSC_API int osc_batch_trajectories(osc_ctx* ctx, const osc_field_desc* fields, int n_fields, const osc_job_desc* jobs,
+                                   int n_jobs, double* out, long long capacity, long long* npoints_out) {
+  return guarded(ctx, [&] {
+    using namespace osc;
+    if (n_fields < 0 || n_jobs < 0) throw Error{OSC_ERR_INVALID, "negative count"};
+    if ((n_fields > 0 && !fields) || (n_jobs > 0 && (!jobs || !out || !npoints_out)))
+      throw Error{OSC_ERR_INVALID, "bad buffers"};
+    std::vector<FieldSpec> fs = fields_from_descs(fields, n_fields);
+    std::vector<BatchJob> bj = jobs_from_descs(jobs, n_jobs);
+    std::vector<int64_t> np(n_jobs);
+    ctx->eng->batch_trajectories(fs, bj, out, capacity, np.data());
+    for (int k = 0; k < n_jobs; ++k) npoints_out[k] = np[k];
   });
 }
 

@@ -78,6 +78,10 @@ class Engine {
   void batch(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
              int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o, bool average,
              double* out, int32_t* level_out, double average_weight = 0.0);  // 0: 1 / jobs
+  // The jobs' trajectories as the batched path integrates them on the device: per job 19 x n knot
+  // values (t, 9 components, their 9 spline second derivatives) in job order, n in npoints.
+  void batch_trajectories(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, double* out,
+                          int64_t capacity, int64_t* npoints);
   // The same jobs one after another through the single-trajectory FP64 path (host RK4).
   void batch_fp64(const std::vector<FieldSpec>& fields, const std::vector<BatchJob>& jobs, const double* obs,
                   int64_t n_obs_total, const double* omega, int64_t n_omega_total, const osc_rad_opts& o,
