@@ -106,7 +106,8 @@ def test_device_trajectory_matches_host(case):
     for c in range(9):
         d_c = float(np.max(np.abs(dev[1 + c] - host[1 + c])))
         bound = 24 * (d_c + 8 * eps * float(np.max(np.abs(host[1 + c])))) / h ** 2
-        d2[ROWS[10 + c]] = float(np.max(np.abs(dev[10 + c] - host[10 + c]))) / bound
+        diff = float(np.max(np.abs(dev[10 + c] - host[10 + c])))
+        d2[ROWS[10 + c]] = diff / bound if bound > 0 else (0.0 if diff == 0 else float("inf"))  # a zero component
     worst_d2 = max(d2, key=d2.get)
     mid = {}
     for c in range(9):
