@@ -164,50 +164,87 @@ def _cpu_impl():
     return "port", 1, OracleSR()
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def _cpu_flux_timed(o, kind, cores, nrows, passes):
+    """`passes` timed passes of the flux on the central `nrows` rows; (list of seconds, samples per
+    pass) with samples counted once from the CPU path's own stop levels (untimed)."""
+    import numpy as np
+    w1 = 0.01 * (nrows - 1) / (GRID - 1)
+    kw = dict(energy_eV=E1, npoints=[nrows, GRID], width=[w1 if nrows > 1 else 1e-9, 0.01], translation=[0, 0, 30])
+    if kind == "reference":
+        kw["nthreads"] = cores
+    times = []
+    for _ in range(passes):
+        t0 = time.perf_counter()
+        o.calculate_flux_rectangle(**kw)
+        times.append(time.perf_counter() - t0)
+    lev = np.array([v for _, v in o.calculate_flux_rectangle(**dict(kw, quantity="level"))])
+    return times, float(np.sum(2.0 ** (lev + 1) - 1))
+
+
 def reference_arm(args):
-    """The reference's own CPU implementation on all host cores (rank 0 only), same workload and
-    metric; each step is the largest set of central grid rows that keeps the run to ~20 s."""
+    """The reference's own CPU implementation on all host threads (rank 0 only): every step is the
+    whole 201 x 201 flux of the product arm's workload, same metric and config."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     kind, cores, o = _cpu_impl()
     setup(o)
     o.calculate_trajectory()
-    dt, _ = _cpu_flux_rows(o, kind, cores, 5)
-    rows = int(max(5, min(GRID, (20.0 / max(1, args.steps)) / max(dt / 5, 1e-6))))
-    rows -= (rows + 1) % 2  # odd: the row set stays centred on the axis
-    times, samples = [], 0.0
-    for _ in range(args.steps):
-        dt, s = _cpu_flux_rows(o, kind, cores, rows)
-        times.append(dt)
-        samples += s
+    if args.warmup > 0:
+        _cpu_flux_timed(o, kind, cores, GRID, 1)
+    times, samples = _cpu_flux_timed(o, kind, cores, GRID, args.steps)
     total = sum(times)
-    value = samples / total / 1e9
-    desc = "central %d of 201 rows x 201 columns per step, %d steps, %d threads" % (rows, args.steps, cores)
+    value = samples * args.steps / total / 1e9
+    desc = "full 201 x 201 grid per step, %d steps, %d threads, %s" % (args.steps, cores, _cpu_model())
     line = {"metric": METRIC, "value": value, "unit": "Gsamples/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": desc}, "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "Gsamples/s", "cores": cores, "kind": kind, "sample": desc},
+            "config": product_config(1), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "Gsamples/s", "cores": cores, "kind": kind, "sample": desc,
+                             "cpu_model": _cpu_model()},
             "e2e": {"value": value, "unit": "Gsamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def product_config(world):
+    return {"workload": WORKLOAD, "compute": "mixed", "l2": "flushed between steps (256 MB write)",
+            "parallelism": "independent job per rank" if world > 1 else "single GPU"}
+
+
 def cpu_baseline_leg():
-    """The reference CPU path on all host cores, bounded to ~10-20 s of work."""
+    """The reference CPU path on the headline workload: all host threads over the whole 201 x 201
+    grid (one pass), and one thread over the central rows that take about 5 s."""
     kind, cores, o = _cpu_impl()
     setup(o)
     o.calculate_trajectory()
-    dt, _ = _cpu_flux_rows(o, kind, cores, 5)
-    rows = int(max(5, min(GRID, 15.0 / max(dt / 5, 1e-6))))
-    rows -= (rows + 1) % 2
-    dt, samples = _cpu_flux_rows(o, kind, cores, rows)
-    return {"value": samples / dt / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": kind,
-            "sample": "central %d of 201 rows x 201 columns, one pass, %.2f s" % (rows, dt)}
+    t_all, s_all = _cpu_flux_timed(o, kind, cores, GRID, 1)
+    out = {"value": s_all / t_all[0] / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": kind,
+           "sample": "whole 201 x 201 grid, one pass, %.2f s" % t_all[0], "cpu_model": _cpu_model()}
+    if kind == "reference":
+        t5, _ = _cpu_flux_timed(o, kind, 1, 5, 1)
+        rows = int(max(5, min(GRID, 5.0 / max(t5[0] / 5, 1e-6))))
+        rows -= (rows + 1) % 2  # odd: the row set stays centred on the axis
+        t1, s1 = _cpu_flux_timed(o, kind, 1, rows, 1)
+        out["value_1thread"] = s1 / t1[0] / 1e9
+        out["sample_1thread"] = "central %d of 201 rows x 201 columns, one pass, %.2f s, 1 thread" % (rows, t1[0])
+    return out
 
 
 def _time_device_steps(ctx, step, stream, flush, steps, warmup, local):
     """Per-step CUDA events on the launching stream, L2 flushed before every step (outside the
-    events).  Returns (total ms, samples per step, launches per step, wave-kernel ms, clocks)."""
+    events), the library's own per-launch profiling off.  Returns (per-step ms list, samples per step,
+    launches per step, clocks)."""
     import ctypes
     import torch
     for _ in range(warmup):
@@ -215,9 +252,6 @@ def _time_device_steps(ctx, step, stream, flush, steps, warmup, local):
     torch.cuda.synchronize()
     sm, ln = ctypes.c_longlong(), ctypes.c_longlong()
     ctx.call("osc_last_stats", ctypes.byref(sm), ctypes.byref(ln))  # the job is identical every step
-    ctx.call("osc_set_profiling", 1)
-    ctx.call("osc_get_profile", None, None, None, 1)
-    torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with ClockSampler(local) as clk:
         time.sleep(0.1)
@@ -227,11 +261,42 @@ def _time_device_steps(ctx, step, stream, flush, steps, warmup, local):
             step()
             evs[i][1].record(stream)
         torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in evs)
+    return [a.elapsed_time(b) for a, b in evs], sm.value, ln.value, clk.summary()
+
+
+def _kernel_time(ctx, step, flush, steps):
+    """Summed device time [ms] and count of the sample-sum kernel launches over `steps` steps, from the
+    library's per-launch CUDA events (a separate pass: those events are off while `value` is timed)."""
+    import ctypes
+    import torch
+    ctx.call("osc_set_profiling", 1)
+    ctx.call("osc_get_profile", None, None, None, 1)
+    for _ in range(steps):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
     kms, kl = ctypes.c_double(), ctypes.c_longlong()
     ctx.call("osc_get_profile", ctypes.byref(kms), ctypes.byref(kl), None, 1)
     ctx.call("osc_set_profiling", 0)
-    return ms, sm.value, ln.value, kms.value, kl.value, clk.summary()
+    return kms.value, kl.value
+
+
+def _long_run(step, stream, flush, min_s=1.0):
+    """Steps repeated (L2 flushed before each, outside the events) until the timed total reaches
+    min_s seconds: (steps, total ms)."""
+    import torch
+    total, n = 0.0, 0
+    while total < 1e3 * min_s:
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(200)]
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            step()
+            b.record(stream)
+        torch.cuda.synchronize()
+        total += sum(a.elapsed_time(b) for a, b in evs)
+        n += len(evs)
+    return n, total
 
 
 def product_arm(args):
@@ -289,7 +354,8 @@ def product_arm(args):
     for m in modes:
         if world > 1:
             dist.barrier()
-        ms, sps, lps, kms, kl, clocks = _time_device_steps(ctx, make_step(m), stream, flush, args.steps, args.warmup, local)
+        per, sps, lps, clocks = _time_device_steps(ctx, make_step(m), stream, flush, args.steps, args.warmup, local)
+        ms = sum(per)
         t = torch.tensor([ms, float(sps * args.steps)], dtype=torch.float64, device=dev)
         if world > 1:
             tmax, tsum = t.clone(), t.clone()
@@ -298,6 +364,8 @@ def product_arm(args):
             ms_max, samples_all = float(tmax[0]), float(tsum[1])
         else:
             ms_max, samples_all = ms, float(sps * args.steps)
+        kms, kl = _kernel_time(ctx, make_step(m), flush, args.steps)
+        long_n, long_ms = _long_run(make_step(m), stream, flush) if not args.quick else (0, 0.0)
         v, nv = ctypes.c_int(), ctypes.c_int()
         ctx.call("osc_get_variant", 2 if m == "mixed" else 0, ctypes.byref(v), ctypes.byref(nv))
         peak = ctypes.c_double()
@@ -305,6 +373,7 @@ def product_arm(args):
         achieved = sps * args.steps * FLOP_PER_SAMPLE / (kms * 1e-3) / 1e12 if kms > 0 else None
         kname = _lib.variant_name(2 if m == "mixed" else 0, v.value)
         traffic = _profiled_traffic().get(kname)
+        srt = sorted(per)
         res[m] = {"value": samples_all / (ms_max * 1e-3) / 1e9, "ms_per_step": ms_max / args.steps,
                   "samples_per_step": sps, "launches_per_step": lps, "variant": v.value, "clocks": clocks,
                   "roofline": {"bound": "fp64" if m == "fp64" else "fp32", "achieved": achieved, "peak": peak.value,
@@ -313,7 +382,10 @@ def product_arm(args):
                                "kernel_ms_per_step": kms / args.steps, "kernel_launches_per_step": kl / args.steps,
                                "peak_source": "in-run FMA-throughput loop on this GPU (osc_measure_fma_peak); the "
                                               "sample sums run on the %s pipe, not the tensor cores or HBM"
-                                              % ("FP64" if m == "fp64" else "FP32/SFU")}}
+                                              % ("FP64" if m == "fp64" else "FP32/SFU"),
+                               "step_ms_median": srt[len(srt) // 2], "step_ms_min": srt[0], "step_ms_max": srt[-1],
+                               "long_run_steps": long_n, "long_run_s": long_ms * 1e-3,
+                               "long_run_value": sps * long_n / (long_ms * 1e-3) / 1e9 if long_ms > 0 else None}}
     head = modes[-1]
     err = None
     if "mixed" in res:
@@ -378,24 +450,28 @@ def product_arm(args):
     if rank == 0:
         cpu = cpu_baseline_leg() if world == 1 else None
         r = res[head]
+        roof = dict(r["roofline"])
+        if "mixed" in res:  # the plain FP64 path of the same run, flat so that the record keeps it
+            f = res["fp64"]
+            roof.update({"fp64_value": f["value"], "fp64_ms_per_step": f["ms_per_step"],
+                         "fp64_kernel": f["roofline"]["kernel"], "fp64_achieved": f["roofline"]["achieved"],
+                         "fp64_peak": f["roofline"]["peak"], "fp64_frac": f["roofline"]["frac"],
+                         "fp64_traffic": f["roofline"]["traffic"], "fp64_long_run_value": f["roofline"]["long_run_value"],
+                         "mixed_over_fp64": r["value"] / f["value"], "mixed_vs_fp64_peak_rel_err": err})
         line = {"metric": METRIC, "value": r["value"], "unit": "Gsamples/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "compute": head, "l2": "flushed between steps (256 MB write)",
-                           "parallelism": "independent job per rank" if world > 1 else "single GPU"},
+                "config": dict(product_config(world), compute=head),
                 "e2e": {"value": e2e_value, "unit": "Gsamples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "host_buffers": "pinned", "path": "osc_flux (C ABI), trajectory computed before the loop as in the reference arm",
-                        "with_new_trajectory": {"value": e2e_traj_value, "unit": "Gsamples/s",
-                                                "h2d_bytes_per_step": h2d + 19 * 20001 * 8,
-                                                "note": "new particle every step: host RK4 + spline + trajectory upload timed too"}},
-                "gpu_launches": r["launches_per_step"] * args.steps, "roofline": r["roofline"], "cpu_baseline": cpu,
+                        "with_new_trajectory_value": e2e_traj_value,
+                        "with_new_trajectory_h2d_bytes_per_step": h2d + 19 * 20001 * 8,
+                        "with_new_trajectory_note": "new particle every step: host RK4 + spline + trajectory upload timed too"},
+                "gpu_launches": r["launches_per_step"] * args.steps, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": r["clocks"]}
         if "mixed" in res:
-            f = res["fp64"]
-            line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
-                            "clocks": f["clocks"]}
-            line["mixed_over_fp64"] = r["value"] / f["value"]
-            line["mixed_vs_fp64_peak_rel_err"] = err
+            line["fp64"] = {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms_per_step"],
+                            "roofline": res["fp64"]["roofline"], "clocks": res["fp64"]["clocks"]}
         if world == 1 and args.batched_steps > 0:
             bw = max(3, args.warmup)
             line["batched"] = {"note": "inputs far larger than L2 (GBs of level records); device time = each "
@@ -403,6 +479,15 @@ def product_arm(args):
                                "epu_beam_10k": beam_leg(args.batched_steps, bw, local),
                                "uneven_512": uneven_leg(args.batched_steps, bw, local)}
             line["tuning"] = tuning_leg(max(5, args.batched_steps), bw, local)
+            bb, bu, bt = line["batched"]["epu_beam_10k"], line["batched"]["uneven_512"], line["tuning"]
+            line["roofline"].update({  # the batched workloads' headline figures, flat so that the record keeps them
+                "beam_value": bb["value"], "beam_fp64_value": bb["fp64"]["value"],
+                "beam_mixed_over_fp64": bb["mixed_over_fp64"], "uneven_value": bu["value"],
+                "uneven_fp64_value": bu["fp64"]["value"], "uneven_mixed_over_fp64": bu["mixed_over_fp64"],
+                "tuning_grad_per_s": bt["value"],
+                "beam_cpu_reference_value": (bb["cpu_reference"] or {}).get("value"),
+                "uneven_cpu_reference_value": (bu["cpu_reference"] or {}).get("value"),
+                "tuning_cpu_reference_grad_per_s": (bt["cpu_reference"] or {}).get("value")})
         if sharded is not None:
             line["epu_beam_10k_sharded"] = sharded
         print(json.dumps(line), flush=True)
@@ -462,9 +547,11 @@ def uneven_jobs(seed=2024, n=UNEVEN_JOBS):
         obs = np.stack([X.ravel(), Y.ravel(), np.full(X.size, z)], 1)
         ne = int(rng.integers(1, 257))
         e1 = _e1_eV(B, lam)
-        jobs.append(Job(fields=[undulator([0, B, 0], [0, 0, lam], N, phase=-math.pi / 2)], energy_GeV=3.0,
-                        ctstartstop=(-half, half), npoints=npts, obs=obs,
-                        energies_eV=np.linspace(0.95 * e1, 1.05 * e1, ne), current=0.5))
+        jb = Job(fields=[undulator([0, B, 0], [0, 0, lam], N, phase=-math.pi / 2)], energy_GeV=3.0,
+                 ctstartstop=(-half, half), npoints=npts, obs=obs, energies_eV=np.linspace(0.95 * e1, 1.05 * e1, ne),
+                 current=0.5)
+        jb.setup = (lam, B, N, half, npts, nx, ny, wx, wy, z)  # for the reference CPU subset
+        jobs.append(jb)
     return jobs
 
 
@@ -488,6 +575,92 @@ def _peak_err(a, b):
     import numpy as np
     a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def _cpu_reference():
+    """(the reference's own CPU module, host threads) or (None, 0) when oracle/_ref is absent."""
+    S = _quiet_import_reference()
+    return (S, os.cpu_count() or 1) if S is not None else (None, 0)
+
+
+def beam_cpu_reference(particles):
+    """The reference CPU path on the first `particles` particles of the EPU beam (seed 1), all host
+    threads: seconds for the 101 x 101 flux (particles are independent, so the time per particle
+    extrapolates linearly to the 10k beam)."""
+    S, cores = _cpu_reference()
+    if S is None:
+        return None, 0
+    o = S.sr(nthreads=cores, gpu=0)
+    setup_epu_beam(o)
+    o.set_seed(1)
+    t0 = time.perf_counter()
+    o.calculate_flux_rectangle(energy_eV=E1_EPU, npoints=[101, 101], width=[0.008, 0.008], translation=[0, 0, 30],
+                               nparticles=particles, nthreads=cores)
+    return time.perf_counter() - t0, cores
+
+
+def uneven_cpu_reference(jobs, n=8):
+    """The reference CPU path on a subset of the uneven jobs: the first n with at least 2 x 2
+    observers, each at the middle one of its energies, all host threads; (seconds, samples counted
+    from the CPU path's own stop levels, jobs, cores)."""
+    import numpy as np
+    S, cores = _cpu_reference()
+    if S is None:
+        return None
+    total_t, samples, used = 0.0, 0.0, 0
+    for jb in jobs:
+        lam, B, N, half, npts, nx, ny, wx, wy, z = jb.setup
+        if nx < 2 or ny < 2:
+            continue
+        o = S.sr(nthreads=cores, gpu=0)
+        o.add_bfield_undulator(bfield=[0, B, 0], period=[0, 0, lam], nperiods=N, phase=-math.pi / 2)
+        o.set_particle_beam(type="electron", energy_GeV=3.0, x0=[0, 0, 0], d0=[0, 0, 1], current=0.5)
+        o.set_ctstartstop(-half, half)
+        o.set_npoints_trajectory(npts)
+        o.calculate_trajectory()
+        e = float(jb.energies_eV[len(jb.energies_eV) // 2])
+        kw = dict(energy_eV=e, npoints=[nx, ny], width=[wx, wy], translation=[0, 0, z], nthreads=cores)
+        t0 = time.perf_counter()
+        o.calculate_flux_rectangle(**kw)
+        total_t += time.perf_counter() - t0
+        lev = np.array([v for _, v in o.calculate_flux_rectangle(**dict(kw, quantity="level"))])
+        samples += float(np.sum(2.0 ** (lev + 1) - 1))
+        used += 1
+        if used == n:
+            break
+    return total_t, samples, used, cores
+
+
+def tuning_cpu_reference(every=16, h=1e-3):
+    """One central-difference gradient component of the field-tuning loss through the reference CPU
+    path (all host threads), on every `every`-th of the 256 energies: two loss evaluations, each a new
+    trajectory through the half-period-scaled undulator (given to the reference as a Python field
+    function with the undulator's operations) and the 21 x 21 flux per energy at level 12.  Returns
+    (seconds for the subset, scale to the full gradient = 82 components x every, cores)."""
+    import numpy as np
+    S, cores = _cpu_reference()
+    if S is None:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from cases import halfscale_function
+    energies = np.linspace(0.95 * E1, 1.05 * E1, 256)[::every]
+    s0 = 1 + np.random.default_rng(82).normal(0.0, 0.005, 82)
+
+    def loss_eval(scale):
+        o = S.sr(nthreads=cores, gpu=0)
+        o.add_bfield_function(halfscale_function([0, 0.5, 0], [0, 0, 0.05], 41, -math.pi / 2, list(scale)))
+        o.set_particle_beam(type="electron", energy_GeV=3, x0=[0, 0, 0], d0=[0, 0, 1], current=0.5)
+        o.set_ctstartstop(-1.5, 1.5)
+        o.set_npoints_trajectory(20001)
+        for e in energies:
+            o.calculate_flux_rectangle(energy_eV=float(e), npoints=[21, 21], width=[0.002, 0.002],
+                                       translation=[0, 0, 30], precision=0, max_level=12, nthreads=cores)
+    e20 = np.zeros(82)
+    e20[20] = h
+    t0 = time.perf_counter()
+    loss_eval(s0 + e20)
+    loss_eval(s0 - e20)
+    return time.perf_counter() - t0, 82 * every, cores
 
 
 def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, check_level=12):
@@ -515,23 +688,36 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
             samples += sm
             launches += ln
     run(fp64_particles, "fp64")
-    _, _, sm64, _, w64 = _profiled(s._ctx, lambda: run(fp64_particles, "fp64"))
+    _, ms64, sm64, _, w64 = _profiled(s._ctx, lambda: run(fp64_particles, "fp64"))
     a = run(check_particles, "mixed", precision=0, max_level=check_level)[1]
     b = run(check_particles, "fp64", precision=0, max_level=check_level)[1]
     mixed_e2e = samples / wall / 1e9
     fp64_e2e = sm64 / w64 / 1e9
+    fp64_dev = sm64 / (ms64 * 1e-3) / 1e9
+    mixed_dev = samples / (dev_ms * 1e-3) / 1e9
+    # the reference CPU path on the first cpu_particles particles (the FP64 GPU path's stop levels --
+    # identical to the reference's -- count their samples)
+    cpu_particles = 16
+    run(cpu_particles, "fp64")
+    _, _, sm_cpu, _, _ = _profiled(s._ctx, lambda: run(cpu_particles, "fp64"))
+    t_cpu, cores = beam_cpu_reference(cpu_particles)
+    cpu = None if t_cpu is None else {
+        "value": sm_cpu / t_cpu / 1e9, "unit": "Gsamples/s", "cores": cores, "kind": "reference",
+        "sample": "first %d of the 10000 particles, 101 x 101, %.1f s; per particle %.2f s, so the 10000-particle "
+                  "beam extrapolates to %.0f s" % (cpu_particles, t_cpu, t_cpu / cpu_particles,
+                                                  t_cpu / cpu_particles * BEAM_PARTICLES)}
     return {"workload": BEAM_WORKLOAD, "steps": steps, "warmup": warmup,
             "value": samples / (dev_ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": dev_ms / steps,
             "samples_per_step": samples // steps, "gpu_launches_per_step": launches // steps,
             "e2e": {"value": mixed_e2e, "unit": "Gsamples/s", "wall_s_per_step": wall / steps,
                     "path": "sr.calculate_flux_rectangle(nparticles=10000, compute='mixed', return_numpy=True)"},
-            "fp64": {"e2e": fp64_e2e, "unit": "Gsamples/s", "particles": fp64_particles,
+            "fp64": {"value": fp64_dev, "e2e": fp64_e2e, "unit": "Gsamples/s", "particles": fp64_particles,
                      "path": "sr.calculate_flux_rectangle(nparticles=%d, compute='fp64') (reference method: host RK4 "
-                             "per particle, FP64 sums)" % fp64_particles},
-            "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
+                             "per particle, FP64 sums); value = device time of its sample-sum kernels" % fp64_particles},
+            "mixed_over_fp64": mixed_dev / fp64_dev, "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
             "mixed_vs_fp64_peak_rel_err": {"value": _peak_err(a, b), "particles": check_particles,
                                            "fixed_level": check_level},
-            "clocks": clk.summary()}
+            "cpu_reference": cpu, "clocks": clk.summary()}
 
 
 def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12):
@@ -556,24 +742,30 @@ def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12):
     sub = jobs[:fp64_jobs]
     r.ctx.call("osc_set_variant", 0, 2)  # FP64 variant fixed: no per-shape tuning runs inside the timing
     r.flux(sub, compute="fp64")
-    _, _, sm64, _, w64 = _profiled(r.ctx, lambda: r.flux(sub, compute="fp64"))
+    _, ms64, sm64, _, w64 = _profiled(r.ctx, lambda: r.flux(sub, compute="fp64"))
     a = r.flux(sub, compute="mixed", precision=0, max_level=check_level)
     b = r.flux(sub, compute="fp64", precision=0, max_level=check_level)
     err = max(_peak_err(x, y) for x, y in zip(a, b))
     mixed_e2e = samples / wall / 1e9
     fp64_e2e = sm64 / w64 / 1e9
+    fp64_dev = sm64 / (ms64 * 1e-3) / 1e9
+    mixed_dev = samples / (dev_ms * 1e-3) / 1e9
+    cr = uneven_cpu_reference(jobs)
+    cpu = None if cr is None else {
+        "value": cr[1] / cr[0] / 1e9, "unit": "Gsamples/s", "cores": cr[3], "kind": "reference",
+        "sample": "first %d jobs with >= 2 x 2 observers, one energy each (the middle one), %.1f s" % (cr[2], cr[0])}
     return {"workload": UNEVEN_WORKLOAD, "steps": steps, "warmup": warmup,
             "value": samples / (dev_ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": dev_ms / steps,
             "samples_per_step": samples // steps, "gpu_launches_per_step": launches // steps, "variant": variant,
             "e2e": {"value": mixed_e2e, "unit": "Gsamples/s", "wall_s_per_step": wall / steps,
                     "path": "oscars_b200.batch.BatchRunner.flux(jobs, compute='mixed')"},
-            "fp64": {"e2e": fp64_e2e, "unit": "Gsamples/s", "jobs": fp64_jobs,
-                     "path": "BatchRunner.flux(jobs[:%d], compute='fp64') (jobs one after another, host RK4)"
-                             % fp64_jobs},
-            "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
+            "fp64": {"value": fp64_dev, "e2e": fp64_e2e, "unit": "Gsamples/s", "jobs": fp64_jobs,
+                     "path": "BatchRunner.flux(jobs[:%d], compute='fp64') (jobs one after another, host RK4); value = "
+                             "device time of its sample-sum kernels" % fp64_jobs},
+            "mixed_over_fp64": mixed_dev / fp64_dev, "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
             "mixed_vs_fp64_peak_rel_err": {"value": err, "jobs": fp64_jobs, "fixed_level": check_level,
                                            "norm": "per job, max over jobs"},
-            "clocks": clk.summary()}
+            "cpu_reference": cpu, "clocks": clk.summary()}
 
 
 def sharded_beam_leg(steps, warmup, local, rank, world):
@@ -666,12 +858,18 @@ def tuning_leg(steps, warmup, local=0, check_params=(3, 20, 41, 70)):
         return (loss(s + e) - loss(s - e)) / (2 * h)
     fd = np.array([(9 * central(k, 1e-3) - central(k, 3e-3)) / 8 for k in check_params])
     err = float(np.max(np.abs(g[list(check_params)] - fd)) / np.max(np.abs(fd)))
+    tr = tuning_cpu_reference()
+    cpu = None if tr is None else {
+        "value": 1.0 / (tr[0] * tr[1]), "unit": "grad/s", "cores": tr[2], "kind": "reference",
+        "sample": "one central-difference component on 16 of the 256 energies, %.1f s; the full gradient by "
+                  "central differences is %d such subsets (82 components x 16), so %.0f s per gradient (derived)"
+                  % (tr[0], tr[1], tr[0] * tr[1])}
     return {"workload": TUNING_WORKLOAD, "steps": steps, "warmup": warmup, "value": steps / t_all,
             "unit": "grad/s", "ms_per_step": 1e3 * t_all / steps, "forward_ms": 1e3 * t_fwd / steps,
             "adjoint_ms": 1e3 * (t_all - t_fwd) / steps,
             "grad_vs_richardson_fd": {"value": err, "params": list(check_params), "steps": [1e-3, 3e-3]},
             "path": "oscars_b200.tuning.TuningProblem.flux + vjp (osc_flux_multi, osc_flux_vjp); wall clock, "
-                    "host buffers", "clocks": clk.summary()}
+                    "host buffers", "cpu_reference": cpu, "clocks": clk.summary()}
 
 
 def _free_port():
