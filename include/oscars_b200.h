@@ -175,6 +175,21 @@ OSC_API int osc_calculate_trajectory(osc_ctx* ctx);
 /* out: 10 x n SoA (t, x, y, z, beta_x, beta_y, beta_z, a_x/c, a_y/c, a_z/c); n_out = points. */
 OSC_API int osc_get_trajectory(osc_ctx* ctx, double* out, long long capacity, long long* n_out);
 
+/* Use a trajectory computed elsewhere -- e.g. by the reference's own host code through any of its
+ * field types -- for the radiation calls that follow: the particle (osc_particle_type, custom charge
+ * [C] and mass [kg], current [A], initial position x0 [m], beta0 and t0 [m] -- what TParticleA holds)
+ * and its trajectory as 10 x n SoA (t [s], x y z [m], beta, a/c [1/s]; the layout of
+ * osc_get_trajectory), times strictly increasing, n >= 3.  The clamped spline is computed here as for
+ * an RK4 trajectory (include/TOMATH.h:141-203).  This is what the reference's GPU seam receives
+ * through OSCARSSR& (src/OSCARSSR_Cuda.cu:609-614 reads OSR's current particle and trajectory). */
+OSC_API int osc_set_particle_trajectory(osc_ctx* ctx, int particle, double charge, double mass, double current,
+                                        const double x0[3], const double beta0[3], double t0, const double* traj,
+                                        long long n);
+/* Replaces OSCARSSR_Cuda_GetDeviceProperties (include/OSCARSSR_Cuda.h:30): a one-line description of
+ * device `device` (name, compute capability, multiprocessors, memory), NUL-terminated into out.
+ * Errors go to osc_last_error(NULL). */
+OSC_API int osc_get_device_properties(int device, char* out, long long capacity);
+
 /* ---- observation surfaces: TSurfacePoints_Rectangle::Init/GetXYZ/GetX1/GetX2
  *      (src/TSurfacePoints_Rectangle.cc:140-315).  Any pointer may be NULL. */
 OSC_API int osc_surface_rectangle(const char* plane, int nx1, int nx2, double width1,

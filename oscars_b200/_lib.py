@@ -82,6 +82,8 @@ SIGNATURES = {
     "osc_power_density_device": (I, [VP, VP, VP, LL, I, ctypes.POINTER(RadOpts), VP, VP, VP]),
     "osc_batch_flux": (I, [VP, ctypes.POINTER(FieldDesc), I, ctypes.POINTER(JobDesc), I, DP, LL, DP, LL,
                            ctypes.POINTER(RadOpts), I, DP, I32P, LLP]),
+    "osc_set_particle_trajectory": (I, [VP, I, D, D, D, DP, DP, D, DP, LL]),
+    "osc_get_device_properties": (I, [I, ctypes.c_char_p, LL]),
     "osc_batch_trajectories": (I, [VP, ctypes.POINTER(FieldDesc), I, ctypes.POINTER(JobDesc), I, DP, LL, LLP]),
     "osc_set_half_period_scale": (I, [VP, I, DP, LL]),
     "osc_trajectory_vjp": (I, [VP, DP, LL, DP, LL]),

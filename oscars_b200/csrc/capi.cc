@@ -1,6 +1,7 @@
 // capi.cc -- the extern "C" boundary (include/oscars_b200.h).  Every entry point catches osc::Error
 // and any other exception and turns it into a status code plus a message for osc_last_error().
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
@@ -331,6 +332,46 @@ OSC_API int osc_get_trajectory(osc_ctx* ctx, double* out, long long capacity, lo
     std::memcpy(out, k.t.data(), sizeof(double) * k.n);
     std::memcpy(out + k.n, k.y.data(), sizeof(double) * 9 * k.n);
   });
+}
+
+OSC_API int osc_set_particle_trajectory(osc_ctx* ctx, int particle, double charge, double mass, double current,
+                                        const double x0[3], const double beta0[3], double t0, const double* traj,
+                                        long long n) {
+  return guarded(ctx, [&] {
+    using namespace osc;
+    if (!x0 || !beta0 || !traj) throw Error{OSC_ERR_INVALID, "bad buffers"};
+    double q = 0, m = 0;
+    if (particle_qm(particle, charge, mass, q, m)) throw Error{OSC_ERR_INVALID, "unknown particle type"};
+    if (particle == OSC_PARTICLE_CUSTOM && (mass == 0 || charge == 0))
+      throw Error{OSC_ERR_INVALID, "'mass' or 'charge' is zero"};
+    Model& M = ctx->eng->model;
+    Particle P;
+    P.q = q;
+    P.m = m;
+    P.current = current;
+    P.set_conditions(V3(x0), V3(beta0), t0);
+    M.particle = P;
+    M.set_trajectory(traj, n);
+  });
+}
+
+OSC_API int osc_get_device_properties(int device, char* out, long long capacity) {
+  try {
+    cudaDeviceProp p;
+    const cudaError_t e = cudaGetDeviceProperties(&p, device);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      g_create_error = cudaGetErrorString(e);
+      return OSC_ERR_CUDA;
+    }
+    if (out && capacity > 0)
+      std::snprintf(out, (size_t)capacity,
+                    "%s, compute capability %d.%d, %d multiprocessors, %.1f GB device memory, %.0f kB L2", p.name,
+                    p.major, p.minor, p.multiProcessorCount, p.totalGlobalMem / 1e9, p.l2CacheSize / 1e3);
+    return OSC_OK;
+  } catch (...) {
+    return OSC_ERR_INVALID;
+  }
 }
 
 OSC_API int osc_surface_rectangle(const char* plane, int nx1, int nx2, double width1, double width2,

@@ -734,6 +734,20 @@ void Model::compute_trajectory() {
   spline_second_derivatives(knots);
 }
 
+void Model::set_trajectory(const double* traj, int64_t n) {
+  if (n < 3) throw Error{OSC_ERR_LENGTH, "TSpline1D3 does not see enough points for interpolation.  Please use >= 3 points"};
+  for (int64_t i = 1; i < n; ++i)
+    if (!(traj[i] > traj[i - 1])) throw Error{OSC_ERR_INVALID, "trajectory times must increase"};
+  knots.clear();
+  ++knots_version;
+  knots.n = n;
+  knots.t.assign(traj, traj + n);
+  knots.y.assign(traj + n, traj + 10 * n);
+  knots.tstart = knots.t.front();
+  knots.tstop = knots.t.back();
+  spline_second_derivatives(knots);
+}
+
 void Model::ensure_trajectory() {
   if (!particle.set) {
     if (!has_beam) throw Error{OSC_ERR_RANGE, "no beam defined"};

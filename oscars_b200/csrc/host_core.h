@@ -160,6 +160,8 @@ class Model {
   // Throws osc::Error on failure.
   void compute_trajectory();
   void ensure_trajectory();
+  // Use a trajectory computed elsewhere (10 x n SoA: t, x y z, beta, a/c) with its spline.
+  void set_trajectory(const double* traj, int64_t n);
 };
 
 // Spline second derivatives of the 9 components (TSpline1D3::Derivatives, include/TOMATH.h:141-203).

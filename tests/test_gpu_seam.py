@@ -1,0 +1,64 @@
+"""The reference's own oscars.sr with gpu=1, computing on this library.
+
+OSCARS sends gpu=1 requests through the seam of include/OSCARSSR_Cuda.h (OSCARSSR::Calculate*GPU,
+src/OSCARSSR.cc:2429, 3125, 4428).  oscars_b200/seam builds the reference's `sr` extension from its
+own sources with that seam served by liboscars_b200 (the reference's host code draws particles and
+integrates trajectories; this library's FP64 kernels integrate the radiation).  Every golden
+radiation case is replayed through that build with gpu=1 and compared with the golden values, which
+the reference's CPU path produced: peak-normalised error <= 1e-9 and identical stop-level maps.  The
+build must have been made beforehand (make -C oscars_b200/seam REF=<OSCARS sources>); the GPU box
+only receives the built files.  The reference runs in a child process, because the CPU reference
+build the other tests load is also a package named `oscars`.
+
+Excluded: pd_und_directional -- the seam's power-density function carries no `Directional`
+argument (include/OSCARSSR_Cuda.h:56-63), so a directional request is answered non-directionally by
+the reference's GPU path and by this seam alike.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from cases import CASES
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BUILD = os.path.join(ROOT, "oscars_b200", "seam", "_build")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+TOL = 1e-9
+EXCLUDED = {"pd_und_directional"}
+NAMES = sorted(k for k, v in CASES.items() if v[-1][0] != "calculate_trajectory" and k not in EXCLUDED)
+
+
+@pytest.fixture(scope="module")
+def seam_results(tmp_path_factory):
+    if not os.path.isdir(os.path.join(BUILD, "oscars")):
+        pytest.fail("the seam build is missing: make -C oscars_b200/seam REF=<OSCARS sources>")
+    out = str(tmp_path_factory.mktemp("seam") / "seam.npz")
+    env = dict(os.environ, PYTHONPATH="")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "seam_worker.py"), BUILD, out] + NAMES,
+                       capture_output=True, text=True, env=env, timeout=1200)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    return dict(np.load(out))
+
+
+def test_seam_build_is_the_one_loaded_and_sees_the_gpu(seam_results):
+    assert str(seam_results["module"]).startswith(BUILD)
+    assert int(seam_results["ngpu"]) >= 1  # CheckGPU() through the seam: gpu=1 requests go to the GPU
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_golden_case_through_reference_gpu_seam(seam_results, name):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    pos, val = seam_results[name + "/pos"], seam_results[name + "/val"]
+    assert np.array_equal(pos.reshape(g["pos"].shape), g["pos"])
+    if CASES[name][-1][1].get("quantity") == "level":
+        assert np.array_equal(val, g["val"])
+    else:
+        err = float(np.max(np.abs(val - g["val"])) / max(np.max(np.abs(g["val"])), 1e-300))
+        assert err <= TOL, "%s: peak-normalised error %.3e" % (name, err)
+    if "level" in g.files and name + "/level" in seam_results:
+        lev = seam_results[name + "/level"]
+        assert np.array_equal(lev, g["level"]), "stop levels differ at %d entries" % int(np.sum(lev != g["level"]))
