@@ -197,6 +197,20 @@ OSC_API int osc_surface_rectangle(const char* plane, int nx1, int nx2, double wi
                                   const double translation[3], int normal, double* xyz,
                                   double* normals, double* x1x2);
 
+/* Rectangle from three points (TSurfacePoints_Rectangle::Init(NX1, NX2, X0, X1, X2, Normal),
+ * src/TSurfacePoints_Rectangle.cc:76-127; GetXYZ / GetX1 / GetX2, :280-317): x0x1x2 = X0, X1, X2 (9
+ * doubles), rotated (RotateSelfXYZ) and translated first as the binding does
+ * (src/OSCARSSR_Python.cc:6652-6658); nx1, nx2 >= 2 (the reference divides by nx - 1).  Pointers
+ * other than x0x1x2 may be NULL. */
+OSC_API int osc_surface_x0x1x2(int nx1, int nx2, const double x0x1x2[9], const double rotations[3],
+                               const double translation[3], int normal, double* xyz, double* normals, double* x1x2);
+/* Arbitrary points with normals as the point-list calls take them (calculate_flux,
+ * src/OSCARSSR_Python.cc:7730-7750; calculate_power_density, :6225-6250): each point and normal
+ * rotated (RotateSelfXYZ), the normal reversed when invert_normals (calculate_power_density with
+ * normal = -1), the point translated.  3 x n doubles in and out. */
+OSC_API int osc_surface_points(long long n, const double* points, const double* normals, const double rotations[3],
+                               const double translation[3], int invert_normals, double* xyz, double* normals_out);
+
 /* ---- radiation: host buffers in and out; results are written (not accumulated). -------------
  * osc_flux          replaces OSCARSSR_Cuda_CalculateFluxGPU         (src/OSCARSSR_Cuda.cu:516)
  * osc_spectrum      replaces OSCARSSR_Cuda_CalculateSpectrumGPU     (src/OSCARSSR_Cuda.cu:1607)

@@ -183,6 +183,59 @@ def rectangle(plane, nx1, nx2, w1, w2, rotations, translation, normal):
 
 
 # ---- grid field files (restating src/TField3D_Grid.cc:365-530 and :572-870) -------------------
+def rectangle_x0x1x2(nx1, nx2, x0, x1, x2, rotations, translation, normal):
+    """TSurfacePoints_Rectangle::Init(NX1, NX2, X0, X1, X2, Normal) + GetXYZ/GetX1/GetX2
+    (src/TSurfacePoints_Rectangle.cc:76-127, 280-317), after the binding rotates and translates the
+    three points (src/OSCARSSR_Python.cc:6652-6658).  Returns (xyz, normals, x1x2)."""
+    if nx1 < 2 or nx2 < 2:
+        raise ValueError("'npoints' must be >= 2 in each direction with 'x0x1x2'")
+    P = []
+    for v in (x0, x1, x2):
+        w = rotate_xyz([float(a) for a in v], rotations)
+        P.append([w[k] + translation[k] for k in range(3)])
+    X0, X1, X2 = P
+    d1 = [X1[k] - X0[k] for k in range(3)]
+    d2 = [X2[k] - X0[k] for k in range(3)]
+    s1 = _mag(d1) / (nx1 - 1)
+    s2 = _mag(d2) / (nx2 - 1)
+    v1 = [d1[k] / (nx1 - 1) for k in range(3)]
+    v2 = [d2[k] / (nx2 - 1) for k in range(3)]
+    c = [v1[1] * v2[2] - v2[1] * v1[2], v1[2] * v2[0] - v2[2] * v1[0], v1[0] * v2[1] - v2[0] * v1[1]]
+    m = _mag(c)
+    nv = [c[0] / m, c[1] / m, c[2] / m]
+    if normal == -1:
+        nv = [nv[0] * -1, nv[1] * -1, nv[2] * -1]
+    elif normal not in (0, 1):
+        raise ValueError("fNormal is of the incorrect form.  Must be -1, 0, 1")
+    n = nx1 * nx2
+    xyz = np.empty((n, 3))
+    x1x2 = np.zeros((n, 3))
+    m1, m2 = _mag(v1), _mag(v2)
+    for i in range(n):
+        ix1, ix2 = i // nx2, i % nx2
+        a = [X0[k] + v1[k] * ix1 for k in range(3)]
+        xyz[i] = [a[k] + v2[k] * ix2 for k in range(3)]
+        x1x2[i, 0] = s1 * ix1 - m1 * (nx1 - 1) / 2.
+        x1x2[i, 1] = s2 * ix2 - m2 * (nx2 - 1) / 2.
+    return xyz, np.tile(np.array(nv), (n, 1)), x1x2
+
+
+def surface_points(points, rotations, translation, invert_normals):
+    """Points with normals as the point-list bindings take them (src/OSCARSSR_Python.cc:7728-7755,
+    6223-6255): point and normal rotated, the normal reversed on request, the point translated."""
+    xyz, nrm = [], []
+    for item in points:
+        if len(item) != 2:
+            raise ValueError("Incorrect format in 'points'")
+        X = rotate_xyz([float(v) for v in item[0]], rotations)
+        N = rotate_xyz([float(v) for v in item[1]], rotations)
+        if invert_normals:
+            N = [N[0] * -1, N[1] * -1, N[2] * -1]
+        xyz.append([X[k] + translation[k] for k in range(3)])
+        nrm.append(N)
+    return np.array(xyz, dtype=np.float64).reshape(-1, 3), np.array(nrm, dtype=np.float64).reshape(-1, 3)
+
+
 def _first_number(line):
     """TField3D_Grid::GetHeaderValue: the first number on the line (0 when there is none)."""
     tok = line.split()
@@ -607,7 +660,9 @@ class OracleSR:
         if abs(normal) > 1:
             raise ValueError("'normal' must be -1, 0, or 1")
         if x0x1x2 is not None:
-            raise ValueError("x0x1x2 surfaces are not part of the oracle")
+            if len(x0x1x2) != 3:
+                raise ValueError("'x0x1x2' must have 3 XYZ points defined correctly")
+            return rectangle_x0x1x2(nx1, nx2, x0x1x2[0], x0x1x2[1], x0x1x2[2], r, t, normal)
         if pd and (w1 <= 0 or w2 <= 0):
             raise ValueError("'width' must be > 0")
         return rectangle(plane, nx1, nx2, w1, w2, r, t, normal)
@@ -656,6 +711,45 @@ class OracleSR:
         self.last_levels = lv
         pos = xyz if dim == 3 else x1x2
         return [[list(pos[i]), float(out[i])] for i in range(n)]
+
+
+    def _points_call(self, points, rotations, translation, invert):
+        r = _v3(rotations) if rotations else [0.0, 0.0, 0.0]
+        t = _v3(translation) if translation else [0.0, 0.0, 0.0]
+        return surface_points(points, r, t, invert)
+
+    def calculate_flux(self, energy_eV=0.0, points=[], normal=0, rotations=None, translation=None, nparticles=0,
+                       nthreads=0, gpu=-1, ngpu=None, precision=0.01, max_level=-2, max_level_extended=0, ofile="",
+                       bofile="", quantity="flux"):
+        """Flux at arbitrary points, polarization 'all' (the reference binding of calculate_flux raises
+        before computing; this is the flux its CalculateFlux would give)."""
+        xyz, _ = self._points_call(points, rotations, translation, False)
+        q = _quantity(quantity)
+        n = xyz.shape[0]
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        h, p = np.array([1.0, 0.0, 0.0]), np.array([0.0, 0.0, 1.0])
+        self._check(self._lib.orc_flux(self._h, _dp(np.ascontiguousarray(xyz)), n, float(energy_eV), 0, 0.0, _dp(h), _dp(p),
+                                       float(precision), int(max_level), int(max_level_extended), int(nparticles), q,
+                                       _dp(out), lv.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.last_levels = lv
+        return [[list(xyz[i]), float(out[i])] for i in range(n)]
+
+    def calculate_power_density(self, points, normal=0, rotations=None, translation=None, nparticles=0, gpu=-1,
+                                ngpu=None, nthreads=0, precision=0.01, max_level=-2, max_level_extended=0,
+                                quantity="power density", ofile="", bofile=""):
+        """Power density at arbitrary points with normals (src/OSCARSSR_Python.cc:6105-6370)."""
+        xyz, nrm = self._points_call(points, rotations, translation, normal == -1)
+        q = _quantity(quantity, pd=True)
+        n = xyz.shape[0]
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        self._check(self._lib.orc_power_density(self._h, _dp(np.ascontiguousarray(xyz)), _dp(np.ascontiguousarray(nrm)), n,
+                                                int(normal != 0), float(precision), int(max_level),
+                                                int(max_level_extended), int(nparticles), q, _dp(out),
+                                                lv.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.last_levels = lv
+        return [[list(xyz[i]), float(out[i])] for i in range(n)]
 
 
 def reference_module():

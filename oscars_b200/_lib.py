@@ -74,6 +74,8 @@ SIGNATURES = {
     "osc_calculate_trajectory": (I, [VP]),
     "osc_get_trajectory": (I, [VP, DP, LL, LLP]),
     "osc_surface_rectangle": (I, [ctypes.c_char_p, I, I, D, D, DP, DP, I, DP, DP, DP]),
+    "osc_surface_x0x1x2": (I, [I, I, DP, DP, DP, I, DP, DP, DP]),
+    "osc_surface_points": (I, [LL, DP, DP, DP, DP, I, DP, DP]),
     "osc_flux": (I, [VP, DP, LL, D, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
     "osc_spectrum": (I, [VP, DP, DP, LL, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
     "osc_flux_multi": (I, [VP, DP, LL, DP, LL, ctypes.POINTER(RadOpts), I, DP, I32P, LLP]),

@@ -391,6 +391,38 @@ OSC_API int osc_surface_rectangle(const char* plane, int nx1, int nx2, double wi
   }
 }
 
+OSC_API int osc_surface_x0x1x2(int nx1, int nx2, const double x0x1x2[9], const double rotations[3],
+                               const double translation[3], int normal, double* xyz, double* normals, double* x1x2) {
+  try {
+    if (!x0x1x2) {
+      g_create_error = "bad buffers";
+      return OSC_ERR_INVALID;
+    }
+    const double zero[3] = {0, 0, 0};
+    osc::surface_x0x1x2(nx1, nx2, V3(x0x1x2), V3(x0x1x2 + 3), V3(x0x1x2 + 6), V3(rotations ? rotations : zero),
+                        V3(translation ? translation : zero), normal, xyz, normals, x1x2);
+    return OSC_OK;
+  } catch (const osc::Error& e) {
+    g_create_error = e.msg;
+    return e.code;
+  } catch (...) {
+    g_create_error = "unexpected error";
+    return OSC_ERR_INVALID;
+  }
+}
+
+OSC_API int osc_surface_points(long long n, const double* points, const double* normals, const double rotations[3],
+                               const double translation[3], int invert_normals, double* xyz, double* normals_out) {
+  if (n < 0 || (n > 0 && (!points || !normals || !xyz || !normals_out))) {
+    g_create_error = "bad buffers";
+    return OSC_ERR_INVALID;
+  }
+  const double zero[3] = {0, 0, 0};
+  osc::surface_points(n, points, normals, V3(rotations ? rotations : zero), V3(translation ? translation : zero),
+                      invert_normals != 0, xyz, normals_out);
+  return OSC_OK;
+}
+
 OSC_API int osc_flux(osc_ctx* ctx, const double* obs_xyz, long long n_obs, double energy_eV, const osc_rad_opts* opts,
                      double* out, int32_t* level_out, long long* n_not_converged) {
   return guarded(ctx, [&] {

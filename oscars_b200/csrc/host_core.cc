@@ -844,4 +844,52 @@ void surface_rectangle(const std::string& plane_in, int nx1, int nx2, double w1,
   }
 }
 
+// Rectangle from three points (TSurfacePoints_Rectangle::Init(NX1, NX2, X0, X1, X2, Normal) and
+// GetXYZ / GetX1 / GetX2, src/TSurfacePoints_Rectangle.cc:76-127, 280-317): the three points are
+// rotated and translated first, as the binding does (src/OSCARSSR_Python.cc:6652-6658).
+void surface_x0x1x2(int nx1, int nx2, Vec3 x0, Vec3 x1, Vec3 x2, Vec3 rot, Vec3 trans, int normal, double* xyz,
+                    double* normals, double* x1x2) {
+  if (nx1 < 2 || nx2 < 2) throw Error{OSC_ERR_INVALID, "'npoints' must be >= 2 in each direction with 'x0x1x2'"};
+  if (normal != -1 && normal != 0 && normal != 1)
+    throw Error{OSC_ERR_INVALID, "fNormal is of the incorrect form.  Must be -1, 0, 1"};
+  x0 = rotate_xyz(x0, rot) + trans;
+  x1 = rotate_xyz(x1, rot) + trans;
+  x2 = rotate_xyz(x2, rot) + trans;
+  const double w1 = mag(x1 - x0), w2 = mag(x2 - x0);
+  const double s1 = w1 / (nx1 - 1), s2 = w2 / (nx2 - 1);
+  const Vec3 v1 = (x1 - x0) / (double)(nx1 - 1), v2 = (x2 - x0) / (double)(nx2 - 1);
+  Vec3 nv = unit(cross(v1, v2));
+  if (normal == -1) nv = nv * -1;
+  const double m1 = mag(v1), m2 = mag(v2);
+  const int64_t n = (int64_t)nx1 * nx2;
+  for (int64_t i = 0; i < n; ++i) {
+    const int ix1 = (int)(i / nx2), ix2 = (int)(i % nx2);
+    if (xyz) {
+      const Vec3 p = (x0 + v1 * (double)ix1) + v2 * (double)ix2;
+      xyz[3 * i] = p.x; xyz[3 * i + 1] = p.y; xyz[3 * i + 2] = p.z;
+    }
+    if (normals) { normals[3 * i] = nv.x; normals[3 * i + 1] = nv.y; normals[3 * i + 2] = nv.z; }
+    if (x1x2) {
+      x1x2[3 * i] = s1 * ix1 - m1 * (nx1 - 1) / 2.;
+      x1x2[3 * i + 1] = s2 * ix2 - m2 * (nx2 - 1) / 2.;
+      x1x2[3 * i + 2] = 0;
+    }
+  }
+}
+
+// Arbitrary surface points with normals as the calculate_flux / calculate_power_density bindings
+// take them (src/OSCARSSR_Python.cc:7730-7750, 6225-6250): point and normal rotated, the normal
+// reversed when invert_normals, the point translated.
+void surface_points(int64_t n, const double* pts, const double* nrm, Vec3 rot, Vec3 trans, bool invert_normals,
+                    double* xyz, double* normals) {
+  for (int64_t i = 0; i < n; ++i) {
+    Vec3 X = rotate_xyz(v3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), rot);
+    Vec3 N = rotate_xyz(v3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]), rot);
+    if (invert_normals) N = N * -1;
+    X = X + trans;
+    xyz[3 * i] = X.x; xyz[3 * i + 1] = X.y; xyz[3 * i + 2] = X.z;
+    normals[3 * i] = N.x; normals[3 * i + 1] = N.y; normals[3 * i + 2] = N.z;
+  }
+}
+
 }  // namespace osc

@@ -175,5 +175,11 @@ void parallel_tasks(int n, const std::function<void(int)>& fn);
 // Rectangle surface (TSurfacePoints_Rectangle).  Throws osc::Error.
 void surface_rectangle(const std::string& plane, int nx1, int nx2, double w1, double w2, Vec3 rot,
                        Vec3 trans, int normal, double* xyz, double* normals, double* x1x2);
+// Rectangle from three points (TSurfacePoints_Rectangle x0x1x2 form).  Throws osc::Error.
+void surface_x0x1x2(int nx1, int nx2, Vec3 x0, Vec3 x1, Vec3 x2, Vec3 rot, Vec3 trans, int normal, double* xyz,
+                    double* normals, double* x1x2);
+// Arbitrary points with normals, rotated / translated as the point-list bindings do.
+void surface_points(int64_t n, const double* pts, const double* nrm, Vec3 rot, Vec3 trans, bool invert_normals,
+                    double* xyz, double* normals);
 
 }  // namespace osc

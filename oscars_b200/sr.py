@@ -23,7 +23,7 @@ import sys
 
 import numpy as np
 
-from . import _lib
+from . import _lib, fileio
 from ._lib import BeamDesc, Context, FieldDesc, RadOpts, dptr, i32ptr
 
 _ANGLE_UNSET = 112188979912321.0  # binding sentinel for "angle not given" (:5662)
@@ -358,9 +358,13 @@ class sr:
         return [[float(a[0, i]), a[1:4, i].tolist(), a[4:7, i].tolist(), a[7:10, i].tolist()] for i in range(a.shape[1])]
 
     def calculate_trajectory(self, ofile="", bofile="", oformat=""):
-        if ofile or bofile:
-            raise ValueError("trajectory file output is not part of this GPU build's drop-in surface")
         self._ctx.call("osc_calculate_trajectory")
+        if ofile or bofile:  # TParticleTrajectoryPoints::WriteToFile / WriteToFileBinary formats
+            a = self.trajectory_array()
+            if ofile:
+                fileio.write_trajectory_text(ofile, a, oformat)
+            if bofile:
+                fileio.write_trajectory_binary(bofile, a, oformat)
         return self.get_trajectory()
 
     # ---- radiation -------------------------------------------------------------------------------
@@ -440,8 +444,10 @@ class sr:
         self._ctx.call("osc_spectrum", dptr(O), dptr(E), E.size, ctypes.byref(o), dptr(out), i32ptr(lv), ctypes.byref(nnc))
         self.last_levels = lv
         self._report(nnc)
-        if ofile or bofile:
-            raise ValueError("spectrum file output is not part of this GPU build's drop-in surface")
+        if ofile:
+            fileio.write_spectrum_text(ofile, E, out)
+        if bofile:
+            fileio.write_spectrum_binary(bofile, E, out)
         if return_numpy:
             return E, out
         return [[float(E[i]), float(out[i])] for i in range(E.size)]
@@ -459,17 +465,111 @@ class sr:
             w1, w2 = float(width[0]), float(width[1])
         if abs(normal) > 1:
             raise ValueError("'normal' must be -1, 0, or 1")
-        if x0x1x2 is not None:
-            raise ValueError("'x0x1x2' surfaces are not part of this GPU build's drop-in surface")
+        n = nx1 * nx2
+        if x0x1x2 is not None:  # the three-point form (src/OSCARSSR_Python.cc:6633-6658, 8146-8172)
+            if len(x0x1x2) != 3:
+                raise ValueError("'x0x1x2' must have 3 XYZ points defined correctly")
+            pts = np.array([_vec3(p, "x0x1x2") for p in x0x1x2], dtype=np.float64).ravel()
+            xyz, nrm, x12 = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
+            rc = _lib.lib().osc_surface_x0x1x2(nx1, nx2, dptr(pts), dptr(r), dptr(t), int(normal), dptr(xyz), dptr(nrm),
+                                               dptr(x12))
+            if rc != 0:
+                raise ValueError(_lib.lib().osc_last_error(None).decode())
+            return xyz, nrm, x12
         if w1 <= 0 or w2 <= 0:
             raise ValueError("'width' must be > 0" if pd else "'width' must be given as [w1, w2] with both > 0")
-        n = nx1 * nx2
         xyz, nrm, x12 = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
         rc = _lib.lib().osc_surface_rectangle(plane.encode(), nx1, nx2, w1, w2, dptr(r), dptr(t), int(normal),
                                               dptr(xyz), dptr(nrm), dptr(x12))
         if rc != 0:
             raise ValueError(_lib.lib().osc_last_error(None).decode())
         return xyz, nrm, x12
+
+    @staticmethod
+    def _write_points(ofile, bofile, pos, out, dim):
+        """ofile / bofile of the flux and power-density calls (T3DScalarContainer formats)."""
+        if ofile:
+            fileio.write_points_text(ofile, pos, out, dim)
+        if bofile:
+            fileio.write_points_binary(bofile, pos, out, dim)
+
+    def _surface_points(self, points, rotations, translation, invert_normals):
+        """Points with normals of the point-list calls (src/OSCARSSR_Python.cc:7728-7755, 6223-6255)."""
+        r = np.array(_vec3(rotations, "rotations") if rotations else [0.0, 0.0, 0.0])
+        t = np.array(_vec3(translation, "translation") if translation else [0.0, 0.0, 0.0])
+        pts, nrm = [], []
+        for item in points:
+            if len(item) != 2:
+                raise ValueError("Incorrect format in 'points'")
+            if len(item[0]) != 3 or len(item[1]) != 3:
+                raise ValueError("Incorrect format in 'points': Point or Normal does not have 3 elements")
+            pts.append([float(v) for v in item[0]])
+            nrm.append([float(v) for v in item[1]])
+        n = len(pts)
+        P = np.ascontiguousarray(np.array(pts, dtype=np.float64).reshape(-1))
+        N = np.ascontiguousarray(np.array(nrm, dtype=np.float64).reshape(-1))
+        xyz, nout = np.zeros(3 * n), np.zeros(3 * n)
+        if n:
+            rc = _lib.lib().osc_surface_points(n, dptr(P), dptr(N), dptr(r), dptr(t), int(bool(invert_normals)),
+                                               dptr(xyz), dptr(nout))
+            if rc != 0:
+                raise ValueError(_lib.lib().osc_last_error(None).decode())
+        return xyz, nout
+
+    def calculate_flux(self, energy_eV=0.0, points=[], normal=0, rotations=None, translation=None, nparticles=0,
+                       nthreads=0, gpu=-1, ngpu=None, precision=0.01, max_level=-2, max_level_extended=0, ofile="",
+                       bofile="", quantity="flux", *, compute="fp64", return_numpy=False, shard=None):
+        """Flux at arbitrary points ([[x, y, z], [nx, ny, nz]] each, rotated then translated), total
+        polarization; returns [[x, y, z], F] (src/OSCARSSR_Python.cc:7628).  The reference binding
+        raises before computing ("not currently used", :7812); here the flux is computed."""
+        if self._nbeams < 1:
+            raise ValueError("No particle beam defined")
+        xyz, _ = self._surface_points(points, rotations, translation, False)
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        self._check_gpu(gpu, nthreads)
+        q = _quantity(quantity)
+        o = self._opts("", _ANGLE_UNSET, None, None, precision, max_level, max_level_extended, nparticles, q, compute,
+                       shard)
+        n = xyz.size // 3
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        nnc = ctypes.c_longlong()
+        if n:
+            self._ctx.call("osc_flux", dptr(xyz), n, float(energy_eV), ctypes.byref(o), dptr(out), i32ptr(lv),
+                           ctypes.byref(nnc))
+        self.last_levels = lv
+        self._report(nnc)
+        self._write_points(ofile, bofile, xyz, out, 3)
+        return self._points_result(xyz, out, return_numpy)
+
+    def calculate_power_density(self, points, normal=0, rotations=None, translation=None, nparticles=0, gpu=-1,
+                                ngpu=None, nthreads=0, precision=0.01, max_level=-2, max_level_extended=0,
+                                quantity="power density", ofile="", bofile="", *, compute="fp64", return_numpy=False,
+                                shard=None):
+        """Power density [W/mm^2] at arbitrary points with surface normals ([[x, y, z], [nx, ny, nz]]
+        each, rotated then translated; normal = -1 reverses the normals, normal != 0 makes it
+        directional), src/OSCARSSR_Python.cc:6105-6370; returns [[x, y, z], P]."""
+        if self._nbeams < 1:
+            raise ValueError("No particle beam defined")
+        xyz, nrm = self._surface_points(points, rotations, translation, normal == -1)
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        self._check_gpu(gpu, nthreads)
+        q = _quantity(quantity, pd=True)
+        o = self._opts("", _ANGLE_UNSET, None, None, precision, max_level, max_level_extended, nparticles, q, compute,
+                       shard)
+        n = xyz.size // 3
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        nnc = ctypes.c_longlong()
+        if n:
+            self._ctx.call("osc_power_density", dptr(xyz), dptr(nrm), n, int(normal != 0), ctypes.byref(o), dptr(out),
+                           i32ptr(lv), ctypes.byref(nnc))
+        self.last_levels = lv
+        self._report(nnc)
+        self._write_points(ofile, bofile, xyz, out, 3)
+        return self._points_result(xyz, out, return_numpy)
 
     @staticmethod
     def _points_result(pos, out, return_numpy):
@@ -502,8 +602,7 @@ class sr:
         self._ctx.call("osc_flux", dptr(xyz), n, float(energy_eV), ctypes.byref(o), dptr(out), i32ptr(lv), ctypes.byref(nnc))
         self.last_levels = lv
         self._report(nnc)
-        if ofile or bofile:
-            raise ValueError("flux file output is not part of this GPU build's drop-in surface")
+        self._write_points(ofile, bofile, xyz if dim == 3 else x12, out, dim)
         return self._points_result(xyz if dim == 3 else x12, out, return_numpy)
 
     def calculate_power_density_rectangle(self, npoints=[51, 51], plane="XY", width=None, x0x1x2=None,
@@ -530,8 +629,7 @@ class sr:
                        i32ptr(lv), ctypes.byref(nnc))
         self.last_levels = lv
         self._report(nnc)
-        if ofile or bofile:
-            raise ValueError("power density file output is not part of this GPU build's drop-in surface")
+        self._write_points(ofile, bofile, xyz if dim == 3 else x12, out, dim)
         return self._points_result(xyz if dim == 3 else x12, out, return_numpy)
 
     def last_stats(self):

@@ -111,6 +111,28 @@ GRID3D = ("add_bfield_file", dict(ifile="grid3d.txt", iformat="OSCARS", rotation
                                   translation=[0.0001, 0, 0], scale=[1, 1, 1, 1, 1.1, 1]))
 HALFSCALE = ("add_bfield_halfscale", dict(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, phase=-math.pi / 2))
 
+# A rectangle 8 mm x 6 mm near z = 30 m, slightly skewed and tilted, given by three corners.
+X0X1X2 = [[-0.004, -0.003, 30.0], [0.004, -0.0025, 30.002], [-0.0038, 0.003, 29.998]]
+
+
+def _arc_points(flip_every=0):
+    """7 x 5 points on a cylinder of radius 30 m about the y axis (angles -0.25 .. 0.25 mrad, y within
+    +-3 mm), normals pointing at the origin; with flip_every = k every k-th normal points away."""
+    pts = []
+    for i in range(7):
+        phi = -2.5e-4 + 5e-4 * i / 6
+        for j in range(5):
+            y = -0.003 + 0.006 * j / 4
+            n = [-math.sin(phi), 0.0, -math.cos(phi)]
+            if flip_every and (5 * i + j) % flip_every == 0:
+                n = [-v for v in n]
+            pts.append([[30 * math.sin(phi), y, 30 * math.cos(phi)], n])
+    return pts
+
+
+ARC_POINTS = _arc_points()
+ARC_POINTS_MIXED = _arc_points(3)
+
 CASES = {
     # trajectory of the planar undulator (checked through a subsample plus whole-array sums)
     "traj_und": UND_SETUP + [("calculate_trajectory", {})],
@@ -158,6 +180,13 @@ CASES = {
     # 41-period undulator with 82 half-period amplitude factors (the field-tuning configuration)
     "halfscale_traj": [HALFSCALE, BEAM] + traj() + [("calculate_trajectory", {})],
     "halfscale_flux": [HALFSCALE, BEAM] + traj() + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[11, 11], width=[0.002, 0.002], translation=[0, 0, 30], precision=0, max_level=11))],
+    # rectangles given by three points (x0x1x2), rotated and translated, and arbitrary point surfaces
+    "flux_x0x1x2": UND_SETUP + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[9, 7], x0x1x2=X0X1X2, rotations=[0.001, -0.002, 0.0005], translation=[0.0005, -0.0002, 0.1], dim=3))],
+    "flux_x0x1x2_dim2": UND_SETUP + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[9, 7], x0x1x2=X0X1X2))],
+    "pd_x0x1x2": UND_SETUP + [("calculate_power_density_rectangle", dict(npoints=[9, 9], x0x1x2=[[-0.005, -0.005, 30], [0.005, -0.005, 30], [-0.005, 0.005, 30]], normal=1))],
+    "pd_points": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, rotations=[0.0, 0.001, 0.0], translation=[0.0, 0.0005, 0.0]))],
+    "pd_points_directional": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS_MIXED, normal=1))],
+    "pd_points_inverted": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, normal=-1))],
 }
 
 
@@ -206,3 +235,14 @@ def adjoint_config():
     energies = np.linspace(0.95 * E1_U, 1.05 * E1_U, 8)
     return obs, energies, ADJ_LEVEL
 
+
+# ---- output files: (setup, call, kwargs) whose ofile / bofile the reference wrote (files.npz) ------
+FILE_CASES = {
+    "flux_rect_dim2": (UND_SETUP, "calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[11, 9], width=[0.01, 0.008], translation=[0, 0, 30])),
+    "flux_rect_dim3": (UND_SETUP, "calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[11, 9], width=[0.01, 0.008], translation=[0, 0, 30], dim=3)),
+    "pd_rect": (UND_SETUP, "calculate_power_density_rectangle", dict(npoints=[9, 9], width=[0.01, 0.01], translation=[0, 0, 30])),
+    "pd_points": (UND_SETUP, "calculate_power_density", dict(points=ARC_POINTS, normal=-1)),
+    "spectrum": (UND_SETUP, "calculate_spectrum", dict(obs=[0, 0, 30], energy_range_eV=[100, 3000], npoints=60)),
+    "traj_default": ([UND, BEAM] + traj(301), "calculate_trajectory", {}),
+    "traj_format": ([UND, BEAM] + traj(301), "calculate_trajectory", dict(oformat="t x bx BPY")),
+}

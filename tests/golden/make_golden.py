@@ -7,6 +7,8 @@ per-entry stop levels from a second ``quantity='level'`` call where the case ret
 
     python tests/golden/make_golden.py            # all cases
     python tests/golden/make_golden.py flux_und_41
+    python tests/golden/make_golden.py files      # the reference's output files (files.npz)
+    python tests/golden/make_golden.py adjoint_fd # finite-difference gradients (adjoint_fd.npz)
 """
 import os
 import subprocess
@@ -71,6 +73,32 @@ def make(name, S):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), pos=pos, val=val, **extra)
 
 
+def make_files(S):
+    """Output files written by the reference for FILE_CASES (ofile and bofile) -> files.npz: per case
+    the text and binary bytes and the returned result (positions / energies / trajectory and values)
+    that the files hold."""
+    import tempfile
+    from cases import FILE_CASES
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, (setup, call, kw) in FILE_CASES.items():
+            obj = S.sr(nthreads=1, gpu=0)
+            txt, binf = os.path.join(d, name + ".txt"), os.path.join(d, name + ".bin")
+            kw = dict(kw, ofile=txt, bofile=binf)
+            if call != "calculate_trajectory":
+                kw.setdefault("nthreads", 1)
+            res = run_case(obj, setup + [(call, kw)])
+            out[name + "/txt"] = np.frombuffer(open(txt, "rb").read(), dtype=np.uint8)
+            out[name + "/bin"] = np.frombuffer(open(binf, "rb").read(), dtype=np.uint8)
+            if call == "calculate_trajectory":
+                out[name + "/traj"] = np.array([[p[0]] + p[1] + p[2] + p[3] for p in res], dtype=np.float64).T
+            else:
+                pos, val = flatten(res)
+                out[name + "/pos"] = pos
+                out[name + "/val"] = val
+    np.savez_compressed(os.path.join(HERE, "files.npz"), **out)
+
+
 def make_adjoint(S):
     """Central finite differences of loss = sum (F(s) - F(1))^2 over the adjoint configuration, every
     one of the 82 half-period factors, with the reference's CPU path (the scaled undulator given to it
@@ -115,6 +143,10 @@ def main(argv):
     if argv[1:] == ["adjoint_fd"]:
         make_adjoint(S)
         print("wrote adjoint_fd")
+        return
+    if argv[1:] == ["files"]:
+        make_files(S)
+        print("wrote files")
         return
     names = argv[1:] or sorted(CASES)
     for n in names:

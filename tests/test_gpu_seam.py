@@ -10,9 +10,9 @@ build must have been made beforehand (make -C oscars_b200/seam REF=<OSCARS sourc
 only receives the built files.  The reference runs in a child process, because the CPU reference
 build the other tests load is also a package named `oscars`.
 
-Excluded: pd_und_directional -- the seam's power-density function carries no `Directional`
-argument (include/OSCARSSR_Cuda.h:56-63), so a directional request is answered non-directionally by
-the reference's GPU path and by this seam alike.
+Excluded: the directional power-density cases (normal != 0) -- the seam's power-density function
+carries no `Directional` argument (include/OSCARSSR_Cuda.h:56-63), so a directional request is
+answered non-directionally by the reference's GPU path and by this seam alike.
 """
 import os
 import subprocess
@@ -28,8 +28,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BUILD = os.path.join(ROOT, "oscars_b200", "seam", "_build")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 TOL = 1e-9
-EXCLUDED = {"pd_und_directional"}
-NAMES = sorted(k for k, v in CASES.items() if v[-1][0] != "calculate_trajectory" and k not in EXCLUDED)
+NAMES = sorted(k for k, v in CASES.items() if v[-1][0] != "calculate_trajectory"
+               and not (v[-1][0].startswith("calculate_power_density") and v[-1][1].get("normal", 0) != 0))
 
 
 @pytest.fixture(scope="module")
