@@ -626,10 +626,11 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
   FdWaveArgs w{};
   w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = obs_.as<double>(); w.omega = omega_.as<double>();
   w.n_e = n_e; w.n_items = N; w.act = nullptr; w.n_act = nullptr; w.first = 1; w.level = level;
-  w.tile_entries = 128; w.min_span = 32; w.target_units = 1; w.part = part_.as<double>(); w.err = cnt + 2;
-  w.work = work;
   const int fv = forced_variant[0] >= 0 ? forced_variant[0] : current_variant_[0];
-  check(launch_fd_wave_fp64(w, (int)std::min<int64_t>((N + 127) / 128, wave_grid(0, fv)), fv, st), "adjoint forward");
+  const int te = fp64_entries_per_cta(fv);  // entries per CTA of that variant
+  w.tile_entries = te; w.min_span = 32; w.target_units = 1; w.part = part_.as<double>(); w.err = cnt + 2;
+  w.work = work;
+  check(launch_fd_wave_fp64(w, (int)std::min<int64_t>((N + te - 1) / te, wave_grid(0, fv)), fv, st), "adjoint forward");
   check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");  // counters start at zero
   const double dtL = dt_inclusive(tstart_, tstop_, level);
   const double c0 = P.q / (four_pi() * kC * kEps0 * kSqrt2Pi);

@@ -728,8 +728,8 @@ OSC_API int osc_variant_name(int kind, int variant, char* name, long long capaci
     if (kind != 0 && kind != 2 && kind != 3)
       throw osc::Error{OSC_ERR_INVALID, "kind must be 0 (fp64), 2 (mixed) or 3 (batched mixed)"};
     if (variant < 0 || variant >= n_variants_of(kind)) throw osc::Error{OSC_ERR_RANGE, "variant out of range"};
-    static const char* const kFp64[] = {"k_fd_wave_fp64<1>", "k_fd_wave_fp64<6>", "k_fd_wave_fp64<7>",
-                                        "k_fd_wave_fp64<8>"};
+    static const char* const kFp64[] = {"k_fd_wave_fp64<1,7>", "k_fd_wave_fp64<2,7>", "k_fd_wave_fp64<4,7>",
+                                        "k_fd_wave_fp64<4,5>"};
     static const char* const kBatch[] = {"k_batch_wave<4,4>", "k_batch_wave<4,1>", "k_batch_wave<2,4>",
                                          "k_batch_wave<1,4>"};
     static_assert(sizeof(kFp64) / sizeof(kFp64[0]) == osc::kFp64Variants, "FP64 variant names");

@@ -241,9 +241,10 @@ void polarization_vector(const osc_rad_opts& o, double P[6], bool& project) {
 // host round trip; entries still unconverged after it make the host extend the cache.
 constexpr int kPrefillLevel = 14;
 constexpr int kMinSpan = 32;
-// Mixed waves: spans of at least one staged chunk's worth of pairs, so that a unit's fixed costs (its
-// first copy, the partial store, the tile counter) stay small beside its arithmetic.
-constexpr int kMinSpanMixed = 128;
+// Sample-split flux / spectrum waves (FP64 and mixed): spans of at least one staged chunk, so that a
+// unit's fixed costs (its first copy, the partial store, the tile counter) stay small beside its
+// arithmetic.
+constexpr int kMinSpanSplit = 128;
 
 int Engine::wave_grid(int kind, int variant) {
   if (wave_grid_[kind][variant] == 0) {
@@ -326,8 +327,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   if (mixed) ensure_mixed(Lpre);
   else ensure_levels(Lpre);
   const int resident = wave_grid(kind, variant);  // CTAs resident at once on the device
-  const int tile = mixed ? mixed_entries_per_cta(variant) : 128;
-  const int min_span = mixed ? kMinSpanMixed : kMinSpan;
+  const int tile = mixed ? mixed_entries_per_cta(variant) : rq.power_density ? 128 : fp64_entries_per_cta(variant);
+  const int min_span = rq.power_density ? kMinSpan : kMinSpanSplit;
   const int64_t target = 4 * (int64_t)resident;   // >= 4 waves of equal units per launch
   const int64_t N = n_items;
   // Partial-sum buffer: a wave has tiles x spans units with spans the smallest power of two reaching
@@ -422,7 +423,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
       f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.level_max = level_max; f.work_reset = nullptr;
-      f.dmax_spans_joined = mixed;
+      f.dmax_spans_joined = 1;  // the flux waves carry the step into each part across groups and spans
       auto ev = timed_begin(st);
       const int g = grid_for(L);
       if (mixed) check(launch_fd_wave_mixed(w, frame_, g, variant, st), "flux wave (mixed)");

@@ -182,6 +182,7 @@ int mixed_entries_per_cta(int variant);
 const char* mixed_variant_name(int variant);  // kernel and template arguments of a variant
 int mixed_blocks_per_sm(int variant);
 int fp64_blocks_per_sm(bool power_density, int variant);
+int fp64_entries_per_cta(int variant);
 
 cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
                               int64_t s_end, double* lev, int64_t cap, int extended_level,

@@ -111,11 +111,34 @@ __device__ __forceinline__ void stage_issue(Stage<NARR, CH>& st, int b, const do
 constexpr int kFdThreads = 128;
 constexpr int kFdChunk = 128;
 
-template <int MINB>
+// Phase -w (t + D/c) of one staged sample for an observer, with the operations of the sum below.
+__device__ __forceinline__ double fd_phase(double T, double X, double Y, double Z, double Ox, double Oy, double Oz,
+                                           double mw) {
+  const double Rx = __dsub_rn(Ox, X), Ry = __dsub_rn(Oy, Y), Rz = __dsub_rn(Oz, Z);
+  const double D = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz)));
+  return __dmul_rn(mw, __dadd_rn(T, __ddiv_rn(D, kCLight)));
+}
+
+// Sample-split FP64 sum: the CTA's 128 threads form SUB groups of TE = 128 / SUB threads, one entry
+// per thread; group g takes the g-th of SUB equal parts of every staged chunk of the 10 level arrays.
+// Each part starts from the phase of the sample before it (the chunk's previous sample, the previous
+// chunk's last one, or the span's predecessor read from the level cache), so the largest phase step
+// of a span covers exactly the consecutive pairs of the serial order and spans need no joining
+// (dmax_spans_joined); the groups' sums are combined in shared memory in group order.  Fused waves
+// finalize their tiles with all threads (fused_unit_done_grouped); unfused waves store entry-major
+// partials for k_fd_finalize.
+template <int SUB, int MINB>
 __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A) {
+  constexpr int TE = kFdThreads / SUB;
+  if (A.tile_entries != TE) {  // the host sized the partials for another tile
+    if (threadIdx.x == 0) atomicOr(A.err, kErrPlan);
+    return;
+  }
   __shared__ __align__(16) Stage<10, kFdChunk> st;
+  __shared__ double red[SUB > 1 ? SUB - 1 : 1][7][TE];
   __shared__ int s_last;
   const int tid = threadIdx.x;
+  const int grp = tid / TE, q = tid % TE;
   if (A.fused && blockIdx.x == 0 && tid == 0) {  // counters of the following wave
     if (A.zero_u32) *A.zero_u32 = 0;
     if (A.zero_u64) *A.zero_u64 = 0;
@@ -124,7 +147,7 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
   // the plan is uniform over the CTA; keeping it in shared memory frees the registers its
   // fields would otherwise hold across the sample loop
   __shared__ WavePlan P;
-  if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, kFdThreads, A.target_units, A.min_span);
+  if (threadIdx.x == 0) P = wave_plan(A.first, A.level, n_act, TE, A.target_units, A.min_span);
   __syncthreads();
   const int64_t units = P.tiles * P.spans;
   if (tid == 0) {
@@ -143,7 +166,7 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
     if (u >= units) break;
     const int64_t tile = u / P.spans;
     const int span = (int)(u % P.spans);
-    const int64_t slot = tile * kFdThreads + tid;
+    const int64_t slot = tile * TE + q;
     const bool live = slot < n_act;
     const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
     const int64_t io = item / A.n_e, ie = item % A.n_e;
@@ -153,9 +176,19 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
       const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
       const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
       double sxr = 0, sxi = 0, syr = 0, syi = 0, szr = 0, szi = 0;
-      double first_phase = 0, last_phase = 0, dmax = 0;
-      bool have = false;
+      double dmax = 0;
+      bool any = false;
       const int64_t nchunks = b1 > b0 ? (b1 - b0 + kFdChunk - 1) / kFdChunk : 0;
+      // phase of the sample before a part that starts a chunk: the span's predecessor (span > 0;
+      // sample 0, the unused slot, never is one), then the previous chunk's last sample
+      double carry = 0;
+      bool have_carry = false;
+      if (live && span > 0 && nchunks > 0 && b0 - 1 >= 1) {
+        const int64_t s = b0 - 1;
+        const double* L = A.lev;
+        carry = fd_phase(L[s], L[A.cap + s], L[2 * A.cap + s], L[3 * A.cap + s], Ox, Oy, Oz, mw);
+        have_carry = true;
+      }
       if (tid == 0 && nchunks > 0) {
         const int64_t lo = b0, hi = min(b1, b0 + kFdChunk);
         stage_issue<10, kFdChunk>(st, 0, A.lev, A.cap, lo & ~(int64_t)1, (hi + 1) & ~(int64_t)1);
@@ -183,22 +216,30 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
         const double* sAx = st.v[buf][7];
         const double* sAy = st.v[buf][8];
         const double* sAz = st.v[buf][9];
-        const int j0 = (int)(max(lo, (int64_t)1) - lo_al);  // sample 0 is the unused slot
-        const int j1 = (int)(hi - lo_al);
-        if (live) {
+        const int ja = (int)(max(lo, (int64_t)1) - lo_al);  // sample 0 is the unused slot
+        const int jb = (int)(hi - lo_al);
+        const int j0 = ja + ((jb - ja) * grp) / SUB, j1 = ja + ((jb - ja) * (grp + 1)) / SUB;  // this group's part
+        if (live && j0 < j1) {
+          double last;
+          bool have;
+          if (j0 > ja) {
+            last = fd_phase(sT[j0 - 1], sX[j0 - 1], sY[j0 - 1], sZ[j0 - 1], Ox, Oy, Oz, mw);
+            have = true;
+          } else {
+            last = carry;
+            have = have_carry;
+          }
           for (int j = j0; j < j1; ++j) {
             const double T = sT[j];
             const double Rx = __dsub_rn(Ox, sX[j]), Ry = __dsub_rn(Oy, sY[j]), Rz = __dsub_rn(Oz, sZ[j]);
             const double D = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz)));
             const double ph = __dmul_rn(mw, __dadd_rn(T, __ddiv_rn(D, kCLight)));
             if (have) {
-              const double dp = fabs(__dsub_rn(ph, last_phase));
+              const double dp = fabs(__dsub_rn(ph, last));
               dmax = dp > dmax ? dp : dmax;
-            } else {
-              first_phase = ph;
-              have = true;
             }
-            last_phase = ph;
+            have = true;
+            last = ph;
             const double bx = sBx[j], by = sBy[j], bz = sBz[j];
             const double nx = __ddiv_rn(Rx, D), ny = __ddiv_rn(Ry, D), nz = __ddiv_rn(Rz, D);
             const double b2 = __dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz));
@@ -228,21 +269,46 @@ __global__ void __launch_bounds__(kFdThreads, MINB) k_fd_wave_fp64(FdWaveArgs A)
             syr = fma(ey, cs, syr); syi = fma(ey, sn, syi);
             szr = fma(ez, cs, szr); szi = fma(ez, sn, szi);
           }
+          any = true;
+        }
+        if (live && c + 1 < nchunks) {  // a full chunk: its last sample precedes the next chunk
+          const int jl = jb - 1;
+          carry = fd_phase(sT[jl], sX[jl], sY[jl], sZ[jl], Ox, Oy, Oz, mw);
+          have_carry = true;
         }
         __syncthreads();  // everyone is done with `buf` before it is refilled
       }
-      if (live) {
+      // combine the groups' sums in group order; group 0 stores the span's partial
+      double S[6] = {sxr, sxi, syr, syi, szr, szi};
+      double dm = any ? dmax : -1.0;
+      if (SUB > 1) {
+        if (grp > 0) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) red[grp - 1][k][q] = S[k];
+          red[grp - 1][6][q] = dm;
+        }
+        __syncthreads();
+        if (grp == 0)
+          for (int o = 0; o < SUB - 1; ++o) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) S[k] += red[o][k][q];
+            dm = fmax(dm, red[o][6][q]);
+          }
+        __syncthreads();
+      }
+      if (live && grp == 0) {
         // entry-major for the finalize kernel (an entry's spans contiguous); tile-major when fused
-        double* p = A.fused ? A.part + fused_part_index(P, tile, g, span, 0, tid, kFdThreads)
+        double* p = A.fused ? A.part + fused_part_index(P, tile, g, span, 0, q, TE)
                             : A.part + (slot * P.nseg * P.spans + g * P.spans + span) * kFdPartials;
-        const int64_t cs = A.fused ? kFdThreads : 1;  // stride between components
-        p[0] = sxr; p[cs] = sxi; p[2 * cs] = syr; p[3 * cs] = syi; p[4 * cs] = szr; p[5 * cs] = szi;
-        p[6 * cs] = have ? first_phase : 0.0;
-        p[7 * cs] = have ? last_phase : 0.0;
-        p[8 * cs] = have ? dmax : -1.0;  // -1 marks an empty span
+        const int64_t cs = A.fused ? TE : 1;  // stride between components
+#pragma unroll
+        for (int k = 0; k < 6; ++k) p[k * cs] = S[k];
+        p[6 * cs] = 0.0;
+        p[7 * cs] = 0.0;
+        p[8 * cs] = dm;  // -1 marks an empty span
       }
     }
-    if (A.fused) fused_unit_done<1, kFdThreads>(A, P, tile, n_act, &s_last);
+    if (A.fused) fused_unit_done_grouped<kFdThreads>(A, P, tile, n_act, &s_last, TE, &red[0][0][0]);
   }
 }
 
@@ -501,15 +567,18 @@ cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, dou
   return cudaGetLastError();
 }
 
-// Compiled variants of the FP64 wave kernel: minimum resident CTAs per SM (register cap).
-static const int kFp64MinBlocks[kFp64Variants] = {1, 6, 7, 8};
+// Compiled variants of the FP64 wave kernel: (groups SUB of 128 / SUB entries, minimum CTAs per SM).
+// Variant 0 keeps 128 entries per CTA (the allocation-free entry point sizes its partials for it).
+static const int kFp64Sub[kFp64Variants] = {1, 2, 4, 4};
+
+int fp64_entries_per_cta(int variant) { return dev::kFdThreads / kFp64Sub[variant]; }
 
 cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int grid, int variant, cudaStream_t st) {
   switch (variant) {
-    case 1: dev::k_fd_wave_fp64<6><<<grid, dev::kFdThreads, 0, st>>>(a); break;
-    case 2: dev::k_fd_wave_fp64<7><<<grid, dev::kFdThreads, 0, st>>>(a); break;
-    case 3: dev::k_fd_wave_fp64<8><<<grid, dev::kFdThreads, 0, st>>>(a); break;
-    default: dev::k_fd_wave_fp64<1><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+    case 1: dev::k_fd_wave_fp64<2, 7><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+    case 2: dev::k_fd_wave_fp64<4, 7><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+    case 3: dev::k_fd_wave_fp64<4, 5><<<grid, dev::kFdThreads, 0, st>>>(a); break;
+    default: dev::k_fd_wave_fp64<1, 7><<<grid, dev::kFdThreads, 0, st>>>(a); break;
   }
   return cudaGetLastError();
 }
@@ -541,13 +610,12 @@ int fp64_blocks_per_sm(bool power_density, int variant) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_pd_wave_fp64, dev::kPdThreads, 0);
   } else {
     switch (variant) {
-      case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<6>, dev::kFdThreads, 0); break;
-      case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<7>, dev::kFdThreads, 0); break;
-      case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<8>, dev::kFdThreads, 0); break;
-      default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<1>, dev::kFdThreads, 0); break;
+      case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<2, 7>, dev::kFdThreads, 0); break;
+      case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<4, 7>, dev::kFdThreads, 0); break;
+      case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<4, 5>, dev::kFdThreads, 0); break;
+      default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_fp64<1, 7>, dev::kFdThreads, 0); break;
     }
   }
-  (void)kFp64MinBlocks;
   return n > 0 ? n : 1;
 }
 
