@@ -663,10 +663,12 @@ def tuning_cpu_reference(every=16, h=1e-3):
     return time.perf_counter() - t0, 82 * every, cores
 
 
-def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, check_level=12):
+def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, check_level=12, particles=BEAM_PARTICLES,
+             quick=False):
     """EPU beam, 10k particles: mixed (batched) timed on the device and end to end; FP64 (reference
     path, host RK4 per particle) end to end on the first `fp64_particles`; mixed vs FP64 error at a
-    fixed level on `check_particles`."""
+    fixed level on `check_particles`.  `particles` < 10000 and `quick` (the mixed timing alone) give
+    the small cases of profiler runs."""
     import numpy as np
     from oscars_b200.sr import sr
     s = sr(gpu=1, device=local)
@@ -677,16 +679,19 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
         s.set_seed(1)
         return s.calculate_flux_rectangle(nparticles=np_, compute=compute, **dict(kw, **extra))
     for _ in range(warmup):
-        run(BEAM_PARTICLES, "mixed")
+        run(particles, "mixed")
     dev_ms = wall = 0.0
     samples = launches = 0
     with ClockSampler(local) as clk:
         for _ in range(steps):
-            _, ms, sm, ln, w = _profiled(s._ctx, lambda: run(BEAM_PARTICLES, "mixed"))
+            _, ms, sm, ln, w = _profiled(s._ctx, lambda: run(particles, "mixed"))
             dev_ms += ms
             wall += w
             samples += sm
             launches += ln
+    if quick:
+        return {"particles": particles, "value": samples / (dev_ms * 1e-3) / 1e9, "unit": "Gsamples/s",
+                "ms_per_step": dev_ms / steps, "gpu_launches_per_step": launches // steps}
     run(fp64_particles, "fp64")
     _, ms64, sm64, _, w64 = _profiled(s._ctx, lambda: run(fp64_particles, "fp64"))
     a = run(check_particles, "mixed", precision=0, max_level=check_level)[1]
@@ -720,12 +725,13 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
             "cpu_reference": cpu, "clocks": clk.summary()}
 
 
-def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12):
+def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12, n_jobs=UNEVEN_JOBS, quick=False):
     """512 uneven jobs through osc_batch_flux: mixed timed on the device and end to end; FP64 (jobs
     one after another through the FP64 path) end to end on the first `fp64_jobs`; mixed vs FP64 error
-    at a fixed level on those jobs."""
+    at a fixed level on those jobs.  `n_jobs` < 512 (the first jobs of the same sequence) and `quick`
+    (the mixed timing alone) give the small cases of profiler runs."""
     from oscars_b200.batch import BatchRunner
-    jobs = uneven_jobs()
+    jobs = uneven_jobs()[:n_jobs]
     r = BatchRunner(local)
     for _ in range(warmup):
         r.flux(jobs, compute="mixed")
@@ -739,6 +745,9 @@ def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12):
             samples += sm
             launches += ln
     variant = r.variant()[0]
+    if quick:
+        return {"jobs": n_jobs, "value": samples / (dev_ms * 1e-3) / 1e9, "unit": "Gsamples/s",
+                "ms_per_step": dev_ms / steps, "gpu_launches_per_step": launches // steps, "variant": variant}
     sub = jobs[:fp64_jobs]
     r.ctx.call("osc_set_variant", 0, 2)  # FP64 variant fixed: no per-shape tuning runs inside the timing
     r.flux(sub, compute="fp64")
@@ -894,6 +903,10 @@ def main():
                     help="timed steps of the batched workloads (EPU beam, uneven jobs); 0 skips them")
     ap.add_argument("--only", default="", choices=["", "beam", "uneven", "tuning", "sharded"],
                     help="run one batched workload alone and print its JSON object (for profiler runs)")
+    ap.add_argument("--particles", type=int, default=BEAM_PARTICLES,
+                    help="with --only beam: particles of the beam (the first ones of the same seeded sequence)")
+    ap.add_argument("--jobs", type=int, default=UNEVEN_JOBS,
+                    help="with --only uneven: the first jobs of the same seeded sequence")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -915,8 +928,13 @@ def main():
     elif args.only:
         import torch
         torch.cuda.set_device(0)
-        leg = {"beam": beam_leg, "uneven": uneven_leg, "tuning": tuning_leg}[args.only]
-        print(json.dumps(leg(args.batched_steps, args.warmup)), flush=True)
+        if args.only == "beam":
+            r = beam_leg(args.batched_steps, args.warmup, particles=args.particles, quick=args.quick)
+        elif args.only == "uneven":
+            r = uneven_leg(args.batched_steps, args.warmup, n_jobs=args.jobs, quick=args.quick)
+        else:
+            r = tuning_leg(args.batched_steps, args.warmup)
+        print(json.dumps(r), flush=True)
     else:
         product_arm(args)
 

@@ -242,16 +242,16 @@ __global__ void k_batch_rk4(const DevJob* __restrict__ jobs, int njobs, const De
   if (c.superluminal) atomicOr(err, kErrSuperluminal);
 }
 
-// Trajectory extent in the job frame: max transverse distance from the axis and max longitudinal
-// coordinate (one block of 256 threads per job).
+// Trajectory extent in the job frame: max transverse distance from the axis, max longitudinal
+// coordinate and max |tau_s| (one block of 256 threads per job).
 __global__ void k_batch_extent(DevJob* __restrict__ jobs, const double* __restrict__ arena) {
-  __shared__ double sx[256], sz[256];
+  __shared__ double sx[256], sz[256], st[256];
   DevJob& J = jobs[blockIdx.x];
   const int64_t n = (int64_t)J.nf + J.nb;
   const double* K = arena + J.knots;
   const double* R = J.frame.rot;
   const double* x0 = J.frame.x0;
-  double xp = 0, zm = -1e300;
+  double xp = 0, zm = -1e300, tm = 0;
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
     const double dx = K[n + i] - x0[0], dy = K[2 * n + i] - x0[1], dz = K[3 * n + i] - x0[2];
     const double a = R[0] * dx + R[1] * dy + R[2] * dz;
@@ -259,20 +259,24 @@ __global__ void k_batch_extent(DevJob* __restrict__ jobs, const double* __restri
     const double c = R[6] * dx + R[7] * dy + R[8] * dz;
     xp = fmax(xp, sqrt(a * a + b * b));
     zm = fmax(zm, c);
+    tm = fmax(tm, fabs((K[i] - J.frame.t_ref) - c / kCLight));
   }
   sx[threadIdx.x] = xp;
   sz[threadIdx.x] = zm;
+  st[threadIdx.x] = tm;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if ((int)threadIdx.x < o) {
       sx[threadIdx.x] = fmax(sx[threadIdx.x], sx[threadIdx.x + o]);
       sz[threadIdx.x] = fmax(sz[threadIdx.x], sz[threadIdx.x + o]);
+      st[threadIdx.x] = fmax(st[threadIdx.x], st[threadIdx.x + o]);
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     J.frame.xperp_max = sx[0];
     J.frame.z_max = sz[0];
+    J.frame.tau_max = st[0];
   }
 }
 
@@ -315,11 +319,14 @@ __global__ void k_batch_spline(const DevJob* __restrict__ jobs, int njobs, doubl
 __global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const double* __restrict__ arena,
                              const unsigned* __restrict__ cnt, float* __restrict__ rec, int64_t stride,
                              int64_t s_off, int64_t s_begin, int64_t s_end) {
+  // The two samples of a pair sit in adjacent lanes (per = s_end - s_begin, s_begin and the block
+  // size are even) and exchange their FP64 values for the pair's step: every lane reaches the
+  // shuffles, lanes past the grid's end or of a finished job on a valid sample, writing nothing.
   const int64_t per = s_end - s_begin;
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= per * njobs) return;
+  const int64_t g_raw = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t g = g_raw < per * njobs ? g_raw : per * njobs - 2 + (g_raw & 1);
   const int j = (int)(g / per);
-  if (cnt && cnt[j] == 0) return;
+  const bool active = g_raw < per * njobs && !(cnt && cnt[j] == 0);
   const DevJob& J = jobs[j];
   const int64_t s = s_begin + g % per;
   const int64_t n = (int64_t)J.nf + J.nb;
@@ -339,8 +346,12 @@ __global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const d
   const double qy = R[3] * v[6] + R[4] * v[7] + R[5] * v[8];
   const double qz = R[6] * v[6] + R[7] * v[7] + R[8] * v[8];
   const double taus = (T - F.t_ref) - z / kCLight;
-  write_pair_record(rec + (kPairFloats / 2) * (int64_t)j * stride, s - s_off, s == 0, x, y, z, taus, px, py, pz, qx,
-                    qy, qz);
+  const unsigned full = 0xffffffffu;
+  const double xo = __shfl_xor_sync(full, x, 1), yo = __shfl_xor_sync(full, y, 1);
+  const double zo = __shfl_xor_sync(full, z, 1), to = __shfl_xor_sync(full, taus, 1);
+  if (active)
+    write_pair_record(rec + (kPairFloats / 2) * (int64_t)j * stride, s - s_off, s == 0, x, y, z, taus, px, py, pz, qx,
+                      qy, qz, xo, yo, zo, to);
 }
 
 // Offsets of one wave over the chunk (one block of 1024 threads): per job the active count n_j (all
@@ -483,7 +494,7 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_batch_wave(BatchWaveArgs A)
       if (live && grp == 0 && span == 0 && !mixed_geometry_ok(fx, fy, fz, om, J.frame)) atomicOr(A.err, kErrBadArgs);
     }
     // pair records of job j: absolute pair p at rec_j[kPairF4 * (p - s_off / 2)]
-    const float4* rec_j = A.rec + (kPairF4 / 2) * (int64_t)j * A.stride - kPairF4 * (A.s_off >> 1);
+    const float4* rec_j = A.rec + kPairF4 * ((int64_t)j * (A.stride >> 1)) - kPairF4 * (A.s_off >> 1);  // stride even
     for (int g = 0; g < P.nseg; ++g) {
       const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
       const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));

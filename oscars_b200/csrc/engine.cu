@@ -165,15 +165,17 @@ void Engine::compute_frame() {
   frame_.x0[0] = P.x0.x; frame_.x0[1] = P.x0.y; frame_.x0[2] = P.x0.z;
   frame_.t_ref = P.t0 / kC;
   const Knots& k = model.knots;
-  double xp = 0, zm = -1e300;
+  double xp = 0, zm = -1e300, tm = 0;
   for (int64_t i = 0; i < k.n; ++i) {
     const Vec3 d = v3(k.y[i] - P.x0.x, k.y[k.n + i] - P.x0.y, k.y[2 * k.n + i] - P.x0.z);
     const double a = dot(d, e1), b = dot(d, e2), c = dot(d, e3);
     xp = std::max(xp, std::sqrt(a * a + b * b));
     zm = std::max(zm, c);
+    tm = std::max(tm, std::fabs((k.t[i] - frame_.t_ref) - c / kC));
   }
   frame_.xperp_max = xp;
   frame_.z_max = zm;
+  frame_.tau_max = tm;
   frame_.theta_max = mixed_theta_max(P.gamma);
 }
 

@@ -65,16 +65,25 @@ __device__ __forceinline__ double level_time(double tstart, double tstop, int64_
 //     w (t + D/c) = w tau_s + (w/c) corr + w Oz/c,   tau_s = t - t0/c - z/c
 // The last term is a constant phase per (observer, energy) entry: it multiplies the whole sum by a
 // unit complex number and drops out of |E|^2, of the polarization projection and of the phase steps
-// of the stop rule, so it is not computed.
+// of the stop rule, so it is not computed.  Phases are carried in turns (units of 2 pi).
 //
-// Phase, FP64.  corr is first formed in FP32 (relative error ~1e-7 -- a few 1e-3 rad when (w/c) corr
-// reaches 1e4 rad, too much for a 1e-4 flux tolerance).  One Newton step on f(c) = c (c + 2 Rz) -
-// rho^2, whose root is D - Rz, refines it in FP64 from the FP64 sample position:
+// Phase of the pair's first sample, FP64.  corr is first formed in FP32 (relative error ~1e-7 -- a
+// few 1e-3 rad when (w/c) corr reaches 1e4 rad, too much for a 1e-4 flux tolerance).  One Newton step
+// on f(c) = c (c + 2 Rz) - rho^2, whose root is D - Rz, refines it in FP64 from the FP64 position:
 //     c1 = c - f(c) / f'(c),   f'(c) = 2 (c + Rz) = 2 D,
 // with 1/(2D) taken from the FP32 rsqrt (its 1e-7 error multiplies a correction that is itself 1e-7
-// of c), so c1 is exact to ~1e-14 relative.  P = w tau_s + (w/c) c1 is then formed and reduced to
-// [-pi, pi] in FP64: k = rint(P / 2pi) by adding 1.5 * 2^52, then P - k 2pi.  Only the reduced
-// phase goes to FP32, for sin / cos.
+// of c), so c1 is exact to ~1e-14 relative.  The phase in turns, (w/2pi) tau_s + (w/2pi c) c1, is
+// accumulated onto 1.5 * 2^22: for |turns| < 2^21 the sum keeps the binade [2^22, 2^23), whose
+// significand has 30 bits below the units place, so the fraction of a turn is read off the low
+// word of the double (rounded to 2^-30 turns, then to the 23 bits of a float: < 4e-7 rad).
+//
+// Phase of the second sample, FP32 step from the first.  With dR = R1 - R0 = -(X1 - X0) and
+// S = R1 + R0 (exact in FP64, stored as FP32 in the record),
+//     corr1 - corr0 = (D1 - D0) - dRz = (dRx Sx + dRy Sy - dRz (corr0 + corr1)) / (D0 + D1)
+// [D1^2 - D0^2 = dR . S and Sz - D0 - D1 = -(corr0 + corr1)], a quotient of small terms with no
+// cancellation; the step (w/2pi) dtau_s + (w/2pi c)(corr1 - corr0) is then good to a few 1e-7 of
+// its own size (a few rad at convergence, where the stop rule bounds the steps by pi), and each
+// pair restarts from its FP64 anchor, so errors do not accumulate along the trajectory.
 //
 // Amplitude, FP32 (src/OSCARSSR.cc:4219), with u = n - b, om = 1 - n.b and |n| = 1:
 //     (1-b^2) u / (D^2 om^2) + n x (u x a) / (D om^2)
@@ -84,14 +93,14 @@ __device__ __forceinline__ double level_time(double tstart, double tstop, int64_
 // The FP32 phase P32 = w tau_s + (w/c) corr of the same operands gives the phase steps of the stop
 // rule (|P_j - P_{j-1}| < pi), where its ~1e-3 rad rounding is immaterial.
 //
-// Pair records: samples 2p and 2p + 1 share 40 floats (160 bytes).  Floats 0..23 hold the FP32
+// Pair records: samples 2p and 2p + 1 share 36 floats (144 bytes).  Floats 0..23 hold the FP32
 // components, component c of sample 2p + b at float 4 (c / 2) + 2 (c % 2) + b, with
 //   x, y, z, tau_s | -bx, -by, 1-bz, bz | 1-b^2, az, ax, ay
 // so that every half of a loaded float4 is one component of both samples (the operand of one packed
-// f32x2 instruction); bytes 96..159 hold the FP64 x, y, z, tau_s as double2 pairs (x0 x1 | y0 y1 |
-// z0 z1 | t0 t1).  Sample 0, the unused slot of the level ladder, holds a zero-amplitude record at
-// the position and time of sample 1 (no contribution, no phase step), so every span is a whole
-// number of pairs.
+// f32x2 instruction); floats 24..27 hold dRx, dRy, dRz, dtau_s (second sample minus first); bytes
+// 112..143 hold the FP64 x, y, z, tau_s of the first sample.  Sample 0, the unused slot of the level
+// ladder, holds a zero-amplitude record at the position and time of sample 1 (no contribution, no
+// phase step), so every span is a whole number of pairs.
 // ---------------------------------------------------------------------------------------------
 // Hardware approximations (MUFU) with denormals flushed: the terms never see denormal operands
 // (distances ~1..100 m, 1 - n.b ~ 1e-9..1e-4, reduced phases in [-pi, pi]).
@@ -110,18 +119,24 @@ __device__ __forceinline__ void sincos_ftz(float x, float* s, float* c) {
   asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*c) : "f"(x));
 }
 
-constexpr int kPairFloats = 40;                        // floats per pair record (160 bytes)
+constexpr int kPairFloats = 36;                        // floats per pair record (144 bytes)
 constexpr int kPairF4 = kPairFloats / 4;               // float4 per pair record
-constexpr double kTwoPiHiD = 6.283185307179586;        // RN(2 pi)
-constexpr double kInvTwoPiD = 0.15915494309189535;     // RN(1 / (2 pi))
-constexpr double kRoundD = 6755399441055744.0;         // 1.5 * 2^52: t + kRoundD rounds t to an integer
+constexpr double kTwoPiD = 6.283185307179586;          // RN(2 pi)
+constexpr float kTwoPiF = 6.28318548202514648f;        // RN_f(2 pi)
+constexpr double kTurnBase = 6291456.0;                // 1.5 * 2^22 (see fp64_turns)
+// Largest |phase| in turns the FP64 accumulation onto kTurnBase allows (2^21), with a factor 2 of
+// margin; the host-side guard (mixed_geometry_ok) keeps every sample's phase below it.
+constexpr double kMaxTurns = 1048576.0;
 
 // Record of one level sample (FP64 values in the particle frame) at sample index s of pair record
 // storage `rec` (s even-aligned with the level ladder).  zero_amplitude writes the record of sample 0
-// (the position and time of sample 1 must be passed for it).
+// (the position and time of sample 1 must be passed for it).  (xo, yo, zo, tauo) are the FP64 values
+// of the pair's other sample: the odd sample writes the step from the even one, the even sample its
+// FP64 values.
 __device__ __forceinline__ void write_pair_record(float* __restrict__ rec, int64_t s, bool zero_amplitude, double x,
                                                   double y, double z, double taus, double px, double py, double pz,
-                                                  double qx, double qy, double qz) {
+                                                  double qx, double qy, double qz, double xo, double yo, double zo,
+                                                  double tauo) {
   const double g2 = 1.0 - (px * px + py * py + pz * pz);       // 1 - b^2, ~1/gamma^2
   const double ebz = (g2 + px * px + py * py) / (1.0 + pz);     // 1 - b_z without cancellation
   float v[12] = {(float)x, (float)y, (float)z, (float)taus, (float)-px, (float)-py,
@@ -131,14 +146,22 @@ __device__ __forceinline__ void write_pair_record(float* __restrict__ rec, int64
     v[6] = 1.f;
     v[7] = v[8] = v[9] = v[10] = v[11] = 0.f;
   }
-  float* base = rec + kPairFloats * (s >> 1) + (s & 1);
+  float* pr = rec + kPairFloats * (s >> 1);
+  float* base = pr + (s & 1);
 #pragma unroll
   for (int c = 0; c < 12; ++c) base[4 * (c >> 1) + 2 * (c & 1)] = v[c];
-  double* d = reinterpret_cast<double*>(rec + kPairFloats * (s >> 1)) + 12 + (s & 1);
-  d[0] = x;
-  d[2] = y;
-  d[4] = z;
-  d[6] = taus;
+  if (s & 1) {  // dR = R1 - R0 = X0 - X1 and dtau = tau1 - tau0, the even sample's values in (xo .. tauo)
+    pr[24] = (float)(xo - x);
+    pr[25] = (float)(yo - y);
+    pr[26] = (float)(zo - z);
+    pr[27] = (float)(taus - tauo);
+  } else {
+    double* d = reinterpret_cast<double*>(pr + 28);
+    d[0] = x;
+    d[1] = y;
+    d[2] = z;
+    d[3] = taus;
+  }
 }
 
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
@@ -146,10 +169,12 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 
-// Per-entry constants: observer in the particle frame, w and w/c, in FP32 (both lanes equal) and FP64.
+// Per-entry constants: observer in the particle frame, w and w/c (radians) in FP32 (both lanes
+// equal), w/2pi and w/(2pi c) (turns) in FP32 and FP64, the FP64 observer.
 struct PairObs {
   float2 ox, oy, oz, w, wc;
-  double dox, doy, doz, dw, dwc;
+  float wt, wct;
+  double dox, doy, doz, dwt, dwct;
 };
 
 __device__ __forceinline__ PairObs make_pair_obs(double fx, double fy, double fz, double om) {
@@ -162,8 +187,10 @@ __device__ __forceinline__ PairObs make_pair_obs(double fx, double fy, double fz
   o.dox = fx;
   o.doy = fy;
   o.doz = fz;
-  o.dw = om;
-  o.dwc = om / kCLight;
+  o.dwt = om / kTwoPiD;
+  o.dwct = om / (kTwoPiD * kCLight);
+  o.wt = (float)o.dwt;
+  o.wct = (float)o.dwct;
   return o;
 }
 
@@ -193,42 +220,30 @@ __device__ __forceinline__ double nonneg_float_to_double(float x) {
   return __hiloint2double((int)((u >> 3) + 0x38000000u), (int)(u << 29));
 }
 
-constexpr double kFourPiD = 12.566370614359172;   // RN(4 pi)
-constexpr float kFourPiF = 12.566370964050293f;   // RN_f(4 pi)
-
-// A reduced phase plus 4 pi, v in [3 pi, 5 pi] (inside [8, 16), one binade), to FP32 on the integer
-// pipe: the float of the same binade takes the top 23 fraction bits of v (truncation, < 1e-6 rad),
-// and subtracting 4 pi in FP32 is exact (Sterbenz).  The offset between kFourPiD and kFourPiF is a
-// constant phase shared by every sample, so it drops out of |E|^2.
-__device__ __forceinline__ float reduced_phase_to_float(double v) {
-  const unsigned lo = (unsigned)__double2loint(v), hi = (unsigned)__double2hiint(v);
-  const unsigned m = __funnelshift_l(lo, hi, 3) & 0x007FFFFFu;
-  return __uint_as_float(m | 0x41000000u) - kFourPiF;
-}
-
-// FP64 retarded phase of one sample, reduced to [-pi, pi] (see the section comment): corr_f and
-// half_iD = 1 / (2 D) are the sample's FP32 values.  The phase is carried as P + 4 pi so that its
-// reduction lands in one binade; 2 - rint((P + 4 pi) / 2pi) multiples of 2pi are removed with the
-// leading double of 2pi only (the trailing part would move the result by < 2e-12 rad).
-__device__ __forceinline__ float fp64_phase(double x, double y, double z, double tau, float corr_f, float half_iD,
+// FP64 retarded phase of one sample as a fraction of a turn in [-1/2, 1/2) (see the section
+// comment), shifted by half a turn: a constant phase shared by every sample, which drops out of
+// |E|^2.  corr_f and half_iD = 1 / (2 D) are the sample's FP32 values.  v = 1.5 * 2^22 + turns lies
+// in [2^22, 2^23) (|turns| < 2^21), so bits 0..29 of its low word are the fraction of a turn in
+// units of 2^-30; bits 7..29, rounded, become the significand of a float in [1, 2).
+__device__ __forceinline__ float fp64_turns(double x, double y, double z, double tau, float corr_f, float half_iD,
                                             const PairObs& o) {
   const double Rx = o.dox - x, Ry = o.doy - y, Rz = o.doz - z;
   const double r2 = fma(Rx, Rx, Ry * Ry);
   const double c = nonneg_float_to_double(corr_f);
   const double f = fma(c, fma(2.0, Rz, c), -r2);
   const double c1 = fma(-f, nonneg_float_to_double(half_iD), c);
-  const double P4 = fma(o.dwc, c1, fma(o.dw, tau, kFourPiD));
-  const double nk = (kRoundD + 2.0) - fma(P4, kInvTwoPiD, kRoundD);
-  return reduced_phase_to_float(fma(nk, kTwoPiHiD, P4));
+  const double v = fma(o.dwct, c1, fma(o.dwt, tau, kTurnBase));
+  const unsigned lo = (unsigned)__double2loint(v) + 0x40u;  // round to 23 fraction bits (a carry wraps mod 1)
+  return __uint_as_float(((lo >> 7) & 0x007FFFFFu) | 0x3F800000u) - 1.5f;
 }
 
 // Both samples of one pair record `q` for one entry: adds e (cos P, sin P) per lane to acc (x re,
 // x im, y re, y im, z re, z im; the imaginary parts with the sign of +sin P) and returns P32 of both
 // samples.  The sum uses exp(-i P): the caller negates the imaginary parts when it folds acc.
 __device__ __forceinline__ float2 pair_sample(const float4* __restrict__ q, const PairObs& o, float2* acc) {
-  const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5];
-  const double2* dq = reinterpret_cast<const double2*>(q + 6);
-  const double2 DX = dq[0], DY = dq[1], DZ = dq[2], DT = dq[3];
+  const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
+  const double2* dq = reinterpret_cast<const double2*>(q + 7);
+  const double2 DXY = dq[0], DZT = dq[1];
   const float2 X = make_float2(q0.x, q0.y), Y = make_float2(q0.z, q0.w);
   const float2 Z = make_float2(q1.x, q1.y), T = make_float2(q1.z, q1.w);
   const float2 NBX = make_float2(q2.x, q2.y), NBY = make_float2(q2.z, q2.w);
@@ -244,12 +259,16 @@ __device__ __forceinline__ float2 pair_sample(const float4* __restrict__ q, cons
   const float2 qq = mul2(ri, iD);
   const float2 corr = mul2(ri, fma2(f2(0.125f), qq, f2(0.5f)));
   const float2 P = fma2(o.wc, corr, mul2(o.w, T));
-  const float2 hD = mul2(iD, f2(0.5f));
-  const float rr0 = fp64_phase(DX.x, DY.x, DZ.x, DT.x, corr.x, hD.x, o);
-  const float rr1 = fp64_phase(DX.y, DY.y, DZ.y, DT.y, corr.y, hD.y, o);
+  const float t0 = fp64_turns(DXY.x, DXY.y, DZT.x, DZT.y, corr.x, 0.5f * iD.x, o);
+  // second sample: the FP32 step from the first (section comment)
+  const float2 DD = mul2(d2, iD);  // D0, D1
+  const float inv = rcp_ftz(DD.x + DD.y);
+  const float num = fmaf(q6.x, rx.x + rx.y, fmaf(q6.y, ry.x + ry.y, -q6.z * (corr.x + corr.y)));
+  const float t1 = t0 + fmaf(o.wct, num * inv, o.wt * q6.w);
+  const float2 ph = mul2(make_float2(t0, t1), f2(kTwoPiF));
   float2 sn, cs;
-  sincos_ftz(rr0, &sn.x, &cs.x);
-  sincos_ftz(rr1, &sn.y, &cs.y);
+  sincos_ftz(ph.x, &sn.x, &cs.x);
+  sincos_ftz(ph.y, &sn.y, &cs.y);
   const float2 nx = mul2(rx, iD), ny = mul2(ry, iD), en = mul2(corr, iD);  // en = 1 - nz
   const float2 ux = add2(nx, NBX), uy = add2(ny, NBY), uz = fma2(en, M1, EB);
   const float2 om = fma2(ny, NBY, fma2(nx, NBX, fma2(en, BZ, EB)));
@@ -271,14 +290,17 @@ __device__ __forceinline__ float2 pair_sample(const float4* __restrict__ q, cons
 }
 
 // Validity of the mixed path for an observer at (fx, fy, fz) in the particle frame: within
-// F.theta_max of the frame axis (trajectory extent included), downstream of the trajectory, and a
-// correction phase (w/c) rho^2 / (2 Rz) of at most 3e4 rad.  theta_max = min(1e-2, 20 / gamma)
-// (mixed_theta_max): beyond ~20 / gamma the flux is a deep cancellation of nearly equal terms
-// (|sum| << sum |terms|) that FP32 amplitudes do not resolve to 1e-4.
+// F.theta_max of the frame axis (trajectory extent included), downstream of the trajectory, a
+// correction phase (w/c) rho^2 / (2 Rz) of at most 3e4 rad, and a phase w |tau_s| + correction below
+// kMaxTurns turns (the range of fp64_turns).  theta_max = min(1e-2, 20 / gamma) (mixed_theta_max):
+// beyond ~20 / gamma the flux is a deep cancellation of nearly equal terms (|sum| << sum |terms|)
+// that FP32 amplitudes do not resolve to 1e-4.
 __device__ __forceinline__ bool mixed_geometry_ok(double fx, double fy, double fz, double om, const MixedFrame& F) {
   const double rho = sqrt(fx * fx + fy * fy) + F.xperp_max;
   const double rz = fz - F.z_max;
-  return rz > 0 && rho < F.theta_max * rz && (om / kCLight) * rho * rho / (2 * rz) < 3e4;
+  const double corr_phase = (om / kCLight) * rho * rho / (2 * rz);
+  return rz > 0 && rho < F.theta_max * rz && corr_phase < 3e4 &&
+         (om * F.tau_max + corr_phase) < kMaxTurns * kTwoPiD;
 }
 
 // ---------------------------------------------------------------------------------------------

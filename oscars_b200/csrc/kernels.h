@@ -148,19 +148,21 @@ struct PdFinalArgs {
 
 // Frame of the mixed-precision path: origin x0 (particle start), rows of rot = e1, e2, e3 with e3 the
 // initial direction; xperp_max / z_max bound the trajectory in that frame; t_ref = t0 / c;
-// theta_max = the largest observer angle the path accepts (mixed_theta_max of the particle's gamma).
+// theta_max = the largest observer angle the path accepts (mixed_theta_max of the particle's gamma);
+// tau_max bounds |tau_s| (the phase range check of mixed_geometry_ok).
 struct MixedFrame {
   double rot[9];
   double x0[3];
   double t_ref;
   double xperp_max, z_max;
   double theta_max;
+  double tau_max;  // largest |t - t_ref - z/c| over the trajectory knots
 };
 
 // Refusal of an observer outside the mixed path's validity region (mixed_geometry_ok).
 constexpr const char* kMixedGeometryMessage =
-    "compute='mixed' needs observers near the beam axis (angle below min(1e-2, 20/gamma) and a correction "
-    "phase below 3e4 rad); use compute='fp64' for this geometry";
+    "compute='mixed' needs observers near the beam axis (angle below min(1e-2, 20/gamma), a correction "
+    "phase below 3e4 rad and retarded phases below 2^20 turns); use compute='fp64' for this geometry";
 
 // Largest observer angle from the frame axis the mixed path accepts for a particle of Lorentz
 // factor gamma: min(1e-2, 20 / gamma) (see mixed_geometry_ok in fd_common.cuh).
@@ -173,7 +175,7 @@ __host__ __device__ inline double mixed_theta_max(double gamma) {
 // evaluated from the trajectory knots (t | y[9] | y''[9], n points).
 cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
                                  int64_t s_end, const MixedFrame& F, float4* rec, cudaStream_t st);
-constexpr int kMixedRecordBytesPerSample = 80;
+constexpr int kMixedRecordBytesPerSample = 72;
 // Compiled kernel variants (see kernels_fp64.cu / kernels_mixed.cu); the engine's autotuner picks one.
 constexpr int kFp64Variants = 4;
 constexpr int kMixedVariants = 4;

@@ -13,22 +13,26 @@ namespace osc {
 namespace dev {
 
 constexpr int kMxThreads = 128;
-constexpr int kPrChunk = 256;   // samples per staged chunk (128 pair records, 20 KB)
 constexpr int kPrFold = 16;     // pairs per FP32 partial sum before it is folded into FP64
 
+template <int CP>  // CP pair records per staged chunk, two buffers
 struct PairStage {
-  float4 v[2][kPrChunk / 2 * kPairF4];
+  float4 v[2][CP * kPairF4];
   uint64_t bar[2];
 };
 
 // Pair records of level samples [s_begin, s_end) straight from the trajectory spline (one thread per
 // sample): the level time (src/TParticleTrajectoryInterpolated.cc:124-158), the spline values
 // (include/TOMATH.h:92-121, bit-identical to the FP64 level cache), the particle frame and the record.
-// Sample 0 is the zero-amplitude record at the position and time of sample 1.
+// Sample 0 is the zero-amplitude record at the position and time of sample 1.  The two samples of a
+// pair sit in adjacent lanes (s_begin and the block size are even) and exchange their FP64 values
+// for the pair's step, so every lane of the grid's last warp takes part (past s_end on a clamped
+// sample, writing nothing).
 __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, double tstart, double tstop,
                                 int64_t s_begin, int64_t s_end, MixedFrame F, float* __restrict__ rec) {
-  const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= s_end) return;
+  const int64_t s_raw = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = s_raw < s_end;
+  const int64_t s = active ? s_raw : s_end - 2 + (s_raw & 1);
   const double t = level_time(tstart, tstop, s == 0 ? 1 : s);
   double v[9];
   spline_eval9(knots, n, t, v);
@@ -44,7 +48,10 @@ __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, dou
   const double qy = R[3] * v[6] + R[4] * v[7] + R[5] * v[8];
   const double qz = R[6] * v[6] + R[7] * v[7] + R[8] * v[8];
   const double taus = (t - F.t_ref) - z / kCLight;
-  write_pair_record(rec, s, s == 0, x, y, z, taus, px, py, pz, qx, qy, qz);
+  const unsigned full = 0xffffffffu;
+  const double xo = __shfl_xor_sync(full, x, 1), yo = __shfl_xor_sync(full, y, 1);
+  const double zo = __shfl_xor_sync(full, z, 1), to = __shfl_xor_sync(full, taus, 1);
+  if (active) write_pair_record(rec, s, s == 0, x, y, z, taus, px, py, pz, qx, qy, qz, xo, yo, zo, to);
 }
 
 // Sample sum over pair records, sample-split: the CTA's 128 threads form SUB groups of TE = 128 / SUB
@@ -54,15 +61,15 @@ __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, dou
 // global memory), so the span maxima already include the step into each span (dmax_spans_joined).
 // The groups' sums are reduced in shared memory in group order and one tile-major partial per entry
 // and span is stored; the CTA that finishes a tile's last span finalizes the tile (fused_unit_done).
-template <int SUB, int MINB>
+template <int SUB, int MINB, int CP, bool SSM>
 __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveArgs A, MixedFrame F) {
   constexpr int TE = kMxThreads / SUB;
   if (A.tile_entries != TE) {  // the host sized the partials for another tile
     if (threadIdx.x == 0) atomicOr(A.err, kErrPlan);
     return;
   }
-  constexpr int CP = kPrChunk / 2;  // pairs per chunk
-  __shared__ __align__(16) PairStage st;
+  __shared__ __align__(16) PairStage<CP> st;
+  __shared__ double ssum[SSM ? 6 : 1][SSM ? kMxThreads : 1];
   __shared__ double red[SUB > 1 ? SUB - 1 : 1][7][TE];
   __shared__ int s_last;
   __shared__ WavePlan P;
@@ -113,6 +120,9 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveA
       const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
       const int64_t p0 = b0 >> 1, p1 = b1 > b0 ? b1 >> 1 : p0;  // spans are whole pairs
       double S[6] = {0, 0, 0, 0, 0, 0};
+      if (SSM)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ssum[k][tid] = 0.0;
       float dmax = 0.f;
       bool any = false;
       const int64_t nchunks = (p1 - p0 + CP - 1) / CP;
@@ -154,10 +164,18 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveA
               dmax = fmaxf(dmax, fmaxf(fabsf(ph.x - last), fabsf(ph.y - ph.x)));
               last = ph.y;
             }
+            if (SSM) {
 #pragma unroll
-            for (int k = 0; k < 6; k += 2) {
-              S[k] += (double)acc[k].x + (double)acc[k].y;
-              S[k + 1] -= (double)acc[k + 1].x + (double)acc[k + 1].y;
+              for (int k = 0; k < 6; k += 2) {
+                ssum[k][tid] += (double)acc[k].x + (double)acc[k].y;
+                ssum[k + 1][tid] -= (double)acc[k + 1].x + (double)acc[k + 1].y;
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < 6; k += 2) {
+                S[k] += (double)acc[k].x + (double)acc[k].y;
+                S[k + 1] -= (double)acc[k + 1].x + (double)acc[k + 1].y;
+              }
             }
           }
           any = true;
@@ -166,6 +184,9 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveA
           carry = pair_phase_at(reinterpret_cast<const float*>(sv + kPairF4 * (CP - 1)), 1, o);
         __syncthreads();  // everyone is done with `buf` before it is refilled
       }
+      if (SSM)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) S[k] = ssum[k][tid];
       // reduce the groups' sums in group order; group 0 stores the span's partial
       if (SUB > 1 && grp > 0) {
 #pragma unroll
@@ -206,39 +227,40 @@ cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, 
   return cudaGetLastError();
 }
 
-// Compiled variants of the mixed wave kernel: (groups SUB of 128 / SUB entries, minimum CTAs per SM).
-static const int kMixedSub[kMixedVariants] = {4, 4, 2, 1};
+// Compiled variants of the mixed wave kernel: groups SUB of 128 / SUB entries, minimum CTAs per SM,
+// pair records per staged chunk, FP64 span sums kept in shared memory.
+#define OSC_MIXED_VARIANTS(X) \
+  X(0, 4, 4, 128, false)      \
+  X(1, 4, 4, 64, true)        \
+  X(2, 4, 5, 64, false)       \
+  X(3, 2, 5, 64, true)
+
+#define OSC_SUB(i, sub, minb, cp, ssm) sub,
+static const int kMixedSub[kMixedVariants] = {OSC_MIXED_VARIANTS(OSC_SUB)};
 
 int mixed_entries_per_cta(int variant) { return dev::kMxThreads / kMixedSub[variant]; }
 const char* mixed_variant_name(int variant) {
-  static const char* const kNames[kMixedVariants] = {"k_fd_wave_mixed_pair<4,4>", "k_fd_wave_mixed_pair<4,1>",
-                                                     "k_fd_wave_mixed_pair<2,4>", "k_fd_wave_mixed_pair<1,4>"};
+#define OSC_NAME(i, sub, minb, cp, ssm) "k_fd_wave_mixed_pair<" #sub "," #minb "," #cp "," #ssm ">",
+  static const char* const kNames[kMixedVariants] = {OSC_MIXED_VARIANTS(OSC_NAME)};
   return variant >= 0 && variant < kMixedVariants ? kNames[variant] : "";
 }
 
-template <int SUB, int MINB>
-static int pair_occ() {
-  int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_mixed_pair<SUB, MINB>, dev::kMxThreads, 0);
-  return n > 0 ? n : 1;
-}
-
 int mixed_blocks_per_sm(int variant) {
+  int n = 0;
   switch (variant) {
-    case 0: return pair_occ<4, 4>();
-    case 1: return pair_occ<4, 1>();
-    case 2: return pair_occ<2, 4>();
-    default: return pair_occ<1, 4>();
+#define OSC_OCC(i, sub, minb, cp, ssm) \
+    case i: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_fd_wave_mixed_pair<sub, minb, cp, ssm>, dev::kMxThreads, 0); break;
+    OSC_MIXED_VARIANTS(OSC_OCC)
   }
+  return n > 0 ? n : 1;
 }
 
 cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int grid, int variant, cudaStream_t st) {
   const int T = dev::kMxThreads;
   switch (variant) {
-    case 0: dev::k_fd_wave_mixed_pair<4, 4><<<grid, T, 0, st>>>(a, F); break;
-    case 1: dev::k_fd_wave_mixed_pair<4, 1><<<grid, T, 0, st>>>(a, F); break;
-    case 2: dev::k_fd_wave_mixed_pair<2, 4><<<grid, T, 0, st>>>(a, F); break;
-    default: dev::k_fd_wave_mixed_pair<1, 4><<<grid, T, 0, st>>>(a, F); break;
+#define OSC_LAUNCH(i, sub, minb, cp, ssm) \
+    case i: dev::k_fd_wave_mixed_pair<sub, minb, cp, ssm><<<grid, T, 0, st>>>(a, F); break;
+    OSC_MIXED_VARIANTS(OSC_LAUNCH)
   }
   return cudaGetLastError();
 }

@@ -169,7 +169,7 @@ def test_variant_names():
     for kind, n in ((0, 4), (2, 4), (3, 4)):
         names = [_lib.variant_name(kind, v) for v in range(n)]
         assert all(names) and len(set(names)) == n
-    assert _lib.variant_name(2, 0) == "k_fd_wave_mixed_pair<4,4>"
+    assert _lib.variant_name(2, 0) == "k_fd_wave_mixed_pair<4,4,128,false>"
     assert _lib.variant_name(3, 3) == "k_batch_wave<1,4>"
     with pytest.raises(ValueError, match="out of range"):
         _lib.variant_name(2, 4)
