@@ -628,7 +628,7 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
   w.n_e = n_e; w.n_items = N; w.act = nullptr; w.n_act = nullptr; w.first = 1; w.level = level;
   const int fv = forced_variant[0] >= 0 ? forced_variant[0] : current_variant_[0];
   const int te = fp64_entries_per_cta(fv);  // entries per CTA of that variant
-  w.tile_entries = te; w.min_span = 32; w.target_units = 1; w.part = part_.as<double>(); w.err = cnt + 2;
+  w.tile_entries = te; w.min_span = 32; w.target_units = 1; w.part = part_.as<double>(); w.err = cnt + kCntErr;
   w.work = work;
   check(launch_fd_wave_fp64(w, (int)std::min<int64_t>((N + te - 1) / te, wave_grid(0, fv)), fv, st), "adjoint forward");
   check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");  // counters start at zero
@@ -665,10 +665,10 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
   if (flux_out) check(cudaMemcpyAsync(flux_out, d_flux, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
   check(cudaMemcpyAsync(grad_params, d_pgrad, sizeof(double) * n_params, cudaMemcpyDeviceToHost, st), "download");
   unsigned err = 0;
-  check(cudaMemcpyAsync(&err, cnt + 2, sizeof err, cudaMemcpyDeviceToHost, st), "error word");
+  check(cudaMemcpyAsync(&err, cnt + kCntErr, sizeof err, cudaMemcpyDeviceToHost, st), "error word");
   check(cudaStreamSynchronize(st), "adjoint");
   if (err & dev::kErrTmaTimeout) {
-    check(cudaMemset(cnt + 2, 0, sizeof(unsigned)), "error word");
+    check(cudaMemset(cnt + kCntErr, 0, sizeof(unsigned)), "error word");
     throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
   }
   last_samples = N * (s_end - 1);

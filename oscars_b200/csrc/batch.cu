@@ -1092,11 +1092,11 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
               "download");
     }
     timed_end(chunk_ev, st);
-    unsigned long long h64[2] = {0, 0};
-    unsigned err = 0;
-    check(cudaMemcpyAsync(h64, m64, sizeof h64, cudaMemcpyDeviceToHost, st), "stats");
-    check(cudaMemcpyAsync(&err, misc, sizeof err, cudaMemcpyDeviceToHost, st), "stats");
+    unsigned long long* h64 = reinterpret_cast<unsigned long long*>(ctl_host_ + 4);  // pinned
+    check(cudaMemcpyAsync(h64, m64, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "stats");
+    check(cudaMemcpyAsync(ctl_host_ + 8, misc, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "stats");
     check(cudaStreamSynchronize(st), "batch");
+    const unsigned err = ctl_host_[8];
     if (err & dev::kErrTmaTimeout)
       throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
     if (err & dev::kErrSuperluminal)

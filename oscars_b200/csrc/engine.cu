@@ -58,9 +58,14 @@ Engine::Engine(int dev) : device(dev) {
         "cudaHostAlloc");
   check(cudaHostAlloc(reinterpret_cast<void**>(&stage_host_), kStageDoubles * sizeof(double), cudaHostAllocDefault),
         "cudaHostAlloc");
+  check(cudaHostAlloc(reinterpret_cast<void**>(&ctl_host_), 16 * sizeof(unsigned), cudaHostAllocDefault),
+        "cudaHostAlloc");
   for (int i = 0; i < kStatSlots; ++i) check(cudaEventCreateWithFlags(&stats_ev_[i], cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&order_ev_, cudaEventDisableTiming), "event");
+  check(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming), "event");
+  check(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming), "event");
   cur_ = stream;
 }
 
@@ -68,14 +73,18 @@ Engine::~Engine() {
   if (device < 0) return;
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
+  if (aux_) cudaStreamSynchronize(aux_);
   for (auto& e : ev_pending_) { ev_pool_.push_back(e.first); ev_pool_.push_back(e.second); }
   for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
   for (int i = 0; i < kStatSlots; ++i) if (stats_ev_[i]) cudaEventDestroy(stats_ev_[i]);
   if (stage_ev_) cudaEventDestroy(stage_ev_);
   if (order_ev_) cudaEventDestroy(order_ev_);
+  if (fork_ev_) cudaEventDestroy(fork_ev_);
+  if (join_ev_) cudaEventDestroy(join_ev_);
   if (last_stream_valid_ && last_stream_ != stream) cudaStreamSynchronize(last_stream_);
   if (stats_host_) cudaFreeHost(stats_host_);
   if (stage_host_) cudaFreeHost(stage_host_);
+  if (ctl_host_) cudaFreeHost(ctl_host_);
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
                     &act_[1], &cnt_, &acc_, &acc_comp_, &mrec_, &b_fields_, &b_fvals_, &b_obs_, &b_omega_, &b_acc_, &b_jobs_,
@@ -83,6 +92,7 @@ Engine::~Engine() {
                     &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_, &fused_})
     b->release();
   if (stream) cudaStreamDestroy(stream);
+  if (aux_) cudaStreamDestroy(aux_);
 }
 
 void Engine::check(cudaError_t e, const char* what) {
@@ -113,40 +123,48 @@ void Engine::upload_trajectory() {
   check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), cur_), "memset");
 }
 
-// Make levels 0..L resident.  The cache grows by doubling; growing refills from level 0.
+// Capacity of the FP64 level cache for levels 0..L; growing keeps what is filled (the 10 arrays are
+// copied into the larger cache).
+void Engine::reserve_levels(int L) {
+  const int64_t need = (int64_t)2 << L;
+  if (need <= lev_cap_) return;
+  int64_t cap = std::max<int64_t>(need, (int64_t)2 << 13);
+  if (lev_cap_ > 0 && lev_filled_ >= 0) {
+    DevBuf nb;
+    nb.reserve(sizeof(double) * 10 * cap);
+    const int64_t used = (int64_t)2 << lev_filled_;
+    for (int a = 0; a < 10; ++a)
+      check(cudaMemcpyAsync(nb.as<double>() + a * cap, lev_.as<double>() + a * lev_cap_, sizeof(double) * used,
+                            cudaMemcpyDeviceToDevice, cur_),
+            "level cache grow");
+    check(cudaStreamSynchronize(cur_), "level cache grow");
+    lev_.release();
+    lev_ = nb;
+    nb.p = nullptr;
+  } else {
+    lev_.reserve(sizeof(double) * 10 * cap);
+  }
+  lev_cap_ = cap;
+}
+
+void Engine::fill_levels(int64_t s_begin, int64_t s_end, cudaStream_t s) {
+  check(launch_level_fill(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, lev_.as<double>(), lev_cap_,
+                          -1, bd_bits_.as<unsigned long long>(), s),
+        "level fill");
+  ++last_launches;
+  bdmax_valid_ = false;
+}
+
+// Make levels 0..L resident.
 void Engine::ensure_levels(int L) {
   if (L <= lev_filled_) return;
-  const int64_t need = (int64_t)2 << L;
-  if (need > lev_cap_) {
-    int64_t cap = std::max<int64_t>(need, (int64_t)2 << 13);
-    if (lev_cap_ > 0 && lev_filled_ >= 0) {
-      // keep what is filled: copy the 10 arrays into the larger cache
-      DevBuf nb;
-      nb.reserve(sizeof(double) * 10 * cap);
-      const int64_t used = (int64_t)2 << lev_filled_;
-      for (int a = 0; a < 10; ++a)
-        check(cudaMemcpyAsync(nb.as<double>() + a * cap, lev_.as<double>() + a * lev_cap_, sizeof(double) * used,
-                              cudaMemcpyDeviceToDevice, cur_),
-              "level cache grow");
-      check(cudaStreamSynchronize(cur_), "level cache grow");
-      lev_.release();
-      lev_ = nb;
-      nb.p = nullptr;
-    } else {
-      lev_.reserve(sizeof(double) * 10 * cap);
-    }
-    lev_cap_ = cap;
-  }
-  if (lev_filled_ < 0)
+  reserve_levels(L);
+  if (lev_filled_ < 0) {
     check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), cur_), "memset");
-  const int64_t s_begin = lev_filled_ < 0 ? 1 : ((int64_t)2 << lev_filled_);
-  const int64_t s_end = (int64_t)2 << L;
-  check(launch_level_fill(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, lev_.as<double>(), lev_cap_,
-                          -1, bd_bits_.as<unsigned long long>(), cur_),
-        "level fill");
-  last_launches += 2;
+    ++last_launches;
+  }
+  fill_levels(lev_filled_ < 0 ? 1 : ((int64_t)2 << lev_filled_), (int64_t)2 << L, cur_);
   lev_filled_ = L;
-  bdmax_valid_ = false;
 }
 
 // Frame of the mixed path (kernels_mixed.cu): origin at the particle start, e3 along its initial
@@ -179,28 +197,70 @@ void Engine::compute_frame() {
   frame_.theta_max = mixed_theta_max(P.gamma);
 }
 
-void Engine::ensure_mixed(int L) {
+// Capacity of the mixed pair records for levels 0..L (the frame is set up for the current knots
+// first); growing refills from sample 0 (one spline evaluation per sample).
+void Engine::reserve_mixed(int L) {
   if (mrec_version_ != knots_version_) {
     compute_frame();
     mrec_version_ = knots_version_;
     mrec_filled_ = -1;
   }
-  if (L <= mrec_filled_) return;
   const int64_t need = (int64_t)2 << L;
-  if (need > mrec_cap_) {  // grows by refilling from sample 0 (one spline evaluation per sample)
-    const int64_t cap = std::max<int64_t>(need, (int64_t)2 << 14);
-    mrec_.release();
-    mrec_.reserve((size_t)kMixedRecordBytesPerSample * cap);
-    mrec_cap_ = cap;
-    mrec_filled_ = -1;
-  }
-  const int64_t s_begin = mrec_filled_ < 0 ? 0 : ((int64_t)2 << mrec_filled_);
-  const int64_t s_end = need;
+  if (need <= mrec_cap_) return;
+  const int64_t cap = std::max<int64_t>(need, (int64_t)2 << 14);
+  mrec_.release();
+  mrec_.reserve((size_t)kMixedRecordBytesPerSample * cap);
+  mrec_cap_ = cap;
+  mrec_filled_ = -1;
+}
+
+void Engine::fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s) {
   check(launch_mixed_records(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, frame_, mrec_.as<float4>(),
-                             cur_),
+                             s),
         "mixed records");
   ++last_launches;
+}
+
+void Engine::ensure_mixed(int L) {
+  reserve_mixed(L);
+  if (L <= mrec_filled_) return;
+  fill_mixed(mrec_filled_ < 0 ? 0 : ((int64_t)2 << mrec_filled_), (int64_t)2 << L, cur_);
   mrec_filled_ = L;
+}
+
+// Levels 0..Lpre resident for the waves enqueued without a host round trip.  The levels above the
+// first wave's (Lhead) are filled on the side stream, concurrently with the first wave; join_prefill()
+// makes the request stream wait for them before the second wave.
+void Engine::prefill(bool mixed, int Lhead, int Lpre) {
+  if (mixed) reserve_mixed(Lpre);
+  else reserve_levels(Lpre);
+  int& filled = mixed ? mrec_filled_ : lev_filled_;
+  if (Lpre <= filled) return;
+  if (!mixed && filled < 0) {
+    check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), cur_), "memset");
+    ++last_launches;
+  }
+  const int lo = std::max(filled, Lhead);
+  if (Lpre > lo) {
+    check(cudaEventRecord(fork_ev_, cur_), "event");
+    check(cudaStreamWaitEvent(aux_, fork_ev_, 0), "stream wait");
+    if (mixed) fill_mixed((int64_t)2 << lo, (int64_t)2 << Lpre, aux_);
+    else fill_levels((int64_t)2 << lo, (int64_t)2 << Lpre, aux_);
+    check(cudaEventRecord(join_ev_, aux_), "event");
+    join_pending_ = true;
+  }
+  if (lo > filled) {
+    const int64_t b = filled < 0 ? (mixed ? 0 : 1) : ((int64_t)2 << filled);
+    if (mixed) fill_mixed(b, (int64_t)2 << lo, cur_);
+    else fill_levels(b, (int64_t)2 << lo, cur_);
+  }
+  filled = Lpre;
+}
+
+void Engine::join_prefill() {
+  if (!join_pending_) return;
+  check(cudaStreamWaitEvent(cur_, join_ev_, 0), "stream wait");
+  join_pending_ = false;
 }
 
 double dt_inclusive(double tstart, double tstop, int L) {  // :224-237
@@ -326,8 +386,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   const int Lpre = std::min(lstop, std::max(Lfirst, Lpre_want));
   const int variant = tuning_ ? current_variant_[kind]
                               : pick_variant(kind, const_cast<RadRequest&>(rq), n_items, Lfirst, lstop, d_out, d_lvl, st);
-  if (mixed) ensure_mixed(Lpre);
-  else ensure_levels(Lpre);
+  prefill(mixed, Lfirst, Lpre);
   const int resident = wave_grid(kind, variant);  // CTAs resident at once on the device
   const int tile = mixed ? mixed_entries_per_cta(variant) : rq.power_density ? 128 : fp64_entries_per_cta(variant);
   const int min_span = rq.power_density ? kMinSpan : kMinSpanSplit;
@@ -355,13 +414,11 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   act_[1].reserve(sizeof(int) * N);
   state_.reserve(sizeof(double) * 7 * N);
 
-  unsigned* cnt = cnt_.as<unsigned>();  // [0], [1] list counts, [2] sticky error word
+  unsigned* cnt = cnt_.as<unsigned>();  // [0], [1] list counts, [kCntErr] sticky error word
   // [0] not converged, [1] samples, [2] unit counter of the running wave
   unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);
-  check(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), st), "memset");
   unsigned* level_max = cnt + 12;  // highest level at which an entry finished
-  check(cudaMemsetAsync(level_max, 0, sizeof(unsigned), st), "memset");
-  check(cudaMemsetAsync(c64, 0, 3 * sizeof(unsigned long long), st), "memset");
+  check(cudaMemsetAsync(cnt, 0, 13 * sizeof(unsigned), st), "memset");  // words 0..12
   // Flux / spectrum waves finalize their own tiles (one launch per level).  Wave w reads its active
   // count from fz3[w % 3], appends survivors to fz3[(w + 1) % 3] and zeroes fz3[(w + 2) % 3] for the
   // wave after; it takes units from fw[w % 2] and zeroes fw[(w + 1) % 2].
@@ -400,6 +457,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   int cur_list = 0;
   auto launch_wave = [&](int L) {
     const bool first = L == Lfirst;
+    if (!first) join_prefill();  // the levels filled on the side stream
     const int wv = L - Lfirst;
     const int* act_in = first ? nullptr : act_[cur_list].as<int>();
     const unsigned* nact_in = first ? nullptr : (fused ? fz3 + wv % 3 : cnt + cur_list);
@@ -411,7 +469,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
-      w.part = part_.as<double>(); w.err = cnt + 2; w.work = fw + wv % 2;
+      w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = fw + wv % 2;
       w.fused = 1;
       w.tile_done = fz3 + 16;
       w.zero_u32 = fz3 + (wv + 2) % 3;
@@ -441,7 +499,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
-      w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
+      w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = c64 + 2;
       auto ev = timed_begin(st);
       const int g = grid_for(L);
       if (mixed) check(launch_fd_wave_mixed(w, frame_, g, variant, st), "flux wave (mixed)");
@@ -462,7 +520,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
-      w.part = part_.as<double>(); w.err = cnt + 2; w.work = c64 + 2;
+      w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = c64 + 2;
       auto ev = timed_begin(st);
       check(launch_pd_wave_fp64(w, grid_for(L), st), "power density wave");
       timed_end(ev, st);
@@ -482,11 +540,12 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   };
   for (int L = Lfirst; L <= Lpre; ++L) launch_wave(L);
   for (int L = Lpre + 1; L <= lstop; ++L) {  // beyond the prefilled levels the host decides
-    unsigned nn = 0, lmax = 0;
+    // pinned destinations: the copies are plain DMA and the wait is one stream synchronisation
     const unsigned* active = fused ? fz3 + (L - Lfirst) % 3 : cnt + cur_list;
-    check(cudaMemcpyAsync(&nn, active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
-    check(cudaMemcpyAsync(&lmax, level_max, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
+    check(cudaMemcpyAsync(ctl_host_, active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
+    check(cudaMemcpyAsync(ctl_host_ + 1, level_max, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
     check(cudaStreamSynchronize(st), "count");
+    const unsigned nn = ctl_host_[0], lmax = ctl_host_[1];
     if (nn == 0) {
       if (!tuning_) prefill_hist_[hist_key] = std::max<int>(Lfirst, (int)lmax);
       break;
@@ -495,6 +554,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     else ensure_levels(L);
     launch_wave(L);
   }
+  join_prefill();
   // statistics of this particle go to a pinned ring slot; collect() reads them when asked
   if ((int)pending_.size() >= kStatSlots) collect();
   const int slot = stats_slot_++ % kStatSlots;
@@ -516,9 +576,9 @@ void Engine::collect() {
   pending_.clear();
   if (profiling) collect_timings();
   unsigned err = 0;
-  check(cudaMemcpy(&err, cnt_.as<unsigned>() + 2, sizeof err, cudaMemcpyDeviceToHost), "error word");
+  check(cudaMemcpy(&err, cnt_.as<unsigned>() + kCntErr, sizeof err, cudaMemcpyDeviceToHost), "error word");
   if (err) {
-    check(cudaMemset(cnt_.as<unsigned>() + 2, 0, sizeof(unsigned)), "error word");
+    check(cudaMemset(cnt_.as<unsigned>() + kCntErr, 0, sizeof(unsigned)), "error word");
     if (err & 1u) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
     if (err & 8u) throw Error{OSC_ERR_STATE, "a sample-sum kernel variant was planned with another tile size"};
     throw Error{OSC_ERR_INVALID, kMixedGeometryMessage};

@@ -129,6 +129,13 @@ class Engine {
   static constexpr int kStageDoubles = 4096;
   unsigned long long* stats_host_ = nullptr;
   double* stage_host_ = nullptr;
+  // Device counter block cnt_ (16 words): [0], [1] survivor-list counts, [4..9] three 64-bit counters
+  // (not converged, samples, unit counter of the running wave), [12] highest finished level -- all
+  // zeroed by one memset of words 0..12 per request -- and [kCntErr] the sticky error word.
+  static constexpr int kCntErr = 15;
+  // pinned words the host reads back: [0] active count and [1] highest finished level between waves,
+  // [4..7] the batch statistics (two 64-bit counters), [8] the batch error word
+  unsigned* ctl_host_ = nullptr;
   static constexpr int kStatSlots = 64;
   cudaEvent_t stats_ev_[kStatSlots] = {};
   cudaEvent_t stage_ev_ = nullptr;
@@ -155,6 +162,8 @@ class Engine {
   uint64_t mrec_version_ = ~0ull;
   MixedFrame frame_{};
   void ensure_mixed(int L);
+  void reserve_mixed(int L);
+  void fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s);
   void compute_frame();
  public:
   int forced_variant[4] = {-1, -1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
@@ -185,6 +194,14 @@ class Engine {
   void use_stream(cudaStream_t s);
   void upload_trajectory();
   void ensure_levels(int L);
+  void reserve_levels(int L);
+  void fill_levels(int64_t s_begin, int64_t s_end, cudaStream_t s);
+  void prefill(bool mixed, int Lhead, int Lpre);
+  void join_prefill();
+  // side stream of the prefill (levels above the first wave's) and its fork / join events
+  cudaStream_t aux_ = nullptr;
+  cudaEvent_t fork_ev_ = nullptr, join_ev_ = nullptr;
+  bool join_pending_ = false;
   void run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,
                   cudaStream_t st);
   void check(cudaError_t e, const char* what);
