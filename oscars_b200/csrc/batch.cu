@@ -31,15 +31,18 @@ namespace osc {
 namespace dev {
 
 // ---------------------------------------------------------------------------------------------
-// Fields and RK4 on the device.  Same operations as the host model (TField3D_IdealUndulator /
-// TField3D_IdealEPU and TParticleA::RK4); sin and cos are CUDA's, so a trajectory agrees with the
-// host's to rounding, not bit for bit -- this path is the mixed-precision one.
+// Fields and RK4 on the device.  The host model's field formulas (TField3D_IdealUndulator /
+// TField3D_IdealEPU and TParticleA::RK4) with the per-field divisions replaced by constants
+// computed once on the host (DevField::k_arg, inv_half_period, shift) and CUDA's sin and cos, so a
+// trajectory agrees with the host's to rounding, not bit for bit -- this path is the mixed-precision
+// one.  The integrator is a serial FP64 dependency chain per (job, direction), so what bounds it is
+// the latency of each step's operations, not throughput.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ void pole_block_d(const DevField& f, const double* __restrict__ vals, const double* amp,
                                              double d, double shift, double tc, double* F) {
   const double L = f.length, lam = f.period_length;
   if (d > L / 2. + shift || d < -L / 2. + shift) return;
-  const double s = sin(2.0 * kPiD * (d - shift) / lam);
+  const double s = sin(f.k_arg * (d - shift));
   if (d < -L / 2. + shift + lam || d > L / 2. + shift - lam) {  // 1/4 and 3/4 end poles
     const double k = (d < -L / 2. + shift + lam / 2. || d > L / 2. + shift - lam / 2.) ? 0.25 : 0.75;
     F[0] += amp[0] * k * s * tc;
@@ -49,7 +52,7 @@ __device__ __forceinline__ void pole_block_d(const DevField& f, const double* __
   }
   double h = 1.0;
   if (f.n_half > 0) {  // half-period k of the full-strength region
-    int64_t k = (int64_t)((d - (-L / 2. + shift + lam)) / (lam / 2.));
+    int64_t k = (int64_t)((d - (-L / 2. + shift + lam)) * f.inv_half_period);
     k = k < 0 ? 0 : (k >= f.n_half ? f.n_half - 1 : k);
     h = vals[f.half_off + k];
   }
@@ -141,12 +144,8 @@ __device__ void field_sum_d(const DevField* __restrict__ fs, int nf, const doubl
                      (z - f.center[2]) * f.period_unit[2];
     const double tc = 1 + d * f.taper;
     double F[3] = {0, 0, 0};
-    if (f.kind == 0) {
-      pole_block_d(f, vals, f.a, d, f.phase * f.period_mag / (2.0 * kPiD), tc, F);
-    } else {  // EPU: A shifted by +phase/2, B by -phase/2 (src/TField3D_IdealEPU.cc:127-165)
-      pole_block_d(f, vals, f.a, d, f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
-      pole_block_d(f, vals, f.b, d, -f.phase / 2. * f.period_mag / (2.0 * kPiD), tc, F);
-    }
+    pole_block_d(f, vals, f.a, d, f.shift[0], tc, F);
+    if (f.kind == 1) pole_block_d(f, vals, f.b, d, f.shift[1], tc, F);  // EPU (src/TField3D_IdealEPU.cc:127-165)
     const double w = f.frequency == 0 ? 1.0 : cos(2.0 * kPiD * f.frequency * (t + f.time_offset) + f.frequency_phase);
     B[0] += F[0] * w;
     B[1] += F[1] * w;
@@ -163,7 +162,8 @@ struct Rk4Ctx {
 };
 
 __device__ __forceinline__ void derivs_d(Rk4Ctx& c, double t, const double* x, double* dxdt) {
-  const double one_minus = 1. - (x[1] * x[1] + x[3] * x[3] + x[5] * x[5]) / (kCLight * kCLight);
+  constexpr double kInvC2 = 1.0 / (kCLight * kCLight);
+  const double one_minus = 1. - (x[1] * x[1] + x[3] * x[3] + x[5] * x[5]) * kInvC2;
   if (one_minus <= 0) {  // a state at or above c: reported to the host, dxdt left as it was
     c.superluminal = true;
     return;
@@ -293,23 +293,69 @@ __global__ void k_batch_spline(const DevJob* __restrict__ jobs, int njobs, doubl
   const double* Y = X + (1 + c) * n;
   double* ypp = arena + J.knots + (10 + c) * n;
   double* u = work + J.u_off + c * n;
-  const double dydx0 = __ddiv_rn(__dsub_rn(Y[1], Y[0]), __dsub_rn(X[1], X[0]));
-  ypp[0] = -0.5;
-  u[0] = __dmul_rn(__ddiv_rn(3., __dsub_rn(X[1], X[0])),
-                   __dsub_rn(__ddiv_rn(__dsub_rn(Y[1], Y[0]), __dsub_rn(X[1], X[0])), dydx0));
-  for (int64_t i = 1; i < n - 1; ++i) {
-    const double sig = __ddiv_rn(__dsub_rn(X[i], X[i - 1]), __dsub_rn(X[i + 1], X[i - 1]));
-    const double p = __dadd_rn(__dmul_rn(sig, ypp[i - 1]), 2.0);
-    ypp[i] = __ddiv_rn(__dsub_rn(sig, 1.), p);
-    const double ui = __dsub_rn(__ddiv_rn(__dsub_rn(Y[i + 1], Y[i]), __dsub_rn(X[i + 1], X[i])),
-                                __ddiv_rn(__dsub_rn(Y[i], Y[i - 1]), __dsub_rn(X[i], X[i - 1])));
-    u[i] = __ddiv_rn(__dsub_rn(__ddiv_rn(__dmul_rn(6., ui), __dsub_rn(X[i + 1], X[i - 1])), __dmul_rn(sig, u[i - 1])), p);
+  // The sweeps carry the recurrence (ypp[i-1], u[i-1] forward, ypp[k+1] backward) in registers and
+  // read the knots through the read-only path a few points ahead, so each step waits only on its own
+  // arithmetic; the operations and their order are those of the reference's sweep.
+  const double dydx0 = __ddiv_rn(__dsub_rn(__ldg(Y + 1), __ldg(Y)), __dsub_rn(__ldg(X + 1), __ldg(X)));
+  double yp_prev = -0.5;
+  double u_prev = __dmul_rn(__ddiv_rn(3., __dsub_rn(__ldg(X + 1), __ldg(X))),
+                            __dsub_rn(__ddiv_rn(__dsub_rn(__ldg(Y + 1), __ldg(Y)), __dsub_rn(__ldg(X + 1), __ldg(X))),
+                                      dydx0));
+  ypp[0] = yp_prev;
+  u[0] = u_prev;
+  double xm = __ldg(X), x0 = __ldg(X + 1), ym = __ldg(Y), y0 = __ldg(Y + 1);
+  constexpr int B = 16;  // knots read per block of points, ahead of the block's recurrence
+  for (int64_t i0 = 1; i0 < n - 1; i0 += B) {
+    double xv[B], yv[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      const int64_t q = min(i0 + j + 1, n - 1);
+      xv[j] = __ldg(X + q);
+      yv[j] = __ldg(Y + q);
+    }
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      const int64_t i = i0 + j;
+      if (i < n - 1) {
+        const double xp = xv[j], yp = yv[j];
+        const double sig = __ddiv_rn(__dsub_rn(x0, xm), __dsub_rn(xp, xm));
+        const double p = __dadd_rn(__dmul_rn(sig, yp_prev), 2.0);
+        const double ypi = __ddiv_rn(__dsub_rn(sig, 1.), p);
+        const double ui = __dsub_rn(__ddiv_rn(__dsub_rn(yp, y0), __dsub_rn(xp, x0)),
+                                    __ddiv_rn(__dsub_rn(y0, ym), __dsub_rn(x0, xm)));
+        const double uu = __ddiv_rn(__dsub_rn(__ddiv_rn(__dmul_rn(6., ui), __dsub_rn(xp, xm)), __dmul_rn(sig, u_prev)), p);
+        ypp[i] = ypi;
+        u[i] = uu;
+        yp_prev = ypi;
+        u_prev = uu;
+        xm = x0; x0 = xp; ym = y0; y0 = yp;
+      }
+    }
   }
-  const double dydxn = __ddiv_rn(__dsub_rn(Y[n - 1], Y[n - 2]), __dsub_rn(X[n - 1], X[n - 2]));
-  const double un = __dmul_rn(__ddiv_rn(3., __dsub_rn(X[n - 1], X[n - 2])),
-                              __dsub_rn(dydxn, __ddiv_rn(__dsub_rn(Y[n - 1], Y[n - 2]), __dsub_rn(X[n - 1], X[n - 2]))));
-  ypp[n - 1] = __ddiv_rn(__dsub_rn(un, __dmul_rn(0.5, u[n - 2])), __dadd_rn(__dmul_rn(0.5, ypp[n - 2]), 1.));
-  for (int64_t k = n - 2; k >= 0; --k) ypp[k] = __dadd_rn(__dmul_rn(ypp[k], ypp[k + 1]), u[k]);
+  const double dydxn = __ddiv_rn(__dsub_rn(__ldg(Y + n - 1), __ldg(Y + n - 2)), __dsub_rn(__ldg(X + n - 1), __ldg(X + n - 2)));
+  const double un = __dmul_rn(__ddiv_rn(3., __dsub_rn(__ldg(X + n - 1), __ldg(X + n - 2))),
+                              __dsub_rn(dydxn, __ddiv_rn(__dsub_rn(__ldg(Y + n - 1), __ldg(Y + n - 2)),
+                                                         __dsub_rn(__ldg(X + n - 1), __ldg(X + n - 2)))));
+  double next = __ddiv_rn(__dsub_rn(un, __dmul_rn(0.5, u_prev)), __dadd_rn(__dmul_rn(0.5, yp_prev), 1.));
+  ypp[n - 1] = next;
+  int64_t k = n - 2;
+  for (; k >= 7; k -= 8) {  // blocks of 8: the block's forward-sweep values are read before its stores
+    double yv[8], uv[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      yv[j] = ypp[k - j];
+      uv[j] = u[k - j];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      next = __dadd_rn(__dmul_rn(yv[j], next), uv[j]);
+      ypp[k - j] = next;
+    }
+  }
+  for (; k >= 0; --k) {
+    next = __dadd_rn(__dmul_rn(ypp[k], next), u[k]);
+    ypp[k] = next;
+  }
 }
 
 // Level samples [s_begin, s_end) of every job whose active count is non-zero (all jobs when `cnt` is
@@ -738,7 +784,7 @@ static cudaError_t launch_batch_wave(const BatchWaveArgs& a, int grid, int varia
 namespace {
 constexpr int kBatchPrefill = 13;        // levels enqueued without the host (records kept resident)
 constexpr int kBatchMinSpan = 128;
-constexpr int kBatchMaxJobsPerChunk = 4096;
+constexpr int kBatchMaxJobsPerChunk = 8192;
 }  // namespace
 
 DevField to_dev_field(FieldSpec f, std::vector<double>& vals) {
@@ -781,6 +827,14 @@ DevField to_dev_field(FieldSpec f, std::vector<double>& vals) {
   d.phase = f.phase; d.taper = f.taper; d.frequency = f.frequency; d.frequency_phase = f.frequency_phase;
   d.time_offset = f.time_offset; d.period_length = f.period_length; d.period_mag = mag(f.period);
   d.length = f.length;
+  d.k_arg = 2.0 * kPi / f.period_length;
+  d.inv_half_period = 2.0 / f.period_length;
+  if (f.kind == 0) {
+    d.shift[0] = f.phase * d.period_mag / (2.0 * kPi);
+  } else {  // EPU: A shifted by +phase/2, B by -phase/2
+    d.shift[0] = f.phase / 2. * d.period_mag / (2.0 * kPi);
+    d.shift[1] = -f.phase / 2. * d.period_mag / (2.0 * kPi);
+  }
   return d;
 }
 
@@ -919,14 +973,31 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
   check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
   const size_t budget = std::min<size_t>(free_b / 2, (size_t)64 << 30);
   const int64_t rec_per_job = (int64_t)2 << Lpre;  // levels 0..Lpre, sample s at index s
+  auto job_bytes = [&](const DevJob& d) {
+    return sizeof(double) * 28 * ((size_t)d.nf + d.nb) + kMixedRecordBytesPerSample * (size_t)rec_per_job +
+           (size_t)(d.n_obs * d.n_e) * (56 + 8 + 4 + 8 + 16 * kFdPartials);
+  };
+  // Chunks: the jobs that fit the budget from the start, then, when more than one chunk is needed,
+  // the same number of chunks with the jobs spread evenly (each chunk runs its serial RK4 once, so
+  // fewer, fuller chunks are faster).
+  size_t fit = 0;
+  {
+    size_t bytes = 0;
+    while (fit < dj.size() && fit < (size_t)kBatchMaxJobsPerChunk) {
+      const size_t need = job_bytes(dj[fit]);
+      if (fit > 0 && bytes + need > budget) break;
+      bytes += need;
+      ++fit;
+    }
+  }
+  const size_t n_chunks = (dj.size() + fit - 1) / fit;
+  const size_t per_chunk = (dj.size() + n_chunks - 1) / n_chunks;
   size_t done_entries = 0;
   size_t j0 = 0;
   while (j0 < dj.size()) {
     size_t j1 = j0, bytes = 0;
-    while (j1 < dj.size() && j1 - j0 < (size_t)kBatchMaxJobsPerChunk) {
-      const DevJob& d = dj[j1];
-      const size_t need = sizeof(double) * 28 * ((size_t)d.nf + d.nb) + kMixedRecordBytesPerSample * (size_t)rec_per_job +
-                          (size_t)(d.n_obs * d.n_e) * (56 + 8 + 4 + 8 + 16 * kFdPartials);
+    while (j1 < dj.size() && j1 - j0 < per_chunk) {
+      const size_t need = job_bytes(dj[j1]);
       if (j1 > j0 && bytes + need > budget) break;
       bytes += need;
       ++j1;

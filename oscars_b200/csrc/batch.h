@@ -18,6 +18,9 @@ struct DevField {
   double a[3], b[3], center[3], period_unit[3];
   double phase, taper, frequency, frequency_phase, time_offset;
   double period_length, period_mag, length;
+  // per-field constants of the device evaluation: 2 pi / period length, 2 / period length, and the
+  // pole-block shifts (undulator: shift[0]; EPU: A at shift[0], B at shift[1])
+  double k_arg, inv_half_period, shift[2];
   // undulator half-period factors: n_half values at half_off of the batch's value array (0: none)
   int64_t half_off;
   int n_half;
