@@ -233,6 +233,17 @@ OSC_API int osc_flux_multi(osc_ctx* ctx, const double* obs_xyz, long long n_obs,
 OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double* normals,
                               long long n_obs, int directional, const osc_rad_opts* opts,
                               double* out, int32_t* level_out, long long* n_not_converged);
+/* Power density on the facets of STL meshes (replaces OSCARSSR::CalculatePowerDensitySTL,
+ * src/OSCARSSR.cc:3154-3521, behind OSCARSSR_Python.cc:6993 calculate_power_density_stl).
+ * facets: n x 12 doubles = vertices A, B, C and the normal as stored; centers: n x 3 (the facet
+ * centres, each the mean of its vertices before the mesh was translated, then translated).  For
+ * every facet the trajectory samples whose ray to the centre crosses another facet are skipped.
+ * out / level_out: n values / stop levels; a facet that does not stop reports the level of the last
+ * facet before it that did (the reference's Result_Level), counted in n_not_converged.  opts: the
+ * precision, levels, nparticles and quantity fields are used. */
+OSC_API int osc_power_density_stl(osc_ctx* ctx, const double* facets, const double* centers, long long n,
+                                  const osc_rad_opts* opts, double* out, int32_t* level_out,
+                                  long long* n_not_converged);
 
 /* ---- batches of independent jobs (no reference counterpart: the reference integrates one
  *      particle through one field container per call).  Job k is the ideal particle of a beam of

@@ -86,6 +86,8 @@ def load():
                                  D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ip]
     lib.orc_power_density.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_long, ctypes.c_int, D,
                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ip]
+    lib.orc_power_density_stl.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_long, D, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, dp, ip]
     _lib = lib
     return lib
 
@@ -425,6 +427,33 @@ def _quantity(q, pd=False):
     raise ValueError("'quantity' must be: 'flux', 'precision', 'level', or blank")
 
 
+def read_stl(path, scale=1.0, translation=(0.0, 0.0, 0.0)):
+    """TTriangle3DContainer::ReadSTLFile (src/TTriangle3DContainer.cc:109-214): binary STL, vertices
+    float x scale, normals as stored, centre (A + B + C) / 3 before the translation, then vertices and
+    centre translated; the rotations argument is reset before it is applied (identity).  Returns
+    (n x 12 array of A, B, C, N; n x 3 centres)."""
+    import struct
+    with open(path, "rb") as f:
+        data = f.read()
+    n = struct.unpack_from("<I", data, 80)[0]
+    tri = np.zeros((n, 12))
+    cen = np.zeros((n, 3))
+    T = [float(v) for v in translation]
+    for i in range(n):
+        vals = struct.unpack_from("<12f", data, 84 + 50 * i)
+        N, A, B, C = vals[0:3], vals[3:6], vals[6:9], vals[9:12]
+        A = [a * scale for a in A]
+        B = [b * scale for b in B]
+        C = [c * scale for c in C]
+        ce = [((A[k] + B[k]) + C[k]) / 3. for k in range(3)]
+        tri[i, 0:3] = [A[k] + T[k] for k in range(3)]
+        tri[i, 3:6] = [B[k] + T[k] for k in range(3)]
+        tri[i, 6:9] = [C[k] + T[k] for k in range(3)]
+        tri[i, 9:12] = N
+        cen[i] = [ce[k] + T[k] for k in range(3)]
+    return tri, cen
+
+
 class OracleSR:
     """CPU oracle with the ``oscars.sr.sr`` method names used on the radiation hot path."""
 
@@ -712,6 +741,30 @@ class OracleSR:
         pos = xyz if dim == 3 else x1x2
         return [[list(pos[i]), float(out[i])] for i in range(n)]
 
+
+    # ---- STL surfaces (src/OSCARSSR_Python.cc:6852-7212, src/TSTLContainer.cc) ---------------------
+    def add_stl(self, ifile, rotations=None, translation=None, scale=1, name=""):
+        if not hasattr(self, "_stl"):
+            self._stl = []
+        t = _v3(translation, "translation") if translation is not None else [0.0, 0.0, 0.0]
+        tri, cen = read_stl(ifile, float(scale), t)
+        self._stl.append((name or "_stl%d" % len(self._stl), tri, cen))
+
+    def calculate_power_density_stl(self, farfield_origin, ofile="", bofile="", stlofile="", nparticles=0, gpu=-1,
+                                    ngpu=None, nthreads=0, precision=0.01, max_level=-2, max_level_extended=0,
+                                    quantity="power density"):
+        stl = getattr(self, "_stl", [])
+        tri = np.ascontiguousarray(np.vstack([t for _, t, _ in stl]) if stl else np.zeros((0, 12)))
+        cen = np.ascontiguousarray(np.vstack([c for _, _, c in stl]) if stl else np.zeros((0, 3)))
+        q = _quantity(quantity, pd=True)
+        n = tri.shape[0]
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        self._check(self._lib.orc_power_density_stl(self._h, _dp(tri), _dp(cen), n, float(precision), int(max_level),
+                                                    int(max_level_extended), int(nparticles), q, _dp(out),
+                                                    lv.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.last_levels = lv
+        return [[[list(tri[i, 0:3]), list(tri[i, 3:6]), list(tri[i, 6:9])], float(out[i])] for i in range(n)]
 
     def _points_call(self, points, rotations, translation, invert):
         r = _v3(rotations) if rotations else [0.0, 0.0, 0.0]

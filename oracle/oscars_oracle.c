@@ -1179,3 +1179,110 @@ int orc_power_density(orc_sim* s, const double* obs, const double* normals, long
   free(comp);
   return ORC_OK;
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * Power density on STL facets: OSCARSSR::CalculatePowerDensityPointsSTL (src/OSCARSSR.cc:3318-3521,
+ * the Mode 2 path: a sample is skipped when any other facet lies between it and the facet centre)
+ * with TTriangle3D::RayIntersectionDistance (src/TTriangle3D.cc, Moller-Trumbore).
+ * tri: n x 12 (vertices A, B, C, normal N as stored); centers: n x 3 (TTriangle3D::fCenter).
+ * ------------------------------------------------------------------------------------------- */
+static double ray_intersection_distance(const double* T, v3 origin, v3 dir_in) {
+  v3 A = V(T[0], T[1], T[2]), B = V(T[3], T[4], T[5]), C = V(T[6], T[7], T[8]);
+  v3 dir = vunit(dir_in);
+  v3 edge1 = vsub(B, A), edge2 = vsub(C, A);
+  v3 pvec = vcross(dir, edge2);
+  double det = vdot(edge1, pvec);
+  if (det > -1e-12 && det < 1e-12) return -1;
+  double inv_det = 1.0 / det;
+  v3 tvec = vsub(origin, A);
+  double u = vdot(tvec, pvec) * inv_det;
+  if (u < 0.0 || u > 1.0) return -1;
+  v3 qvec = vcross(tvec, edge1);
+  double v = vdot(dir, qvec) * inv_det;
+  if (v < 0.0 || u + v > 1.0) return -1;
+  double t = vdot(edge2, qvec) * inv_det;
+  if (t < 0) return -1;
+  return t;
+}
+
+int orc_power_density_stl(orc_sim* s, const double* tri, const double* centers, long n, double precision,
+                          int max_level, int max_level_extended, int nparticles, int quantity, double* out,
+                          int* out_level) {
+  int lstop_mem = max_level >= -1 && max_level <= MAX_LEVEL_MEMORY ? max_level : MAX_LEVEL_MEMORY;
+  int lstop_ext = max_level_extended > lstop_mem ? max_level_extended : lstop_mem;
+  for (long i = 0; i < n; ++i) out[i] = 0;
+  int np = nparticles > 0 ? nparticles : 1;
+  double weight = nparticles > 0 ? 1.0 / (double)nparticles : 1;
+  for (int ip = 0; ip < np; ++ip) {
+    int rc;
+    if (nparticles > 0) {
+      if ((rc = orc_set_new_particle(s, 0))) return rc;
+      if ((rc = orc_calculate_trajectory(s))) return rc;
+    } else if ((rc = ensure_trajectory(s))) return rc;
+    double scale = fabs(s->p.q * s->p.current) / (16 * (K_PI * K_PI) * K_EPS0 * K_C);
+    /* Result_Precision and Result_Level live outside the loop over facets (:3348-3349) */
+    double result_precision = -1;
+    int result_level = -1;
+    for (long i = 0; i < n; ++i) {
+      v3 obs = V(centers[3 * i], centers[3 * i + 1], centers[3 * i + 2]);
+      v3 normal = V(tri[12 * i + 9], tri[12 * i + 10], tri[12 * i + 11]);
+      double last_sum = -1, sum = 0;
+      int last_level = 0;
+      for (int L = 0; L <= lstop_ext; ++L) {
+        last_level = L;
+        v3 last_beta = V(0, 0, 0);
+        double bdmax = -1;
+        level_view lv;
+        if (level_open(&s->tr, L, lstop_mem, &lv)) return fail(s, ORC_ERR_ALLOC, "alloc");
+        for (long it = 0; it != lv.np; ++it) {
+          double T; v3 X, B, A;
+          level_point(&s->tr, &lv, it, &T, &X, &B, &A);
+          int blocked = 0;
+          for (long j = 0; j != n; ++j) {
+            if (j == i) continue;
+            v3 to = vsub(obs, X);
+            double d = ray_intersection_distance(tri + 12 * j, X, vunit(to));
+            if (d > 0 && d < vmag(to)) { blocked = 1; break; }
+          }
+          if (blocked) continue;
+          double bd = vmag(vsub(B, last_beta));
+          if (it > 0 && bd > bdmax) bdmax = bd;
+          last_beta = B;
+          v3 N1 = vunit(vsub(obs, X));
+          v3 N2 = vunit(vorthogonal(N1));
+          v3 N3 = vunit(vcross(N1, N2));
+          double n1dn = fabs(vdot(N1, normal));
+          v3 num = vcross(N1, vcross(vsub(N1, B), A));
+          double den = pow(1 - vdot(B, N1), 5);
+          double m2 = vmag2(vsub(obs, X));
+          double d2 = vdot(num, N2), d3 = vdot(num, N3);
+          sum += pow(d2, 2) / den / m2 * n1dn;
+          sum += pow(d3, 2) / den / m2 * n1dn;
+        }
+        double ts = sum * delta_t_inclusive(&s->tr, L);
+        result_precision = fabs(ts - last_sum) / last_sum;
+        if ((L > 8 && result_precision < precision && bdmax < 2. / s->p.gamma) ||
+            (L > 8 && bdmax < 2. / s->p.gamma && ts == last_sum)) {
+          result_level = L;
+          break;
+        } else if (L > 8 && ts == last_sum) {
+          result_level = L;
+          result_precision = 0;
+          break;
+        }
+        last_sum = ts;
+      }
+      sum *= scale * delta_t_inclusive(&s->tr, last_level);
+      sum /= 1e6;
+      double v;
+      switch (quantity) {
+        case 1: v = result_precision * weight; break;
+        case 2: v = ((double)result_level) * weight; break;
+        default: v = sum * weight; break;
+      }
+      out[i] = v + out[i];  /* TTriangle3D::AddToValue */
+      if (out_level) out_level[i] = result_level;
+    }
+  }
+  return ORC_OK;
+}

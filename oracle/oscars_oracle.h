@@ -91,6 +91,12 @@ int orc_spectrum(orc_sim*, const double obs[3], const double* energies_eV, long 
 int orc_power_density(orc_sim*, const double* obs, const double* normals, long n_obs,
                       int directional, double precision, int max_level, int max_level_extended,
                       int nparticles, int quantity, double* out, int* out_level);
+/* Power density on STL facets (tri: n x 12 = vertices A, B, C and normal; centers: n x 3).  out_level
+ * receives the level the reference's Result_Level holds after each facet (carried over from the
+ * previous facet when one does not converge). */
+int orc_power_density_stl(orc_sim*, const double* tri, const double* centers, long n, double precision,
+                          int max_level, int max_level_extended, int nparticles, int quantity, double* out,
+                          int* out_level);
 
 #ifdef __cplusplus
 }

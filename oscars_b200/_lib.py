@@ -80,6 +80,7 @@ SIGNATURES = {
     "osc_spectrum": (I, [VP, DP, DP, LL, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
     "osc_flux_multi": (I, [VP, DP, LL, DP, LL, ctypes.POINTER(RadOpts), I, DP, I32P, LLP]),
     "osc_power_density": (I, [VP, DP, DP, LL, I, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
+    "osc_power_density_stl": (I, [VP, DP, DP, LL, ctypes.POINTER(RadOpts), DP, I32P, LLP]),
     "osc_flux_device": (I, [VP, VP, LL, D, ctypes.POINTER(RadOpts), VP, VP, VP]),
     "osc_power_density_device": (I, [VP, VP, VP, LL, I, ctypes.POINTER(RadOpts), VP, VP, VP]),
     "osc_batch_flux": (I, [VP, ctypes.POINTER(FieldDesc), I, ctypes.POINTER(JobDesc), I, DP, LL, DP, LL,

@@ -28,7 +28,7 @@ HOST_FLAGS = ["-O3", "-fPIC", "-ffp-contract=off", "-fvisibility=hidden", "-pthr
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xptxas=-v"] + \
     sum([["-Xcompiler", f] for f in HOST_FLAGS], [])
 
-CU_SOURCES = ["kernels_fp64.cu", "kernels_mixed.cu", "engine.cu", "noalloc.cu", "batch.cu", "adjoint.cu"]
+CU_SOURCES = ["kernels_fp64.cu", "kernels_mixed.cu", "kernels_stl.cu", "engine.cu", "stl.cu", "noalloc.cu", "batch.cu", "adjoint.cu"]
 CC_SOURCES = ["host_core.cc", "capi.cc"]
 HEADERS = ["host_core.h", "engine.h", "kernels.h", "batch.h", "device_common.cuh", "fd_common.cuh"]
 

@@ -637,6 +637,17 @@ OSC_API int osc_power_density(osc_ctx* ctx, const double* obs_xyz, const double*
   });
 }
 
+OSC_API int osc_power_density_stl(osc_ctx* ctx, const double* facets, const double* centers, long long n,
+                                  const osc_rad_opts* opts, double* out, int32_t* level_out,
+                                  long long* n_not_converged) {
+  return guarded(ctx, [&] {
+    check_opts(opts);
+    if (n < 0 || (n > 0 && (!facets || !centers || !out))) throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
+    ctx->eng->power_density_stl(facets, centers, n, *opts, out, level_out);
+    if (n_not_converged) *n_not_converged = ctx->eng->last_not_converged;
+  });
+}
+
 OSC_API int osc_flux_device(osc_ctx* ctx, const double* d_obs_xyz, long long n_obs, double energy_eV,
                             const osc_rad_opts* opts, double* d_out, int32_t* d_level, void* stream) {
   return guarded(ctx, [&] {

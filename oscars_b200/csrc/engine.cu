@@ -89,7 +89,8 @@ Engine::~Engine() {
   for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
                     &act_[1], &cnt_, &acc_, &acc_comp_, &mrec_, &b_fields_, &b_fvals_, &b_obs_, &b_omega_, &b_acc_, &b_jobs_,
                     &b_knots_, &b_work_, &b_rec_, &b_rec_ext_, &b_state_, &b_out_, &b_lvl_, &b_act_[0], &b_act_[1],
-                    &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_, &fused_})
+                    &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_, &fused_, &stl_geo_, &stl_cen_, &stl_nrm_,
+                    &stl_state_, &stl_flags_})
     b->release();
   if (stream) cudaStreamDestroy(stream);
   if (aux_) cudaStreamDestroy(aux_);

@@ -94,6 +94,10 @@ class Engine {
   // Gradient of <knot_grad, knots> (knot_grad: host, 9 x n in the knot layout x y z bx by bz ax ay az)
   // with respect to the half-period factors: reverse mode through the RK4 steps.
   void trajectory_vjp(const double* knot_grad, double* grad_params, int64_t n_params);
+  // Power density on STL facets (tri: host n x 12 = vertices A, B, C and stored normal; centers:
+  // host n x 3), src/OSCARSSR.cc:3154-3521; `out` / `level_out` (host) per facet.
+  void power_density_stl(const double* tri, const double* centers, int64_t n, const osc_rad_opts& o, double* out,
+                         int32_t* level_out);
   bool use_graphs = true;            // replay the batched front of a known shape as a CUDA graph
   long long graph_launches() const { return graph_launches_; }
 
@@ -198,6 +202,8 @@ class Engine {
   void fill_levels(int64_t s_begin, int64_t s_end, cudaStream_t s);
   void prefill(bool mixed, int Lhead, int Lpre);
   void join_prefill();
+  // STL request buffers: facet geometry (A, B - A, C - A), centres, normals, per-facet state and flags
+  DevBuf stl_geo_, stl_cen_, stl_nrm_, stl_state_, stl_flags_;
   // side stream of the prefill (levels above the first wave's) and its fork / join events
   cudaStream_t aux_ = nullptr;
   cudaEvent_t fork_ev_ = nullptr, join_ev_ = nullptr;

@@ -146,6 +146,23 @@ struct PdFinalArgs {
   unsigned* level_max;      // highest level at which an entry finished (may be NULL)
 };
 
+// One level of the STL power density (kernels_stl.cu): one CTA per facet not yet done.
+struct StlLevelArgs {
+  const double* lev;        // FP64 level cache (10 arrays of cap doubles)
+  int64_t cap;
+  const double* geometry;   // n x 9: vertex A, B - A, C - A of each facet
+  const double* centers;    // n x 3: facet centres (the observation points)
+  const double* normals;    // n x 3: stored facet normals
+  int64_t n;
+  int level;
+  double dt_level, precision, two_over_gamma;
+  double* state;            // n x 4: running sum, last level value, result precision, last level
+  int* done;                // n: stopped
+  int* level_out;           // n: level at which the facet stopped (-1 set by the host beforehand)
+  unsigned* n_active;       // facets not stopped after this level (zeroed by the host per level)
+};
+cudaError_t launch_stl_level(const StlLevelArgs& a, cudaStream_t st);
+
 // Frame of the mixed-precision path: origin x0 (particle start), rows of rot = e1, e2, e3 with e3 the
 // initial direction; xperp_max / z_max bound the trajectory in that frame; t_ref = t0 / c;
 // theta_max = the largest observer angle the path accepts (mixed_theta_max of the particle's gamma);

@@ -24,6 +24,7 @@ import sys
 import numpy as np
 
 from . import _lib, fileio
+from .stl import StlContainer
 from ._lib import BeamDesc, Context, FieldDesc, RadOpts, dptr, i32ptr
 
 _ANGLE_UNSET = 112188979912321.0  # binding sentinel for "angle not given" (:5662)
@@ -91,7 +92,7 @@ def _quantity(q, pd=False):
         return 1
     if Q == "LEVEL":
         return 2
-    raise ValueError("'quantity' must be: 'flux', 'precision', 'level', or blank")
+    raise ValueError("'quantity' must be: '%s', 'precision', 'level', or blank" % ("power density" if pd else "flux"))
 
 
 def _compute_mode(compute):
@@ -114,6 +115,7 @@ class sr:
         self._gpu_global = 1
         self._nthreads_global = nthreads if nthreads > 0 else 2
         self._nbeams = 0
+        self._stl = StlContainer()
 
     # ---- global settings ------------------------------------------------------------------------
     def set_gpu_global(self, gpu):
@@ -631,6 +633,54 @@ class sr:
         self._report(nnc)
         self._write_points(ofile, bofile, xyz if dim == 3 else x12, out, dim)
         return self._points_result(xyz if dim == 3 else x12, out, return_numpy)
+
+    # ---- STL surfaces (src/OSCARSSR_Python.cc:6852-7280, 9262-9276) ----------------------------------
+    def add_stl(self, ifile, rotations=None, translation=None, scale=1, name=""):
+        """Import a binary STL mesh: vertices times `scale`, then translated; `rotations` is accepted
+        and, as in the reference, not applied."""
+        if rotations is not None:
+            _vec3(rotations, "rotations")
+        t = _vec3(translation, "translation") if translation is not None else [0.0, 0.0, 0.0]
+        self._stl.add(ifile, float(scale), t, name)
+
+    def clear_stl(self):
+        self._stl.clear()
+
+    def remove_stl(self, name):
+        self._stl.remove(name)
+
+    def print_stl(self):
+        sys.stdout.write(self._stl.describe())
+
+    def calculate_power_density_stl(self, farfield_origin, ofile="", bofile="", stlofile="", nparticles=0, gpu=-1,
+                                    ngpu=None, nthreads=0, precision=0.01, max_level=-2, max_level_extended=0,
+                                    quantity="power density"):
+        """Power density [W/mm^2] at the centre of every facet of the STL objects, each trajectory
+        sample skipped when another facet lies between it and the centre (src/OSCARSSR.cc:3154-3521);
+        returns [[[A], [B], [C]], P] per facet.  As in the reference binding, ofile and bofile write
+        nothing for this call and stlofile re-exports the meshes (TSTLContainer::WriteSTLFile);
+        farfield_origin is read and not used (the reference's shadowing mode that used it is off)."""
+        if self._nbeams < 1:
+            raise ValueError("No particle beam defined")
+        _vec3(farfield_origin, "farfield_origin")
+        if nparticles < 0:
+            raise ValueError("'nparticles' must be >= 1 (sort of)")
+        self._check_gpu(gpu, nthreads)
+        q = _quantity(quantity, pd=True)
+        o = self._opts("", _ANGLE_UNSET, None, None, precision, max_level, max_level_extended, nparticles, q, "fp64")
+        facets, centers = self._stl.facets()
+        n = facets.shape[0]
+        out = np.zeros(n)
+        lv = np.zeros(n, dtype=np.int32)
+        nnc = ctypes.c_longlong()
+        if n:
+            self._ctx.call("osc_power_density_stl", dptr(facets), dptr(centers), n, ctypes.byref(o), dptr(out),
+                           i32ptr(lv), ctypes.byref(nnc))
+        self.last_levels = lv
+        if stlofile:
+            self._stl.write_stl(stlofile)
+        return [[[facets[i, 0:3].tolist(), facets[i, 3:6].tolist(), facets[i, 6:9].tolist()], float(out[i])]
+                for i in range(n)]
 
     def last_stats(self):
         """(samples integrated, kernel launches) of the last radiation call."""

@@ -29,6 +29,9 @@ def traj(n=20001, a=-1.5, b=1.5):
 
 
 UND_SETUP = [UND, BEAM] + traj()
+UND_SHORT = ("add_bfield_undulator", dict(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=11, phase=-math.pi / 2))
+UND_SHORT_SETUP = [UND_SHORT, BEAM] + traj(5001, -0.5, 0.5)
+STL_PD = ("calculate_power_density_stl", dict(farfield_origin=[0, 0, 0], max_level=12))
 EPU_SETUP = [EPU_Y, EPU_X, BEAM] + traj(16001)
 
 
@@ -69,6 +72,55 @@ def write_field_files():
 
 def field_file(name):
     return os.path.join(FIELDS, name)
+
+
+# ---- STL meshes (binary STL: 80-byte header, triangle count, 50-byte records N A B C attribute) ----
+STL_DIR = os.path.join(HERE, "stl")
+
+
+def stl_file(name):
+    return os.path.join(STL_DIR, name)
+
+
+def _write_stl(path, tris):
+    """tris: list of (normal, A, B, C) 3-vectors, written as float32."""
+    import struct
+    with open(path, "wb") as f:
+        f.write(b"parity mesh".ljust(80, b"\0"))
+        f.write(struct.pack("<I", len(tris)))
+        for n, a, b, c in tris:
+            f.write(struct.pack("<12fH", *(list(n) + list(a) + list(b) + list(c)), 0))
+
+
+def _grid_plate(nx, ny, x0, x1, y0, y1, normal, z_of=lambda x, y: 0.0, normal_of=None):
+    tris = []
+    for i in range(nx):
+        for j in range(ny):
+            xa, xb = x0 + (x1 - x0) * i / nx, x0 + (x1 - x0) * (i + 1) / nx
+            ya, yb = y0 + (y1 - y0) * j / ny, y0 + (y1 - y0) * (j + 1) / ny
+            p00, p10 = (xa, ya, z_of(xa, ya)), (xb, ya, z_of(xb, ya))
+            p01, p11 = (xa, yb, z_of(xa, yb)), (xb, yb, z_of(xb, yb))
+            k = 2 * (i * ny + j)
+            tris.append((normal_of(k) if normal_of else normal, p00, p10, p11))
+            tris.append((normal_of(k + 1) if normal_of else normal, p00, p11, p01))
+    return tris
+
+
+def write_stl_files():
+    """Write the meshes under stl/ (deterministic; the committed copies are what the tests and the
+    fixtures read).  plate.stl: 20 mm x 20 mm in the XY plane, 4 x 4 squares as 32 triangles, normal
+    +z.  shield_mm.stl: a 6 mm x 3.3 mm rectangle in millimetres (2 triangles, normal -z), used with
+    scale 0.001; at 10 m in front of the plate at 20 m its upper edge shadows the facets centred at
+y = 6.67 mm from part of the 1 m trajectory only.  tilted.stl: 3 x 3 squares of 12 mm, tilted 30 degrees about x, stored normals of
+    length 2 (as some exporters write them) and one zero normal."""
+    os.makedirs(STL_DIR, exist_ok=True)
+    _write_stl(stl_file("plate.stl"), _grid_plate(4, 4, -0.01, 0.01, -0.01, 0.01, (0.0, 0.0, 1.0)))
+    _write_stl(stl_file("shield_mm.stl"), _grid_plate(1, 1, -3.0, 3.0, 0.0, 3.3, (0.0, 0.0, -1.0)))
+    t = math.radians(30)
+    nrm = (0.0, -2 * math.sin(t), 2 * math.cos(t))
+    _write_stl(stl_file("tilted.stl"), _grid_plate(3, 3, -0.006, 0.006, -0.006, 0.006, nrm,
+                                                   z_of=lambda x, y: y * math.tan(t),
+                                                   normal_of=lambda k: (0.0, 0.0, 0.0) if k == 7 else nrm))
 
 
 def halfscale_41():
@@ -187,6 +239,31 @@ CASES = {
     "pd_points": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, rotations=[0.0, 0.001, 0.0], translation=[0.0, 0.0005, 0.0]))],
     "pd_points_directional": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS_MIXED, normal=1))],
     "pd_points_inverted": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, normal=-1))],
+    # power density on STL facets (11-period undulator, 1 m trajectory, levels up to 12): a plate in
+    # the beam, the plate partly shadowed by a shield (millimetre file, scale 0.001), a tilted plate
+    # with stored normals of length 2 and one zero normal (also capped at level 10, where facets that
+    # do not stop report the previous facet's level), the precision of the shadowed case, and a
+    # 3-particle beam on the plate
+    "stl_plate": UND_SHORT_SETUP + [("add_stl", dict(ifile="plate.stl", translation=[0, 0, 20])), STL_PD],
+    "stl_shadow": UND_SHORT_SETUP + [("add_stl", dict(ifile="plate.stl", translation=[0, 0, 20], name="plate")),
+                                     ("add_stl", dict(ifile="shield_mm.stl", scale=0.001, translation=[0, 0, 10],
+                                                      name="shield")), STL_PD],
+    "stl_tilted": UND_SHORT_SETUP + [("add_stl", dict(ifile="tilted.stl", translation=[0, 0.002, 25],
+                                                      rotations=[0.3, 0, 0])),
+                                     ("calculate_power_density_stl", dict(farfield_origin=[0, 0, 0], max_level=12,
+                                                                          precision=0.0005))],
+    "stl_tilted_capped": UND_SHORT_SETUP + [("add_stl", dict(ifile="tilted.stl", translation=[0, 0.002, 25])),
+                                            ("calculate_power_density_stl", dict(farfield_origin=[0, 0, 0], max_level=10,
+                                                                                 precision=0.0005))],
+    "stl_shadow_precision": UND_SHORT_SETUP + [("add_stl", dict(ifile="plate.stl", translation=[0, 0, 20])),
+                                               ("add_stl", dict(ifile="shield_mm.stl", scale=0.001,
+                                                                translation=[0, 0, 10])),
+                                               ("calculate_power_density_stl", dict(farfield_origin=[0, 0, 0],
+                                                                                    max_level=12,
+                                                                                    quantity="precision"))],
+    "stl_beam": [UND_SHORT, BEAM_GAUSS, ("set_seed", dict(seed=7))] + traj(5001, -0.5, 0.5) +
+                [("add_stl", dict(ifile="plate.stl", translation=[0, 0, 20])),
+                 ("calculate_power_density_stl", dict(farfield_origin=[0, 0, 0], max_level=12, nparticles=3))],
 }
 
 
@@ -200,6 +277,9 @@ def run_case(obj, calls):
             out = obj.set_npoints_trajectory(kw["n"])
         elif name == "set_seed":
             out = obj.set_seed(kw["seed"])
+        elif name == "add_stl":
+            kw = dict(kw, ifile=stl_file(kw["ifile"]))
+            out = obj.add_stl(**kw)
         elif name == "add_bfield_file":
             kw = dict(kw, ifile=field_file(kw["ifile"]))
             out = obj.add_bfield_file(**kw)

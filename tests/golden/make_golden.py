@@ -9,6 +9,7 @@ per-entry stop levels from a second ``quantity='level'`` call where the case ret
     python tests/golden/make_golden.py flux_und_41
     python tests/golden/make_golden.py files      # the reference's output files (files.npz)
     python tests/golden/make_golden.py adjoint_fd # finite-difference gradients (adjoint_fd.npz)
+    python tests/golden/make_golden.py stl_files  # the mesh file of stlofile (stl_files.npz)
 """
 import os
 import subprocess
@@ -99,6 +100,23 @@ def make_files(S):
     np.savez_compressed(os.path.join(HERE, "files.npz"), **out)
 
 
+def make_stl_file(S):
+    """The mesh file the reference writes for calculate_power_density_stl(stlofile=...) on the plate
+    and the shield (stl_files.npz: the bytes after the 80-byte header, which the reference leaves
+    partly uninitialised)."""
+    import tempfile
+    from cases import stl_file
+    obj = S.sr(nthreads=1, gpu=0)
+    run_case(obj, CASES["stl_shadow"][:-1])
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "out.stl")
+        obj.calculate_power_density_stl([0, 0, 0], stlofile=path, nthreads=1, max_level=9)
+        with open(path, "rb") as f:
+            data = f.read()
+    np.savez_compressed(os.path.join(HERE, "stl_files.npz"), head=np.frombuffer(data[:37], dtype=np.uint8),
+                        body=np.frombuffer(data[80:], dtype=np.uint8))
+
+
 def make_adjoint(S):
     """Central finite differences of loss = sum (F(s) - F(1))^2 over the adjoint configuration, every
     one of the 82 half-period factors, with the reference's CPU path (the scaled undulator given to it
@@ -147,6 +165,10 @@ def main(argv):
     if argv[1:] == ["files"]:
         make_files(S)
         print("wrote files")
+        return
+    if argv[1:] == ["stl_files"]:
+        make_stl_file(S)
+        print("wrote stl_files")
         return
     names = argv[1:] or sorted(CASES)
     for n in names:

@@ -37,7 +37,9 @@ def test_oracle_matches_golden(name):
         return
     pos, val = _flat(res)
     assert np.array_equal(pos, g["pos"]), "observation points / energies differ"
-    assert np.array_equal(val, g["val"]), "max rel diff %g" % (np.max(np.abs(val - g["val"])) / np.max(np.abs(g["val"])))
+    # NaN where the reference divides 0 by 0 (the precision of a fully shadowed STL facet)
+    assert np.array_equal(val, g["val"], equal_nan=True), \
+        "max rel diff %g" % (np.nanmax(np.abs(val - g["val"])) / np.nanmax(np.abs(g["val"])))
     if "level" in g.files:
         last, kw = CASES[name][-1]
         lev = run_case(OracleSR(), CASES[name][:-1] + [(last, dict(kw, quantity="level"))])
