@@ -169,6 +169,12 @@ OSC_API int osc_set_ctstartstop(osc_ctx* ctx, double start, double stop);       
 OSC_API int osc_get_ctstartstop(osc_ctx* ctx, double* start, double* stop);
 OSC_API int osc_set_npoints_trajectory(osc_ctx* ctx, long long n);
 OSC_API int osc_get_npoints_trajectory(osc_ctx* ctx, long long* n);
+/* Trajectory method (OSCARSSR::SetTrajectoryCalculation, src/OSCARSSR.cc:784-820): "RK4" (fixed
+ * step; precision must be -1) or "RKAS" (adaptive Cash-Karp, src/OSCARSSR.cc:1015-1072 and
+ * 1392-1618; precision > 0, or -1 to keep the current one, default 1e-6).  Case-insensitive. */
+OSC_API int osc_set_trajectory_calculation(osc_ctx* ctx, const char* method, double precision);
+/* method_out: 0 RK4, 1 RKAS. */
+OSC_API int osc_get_trajectory_calculation(osc_ctx* ctx, int* method_out, double* precision_out);
 
 /* ---- trajectory: OSCARSSR::CalculateTrajectory (src/OSCARSSR.cc:853-1009) -------------------- */
 OSC_API int osc_calculate_trajectory(osc_ctx* ctx);

@@ -86,6 +86,7 @@ def load():
                                  D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ip]
     lib.orc_power_density.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_long, ctypes.c_int, D,
                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, ip]
+    lib.orc_set_trajectory_calculation.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
     lib.orc_power_density_stl.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_long, D, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, dp, ip]
     _lib = lib
@@ -741,6 +742,22 @@ class OracleSR:
         pos = xyz if dim == 3 else x1x2
         return [[list(pos[i]), float(out[i])] for i in range(n)]
 
+
+    def set_trajectory_calculation(self, method, precision=-1):
+        """OSCARSSR::SetTrajectoryCalculation (src/OSCARSSR.cc:784-820)."""
+        m = method.upper()
+        msg = "RK4 Trajectory does not use the precision parameter and you are attempting to set it"
+        if m == "RK4":
+            if precision != -1:
+                raise ValueError(msg)
+            code = 0
+        elif m == "RKAS":
+            if precision != -1 and precision <= 0:
+                raise ValueError("Trajectory precision cannot be >= 0")
+            code = 1
+        else:
+            raise ValueError("Method requested is invalid.  Try again")
+        self._check(self._lib.orc_set_trajectory_calculation(self._h, code, float(precision)))
 
     # ---- STL surfaces (src/OSCARSSR_Python.cc:6852-7212, src/TSTLContainer.cc) ---------------------
     def add_stl(self, ifile, rotations=None, translation=None, scale=1, name=""):

@@ -325,6 +325,8 @@ struct orc_sim {
   orc_rng rng;
   orc_traj tr;
   int error_gamma;
+  int traj_method;        /* 0 RK4, 1 RKAS (OSCARSSR::SetTrajectoryCalculation) */
+  double traj_precision;  /* RKAS precision, default 1e-6 (src/OSCARSSR.cc:47) */
   char err[256];
 };
 
@@ -344,6 +346,7 @@ orc_sim* orc_new(void) {
   orc_sim* s = (orc_sim*)calloc(1, sizeof(orc_sim));
   if (!s) return NULL;
   s->npoints_per_meter = 10000; /* OSCARSSR.cc:42 */
+  s->traj_precision = 1e-6;     /* OSCARSSR.cc:47 */
   rng_seed(&s->rng, 5489u);
   return s;
 }
@@ -725,6 +728,81 @@ static void dbuf_reverse(dbuf* d) {
 
 static int spline_setup(orc_traj* tr); /* below */
 
+/* ---- RKAS: OSCARSSR::RKCK / RKQS / PropogateRKAS (src/OSCARSSR.cc:1392-1618) ------------------- */
+static void rkck(orc_sim* s, const double* x, const double* dxdt, double t, double h, double* xout, double* xerr) {
+  static const double a2 = 0.2, a3 = 0.3, a4 = 0.6, a5 = 1.0, a6 = 0.875;
+  static const double b21 = 0.2, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0, b41 = 0.3, b42 = -0.9, b43 = 1.2;
+  static const double b51 = -11.0 / 54.0, b52 = 2.5, b53 = -70.0 / 27.0, b54 = 35.0 / 27.0;
+  static const double b61 = 1631.0 / 55296.0, b62 = 175.0 / 512.0, b63 = 575.0 / 13824.0;
+  static const double b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0;
+  static const double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0, c6 = 512.0 / 1771.0;
+  static const double dc5 = -277.00 / 14336.0;
+  const double dc1 = c1 - 2825.0 / 27648.0, dc3 = c3 - 18575.0 / 48384.0, dc4 = c4 - 13525.0 / 55296.0;
+  const double dc6 = c6 - 0.25;
+  double dx2[6], dx3[6], dx4[6], dx5[6], dx6[6], xt[6];
+  for (int i = 0; i != 6; ++i) xt[i] = x[i] + b21 * h * dxdt[i];
+  derivs(s, t + a2 * h, xt, dx2);
+  for (int i = 0; i != 6; ++i) xt[i] = x[i] + h * (b31 * dxdt[i] + b32 * dx2[i]);
+  derivs(s, t + a3 * h, xt, dx3);
+  for (int i = 0; i != 6; ++i) xt[i] = x[i] + h * (b41 * dxdt[i] + b42 * dx2[i] + b43 * dx3[i]);
+  derivs(s, t + a4 * h, xt, dx4);
+  for (int i = 0; i != 6; ++i) xt[i] = x[i] + h * (b51 * dxdt[i] + b52 * dx2[i] + b53 * dx3[i] + b54 * dx4[i]);
+  derivs(s, t + a5 * h, xt, dx5);
+  for (int i = 0; i != 6; ++i) xt[i] = x[i] + h * (b61 * dxdt[i] + b62 * dx2[i] + b63 * dx3[i] + b64 * dx4[i] + b65 * dx5[i]);
+  derivs(s, t + a6 * h, xt, dx6);
+  for (int i = 0; i != 6; ++i) xout[i] = x[i] + h * (c1 * dxdt[i] + c3 * dx3[i] + c4 * dx4[i] + c6 * dx6[i]);
+  for (int i = 0; i != 6; ++i) xerr[i] = h * (dc1 * dxdt[i] + dc3 * dx3[i] + dc4 * dx4[i] + dc5 * dx5[i] + dc6 * dx6[i]);
+}
+
+static int rkqs(orc_sim* s, double* x, double* dxdt, double* t, double htry, double prec, const double* xscale,
+                double delta_t, double* hnext) {
+  double h = htry, max_error = 0, xt[6], xe[6];
+  for (;;) {
+    s->error_gamma = 0;
+    rkck(s, x, dxdt, *t, h, xt, xe);
+    max_error = 0.0;
+    for (int i = 0; i != 6; ++i) max_error = fmax(max_error, fabs(xe[i] / xscale[i]));
+    max_error /= prec;
+    if (max_error <= 1.0 && !s->error_gamma) break;
+    double htemp = s->error_gamma ? 0.25 * h : 0.9 * h * pow(max_error, -0.25);
+    h = (h >= 0.0 ? fmax(htemp, 0.1 * h) : fmin(htemp, 0.1 * h));
+    if ((*t) + h == *t) return fail(s, ORC_ERR_RANGE, "stepsize underflow in rkqs.  Possible you have a discontinuous field");
+  }
+  *hnext = max_error > 1.89e-4 ? 0.9 * h * pow(max_error, -0.2) : 5.0 * h;
+  if (fabs(*hnext) > delta_t) *hnext = delta_t * (*hnext >= 0 ? 1 : -1);
+  *t += h;
+  for (int i = 0; i != 6; ++i) x[i] = xt[i];
+  return ORC_OK;
+}
+
+static int propagate_rkas(orc_sim* s, double* xstart, double T1, double T2, double prec, double delta_t, dbuf* d) {
+  double x[6], dxdt[6] = {0, 0, 0, 0, 0, 0}, xscale[6], hnext = 0;
+  double t = T1, h = (T2 >= T1 ? delta_t : -delta_t);
+  for (int i = 0; i != 6; ++i) x[i] = xstart[i];
+  for (long nstp = 0; nstp != 10000000; ++nstp) {
+    derivs(s, t, x, dxdt);
+    for (int i = 0; i != 6; ++i) xscale[i] = fabs(x[i]) + fabs(dxdt[i] * h) + 1.0e-30;
+    if (dbuf_push(d, x, dxdt, t)) return fail(s, ORC_ERR_ALLOC, "alloc");
+    if ((t + h - T2) * (t + h - T1) > 0.0) h = T2 - t;
+    int rc = rkqs(s, x, dxdt, &t, h, prec, xscale, delta_t, &hnext);
+    if (rc) return rc;
+    if ((t - T2) * (T2 - T1) >= 0.0) {
+      for (int i = 0; i != 6; ++i) xstart[i] = x[i];
+      if (dbuf_push(d, x, dxdt, t)) return fail(s, ORC_ERR_ALLOC, "alloc");
+      return ORC_OK;
+    }
+    if (fabs(hnext) <= 1e-30) return fail(s, ORC_ERR_RANGE, "Reached minimum stepsize in PropogateRKAS without convergence");
+    h = hnext;
+  }
+  return fail(s, ORC_ERR_RANGE, "Too many steps taken in routine PropogateRKAS");
+}
+
+int orc_set_trajectory_calculation(orc_sim* s, int method, double precision) {
+  s->traj_method = method;
+  if (precision != -1) s->traj_precision = precision;
+  return ORC_OK;
+}
+
 int orc_calculate_trajectory(orc_sim* s) {
   if (!s->p.set) return fail(s, ORC_ERR_STATE, "particle not initialized.  make sure you have a particle or beam defined");
   if (s->ctstart > s->p.t0 || s->ctstop < s->p.t0)
@@ -741,6 +819,17 @@ int orc_calculate_trajectory(orc_sim* s) {
   x[0] = s->p.x0.x; x[1] = s->p.b0.x * K_C; x[2] = s->p.x0.y;
   x[3] = s->p.b0.y * K_C; x[4] = s->p.x0.z; x[5] = s->p.b0.z * K_C;
   derivs(s, s->p.t0 / K_C, x, dxdt);
+  if (s->traj_method == 1) {  /* OSCARSSR::CalculateTrajectoryRKAS (src/OSCARSSR.cc:1015-1072) */
+    int rc = propagate_rkas(s, x, s->p.t0 / K_C, s->ctstop / K_C, s->traj_precision, DeltaT, &d);
+    if (rc) { free(d.v); return rc; }
+    dbuf_reverse(&d);
+    x[0] = s->p.x0.x; x[1] = s->p.b0.x * K_C; x[2] = s->p.x0.y;
+    x[3] = s->p.b0.y * K_C; x[4] = s->p.x0.z; x[5] = s->p.b0.z * K_C;
+    derivs(s, s->p.t0 / K_C, x, dxdt);
+    rc = propagate_rkas(s, x, s->p.t0 / K_C, s->ctstart / K_C, s->traj_precision, DeltaT, &d);
+    if (rc) { free(d.v); return rc; }
+    nf = nb = 0;
+  }
   for (size_t i = 0; i != nf; ++i) {
     double t = s->p.t0 / K_C + DeltaT * i;
     if (i == 0) derivs(s, t, x, dxdt);
@@ -748,7 +837,7 @@ int orc_calculate_trajectory(orc_sim* s) {
     derivs(s, t, x, dxdt);
     rk4(s, x, dxdt, t, DeltaT, x);
   }
-  dbuf_reverse(&d);
+  if (s->traj_method != 1) dbuf_reverse(&d);
   x[0] = s->p.x0.x; x[1] = s->p.b0.x * K_C; x[2] = s->p.x0.y;
   x[3] = s->p.b0.y * K_C; x[4] = s->p.x0.z; x[5] = s->p.b0.z * K_C;
   double const dtr = -DeltaT;

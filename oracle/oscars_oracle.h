@@ -78,6 +78,9 @@ int orc_get_spline_ypp(const orc_sim*, double* out, long cap);
 /* level samples of the current trajectory: 10 x 2^level SoA */
 int orc_get_level(orc_sim*, int level, double* out, long cap);
 
+/* Trajectory method: 0 RK4, 1 RKAS; precision -1 keeps the current one (default 1e-6). */
+int orc_set_trajectory_calculation(orc_sim*, int method, double precision);
+
 /* Radiation entry points.  out has n entries (quantity 0=value, 1=precision, 2=level);
  * out_level (optional) receives the per-entry stop level, -1 when not converged. */
 int orc_flux(orc_sim*, const double* obs, long n_obs, double energy_eV, int pol, double angle,

@@ -70,6 +70,8 @@ SIGNATURES = {
     "osc_set_ctstartstop": (I, [VP, D, D]),
     "osc_get_ctstartstop": (I, [VP, DP, DP]),
     "osc_set_npoints_trajectory": (I, [VP, LL]),
+    "osc_set_trajectory_calculation": (I, [VP, ctypes.c_char_p, D]),
+    "osc_get_trajectory_calculation": (I, [VP, ctypes.POINTER(ctypes.c_int), DP]),
     "osc_get_npoints_trajectory": (I, [VP, LLP]),
     "osc_calculate_trajectory": (I, [VP]),
     "osc_get_trajectory": (I, [VP, DP, LL, LLP]),

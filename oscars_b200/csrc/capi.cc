@@ -312,6 +312,20 @@ OSC_API int osc_get_npoints_trajectory(osc_ctx* ctx, long long* n) {
   return guarded(ctx, [&] { if (n) *n = ctx->eng->model.npoints; });
 }
 
+OSC_API int osc_set_trajectory_calculation(osc_ctx* ctx, const char* method, double precision) {
+  return guarded(ctx, [&] {
+    if (!method) throw osc::Error{OSC_ERR_INVALID, "Method requested is invalid.  Try again"};
+    ctx->eng->model.set_trajectory_calculation(method, precision);
+  });
+}
+
+OSC_API int osc_get_trajectory_calculation(osc_ctx* ctx, int* method_out, double* precision_out) {
+  return guarded(ctx, [&] {
+    if (method_out) *method_out = ctx->eng->model.traj_method;
+    if (precision_out) *precision_out = ctx->eng->model.traj_precision;
+  });
+}
+
 OSC_API int osc_calculate_trajectory(osc_ctx* ctx) {
   return guarded(ctx, [&] {
     osc::Model& M = ctx->eng->model;

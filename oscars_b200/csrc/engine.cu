@@ -638,7 +638,9 @@ void Engine::radiation(RadRequest& rq) {
   if (!d_lvl) d_lvl = lvl_.as<int32_t>();
 
   const int np = rq.opts.nparticles;
-  if (np > 0 && rq.opts.precision_mode == OSC_MIXED && !rq.power_density) {
+  // mixed multi-particle requests integrate their trajectories with the device RK4; with RKAS selected
+  // each particle's trajectory comes from the host integrator like the FP64 path's
+  if (np > 0 && rq.opts.precision_mode == OSC_MIXED && !rq.power_density && model.traj_method == Model::kRK4) {
     radiation_beam_mixed(rq, N);
     return;
   }

@@ -648,6 +648,66 @@ struct Integrator {
   }
 };
 
+// Adaptive Cash-Karp RK5(4) (src/OSCARSSR.cc:1392-1618, the driver / step / stage functions of the
+// reference): stage and error coefficients as the reference declares them, the step controller with
+// its safety factors, and output steps capped at the fixed-step interval DeltaT.
+struct Rkas {
+  Integrator& I;
+  double delta_t, precision;
+
+  void rkck(const double* x, const double* dxdt, double t, double h, double* xout, double* xerr) {
+    static constexpr double a2 = 0.2, a3 = 0.3, a4 = 0.6, a5 = 1.0, a6 = 0.875;
+    static constexpr double b21 = 0.2, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0, b41 = 0.3, b42 = -0.9, b43 = 1.2;
+    static constexpr double b51 = -11.0 / 54.0, b52 = 2.5, b53 = -70.0 / 27.0, b54 = 35.0 / 27.0;
+    static constexpr double b61 = 1631.0 / 55296.0, b62 = 175.0 / 512.0, b63 = 575.0 / 13824.0;
+    static constexpr double b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0;
+    static constexpr double c1 = 37.0 / 378.0, c3 = 250.0 / 621.0, c4 = 125.0 / 594.0, c6 = 512.0 / 1771.0;
+    static constexpr double dc5 = -277.00 / 14336.0, dc1 = c1 - 2825.0 / 27648.0, dc3 = c3 - 18575.0 / 48384.0;
+    static constexpr double dc4 = c4 - 13525.0 / 55296.0, dc6 = c6 - 0.25;
+    double dx2[6], dx3[6], dx4[6], dx5[6], dx6[6], xt[6];
+    for (int i = 0; i != 6; ++i) xt[i] = x[i] + b21 * h * dxdt[i];
+    I.derivs(t + a2 * h, xt, dx2);
+    for (int i = 0; i != 6; ++i) xt[i] = x[i] + h * (b31 * dxdt[i] + b32 * dx2[i]);
+    I.derivs(t + a3 * h, xt, dx3);
+    for (int i = 0; i != 6; ++i) xt[i] = x[i] + h * (b41 * dxdt[i] + b42 * dx2[i] + b43 * dx3[i]);
+    I.derivs(t + a4 * h, xt, dx4);
+    for (int i = 0; i != 6; ++i) xt[i] = x[i] + h * (b51 * dxdt[i] + b52 * dx2[i] + b53 * dx3[i] + b54 * dx4[i]);
+    I.derivs(t + a5 * h, xt, dx5);
+    for (int i = 0; i != 6; ++i)
+      xt[i] = x[i] + h * (b61 * dxdt[i] + b62 * dx2[i] + b63 * dx3[i] + b64 * dx4[i] + b65 * dx5[i]);
+    I.derivs(t + a6 * h, xt, dx6);
+    for (int i = 0; i != 6; ++i) xout[i] = x[i] + h * (c1 * dxdt[i] + c3 * dx3[i] + c4 * dx4[i] + c6 * dx6[i]);
+    for (int i = 0; i != 6; ++i)
+      xerr[i] = h * (dc1 * dxdt[i] + dc3 * dx3[i] + dc4 * dx4[i] + dc5 * dx5[i] + dc6 * dx6[i]);
+  }
+
+  // One accepted step from t with trial step htry; returns the step size for the next one.
+  double rkqs(double* x, double* dxdt, double* t, double htry, const double* xscale) {
+    double h = htry, max_error = 0, xt[6], xe[6];
+    for (;;) {
+      I.error_gamma = false;
+      rkck(x, dxdt, *t, h, xt, xe);
+      max_error = 0.0;
+      for (int i = 0; i != 6; ++i) max_error = std::fmax(max_error, std::fabs(xe[i] / xscale[i]));
+      max_error /= precision;
+      if (max_error <= 1.0 && !I.error_gamma) break;
+      const double htemp = I.error_gamma ? 0.25 * h : 0.9 * h * std::pow(max_error, -0.25);
+      h = (h >= 0.0 ? std::fmax(htemp, 0.1 * h) : std::fmin(htemp, 0.1 * h));
+      if ((*t) + h == *t)
+        throw Error{OSC_ERR_RANGE, "stepsize underflow in rkqs.  Possible you have a discontinuous field"};
+    }
+    double hnext = max_error > 1.89e-4 ? 0.9 * h * std::pow(max_error, -0.2) : 5.0 * h;
+    if (std::fabs(hnext) > delta_t) hnext = delta_t * (hnext >= 0 ? 1 : -1);  // output step cap
+    *t += h;
+    for (int i = 0; i != 6; ++i) x[i] = xt[i];
+    return hnext;
+  }
+
+  // From T1 to T2: every accepted step's start point with its derivative, then the end point (with
+  // the derivative of the last step's start, as the reference stores it).
+  void propagate(double* xstart, double T1, double T2, std::vector<double>& buf);
+};
+
 inline void push_point(std::vector<double>& buf, const double* x, const double* dxdt, double t) {
   buf.push_back(t);
   buf.push_back(x[0]); buf.push_back(x[2]); buf.push_back(x[4]);
@@ -655,7 +715,51 @@ inline void push_point(std::vector<double>& buf, const double* x, const double* 
   buf.push_back(dxdt[1] / kC); buf.push_back(dxdt[3] / kC); buf.push_back(dxdt[5] / kC);
 }
 
+void Rkas::propagate(double* xstart, double T1, double T2, std::vector<double>& buf) {
+  double x[6], dxdt[6] = {0, 0, 0, 0, 0, 0}, xscale[6];
+  double t = T1;
+  double h = (T2 >= T1 ? delta_t : -delta_t);
+  for (int i = 0; i != 6; ++i) x[i] = xstart[i];
+  for (int nstp = 0; nstp != 10000000; ++nstp) {
+    I.derivs(t, x, dxdt);
+    for (int i = 0; i != 6; ++i) xscale[i] = std::fabs(x[i]) + std::fabs(dxdt[i] * h) + 1.0e-30;
+    push_point(buf, x, dxdt, t);
+    if ((t + h - T2) * (t + h - T1) > 0.0) h = T2 - t;
+    const double hnext = rkqs(x, dxdt, &t, h, xscale);
+    if ((t - T2) * (T2 - T1) >= 0.0) {
+      for (int i = 0; i != 6; ++i) xstart[i] = x[i];
+      push_point(buf, x, dxdt, t);
+      return;
+    }
+    if (std::fabs(hnext) <= 1e-30)
+      throw Error{OSC_ERR_RANGE, "Reached minimum stepsize in PropogateRKAS without convergence"};
+    h = hnext;
+  }
+  throw Error{OSC_ERR_RANGE, "Too many steps taken in routine PropogateRKAS"};
+}
+
 }  // namespace
+
+void Model::set_trajectory_calculation(const std::string& method, double precision) {
+  std::string m = method;
+  for (char& c : m) c = (char)std::toupper((unsigned char)c);
+  const char* kRk4Precision = "RK4 Trajectory does not use the precision parameter and you are attempting to set it";
+  int which;
+  if (m == "RK4") {
+    if (precision != -1) throw Error{OSC_ERR_INVALID, kRk4Precision};
+    which = kRK4;
+  } else if (m == "RKAS") {
+    which = kRKAS;
+  } else {
+    throw Error{OSC_ERR_INVALID, "Method requested is invalid.  Try again"};
+  }
+  traj_method = which;  // src/OSCARSSR.cc:805-818: the method is set before the precision is checked
+  if (precision != -1) {
+    if (which == kRK4) throw Error{OSC_ERR_INVALID, kRk4Precision};
+    if (precision <= 0) throw Error{OSC_ERR_INVALID, "Trajectory precision cannot be >= 0"};
+    traj_precision = precision;
+  }
+}
 
 void Model::compute_trajectory() {
   const Particle& P = particle;
@@ -667,6 +771,43 @@ void Model::compute_trajectory() {
   knots.clear();
   ++knots_version;
   const double dt = ((ctstop - ctstart) / kC / (npoints - 1));
+  if (traj_method == kRKAS) {  // src/OSCARSSR.cc:1015-1072
+    std::vector<double>& fwd = sweep[0];
+    std::vector<double>& bwd = sweep[1];
+    fwd.clear();
+    bwd.clear();
+    auto run = [&](int dir) {
+      Integrator I{fields, P.qomg};
+      Rkas R{I, dt, traj_precision};
+      double x[6] = {P.x0.x, P.b0.x * kC, P.x0.y, P.b0.y * kC, P.x0.z, P.b0.z * kC};
+      double dxdt[6] = {0, 0, 0, 0, 0, 0};
+      I.derivs(P.t0 / kC, x, dxdt);  // the reference evaluates it first (its value is not used)
+      R.propagate(x, P.t0 / kC, (dir == 0 ? ctstop : ctstart) / kC, dir == 0 ? fwd : bwd);
+    };
+    parallel_tasks(2, run);
+    // forward reversed, backward appended, all reversed: the backward points earliest first, then the
+    // forward ones; both start at t0, so t0 appears twice (as in the reference)
+    const int64_t nf = (int64_t)fwd.size() / 10, nb = (int64_t)bwd.size() / 10, n = nf + nb;
+    if (n < 3)
+      throw Error{OSC_ERR_LENGTH, "TSpline1D3 does not see enough points for interpolation.  Please use >= 3 points"};
+    knots.n = n;
+    knots.t.resize(n);
+    knots.y.resize(9 * n);
+    for (int64_t j = 0; j < nb; ++j) {
+      const double* r = &bwd[10 * (nb - 1 - j)];
+      knots.t[j] = r[0];
+      for (int c = 0; c < 9; ++c) knots.y[c * n + j] = r[1 + c];
+    }
+    for (int64_t j = 0; j < nf; ++j) {
+      const double* r = &fwd[10 * j];
+      knots.t[nb + j] = r[0];
+      for (int c = 0; c < 9; ++c) knots.y[c * n + nb + j] = r[1 + c];
+    }
+    knots.tstart = knots.t.front();
+    knots.tstop = knots.t.back();
+    spline_second_derivatives(knots);
+    return;
+  }
   const size_t nf = (size_t)(1 + (ctstop - P.t0) / kC / dt);
   const size_t nb = (size_t)((P.t0 - ctstart) / kC / dt);
 

@@ -151,6 +151,11 @@ class Model {
   Knots knots;
   uint64_t knots_version = 0;  // bumps whenever `knots` changes
   std::vector<double> sweep[2];  // forward / backward integration points, kept between calls
+  // Trajectory method (OSCARSSR::SetTrajectoryCalculation, src/OSCARSSR.cc:784-820): fixed-step RK4
+  // or the adaptive Cash-Karp RKAS with its precision (default 1e-6).
+  enum TrajectoryMethod { kRK4 = 0, kRKAS = 1 };
+  int traj_method = kRK4;
+  double traj_precision = 1e-6;
 
   void add_field(const FieldSpec& f);
   void clear_fields();
@@ -160,6 +165,8 @@ class Model {
   // Throws osc::Error on failure.
   void compute_trajectory();
   void ensure_trajectory();
+  // Select the method: "RK4" (precision must be -1, the binding's "not given") or "RKAS".
+  void set_trajectory_calculation(const std::string& method, double precision);
   // Use a trajectory computed elsewhere (10 x n SoA: t, x y z, beta, a/c) with its spline.
   void set_trajectory(const double* traj, int64_t n);
 };

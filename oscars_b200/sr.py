@@ -342,6 +342,17 @@ class sr:
     def set_npoints_trajectory(self, npoints):
         self._ctx.call("osc_set_npoints_trajectory", int(npoints))
 
+    def set_trajectory_calculation(self, method, precision=-1):
+        """'RK4' (fixed step, the default) or 'RKAS' (adaptive Cash-Karp steps at `precision`, default
+        1e-6), src/OSCARSSR_Python.cc:5115-5146."""
+        self._ctx.call("osc_set_trajectory_calculation", str(method).encode(), float(precision))
+
+    def print_trajectory(self):
+        m, p = ctypes.c_int(), ctypes.c_double()
+        self._ctx.call("osc_get_trajectory_calculation", ctypes.byref(m), ctypes.byref(p))
+        sys.stdout.write("*Trajectory Calculation Globals*\nMethod:    %s\nPrecision: %s\n\n"
+                         % ("RKAS" if m.value == 1 else "RK4", "%g" % p.value))
+
     def get_npoints_trajectory(self):
         n = ctypes.c_longlong()
         self._ctx.call("osc_get_npoints_trajectory", ctypes.byref(n))

@@ -239,6 +239,16 @@ CASES = {
     "pd_points": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, rotations=[0.0, 0.001, 0.0], translation=[0.0, 0.0005, 0.0]))],
     "pd_points_directional": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS_MIXED, normal=1))],
     "pd_points_inverted": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, normal=-1))],
+    # adaptive Cash-Karp trajectories (RKAS): the 11-period undulator at the default precision, the
+    # elliptical configuration at 1e-7; a spectrum on an RKAS trajectory (the reference's RKAS
+    # trajectory holds the start time twice, so its spline and every radiation result are NaN)
+    "traj_rkas": [UND_SHORT, BEAM] + traj(5001, -0.5, 0.5) + [("set_trajectory_calculation", dict(method="RKAS")),
+                                                             ("calculate_trajectory", {})],
+    "traj_rkas_epu": [EPU_Y, EPU_X, BEAM] + traj(16001, -1.0, 1.0) +
+                     [("set_trajectory_calculation", dict(method="rkas", precision=1e-7)), ("calculate_trajectory", {})],
+    "spec_rkas": [UND_SHORT, BEAM] + traj(5001, -0.5, 0.5) +
+                 [("set_trajectory_calculation", dict(method="RKAS")),
+                  ("calculate_spectrum", dict(obs=[0, 0, 30], energy_range_eV=[400, 500], npoints=3, max_level=10))],
     # power density on STL facets (11-period undulator, 1 m trajectory, levels up to 12): a plate in
     # the beam, the plate partly shadowed by a shield (millimetre file, scale 0.001), a tilted plate
     # with stored normals of length 2 and one zero normal (also capped at level 10, where facets that
