@@ -9,7 +9,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <exception>
+#include <mutex>
+#include <thread>
 
 #include "kernels.h"
 
@@ -85,6 +89,13 @@ Engine::~Engine() {
   if (stats_host_) cudaFreeHost(stats_host_);
   if (stage_host_) cudaFreeHost(stage_host_);
   if (ctl_host_) cudaFreeHost(ctl_host_);
+  for (PinnedStage& p : pin_pool_) {
+    if (p.copied) {
+      cudaEventSynchronize(p.copied);
+      cudaEventDestroy(p.copied);
+    }
+    if (p.pinned) cudaFreeHost(p.pinned);
+  }
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
                     &act_[1], &cnt_, &acc_, &acc_comp_, &mrec_, &b_fields_, &b_fvals_, &b_obs_, &b_omega_, &b_acc_, &b_jobs_,
@@ -100,20 +111,24 @@ void Engine::check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw Error{OSC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
-void Engine::upload_trajectory() {
+void Engine::upload_trajectory(const double* pinned) {
   const Knots& k = model.knots;
   if (knots_version_ == model.knots_version && nknots_ == k.n) return;
   levels_dropped_ = false;
   const int64_t n = k.n;
   knots_.reserve(sizeof(double) * 20 * n);
   double* d = knots_.as<double>();
-  check(cudaMemcpyAsync(d, k.t.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cur_), "upload t");
-  check(cudaMemcpyAsync(d + n, k.y.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, cur_), "upload y");
-  check(cudaMemcpyAsync(d + 10 * n, k.ypp.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, cur_),
-        "upload ypp");
-  if ((int64_t)k.diag.size() == n)
-    check(cudaMemcpyAsync(d + 19 * n, k.diag.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cur_),
-          "upload diag");
+  if (pinned) {  // the same knots already laid out in pinned memory: one asynchronous copy
+    check(cudaMemcpyAsync(d, pinned, sizeof(double) * 20 * n, cudaMemcpyHostToDevice, cur_), "upload knots");
+  } else {
+    check(cudaMemcpyAsync(d, k.t.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cur_), "upload t");
+    check(cudaMemcpyAsync(d + n, k.y.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, cur_), "upload y");
+    check(cudaMemcpyAsync(d + 10 * n, k.ypp.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, cur_),
+          "upload ypp");
+    if ((int64_t)k.diag.size() == n)
+      check(cudaMemcpyAsync(d + 19 * n, k.diag.data(), sizeof(double) * n, cudaMemcpyHostToDevice, cur_),
+            "upload diag");
+  }
   nknots_ = n;
   tstart_ = k.tstart;
   tstop_ = k.tstop;
@@ -599,6 +614,131 @@ void Engine::use_stream(cudaStream_t s) {
   cur_ = s;
 }
 
+// Trajectories of a list of particles integrated on host worker threads ahead of their use: worker
+// threads claim particles in order and fill a ring of slots; the consumer takes particle k's slot
+// when it is ready and releases it for particle k + slots.  A worker's exception is rethrown to
+// the consumer at that particle.
+class TrajectoryPipeline {
+ public:
+  // `device`: the workers also lay each trajectory out in pinned host memory in the device knot
+  // layout (t | y[9] | ypp[9] | diag), so that its upload is one asynchronous copy.
+  // `pool`: pinned staging buffers and their copy events, kept by the engine between requests (pinned
+  // allocations are slow); grown here to the slots this pipeline uses.
+  TrajectoryPipeline(const Model& m, const std::vector<Particle>& parts, int device, std::vector<PinnedStage>& pool)
+      : m_(m), parts_(parts), device_(device) {
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const int nthreads = (int)std::min<size_t>(std::min(hw - 1u, 32u), std::max<size_t>(1, parts.size()));
+    const size_t nslots = std::min<size_t>(2 * nthreads, std::max<size_t>(1, parts.size()));
+    while (pool.size() < nslots) {
+      pool.emplace_back();
+      const cudaError_t e = cudaEventCreateWithFlags(&pool.back().copied, cudaEventDisableTiming);
+      if (e != cudaSuccess) throw Error{OSC_ERR_CUDA, std::string("event: ") + cudaGetErrorString(e)};
+    }
+    slots_.resize(nslots);
+    for (size_t i = 0; i < nslots; ++i) slots_[i].stage = &pool[i];
+    for (int i = 0; i < nthreads; ++i) workers_.emplace_back([this] { work(); });
+  }
+  ~TrajectoryPipeline() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  // The upload of particle k's pinned copy was enqueued on `st`: the slot's next trajectory is staged
+  // only after that copy has run (the request need not have waited for the device by then).
+  void uploaded(size_t k, cudaStream_t st) {
+    const cudaError_t e = cudaEventRecord(slots_[k % slots_.size()].stage->copied, st);
+    if (e != cudaSuccess) throw Error{OSC_ERR_CUDA, std::string("event: ") + cudaGetErrorString(e)};
+  }
+  // Particle k's trajectory: its knots and their pinned copy in the device layout.  The slot stays
+  // the caller's until release(k), so the copy may still be read by the device until then.
+  Knots& wait(size_t k, const double** pinned) {
+    Slot& s = slots_[k % slots_.size()];
+    std::unique_lock<std::mutex> g(mu_);
+    cv_.wait(g, [&] { return s.ready && s.particle == (int64_t)k; });
+    if (s.err) std::rethrow_exception(s.err);
+    *pinned = s.stage->pinned;
+    return s.knots;
+  }
+  void release(size_t k) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      slots_[k % slots_.size()].ready = false;
+      consumed_ = k + 1;
+    }
+    cv_.notify_all();
+  }
+
+ private:
+  struct Slot {
+    Knots knots;
+    std::vector<double> sweep[2];
+    PinnedStage* stage = nullptr;
+    int64_t particle = -1;
+    bool ready = false;
+    std::exception_ptr err;
+  };
+  static void stage(Slot& s, int device) {  // knots -> pinned t | y | ypp | diag
+    const Knots& k = s.knots;
+    PinnedStage& p = *s.stage;
+    const size_t n = (size_t)k.n, need = 20 * n;
+    cudaError_t ev = cudaEventSynchronize(p.copied);  // the previous copy out of this buffer has run
+    if (ev != cudaSuccess) throw Error{OSC_ERR_CUDA, std::string("event: ") + cudaGetErrorString(ev)};
+    if (p.doubles < need) {
+      if (p.pinned) cudaFreeHost(p.pinned);
+      p.pinned = nullptr;
+      p.doubles = 0;
+      cudaError_t e = cudaSetDevice(device);
+      if (e == cudaSuccess)
+        e = cudaHostAlloc(reinterpret_cast<void**>(&p.pinned), sizeof(double) * need, cudaHostAllocPortable);
+      if (e != cudaSuccess) throw Error{OSC_ERR_CUDA, std::string("cudaHostAlloc: ") + cudaGetErrorString(e)};
+      p.doubles = need;
+    }
+    std::memcpy(p.pinned, k.t.data(), sizeof(double) * n);
+    std::memcpy(p.pinned + n, k.y.data(), sizeof(double) * 9 * n);
+    std::memcpy(p.pinned + 10 * n, k.ypp.data(), sizeof(double) * 9 * n);
+    if (k.diag.size() == n) std::memcpy(p.pinned + 19 * n, k.diag.data(), sizeof(double) * n);
+    else std::memset(p.pinned + 19 * n, 0, sizeof(double) * n);
+  }
+  void work() {
+    for (;;) {
+      size_t k;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return stop_ || next_ >= parts_.size() || next_ < consumed_ + slots_.size(); });
+        if (stop_ || next_ >= parts_.size()) return;
+        k = next_++;
+      }
+      Slot& s = slots_[k % slots_.size()];
+      std::exception_ptr err;
+      try {
+        m_.integrate(parts_[k], s.knots, s.sweep, false);
+        stage(s, device_);
+      } catch (...) {
+        err = std::current_exception();
+      }
+      {
+        std::lock_guard<std::mutex> g(mu_);
+        s.err = err;
+        s.particle = (int64_t)k;
+        s.ready = true;
+      }
+      cv_.notify_all();
+    }
+  }
+  const Model& m_;
+  const std::vector<Particle>& parts_;
+  const int device_;
+  std::vector<Slot> slots_;
+  std::vector<std::thread> workers_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  size_t next_ = 0, consumed_ = 0;
+  bool stop_ = false;
+};
+
 void Engine::radiation(RadRequest& rq) {
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
@@ -656,17 +796,32 @@ void Engine::radiation(RadRequest& rq) {
     check(cudaMemsetAsync(acc_.p, 0, sizeof(double) * N, st), "memset");
     check(cudaMemsetAsync(acc_comp_.p, 0, sizeof(double) * N, st), "memset");
     const int shards = rq.opts.shard_count > 1 ? rq.opts.shard_count : 1;
+    std::vector<Particle> mine;  // this process's particles, drawn in the reference's order
     for (int ip = 0; ip < np; ++ip) {
       model.random_particle();
       if (ip % shards != rq.opts.shard_rank % shards) continue;  // another process's particle
-      model.compute_trajectory();  // host RK4 of particle ip overlaps the GPU work of particle ip-1
-      check(cudaStreamSynchronize(st), "particle");
-      upload_trajectory();
-      run_single(rq, N, weight, out_.as<double>(), d_lvl, st);
-      k_kahan_add<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(acc_.as<double>(), acc_comp_.as<double>(),
-                                                                out_.as<double>(), N);
-      check(cudaGetLastError(), "accumulate");
-      ++last_launches;
+      mine.push_back(model.particle);
+    }
+    {
+      // their trajectories are integrated on host worker threads while the GPU sums earlier ones;
+      // the model holds the particle in use and its trajectory (the last ones when done, as the
+      // reference leaves them)
+      TrajectoryPipeline pipe(model, mine, device, pin_pool_);
+      for (size_t k = 0; k < mine.size(); ++k) {
+        const double* pinned = nullptr;
+        Knots& kn = pipe.wait(k, &pinned);
+        model.particle = mine[k];
+        std::swap(model.knots, kn);
+        ++model.knots_version;
+        upload_trajectory(pinned);
+        pipe.uploaded(k, cur_);
+        run_single(rq, N, weight, out_.as<double>(), d_lvl, st);
+        pipe.release(k);
+        k_kahan_add<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(acc_.as<double>(), acc_comp_.as<double>(),
+                                                                  out_.as<double>(), N);
+        check(cudaGetLastError(), "accumulate");
+        ++last_launches;
+      }
     }
     check(cudaMemcpyAsync(d_out, acc_.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "result");
   }

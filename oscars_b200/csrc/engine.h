@@ -57,6 +57,14 @@ struct BatchJob {
 double dt_inclusive(double tstart, double tstop, int L);
 void polarization_vector(const osc_rad_opts& o, double P[6], bool& project);
 
+// A pinned host buffer for staging one trajectory's upload, with the event recorded after its copy
+// to the device was enqueued (kept by the engine across multi-particle requests).
+struct PinnedStage {
+  double* pinned = nullptr;
+  size_t doubles = 0;
+  cudaEvent_t copied = nullptr;
+};
+
 class Engine {
  public:
   explicit Engine(int device);
@@ -196,12 +204,14 @@ class Engine {
   bool last_stream_valid_ = false;
   cudaEvent_t order_ev_ = nullptr;
   void use_stream(cudaStream_t s);
-  void upload_trajectory();
+  // model.knots to the device (pinned: the same knots laid out t | y | ypp | diag in pinned memory)
+  void upload_trajectory(const double* pinned = nullptr);
   void ensure_levels(int L);
   void reserve_levels(int L);
   void fill_levels(int64_t s_begin, int64_t s_end, cudaStream_t s);
   void prefill(bool mixed, int Lhead, int Lpre);
   void join_prefill();
+  std::vector<PinnedStage> pin_pool_;  // trajectory staging of multi-particle requests
   // STL request buffers: facet geometry (A, B - A, C - A), centres, normals, per-facet state and flags
   DevBuf stl_geo_, stl_cen_, stl_nrm_, stl_state_, stl_flags_;
   // side stream of the prefill (levels above the first wave's) and its fork / join events

@@ -762,14 +762,18 @@ void Model::set_trajectory_calculation(const std::string& method, double precisi
 }
 
 void Model::compute_trajectory() {
-  const Particle& P = particle;
+  knots.clear();
+  ++knots_version;
+  integrate(particle, knots, sweep, true);
+}
+
+void Model::integrate(const Particle& P, Knots& knots, std::vector<double>* sweep, bool threads) const {
   if (!P.set) throw Error{OSC_ERR_RANGE, "particle not initialized.  make sure you have a particle or beam defined"};
   if (ctstart > P.t0 || ctstop < P.t0)
     throw Error{OSC_ERR_RANGE, "start time is greater than T0 or stop time is less than T0"};
   if (ctstart >= ctstop)
     throw Error{OSC_ERR_RANGE, "start time is greater than stop time.  check that set_ctstartstop is set"};
   knots.clear();
-  ++knots_version;
   const double dt = ((ctstop - ctstart) / kC / (npoints - 1));
   if (traj_method == kRKAS) {  // src/OSCARSSR.cc:1015-1072
     std::vector<double>& fwd = sweep[0];
@@ -784,7 +788,12 @@ void Model::compute_trajectory() {
       I.derivs(P.t0 / kC, x, dxdt);  // the reference evaluates it first (its value is not used)
       R.propagate(x, P.t0 / kC, (dir == 0 ? ctstop : ctstart) / kC, dir == 0 ? fwd : bwd);
     };
-    parallel_tasks(2, run);
+    if (threads) {
+      parallel_tasks(2, run);
+    } else {
+      run(0);
+      run(1);
+    }
     // forward reversed, backward appended, all reversed: the backward points earliest first, then the
     // forward ones; both start at t0, so t0 appears twice (as in the reference)
     const int64_t nf = (int64_t)fwd.size() / 10, nb = (int64_t)bwd.size() / 10, n = nf + nb;
@@ -805,7 +814,7 @@ void Model::compute_trajectory() {
     }
     knots.tstart = knots.t.front();
     knots.tstop = knots.t.back();
-    spline_second_derivatives(knots);
+    spline_second_derivatives(knots, threads);
     return;
   }
   const size_t nf = (size_t)(1 + (ctstop - P.t0) / kC / dt);
@@ -845,7 +854,7 @@ void Model::compute_trajectory() {
       push_point(bwd, x, dxdt, t2);
     }
   };
-  if (nf + nb > 4096) {
+  if (threads && nf + nb > 4096) {
     parallel_tasks(2, [&](int i) {
       if (i == 0) forward();
       else backward();
@@ -872,7 +881,7 @@ void Model::compute_trajectory() {
   }
   knots.tstart = knots.t.front();
   knots.tstop = knots.t.back();
-  spline_second_derivatives(knots);
+  spline_second_derivatives(knots, threads);
 }
 
 void Model::set_trajectory(const double* traj, int64_t n) {
@@ -901,7 +910,7 @@ void Model::ensure_trajectory() {
 // Spline (include/TOMATH.h:141-203): the diagonal recurrence depends only on the knot times, so it
 // is shared by the 9 components; each component's right-hand side sweep runs on its own.
 // ---------------------------------------------------------------------------------------------
-void spline_second_derivatives(Knots& k) {
+void spline_second_derivatives(Knots& k, bool threads) {
   const int64_t N = k.n;
   const double* X = k.t.data();
   k.ypp.assign(9 * N, 0.0);
@@ -935,7 +944,7 @@ void spline_second_derivatives(Knots& k) {
     ypp[N - 1] = (un - qn * u[N - 2]) / (qn * diag[N - 2] + 1.);
     for (int64_t j = N - 2; j >= 0; --j) ypp[j] = ypp[j] * ypp[j + 1] + u[j];
   };
-  if (N > 4096) {
+  if (threads && N > 4096) {
     parallel_tasks(9, component);
   } else {
     for (int c = 0; c < 9; ++c) component(c);

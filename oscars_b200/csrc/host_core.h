@@ -165,6 +165,11 @@ class Model {
   // Throws osc::Error on failure.
   void compute_trajectory();
   void ensure_trajectory();
+  // The trajectory of particle P with this model's fields, times and method into `out` (knots and
+  // spline); `sweep` (2 vectors) holds the forward / backward points.  Reads the model only, so
+  // several threads may integrate different particles at once (threads = false: no use of the host
+  // task pool inside).
+  void integrate(const Particle& P, Knots& out, std::vector<double>* sweep, bool threads) const;
   // Select the method: "RK4" (precision must be -1, the binding's "not given") or "RKAS".
   void set_trajectory_calculation(const std::string& method, double precision);
   // Use a trajectory computed elsewhere (10 x n SoA: t, x y z, beta, a/c) with its spline.
@@ -172,7 +177,9 @@ class Model {
 };
 
 // Spline second derivatives of the 9 components (TSpline1D3::Derivatives, include/TOMATH.h:141-203).
-void spline_second_derivatives(Knots& k);
+// `threads`: the 9 components on the host task pool (callers that are themselves worker threads pass
+// false).
+void spline_second_derivatives(Knots& k, bool threads = true);
 
 // Runs fn(0) .. fn(n - 1) on a process-wide set of persistent host threads (the caller works too)
 // and returns when all have finished; the first exception a task throws is rethrown here.  Calls
