@@ -4,8 +4,8 @@
   and that sequence is the reference's (pinned through the CPU oracle's sampler).
 * Two gloo ranks each integrate their particles (round robin, weight 1/N) and one all_reduce gives
   the whole multi-particle flux: checked against the oracle's own N-particle request.  The
-  per-particle integrals run on the CPU oracle here; on the GPU the same split is made by the
-  ``shard=(rank, count)`` option (test_gpu_batch.py checks that shards add up to the whole).
+  per-particle integrals run on the CPU oracle here (no GPU); test_gpu_shard.py runs the same split
+  with two processes computing with the product.
 """
 import math
 import os
