@@ -62,7 +62,7 @@ Engine::Engine(int dev) : device(dev) {
         "cudaHostAlloc");
   check(cudaHostAlloc(reinterpret_cast<void**>(&stage_host_), kStageDoubles * sizeof(double), cudaHostAllocDefault),
         "cudaHostAlloc");
-  check(cudaHostAlloc(reinterpret_cast<void**>(&ctl_host_), 16 * sizeof(unsigned), cudaHostAllocDefault),
+  check(cudaHostAlloc(reinterpret_cast<void**>(&ctl_host_), 16 * sizeof(unsigned), cudaHostAllocMapped),
         "cudaHostAlloc");
   for (int i = 0; i < kStatSlots; ++i) check(cudaEventCreateWithFlags(&stats_ev_[i], cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming), "event");
@@ -556,12 +556,11 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   };
   for (int L = Lfirst; L <= Lpre; ++L) launch_wave(L);
   for (int L = Lpre + 1; L <= lstop; ++L) {  // beyond the prefilled levels the host decides
-    // pinned destinations: the copies are plain DMA and the wait is one stream synchronisation
+    // a one-thread kernel writes the active count and the highest finished level into mapped host
+    // memory behind a sequence word that the host polls (no copy engine, no stream wake-up)
     const unsigned* active = fused ? fz3 + (L - Lfirst) % 3 : cnt + cur_list;
-    check(cudaMemcpyAsync(ctl_host_, active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
-    check(cudaMemcpyAsync(ctl_host_ + 1, level_max, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
-    check(cudaStreamSynchronize(st), "count");
-    const unsigned nn = ctl_host_[0], lmax = ctl_host_[1];
+    unsigned nn = 0, lmax = 0;
+    report_counts(active, level_max, &nn, &lmax, st);
     if (nn == 0) {
       if (!tuning_) prefill_hist_[hist_key] = std::max<int>(Lfirst, (int)lmax);
       break;
@@ -738,6 +737,37 @@ class TrajectoryPipeline {
   size_t next_ = 0, consumed_ = 0;
   bool stop_ = false;
 };
+
+__global__ void k_report_counts(const unsigned* __restrict__ a, const unsigned* __restrict__ b,
+                                volatile unsigned* host, unsigned seq) {
+  host[1] = *a;
+  host[2] = *b;
+  __threadfence_system();
+  host[0] = seq;
+}
+
+// The two device words `a` and `b` once the stream reaches this point: a one-thread kernel stores
+// them into the mapped control words (ctl_host_[1], [2]) and then the sequence number into [0],
+// which the host polls; every 4096 polls it asks whether the stream has finished, so a failed or
+// lost launch ends in the stream's error instead of a wait that does not end.
+void Engine::report_counts(const unsigned* a, const unsigned* b, unsigned* va, unsigned* vb, cudaStream_t st) {
+  const unsigned seq = ++report_seq_;
+  volatile unsigned* w = ctl_host_;
+  k_report_counts<<<1, 1, 0, st>>>(a, b, ctl_host_, seq);
+  check(cudaGetLastError(), "count");
+  ++last_launches;
+  for (unsigned i = 1; w[0] != seq; ++i) {
+    if ((i & 4095u) == 0) {
+      const cudaError_t e = cudaStreamQuery(st);
+      if (e != cudaErrorNotReady) {
+        check(e, "count");
+        if (w[0] != seq) throw Error{OSC_ERR_CUDA, "count: the report kernel did not write its sequence number"};
+      }
+    }
+  }
+  *va = w[1];
+  *vb = w[2];
+}
 
 void Engine::radiation(RadRequest& rq) {
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};

@@ -145,9 +145,12 @@ class Engine {
   // (not converged, samples, unit counter of the running wave), [12] highest finished level -- all
   // zeroed by one memset of words 0..12 per request -- and [kCntErr] the sticky error word.
   static constexpr int kCntErr = 15;
-  // pinned words the host reads back: [0] active count and [1] highest finished level between waves,
-  // [4..7] the batch statistics (two 64-bit counters), [8] the batch error word
-  unsigned* ctl_host_ = nullptr;
+  // pinned words the host reads back: [0] sequence word, [1] active count and [2] highest finished
+  // level between waves (report_counts), [4..7] the batch statistics (two 64-bit counters), [8] the
+  // batch error word, [9] the STL active count
+  unsigned* ctl_host_ = nullptr;  // mapped (cudaHostAllocMapped): also written by k_report_counts
+  unsigned report_seq_ = 0;
+  void report_counts(const unsigned* a, const unsigned* b, unsigned* va, unsigned* vb, cudaStream_t st);
   static constexpr int kStatSlots = 64;
   cudaEvent_t stats_ev_[kStatSlots] = {};
   cudaEvent_t stage_ev_ = nullptr;

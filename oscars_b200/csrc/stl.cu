@@ -93,9 +93,9 @@ void Engine::power_density_stl(const double* tri, const double* centers, int64_t
       last_samples += ((int64_t)1 << L) * n;
       last_level = L;
       if (L > 8) {  // facets can stop from level 9 on
-        check(cudaMemcpyAsync(ctl_host_, n_active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
+        check(cudaMemcpyAsync(ctl_host_ + 9, n_active, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "count");
         check(cudaStreamSynchronize(st), "count");
-        if (ctl_host_[0] == 0) break;
+        if (ctl_host_[9] == 0) break;
       }
     }
     (void)last_level;
