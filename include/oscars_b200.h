@@ -111,7 +111,24 @@ typedef struct {
   int distribution;         /* osc_distribution */
   double ctstartstop[2];
   int has_ctstartstop;
+  /* Twiss gamma and the lattice reference point of the Twiss values (add_particle_beam's 'gamma',
+   * 'lattice_reference'); any two of beta / alpha / gamma (or all three) define the optics. */
+  double gamma[2];
+  int has_gamma;
+  double lattice_reference[3];
+  int has_lattice_reference;
+  int predefined;           /* osc_predefined_beam: 0 none, else TParticleBeam::SetPredefinedBeam */
+  int has_d0;               /* predefined beams: d0 given (replaces the beam's direction) */
+  double weight;            /* share of the particles drawn from this beam (> 0; 0 counts as 1) */
 } osc_beam_desc;
+
+/* Predefined beams of TParticleBeam::SetPredefinedBeam (src/TParticleBeam.cc:135-206). */
+typedef enum {
+  OSC_BEAM_NONE = 0,
+  OSC_BEAM_NSLSII = 1,
+  OSC_BEAM_NSLSII_LONGSTRAIGHT = 2,
+  OSC_BEAM_NSLSII_SHORTSTRAIGHT = 3
+} osc_predefined_beam;
 
 typedef struct {
   int polarization;         /* osc_polarization */
@@ -156,7 +173,16 @@ OSC_API int osc_add_field_file(osc_ctx* ctx, const char* path, const char* forma
 
 /* ---- beam: set_particle_beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) ------------------ */
 OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* beam);
-OSC_API int osc_set_seed(osc_ctx* ctx, int seed);                  /* TRandomA::SetSeed */
+OSC_API int osc_set_seed(osc_ctx* ctx, int seed);
+/* Several beams (OSCARSSR::AddParticleBeam, binding src/OSCARSSR_Python.cc:3699-4100): append a beam
+ * named `name` ("" = "_beam<k>", k the beams held; a repeated name is refused).  Each new random
+ * particle comes from a beam picked by weight; adding the first beam makes its ideal particle the
+ * current one.  osc_set_beam is osc_clear_beams followed by osc_add_beam with name "". */
+OSC_API int osc_add_beam(osc_ctx* ctx, const osc_beam_desc* beam, const char* name);
+OSC_API int osc_clear_beams(osc_ctx* ctx);
+/* OSCARSSR::SetNewParticle(beam, "ideal" or random) (src/OSCARSSR.cc:510-524): beam "" picks one by
+ * weight. */
+OSC_API int osc_set_new_particle_of_beam(osc_ctx* ctx, const char* beam, int ideal);                  /* TRandomA::SetSeed */
 OSC_API int osc_set_new_particle(osc_ctx* ctx, int ideal);         /* OSCARSSR::SetNewParticle */
 OSC_API int osc_get_particle(osc_ctx* ctx, double x0[3], double beta0[3], double* t0, double* gamma);
 /* Draw n particles from the beam exactly as a request with nparticles = n does (advancing the

@@ -59,9 +59,11 @@ def load():
     lib.orc_get_bfield.argtypes = [ctypes.c_void_p, dp, D, dp]
     lib.orc_set_half_period_scale.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
     lib.orc_add_grid.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_long), dp, dp, dp, dp, dp, dp, D, D, D]
-    lib.orc_set_beam.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D, D, dp, dp, D, D, dp,
-                                 ctypes.c_int, D, dp, ctypes.c_int, dp, dp, ctypes.c_int,
-                                 ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int]
+    lib.orc_set_beam.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D, D, dp, dp, D, D, dp, ctypes.c_int, D, dp,
+                                 ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, dp,
+                                 ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, D,
+                                 ctypes.c_int]
+    lib.orc_set_new_particle_of.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.orc_set_ctstartstop.argtypes = [ctypes.c_void_p, D, D]
     lib.orc_set_npoints_trajectory.argtypes = [ctypes.c_void_p, ctypes.c_long]
     lib.orc_get_npoints_trajectory.argtypes = [ctypes.c_void_p]
@@ -558,14 +560,33 @@ class OracleSR:
         self._lib.orc_get_bfield(self._h, _dp(X), float(t), _dp(out))
         return list(out)
 
-    def set_particle_beam(self, type="electron", name="", energy_GeV=-1, d0=None, x0=None, beam="",
+    def clear_particle_beams(self):
+        self._beam_names = []
+
+    def set_particle_beam(self, **kw):
+        self._beam_names = []
+        self.add_particle_beam(_append=0, **kw)
+
+    def add_particle_beam(self, type="electron", name="", energy_GeV=-1, d0=None, x0=None, beam="",
                           sigma_energy_GeV=0, t0=0, current=0, weight=1, rotations=None,
                           translation=None, horizontal_direction=None, beta=None, alpha=None,
                           gamma=None, emittance=None, eta=None, lattice_reference=None, mass=0,
-                          charge=0, ctstartstop=None, distribution=""):
+                          charge=0, ctstartstop=None, distribution="", _append=1):
+        """OSCARSSR_AddParticleBeam (src/OSCARSSR_Python.cc:3699-4100)."""
+        names = getattr(self, "_beam_names", [])
+        if not _append:
+            names = []
+        predefined = 0
         if beam:
-            raise ValueError("predefined beams are not part of the oracle")
-        if type not in _PARTICLE_TYPES:
+            predefined = {"NSLSII": 1, "NSLS2": 1, "NSLS-II": 1, "NSLSII-LONGSTRAIGHT": 2, "NSLS2-LONGSTRAIGHT": 2,
+                          "NSLS-II-LONGSTRAIGHT": 2, "NSLSII-SHORTSTRAIGHT": 3, "NSLS2-SHORTSTRAIGHT": 3,
+                          "NSLS-II-SHORTSTRAIGHT": 3}.get(beam.upper(), 0)
+            if not predefined:
+                raise ValueError("Error in predefined beam name / definition")
+        elif type not in _PARTICLE_TYPES:
+            raise ValueError("invalid argument in adding particle beam.  possibly 'name' already exists")
+        my_name = name if name else "_beam%d" % len(names)
+        if my_name in names:
             raise ValueError("invalid argument in adding particle beam.  possibly 'name' already exists")
         d = _v3(d0, "d0") if d0 is not None else [0.0, 0.0, 1.0]
         x = _v3(x0, "x0") if x0 is not None else [0.0, 0.0, 0.0]
@@ -588,14 +609,19 @@ class OracleSR:
         em = a(emittance if emittance is not None else [0, 0])
         bt = a(beta if beta is not None else [0, 0])
         al = a(alpha if alpha is not None else [0, 0])
+        gm = a(gamma if gamma is not None else [0, 0])
         et = a(eta if eta is not None else [0, 0])
+        lr = a(lattice_reference if lattice_reference is not None else [0, 0, 0])
         cs = a(ctstartstop if ctstartstop is not None else [0, 0])
         dist = {"": -1, "filament": 1, "gaussian": 2, "kv": 3}[distribution.lower()]
         self._check(self._lib.orc_set_beam(
-            self._h, _PARTICLE_TYPES[type], float(charge), float(mass), float(energy_GeV), _dp(X),
+            self._h, _PARTICLE_TYPES.get(type, 0), float(charge), float(mass), float(energy_GeV), _dp(X),
             _dp(Dd), float(t0), float(current), _dp(H), 1, float(sigma_energy_GeV), _dp(em),
             int(emittance is not None), _dp(bt), _dp(al), int(beta is not None),
-            int(alpha is not None), _dp(et), dist, _dp(cs), int(ctstartstop is not None)))
+            int(alpha is not None), _dp(et), dist, _dp(cs), int(ctstartstop is not None), _dp(gm),
+            int(gamma is not None), _dp(lr), int(lattice_reference is not None), predefined, int(d0 is not None),
+            float(weight), int(_append)))
+        self._beam_names = names + [my_name]
 
     def set_ctstartstop(self, start, stop):
         self._lib.orc_set_ctstartstop(self._h, float(start), float(stop))
@@ -607,7 +633,11 @@ class OracleSR:
         return self._lib.orc_get_npoints_trajectory(self._h)
 
     def set_new_particle(self, beam="", particle=""):
-        self._check(self._lib.orc_set_new_particle(self._h, int(particle == "ideal")))
+        names = getattr(self, "_beam_names", [])
+        if beam and beam not in names:
+            raise ValueError("beam name not in map")
+        self._check(self._lib.orc_set_new_particle_of(self._h, names.index(beam) if beam else -1,
+                                                      int(particle.lower() == "ideal")))
 
     def get_particle(self):
         vals = [np.zeros(3), np.zeros(3)] + [np.zeros(1) for _ in range(5)]

@@ -317,7 +317,9 @@ typedef struct {
 struct orc_sim {
   orc_field fields[64];
   int nfields;
-  orc_beam beam;
+  orc_beam beams[16];   /* TParticleBeamContainer: beams and the running sums of their weights */
+  double wsum[16];
+  int nbeams;
   int has_beam;
   orc_particle p;
   double ctstart, ctstop;
@@ -513,9 +515,17 @@ static void beam_ideal_particle(const orc_beam* b, orc_particle* p) {
   particle_set_conditions(p, b->x0, vmul(b->u0, beta), b->t0);
 }
 
+/* TParticleBeamContainer::GetRandomBeamIndexByWeight (TParticleBeamContainer.cc:135-166) */
+static int pick_beam(orc_sim* s) {
+  if (s->nbeams == 1) return 0;
+  double r = rng_canonical(&s->rng) * s->wsum[s->nbeams - 1];
+  for (int i = 0; i != s->nbeams; ++i)
+    if (r < s->wsum[i]) return i;
+  return s->nbeams - 1;
+}
+
 /* TParticleBeam::GetNewParticle() Gaussian branch (TParticleBeam.cc:713-774) */
-static void beam_random_particle(orc_sim* s, orc_particle* p) {
-  const orc_beam* b = &s->beam;
+static void beam_random_particle(orc_sim* s, const orc_beam* b, orc_particle* p) {
   if (b->distribution == ORC_DIST_FILAMENT || b->distribution == ORC_DIST_NONE) {
     beam_ideal_particle(b, p);
     return;
@@ -586,74 +596,141 @@ static void beam_random_particle(orc_sim* s, orc_particle* p) {
   particle_set_conditions(p, xn, bn, b->t0);
 }
 
+/* add_particle_beam (OSCARSSR_Python.cc:3796-4096) with TParticleBeam's constructor, its setters and
+ * SetPredefinedBeam (TParticleBeam.cc:97-125, 135-206, 219-350, 374-381, 551-612); x0 / d0 already
+ * rotated and translated, `horizontal` the given direction or -d0.Orthogonal() of the unrotated one.
+ * append = 0 replaces the beams (set_particle_beam). */
 int orc_set_beam(orc_sim* s, int type_code, double charge, double mass, double energy_GeV,
                  const double x0[3], const double d0[3], double t0, double current,
                  const double horizontal[3], int has_horizontal, double sigma_energy_GeV,
                  const double emittance[2], int has_emittance, const double beta[2],
                  const double alpha[2], int has_beta, int has_alpha, const double eta[2],
-                 int distribution_override, const double ctstartstop[2], int has_ctstartstop) {
-  orc_beam* b = &s->beam;
+                 int distribution_override, const double ctstartstop[2], int has_ctstartstop,
+                 const double gamma[2], int has_gamma, const double lattice_ref[3], int has_lattice_ref,
+                 int predefined, int has_d0, double weight, int append) {
+  if (!append) s->nbeams = 0;
+  if (s->nbeams >= 16) return fail(s, ORC_ERR_ARG, "too many beams");
+  int first = s->nbeams == 0;
+  orc_beam bb;
+  orc_beam* b = &bb;
   memset(b, 0, sizeof *b);
-  if (type_qm(type_code, charge, mass, &b->q, &b->m)) return fail(s, ORC_ERR_ARG, "bad particle type");
+  if (predefined) {                                                     /* SetPredefinedBeam */
+    if (type_qm(0, 0, 0, &b->q, &b->m)) return fail(s, ORC_ERR_ARG, "bad particle type");
+    b->current = 0.500;
+    b->e0 = 3 < kg_to_gev(b->m) ? b->m : 3;
+    b->u0 = vunit(V(0, 0, 1));
+    b->t0 = 0;
+    b->x0 = V(0, 0, 0);
+    beam_twiss_at_x0(b);
+    b->emit[0] = 0.55e-9; b->emit[1] = 0.008e-9;
+    b->lattice_ref = V(0, 0, 0);
+    beam_twiss_at_x0(b);
+    double bt0 = predefined == 2 ? 18 : 1.5, bt1 = predefined == 2 ? 3.1 : 0.8;
+    b->tw_beta[0] = bt0; b->tw_beta[1] = bt1;
+    b->tw_gamma[0] = (1. + 0. * 0.) / bt0; b->tw_gamma[1] = (1. + 0. * 0.) / bt1;
+    b->tw_alpha[0] = 0; b->tw_alpha[1] = 0;
+    beam_twiss_at_x0(b);
+    b->sigma_e = predefined == 1 ? 0 : 3. * 0.00089;
+    b->vdir = vunit(V(0, 1, 0));                                        /* SetVerticalDirection */
+    b->hdir = vunit(vcross(b->vdir, b->u0));
+    b->distribution = predefined == 1 ? ORC_DIST_FILAMENT : ORC_DIST_GAUSSIAN;
+    if (energy_GeV >= 0) b->e0 = energy_GeV < kg_to_gev(b->m) ? b->m : energy_GeV;
+  }
   if (energy_GeV == -1) energy_GeV = 0;
   if (energy_GeV < 0) return fail(s, ORC_ERR_ARG, "negative energy");
+  if (weight == 0) weight = 1;
+  if (weight <= 0) return fail(s, ORC_ERR_ARG, "Particle weight cannot be negative");
   v3 dir = d0 ? V(d0[0], d0[1], d0[2]) : V(0, 0, 1);
   v3 pos = x0 ? V(x0[0], x0[1], x0[2]) : V(0, 0, 0);
   v3 hd = has_horizontal ? V(horizontal[0], horizontal[1], horizontal[2]) : vneg(vorthogonal(dir));
   hd = vunit(hd);
-  /* TParticleBeam 10-argument constructor (TParticleBeam.cc:68-101) */
-  b->x0 = pos;
-  b->u0 = vmag2(dir) > 0 ? vunit(dir) : V(0, 0, 0);
-  b->e0 = energy_GeV < kg_to_gev(b->m) ? b->m : energy_GeV;
-  b->t0 = t0;
-  double g = b->e0 / kg_to_gev(b->m);
-  double bt = sqrt(1.0 - 1.0 / (g * g));
-  b->b0 = vmul(b->u0, bt);
-  b->current = current != 0 ? current : b->q;                         /* TParticleA::SetCurrent */
-  /* SetHorizontalDirection (TParticleBeam.cc:306-312) */
+  if (!predefined) {                           /* TParticleBeam 10-argument constructor (TParticleBeam.cc:97-125) */
+    if (type_qm(type_code, charge, mass, &b->q, &b->m)) return fail(s, ORC_ERR_ARG, "bad particle type");
+    b->x0 = pos;
+    b->u0 = vmag2(dir) > 0 ? vunit(dir) : V(0, 0, 0);
+    b->e0 = energy_GeV < kg_to_gev(b->m) ? b->m : energy_GeV;
+    b->t0 = t0;
+    b->current = current != 0 ? current : b->q;                       /* TParticleA::SetCurrent */
+  } else {
+    if (has_d0) b->u0 = vunit(dir);                                    /* SetU0 */
+    b->x0 = pos;                                                       /* SetX0 */
+    beam_twiss_at_x0(b);
+  }
+  {
+    double g = b->e0 / kg_to_gev(b->m);
+    double bt = sqrt(1.0 - 1.0 / (g * g));
+    b->b0 = vmul(b->u0, bt);
+  }
+  /* SetHorizontalDirection (TParticleBeam.cc:374-381) */
   b->hdir = vunit(hd);
   b->vdir = vneg(vunit(vcross(hd, b->u0)));
-  b->distribution = ORC_DIST_FILAMENT;
   if (has_emittance) {
     b->emit[0] = emittance[0]; b->emit[1] = emittance[1];
     b->distribution = ORC_DIST_GAUSSIAN;
+  } else if (!predefined) {
+    b->distribution = ORC_DIST_FILAMENT;
   }
   if (distribution_override >= 0) b->distribution = distribution_override;
   if (sigma_energy_GeV < 0) return fail(s, ORC_ERR_ARG, "'sigma_energy_GeV' cannot be less than zero");
-  b->sigma_e = sigma_energy_GeV;
-  b->lattice_ref = V(0, 0, 0);
+  if (sigma_energy_GeV > 0) b->sigma_e = sigma_energy_GeV;
+  v3 ref = has_lattice_ref ? V(lattice_ref[0], lattice_ref[1], lattice_ref[2]) : V(0, 0, 0);
+  b->lattice_ref = ref;                                                 /* SetTwissLatticeReference */
   beam_twiss_at_x0(b);
-  if (has_beta) {                                                       /* SetTwissBetaAlpha */
-    double a0 = has_alpha ? alpha[0] : 0, a1 = has_alpha ? alpha[1] : 0;
+  int bag = (has_beta ? 4 : 0) | (has_alpha ? 2 : 0) | (has_gamma ? 1 : 0);
+  if (bag == 7) {                                                       /* SetTwissParameters */
+    for (int i = 0; i < 2; ++i) { b->tw_beta[i] = beta[i]; b->tw_alpha[i] = alpha[i]; b->tw_gamma[i] = gamma[i]; }
+  } else if (bag == 6 || bag == 4) {                                    /* SetTwissBetaAlpha */
+    double a0 = bag == 6 ? alpha[0] : 0, a1 = bag == 6 ? alpha[1] : 0;
     if (beta[0] <= 0 || beta[1] <= 0) return fail(s, ORC_ERR_ARG, "Beta cannot be <= 0");
     b->tw_beta[0] = beta[0]; b->tw_beta[1] = beta[1];
     b->tw_gamma[0] = (1. + a0 * a0) / beta[0];
     b->tw_gamma[1] = (1. + a1 * a1) / beta[1];
     b->tw_alpha[0] = a0; b->tw_alpha[1] = a1;
+  } else if (bag == 5) {                                                /* SetTwissBetaGamma */
+    for (int i = 0; i < 2; ++i) {
+      b->tw_beta[i] = beta[i]; b->tw_alpha[i] = sqrt(gamma[i] * beta[i] - 1); b->tw_gamma[i] = gamma[i];
+    }
+  } else if (bag == 3) {                                                /* SetTwissAlphaGamma */
+    if (gamma[0] == 0 || gamma[1] == 0) return fail(s, ORC_ERR_ARG, "Gamma cannot be <= 0");
+    for (int i = 0; i < 2; ++i) {
+      b->tw_beta[i] = (1. + alpha[i] * alpha[i]) / gamma[i]; b->tw_alpha[i] = alpha[i]; b->tw_gamma[i] = gamma[i];
+    }
+  }
+  if (bag == 7 || bag == 6 || bag == 5 || bag == 4 || bag == 3) {
+    if (has_lattice_ref) b->lattice_ref = ref;
     beam_twiss_at_x0(b);
   }
   if (eta) { b->eta[0] = eta[0]; b->eta[1] = eta[1]; }
+  if (t0 != 0) b->t0 = t0;
+  s->beams[s->nbeams] = *b;
+  s->wsum[s->nbeams] = s->nbeams == 0 ? weight : s->wsum[s->nbeams - 1] + weight;
+  s->nbeams++;
   s->has_beam = 1;
   if (has_ctstartstop) orc_set_ctstartstop(s, ctstartstop[0], ctstartstop[1]);
   else orc_set_ctstartstop(s, -3, 3);                                    /* Python.cc:4087-4093 */
-  beam_ideal_particle(b, &s->p);                                         /* SetNewParticle("", "ideal") */
+  if (first) beam_ideal_particle(&s->beams[0], &s->p);                  /* SetNewParticle("", "ideal") */
   traj_clear(&s->tr);
   return ORC_OK;
 }
 
-int orc_set_new_particle(orc_sim* s, int ideal) {
+/* OSCARSSR::SetNewParticle(beam, ideal or random) (OSCARSSR.cc:510-524); beam < 0 picks one by weight. */
+int orc_set_new_particle_of(orc_sim* s, int beam, int ideal) {
   if (!s->has_beam) return fail(s, ORC_ERR_STATE, "no beam defined");
-  if (ideal) beam_ideal_particle(&s->beam, &s->p);
-  else beam_random_particle(s, &s->p);
+  if (beam >= s->nbeams) return fail(s, ORC_ERR_RANGE, "beam name not in map");
+  const orc_beam* b = &s->beams[beam < 0 ? pick_beam(s) : beam];
+  if (ideal) beam_ideal_particle(b, &s->p);
+  else beam_random_particle(s, b, &s->p);
   traj_clear(&s->tr);
   return ORC_OK;
 }
+
+int orc_set_new_particle(orc_sim* s, int ideal) { return orc_set_new_particle_of(s, -1, ideal); }
 
 int orc_set_particle(orc_sim* s, const double x0[3], const double b0[3], double t0) {
   if (!s->has_beam) return fail(s, ORC_ERR_STATE, "no beam defined");
   orc_particle p;
   memset(&p, 0, sizeof p);
-  p.q = s->beam.q; p.m = s->beam.m; p.current = s->beam.current;
+  p.q = s->beams[0].q; p.m = s->beams[0].m; p.current = s->beams[0].current;
   particle_set_conditions(&p, V(x0[0], x0[1], x0[2]), V(b0[0], b0[1], b0[2]), t0);
   s->p = p;
   traj_clear(&s->tr);
@@ -1106,7 +1183,7 @@ static void kahan_add(double* sum, double* comp, double v) {          /* T3DScal
 static int ensure_trajectory(orc_sim* s) {
   if (!s->p.set) {
     if (!s->has_beam) return fail(s, ORC_ERR_STATE, "no beam defined");
-    beam_random_particle(s, &s->p);
+    beam_random_particle(s, &s->beams[pick_beam(s)], &s->p);
   }
   if (s->tr.n == 0) return orc_calculate_trajectory(s);
   return ORC_OK;

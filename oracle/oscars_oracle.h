@@ -56,7 +56,10 @@ int orc_set_beam(orc_sim*, int type_code, double charge, double mass, double ene
                  const double horizontal[3], int has_horizontal, double sigma_energy_GeV,
                  const double emittance[2], int has_emittance, const double beta[2],
                  const double alpha[2], int has_beta, int has_alpha, const double eta[2],
-                 int distribution_override, const double ctstartstop[2], int has_ctstartstop);
+                 int distribution_override, const double ctstartstop[2], int has_ctstartstop,
+                 const double gamma[2], int has_gamma, const double lattice_ref[3], int has_lattice_ref,
+                 int predefined, int has_d0, double weight, int append);
+int orc_set_new_particle_of(orc_sim*, int beam, int ideal);
 int orc_set_ctstartstop(orc_sim*, double start, double stop);
 int orc_set_npoints_trajectory(orc_sim*, long n);
 long orc_get_npoints_trajectory(const orc_sim*);

@@ -35,7 +35,9 @@ class BeamDesc(ctypes.Structure):
     _fields_ = [("particle", I), ("charge", D), ("mass", D), ("energy_GeV", D), ("x0", D * 3), ("d0", D * 3),
                 ("horizontal", D * 3), ("t0", D), ("current", D), ("sigma_energy_GeV", D), ("emittance", D * 2),
                 ("has_emittance", I), ("beta", D * 2), ("alpha", D * 2), ("has_beta", I), ("has_alpha", I),
-                ("eta", D * 2), ("distribution", I), ("ctstartstop", D * 2), ("has_ctstartstop", I)]
+                ("eta", D * 2), ("distribution", I), ("ctstartstop", D * 2), ("has_ctstartstop", I),
+                ("gamma", D * 2), ("has_gamma", I), ("lattice_reference", D * 3), ("has_lattice_reference", I),
+                ("predefined", I), ("has_d0", I), ("weight", D)]
 
 
 class RadOpts(ctypes.Structure):
@@ -63,6 +65,9 @@ SIGNATURES = {
     "osc_get_bfield": (I, [VP, DP, D, DP]),
     "osc_add_field_file": (I, [VP, ctypes.c_char_p, ctypes.c_char_p, DP, DP, DP, I, D, D, D]),
     "osc_set_beam": (I, [VP, ctypes.POINTER(BeamDesc)]),
+    "osc_add_beam": (I, [VP, ctypes.POINTER(BeamDesc), ctypes.c_char_p]),
+    "osc_clear_beams": (I, [VP]),
+    "osc_set_new_particle_of_beam": (I, [VP, ctypes.c_char_p, I]),
     "osc_set_seed": (I, [VP, I]),
     "osc_set_new_particle": (I, [VP, I]),
     "osc_get_particle": (I, [VP, DP, DP, DP, DP]),

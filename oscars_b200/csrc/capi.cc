@@ -199,53 +199,177 @@ OSC_API int osc_get_bfield(osc_ctx* ctx, const double x[3], double t, double out
 
 // add_particle_beam + set_particle_beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) for a
 // single user-defined beam; the TParticleBeam 10-argument constructor (src/TParticleBeam.cc:68-101).
-OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* d) {
-  return guarded(ctx, [&] {
-    using namespace osc;
-    if (!d) throw Error{OSC_ERR_INVALID, "beam descriptor is NULL"};
-    Model& M = ctx->eng->model;
-    BeamSpec b;
+// TParticleBeam::SetPredefinedBeam (src/TParticleBeam.cc:135-206): the beam's fields in the order
+// the reference sets them (each setter's recomputation included).
+static osc::BeamSpec predefined_beam(int code) {
+  using namespace osc;
+  BeamSpec b;
+  if (particle_qm(OSC_PARTICLE_ELECTRON, 0, 0, b.q, b.m)) throw Error{OSC_ERR_INVALID, "particle type"};
+  b.current = 0.500;
+  b.e0 = 3 < kg_to_gev(b.m) ? b.m : 3;  // SetE0
+  b.u0 = unit(v3(0, 0, 1));
+  b.t0 = 0;
+  b.x0 = v3(0, 0, 0);
+  b.twiss_at_x0();                      // SetX0
+  b.emit[0] = 0.55e-9;
+  b.emit[1] = 0.008e-9;
+  b.lattice_ref = v3(0, 0, 0);
+  b.twiss_at_x0();                      // SetTwissLatticeReference
+  const bool straight = code != OSC_BEAM_NSLSII;
+  const double beta[2] = {code == OSC_BEAM_NSLSII_LONGSTRAIGHT ? 18. : 1.5,
+                          code == OSC_BEAM_NSLSII_LONGSTRAIGHT ? 3.1 : 0.8};
+  for (int i = 0; i < 2; ++i) {        // SetTwissBetaAlpha(beta, (0, 0))
+    b.tw_beta[i] = beta[i];
+    b.tw_gamma[i] = (1. + 0. * 0.) / beta[i];
+    b.tw_alpha[i] = 0;
+  }
+  b.twiss_at_x0();
+  b.sigma_e = straight ? 3. * 0.00089 : 0;
+  b.vdir = unit(v3(0, 1, 0));           // SetVerticalDirection
+  b.hdir = unit(cross(b.vdir, b.u0));
+  b.distribution = straight ? OSC_DIST_GAUSSIAN : OSC_DIST_FILAMENT;
+  return b;
+}
+
+// One beam as add_particle_beam builds it (src/OSCARSSR_Python.cc:3796-4096), from a descriptor
+// whose x0 / d0 are already rotated and translated and whose horizontal direction is the one given
+// or -d0.Orthogonal() of the unrotated direction.
+static osc::BeamSpec build_beam(const osc_beam_desc* d) {
+  using namespace osc;
+  const bool pre = d->predefined != OSC_BEAM_NONE;
+  if (pre && d->predefined != OSC_BEAM_NSLSII && d->predefined != OSC_BEAM_NSLSII_LONGSTRAIGHT &&
+      d->predefined != OSC_BEAM_NSLSII_SHORTSTRAIGHT)
+    throw Error{OSC_ERR_INVALID, "Error in predefined beam name / definition"};
+  BeamSpec b;
+  if (pre) {
+    b = predefined_beam(d->predefined);
+    if (d->energy_GeV >= 0) b.e0 = d->energy_GeV < kg_to_gev(b.m) ? b.m : d->energy_GeV;  // SetE0
+  }
+  const double e = d->energy_GeV == -1 ? 0 : d->energy_GeV;
+  if (e < 0) throw Error{OSC_ERR_INVALID, "We do not currently support negative energy beams.  Please change 'energy_GeV' to >= 0"};
+  const double w = d->weight == 0 ? 1 : d->weight;
+  if (w <= 0) throw Error{OSC_ERR_INVALID, "Particle weight cannot be negative"};
+  const Vec3 dir = V3(d->d0);
+  const Vec3 hd = unit(V3(d->horizontal));  // the binding normalises once ...
+  if (!pre) {  // the TParticleBeam constructor (src/TParticleBeam.cc:97-125)
     if (particle_qm(d->particle, d->charge, d->mass, b.q, b.m))
       throw Error{OSC_ERR_INVALID, "invalid argument in adding particle beam.  possibly 'name' already exists"};
     if (d->particle == OSC_PARTICLE_CUSTOM && (d->mass == 0 || d->charge == 0))
       throw Error{OSC_ERR_INVALID, "'mass' or 'charge' is zero"};
-    double e = d->energy_GeV == -1 ? 0 : d->energy_GeV;
-    if (e < 0) throw Error{OSC_ERR_INVALID, "We do not currently support negative energy beams.  Please change 'energy_GeV' to >= 0"};
-    if (d->sigma_energy_GeV < 0) throw Error{OSC_ERR_INVALID, "'sigma_energy_GeV' cannot be less than zero"};
-    const Vec3 dir = V3(d->d0);
-    const Vec3 hd = unit(V3(d->horizontal));  // binding normalises once ...
     b.x0 = V3(d->x0);
     b.u0 = mag2(dir) > 0 ? unit(dir) : Vec3{};
     b.e0 = e < kg_to_gev(b.m) ? b.m : e;
     b.t0 = d->t0;
     b.current = d->current != 0 ? d->current : b.q;
-    b.hdir = unit(hd);  // ... and SetHorizontalDirection again (src/TParticleBeam.cc:306-312)
-    b.vdir = -unit(cross(hd, b.u0));
-    b.distribution = OSC_DIST_FILAMENT;
-    if (d->has_emittance) {
-      b.emit[0] = d->emittance[0];
-      b.emit[1] = d->emittance[1];
-      b.distribution = OSC_DIST_GAUSSIAN;
-    }
-    if (d->distribution != OSC_DIST_DEFAULT) b.distribution = d->distribution;
-    b.sigma_e = d->sigma_energy_GeV;
+  } else {
+    if (d->has_d0) b.u0 = unit(dir);  // SetU0
+    b.x0 = V3(d->x0);                 // SetX0
     b.twiss_at_x0();
-    if (d->has_beta) {  // SetTwissBetaAlpha (src/TParticleBeam.cc:177-196)
-      const double a0 = d->has_alpha ? d->alpha[0] : 0, a1 = d->has_alpha ? d->alpha[1] : 0;
-      if (d->beta[0] <= 0 || d->beta[1] <= 0) throw Error{OSC_ERR_RANGE, "Beta cannot be <= 0"};
-      b.tw_beta[0] = d->beta[0]; b.tw_beta[1] = d->beta[1];
-      b.tw_gamma[0] = (1. + a0 * a0) / d->beta[0];
-      b.tw_gamma[1] = (1. + a1 * a1) / d->beta[1];
+  }
+  b.weight = w;
+  b.hdir = unit(hd);  // ... and SetHorizontalDirection again (src/TParticleBeam.cc:374-381)
+  b.vdir = -unit(cross(hd, b.u0));
+  if (d->has_emittance) {
+    b.emit[0] = d->emittance[0];
+    b.emit[1] = d->emittance[1];
+    b.distribution = OSC_DIST_GAUSSIAN;
+  } else if (!pre) {
+    b.distribution = OSC_DIST_FILAMENT;
+  }
+  if (d->distribution != OSC_DIST_DEFAULT) b.distribution = d->distribution;
+  if (d->sigma_energy_GeV < 0) throw Error{OSC_ERR_INVALID, "'sigma_energy_GeV' cannot be less than zero"};
+  if (d->sigma_energy_GeV > 0) b.sigma_e = d->sigma_energy_GeV;
+  const Vec3 ref = d->has_lattice_reference ? V3(d->lattice_reference) : v3(0, 0, 0);
+  b.lattice_ref = ref;  // SetTwissLatticeReference
+  b.twiss_at_x0();
+  const int bag = (d->has_beta ? 4 : 0) | (d->has_alpha ? 2 : 0) | (d->has_gamma ? 1 : 0);
+  const double* B = d->beta;
+  const double* A = d->alpha;
+  const double* G = d->gamma;
+  const bool set_ref = d->has_lattice_reference != 0;
+  auto finish = [&]() {
+    if (set_ref) b.lattice_ref = ref;
+    b.twiss_at_x0();
+  };
+  switch (bag) {  // src/TParticleBeam.cc:219-350
+    case 7:
+      for (int i = 0; i < 2; ++i) { b.tw_beta[i] = B[i]; b.tw_alpha[i] = A[i]; b.tw_gamma[i] = G[i]; }
+      finish();
+      break;
+    case 6:
+    case 4: {
+      const double a0 = bag == 6 ? A[0] : 0, a1 = bag == 6 ? A[1] : 0;
+      if (B[0] <= 0 || B[1] <= 0) throw Error{OSC_ERR_RANGE, "Beta cannot be <= 0"};
+      b.tw_beta[0] = B[0]; b.tw_beta[1] = B[1];
+      b.tw_gamma[0] = (1. + a0 * a0) / B[0];
+      b.tw_gamma[1] = (1. + a1 * a1) / B[1];
       b.tw_alpha[0] = a0; b.tw_alpha[1] = a1;
-      b.twiss_at_x0();
+      finish();
+      break;
     }
-    b.eta[0] = d->eta[0];
-    b.eta[1] = d->eta[1];
-    M.beam = b;
-    M.has_beam = true;
-    if (d->has_ctstartstop) M.set_ctstartstop(d->ctstartstop[0], d->ctstartstop[1]);
-    else M.set_ctstartstop(-3, 3);
-    M.ideal_particle();
+    case 5:
+      for (int i = 0; i < 2; ++i) {
+        b.tw_beta[i] = B[i];
+        b.tw_alpha[i] = std::sqrt(G[i] * B[i] - 1);
+        b.tw_gamma[i] = G[i];
+      }
+      finish();
+      break;
+    case 3:
+      if (G[0] == 0 || G[1] == 0) throw Error{OSC_ERR_RANGE, "Gamma cannot be <= 0"};
+      for (int i = 0; i < 2; ++i) {
+        b.tw_beta[i] = (1. + A[i] * A[i]) / G[i];
+        b.tw_alpha[i] = A[i];
+        b.tw_gamma[i] = G[i];
+      }
+      finish();
+      break;
+    default:
+      break;
+  }
+  b.eta[0] = d->eta[0];
+  b.eta[1] = d->eta[1];
+  if (d->t0 != 0) b.t0 = d->t0;
+  return b;
+}
+
+static void add_beam(osc::Model& M, const osc_beam_desc* d, const char* name) {
+  using namespace osc;
+  if (!d) throw Error{OSC_ERR_INVALID, "beam descriptor is NULL"};
+  const bool first = M.beams.empty();
+  BeamSpec b = build_beam(d);
+  b.name = name && *name ? std::string(name) : "_beam" + std::to_string(M.beams.size());
+  for (const BeamSpec& o : M.beams)
+    if (o.name == b.name)
+      throw Error{OSC_ERR_INVALID, d->predefined != OSC_BEAM_NONE
+                                       ? "Error in predefined beam name / definition"
+                                       : "invalid argument in adding particle beam.  possibly 'name' already exists"};
+  M.add_beam(b);
+  if (d->has_ctstartstop) M.set_ctstartstop(d->ctstartstop[0], d->ctstartstop[1]);
+  else M.set_ctstartstop(-3, 3);
+  if (first) M.new_particle("", true);  // SetNewParticle("", "ideal")
+}
+
+OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* d) {
+  return guarded(ctx, [&] {
+    ctx->eng->model.clear_beams();
+    add_beam(ctx->eng->model, d, "");
+  });
+}
+
+OSC_API int osc_add_beam(osc_ctx* ctx, const osc_beam_desc* d, const char* name) {
+  return guarded(ctx, [&] { add_beam(ctx->eng->model, d, name); });
+}
+
+OSC_API int osc_clear_beams(osc_ctx* ctx) {
+  return guarded(ctx, [&] { ctx->eng->model.clear_beams(); });
+}
+
+OSC_API int osc_set_new_particle_of_beam(osc_ctx* ctx, const char* beam, int ideal) {
+  return guarded(ctx, [&] {
+    osc::Model& M = ctx->eng->model;
+    if (!M.has_beam) throw osc::Error{OSC_ERR_RANGE, "no beam defined"};
+    M.new_particle(beam ? std::string(beam) : std::string(), ideal != 0);
   });
 }
 

@@ -513,7 +513,45 @@ void Model::set_ctstartstop(double a, double b) {  // OSCARSSR::SetCTStartStop (
   ctstop = b;
 }
 
-void Model::ideal_particle() {  // TParticleBeam::GetNewParticle("ideal") (:667-688)
+void Model::add_beam(const BeamSpec& b) {  // TParticleBeamContainer::AddNewParticleBeam
+  beam_weight_sums.push_back(beam_weight_sums.empty() ? b.weight : beam_weight_sums.back() + b.weight);
+  beams.push_back(b);
+  has_beam = true;
+}
+
+void Model::clear_beams() {
+  beams.clear();
+  beam_weight_sums.clear();
+  has_beam = false;
+}
+
+size_t Model::pick_beam() {  // TParticleBeamContainer::GetRandomBeamIndexByWeight (:135-166)
+  const size_t N = beam_weight_sums.size();
+  if (N == 0) throw Error{OSC_ERR_RANGE, "no beam defined"};
+  if (N == 1) return 0;
+  const double r = rng.uniform(rng.mt) * beam_weight_sums[N - 1];
+  for (size_t i = 0; i != N; ++i)
+    if (r < beam_weight_sums[i]) return i;
+  throw Error{OSC_ERR_RANGE, "random weight out of range.  SERIOUS ERROR"};
+}
+
+size_t Model::find_beam(const std::string& name) const {
+  for (size_t i = 0; i < beams.size(); ++i)
+    if (beams[i].name == name) return i;
+  throw Error{OSC_ERR_RANGE, "beam name not in map"};
+}
+
+void Model::new_particle(const std::string& name, bool ideal) {  // OSCARSSR::SetNewParticle (:510-524)
+  const BeamSpec& b = beams[name.empty() ? pick_beam() : find_beam(name)];
+  if (ideal) ideal_of(b);
+  else sample_of(b);
+}
+
+void Model::ideal_particle() { ideal_of(beams[pick_beam()]); }
+
+void Model::random_particle() { sample_of(beams[pick_beam()]); }
+
+void Model::ideal_of(const BeamSpec& beam) {  // TParticleBeam::GetNewParticle("ideal") (:667-688)
   const double g = beam.e0 / kg_to_gev(beam.m) < 1 ? 1 : beam.e0 / kg_to_gev(beam.m);
   const double b = g != 1 ? std::sqrt(1.0 - 1.0 / (g * g)) : 0;
   particle = Particle{};
@@ -525,9 +563,9 @@ void Model::ideal_particle() {  // TParticleBeam::GetNewParticle("ideal") (:667-
   ++knots_version;
 }
 
-void Model::random_particle() {  // TParticleBeam::GetNewParticle() (:692-850)
+void Model::sample_of(const BeamSpec& beam) {  // TParticleBeam::GetNewParticle() (:692-850)
   if (beam.distribution != 2 && beam.distribution != 3) {
-    ideal_particle();
+    ideal_of(beam);
     return;
   }
   const double PI = kPi;
@@ -886,8 +924,10 @@ void Model::integrate(const Particle& P, Knots& knots, std::vector<double>* swee
 
 void Model::set_trajectory(const double* traj, int64_t n) {
   if (n < 3) throw Error{OSC_ERR_LENGTH, "TSpline1D3 does not see enough points for interpolation.  Please use >= 3 points"};
+  // times may repeat (an RKAS trajectory stores its start time twice; the spline is then NaN there, as
+  // in the reference) but not decrease
   for (int64_t i = 1; i < n; ++i)
-    if (!(traj[i] > traj[i - 1])) throw Error{OSC_ERR_INVALID, "trajectory times must increase"};
+    if (!(traj[i] >= traj[i - 1])) throw Error{OSC_ERR_INVALID, "trajectory times must not decrease"};
   knots.clear();
   ++knots_version;
   knots.n = n;

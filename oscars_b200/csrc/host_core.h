@@ -108,6 +108,8 @@ struct BeamSpec {
   double beta_x0[2] = {0, 0}, alpha_x0[2] = {0, 0}, gamma_x0[2] = {0, 0};
   Vec3 lattice_ref;
   int distribution = 1;  // 1 filament, 2 gaussian, 3 KV
+  double weight = 1;     // share of the particles drawn from this beam among all beams
+  std::string name;
   void twiss_at_x0();
 };
 
@@ -142,7 +144,10 @@ struct Error {
 class Model {
  public:
   std::vector<FieldSpec> fields;
-  BeamSpec beam;
+  // Particle beams (TParticleBeamContainer, src/TParticleBeamContainer.cc): particles are drawn from
+  // a beam picked at random by weight (one uniform draw when there are several beams).
+  std::vector<BeamSpec> beams;
+  std::vector<double> beam_weight_sums;
   bool has_beam = false;
   Particle particle;
   double ctstart = 0, ctstop = 0;
@@ -160,8 +165,16 @@ class Model {
   void add_field(const FieldSpec& f);
   void clear_fields();
   void set_ctstartstop(double a, double b);
-  void ideal_particle();
-  void random_particle();
+  void add_beam(const BeamSpec& b);  // name must be unique (set by the caller)
+  void clear_beams();
+  size_t pick_beam();                 // GetRandomBeamIndexByWeight
+  size_t find_beam(const std::string& name) const;
+  // OSCARSSR::SetNewParticle(beam, "ideal" or random): `name` empty picks a beam by weight.
+  void new_particle(const std::string& name, bool ideal);
+  void ideal_particle();   // SetNewParticle("", "ideal")
+  void random_particle();  // SetNewParticle(): a beam by weight, then its random particle
+  void ideal_of(const BeamSpec& b);
+  void sample_of(const BeamSpec& b);
   // Throws osc::Error on failure.
   void compute_trajectory();
   void ensure_trajectory();

@@ -28,6 +28,9 @@ from .stl import StlContainer
 from ._lib import BeamDesc, Context, FieldDesc, RadOpts, dptr, i32ptr
 
 _ANGLE_UNSET = 112188979912321.0  # binding sentinel for "angle not given" (:5662)
+_PREDEFINED_BEAMS = {"NSLSII": 1, "NSLS2": 1, "NSLS-II": 1,
+                     "NSLSII-LONGSTRAIGHT": 2, "NSLS2-LONGSTRAIGHT": 2, "NSLS-II-LONGSTRAIGHT": 2,
+                     "NSLSII-SHORTSTRAIGHT": 3, "NSLS2-SHORTSTRAIGHT": 3, "NSLS-II-SHORTSTRAIGHT": 3}
 _PARTICLES = {"electron": 0, "anti-positron": 0, "positron": 1, "anti-electron": 1, "muon": 2,
               "anti-muon": 3, "proton": 4, "anti-proton": 5, "pi+": 6, "pi-": 7, "custom": 8}
 _NOT_CONVERGED = "Not all points converged to desired precision.  Can try increasing 'max_level_extended'\n"
@@ -236,23 +239,23 @@ class sr:
 
     # ---- beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) --------------------------------------
     def clear_particle_beams(self):
+        self._ctx.call("osc_clear_beams")
         self._nbeams = 0
 
     def set_particle_beam(self, **kw):
-        self._nbeams = 0
+        self.clear_particle_beams()
         self.add_particle_beam(**kw)
 
     def add_particle_beam(self, type="electron", name="", energy_GeV=-1, d0=None, x0=None, beam="",
                           sigma_energy_GeV=0, t0=0, current=0, weight=1, rotations=None, translation=None,
                           horizontal_direction=None, beta=None, alpha=None, gamma=None, emittance=None, eta=None,
                           lattice_reference=None, mass=0, charge=0, ctstartstop=None, distribution=""):
-        if beam:
-            raise ValueError("predefined beams are not part of this GPU build's drop-in surface")
-        if self._nbeams >= 1:
-            raise ValueError("this GPU build holds one beam; call set_particle_beam to replace it")
-        if gamma is not None or lattice_reference is not None:
-            raise ValueError("'gamma' and 'lattice_reference' are not part of this GPU build's drop-in surface")
-        if type not in _PARTICLES:
+        predefined = 0
+        if beam:  # TParticleBeam::SetPredefinedBeam (src/TParticleBeam.cc:135-206)
+            predefined = _PREDEFINED_BEAMS.get(beam.upper(), -1)
+            if predefined < 0:
+                raise ValueError("Error in predefined beam name / definition")
+        elif type not in _PARTICLES:
             raise ValueError("invalid argument in adding particle beam.  possibly 'name' already exists")
         pos = _vec3(x0, "x0") if x0 is not None else [0.0, 0.0, 0.0]
         if energy_GeV != -1 and energy_GeV < 0:
@@ -274,8 +277,10 @@ class sr:
         pos = [pos[0] + tr[0], pos[1] + tr[1], pos[2] + tr[2]]
         if type == "custom" and (mass == 0 or charge == 0):
             raise ValueError("'mass' or 'charge' is zero")
-        d = BeamDesc(particle=_PARTICLES[type], charge=float(charge), mass=float(mass), energy_GeV=float(energy_GeV),
-                     t0=float(t0), current=float(current), sigma_energy_GeV=float(sigma_energy_GeV))
+        d = BeamDesc(particle=_PARTICLES.get(type, 0), charge=float(charge), mass=float(mass),
+                     energy_GeV=float(energy_GeV), t0=float(t0), current=float(current),
+                     sigma_energy_GeV=float(sigma_energy_GeV), predefined=predefined, has_d0=int(d0 is not None),
+                     weight=float(weight))
         d.x0[:] = pos
         d.d0[:] = dr
         d.horizontal[:] = hd
@@ -288,6 +293,12 @@ class sr:
         if alpha is not None:
             d.alpha[:] = _vec2(alpha, "alpha")
             d.has_alpha = 1
+        if gamma is not None:
+            d.gamma[:] = _vec2(gamma, "gamma")
+            d.has_gamma = 1
+        if lattice_reference is not None:
+            d.lattice_reference[:] = _vec3(lattice_reference, "lattice_reference")
+            d.has_lattice_reference = 1
         if eta is not None:
             d.eta[:] = _vec2(eta, "gamma")
         dist = {"": -1, "filament": 1, "gaussian": 2, "kv": 3}
@@ -297,11 +308,13 @@ class sr:
         if ctstartstop is not None:
             d.ctstartstop[:] = _vec2(ctstartstop, "ctstartstop")
             d.has_ctstartstop = 1
-        self._ctx.call("osc_set_beam", ctypes.byref(d))
-        self._nbeams = 1
+        self._ctx.call("osc_add_beam", ctypes.byref(d), str(name).encode())
+        self._nbeams += 1
 
     def set_new_particle(self, beam="", particle=""):
-        self._ctx.call("osc_set_new_particle", int(particle.lower() == "ideal"))
+        """A new particle from the named beam, or from a beam picked by weight (beam=""): the ideal one
+        (particle='ideal') or a random one (src/OSCARSSR.cc:510-524)."""
+        self._ctx.call("osc_set_new_particle_of_beam", str(beam).encode(), int(particle.lower() == "ideal"))
 
     def _particle(self):
         x0, b0 = np.zeros(3), np.zeros(3)

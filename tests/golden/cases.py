@@ -239,6 +239,40 @@ CASES = {
     "pd_points": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, rotations=[0.0, 0.001, 0.0], translation=[0.0, 0.0005, 0.0]))],
     "pd_points_directional": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS_MIXED, normal=1))],
     "pd_points_inverted": UND_SETUP + [("calculate_power_density", dict(points=ARC_POINTS, normal=-1))],
+    # several beams picked by weight for every particle, predefined beams, Twiss given with gamma and
+    # a lattice reference point, and the ideal particle of a named beam
+    "flux_two_beams": [EPU_Y, EPU_X,
+                       ("add_particle_beam", dict(type="electron", name="a", energy_GeV=3, x0=[0, 0, 0], d0=[0, 0, 1],
+                                                  current=0.5, sigma_energy_GeV=0.003, beta=[1.5, 0.8],
+                                                  emittance=[0.9e-9, 8e-12], weight=1)),
+                       ("add_particle_beam", dict(type="electron", name="b", energy_GeV=3.01, x0=[0.0002, 0, 0],
+                                                  d0=[0.0001, 0, 1], current=0.5, sigma_energy_GeV=0.002,
+                                                  beta=[3.0, 1.2], alpha=[0.5, -0.2], emittance=[2e-9, 2e-11],
+                                                  weight=2))] + traj(16001) +
+                      [("set_seed", dict(seed=5)),
+                       ("calculate_flux_rectangle", dict(energy_eV=E1_EPU, npoints=[7, 7], width=[0.008, 0.008],
+                                                         translation=[0, 0, 30], nparticles=6))],
+    "traj_predefined_beam": [UND,
+                             ("add_particle_beam", dict(beam="NSLSII-LONGSTRAIGHT", name="ls", x0=[0, 0, -0.2],
+                                                        d0=[0.0002, 0, 1], energy_GeV=3.05))] +
+                            traj(20001) + [("set_seed", dict(seed=9)), ("set_new_particle", dict(particle="")),
+                                           ("calculate_trajectory", {})],
+    "pd_predefined_and_twiss": [UND,
+                                ("add_particle_beam", dict(beam="nsls2", name="n", weight=1)),
+                                ("add_particle_beam", dict(type="positron", name="p", energy_GeV=3, current=0.4,
+                                                           sigma_energy_GeV=0.001, beta=[2.0, 1.0], gamma=[0.6, 1.1],
+                                                           emittance=[1e-9, 1e-11], lattice_reference=[0, 0, -1],
+                                                           weight=3))] + traj() +
+                               [("set_seed", dict(seed=13)),
+                                ("calculate_power_density_rectangle", dict(npoints=[7, 7], width=[0.01, 0.01],
+                                                                           translation=[0, 0, 30], nparticles=4))],
+    "traj_named_beam_ideal": [UND,
+                              ("add_particle_beam", dict(type="electron", name="first", energy_GeV=3, current=0.5)),
+                              ("add_particle_beam", dict(type="electron", name="second", energy_GeV=2.5,
+                                                         x0=[0.001, 0, 0], d0=[0, 0.0003, 1], current=0.3,
+                                                         alpha=[0.4, 0.1], gamma=[1.0, 2.0], emittance=[1e-9, 1e-11],
+                                                         distribution="kv"))] + traj(20001) +
+                             [("set_new_particle", dict(beam="second", particle="ideal")), ("calculate_trajectory", {})],
     # adaptive Cash-Karp trajectories (RKAS): the 11-period undulator at the default precision, the
     # elliptical configuration at 1e-7; a spectrum on an RKAS trajectory (the reference's RKAS
     # trajectory holds the start time twice, so its spline and every radiation result are NaN)
