@@ -173,7 +173,7 @@ OSC_API int osc_add_field_file(osc_ctx* ctx, const char* path, const char* forma
 
 /* ---- beam: set_particle_beam (src/OSCARSSR_Python.cc:3561-3576, 3699-4100) ------------------ */
 OSC_API int osc_set_beam(osc_ctx* ctx, const osc_beam_desc* beam);
-OSC_API int osc_set_seed(osc_ctx* ctx, int seed);
+OSC_API int osc_set_seed(osc_ctx* ctx, int seed);                 /* TRandomA::SetSeed */
 /* Several beams (OSCARSSR::AddParticleBeam, binding src/OSCARSSR_Python.cc:3699-4100): append a beam
  * named `name` ("" = "_beam<k>", k the beams held; a repeated name is refused).  Each new random
  * particle comes from a beam picked by weight; adding the first beam makes its ideal particle the
@@ -182,7 +182,7 @@ OSC_API int osc_add_beam(osc_ctx* ctx, const osc_beam_desc* beam, const char* na
 OSC_API int osc_clear_beams(osc_ctx* ctx);
 /* OSCARSSR::SetNewParticle(beam, "ideal" or random) (src/OSCARSSR.cc:510-524): beam "" picks one by
  * weight. */
-OSC_API int osc_set_new_particle_of_beam(osc_ctx* ctx, const char* beam, int ideal);                  /* TRandomA::SetSeed */
+OSC_API int osc_set_new_particle_of_beam(osc_ctx* ctx, const char* beam, int ideal);
 OSC_API int osc_set_new_particle(osc_ctx* ctx, int ideal);         /* OSCARSSR::SetNewParticle */
 OSC_API int osc_get_particle(osc_ctx* ctx, double x0[3], double beta0[3], double* t0, double* gamma);
 /* Draw n particles from the beam exactly as a request with nparticles = n does (advancing the
