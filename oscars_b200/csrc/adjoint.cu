@@ -151,7 +151,7 @@ __global__ void k_adj_spline_eval(const double* __restrict__ knots, int64_t n, d
   const int64_t s = 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= s_end) return;
   const double* t = knots;
-  const double T = level_time(tstart, tstop, s);
+  const double T = level_time(tstart, tstop, s, kMaxLevelMemory);  // fixed levels, all in memory
   int64_t k = (int64_t)((T - t[0]) / (t[n - 1] - t[0]) * (double)(n - 1));
   k = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
   while (k > 0 && t[k] > T) --k;
@@ -605,6 +605,7 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
 
   model.ensure_trajectory();
   upload_trajectory();
+  set_level_grid(kMaxLevelMemory);  // fixed levels on the memory grid
   ensure_levels(level);
   const Particle& P = model.particle;
   // inputs

@@ -8,7 +8,7 @@
 //   k_batch_rk4       FP64 RK4, one thread per (job, direction)           src/OSCARSSR.cc:910-1009
 //   k_batch_extent    trajectory extent in the job frame (validity bound of the mixed phase form)
 //   k_batch_spline    clamped cubic spline, one thread per (job, component) include/TOMATH.h:141-203
-//   k_batch_fill      level samples written straight as 48-byte mixed records, one thread per sample
+//   k_batch_fill      level samples written straight as mixed pair records, one thread per sample
 //   k_batch_plan      per-job tiles, units, partial offsets and active offsets of a wave (one block)
 //   k_batch_wave      the mixed sample sum; persistent CTAs take (job, tile, span) units from a counter
 //   k_batch_finalize  span reduction and the stop rule of src/OSCARSSR.cc:4222-4238 per entry
@@ -361,10 +361,11 @@ __global__ void k_batch_spline(const DevJob* __restrict__ jobs, int njobs, doubl
 // Level samples [s_begin, s_end) of every job whose active count is non-zero (all jobs when `cnt` is
 // NULL), evaluated from its spline and written as pair records (fd_common.cuh): job j's records
 // start at float kPairFloats / 2 * j * stride of `rec`, sample s at local index s - s_off (s_off
-// even); sample 0 is the zero-amplitude record.  One thread per (job, sample).
+// even); sample 0 is the zero-amplitude record; levels above ext_from are extended levels
+// (level_time).  One thread per (job, sample).
 __global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const double* __restrict__ arena,
                              const unsigned* __restrict__ cnt, float* __restrict__ rec, int64_t stride,
-                             int64_t s_off, int64_t s_begin, int64_t s_end) {
+                             int64_t s_off, int64_t s_begin, int64_t s_end, int ext_from) {
   // The two samples of a pair sit in adjacent lanes (per = s_end - s_begin, s_begin and the block
   // size are even) and exchange their FP64 values for the pair's step: every lane reaches the
   // shuffles, lanes past the grid's end or of a finished job on a valid sample, writing nothing.
@@ -376,7 +377,7 @@ __global__ void k_batch_fill(const DevJob* __restrict__ jobs, int njobs, const d
   const DevJob& J = jobs[j];
   const int64_t s = s_begin + g % per;
   const int64_t n = (int64_t)J.nf + J.nb;
-  const double T = level_time(J.tstart, J.tstop, s == 0 ? 1 : s);
+  const double T = level_time(J.tstart, J.tstop, s == 0 ? 1 : s, ext_from);
   double v[9];
   spline_eval9(arena + J.knots, n, T, v);
   const MixedFrame& F = J.frame;
@@ -920,11 +921,9 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
   pending_.clear();
   last_samples = last_launches = last_not_converged = 0;
   if (jobs.empty()) return;
-  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
-  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
-  if (lstop > kMaxLevelMemory)
-    throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
-  if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
+  // the chunking sizes every job's records up to the prefill level, so the levels stop at 26 here
+  int ext_from = kMaxLevelMemory;  // levels above it are extended levels (level_time)
+  const int lstop = request_levels(o, kMaxLevelMemory, &ext_from);
   const int Lfirst = std::min(9, lstop);
   const int Lpre = std::min(lstop, std::max(Lfirst, kBatchPrefill));
   double pol[6];
@@ -1075,7 +1074,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
       dev::k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_knots_.as<double>(), b_work_.as<double>());
       const int64_t fill_n = rec_per_job * nj;  // samples 0 .. 2^(Lpre+1) - 1 of every job
       dev::k_batch_fill<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(
-          d_jobs, nj, b_knots_.as<double>(), nullptr, b_rec_.as<float>(), rec_per_job, 0, 0, rec_per_job);
+          d_jobs, nj, b_knots_.as<double>(), nullptr, b_rec_.as<float>(), rec_per_job, 0, 0, rec_per_job, ext_from);
       check(cudaGetLastError(), "batch trajectories");
       last_launches += 4;
       if (tune) v = tune_batch(nj, Lfirst, target, d_jobs, plan, misc, m64, rec_per_job);
@@ -1140,7 +1139,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
       b_rec_ext_.reserve((size_t)kMixedRecordBytesPerSample * len * nj);
       const int64_t fill_n = len * nj;
       dev::k_batch_fill<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(
-          d_jobs, nj, b_knots_.as<double>(), cnts[cur], b_rec_ext_.as<float>(), len, len, len, 2 * len);
+          d_jobs, nj, b_knots_.as<double>(), cnts[cur], b_rec_ext_.as<float>(), len, len, len, 2 * len, ext_from);
       check(cudaGetLastError(), "batch fill");
       ++last_launches;
       wave(L, v, len, len, b_rec_ext_.as<float4>());

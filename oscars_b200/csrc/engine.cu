@@ -165,10 +165,48 @@ void Engine::reserve_levels(int L) {
 
 void Engine::fill_levels(int64_t s_begin, int64_t s_end, cudaStream_t s) {
   check(launch_level_fill(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, lev_.as<double>(), lev_cap_,
-                          -1, bd_bits_.as<unsigned long long>(), s),
+                          lev_ext_, bd_bits_.as<unsigned long long>(), s),
         "level fill");
   ++last_launches;
   bdmax_valid_ = false;
+}
+
+// Levels above ext_from are the reference's extended levels (src/OSCARSSR.cc:4181-4186: above
+// LevelStopMemory = max_level the levels are evaluated on the fly with their own time spacing,
+// level_time in fd_common.cuh).  Cached levels whose times differ under the new split are dropped.
+void Engine::set_level_grid(int ext_from) {
+  if (ext_from != lev_ext_) {
+    const int keep = std::min(ext_from, lev_ext_);
+    if (lev_filled_ > keep) {
+      lev_filled_ = keep;
+      bdmax_valid_ = false;
+      // the beta-difference maxima of the dropped levels are folded again by their refill
+      check(cudaMemsetAsync(bd_bits_.as<unsigned long long>() + keep + 1, 0, sizeof(unsigned long long) * (31 - keep),
+                            cur_),
+            "memset");
+      ++last_launches;
+    }
+    lev_ext_ = ext_from;
+  }
+  if (ext_from != mrec_ext_) {
+    mrec_filled_ = std::min(mrec_filled_, std::min(ext_from, mrec_ext_));
+    mrec_ext_ = ext_from;
+  }
+}
+
+// Last level of a request and the split between the reference's memory levels and its extended
+// levels (src/OSCARSSR.cc:4108-4109): LevelStopMemory = max_level (within [-1, 26]), levels up to
+// max(max_level_extended, LevelStopMemory).  Returns the last level; `ext_from` is the highest level
+// on the memory grid (26 when no extended level is used, so requests without them share the cache).
+int request_levels(const osc_rad_opts& o, int max_supported, int* ext_from) {
+  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
+  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
+  if (lstop > max_supported)
+    throw Error{OSC_ERR_RANGE, "max_level_extended above " + std::to_string(max_supported) +
+                                   " is not supported by this GPU build for this calculation"};
+  if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
+  *ext_from = lstop > lstop_mem ? lstop_mem : kMaxLevelMemory;
+  return lstop;
 }
 
 // Make levels 0..L resident.
@@ -231,8 +269,8 @@ void Engine::reserve_mixed(int L) {
 }
 
 void Engine::fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s) {
-  check(launch_mixed_records(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, frame_, mrec_.as<float4>(),
-                             s),
+  check(launch_mixed_records(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, mrec_ext_, frame_,
+                             mrec_.as<float4>(), s),
         "mixed records");
   ++last_launches;
 }
@@ -382,11 +420,9 @@ int Engine::pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, 
 void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,
                         cudaStream_t st) {
   const osc_rad_opts& o = rq.opts;
-  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
-  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
-  if (lstop > kMaxLevelMemory)
-    throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
-  if (lstop < 0) throw Error{OSC_ERR_RANGE, "max_level -1 selects only extended levels, which this GPU build does not support"};
+  int ext_from = kMaxLevelMemory;
+  const int lstop = request_levels(o, kMaxLevelExtendedGpu, &ext_from);
+  set_level_grid(ext_from);
   const Particle& P = model.particle;
   const bool mixed = o.precision_mode == OSC_MIXED;
   if (mixed && rq.power_density)

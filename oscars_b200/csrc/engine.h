@@ -17,6 +17,13 @@
 namespace osc {
 
 // Device buffer that only grows.
+// Highest level a flux, spectrum or power-density request may reach: levels above 26 (the reference's
+// extended levels) are held in device memory like the others (2^(L+1) samples of 80 bytes, FP64; 72
+// bytes, mixed), so a request is bounded by the free memory; the reference's own point count of a
+// level is an int, which caps it at 30.
+constexpr int kMaxLevelExtendedGpu = 30;
+int request_levels(const osc_rad_opts& o, int max_supported, int* ext_from);
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -128,6 +135,9 @@ class Engine {
   DevBuf lev_;
   int64_t lev_cap_ = 0;
   int lev_filled_ = -1;
+  // levels above these in lev_ / mrec_ are the reference's extended levels (their own time spacing)
+  int lev_ext_ = kMaxLevelMemory, mrec_ext_ = kMaxLevelMemory;
+  void set_level_grid(int ext_from);
   DevBuf bd_bits_;                 // 32 x u64
   std::vector<double> bdmax_;      // per level, host copy
   bool bdmax_valid_ = false;

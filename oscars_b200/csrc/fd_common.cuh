@@ -47,12 +47,18 @@ __device__ __forceinline__ void spline_eval9(const double* __restrict__ knots, i
 }
 
 // Time of sample s of the level ladder (level L = floor(log2 s), i = s - 2^L):
-// tstart + T/2^(L+1) + i T/2^L  (src/TParticleTrajectoryInterpolated.cc:124-158).
-__device__ __forceinline__ double level_time(double tstart, double tstop, int64_t s) {
+// tstart + T/2^(L+1) + i dt_L.  Levels up to ext_from are the ones the reference holds in memory,
+// dt_L = T/2^L (src/TParticleTrajectoryInterpolated.cc:124-158); the levels above them are its
+// extended levels, evaluated on the fly with dt_L = T/(2^L - 1) (TParticleTrajectoryInterpolatedPoints::Set
+// and GetT, src/TParticleTrajectoryInterpolatedPoints.cc:32-55; GetDeltaTThisLevel,
+// src/TParticleTrajectoryInterpolated.cc:242-251).  Extended levels do not nest with the lower ones and
+// their last samples lie past tstop, where the spline continues its last interval's cubic, as the
+// reference's does.
+__device__ __forceinline__ double level_time(double tstart, double tstop, int64_t s, int ext_from) {
   const int L = 63 - __clzll((unsigned long long)s);
   const int64_t i = s - ((int64_t)1 << L);
   const double ts = __dadd_rn(tstart, __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L + 1)));
-  const double sp = __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L));
+  const double sp = __ddiv_rn(__dsub_rn(tstop, tstart), L > ext_from ? __dsub_rn(ldexp(1.0, L), 1.0) : ldexp(1.0, L));
   return __dadd_rn(ts, __dmul_rn(sp, (double)i));
 }
 

@@ -188,10 +188,11 @@ __host__ __device__ inline double mixed_theta_max(double gamma) {
   return t < 1e-2 ? t : 1e-2;
 }
 
-// Mixed pair records (fd_common.cuh, 160 bytes per two samples) of level samples [s_begin, s_end),
-// evaluated from the trajectory knots (t | y[9] | y''[9], n points).
+// Mixed pair records (fd_common.cuh, 144 bytes per two samples) of level samples [s_begin, s_end),
+// evaluated from the trajectory knots (t | y[9] | y''[9], n points); levels above ext_from are the
+// reference's extended levels (their own time spacing, fd_common.cuh level_time).
 cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
-                                 int64_t s_end, const MixedFrame& F, float4* rec, cudaStream_t st);
+                                 int64_t s_end, int ext_from, const MixedFrame& F, float4* rec, cudaStream_t st);
 constexpr int kMixedRecordBytesPerSample = 72;
 // Compiled kernel variants (see kernels_fp64.cu / kernels_mixed.cu); the engine's autotuner picks one.
 constexpr int kFp64Variants = 4;
@@ -203,8 +204,10 @@ int mixed_blocks_per_sm(int variant);
 int fp64_blocks_per_sm(bool power_density, int variant);
 int fp64_entries_per_cta(int variant);
 
+// FP64 level samples [s_begin, s_end) (10 SoA arrays of stride cap) and their per-level beta-difference
+// maxima; levels above ext_from are the reference's extended levels.
 cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
-                              int64_t s_end, double* lev, int64_t cap, int extended_level,
+                              int64_t s_end, double* lev, int64_t cap, int ext_from,
                               unsigned long long* bdmax_bits, cudaStream_t st);
 cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int grid, int variant, cudaStream_t st);
 cudaError_t launch_fd_finalize(const FdFinalArgs& a, int64_t n_act_bound, cudaStream_t st);

@@ -29,27 +29,14 @@ namespace dev {
 // (src/TParticleTrajectoryInterpolated.cc:124-158) + TSpline1D3::GetValue (include/TOMATH.h:92-121).
 // Sample i of level L lives at index 2^L + i of each of the 10 SoA arrays (index 0 unused), so the
 // union of levels 0..L is the contiguous range [1, 2^(L+1)) and every level starts 16-byte aligned.
+// Levels above ext_from hold the reference's extended levels (same count 2^L, their own spacing:
+// level_time), which it evaluates on the fly instead of storing.
 // ---------------------------------------------------------------------------------------------
 __global__ void k_level_fill(const double* __restrict__ knots, int64_t n, double tstart, double tstop,
-                             int64_t s_begin, int64_t s_end, double* __restrict__ lev, int64_t cap,
-                             int extended_level) {
+                             int64_t s_begin, int64_t s_end, double* __restrict__ lev, int64_t cap, int ext_from) {
   const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= s_end) return;
-  int L;
-  int64_t i;
-  double ts, sp;
-  if (extended_level >= 0) {  // extended level: spacing T/(2^L - 1), stored at [0, 2^L)
-    L = extended_level;
-    i = s;
-    ts = __dadd_rn(tstart, __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L + 1)));
-    sp = __ddiv_rn(__dsub_rn(tstop, tstart), __dsub_rn(ldexp(1.0, L), 1.0));
-  } else {
-    L = 63 - __clzll((unsigned long long)s);
-    i = s - ((int64_t)1 << L);
-    ts = __dadd_rn(tstart, __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L + 1)));
-    sp = __ddiv_rn(__dsub_rn(tstop, tstart), ldexp(1.0, L));
-  }
-  const double T = __dadd_rn(ts, __dmul_rn(sp, (double)i));
+  const double T = level_time(tstart, tstop, s, ext_from);
   double v[9];
   spline_eval9(knots, n, T, v);
   lev[s] = T;
@@ -60,16 +47,14 @@ __global__ void k_level_fill(const double* __restrict__ knots, int64_t n, double
 // Per-level max |beta_i - beta_{i-1}| over i >= 1 (the power-density stop rule, src/OSCARSSR.cc:
 // 2887-2891).  Positive doubles order like their bit patterns, so atomicMax on the bits is exact.
 __global__ void k_level_betadiff(const double* __restrict__ lev, int64_t cap, int64_t s_begin, int64_t s_end,
-                                 unsigned long long* __restrict__ bdmax_bits, int extended_level) {
+                                 unsigned long long* __restrict__ bdmax_bits) {
   __shared__ unsigned long long blk[32];  // per-level maxima of this block, merged into global at the end
   if (threadIdx.x < 32) blk[threadIdx.x] = 0;
   __syncthreads();
   const int64_t s = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s < s_end) {
-    int L;
-    int64_t i;
-    if (extended_level >= 0) { L = extended_level; i = s; }
-    else { L = 63 - __clzll((unsigned long long)s); i = s - ((int64_t)1 << L); }
+    const int L = 63 - __clzll((unsigned long long)s);
+    const int64_t i = s - ((int64_t)1 << L);
     if (i > 0) {
       const double* bx = lev + 4 * cap;
       const double* by = lev + 5 * cap;
@@ -557,13 +542,13 @@ __global__ void k_pd_finalize(PdFinalArgs A) {
 
 // ---- launch wrappers ------------------------------------------------------------------------
 cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
-                              int64_t s_end, double* lev, int64_t cap, int extended_level,
+                              int64_t s_end, double* lev, int64_t cap, int ext_from,
                               unsigned long long* bdmax_bits, cudaStream_t st) {
   if (s_end <= s_begin) return cudaSuccess;
   const int T = 256;
   const int64_t nblk = (s_end - s_begin + T - 1) / T;
-  dev::k_level_fill<<<(unsigned)nblk, T, 0, st>>>(knots, n, tstart, tstop, s_begin, s_end, lev, cap, extended_level);
-  dev::k_level_betadiff<<<(unsigned)nblk, T, 0, st>>>(lev, cap, s_begin, s_end, bdmax_bits, extended_level);
+  dev::k_level_fill<<<(unsigned)nblk, T, 0, st>>>(knots, n, tstart, tstop, s_begin, s_end, lev, cap, ext_from);
+  dev::k_level_betadiff<<<(unsigned)nblk, T, 0, st>>>(lev, cap, s_begin, s_end, bdmax_bits);
   return cudaGetLastError();
 }
 

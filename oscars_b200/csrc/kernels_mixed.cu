@@ -22,18 +22,19 @@ struct PairStage {
 };
 
 // Pair records of level samples [s_begin, s_end) straight from the trajectory spline (one thread per
-// sample): the level time (src/TParticleTrajectoryInterpolated.cc:124-158), the spline values
+// sample): the level time (levels above ext_from are extended levels, see level_time), the spline values
 // (include/TOMATH.h:92-121, bit-identical to the FP64 level cache), the particle frame and the record.
 // Sample 0 is the zero-amplitude record at the position and time of sample 1.  The two samples of a
 // pair sit in adjacent lanes (s_begin and the block size are even) and exchange their FP64 values
 // for the pair's step, so every lane of the grid's last warp takes part (past s_end on a clamped
 // sample, writing nothing).
 __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, double tstart, double tstop,
-                                int64_t s_begin, int64_t s_end, MixedFrame F, float* __restrict__ rec) {
+                                int64_t s_begin, int64_t s_end, int ext_from, MixedFrame F,
+                                float* __restrict__ rec) {
   const int64_t s_raw = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s_raw < s_end;
   const int64_t s = active ? s_raw : s_end - 2 + (s_raw & 1);
-  const double t = level_time(tstart, tstop, s == 0 ? 1 : s);
+  const double t = level_time(tstart, tstop, s == 0 ? 1 : s, ext_from);
   double v[9];
   spline_eval9(knots, n, t, v);
   const double dx = v[0] - F.x0[0], dy = v[1] - F.x0[1], dz = v[2] - F.x0[2];
@@ -219,11 +220,12 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveA
 }  // namespace dev
 
 cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
-                                 int64_t s_end, const MixedFrame& F, float4* rec, cudaStream_t st) {
+                                 int64_t s_end, int ext_from, const MixedFrame& F, float4* rec, cudaStream_t st) {
   if (s_end <= s_begin) return cudaSuccess;
   const int T = 128;
   const unsigned grid = (unsigned)((s_end - s_begin + T - 1) / T);
-  dev::k_mixed_records<<<grid, T, 0, st>>>(knots, n, tstart, tstop, s_begin, s_end, F, reinterpret_cast<float*>(rec));
+  dev::k_mixed_records<<<grid, T, 0, st>>>(knots, n, tstart, tstop, s_begin, s_end, ext_from, F,
+                                            reinterpret_cast<float*>(rec));
   return cudaGetLastError();
 }
 

@@ -218,7 +218,7 @@ extern "C" OSC_API int osc_flux_fixed_level_noalloc(int device, const double* tr
     k_spline_second_derivatives<<<1, 32, 0, st>>>(knots, u, n);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = launch_level_fill(knots, n, tstart, tstop, 1, cap, lev, cap, -1, bd, st);
+  if (e == cudaSuccess) e = launch_level_fill(knots, n, tstart, tstop, 1, cap, lev, cap, kMaxLevelMemory, bd, st);
   if (e == cudaSuccess) {
     FdWaveArgs a{};
     a.lev = lev; a.cap = cap; a.obs = obs; a.omega = omega; a.n_e = 1; a.n_items = n_obs;

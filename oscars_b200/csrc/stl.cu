@@ -20,11 +20,11 @@ void Engine::power_density_stl(const double* tri, const double* centers, int64_t
   cudaStream_t st = stream;
   pending_.clear();
   last_samples = last_launches = last_not_converged = 0;
-  const int lstop_mem = o.max_level >= -1 && o.max_level <= kMaxLevelMemory ? o.max_level : kMaxLevelMemory;
-  const int lstop = o.max_level_extended > lstop_mem ? o.max_level_extended : lstop_mem;
-  if (lstop > kMaxLevelMemory)
-    throw Error{OSC_ERR_RANGE, "max_level_extended above 26 is not supported by this GPU build"};
+  // one CTA per facet walks a whole level, so the levels stop at 26 here
+  int ext_from = kMaxLevelMemory;
+  const int lstop = request_levels(o, kMaxLevelMemory, &ext_from);
   if (n <= 0) return;
+  set_level_grid(ext_from);
   for (int64_t i = 0; i < n; ++i) out[i] = 0;
   // facet geometry as RayIntersectionDistance forms it: A, B - A, C - A (src/TTriangle3D.cc)
   std::vector<double> geo(9 * n), nrm(3 * n);

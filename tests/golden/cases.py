@@ -32,6 +32,11 @@ UND_SETUP = [UND, BEAM] + traj()
 UND_SHORT = ("add_bfield_undulator", dict(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=11, phase=-math.pi / 2))
 UND_SHORT_SETUP = [UND_SHORT, BEAM] + traj(5001, -0.5, 0.5)
 STL_PD = ("calculate_power_density_stl", dict(farfield_origin=[0, 0, 0], max_level=12))
+# Levels past the reference's memory limit of 26: memory levels 0..12, extended levels 13..27 (2^28
+# samples per entry; precision 0 never converges, so every entry runs to 27).  Its fixture
+# (deep_levels.npz) takes the reference a few minutes and is not replayed on the oracle.
+DEEP_LEVELS = UND_SHORT_SETUP + [("calculate_spectrum", dict(obs=[0, 0, 20], energy_points_eV=[458.9458, 1600.0], precision=0,
+                                                             max_level=12, max_level_extended=27))]
 EPU_SETUP = [EPU_Y, EPU_X, BEAM] + traj(16001)
 
 
@@ -204,6 +209,11 @@ CASES = {
     "flux_und_lowlevel": UND_SETUP + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[7, 7], width=[0.01, 0.01], translation=[0, 0, 30], max_level=6))],
     "flux_und_level": UND_SETUP + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[21, 21], width=[0.01, 0.01], translation=[0, 0, 30], quantity="level"))],
     "flux_und_dim3_yz": UND_SETUP + [("calculate_flux_rectangle", dict(energy_eV=3 * E1_U, npoints=[9, 13], plane="XZ", width=[0.004, 0.006], rotations=[0, 0, 0.1], translation=[0, 0.0005, 30], dim=3, polarization="lv"))],
+    # extended levels: above max_level the reference evaluates each level on the fly on its own time
+    # grid (spacing T / (2^L - 1), not nested with the lower levels), up to max_level_extended
+    "flux_und_extended": UND_SETUP + [("calculate_flux_rectangle", dict(energy_eV=E1_U, npoints=[7, 7], width=[0.01, 0.01], translation=[0, 0, 30], precision=0.001, max_level=9, max_level_extended=13))],
+    "spec_und_extended": UND_SETUP + [("calculate_spectrum", dict(obs=[0.0005, 0, 30], energy_range_eV=[400, 500], npoints=20, precision=0.01, max_level=9, max_level_extended=13))],
+    "pd_und_extended": UND_SETUP + [("calculate_power_density_rectangle", dict(npoints=[7, 7], width=[0.01, 0.01], translation=[0, 0, 30], precision=0.001, max_level=9, max_level_extended=12))],
     # power density on the same rectangles
     "pd_und_41": UND_SETUP + [("calculate_power_density_rectangle", dict(npoints=[41, 41], width=[0.01, 0.01], translation=[0, 0, 30]))],
     "pd_und_directional": UND_SETUP + [("calculate_power_density_rectangle", dict(npoints=[11, 11], width=[0.02, 0.02], translation=[0, 0, 30], normal=1))],
@@ -309,6 +319,22 @@ CASES = {
                 [("add_stl", dict(ifile="plate.stl", translation=[0, 0, 20])),
                  ("calculate_power_density_stl", dict(farfield_origin=[0, 0, 0], max_level=12, nparticles=3))],
 }
+
+
+def carried_levels(levels):
+    """Stop levels as the reference's single-thread point loop reports them with quantity='level':
+    Result_Level is declared outside the loop (src/OSCARSSR.cc:4160), so an entry that did not
+    converge (-1 here) repeats the level of the last entry before it that did (-1 before any).  The
+    golden fixtures come from nthreads=1 runs; this library reports -1 for every such entry."""
+    import numpy as np
+    out = np.array(levels, dtype=np.float64)
+    carry = -1.0
+    for i in range(out.size):
+        if out.flat[i] == -1:
+            out.flat[i] = carry
+        else:
+            carry = out.flat[i]
+    return out
 
 
 def run_case(obj, calls):

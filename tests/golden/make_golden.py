@@ -10,6 +10,7 @@ per-entry stop levels from a second ``quantity='level'`` call where the case ret
     python tests/golden/make_golden.py files      # the reference's output files (files.npz)
     python tests/golden/make_golden.py adjoint_fd # finite-difference gradients (adjoint_fd.npz)
     python tests/golden/make_golden.py stl_files  # the mesh file of stlofile (stl_files.npz)
+    python tests/golden/make_golden.py deep_levels  # extended levels up to 27 (deep_levels.npz)
 """
 import os
 import subprocess
@@ -117,6 +118,13 @@ def make_stl_file(S):
                         body=np.frombuffer(data[80:], dtype=np.uint8))
 
 
+def make_deep_levels(S):
+    """The spectrum of cases.DEEP_LEVELS (extended levels up to 27) -> deep_levels.npz."""
+    from cases import DEEP_LEVELS
+    pos, val = flatten(run_case(S.sr(nthreads=1, gpu=0), DEEP_LEVELS))
+    np.savez_compressed(os.path.join(HERE, "deep_levels.npz"), pos=pos, val=val)
+
+
 def make_adjoint(S):
     """Central finite differences of loss = sum (F(s) - F(1))^2 over the adjoint configuration, every
     one of the 82 half-period factors, with the reference's CPU path (the scaled undulator given to it
@@ -165,6 +173,10 @@ def main(argv):
     if argv[1:] == ["files"]:
         make_files(S)
         print("wrote files")
+        return
+    if argv[1:] == ["deep_levels"]:
+        make_deep_levels(S)
+        print("wrote deep_levels")
         return
     if argv[1:] == ["stl_files"]:
         make_stl_file(S)
