@@ -484,7 +484,8 @@ def product_arm(args):
                 "beam_value": bb["value"], "beam_fp64_value": bb["fp64"]["value"],
                 "beam_mixed_over_fp64": bb["mixed_over_fp64"], "uneven_value": bu["value"],
                 "uneven_fp64_value": bu["fp64"]["value"], "uneven_mixed_over_fp64": bu["mixed_over_fp64"],
-                "tuning_grad_per_s": bt["value"],
+                "tuning_grad_per_s": bt["value"], "tuning_fp64_grad_per_s": bt["fp64"]["value"],
+                "tuning_grad_vs_fd": bt["grad_vs_richardson_fd"]["value"],
                 "beam_cpu_reference_value": (bb["cpu_reference"] or {}).get("value"),
                 "uneven_cpu_reference_value": (bu["cpu_reference"] or {}).get("value"),
                 "tuning_cpu_reference_grad_per_s": (bt["cpu_reference"] or {}).get("value")})
@@ -827,38 +828,49 @@ def sharded_beam_leg(steps, warmup, local, rank, world):
 # ---------------------------------------------------------------------------------------------
 TUNING_WORKLOAD = ("41-period undulator B0=0.5T lambda=50mm with 82 half-period factors 1+delta, delta~N(0,0.005) "
                    "(seed 82); 3 GeV; 20001-point RK4; loss=sum (F-F_ideal)^2 over 21x21 observers (2mm x 2mm at "
-                   "z=30m) x 256 energies over E1 +-5%; fixed level 12; FP64 forward and adjoint")
+                   "z=30m) x 256 energies over E1 +-5%; fixed level 12; radiation sums and their adjoint in mixed "
+                   "precision (FP64 phase, FP32 amplitudes and reverse sweep), RK4 adjoint in FP64 from checkpoints "
+                   "every 256 steps")
 
 
 def tuning_leg(steps, warmup, local=0, check_params=(3, 20, 41, 70)):
-    """One step = the forward flux and its adjoint gradient (osc_flux_multi + osc_flux_vjp); grad/s
-    with Richardson central differences (h = 1e-3, 3e-3) on a few factors as a check."""
+    """One step = the forward flux and its adjoint gradient (osc_flux_vjp forward pass, then the
+    backward pass reusing its sums); grad/s with compute='mixed' (the value) and 'fp64'; Richardson
+    central differences (h = 1e-3, 3e-3) on a few factors as a check of the mixed gradient."""
     import numpy as np
     from oscars_b200.tuning import TuningProblem
     xs = np.linspace(-0.001, 0.001, 21)
     X, Y = np.meshgrid(xs, xs, indexing="ij")
     obs = np.stack([X.ravel(), Y.ravel(), np.full(X.size, 30.0)], 1)
     energies = np.linspace(0.95 * E1, 1.05 * E1, 256)
-    p = TuningProblem(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, obs=obs, energies_eV=energies,
-                      level=12, gpu=local)
     s = 1 + np.random.default_rng(82).normal(0.0, 0.005, 82)
-    F_ideal = p.flux(np.ones(82))
 
-    def step():
-        F = p.flux(s)
-        return p.vjp(s, 2 * (F - F_ideal))[1]
-    for _ in range(warmup):
-        step()
-    t_fwd = t_all = 0.0
-    with ClockSampler(local) as clk:
-        for _ in range(steps):
-            t0 = time.perf_counter()
-            F = p.flux(s)
-            t1 = time.perf_counter()
-            g = p.vjp(s, 2 * (F - F_ideal))[1]
-            t2 = time.perf_counter()
-            t_fwd += t1 - t0
-            t_all += t2 - t0
+    def run(compute):
+        p = TuningProblem(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, obs=obs, energies_eV=energies,
+                          level=12, gpu=local, compute=compute)
+        F_ideal = p.flux(np.ones(82))
+        for _ in range(warmup):
+            p.vjp(s, 2 * (p.flux(s) - F_ideal))
+            p.flux(np.ones(82))  # new factors: the next step recomputes the trajectory and the sums
+        t_fwd = t_all = 0.0
+        g = None
+        with ClockSampler(local) as clk:
+            for k in range(steps):
+                sk = s if k % 2 == 0 else s * (1 + 1e-12)  # alternate factors: nothing carries over a step
+                t0 = time.perf_counter()
+                F = p.flux(sk)
+                t1 = time.perf_counter()
+                gk = p.vjp(sk, 2 * (F - F_ideal))[1]
+                t2 = time.perf_counter()
+                if k % 2 == 0:
+                    g = gk
+                t_fwd += t1 - t0
+                t_all += t2 - t0
+        return p, F_ideal, g, {"value": steps / t_all, "unit": "grad/s", "ms_per_step": 1e3 * t_all / steps,
+                               "forward_ms": 1e3 * t_fwd / steps, "adjoint_ms": 1e3 * (t_all - t_fwd) / steps,
+                               "clocks": clk.summary()}
+    p, F_ideal, g, mx = run("mixed")
+    _, _, g64, f64 = run("fp64")
     loss = lambda v: float(np.sum((p.flux(v) - F_ideal) ** 2))
 
     def central(k, h):
@@ -873,12 +885,15 @@ def tuning_leg(steps, warmup, local=0, check_params=(3, 20, 41, 70)):
         "sample": "one central-difference component on 16 of the 256 energies, %.1f s; the full gradient by "
                   "central differences is %d such subsets (82 components x 16), so %.0f s per gradient (derived)"
                   % (tr[0], tr[1], tr[0] * tr[1])}
-    return {"workload": TUNING_WORKLOAD, "steps": steps, "warmup": warmup, "value": steps / t_all,
-            "unit": "grad/s", "ms_per_step": 1e3 * t_all / steps, "forward_ms": 1e3 * t_fwd / steps,
-            "adjoint_ms": 1e3 * (t_all - t_fwd) / steps,
-            "grad_vs_richardson_fd": {"value": err, "params": list(check_params), "steps": [1e-3, 3e-3]},
-            "path": "oscars_b200.tuning.TuningProblem.flux + vjp (osc_flux_multi, osc_flux_vjp); wall clock, "
-                    "host buffers", "cpu_reference": cpu, "clocks": clk.summary()}
+    out = {"workload": TUNING_WORKLOAD, "steps": steps, "warmup": warmup}
+    out.update(mx)
+    out.update({"grad_vs_richardson_fd": {"value": err, "params": list(check_params), "steps": [1e-3, 3e-3]},
+                "mixed_vs_fp64_grad_rel": float(np.max(np.abs(g - g64)) / np.max(np.abs(g64))),
+                "fp64": f64,
+                "path": "oscars_b200.tuning.TuningProblem(compute='mixed').flux + vjp (osc_flux_vjp forward, then "
+                        "backward on the kept sums); wall clock, host buffers; a new trajectory every step",
+                "cpu_reference": cpu})
+    return out
 
 
 def _free_port():

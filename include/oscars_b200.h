@@ -325,13 +325,20 @@ OSC_API int osc_batch_trajectories(osc_ctx* ctx, const osc_field_desc* fields, i
 
 /* ---- differentiation (no reference counterpart: the reference has no gradients) ------------
  * osc_set_half_period_scale replaces the half-period amplitude factors of field `field_index`
- * (an undulator added with them; -1 = the one field that has them) and drops the trajectory.
+ * (an undulator added with them; -1 = the one field that has them) and drops the trajectory (the
+ * same factors again leave it in place).
  * osc_flux_vjp computes, at the fixed level `level` (all samples of levels 0..level, no stop rule),
  * the flux F of every (observer, energy) entry -- the value osc_flux / osc_spectrum return with
  * precision 0 and max_level = level -- and grad_half_scale = (dF/ds)^T grad_flux, the gradient of any
  * loss with dLoss/dF = grad_flux with respect to those factors, by reverse mode through the
- * radiation sum, the trajectory spline and the RK4 steps (FP64; the RK4 part runs parallel in time
- * over 64-step segments joined by their 6 x 6 Jacobians).
+ * radiation sum, the trajectory spline and the RK4 steps.  opts->precision_mode selects the
+ * arithmetic of the radiation part: OSC_FP64, or OSC_MIXED (the mixed path's sums and an FP32
+ * reverse sweep with the FP64 phase of each pair of samples); the RK4 part is FP64 either way and
+ * recomputes the trajectory states from checkpoints every 256 steps, its reverse pass parallel in
+ * time over 64-step segments joined by their 6 x 6 Jacobians.
+ * grad_flux may be NULL: the call then computes flux_out only and keeps the entry sums, which a
+ * following call on the same trajectory, observers, energies, level and arithmetic reuses (a
+ * forward pass followed by its backward pass computes the sums once).
  * Entries are observer-major with energies fastest; spectrum = 1 normalises like osc_spectrum.
  * grad_knots (may be NULL) receives the gradient with respect to the trajectory knots (9 x n_points,
  * the layout of osc_trajectory_vjp's knot_grad).

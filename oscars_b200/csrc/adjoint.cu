@@ -1,21 +1,26 @@
 // adjoint.cu -- gradient of a fixed-level flux with respect to the per-half-period amplitude factors
-// of an undulator (reverse mode, FP64).
+// of an undulator (reverse mode; the radiation part in FP64 or mixed precision, the trajectory part
+// in FP64).
 //
 // Forward (what is differentiated): the RK4 trajectory through the fields (src/OSCARSSR.cc:910-1009),
 // its clamped spline (include/TOMATH.h:141-203), the level samples s = 1 .. 2^(L+1)-1 of the fixed
 // level L (src/TParticleTrajectoryInterpolated.cc:124-158), and per (observer, energy) entry the
 // complex sum S = sum_s A_s exp(-i w (t_s + D_s/c)), F = C2 |C0 dT_L S|^2 (src/OSCARSSR.cc:4179-4268).
 // Given dLoss/dF per entry, the reverse sweep is:
-//   k_adj_weights      W = 2 C2 (C0 dT)^2 dLoss/dF conj(S) per entry (and F itself)
-//   k_adj_samples      per level sample, sum over entries of d Re(W . A e^{i phi}) / d(X, beta, a/c);
-//                      one thread per sample, entries staged through shared memory
-//   k_adj_spline_eval  sample -> knot values and second derivatives (transpose of the evaluation)
-//   k_adj_spline_solve second derivatives -> knot values (transpose of the tridiagonal sweeps)
-//   k_adj_rk4_segments knots -> RK4 states -> field amplitudes, parallel in time: every 64-step
-//                      segment of both integration chains runs its reverse pass at once (states read
-//                      back from the knots, each step's stages recomputed and differentiated), once
-//                      with the knot adjoints and once per unit adjoint entering it;
-//   k_adj_rk4_combine  a sequential sweep of the 6 x 6 segment Jacobians joins the segments.
+//   k_adj_sums          S and F per entry from the forward wave's partials (kept for the next call)
+//   k_adj_weights       W = 2 C2 (C0 dT)^2 dLoss/dF conj(S) per entry
+//   k_adj_samples       per level sample, sum over entries of d Re(W . A e^{i phi}) / d(X, beta, a/c);
+//                       one thread per sample, entries staged through shared memory (FP64)
+//   k_adj_samples_mixed the same over the mixed pair records, one thread per pair of samples (FP32
+//                       with the FP64 phase of each pair)
+//   k_adj_spline_eval   sample -> knot values and second derivatives (transpose of the evaluation)
+//   k_adj_spline_solve  second derivatives -> knot values (transpose of the tridiagonal sweeps)
+//   k_adj_rk4_recompute trajectory states recomputed from checkpoints every 256 steps
+//   k_adj_rk4_segments  knots -> RK4 states -> field amplitudes, parallel in time: every 64-step
+//                       segment of both integration chains runs its reverse pass at once (each
+//                       step's stages recomputed and differentiated), once with the knot adjoints and
+//                       once per unit adjoint entering it;
+//   k_adj_rk4_combine   a sequential sweep of the 6 x 6 segment Jacobians joins the segments.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -31,22 +36,44 @@
 namespace osc {
 namespace dev {
 
-// ---- 1. entry weights ----------------------------------------------------------------------
-// part: first-wave partials of level L with one span ([entry][segment][kFdPartials]).
-__global__ void k_adj_weights(const double* __restrict__ part, int64_t n, const double* __restrict__ grad_flux,
-                              double c0dt, double c2, double* __restrict__ W, double* __restrict__ flux) {
+// ---- 1. entry sums and weights ------------------------------------------------------------
+// part: partials of a one-span first wave at level L (two segments: levels 0..L-1 and level L),
+// entry-major [entry][segment][kFdPartials] (the FP64 wave, unfused) when tile_entries == 0, else
+// tile-major [tile][segment][kFdPartials][entry in tile] (the mixed wave).  S: the 6 sums of every
+// entry; flux: F = C2 |C0 dT S|^2.
+__global__ void k_adj_sums(const double* __restrict__ part, int64_t n, int tile_entries, double c0dt, double c2,
+                           double* __restrict__ S, double* __restrict__ flux) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
-  double S[6];
-  for (int k = 0; k < 6; ++k) S[k] = part[e * 2 * kFdPartials + k] + part[e * 2 * kFdPartials + kFdPartials + k];
+  const int te = tile_entries;
+  const double* p0 = te == 0 ? part + e * 2 * kFdPartials : part + (e / te) * 2 * kFdPartials * te + e % te;
+  const int64_t seg = te == 0 ? kFdPartials : (int64_t)kFdPartials * te;  // segment 1 relative to segment 0
+  const int64_t cs = te == 0 ? 1 : te;                                    // stride between components
   double m = 0;
-  for (int k = 0; k < 6; ++k) m += (c0dt * S[k]) * (c0dt * S[k]);
-  flux[e] = c2 * m;
-  const double w = 2.0 * c2 * c0dt * c0dt * grad_flux[e];
-  for (int k = 0; k < 3; ++k) {
-    W[6 * e + 2 * k] = w * S[2 * k];           // Re conj(S)
-    W[6 * e + 2 * k + 1] = -w * S[2 * k + 1];  // Im conj(S)
+  for (int k = 0; k < 6; ++k) {
+    const double v = p0[k * cs] + p0[seg + k * cs];
+    S[6 * e + k] = v;
+    m += (c0dt * v) * (c0dt * v);
   }
+  flux[e] = c2 * m;
+}
+
+// W = 2 C2 (C0 dT)^2 dLoss/dF conj(S) per entry, and the largest |W| component (bits of a positive
+// double, folded with atomicMax) for the mixed samples kernel's scaling.
+__global__ void k_adj_weights(const double* __restrict__ S, int64_t n, const double* __restrict__ grad_flux,
+                              double c0dt, double c2, double* __restrict__ W,
+                              unsigned long long* __restrict__ wmax_bits) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const double w = 2.0 * c2 * c0dt * c0dt * grad_flux[e];
+  double mx = 0;
+  for (int k = 0; k < 3; ++k) {
+    const double re = w * S[6 * e + 2 * k], im = -w * S[6 * e + 2 * k + 1];  // conj(S)
+    W[6 * e + 2 * k] = re;
+    W[6 * e + 2 * k + 1] = im;
+    mx = fmax(mx, fmax(fabs(re), fabs(im)));
+  }
+  if (mx > 0) atomicMax(wmax_bits, (unsigned long long)__double_as_longlong(mx));
 }
 
 // ---- 2. per-sample gradients --------------------------------------------------------------
@@ -142,6 +169,160 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_samples(const double* __res
   }
   if (live)
     for (int c = 0; c < 9; ++c) atomicAdd(&gs[c * cap + s], acc[c]);
+}
+
+// ---- 2b. per-sample gradients, mixed precision -----------------------------------------------
+// The same reverse sweep over the mixed pair records of levels 0..L (fd_common.cuh), one thread per
+// pair of samples, in the particle frame: the phase of the pair's first sample in FP64 (fp64_turns),
+// the second's as the FP32 step from it, amplitudes, sincos and the reverse sweep in FP32, the
+// entries' contributions summed in FP32 over a staged chunk and folded into FP64 sums in shared
+// memory.  The phase constant the frame drops (w (t_ref + O_z / c) and the half turn of fp64_turns,
+// also absent from the mixed wave's sums S) cancels in Re(W A e^{i phi}) with W from conj(S).  W is
+// scaled by 1 / max|W| into FP32 range and the sums by max|W| back; the gradients are rotated back
+// to the lab frame (g = R^T g').
+constexpr int kAdjMxThreads = 128;
+constexpr int kAdjMxStage = 64;
+
+struct AdjEntryMx {
+  PairObs o;
+  float wr[3], wi[3];
+};
+
+// Reverse sweep of one sample: geometry (rx, ry, iD = 1/D, en = 1 - n_z), the record's beta
+// components (-bx, -by, 1 - bz, bz, 1 - b^2) and a/c, and c = cos(2 pi t), sn = sin(2 pi t) of its
+// phase in turns (phi = -2 pi t).  acc: dJ/dX (3), dJ/dbeta (3), dJ/d(a/c) (3).
+__device__ __forceinline__ void adj_sample_mx(float rx, float ry, float iD, float en, float mbx, float mby, float eb,
+                                              float bz, float g, float ax, float ay, float az, float c, float sn,
+                                              const float* wr, const float* wi, float wc, float* acc) {
+  const float nx = rx * iD, ny = ry * iD, nz = 1.f - en;
+  const float ux = nx + mbx, uy = ny + mby, uz = eb - en;
+  const float om = fmaf(ny, mby, fmaf(nx, mbx, fmaf(en, bz, eb)));  // 1 - n.b without cancellation
+  const float iom = rcp_ftz(om);
+  const float na = fmaf(nx, ax, fmaf(ny, ay, nz * az));
+  const float k2 = iD * iom;
+  const float h = fmaf(g, iD, na);
+  const float k1 = k2 * iom * h;
+  const float Ax = fmaf(ux, k1, -ax * k2), Ay = fmaf(uy, k1, -ay * k2), Az = fmaf(uz, k1, -az * k2);
+  // W e^{i phi} = (Wr + i Wi)(c - i sn): P its real part, Q its imaginary part
+  const float Px = fmaf(wr[0], c, wi[0] * sn), Py = fmaf(wr[1], c, wi[1] * sn), Pz = fmaf(wr[2], c, wi[2] * sn);
+  const float Qx = fmaf(wi[0], c, -wr[0] * sn), Qy = fmaf(wi[1], c, -wr[1] * sn), Qz = fmaf(wi[2], c, -wr[2] * sn);
+  // reverse sweep (the FP64 kernel's, in FP32)
+  const float phb = -fmaf(Qx, Ax, fmaf(Qy, Ay, Qz * Az));
+  float Db = -wc * phb;
+  const float ubx = Px * k1, uby = Py * k1, ubz = Pz * k1;
+  const float k1b = fmaf(Px, ux, fmaf(Py, uy, Pz * uz));
+  float abx = -Px * k2, aby = -Py * k2, abz = -Pz * k2;
+  const float k2b = fmaf(k1b * iom, h, -fmaf(Px, ax, fmaf(Py, ay, Pz * az)));
+  const float hb = k1b * k2 * iom;
+  const float gb = hb * iD;
+  const float iDb = fmaf(hb, g, k2b * iom);
+  const float iomb = fmaf(k1b * k2, h, k2b * iD);
+  const float omb = -iomb * iom * iom;
+  Db = fmaf(-iDb * iD, iD, Db);
+  const float bx = -mbx, by = -mby;
+  const float bbx = -2.f * gb * bx - omb * nx - ubx;
+  const float bby = -2.f * gb * by - omb * ny - uby;
+  const float bbz = -2.f * gb * bz - omb * nz - ubz;
+  const float nbx = hb * ax - omb * bx + ubx;
+  const float nby = hb * ay - omb * by + uby;
+  const float nbz = hb * az - omb * bz + ubz;
+  abx = fmaf(hb, nx, abx);
+  aby = fmaf(hb, ny, aby);
+  abz = fmaf(hb, nz, abz);
+  const float nbn = fmaf(nbx, nx, fmaf(nby, ny, nbz * nz));
+  Db = fmaf(-nbn, iD, Db);
+  acc[0] -= fmaf(nbx, iD, Db * nx);
+  acc[1] -= fmaf(nby, iD, Db * ny);
+  acc[2] -= fmaf(nbz, iD, Db * nz);
+  acc[3] += bbx;
+  acc[4] += bby;
+  acc[5] += bbz;
+  acc[6] += abx;
+  acc[7] += aby;
+  acc[8] += abz;
+}
+
+__global__ void __launch_bounds__(kAdjMxThreads, 3)
+    k_adj_samples_mixed(const float4* __restrict__ rec, int64_t n_pairs, MixedFrame F, const double* __restrict__ obs,
+                        const double* __restrict__ omega, int64_t n_e, const double* __restrict__ W,
+                        const unsigned long long* __restrict__ wmax_bits, int64_t n_entries, int64_t entries_per_cta,
+                        double* __restrict__ gs, int64_t gcap) {
+  __shared__ AdjEntryMx se[kAdjMxStage];
+  __shared__ double sacc[18][kAdjMxThreads];
+  const int tid = threadIdx.x;
+  const int64_t p = (int64_t)blockIdx.x * kAdjMxThreads + tid;
+  const bool live = p < n_pairs;
+  const float4* q = rec + kPairF4 * (live ? p : 0);
+  const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
+  const double2* dq = reinterpret_cast<const double2*>(q + 7);
+  const double2 DXY = dq[0], DZT = dq[1];
+  const double wmax = __longlong_as_double((long long)*wmax_bits);
+  const double wscale = wmax > 0 ? 1.0 / wmax : 0.0;
+#pragma unroll
+  for (int k = 0; k < 18; ++k) sacc[k][tid] = 0.0;
+  const int64_t e0 = (int64_t)blockIdx.y * entries_per_cta;
+  const int64_t e1 = min(n_entries, e0 + entries_per_cta);
+  for (int64_t base = e0; base < e1; base += kAdjMxStage) {
+    const int64_t e = base + tid;
+    if (tid < kAdjMxStage && e < e1) {
+      const int64_t io = e / n_e, ie = e % n_e;
+      const double* R = F.rot;
+      const double ox = obs[3 * io] - F.x0[0], oy = obs[3 * io + 1] - F.x0[1], oz = obs[3 * io + 2] - F.x0[2];
+      AdjEntryMx& E = se[tid];
+      E.o = make_pair_obs(R[0] * ox + R[1] * oy + R[2] * oz, R[3] * ox + R[4] * oy + R[5] * oz,
+                          R[6] * ox + R[7] * oy + R[8] * oz, omega[ie]);
+      for (int k = 0; k < 3; ++k) {
+        E.wr[k] = (float)(W[6 * e + 2 * k] * wscale);
+        E.wi[k] = (float)(W[6 * e + 2 * k + 1] * wscale);
+      }
+    }
+    __syncthreads();
+    const int cnt = (int)min((int64_t)kAdjMxStage, e1 - base);
+    if (live) {
+      float acc[18];
+#pragma unroll
+      for (int k = 0; k < 18; ++k) acc[k] = 0.f;
+      for (int j = 0; j < cnt; ++j) {
+        const PairObs& o = se[j].o;
+        // geometry of both samples (pair_sample)
+        const float rx0 = o.ox.x - q0.x, rx1 = o.ox.x - q0.y, ry0 = o.oy.x - q0.z, ry1 = o.oy.x - q0.w;
+        const float rz0 = o.oz.x - q1.x, rz1 = o.oz.x - q1.y;
+        const float r20 = fmaf(rx0, rx0, ry0 * ry0), r21 = fmaf(rx1, rx1, ry1 * ry1);
+        const float d20 = fmaf(rz0, rz0, r20), d21 = fmaf(rz1, rz1, r21);
+        const float iD0 = rsqrt_ftz(d20), iD1 = rsqrt_ftz(d21);
+        const float ri0 = r20 * iD0, ri1 = r21 * iD1;
+        const float c0 = ri0 * fmaf(0.125f, ri0 * iD0, 0.5f), c1 = ri1 * fmaf(0.125f, ri1 * iD1, 0.5f);
+        // phases in turns: the first in FP64, the second as the FP32 step from it
+        const float t0 = fp64_turns(DXY.x, DXY.y, DZT.x, DZT.y, c0, 0.5f * iD0, o);
+        const float inv = rcp_ftz(d20 * iD0 + d21 * iD1);
+        const float num = fmaf(q6.x, rx0 + rx1, fmaf(q6.y, ry0 + ry1, -q6.z * (c0 + c1)));
+        const float t1 = t0 + fmaf(o.wct, num * inv, o.wt * q6.w);
+        float sn0, cs0, sn1, cs1;
+        sincos_ftz(t0 * kTwoPiF, &sn0, &cs0);
+        sincos_ftz(t1 * kTwoPiF, &sn1, &cs1);
+        const float* wr = se[j].wr;
+        const float* wi = se[j].wi;
+        adj_sample_mx(rx0, ry0, iD0, c0 * iD0, q2.x, q2.z, q3.x, q3.z, q4.x, q5.x, q5.z, q4.z, cs0, sn0, wr, wi, o.wc.x,
+                      acc);
+        adj_sample_mx(rx1, ry1, iD1, c1 * iD1, q2.y, q2.w, q3.y, q3.w, q4.y, q5.y, q5.w, q4.w, cs1, sn1, wr, wi, o.wc.x,
+                      acc + 9);
+      }
+#pragma unroll
+      for (int k = 0; k < 18; ++k) sacc[k][tid] += (double)acc[k];
+    }
+    __syncthreads();
+  }
+  if (!live) return;
+  const double* R = F.rot;
+  for (int b = 0; b < 2; ++b) {
+    const int64_t smp = 2 * p + b;
+    if (smp == 0) continue;  // the unused slot of the level ladder
+    for (int v = 0; v < 3; ++v) {  // X, beta, a/c: g = R^T g'
+      const double gx = sacc[9 * b + 3 * v][tid], gy = sacc[9 * b + 3 * v + 1][tid], gz = sacc[9 * b + 3 * v + 2][tid];
+      for (int r = 0; r < 3; ++r)
+        atomicAdd(&gs[(3 * v + r) * gcap + smp], wmax * (R[r] * gx + R[3 + r] * gy + R[6 + r] * gz));
+    }
+  }
 }
 
 // ---- 3. sample -> knots ---------------------------------------------------------------------
@@ -383,14 +564,18 @@ __device__ void rk4_vjp(const AdjFields& F, const double* y, double t, double h,
 
 // The two integration chains: z_0 = initial state; the forward chain has z_i at t0 + i dt at knot
 // nb + i (i = 0 .. nf-1, knot nb + i + 1 holds f(t_i, z_i), knot nb also f(t_0, z_0)); the backward
-// chain has z_i at t0 - i dt at knot nb - i (i = 0 .. nb; knot nb - 1 - i holds f(t_i, z_i)).  States
-// are read back from the knots.  Each chain is cut into segments (s0, s1] of kSegSteps steps.
+// chain has z_i at t0 - i dt at knot nb - i (i = 0 .. nb; knot nb - 1 - i holds f(t_i, z_i)).  The
+// states are read from the knots only at checkpoints, every kCheckpointSteps-th step of a chain, and
+// recomputed between them (k_adj_rk4_recompute).  Each chain's reverse pass is cut into segments
+// (s0, s1] of kSegSteps steps.
 constexpr int kSegSteps = 64;
+constexpr int kCheckpointSteps = 256;
 
 struct AdjSegs {
   double t0, dt;
   int nf, nb;
   const double* knots;  // t | y[9] | ... (n each)
+  const double* zs;     // recomputed states: forward chain 0..nf-1, then backward chain 0..nb (6 each)
   const double* kb;     // knot adjoints, 9 x n
   int64_t nseg[2];      // segments of the forward and backward chains
   int64_t base[2];      // index of each chain's first segment
@@ -410,6 +595,33 @@ __device__ __forceinline__ void chain_state(const AdjSegs& S, int dir, int64_t i
   z[3] = y[4 * n + j] * kCLight;
   z[4] = y[2 * n + j];
   z[5] = y[5 * n + j] * kCLight;
+}
+
+// State i of chain dir from the recomputed states.
+__device__ __forceinline__ void seg_state(const AdjSegs& S, int dir, int64_t i, double* z) {
+  const double* p = S.zs + 6 * ((dir == 0 ? 0 : (int64_t)S.nf) + i);
+  for (int k = 0; k < 6; ++k) z[k] = p[k];
+}
+
+// Checkpoint interval c of a chain: its first state from the knots (chain_state), the next
+// kCheckpointSteps - 1 recomputed by RK4 steps (rk4_step, the stages of src/OSCARSSR.cc:1247-1386)
+// into zs.  One thread per interval; nck0 intervals of the forward chain, then those of the backward.
+__global__ void k_adj_rk4_recompute(AdjFields F, AdjSegs S, double* __restrict__ zs, int64_t nck0, int64_t nck1) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nck0 + nck1) return;
+  const int dir = g < nck0 ? 0 : 1;
+  const int64_t c = dir == 0 ? g : g - nck0;
+  const int64_t M = dir == 0 ? (int64_t)S.nf - 1 : (int64_t)S.nb;  // last state of the chain
+  const int64_t i0 = c * kCheckpointSteps, i1 = min(M, i0 + kCheckpointSteps - 1);
+  const double h = dir == 0 ? S.dt : -S.dt;
+  double* out = zs + 6 * ((dir == 0 ? 0 : (int64_t)S.nf) + i0);
+  double z[6];
+  chain_state(S, dir, i0, z);
+  for (int k = 0; k < 6; ++k) out[k] = z[k];
+  for (int64_t i = i0 + 1; i <= i1; ++i) {
+    rk4_step(F, z, S.t0 + h * (double)(i - 1), h);
+    for (int k = 0; k < 6; ++k) out[6 * (i - i0) + k] = z[k];
+  }
 }
 
 // Knot state / acceleration adjoints in the RK4 state layout.
@@ -443,7 +655,7 @@ __global__ void __launch_bounds__(32) k_adj_rk4_segments(AdjFields F, AdjSegs S)
   if (r > 0) lam[r - 1] = 1.0;
   double zi[6], zp[6];
   for (int64_t i = s1; i >= lo; --i) {
-    chain_state(S, dir, i, zi);
+    seg_state(S, dir, i, zi);
     if (r == 0) {
       const int64_t sk = dir == 0 ? S.nb + i : (i >= 1 ? S.nb - i : -1);
       if (sk >= 0) knot_state_adj(S.kb, n, sk, lam);
@@ -460,7 +672,7 @@ __global__ void __launch_bounds__(32) k_adj_rk4_segments(AdjFields F, AdjSegs S)
       }
     }
     if (i > 0) {
-      chain_state(S, dir, i - 1, zp);
+      seg_state(S, dir, i - 1, zp);
       rk4_vjp(Fr, zp, S.t0 + h * (double)(i - 1), h, lam);
     }
   }
@@ -515,7 +727,7 @@ double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_param
   auto segs = [](int64_t M) -> int64_t { return M < 0 ? 0 : (M == 0 ? 1 : (M + dev::kSegSteps - 1) / dev::kSegSteps); };
   const int64_t ns0 = segs(nf - 1), ns1 = segs(nb), nseg = ns0 + ns1;
   const size_t field_bytes = (sizeof(DevField) * df.size() + 255) & ~(size_t)255;
-  adj_r_.reserve(field_bytes + sizeof(double) * (fvals.size() + n_params + nseg * (6 + 36 + 6 * n_params)));
+  adj_r_.reserve(field_bytes + sizeof(double) * (fvals.size() + n_params + nseg * (6 + 36 + 6 * n_params) + 6 * (n + 1)));
   char* base = adj_r_.as<char>();
   DevField* d_fields = reinterpret_cast<DevField*>(base);
   double* d_vals = reinterpret_cast<double*>(base + field_bytes);
@@ -523,6 +735,7 @@ double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_param
   double* d_lam = d_pgrad + n_params;
   double* d_jt = d_lam + 6 * nseg;
   double* d_pseg = d_jt + 36 * nseg;
+  double* d_zs = d_pseg + 6 * n_params * nseg;  // recomputed states (6 x (nf + nb + 1))
   check(cudaMemcpyAsync(d_fields, df.data(), sizeof(DevField) * df.size(), cudaMemcpyHostToDevice, st), "fields");
   check(cudaMemcpyAsync(d_vals, fvals.data(), sizeof(double) * fvals.size(), cudaMemcpyHostToDevice, st), "fields");
   check(cudaMemsetAsync(d_pgrad, 0, sizeof(double) * n_params, st), "memset");
@@ -534,6 +747,7 @@ double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_param
   S.nf = (int)nf;
   S.nb = (int)nb;
   S.knots = knots_.as<double>();
+  S.zs = d_zs;
   S.kb = d_kb;
   S.nseg[0] = ns0;
   S.nseg[1] = ns1;
@@ -544,11 +758,14 @@ double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_param
   S.pseg = d_pseg;
   S.n_params = (int)n_params;
   if (nseg > 0) {
+    const int64_t nck0 = nf > 0 ? (nf + dev::kCheckpointSteps - 1) / dev::kCheckpointSteps : 0;
+    const int64_t nck1 = (nb + 1 + dev::kCheckpointSteps - 1) / dev::kCheckpointSteps;
+    dev::k_adj_rk4_recompute<<<(unsigned)((nck0 + nck1 + 31) / 32), 32, 0, st>>>(AF, S, d_zs, nck0, nck1);
     dev::k_adj_rk4_segments<<<(unsigned)nseg, 32, 0, st>>>(AF, S);
     dev::k_adj_rk4_combine<<<1, 64, 0, st>>>(S, d_pgrad);
   }
   check(cudaGetLastError(), "trajectory adjoint");
-  last_launches += 2;
+  last_launches += 3;
   return d_pgrad;
 }
 
@@ -584,11 +801,18 @@ void Engine::trajectory_vjp(const double* knot_grad, double* grad_params, int64_
   check(cudaStreamSynchronize(st), "trajectory adjoint");
 }
 
+// FNV-1a over the bytes of an array (the key of the kept forward sums).
+static uint64_t bytes_hash(const void* p, size_t n, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
+}
+
 void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double>& omega, int level,
                       const osc_rad_opts& o, bool current_abs, const double* grad_flux, double* flux_out,
                       double* grad_params, int64_t n_params, double* grad_knots) {
   if (level < 1 || level > 20) throw Error{OSC_ERR_RANGE, "adjoint level must be in [1, 20]"};
-  const int param_field = param_field_of(model, n_params);
+  const int param_field = grad_flux ? param_field_of(model, n_params) : -1;
   double pol[6];
   bool project = false;
   polarization_vector(o, pol, project);
@@ -599,6 +823,7 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
   pending_.clear();
   last_samples = last_launches = last_not_converged = 0;
   cudaStream_t st = stream;
+  const bool mixed = o.precision_mode == OSC_MIXED;
   const int64_t n_e = (int64_t)omega.size();
   const int64_t N = n_obs * n_e;
   if (N <= 0) return;
@@ -606,72 +831,128 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
   model.ensure_trajectory();
   upload_trajectory();
   set_level_grid(kMaxLevelMemory);  // fixed levels on the memory grid
-  ensure_levels(level);
   const Particle& P = model.particle;
-  // inputs
-  obs_.reserve(sizeof(double) * 3 * n_obs);
-  omega_.reserve(sizeof(double) * n_e);
-  adj_.reserve(sizeof(double) * (N /*grad*/ + N /*flux*/ + 6 * N /*W*/));
-  check(cudaMemcpyAsync(obs_.p, obs, sizeof(double) * 3 * n_obs, cudaMemcpyHostToDevice, st), "obs");
-  check(cudaMemcpyAsync(omega_.p, omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
-  double* d_grad = adj_.as<double>();
-  double* d_flux = d_grad + N;
-  double* d_W = d_flux + N;
-  check(cudaMemcpyAsync(d_grad, grad_flux, sizeof(double) * N, cudaMemcpyHostToDevice, st), "grad");
-  // forward sums at level L: the first-wave kernel with one span per segment
-  part_.reserve(sizeof(double) * 2 * kFdPartials * N);
-  cnt_.reserve(64);
-  unsigned* cnt = cnt_.as<unsigned>();
-  unsigned long long* work = reinterpret_cast<unsigned long long*>(cnt + 4) + 2;
-  check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");
-  FdWaveArgs w{};
-  w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = obs_.as<double>(); w.omega = omega_.as<double>();
-  w.n_e = n_e; w.n_items = N; w.act = nullptr; w.n_act = nullptr; w.first = 1; w.level = level;
-  const int fv = forced_variant[0] >= 0 ? forced_variant[0] : current_variant_[0];
-  const int te = fp64_entries_per_cta(fv);  // entries per CTA of that variant
-  w.tile_entries = te; w.min_span = 32; w.target_units = 1; w.part = part_.as<double>(); w.err = cnt + kCntErr;
-  w.work = work;
-  check(launch_fd_wave_fp64(w, (int)std::min<int64_t>((N + te - 1) / te, wave_grid(0, fv)), fv, st), "adjoint forward");
-  check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");  // counters start at zero
   const double dtL = dt_inclusive(tstart_, tstop_, level);
   const double c0 = P.q / (four_pi() * kC * kEps0 * kSqrt2Pi);
   const double cur = current_abs ? std::fabs(P.current) : P.current;
   const double c2 = four_pi() * cur / (kH * std::fabs(P.q) * kMu0 * kC) * 1e-6 * 0.001;
-  dev::k_adj_weights<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(part_.as<double>(), N, d_grad, c0 * dtL, c2, d_W,
-                                                                  d_flux);
-  // per-sample gradients
   const int64_t s_end = (int64_t)2 << level;
+  unsigned* cnt = cnt_.as<unsigned>();
+
+  // ---- forward sums S of every entry at level L, kept for a following call on the same inputs
+  // (same trajectory, observers, energies, level, arithmetic and normalisation)
+  uint64_t key = bytes_hash(obs, sizeof(double) * 3 * n_obs);
+  key = bytes_hash(omega.data(), sizeof(double) * n_e, key);
+  const int64_t kv[6] = {(int64_t)knots_version_, n_obs, n_e, level, mixed ? 1 : 0, current_abs ? 1 : 0};
+  key = bytes_hash(kv, sizeof kv, key);
+  adj_sums_.reserve(sizeof(double) * 7 * N);
+  double* d_S = adj_sums_.as<double>();
+  double* d_flux = d_S + 6 * N;
+  // inputs and level samples (shared with other requests, so always refreshed; cheap when resident)
+  obs_.reserve(sizeof(double) * 3 * n_obs);
+  omega_.reserve(sizeof(double) * n_e);
+  check(cudaMemcpyAsync(obs_.p, obs, sizeof(double) * 3 * n_obs, cudaMemcpyHostToDevice, st), "obs");
+  check(cudaMemcpyAsync(omega_.p, omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
+  if (mixed) ensure_mixed(level);
+  else ensure_levels(level);
+  if (!(adj_key_valid_ && adj_key_ == key)) {
+    adj_key_valid_ = false;
+    // the first-wave kernel at level L with one span per segment (levels 0..L-1, level L)
+    unsigned long long* work = reinterpret_cast<unsigned long long*>(cnt + 4) + 2;
+    check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");
+    FdWaveArgs w{};
+    w.obs = obs_.as<double>(); w.omega = omega_.as<double>();
+    w.n_e = n_e; w.n_items = N; w.act = nullptr; w.n_act = nullptr; w.first = 1; w.level = level;
+    w.min_span = 32; w.target_units = 1; w.err = cnt + kCntErr; w.work = work; w.fused = 0;
+    int te = 0;
+    if (mixed) {
+      const int v = variant_in_use(2);
+      te = mixed_entries_per_cta(v);
+      part_.reserve(sizeof(double) * 2 * kFdPartials * te * ((N + te - 1) / te));
+      w.lev = reinterpret_cast<const double*>(mrec_.p); w.tile_entries = te; w.part = part_.as<double>();
+      check(launch_fd_wave_mixed(w, frame_, (int)std::min<int64_t>((N + te - 1) / te, wave_grid(2, v)), v, st),
+            "adjoint forward (mixed)");
+    } else {
+      const int v = variant_in_use(0);
+      const int tev = fp64_entries_per_cta(v);  // entries per CTA of that variant
+      part_.reserve(sizeof(double) * 2 * kFdPartials * N);
+      w.lev = lev_.as<double>(); w.cap = lev_cap_; w.tile_entries = tev; w.part = part_.as<double>();
+      check(launch_fd_wave_fp64(w, (int)std::min<int64_t>((N + tev - 1) / tev, wave_grid(0, v)), v, st),
+            "adjoint forward");
+    }
+    check(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st), "memset");  // counters start at zero
+    dev::k_adj_sums<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(part_.as<double>(), N, te, c0 * dtL, c2, d_S, d_flux);
+    check(cudaGetLastError(), "adjoint sums");
+    last_launches += 2;
+    adj_key_ = key;
+    adj_key_valid_ = true;
+  }
+  auto finish = [&]() {  // wait, then report the forward's device errors
+    unsigned err = 0;
+    check(cudaMemcpyAsync(&err, cnt + kCntErr, sizeof err, cudaMemcpyDeviceToHost, st), "error word");
+    check(cudaStreamSynchronize(st), "adjoint");
+    if (err) {
+      adj_key_valid_ = false;
+      check(cudaMemset(cnt + kCntErr, 0, sizeof(unsigned)), "error word");
+      if (err & dev::kErrTmaTimeout)
+        throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
+      if (err & dev::kErrPlan) throw Error{OSC_ERR_STATE, "a sample-sum kernel variant was planned with another tile size"};
+      throw Error{OSC_ERR_INVALID, kMixedGeometryMessage};
+    }
+  };
+  if (flux_out) check(cudaMemcpyAsync(flux_out, d_flux, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
+  if (!grad_flux) {  // forward only
+    finish();
+    return;
+  }
+
+  // ---- weights and per-sample gradients
+  adj_.reserve(sizeof(double) * (N /*grad*/ + 6 * N /*W*/ + 1 /*max |W|*/));
+  double* d_grad = adj_.as<double>();
+  double* d_W = d_grad + N;
+  unsigned long long* d_wmax = reinterpret_cast<unsigned long long*>(d_W + 6 * N);
+  check(cudaMemcpyAsync(d_grad, grad_flux, sizeof(double) * N, cudaMemcpyHostToDevice, st), "grad");
+  check(cudaMemsetAsync(d_wmax, 0, sizeof(unsigned long long), st), "memset");
+  dev::k_adj_weights<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(d_S, N, d_grad, c0 * dtL, c2, d_W, d_wmax);
   const int64_t n = nknots_;
-  adj_s_.reserve(sizeof(double) * (9 * lev_cap_ + 2 * 9 * n + 9 * n));
+  const int64_t gcap = mixed ? s_end : lev_cap_;  // stride of the 9 per-sample gradient arrays
+  adj_s_.reserve(sizeof(double) * (9 * gcap + 2 * 9 * n + 9 * n));
   double* d_gs = adj_s_.as<double>();
-  double* d_yb = d_gs + 9 * lev_cap_;
+  double* d_yb = d_gs + 9 * gcap;
   double* d_pb = d_yb + 9 * n;
   double* d_diag = d_pb + 9 * n;
-  check(cudaMemsetAsync(d_gs, 0, sizeof(double) * (9 * lev_cap_ + 2 * 9 * n), st), "memset");
+  check(cudaMemsetAsync(d_gs, 0, sizeof(double) * (9 * gcap + 2 * 9 * n), st), "memset");
   int sms = 0;
   check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
-  const int64_t gx = (s_end - 1 + dev::kAdjThreads - 1) / dev::kAdjThreads;
-  const int64_t want = 16 * (int64_t)sms;  // CTAs in flight
-  int64_t gy = std::max<int64_t>(1, std::min<int64_t>((want + gx - 1) / gx, (N + dev::kAdjStage - 1) / dev::kAdjStage));
-  const int64_t per = ((N + gy - 1) / gy + dev::kAdjStage - 1) / dev::kAdjStage * dev::kAdjStage;
-  gy = (N + per - 1) / per;
-  dev::k_adj_samples<<<dim3((unsigned)gx, (unsigned)gy), dev::kAdjThreads, 0, st>>>(
-      lev_.as<double>(), lev_cap_, s_end, obs_.as<double>(), omega_.as<double>(), n_e, d_W, N, per, d_gs);
+  if (mixed) {
+    const int64_t n_pairs = s_end / 2;
+    const int64_t gx = (n_pairs + dev::kAdjMxThreads - 1) / dev::kAdjMxThreads;
+    const int64_t want = 12 * (int64_t)sms;  // CTAs in flight
+    int64_t gy = std::max<int64_t>(1, std::min<int64_t>((want + gx - 1) / gx, (N + dev::kAdjMxStage - 1) / dev::kAdjMxStage));
+    const int64_t per = ((N + gy - 1) / gy + dev::kAdjMxStage - 1) / dev::kAdjMxStage * dev::kAdjMxStage;
+    gy = (N + per - 1) / per;
+    dev::k_adj_samples_mixed<<<dim3((unsigned)gx, (unsigned)gy), dev::kAdjMxThreads, 0, st>>>(
+        reinterpret_cast<const float4*>(mrec_.p), n_pairs, frame_, obs_.as<double>(), omega_.as<double>(), n_e, d_W,
+        d_wmax, N, per, d_gs, gcap);
+  } else {
+    const int64_t gx = (s_end - 1 + dev::kAdjThreads - 1) / dev::kAdjThreads;
+    const int64_t want = 16 * (int64_t)sms;  // CTAs in flight
+    int64_t gy = std::max<int64_t>(1, std::min<int64_t>((want + gx - 1) / gx, (N + dev::kAdjStage - 1) / dev::kAdjStage));
+    const int64_t per = ((N + gy - 1) / gy + dev::kAdjStage - 1) / dev::kAdjStage * dev::kAdjStage;
+    gy = (N + per - 1) / per;
+    dev::k_adj_samples<<<dim3((unsigned)gx, (unsigned)gy), dev::kAdjThreads, 0, st>>>(
+        lev_.as<double>(), lev_cap_, s_end, obs_.as<double>(), omega_.as<double>(), n_e, d_W, N, per, d_gs);
+  }
   dev::k_adj_spline_eval<<<(unsigned)((s_end - 1 + 255) / 256), 256, 0, st>>>(knots_.as<double>(), n, tstart_, tstop_,
-                                                                             s_end, d_gs, lev_cap_, d_yb, d_pb);
+                                                                             s_end, d_gs, gcap, d_yb, d_pb);
   dev::k_adj_spline_solve<<<9, dev::kScanThreads, 0, st>>>(knots_.as<double>(), n, d_yb, d_pb, d_diag);
+  check(cudaGetLastError(), "adjoint");
+  last_launches += 4;
   // RK4 adjoint
   double* d_pgrad = rk4_adjoint(d_yb, param_field, n_params, st);
   if (grad_knots) check(cudaMemcpyAsync(grad_knots, d_yb, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, st), "download");
-  if (flux_out) check(cudaMemcpyAsync(flux_out, d_flux, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
   check(cudaMemcpyAsync(grad_params, d_pgrad, sizeof(double) * n_params, cudaMemcpyDeviceToHost, st), "download");
-  unsigned err = 0;
-  check(cudaMemcpyAsync(&err, cnt + kCntErr, sizeof err, cudaMemcpyDeviceToHost, st), "error word");
-  check(cudaStreamSynchronize(st), "adjoint");
-  if (err & dev::kErrTmaTimeout) {
-    check(cudaMemset(cnt + kCntErr, 0, sizeof(unsigned)), "error word");
-    throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
-  }
+  finish();
   last_samples = N * (s_end - 1);
 }
 

@@ -701,6 +701,8 @@ OSC_API int osc_set_half_period_scale(osc_ctx* ctx, int field_index, const doubl
     osc::FieldSpec& f = M.fields[idx];
     if (f.kind != OSC_FIELD_UNDULATOR) throw osc::Error{OSC_ERR_INVALID, "half-period factors apply to undulators"};
     if (!scale || n != 2 * (long long)f.nperiods) throw osc::Error{OSC_ERR_LENGTH, "n must be 2 * nperiods"};
+    if ((long long)f.half_scale.size() == n && std::memcmp(f.half_scale.data(), scale, sizeof(double) * n) == 0)
+      return;  // the same factors: the trajectory stands
     f.half_scale.assign(scale, scale + n);
     M.knots.clear();
     ++M.knots_version;
@@ -725,7 +727,7 @@ OSC_API int osc_flux_vjp(osc_ctx* ctx, const double* obs_xyz, long long n_obs, c
   return guarded(ctx, [&] {
     check_opts(opts);
     if (opts->nparticles != 0) throw osc::Error{OSC_ERR_INVALID, "the adjoint is for one particle: nparticles must be 0"};
-    if (n_obs < 1 || n_energies < 1 || !obs_xyz || !energies_eV || !grad_flux || !grad_half_scale)
+    if (n_obs < 1 || n_energies < 1 || !obs_xyz || !energies_eV || (grad_flux ? !grad_half_scale : !flux_out))
       throw osc::Error{OSC_ERR_INVALID, "bad buffers"};
     std::vector<double> omega(n_energies);
     for (long long i = 0; i < n_energies; ++i) omega[i] = osc::ev_to_omega(energies_eV[i]);

@@ -201,6 +201,11 @@ class Engine {
   DevBuf b_fields_, b_fvals_, b_obs_, b_omega_, b_acc_, b_jobs_, b_knots_, b_work_, b_rec_, b_rec_ext_, b_state_, b_out_,
       b_lvl_, b_act_[2], b_part_, b_plan_, b_cnt_;
   DevBuf adj_, adj_s_, adj_r_;      // adjoint scratch
+  // forward sums S (6 per entry) and flux of the last osc_flux_vjp, kept for a following call with
+  // the same key (trajectory version, observers, energies, level, arithmetic, normalisation)
+  DevBuf adj_sums_;
+  uint64_t adj_key_ = 0;
+  bool adj_key_valid_ = false;
   cudaGraphExec_t graph_exec_ = nullptr;
   long long graph_launches_ = 0;
   std::map<std::tuple<int, int64_t, int, int>, int> tuned_batch_;  // (jobs, entries, first, prefill level)

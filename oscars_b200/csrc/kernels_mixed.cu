@@ -62,6 +62,7 @@ __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, dou
 // global memory), so the span maxima already include the step into each span (dmax_spans_joined).
 // The groups' sums are reduced in shared memory in group order and one tile-major partial per entry
 // and span is stored; the CTA that finishes a tile's last span finalizes the tile (fused_unit_done).
+// With A.fused == 0 the partials are only stored (the adjoint's forward sums read them).
 template <int SUB, int MINB, int CP, bool SSM>
 __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveArgs A, MixedFrame F) {
   constexpr int TE = kMxThreads / SUB;
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveA
       }
       if (SUB > 1) __syncthreads();
     }
-    fused_unit_done_grouped<kMxThreads>(A, P, tile, n_act, &s_last, TE, &red[0][0][0]);
+    if (A.fused) fused_unit_done_grouped<kMxThreads>(A, P, tile, n_act, &s_last, TE, &red[0][0][0]);
   }
 }
 

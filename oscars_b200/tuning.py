@@ -4,13 +4,15 @@ The field is an ideal planar undulator whose full-strength region (the 2 * nperi
 between the end poles) has one amplitude factor s_k per half-period (``add_bfield_undulator(...,
 half_period_scale=s)``).  ``UndulatorFlux.apply(s, problem)`` returns the fixed-level flux of every
 (observer, energy) entry as a torch tensor; its backward pass is the hand-written adjoint
-(``osc_flux_vjp``: reverse mode through the radiation sum, the trajectory spline and the RK4 steps,
-FP64; the RK4 part runs parallel in time over 64-step segments, each step's stages recomputed from
-the stored states, joined by a sweep of the segments' 6 x 6 Jacobians).  PyTorch only carries the
-tensors.
+(``osc_flux_vjp``: reverse mode through the radiation sum, the trajectory spline and the RK4 steps).
+``compute='mixed'`` runs the radiation part in mixed precision (the mixed path's sums, an FP32
+reverse sweep with the FP64 phase of each pair of samples), ``'fp64'`` in FP64; the RK4 part is FP64,
+recomputes the trajectory from checkpoints every 256 steps and runs parallel in time over 64-step
+segments joined by a sweep of their 6 x 6 Jacobians.  The forward pass keeps the entry sums, which
+the backward pass on the same factors reuses.  PyTorch only carries the tensors.
 
     problem = TuningProblem(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41,
-                            obs=obs_xyz, energies_eV=E, level=12)
+                            obs=obs_xyz, energies_eV=E, level=12, compute='mixed')
     s = torch.ones(82, dtype=torch.float64, requires_grad=True)
     F = UndulatorFlux.apply(s, problem)          # (n_obs, n_energies)
     loss = ((F - F_ideal) ** 2).sum(); loss.backward()   # s.grad
@@ -32,7 +34,9 @@ class TuningProblem:
     """One undulator (with half-period factors), a 3 GeV-style beam and a fixed observation set."""
 
     def __init__(self, bfield, period, nperiods, obs, energies_eV, level=12, phase=-math.pi / 2,
-                 beam=None, ctstartstop=(-1.5, 1.5), npoints=20001, spectrum=False, gpu=0):
+                 beam=None, ctstartstop=(-1.5, 1.5), npoints=20001, spectrum=False, gpu=0, compute="fp64"):
+        if compute not in ("fp64", "mixed"):
+            raise ValueError("compute must be 'fp64' or 'mixed'")
         self.nperiods = int(nperiods)
         self.n_half = 2 * self.nperiods
         self.obs = np.ascontiguousarray(np.asarray(obs, dtype=np.float64).reshape(-1, 3))
@@ -46,7 +50,8 @@ class TuningProblem:
                                                   current=0.5)))
         self.sr.set_ctstartstop(*ctstartstop)
         self.sr.set_npoints_trajectory(npoints)
-        self._opts = self.sr._opts("", _lib_angle_unset(), None, None, 0.0, self.level, 0, 0, 0, "fp64")
+        self.compute = compute
+        self._opts = self.sr._opts("", _lib_angle_unset(), None, None, 0.0, self.level, 0, 0, 0, compute)
 
     @property
     def shape(self):
@@ -59,12 +64,14 @@ class TuningProblem:
         self.sr._ctx.call("osc_set_half_period_scale", -1, _lib.dptr(s), s.size)
 
     def flux(self, s):
-        """Fixed-level flux (FP64) for factors s, shape (n_obs, n_energies)."""
+        """Fixed-level flux for factors s, shape (n_obs, n_energies) (the forward pass of osc_flux_vjp,
+        whose entry sums a following vjp at the same factors reuses)."""
         self.set_scale(s)
         n_o, n_e = self.shape
         out = np.zeros(n_o * n_e)
-        self.sr._ctx.call("osc_flux_multi", _lib.dptr(self.obs), n_o, _lib.dptr(self.energies), n_e,
-                          ctypes.byref(self._opts), 1 if self.spectrum else 0, _lib.dptr(out), None, None)
+        self.sr._ctx.call("osc_flux_vjp", _lib.dptr(self.obs), n_o, _lib.dptr(self.energies), n_e, self.level,
+                          ctypes.byref(self._opts), 1 if self.spectrum else 0, None, _lib.dptr(out), None, self.n_half,
+                          None)
         return out.reshape(n_o, n_e)
 
     def vjp(self, s, grad_flux, knots=False):

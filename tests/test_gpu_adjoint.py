@@ -9,7 +9,8 @@ reference exactly as here), which is the size of the phase change a step of 1e-6
 central differences of the flux loss with h = 1e-6 are therefore rounding noise at the 20 % level
 (measured: 0.22 at 1e-6, 3e-2 at 1e-5, 7e-4 at 3e-4, 4e-4 at 1e-3).  The flux-loss checks use the
 Richardson extrapolation of steps 1e-3 and 3e-3; the trajectory part, which has no phase, is checked
-with h = 1e-6 directly.
+with h = 1e-6 directly.  The mixed-precision adjoint (compute='mixed') is checked against the FP64
+adjoint and against the reference's differences; its flux against FP64 at 1e-4 of the peak.
 """
 import os
 
@@ -23,11 +24,11 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 TOL = 1e-3
 
 
-def _problem():
+def _problem(compute="fp64"):
     from oscars_b200.tuning import TuningProblem
     obs, energies, level = adjoint_config()
     return TuningProblem(bfield=[0, 0.5, 0], period=[0, 0, 0.05], nperiods=41, obs=obs, energies_eV=energies,
-                         level=level)
+                         level=level, compute=compute)
 
 
 def _rel(a, b):
@@ -120,3 +121,39 @@ def test_torch_autograd_and_a_descent_step():
         step = 1e-3 / float(s.grad.abs().max())
         loss2 = ((UndulatorFlux.apply(s - step * s.grad, p) - F1) ** 2).sum()
     assert float(loss2) < float(loss.detach())
+
+
+def test_mixed_adjoint_against_fp64_and_reference():
+    g = np.load(os.path.join(GOLDEN, "adjoint_fd.npz"))
+    h = list(g["h"])
+    ref = richardson(g["grad_h%d" % h.index(1e-3)], g["grad_h%d" % h.index(3e-3)], 3.0)
+    p64, pmx = _problem(), _problem("mixed")
+    F1, F1m = p64.flux(np.ones(82)), pmx.flux(np.ones(82))
+    assert _rel(F1m, F1) <= 1e-4
+    F, grad = p64.vjp(g["s"], 2 * (p64.flux(g["s"]) - F1))
+    Fm, gradm = pmx.vjp(g["s"], 2 * (pmx.flux(g["s"]) - F1m))
+    assert _rel(Fm, F) <= 1e-4
+    e64, eref = _rel(gradm, grad), _rel(gradm, ref)
+    print("mixed adjoint vs FP64 adjoint: %.3e; vs reference differences (Richardson): %.3e" % (e64, eref))
+    assert e64 <= TOL
+    assert eref <= TOL
+
+
+@pytest.mark.parametrize("compute", ["fp64", "mixed"])
+def test_forward_sums_are_reused_only_for_the_same_inputs(compute):
+    """flux(s) keeps the entry sums; vjp at the same s reuses them and must equal a vjp computed from
+    scratch; after flux at other factors, vjp at s must recompute."""
+    g = np.load(os.path.join(GOLDEN, "adjoint_fd.npz"))
+    s0 = g["s"]
+    rng = np.random.default_rng(5)
+    gf = rng.standard_normal(_problem().shape)
+    fresh = _problem(compute)
+    F_a, grad_a = fresh.vjp(s0, gf)
+    p = _problem(compute)
+    F_b = p.flux(s0)
+    F_c, grad_c = p.vjp(s0, gf)
+    assert np.array_equal(F_b, F_a) and np.array_equal(F_c, F_a)
+    assert _rel(grad_c, grad_a) <= 1e-10  # the per-sample sums are folded with atomics (order varies)
+    p.flux(np.ones(82))
+    F_d, grad_d = p.vjp(s0, gf)
+    assert np.array_equal(F_d, F_a) and _rel(grad_d, grad_a) <= 1e-10
