@@ -20,7 +20,8 @@
 //                       segment of both integration chains runs its reverse pass at once (each
 //                       step's stages recomputed and differentiated), once with the knot adjoints and
 //                       once per unit adjoint entering it;
-//   k_adj_rk4_combine   a sequential sweep of the 6 x 6 segment Jacobians joins the segments.
+//   k_adj_rk4_lam       a sequential sweep of the 6 x 6 segment Jacobians joins the segments
+//   k_adj_rk4_pgrad     the parameter gradients of the unit-adjoint passes, weighted by it.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -637,7 +638,7 @@ __device__ __forceinline__ void knot_accel_adj(const double* kb, int64_t n, int6
 // One block per segment; thread 0 runs the segment's reverse pass with the knot adjoints and zero
 // adjoint entering (its parameter gradient goes straight to the result), threads 1..6 run it with the
 // unit adjoint e_{r-1} entering and no knot adjoints (the columns of the segment's transposed
-// Jacobian and parameter sensitivities, combined by k_adj_rk4_combine).
+// Jacobian and parameter sensitivities, combined by k_adj_rk4_lam and k_adj_rk4_pgrad).
 __global__ void __launch_bounds__(32) k_adj_rk4_segments(AdjFields F, AdjSegs S) {
   const int r = threadIdx.x;
   if (r > 6) return;
@@ -683,25 +684,50 @@ __global__ void __launch_bounds__(32) k_adj_rk4_segments(AdjFields F, AdjSegs S)
   }
 }
 
-// Sequential sweep over the segments of each chain (warp 0: forward chain, warp 1: backward chain):
-// the adjoint entering segment m is the one leaving segment m + 1.
-__global__ void __launch_bounds__(64) k_adj_rk4_combine(AdjSegs S, double* __restrict__ pbar) {
-  const int d = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// The adjoint entering every segment: a sequential sweep over the segments of each chain (block 0:
+// forward chain, block 1: backward chain), the adjoint entering segment m being the one leaving
+// segment m + 1 (lam_loc + J^T lam).  The segments' transposed Jacobians are staged through shared
+// memory a chunk at a time; one thread runs the 6 x 6 recurrence.
+constexpr int kLamChunk = 128;
+__global__ void __launch_bounds__(128) k_adj_rk4_lam(AdjSegs S, double* __restrict__ lam_in) {
+  __shared__ double sj[kLamChunk][42];  // per segment: J^T e_r (36), lam_loc (6)
+  const int d = blockIdx.x;
   double lam[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t m = S.nseg[d] - 1; m >= 0; --m) {
-    const int64_t g = S.base[d] + m;
-    for (int k = lane; k < S.n_params; k += 32) {
-      double acc = 0;
-      for (int r = 0; r < 6; ++r) acc += lam[r] * S.pseg[(g * 6 + r) * S.n_params + k];
-      if (acc != 0) atomicAdd(&pbar[k], acc);
+  for (int64_t hi = S.nseg[d]; hi > 0; hi -= kLamChunk) {
+    const int64_t lo = hi > kLamChunk ? hi - kLamChunk : 0;
+    for (int64_t idx = threadIdx.x; idx < (hi - lo) * 42; idx += blockDim.x) {
+      const int64_t g = S.base[d] + lo + idx / 42;
+      const int k = (int)(idx % 42);
+      sj[idx / 42][k] = k < 36 ? S.jt[g * 36 + k] : S.lam_loc[g * 6 + (k - 36)];
     }
-    double nl[6];
-    for (int j = 0; j < 6; ++j) {
-      double v = S.lam_loc[g * 6 + j];
-      for (int r = 0; r < 6; ++r) v += S.jt[(g * 6 + r) * 6 + j] * lam[r];
-      nl[j] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int64_t m = hi - 1; m >= lo; --m) {
+        const double* J = sj[m - lo];
+        double* out = lam_in + 6 * (S.base[d] + m);
+        double nl[6];
+        for (int jj = 0; jj < 6; ++jj) {
+          out[jj] = lam[jj];
+          double v = J[36 + jj];
+          for (int r = 0; r < 6; ++r) v = fma(J[r * 6 + jj], lam[r], v);
+          nl[jj] = v;
+        }
+        for (int jj = 0; jj < 6; ++jj) lam[jj] = nl[jj];
+      }
     }
-    for (int j = 0; j < 6; ++j) lam[j] = nl[j];
+    __syncthreads();
+  }
+}
+
+// Parameter gradient of the unit-adjoint passes: pbar[k] += sum over segments g and r of
+// lam_in[g][r] * pseg[g][r][k], a block per chunk of 32 segments, a thread per parameter.
+__global__ void k_adj_rk4_pgrad(AdjSegs S, const double* __restrict__ lam_in, int64_t nseg, double* __restrict__ pbar) {
+  const int64_t g0 = (int64_t)blockIdx.x * 32, g1 = min(nseg, g0 + 32);
+  for (int k = threadIdx.x; k < S.n_params; k += blockDim.x) {
+    double acc = 0;
+    for (int64_t g = g0; g < g1; ++g)
+      for (int r = 0; r < 6; ++r) acc = fma(lam_in[6 * g + r], S.pseg[(g * 6 + r) * S.n_params + k], acc);
+    if (acc != 0) atomicAdd(&pbar[k], acc);
   }
 }
 
@@ -710,42 +736,99 @@ __global__ void __launch_bounds__(64) k_adj_rk4_combine(AdjSegs S, double* __res
 // ---------------------------------------------------------------------------------------------
 // Host orchestration
 // ---------------------------------------------------------------------------------------------
+// Geometry of the two integration chains of the current trajectory and its fields on the device.
+struct RkChains {
+  std::vector<DevField> df;
+  std::vector<double> fvals;
+  double dt;
+  int64_t nf, nb;
+};
+static RkChains rk_chains(const Model& model, int64_t n) {
+  RkChains c;
+  for (const FieldSpec& f : model.fields) c.df.push_back(to_dev_field(f, c.fvals));
+  if (c.fvals.empty()) c.fvals.push_back(0.0);
+  const Particle& P = model.particle;
+  c.dt = ((model.ctstop - model.ctstart) / kC / (model.npoints - 1));
+  c.nf = (int64_t)(1 + (model.ctstop - P.t0) / kC / c.dt);
+  c.nb = (int64_t)((P.t0 - model.ctstart) / kC / c.dt);
+  if (c.nf + c.nb != n) throw Error{OSC_ERR_STATE, "trajectory and its knots disagree"};
+  return c;
+}
+
+// The RK4 adjoint's trajectory states: read from the knots at checkpoints every kCheckpointSteps
+// steps and recomputed between them (k_adj_rk4_recompute), on the side stream -- they depend on the
+// trajectory only, so the recomputation overlaps the radiation part of the adjoint -- into adj_z_
+// (the fields, their values, then the states), kept until the trajectory changes.
+void Engine::prepare_rk4_states(cudaStream_t st) {
+  if (zs_version_ == knots_version_) return;
+  const int64_t n = nknots_;
+  const RkChains c = rk_chains(model, n);
+  const size_t field_bytes = (sizeof(DevField) * c.df.size() + 255) & ~(size_t)255;
+  if (zs_pending_) check(cudaStreamSynchronize(aux_), "trajectory states");  // the buffer may be in use
+  zs_pending_ = false;
+  adj_z_.reserve(field_bytes + sizeof(double) * (c.fvals.size() + 6 * (n + 1)));
+  char* base = adj_z_.as<char>();
+  DevField* d_fields = reinterpret_cast<DevField*>(base);
+  double* d_vals = reinterpret_cast<double*>(base + field_bytes);
+  double* d_zs = d_vals + c.fvals.size();
+  check(cudaMemcpyAsync(d_fields, c.df.data(), sizeof(DevField) * c.df.size(), cudaMemcpyHostToDevice, st), "fields");
+  check(cudaMemcpyAsync(d_vals, c.fvals.data(), sizeof(double) * c.fvals.size(), cudaMemcpyHostToDevice, st), "fields");
+  dev::AdjFields AF{d_fields, (int)c.df.size(), d_vals, -1, model.particle.qomg, nullptr};
+  dev::AdjSegs S{};
+  S.t0 = model.particle.t0 / kC;
+  S.dt = c.dt;
+  S.nf = (int)c.nf;
+  S.nb = (int)c.nb;
+  S.knots = knots_.as<double>();
+  const int64_t nck0 = c.nf > 0 ? (c.nf + dev::kCheckpointSteps - 1) / dev::kCheckpointSteps : 0;
+  const int64_t nck1 = (c.nb + 1 + dev::kCheckpointSteps - 1) / dev::kCheckpointSteps;
+  check(cudaEventRecord(zs_fork_ev_, st), "event");
+  check(cudaStreamWaitEvent(aux_, zs_fork_ev_, 0), "stream wait");
+  dev::k_adj_rk4_recompute<<<(unsigned)((nck0 + nck1 + 31) / 32), 32, 0, aux_>>>(AF, S, d_zs, nck0, nck1);
+  check(cudaGetLastError(), "trajectory states");
+  check(cudaEventRecord(zs_ev_, aux_), "event");
+  ++last_launches;
+  zs_version_ = knots_version_;
+  zs_pending_ = true;
+}
+
+// The stream `st` waits for the recomputed states (before their use, or before the knots change).
+void Engine::join_rk4_states(cudaStream_t st) {
+  if (!zs_pending_) return;
+  check(cudaStreamWaitEvent(st, zs_ev_, 0), "stream wait");
+  zs_pending_ = false;
+}
+
 // Knot adjoints (9 x n on the device, layout of the knot values) -> gradient of the half-period
 // factors of field `param_field` (device pointer, n_params values; valid after the stream
 // completes).
 double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_params, cudaStream_t st) {
   const Particle& P = model.particle;
   const int64_t n = nknots_;
-  std::vector<double> fvals;
-  std::vector<DevField> df;
-  for (const FieldSpec& f : model.fields) df.push_back(to_dev_field(f, fvals));
-  if (fvals.empty()) fvals.push_back(0.0);
-  const double dt = ((model.ctstop - model.ctstart) / kC / (model.npoints - 1));
-  const int64_t nf = (int64_t)(1 + (model.ctstop - P.t0) / kC / dt);
-  const int64_t nb = (int64_t)((P.t0 - model.ctstart) / kC / dt);
-  if (nf + nb != n) throw Error{OSC_ERR_STATE, "trajectory and its knots disagree"};
+  prepare_rk4_states(st);
+  join_rk4_states(st);
+  const RkChains c = rk_chains(model, n);
+  const size_t field_bytes = (sizeof(DevField) * c.df.size() + 255) & ~(size_t)255;
+  char* zbase = adj_z_.as<char>();
+  const DevField* d_fields = reinterpret_cast<const DevField*>(zbase);
+  const double* d_vals = reinterpret_cast<const double*>(zbase + field_bytes);
+  const double* d_zs = d_vals + c.fvals.size();
   auto segs = [](int64_t M) -> int64_t { return M < 0 ? 0 : (M == 0 ? 1 : (M + dev::kSegSteps - 1) / dev::kSegSteps); };
-  const int64_t ns0 = segs(nf - 1), ns1 = segs(nb), nseg = ns0 + ns1;
-  const size_t field_bytes = (sizeof(DevField) * df.size() + 255) & ~(size_t)255;
-  adj_r_.reserve(field_bytes + sizeof(double) * (fvals.size() + n_params + nseg * (6 + 36 + 6 * n_params) + 6 * (n + 1)));
-  char* base = adj_r_.as<char>();
-  DevField* d_fields = reinterpret_cast<DevField*>(base);
-  double* d_vals = reinterpret_cast<double*>(base + field_bytes);
-  double* d_pgrad = d_vals + fvals.size();
+  const int64_t ns0 = segs(c.nf - 1), ns1 = segs(c.nb), nseg = ns0 + ns1;
+  adj_r_.reserve(sizeof(double) * (n_params + nseg * (6 + 36 + 6 * n_params + 6)));
+  double* d_pgrad = adj_r_.as<double>();
   double* d_lam = d_pgrad + n_params;
   double* d_jt = d_lam + 6 * nseg;
   double* d_pseg = d_jt + 36 * nseg;
-  double* d_zs = d_pseg + 6 * n_params * nseg;  // recomputed states (6 x (nf + nb + 1))
-  check(cudaMemcpyAsync(d_fields, df.data(), sizeof(DevField) * df.size(), cudaMemcpyHostToDevice, st), "fields");
-  check(cudaMemcpyAsync(d_vals, fvals.data(), sizeof(double) * fvals.size(), cudaMemcpyHostToDevice, st), "fields");
+  double* d_lam_in = d_pseg + 6 * n_params * nseg;  // adjoint entering each segment
   check(cudaMemsetAsync(d_pgrad, 0, sizeof(double) * n_params, st), "memset");
   check(cudaMemsetAsync(d_pseg, 0, sizeof(double) * 6 * n_params * nseg, st), "memset");
-  dev::AdjFields AF{d_fields, (int)df.size(), d_vals, param_field, P.qomg, d_pgrad};
+  dev::AdjFields AF{d_fields, (int)c.df.size(), d_vals, param_field, P.qomg, d_pgrad};
   dev::AdjSegs S{};
   S.t0 = P.t0 / kC;
-  S.dt = dt;
-  S.nf = (int)nf;
-  S.nb = (int)nb;
+  S.dt = c.dt;
+  S.nf = (int)c.nf;
+  S.nb = (int)c.nb;
   S.knots = knots_.as<double>();
   S.zs = d_zs;
   S.kb = d_kb;
@@ -758,11 +841,9 @@ double* Engine::rk4_adjoint(const double* d_kb, int param_field, int64_t n_param
   S.pseg = d_pseg;
   S.n_params = (int)n_params;
   if (nseg > 0) {
-    const int64_t nck0 = nf > 0 ? (nf + dev::kCheckpointSteps - 1) / dev::kCheckpointSteps : 0;
-    const int64_t nck1 = (nb + 1 + dev::kCheckpointSteps - 1) / dev::kCheckpointSteps;
-    dev::k_adj_rk4_recompute<<<(unsigned)((nck0 + nck1 + 31) / 32), 32, 0, st>>>(AF, S, d_zs, nck0, nck1);
     dev::k_adj_rk4_segments<<<(unsigned)nseg, 32, 0, st>>>(AF, S);
-    dev::k_adj_rk4_combine<<<1, 64, 0, st>>>(S, d_pgrad);
+    dev::k_adj_rk4_lam<<<2, 128, 0, st>>>(S, d_lam_in);
+    dev::k_adj_rk4_pgrad<<<(unsigned)((nseg + 31) / 32), 128, 0, st>>>(S, d_lam_in, nseg, d_pgrad);
   }
   check(cudaGetLastError(), "trajectory adjoint");
   last_launches += 3;
@@ -830,6 +911,9 @@ void Engine::flux_vjp(const double* obs, int64_t n_obs, const std::vector<double
 
   model.ensure_trajectory();
   upload_trajectory();
+  bool tuned_field = false;  // a forward pass of the tuning: the backward pass will need the states
+  for (const FieldSpec& f : model.fields) tuned_field = tuned_field || !f.half_scale.empty();
+  if (grad_flux || tuned_field) prepare_rk4_states(st);  // overlaps the radiation part
   set_level_grid(kMaxLevelMemory);  // fixed levels on the memory grid
   const Particle& P = model.particle;
   const double dtL = dt_inclusive(tstart_, tstop_, level);

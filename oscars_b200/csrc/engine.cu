@@ -70,6 +70,8 @@ Engine::Engine(int dev) : device(dev) {
   check(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming), "event");
+  check(cudaEventCreateWithFlags(&zs_fork_ev_, cudaEventDisableTiming), "event");
+  check(cudaEventCreateWithFlags(&zs_ev_, cudaEventDisableTiming), "event");
   cur_ = stream;
 }
 
@@ -85,6 +87,8 @@ Engine::~Engine() {
   if (order_ev_) cudaEventDestroy(order_ev_);
   if (fork_ev_) cudaEventDestroy(fork_ev_);
   if (join_ev_) cudaEventDestroy(join_ev_);
+  if (zs_fork_ev_) cudaEventDestroy(zs_fork_ev_);
+  if (zs_ev_) cudaEventDestroy(zs_ev_);
   if (last_stream_valid_ && last_stream_ != stream) cudaStreamSynchronize(last_stream_);
   if (stats_host_) cudaFreeHost(stats_host_);
   if (stage_host_) cudaFreeHost(stage_host_);
@@ -100,7 +104,8 @@ Engine::~Engine() {
   for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
                     &act_[1], &cnt_, &acc_, &acc_comp_, &mrec_, &b_fields_, &b_fvals_, &b_obs_, &b_omega_, &b_acc_, &b_jobs_,
                     &b_knots_, &b_work_, &b_rec_, &b_rec_ext_, &b_state_, &b_out_, &b_lvl_, &b_act_[0], &b_act_[1],
-                    &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_, &fused_, &stl_geo_, &stl_cen_, &stl_nrm_,
+                    &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_, &adj_sums_, &adj_z_, &fused_, &stl_geo_,
+                    &stl_cen_, &stl_nrm_,
                     &stl_state_, &stl_flags_})
     b->release();
   if (stream) cudaStreamDestroy(stream);
@@ -116,6 +121,7 @@ void Engine::upload_trajectory(const double* pinned) {
   if (knots_version_ == model.knots_version && nknots_ == k.n) return;
   levels_dropped_ = false;
   const int64_t n = k.n;
+  join_rk4_states(cur_);  // the side stream may still read the knots
   knots_.reserve(sizeof(double) * 20 * n);
   double* d = knots_.as<double>();
   if (pinned) {  // the same knots already laid out in pinned memory: one asynchronous copy

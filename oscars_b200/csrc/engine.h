@@ -172,7 +172,7 @@ class Engine {
   std::map<std::tuple<int, int, int, int>, int> tuned_;   // (kind, log2 entries, first level, last level) -> variant
   // (kind, entries, energies, last level, precision) -> highest level the last such request needed
   std::map<std::tuple<int, int64_t, int64_t, int, double>, int> prefill_hist_;
-  int current_variant_[4] = {2, 0, 3, 3};
+  int current_variant_[4] = {2, 0, 0, 3};
   int pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out, int32_t* d_lvl,
                    cudaStream_t st);
   bool tuning_ = false;
@@ -214,6 +214,13 @@ class Engine {
                  unsigned long long* m64, int64_t rec_stride);
   void radiation_beam_mixed(RadRequest& rq, int64_t N);
   double* rk4_adjoint(const double* d_kb, int param_field, int64_t n_params, cudaStream_t st);
+  // RK4 adjoint states recomputed from checkpoints on the side stream (adj_z_), per trajectory version
+  DevBuf adj_z_;
+  uint64_t zs_version_ = ~0ull;
+  bool zs_pending_ = false;
+  cudaEvent_t zs_fork_ev_ = nullptr, zs_ev_ = nullptr;
+  void prepare_rk4_states(cudaStream_t st);
+  void join_rk4_states(cudaStream_t st);
 
   // stream of the running request (caches and scratch are written on it), and the ordering of
   // requests that arrive on different streams
