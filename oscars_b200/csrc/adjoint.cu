@@ -189,58 +189,83 @@ struct AdjEntryMx {
   float wr[3], wi[3];
 };
 
-// Reverse sweep of one sample: geometry (rx, ry, iD = 1/D, en = 1 - n_z), the record's beta
-// components (-bx, -by, 1 - bz, bz, 1 - b^2) and a/c, and c = cos(2 pi t), sn = sin(2 pi t) of its
-// phase in turns (phi = -2 pi t).  acc: dJ/dX (3), dJ/dbeta (3), dJ/d(a/c) (3).
-__device__ __forceinline__ void adj_sample_mx(float rx, float ry, float iD, float en, float mbx, float mby, float eb,
-                                              float bz, float g, float ax, float ay, float az, float c, float sn,
-                                              const float* wr, const float* wi, float wc, float* acc) {
-  const float nx = rx * iD, ny = ry * iD, nz = 1.f - en;
-  const float ux = nx + mbx, uy = ny + mby, uz = eb - en;
-  const float om = fmaf(ny, mby, fmaf(nx, mbx, fmaf(en, bz, eb)));  // 1 - n.b without cancellation
-  const float iom = rcp_ftz(om);
-  const float na = fmaf(nx, ax, fmaf(ny, ay, nz * az));
-  const float k2 = iD * iom;
-  const float h = fmaf(g, iD, na);
-  const float k1 = k2 * iom * h;
-  const float Ax = fmaf(ux, k1, -ax * k2), Ay = fmaf(uy, k1, -ay * k2), Az = fmaf(uz, k1, -az * k2);
+// Reverse sweep of both samples of a pair record for one entry, each f32x2 lane one sample (the
+// operand layout of pair_sample): geometry and phases as the mixed forward kernel forms them (the
+// first sample's phase in FP64, the second's as the FP32 step), the amplitude
+// A = u k1 - a k2 (u = n - b, k2 = 1/(D om), k1 = k2 (g/D + n.a)/om, om = 1 - n.b, g = 1 - b.b) and
+// the reverse sweep of J = Re(sum_c W_c A_c e^{i phi}), phi = -2 pi t.  acc: dJ/dX (3), dJ/dbeta (3),
+// dJ/d(a/c) (3) of the two samples.
+__device__ __forceinline__ void adj_pair_mx(const float4 q0, const float4 q1, const float4 q2, const float4 q3,
+                                            const float4 q4, const float4 q5, const float4 q6, const double2 DXY,
+                                            const double2 DZT, const PairObs& o, const float* wr, const float* wi,
+                                            float2* acc) {
+  const float2 X = make_float2(q0.x, q0.y), Y = make_float2(q0.z, q0.w), Z = make_float2(q1.x, q1.y);
+  const float2 MBX = make_float2(q2.x, q2.y), MBY = make_float2(q2.z, q2.w);
+  const float2 EB = make_float2(q3.x, q3.y), BZ = make_float2(q3.z, q3.w);
+  const float2 G = make_float2(q4.x, q4.y), AZ = make_float2(q4.z, q4.w);
+  const float2 AX = make_float2(q5.x, q5.y), AY = make_float2(q5.z, q5.w);
+  const float2 M1 = f2(-1.f), ONE = f2(1.f);
+  // geometry and phases (pair_sample)
+  const float2 rx = fma2(X, M1, o.ox), ry = fma2(Y, M1, o.oy), rz = fma2(Z, M1, o.oz);
+  const float2 rho2 = fma2(rx, rx, mul2(ry, ry));
+  const float2 d2 = fma2(rz, rz, rho2);
+  const float2 iD = make_float2(rsqrt_ftz(d2.x), rsqrt_ftz(d2.y));
+  const float2 ri = mul2(rho2, iD);
+  const float2 corr = mul2(ri, fma2(f2(0.125f), mul2(ri, iD), f2(0.5f)));
+  const float t0 = fp64_turns(DXY.x, DXY.y, DZT.x, DZT.y, corr.x, 0.5f * iD.x, o);
+  const float2 DD = mul2(d2, iD);
+  const float inv = rcp_ftz(DD.x + DD.y);
+  const float num = fmaf(q6.x, rx.x + rx.y, fmaf(q6.y, ry.x + ry.y, -q6.z * (corr.x + corr.y)));
+  const float t1 = t0 + fmaf(o.wct, num * inv, o.wt * q6.w);
+  const float2 ph = mul2(make_float2(t0, t1), f2(kTwoPiF));
+  float2 sn, c;
+  sincos_ftz(ph.x, &sn.x, &c.x);
+  sincos_ftz(ph.y, &sn.y, &c.y);
+  // amplitude
+  const float2 nx = mul2(rx, iD), ny = mul2(ry, iD), en = mul2(corr, iD), nz = fma2(en, M1, ONE);
+  const float2 ux = add2(nx, MBX), uy = add2(ny, MBY), uz = fma2(en, M1, EB);
+  const float2 om = fma2(ny, MBY, fma2(nx, MBX, fma2(en, BZ, EB)));  // 1 - n.b without cancellation
+  const float2 iom = make_float2(rcp_ftz(om.x), rcp_ftz(om.y));
+  const float2 na = fma2(nx, AX, fma2(ny, AY, mul2(nz, AZ)));
+  const float2 k2 = mul2(iD, iom), mk2 = mul2(k2, M1);
+  const float2 h = fma2(G, iD, na);
+  const float2 k1 = mul2(mul2(k2, iom), h);
+  const float2 Ax = fma2(ux, k1, mul2(AX, mk2)), Ay = fma2(uy, k1, mul2(AY, mk2)), Az = fma2(uz, k1, mul2(AZ, mk2));
   // W e^{i phi} = (Wr + i Wi)(c - i sn): P its real part, Q its imaginary part
-  const float Px = fmaf(wr[0], c, wi[0] * sn), Py = fmaf(wr[1], c, wi[1] * sn), Pz = fmaf(wr[2], c, wi[2] * sn);
-  const float Qx = fmaf(wi[0], c, -wr[0] * sn), Qy = fmaf(wi[1], c, -wr[1] * sn), Qz = fmaf(wi[2], c, -wr[2] * sn);
+  const float2 Px = fma2(f2(wr[0]), c, mul2(f2(wi[0]), sn)), Py = fma2(f2(wr[1]), c, mul2(f2(wi[1]), sn)),
+               Pz = fma2(f2(wr[2]), c, mul2(f2(wi[2]), sn));
+  const float2 Qx = fma2(f2(wi[0]), c, mul2(f2(-wr[0]), sn)), Qy = fma2(f2(wi[1]), c, mul2(f2(-wr[1]), sn)),
+               Qz = fma2(f2(wi[2]), c, mul2(f2(-wr[2]), sn));
   // reverse sweep (the FP64 kernel's, in FP32)
-  const float phb = -fmaf(Qx, Ax, fmaf(Qy, Ay, Qz * Az));
-  float Db = -wc * phb;
-  const float ubx = Px * k1, uby = Py * k1, ubz = Pz * k1;
-  const float k1b = fmaf(Px, ux, fmaf(Py, uy, Pz * uz));
-  float abx = -Px * k2, aby = -Py * k2, abz = -Pz * k2;
-  const float k2b = fmaf(k1b * iom, h, -fmaf(Px, ax, fmaf(Py, ay, Pz * az)));
-  const float hb = k1b * k2 * iom;
-  const float gb = hb * iD;
-  const float iDb = fmaf(hb, g, k2b * iom);
-  const float iomb = fmaf(k1b * k2, h, k2b * iD);
-  const float omb = -iomb * iom * iom;
-  Db = fmaf(-iDb * iD, iD, Db);
-  const float bx = -mbx, by = -mby;
-  const float bbx = -2.f * gb * bx - omb * nx - ubx;
-  const float bby = -2.f * gb * by - omb * ny - uby;
-  const float bbz = -2.f * gb * bz - omb * nz - ubz;
-  const float nbx = hb * ax - omb * bx + ubx;
-  const float nby = hb * ay - omb * by + uby;
-  const float nbz = hb * az - omb * bz + ubz;
-  abx = fmaf(hb, nx, abx);
-  aby = fmaf(hb, ny, aby);
-  abz = fmaf(hb, nz, abz);
-  const float nbn = fmaf(nbx, nx, fmaf(nby, ny, nbz * nz));
-  Db = fmaf(-nbn, iD, Db);
-  acc[0] -= fmaf(nbx, iD, Db * nx);
-  acc[1] -= fmaf(nby, iD, Db * ny);
-  acc[2] -= fmaf(nbz, iD, Db * nz);
-  acc[3] += bbx;
-  acc[4] += bby;
-  acc[5] += bbz;
-  acc[6] += abx;
-  acc[7] += aby;
-  acc[8] += abz;
+  float2 Db = mul2(o.wc, fma2(Qx, Ax, fma2(Qy, Ay, mul2(Qz, Az))));  // -(w/c) phib, phib = -Q.A
+  const float2 ubx = mul2(Px, k1), uby = mul2(Py, k1), ubz = mul2(Pz, k1);
+  const float2 k1b = fma2(Px, ux, fma2(Py, uy, mul2(Pz, uz)));
+  const float2 pa = fma2(Px, AX, fma2(Py, AY, mul2(Pz, AZ)));
+  const float2 k2b = fma2(mul2(k1b, iom), h, mul2(pa, M1));
+  const float2 hb = mul2(mul2(k1b, k2), iom);
+  const float2 gb2 = mul2(mul2(hb, iD), f2(-2.f));  // -2 gb
+  const float2 iDb = fma2(hb, G, mul2(k2b, iom));
+  const float2 iomb = fma2(mul2(k1b, k2), h, mul2(k2b, iD));
+  const float2 momb = mul2(mul2(iomb, iom), iom);  // -omb
+  Db = fma2(mul2(mul2(iDb, iD), M1), iD, Db);
+  // b = (-MBX, -MBY, BZ): bb = -2 gb b - omb n - ub, nb = hb a - omb b + ub
+  const float2 bbx = fma2(momb, nx, fma2(gb2, mul2(MBX, M1), mul2(ubx, M1)));
+  const float2 bby = fma2(momb, ny, fma2(gb2, mul2(MBY, M1), mul2(uby, M1)));
+  const float2 bbz = fma2(momb, nz, fma2(gb2, BZ, mul2(ubz, M1)));
+  const float2 nbx = fma2(hb, AX, fma2(momb, mul2(MBX, M1), ubx));
+  const float2 nby = fma2(hb, AY, fma2(momb, mul2(MBY, M1), uby));
+  const float2 nbz = fma2(hb, AZ, fma2(momb, BZ, ubz));
+  const float2 nbn = fma2(nbx, nx, fma2(nby, ny, mul2(nbz, nz)));
+  Db = fma2(mul2(nbn, M1), iD, Db);
+  acc[0] = fma2(fma2(nbx, iD, mul2(Db, nx)), M1, acc[0]);
+  acc[1] = fma2(fma2(nby, iD, mul2(Db, ny)), M1, acc[1]);
+  acc[2] = fma2(fma2(nbz, iD, mul2(Db, nz)), M1, acc[2]);
+  acc[3] = add2(acc[3], bbx);
+  acc[4] = add2(acc[4], bby);
+  acc[5] = add2(acc[5], bbz);
+  acc[6] = fma2(hb, nx, add2(acc[6], mul2(Px, mk2)));
+  acc[7] = fma2(hb, ny, add2(acc[7], mul2(Py, mk2)));
+  acc[8] = fma2(hb, nz, add2(acc[8], mul2(Pz, mk2)));
 }
 
 __global__ void __launch_bounds__(kAdjMxThreads, 3)
@@ -280,36 +305,16 @@ __global__ void __launch_bounds__(kAdjMxThreads, 3)
     __syncthreads();
     const int cnt = (int)min((int64_t)kAdjMxStage, e1 - base);
     if (live) {
-      float acc[18];
+      float2 acc[9];
 #pragma unroll
-      for (int k = 0; k < 18; ++k) acc[k] = 0.f;
-      for (int j = 0; j < cnt; ++j) {
-        const PairObs& o = se[j].o;
-        // geometry of both samples (pair_sample)
-        const float rx0 = o.ox.x - q0.x, rx1 = o.ox.x - q0.y, ry0 = o.oy.x - q0.z, ry1 = o.oy.x - q0.w;
-        const float rz0 = o.oz.x - q1.x, rz1 = o.oz.x - q1.y;
-        const float r20 = fmaf(rx0, rx0, ry0 * ry0), r21 = fmaf(rx1, rx1, ry1 * ry1);
-        const float d20 = fmaf(rz0, rz0, r20), d21 = fmaf(rz1, rz1, r21);
-        const float iD0 = rsqrt_ftz(d20), iD1 = rsqrt_ftz(d21);
-        const float ri0 = r20 * iD0, ri1 = r21 * iD1;
-        const float c0 = ri0 * fmaf(0.125f, ri0 * iD0, 0.5f), c1 = ri1 * fmaf(0.125f, ri1 * iD1, 0.5f);
-        // phases in turns: the first in FP64, the second as the FP32 step from it
-        const float t0 = fp64_turns(DXY.x, DXY.y, DZT.x, DZT.y, c0, 0.5f * iD0, o);
-        const float inv = rcp_ftz(d20 * iD0 + d21 * iD1);
-        const float num = fmaf(q6.x, rx0 + rx1, fmaf(q6.y, ry0 + ry1, -q6.z * (c0 + c1)));
-        const float t1 = t0 + fmaf(o.wct, num * inv, o.wt * q6.w);
-        float sn0, cs0, sn1, cs1;
-        sincos_ftz(t0 * kTwoPiF, &sn0, &cs0);
-        sincos_ftz(t1 * kTwoPiF, &sn1, &cs1);
-        const float* wr = se[j].wr;
-        const float* wi = se[j].wi;
-        adj_sample_mx(rx0, ry0, iD0, c0 * iD0, q2.x, q2.z, q3.x, q3.z, q4.x, q5.x, q5.z, q4.z, cs0, sn0, wr, wi, o.wc.x,
-                      acc);
-        adj_sample_mx(rx1, ry1, iD1, c1 * iD1, q2.y, q2.w, q3.y, q3.w, q4.y, q5.y, q5.w, q4.w, cs1, sn1, wr, wi, o.wc.x,
-                      acc + 9);
+      for (int k = 0; k < 9; ++k) acc[k] = f2(0.f);
+      for (int j = 0; j < cnt; ++j)
+        adj_pair_mx(q0, q1, q2, q3, q4, q5, q6, DXY, DZT, se[j].o, se[j].wr, se[j].wi, acc);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        sacc[k][tid] += (double)acc[k].x;
+        sacc[9 + k][tid] += (double)acc[k].y;
       }
-#pragma unroll
-      for (int k = 0; k < 18; ++k) sacc[k][tid] += (double)acc[k];
     }
     __syncthreads();
   }
