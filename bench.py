@@ -299,6 +299,51 @@ def _long_run(step, stream, flush, min_s=1.0):
     return n, total
 
 
+PD_WORKLOAD = ("power density on the flux headline's 201x201 XY rectangle (10mm x 10mm at z=30m), same undulator, "
+               "beam and trajectory; adaptive levels (precision 0.01); device-resident observers and outputs, level "
+               "samples rebuilt every step")
+
+
+def power_density_leg(ctx, d_obs, n, stream, flush, steps, warmup, local):
+    """Power density on the headline grid (config 1), FP64 and mixed, timed like the flux headline;
+    the mixed / FP64 peak-normalised difference at the fixed level 12."""
+    import ctypes
+    import numpy as np
+    import torch
+    from oscars_b200._lib import RadOpts
+    dev = d_obs.device
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    d_lvl = torch.zeros(n, dtype=torch.int32, device=dev)
+    out, arrays = {}, {}
+    for m in ("fp64", "mixed"):
+        def opts(**kw):
+            o = RadOpts(precision=kw.get("precision", 0.01), max_level=kw.get("max_level", -2), max_level_extended=0,
+                        nparticles=0, quantity=0, precision_mode=1 if m == "mixed" else 0)
+            o.horizontal[:] = [1, 0, 0]
+            o.propagation[:] = [0, 0, 1]
+            return o
+        o = opts()
+        d_out = torch.zeros(n, dtype=torch.float64, device=dev)
+
+        def step(o=o, d_out=d_out):
+            ctx.call("osc_drop_level_cache")
+            ctx.call("osc_power_density_device", ctypes.c_void_p(d_obs.data_ptr()), None, n, 0, ctypes.byref(o),
+                     ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_lvl.data_ptr()), sptr)
+        per, sps, lps, clocks = _time_device_steps(ctx, step, stream, flush, steps, warmup, local)
+        ms = sum(per)
+        out[m] = {"value": sps * steps / (ms * 1e-3) / 1e9, "unit": "Gsamples/s", "ms_per_step": ms / steps,
+                  "samples_per_step": sps, "gpu_launches_per_step": lps, "clocks": clocks}
+        of = opts(precision=0.0, max_level=12)
+        ctx.call("osc_power_density_device", ctypes.c_void_p(d_obs.data_ptr()), None, n, 0, ctypes.byref(of),
+                 ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_lvl.data_ptr()), sptr)
+        torch.cuda.synchronize(dev)
+        arrays[m] = d_out.cpu().numpy().copy()
+    err = float(np.max(np.abs(arrays["mixed"] - arrays["fp64"])) / np.max(np.abs(arrays["fp64"])))
+    return {"workload": PD_WORKLOAD, "steps": steps, "warmup": warmup, "fp64": out["fp64"], "mixed": out["mixed"],
+            "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+            "mixed_vs_fp64_peak_rel_err": {"value": err, "fixed_level": 12}}
+
+
 def product_arm(args):
     import ctypes
     import numpy as np
@@ -439,6 +484,9 @@ def product_arm(args):
 
     e2e_value = e2e_run(False)
     e2e_traj_value = e2e_run(True)
+    pd = None
+    if "mixed" in modes:  # config 1's power density on the same grid, FP64 and mixed
+        pd = power_density_leg(ctx, d_obs, n, stream, flush, min(args.steps, 50), max(3, args.warmup), local)
     h2d = xyz.nbytes + 8
     d2h = n * 8 + n * 4
     sharded = None
@@ -472,6 +520,11 @@ def product_arm(args):
         if "mixed" in res:
             line["fp64"] = {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms_per_step"],
                             "roofline": res["fp64"]["roofline"], "clocks": res["fp64"]["clocks"]}
+        if pd is not None:
+            line["power_density"] = pd
+            line["roofline"].update({"pd_value": pd["mixed"]["value"], "pd_fp64_value": pd["fp64"]["value"],
+                                     "pd_mixed_over_fp64": pd["mixed_over_fp64"],
+                                     "pd_mixed_vs_fp64_peak_rel_err": pd["mixed_vs_fp64_peak_rel_err"]["value"]})
         if world == 1 and args.batched_steps > 0:
             bw = max(3, args.warmup)
             line["batched"] = {"note": "inputs far larger than L2 (GBs of level records); device time = each "

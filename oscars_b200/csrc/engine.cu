@@ -55,6 +55,7 @@ Engine::Engine(int dev) : device(dev) {
   check(cudaSetDevice(dev), "cudaSetDevice");
   check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
   bd_bits_.reserve(32 * sizeof(unsigned long long));
+  mrec_bd_.reserve(32 * sizeof(unsigned long long));
   cnt_.reserve(64);
   check(cudaMemset(cnt_.p, 0, 64), "memset");
   check(cudaHostAlloc(reinterpret_cast<void**>(&stats_host_), 2 * kStatSlots * sizeof(unsigned long long),
@@ -101,7 +102,7 @@ Engine::~Engine() {
     if (p.pinned) cudaFreeHost(p.pinned);
   }
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
-  for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
+  for (DevBuf* b : {&knots_, &lev_, &bd_bits_, &mrec_bd_, &obs_, &nrm_, &omega_, &out_, &lvl_, &state_, &part_, &act_[0],
                     &act_[1], &cnt_, &acc_, &acc_comp_, &mrec_, &b_fields_, &b_fvals_, &b_obs_, &b_omega_, &b_acc_, &b_jobs_,
                     &b_knots_, &b_work_, &b_rec_, &b_rec_ext_, &b_state_, &b_out_, &b_lvl_, &b_act_[0], &b_act_[1],
                     &b_part_, &b_plan_, &b_cnt_, &adj_, &adj_s_, &adj_r_, &adj_sums_, &adj_z_, &fused_, &stl_geo_,
@@ -275,10 +276,16 @@ void Engine::reserve_mixed(int L) {
 }
 
 void Engine::fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s) {
+  if (s_end <= s_begin) return;
+  // the beta-difference maxima of the levels filled here start from zero
+  const int Lb = s_begin <= 1 ? 0 : 63 - __builtin_clzll((unsigned long long)s_begin);
+  const int Le = 63 - __builtin_clzll((unsigned long long)(s_end - 1));
+  check(cudaMemsetAsync(mrec_bd_.as<unsigned long long>() + Lb, 0, sizeof(unsigned long long) * (Le - Lb + 1), s),
+        "memset");
   check(launch_mixed_records(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, mrec_ext_, frame_,
-                             mrec_.as<float4>(), s),
+                             mrec_.as<float4>(), mrec_bd_.as<unsigned long long>(), s),
         "mixed records");
-  ++last_launches;
+  last_launches += 2;
 }
 
 void Engine::ensure_mixed(int L) {
@@ -372,7 +379,9 @@ int Engine::wave_grid(int kind, int variant) {
   if (wave_grid_[kind][variant] == 0) {
     int sms = 0;
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
-    const int per = kind == 2 ? mixed_blocks_per_sm(variant) : fp64_blocks_per_sm(kind == 1, variant);
+    const int per = kind == 2   ? mixed_blocks_per_sm(variant)
+                    : kind == 4 ? pd_mixed_blocks_per_sm()
+                                : fp64_blocks_per_sm(kind == 1, variant);
     wave_grid_[kind][variant] = sms * per;
   }
   return wave_grid_[kind][variant];
@@ -385,7 +394,7 @@ int Engine::wave_grid(int kind, int variant) {
 int Engine::pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out,
                          int32_t* d_lvl, cudaStream_t st) {
   if (forced_variant[kind] >= 0) return forced_variant[kind];
-  if (!autotune || tuning_ || kind == 1) return current_variant_[kind];
+  if (!autotune || tuning_ || kind == 1 || kind == 4) return current_variant_[kind];
   int lg = 0;
   while (((int64_t)1 << (lg + 1)) <= n_items) ++lg;
   const auto key = std::make_tuple(kind, lg, Lfirst, lstop);
@@ -431,10 +440,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   set_level_grid(ext_from);
   const Particle& P = model.particle;
   const bool mixed = o.precision_mode == OSC_MIXED;
-  if (mixed && rq.power_density)
-    throw Error{OSC_ERR_INVALID, "compute='mixed' applies to flux and spectrum; power density runs in FP64"};
   const int Lfirst = std::min(9, lstop);
-  const int kind = rq.power_density ? 1 : (mixed ? 2 : 0);
+  const int kind = rq.power_density ? (mixed ? 4 : 1) : (mixed ? 2 : 0);
   // Levels enqueued without a host round trip: up to kPrefillLevel, or, for a request shape seen
   // before, up to the highest level its previous call needed (waves past it would find no entries;
   // levels beyond are still added by the host loop below when entries remain).
@@ -446,7 +453,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
                               : pick_variant(kind, const_cast<RadRequest&>(rq), n_items, Lfirst, lstop, d_out, d_lvl, st);
   prefill(mixed, Lfirst, Lpre);
   const int resident = wave_grid(kind, variant);  // CTAs resident at once on the device
-  const int tile = mixed ? mixed_entries_per_cta(variant) : rq.power_density ? 128 : fp64_entries_per_cta(variant);
+  const int tile = rq.power_density ? (mixed ? pd_mixed_entries_per_cta() : 128)
+                                    : (mixed ? mixed_entries_per_cta(variant) : fp64_entries_per_cta(variant));
   const int min_span = rq.power_density ? kMinSpan : kMinSpanSplit;
   const int64_t target = 4 * (int64_t)resident;   // >= 4 waves of equal units per launch
   const int64_t N = n_items;
@@ -575,19 +583,21 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
       check(launch_fd_finalize(f, N, st), "flux finalize");
     } else {
       PdWaveArgs w{};
-      w.lev = lev_.as<double>(); w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
+      w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
+      w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = c64 + 2;
       auto ev = timed_begin(st);
-      check(launch_pd_wave_fp64(w, grid_for(L), st), "power density wave");
+      if (mixed) check(launch_pd_wave_mixed(w, frame_, grid_for(L), st), "power density wave (mixed)");
+      else check(launch_pd_wave_fp64(w, grid_for(L), st), "power density wave");
       timed_end(ev, st);
       PdFinalArgs f{};
       f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
       f.directional = rq.directional; f.tile_entries = tile; f.min_span = min_span; f.target_units = target;
       f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
       f.precision = o.precision; f.scale = scale; f.weight = weight; f.two_over_gamma = 2. / P.gamma;
-      f.bdmax_levels = reinterpret_cast<const double*>(bd_bits_.p);
+      f.bdmax_levels = reinterpret_cast<const double*>(mixed ? mrec_bd_.p : bd_bits_.p);
       f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
       f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
       f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.level_max = level_max; f.work_reset = c64 + 2;

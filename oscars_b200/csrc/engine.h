@@ -166,13 +166,14 @@ class Engine {
   cudaEvent_t stage_ev_ = nullptr;
   int stats_slot_ = 0;
   std::vector<int> pending_;
-  // kernel variants: kind 0 = FP64 flux, 1 = FP64 power density, 2 = mixed flux, 3 = batched mixed
-  int wave_grid_[4][16] = {};
+  // kernel variants: kind 0 = FP64 flux, 1 = FP64 power density, 2 = mixed flux, 3 = batched mixed,
+  // 4 = mixed power density
+  int wave_grid_[5][16] = {};
   int wave_grid(int kind, int variant);
   std::map<std::tuple<int, int, int, int>, int> tuned_;   // (kind, log2 entries, first level, last level) -> variant
   // (kind, entries, energies, last level, precision) -> highest level the last such request needed
   std::map<std::tuple<int, int64_t, int64_t, int, double>, int> prefill_hist_;
-  int current_variant_[4] = {2, 0, 0, 3};
+  int current_variant_[5] = {2, 0, 0, 3, 0};
   int pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out, int32_t* d_lvl,
                    cudaStream_t st);
   bool tuning_ = false;
@@ -182,6 +183,7 @@ class Engine {
   DevBuf acc_, acc_comp_;          // multi-particle compensated accumulation
   // mixed-precision pair records (kMixedRecordBytesPerSample per sample, level-cache indexing)
   DevBuf mrec_;
+  DevBuf mrec_bd_;                 // 32 x u64: per-level beta-difference maxima of the filled records
   int64_t mrec_cap_ = 0;
   int mrec_filled_ = -1;
   uint64_t mrec_version_ = ~0ull;
@@ -191,7 +193,7 @@ class Engine {
   void fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s);
   void compute_frame();
  public:
-  int forced_variant[4] = {-1, -1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
+  int forced_variant[5] = {-1, -1, -1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
   bool autotune = true;
   int variant_in_use(int kind) const { return forced_variant[kind] >= 0 ? forced_variant[kind] : current_variant_[kind]; }
   std::map<std::tuple<int, int, int, int>, int> tuned() const { return tuned_; }

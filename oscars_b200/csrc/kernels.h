@@ -190,9 +190,12 @@ __host__ __device__ inline double mixed_theta_max(double gamma) {
 
 // Mixed pair records (fd_common.cuh, 144 bytes per two samples) of level samples [s_begin, s_end),
 // evaluated from the trajectory knots (t | y[9] | y''[9], n points); levels above ext_from are the
-// reference's extended levels (their own time spacing, fd_common.cuh level_time).
+// reference's extended levels (their own time spacing, fd_common.cuh level_time).  bd_bits (32
+// words, may be NULL): per level, the largest |beta_i - beta_{i-1}| is folded in (atomicMax on the
+// bits of the positive double; the caller zeroes the words of the levels it fills).
 cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
-                                 int64_t s_end, int ext_from, const MixedFrame& F, float4* rec, cudaStream_t st);
+                                 int64_t s_end, int ext_from, const MixedFrame& F, float4* rec,
+                                 unsigned long long* bd_bits, cudaStream_t st);
 constexpr int kMixedRecordBytesPerSample = 72;
 // Compiled kernel variants (see kernels_fp64.cu / kernels_mixed.cu); the engine's autotuner picks one.
 constexpr int kFp64Variants = 4;
@@ -212,6 +215,11 @@ cudaError_t launch_level_fill(const double* knots, int64_t n, double tstart, dou
 cudaError_t launch_fd_wave_fp64(const FdWaveArgs& a, int grid, int variant, cudaStream_t st);
 cudaError_t launch_fd_finalize(const FdFinalArgs& a, int64_t n_act_bound, cudaStream_t st);
 cudaError_t launch_pd_wave_fp64(const PdWaveArgs& a, int grid, cudaStream_t st);
+// Mixed-precision power density over the pair records (kernels_mixed.cu): a.lev = the records,
+// partials entry-major like the FP64 kernel's, tile_entries = pd_mixed_entries_per_cta().
+cudaError_t launch_pd_wave_mixed(const PdWaveArgs& a, const MixedFrame& F, int grid, cudaStream_t st);
+int pd_mixed_entries_per_cta();
+int pd_mixed_blocks_per_sm();
 cudaError_t launch_pd_finalize(const PdFinalArgs& a, int64_t n_act_bound, cudaStream_t st);
 
 }  // namespace osc

@@ -27,10 +27,16 @@ struct PairStage {
 // Sample 0 is the zero-amplitude record at the position and time of sample 1.  The two samples of a
 // pair sit in adjacent lanes (s_begin and the block size are even) and exchange their FP64 values
 // for the pair's step, so every lane of the grid's last warp takes part (past s_end on a clamped
-// sample, writing nothing).
+// sample, writing nothing).  Also folds, per level, the largest |beta_i - beta_{i-1}| over its
+// samples i >= 1 into bd_bits (the power-density stop rule, src/OSCARSSR.cc:2887-2891; the FP64 values
+// and operations of k_level_betadiff): the predecessor's beta comes from the lane before, or, in
+// lane 0, from the spline at its time.
 __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, double tstart, double tstop,
                                 int64_t s_begin, int64_t s_end, int ext_from, MixedFrame F,
-                                float* __restrict__ rec) {
+                                float* __restrict__ rec, unsigned long long* __restrict__ bd_bits) {
+  __shared__ unsigned long long blk[32];  // per-level maxima of this block
+  if (threadIdx.x < 32) blk[threadIdx.x] = 0;
+  __syncthreads();
   const int64_t s_raw = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s_raw < s_end;
   const int64_t s = active ? s_raw : s_end - 2 + (s_raw & 1);
@@ -53,6 +59,22 @@ __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, dou
   const double xo = __shfl_xor_sync(full, x, 1), yo = __shfl_xor_sync(full, y, 1);
   const double zo = __shfl_xor_sync(full, z, 1), to = __shfl_xor_sync(full, taus, 1);
   if (active) write_pair_record(rec, s, s == 0, x, y, z, taus, px, py, pz, qx, qy, qz, xo, yo, zo, to);
+  // beta step from the previous sample of the same level
+  double pbx = __shfl_up_sync(full, v[3], 1), pby = __shfl_up_sync(full, v[4], 1), pbz = __shfl_up_sync(full, v[5], 1);
+  const int L = 63 - __clzll((unsigned long long)(s == 0 ? 1 : s));
+  const bool step = active && s >= 1 && s - ((int64_t)1 << L) > 0;
+  if (step && (threadIdx.x & 31) == 0) {  // the predecessor belongs to the previous warp
+    double w[9];
+    spline_eval9(knots, n, level_time(tstart, tstop, s - 1, ext_from), w);
+    pbx = w[3]; pby = w[4]; pbz = w[5];
+  }
+  if (step && bd_bits) {
+    const double dx = __dsub_rn(v[3], pbx), dy = __dsub_rn(v[4], pby), dz = __dsub_rn(v[5], pbz);
+    const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    atomicMax(&blk[L & 31], (unsigned long long)__double_as_longlong(d));
+  }
+  __syncthreads();
+  if (bd_bits && threadIdx.x < 32 && blk[threadIdx.x]) atomicMax(&bd_bits[threadIdx.x], blk[threadIdx.x]);
 }
 
 // Sample sum over pair records, sample-split: the CTA's 128 threads form SUB groups of TE = 128 / SUB
@@ -218,15 +240,173 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_fd_wave_mixed_pair(FdWaveA
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Power density over the pair records, mixed precision (src/OSCARSSR.cc:2869-2922):
+//   sum += |N1 x ((N1 - b) x a/c)|^2 / (1 - b.N1)^5 / |O - X|^2 * (N1 . normal)
+// (the sum of the squared projections on N2 and N3, an orthonormal pair across N1, is the squared
+// norm of the numerator, which is across N1).  Geometry, 1 - b.N1 without cancellation
+// ((1 - b_z) + (1 - n_z) b_z - n_x b_x - n_y b_y, with 1 - n_z = (rho^2 / (D + |R_z|) + |R_z| - R_z) / D
+// for any direction) and the numerator run on packed f32x2 operands in the particle frame; the fifth
+// power of 1 / (1 - b.N1) (~1e40 near the axis, beyond FP32) and the sums in FP64.  Sample-split like
+// the flux kernel: SUB groups of TE = 128 / SUB entries, each taking 1/SUB of every staged chunk, the
+// groups' sums reduced in group order; entry-major partials for k_pd_finalize.
+// ---------------------------------------------------------------------------------------------
+struct PdObsMx {
+  float2 ox, oy, oz;  // observer in the particle frame (both lanes)
+  float2 nx, ny, nz;  // surface normal in the particle frame (both lanes)
+};
+
+// Exact float -> double of any finite normal float (or +-0, which comes out as +-6e-39) on the
+// integer pipe.
+__device__ __forceinline__ double float_to_double_bits(float x) {
+  const unsigned u = __float_as_uint(x);
+  return __hiloint2double((int)((((u & 0x7FFFFFFFu) >> 3) + 0x38000000u) | (u & 0x80000000u)), (int)(u << 29));
+}
+
+template <bool NORMAL, bool DIRECTIONAL>
+__device__ __forceinline__ double pd_pair(const float4* __restrict__ q, const PdObsMx& o) {
+  const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5];
+  const float2 X = make_float2(q0.x, q0.y), Y = make_float2(q0.z, q0.w), Z = make_float2(q1.x, q1.y);
+  const float2 MBX = make_float2(q2.x, q2.y), MBY = make_float2(q2.z, q2.w);
+  const float2 EB = make_float2(q3.x, q3.y), BZ = make_float2(q3.z, q3.w);
+  const float2 AZ = make_float2(q4.z, q4.w), AX = make_float2(q5.x, q5.y), AY = make_float2(q5.z, q5.w);
+  const float2 M1 = f2(-1.f);
+  const float2 rx = fma2(X, M1, o.ox), ry = fma2(Y, M1, o.oy), rz = fma2(Z, M1, o.oz);
+  const float2 rho2 = fma2(rx, rx, mul2(ry, ry));
+  const float2 d2 = fma2(rz, rz, rho2);
+  const float2 iD = make_float2(rsqrt_ftz(d2.x), rsqrt_ftz(d2.y));
+  const float2 arz = make_float2(fabsf(rz.x), fabsf(rz.y));
+  const float2 den = fma2(d2, iD, arz);  // D + |R_z|
+  const float2 ide = make_float2(rcp_ftz(den.x), rcp_ftz(den.y));
+  const float2 en = mul2(fma2(rho2, ide, fma2(rz, M1, arz)), iD);  // 1 - n_z
+  const float2 nx = mul2(rx, iD), ny = mul2(ry, iD), nz = fma2(en, M1, f2(1.f));
+  const float2 om = fma2(ny, MBY, fma2(nx, MBX, fma2(en, BZ, EB)));  // 1 - n.b
+  const float2 iom = make_float2(rcp_ftz(om.x), rcp_ftz(om.y));
+  const float2 ux = add2(nx, MBX), uy = add2(ny, MBY), uz = fma2(en, M1, EB);  // n - b
+  const float2 wx = fma2(uy, AZ, mul2(mul2(uz, AY), M1));
+  const float2 wy = fma2(uz, AX, mul2(mul2(ux, AZ), M1));
+  const float2 wz = fma2(ux, AY, mul2(mul2(uy, AX), M1));
+  const float2 mx = fma2(ny, wz, mul2(mul2(nz, wy), M1));
+  const float2 my = fma2(nz, wx, mul2(mul2(nx, wz), M1));
+  const float2 mz = fma2(nx, wy, mul2(mul2(ny, wx), M1));
+  float2 t = mul2(mul2(fma2(mx, mx, fma2(my, my, mul2(mz, mz))), iD), iD);
+  if (NORMAL) {
+    const float2 n1dn = fma2(nx, o.nx, fma2(ny, o.ny, mul2(nz, o.nz)));
+    t = mul2(t, n1dn);
+    if (DIRECTIONAL) t = make_float2(n1dn.x > 0.f ? t.x : 0.f, n1dn.y > 0.f ? t.y : 0.f);
+  }
+  const double q0d = nonneg_float_to_double(iom.x), q1d = nonneg_float_to_double(iom.y);
+  const double q02 = q0d * q0d, q12 = q1d * q1d;
+  return fma(float_to_double_bits(t.x), q02 * q02 * q0d, float_to_double_bits(t.y) * (q12 * q12 * q1d));
+}
+
+template <int SUB, int MINB, int CP>
+__global__ void __launch_bounds__(kMxThreads, MINB) k_pd_wave_mixed(PdWaveArgs A, MixedFrame F) {
+  constexpr int TE = kMxThreads / SUB;
+  if (A.tile_entries != TE) {  // the host sized the partials for another tile
+    if (threadIdx.x == 0) atomicOr(A.err, kErrPlan);
+    return;
+  }
+  __shared__ __align__(16) PairStage<CP> st;
+  __shared__ double red[SUB > 1 ? SUB - 1 : 1][TE];
+  __shared__ WavePlan P;
+  __shared__ int64_t next_unit;
+  const int tid = threadIdx.x;
+  const int grp = tid / TE, q = tid % TE;
+  const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
+  if (tid == 0) {
+    P = wave_plan(A.first, A.level, n_act, TE, A.target_units, A.min_span);
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int64_t units = P.tiles * P.spans;
+  const float4* rec = reinterpret_cast<const float4*>(A.lev);
+  uint32_t phase_bits = 0;
+  for (;;) {
+    if (tid == 0) next_unit = (int64_t)atomicAdd(A.work, 1ull);
+    __syncthreads();
+    const int64_t u = next_unit;
+    __syncthreads();
+    if (u >= units) break;
+    const int64_t tile = u / P.spans;
+    const int span = (int)(u % P.spans);
+    const int64_t slot = tile * TE + q;
+    const bool live = slot < n_act;
+    const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+    PdObsMx o;
+    {
+      const double* R = F.rot;
+      const double ox = A.obs[3 * item] - F.x0[0], oy = A.obs[3 * item + 1] - F.x0[1], oz = A.obs[3 * item + 2] - F.x0[2];
+      o.ox = f2((float)(R[0] * ox + R[1] * oy + R[2] * oz));
+      o.oy = f2((float)(R[3] * ox + R[4] * oy + R[5] * oz));
+      o.oz = f2((float)(R[6] * ox + R[7] * oy + R[8] * oz));
+      double nx = 0, ny = 0, nz = 0;
+      if (A.has_normal) { nx = A.normals[3 * item]; ny = A.normals[3 * item + 1]; nz = A.normals[3 * item + 2]; }
+      o.nx = f2((float)(R[0] * nx + R[1] * ny + R[2] * nz));
+      o.ny = f2((float)(R[3] * nx + R[4] * ny + R[5] * nz));
+      o.nz = f2((float)(R[6] * nx + R[7] * ny + R[8] * nz));
+    }
+    for (int g = 0; g < P.nseg; ++g) {
+      const int64_t b0 = seg_begin(P, g) + (int64_t)span * seg_span(P, g);
+      const int64_t b1 = min(seg_end(P, g), b0 + seg_span(P, g));
+      const int64_t p0 = b0 >> 1, p1 = b1 > b0 ? b1 >> 1 : p0;  // spans are whole pairs
+      double S = 0;
+      const int64_t nchunks = (p1 - p0 + CP - 1) / CP;
+      if (tid == 0 && nchunks > 0) {
+        const int64_t hi = min(p1, p0 + CP);
+        mbar_arrive_expect_tx(&st.bar[0], (uint32_t)((hi - p0) * (kPairFloats * 4)));
+        tma_load_1d(&st.v[0][0], rec + kPairF4 * p0, (uint32_t)((hi - p0) * (kPairFloats * 4)), &st.bar[0]);
+      }
+      for (int64_t c = 0; c < nchunks; ++c) {
+        const int buf = (int)(c & 1);
+        const int64_t lo = p0 + c * CP, hi = min(p1, lo + CP);
+        if (tid == 0 && c + 1 < nchunks) {
+          const int64_t lo2 = lo + CP, hi2 = min(p1, lo2 + CP);
+          mbar_arrive_expect_tx(&st.bar[buf ^ 1], (uint32_t)((hi2 - lo2) * (kPairFloats * 4)));
+          tma_load_1d(&st.v[buf ^ 1][0], rec + kPairF4 * lo2, (uint32_t)((hi2 - lo2) * (kPairFloats * 4)), &st.bar[buf ^ 1]);
+        }
+        if (!mbar_wait(&st.bar[buf], (phase_bits >> buf) & 1u)) {
+          if (tid == 0) atomicOr(A.err, kErrTmaTimeout);
+          return;
+        }
+        phase_bits ^= 1u << buf;
+        const float4* sv = st.v[buf];
+        const int n = (int)(hi - lo);
+        const int j0 = (grp * n) / SUB, j1 = ((grp + 1) * n) / SUB;  // the chunk's pairs split evenly
+        if (live) {
+          if (A.has_normal && A.directional)
+            for (int j = j0; j < j1; ++j) S += pd_pair<true, true>(sv + kPairF4 * j, o);
+          else if (A.has_normal)
+            for (int j = j0; j < j1; ++j) S += pd_pair<true, false>(sv + kPairF4 * j, o);
+          else
+            for (int j = j0; j < j1; ++j) S += pd_pair<false, false>(sv + kPairF4 * j, o);
+        }
+        __syncthreads();  // everyone is done with `buf` before it is refilled
+      }
+      // reduce the groups' sums in group order; group 0 stores the span's partial (entry-major)
+      if (SUB > 1 && grp > 0) red[grp - 1][q] = S;
+      if (SUB > 1) __syncthreads();
+      if (grp == 0) {
+        for (int o2 = 0; o2 < SUB - 1; ++o2) S += red[o2][q];
+        if (live) A.part[slot * P.nseg * P.spans + g * P.spans + span] = S;
+      }
+      if (SUB > 1) __syncthreads();
+    }
+  }
+}
+
 }  // namespace dev
 
 cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, double tstop, int64_t s_begin,
-                                 int64_t s_end, int ext_from, const MixedFrame& F, float4* rec, cudaStream_t st) {
+                                 int64_t s_end, int ext_from, const MixedFrame& F, float4* rec,
+                                 unsigned long long* bd_bits, cudaStream_t st) {
   if (s_end <= s_begin) return cudaSuccess;
   const int T = 128;
   const unsigned grid = (unsigned)((s_end - s_begin + T - 1) / T);
   dev::k_mixed_records<<<grid, T, 0, st>>>(knots, n, tstart, tstop, s_begin, s_end, ext_from, F,
-                                            reinterpret_cast<float*>(rec));
+                                            reinterpret_cast<float*>(rec), bd_bits);
   return cudaGetLastError();
 }
 
@@ -265,6 +445,20 @@ cudaError_t launch_fd_wave_mixed(const FdWaveArgs& a, const MixedFrame& F, int g
     case i: dev::k_fd_wave_mixed_pair<sub, minb, cp, ssm><<<grid, T, 0, st>>>(a, F); break;
     OSC_MIXED_VARIANTS(OSC_LAUNCH)
   }
+  return cudaGetLastError();
+}
+
+// The mixed power-density kernel: 4 groups of 32 entries, at least 4 CTAs per SM, 128 pair records
+// per staged chunk.
+constexpr int kPdMxSub = 4;
+int pd_mixed_entries_per_cta() { return dev::kMxThreads / kPdMxSub; }
+int pd_mixed_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::k_pd_wave_mixed<kPdMxSub, 4, 128>, dev::kMxThreads, 0);
+  return n > 0 ? n : 1;
+}
+cudaError_t launch_pd_wave_mixed(const PdWaveArgs& a, const MixedFrame& F, int grid, cudaStream_t st) {
+  dev::k_pd_wave_mixed<kPdMxSub, 4, 128><<<grid, dev::kMxThreads, 0, st>>>(a, F);
   return cudaGetLastError();
 }
 

@@ -7,6 +7,8 @@ own peak, so small grids away from the axis test the path where the flux is weak
 on-axis maximum.  The cases span the region the mixed path accepts (mixed_geometry_ok): observer
 angles up to min(1e-2, 20/gamma), correction phases (w/c) rho^2 / (2 Rz) up to 3e4 rad, harmonics
 up to the 7th, the 2-3 keV end of the 100-3000 eV spectrum off axis; outside it the path refuses.
+Power density (no phase: every direction is accepted) on the 201 x 201 grid, on points with normals
+(directional and not), on a side wall at large angles, adaptively and for a seeded beam.
 """
 import math
 
@@ -173,8 +175,6 @@ def test_far_off_axis_observer_is_rejected():
     run_case(s, UND_SETUP)
     with pytest.raises(ValueError, match="compute='mixed' needs observers near the beam axis"):
         s.calculate_spectrum(obs=[3, 0, 30], energy_range_eV=[100, 200], npoints=3, compute="mixed")
-    with pytest.raises(ValueError, match="power density runs in FP64"):
-        s.calculate_power_density_rectangle(npoints=[3, 3], width=[0.01, 0.01], translation=[0, 0, 30], compute="mixed")
 
 
 def _variants(kind):
@@ -205,3 +205,62 @@ def test_every_mixed_variant_matches_fp64(variant):
         e = _err(out["mixed"], out["fp64"])
         print("variant %d %s: mixed vs fp64 %.3e" % (variant, call, e))
         assert e <= TOL
+
+
+# ---- power density ------------------------------------------------------------------------------
+def test_power_density_201x201_fixed_level_12():
+    f64, mx = _pair(UND_SETUP, "calculate_power_density_rectangle",
+                    dict(npoints=[201, 201], width=[0.01, 0.01], translation=[0, 0, 30], precision=0, max_level=12))
+    e = _err(mx, f64)
+    print("power density 201x201 L=12 mixed vs fp64: %.3e" % e)
+    assert e <= TOL
+
+
+def test_power_density_adaptive_levels():
+    kw = dict(npoints=[41, 41], width=[0.02, 0.02], translation=[0, 0, 30])
+    f64, mx = _pair(UND_SETUP, "calculate_power_density_rectangle", kw)
+    assert _err(mx, f64) <= TOL
+    l64, lmx = _pair(UND_SETUP, "calculate_power_density_rectangle", dict(kw, quantity="level"))
+    same = float(np.mean(l64 == lmx))
+    print("power density adaptive: %.3e, levels equal at %.4f of the entries" % (_err(mx, f64), same))
+    assert same >= 0.97
+
+
+@pytest.mark.parametrize("normal", [1, -1, 0])
+def test_power_density_points_with_normals(normal):
+    """Points on a 30 m arc with tilted normals (directional for normal = +-1), and the same points
+    with normals that half of the samples see from behind."""
+    from cases import ARC_POINTS, ARC_POINTS_MIXED
+    for pts in (ARC_POINTS, ARC_POINTS_MIXED):
+        f64, mx = _pair(UND_SETUP, "calculate_power_density", dict(points=pts, normal=normal, precision=0, max_level=11))
+        e = _err(mx, f64)
+        print("power density points normal=%d mixed vs fp64: %.3e" % (normal, e))
+        assert e <= TOL
+
+
+def test_power_density_side_wall_at_large_angles():
+    """A wall 0.1 m beside the beam from z = -1 m to 3 m (angles up to 90 degrees and beyond), facing
+    the beam: no near-axis observer, each entry normalised by the case's own peak."""
+    zs = np.linspace(-1.0, 3.0, 41)
+    ys = np.linspace(-0.05, 0.05, 5)
+    pts = [[[0.1, float(y), float(z)], [-1.0, 0.0, 0.0]] for z in zs for y in ys]
+    for normal in (0, 1):
+        f64, mx = _pair(UND_SETUP, "calculate_power_density", dict(points=pts, normal=normal, precision=0, max_level=12))
+        e = _err(mx, f64)
+        print("side wall normal=%d mixed vs fp64: %.3e" % (normal, e))
+        assert e <= TOL
+        # far from the axis the values are tiny but must keep their relative accuracy too
+        far = np.abs(f64) > 0
+        rel = np.max(np.abs(mx[far] - f64[far]) / np.abs(f64[far]))
+        assert rel <= 1e-3, rel
+
+
+def test_power_density_beam_mixed_matches_fp64():
+    from cases import BEAM_GAUSS, EPU_X, EPU_Y, traj
+    setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=11))]
+    f64, mx = _pair(setup, "calculate_power_density_rectangle",
+                    dict(npoints=[21, 21], width=[0.01, 0.01], translation=[0, 0, 30], nparticles=6, precision=0,
+                         max_level=11))
+    e = _err(mx, f64)
+    print("power density beam (6 particles) mixed vs fp64: %.3e" % e)
+    assert e <= TOL
