@@ -256,11 +256,12 @@ struct PdObsMx {
   float2 nx, ny, nz;  // surface normal in the particle frame (both lanes)
 };
 
-// Exact float -> double of any finite normal float (or +-0, which comes out as +-6e-39) on the
-// integer pipe.
+// Exact float -> double of any finite normal float or zero on the integer pipe (denormals, which the
+// flushed FP32 arithmetic does not produce, would come out as ~6e-39).
 __device__ __forceinline__ double float_to_double_bits(float x) {
   const unsigned u = __float_as_uint(x);
-  return __hiloint2double((int)((((u & 0x7FFFFFFFu) >> 3) + 0x38000000u) | (u & 0x80000000u)), (int)(u << 29));
+  const unsigned hi = (u & 0x7FFFFFFFu) ? ((((u & 0x7FFFFFFFu) >> 3) + 0x38000000u) | (u & 0x80000000u)) : u;
+  return __hiloint2double((int)hi, (int)(u << 29));
 }
 
 template <bool NORMAL, bool DIRECTIONAL>

@@ -233,17 +233,21 @@ def test_power_density_points_with_normals(normal):
     from cases import ARC_POINTS, ARC_POINTS_MIXED
     for pts in (ARC_POINTS, ARC_POINTS_MIXED):
         f64, mx = _pair(UND_SETUP, "calculate_power_density", dict(points=pts, normal=normal, precision=0, max_level=11))
+        if not np.any(f64):  # every point sees the trajectory from behind its surface
+            assert not np.any(mx)
+            continue
         e = _err(mx, f64)
         print("power density points normal=%d mixed vs fp64: %.3e" % (normal, e))
         assert e <= TOL
 
 
 def test_power_density_side_wall_at_large_angles():
-    """A wall 0.1 m beside the beam from z = -1 m to 3 m (angles up to 90 degrees and beyond), facing
-    the beam: no near-axis observer, each entry normalised by the case's own peak."""
+    """A wall 0.1 m beside the beam from z = -1 m to 3 m (angles up to 90 degrees and beyond) whose
+    normal points along the direction of view: no near-axis observer, each case normalised by its own
+    peak."""
     zs = np.linspace(-1.0, 3.0, 41)
     ys = np.linspace(-0.05, 0.05, 5)
-    pts = [[[0.1, float(y), float(z)], [-1.0, 0.0, 0.0]] for z in zs for y in ys]
+    pts = [[[0.1, float(y), float(z)], [1.0, 0.0, 0.0]] for z in zs for y in ys]  # N1 . normal > 0: seen
     for normal in (0, 1):
         f64, mx = _pair(UND_SETUP, "calculate_power_density", dict(points=pts, normal=normal, precision=0, max_level=12))
         e = _err(mx, f64)
