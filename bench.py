@@ -344,6 +344,23 @@ def power_density_leg(ctx, d_obs, n, stream, flush, steps, warmup, local):
             "mixed_vs_fp64_peak_rel_err": {"value": err, "fixed_level": 12}}
 
 
+def power_density_only(steps, warmup):
+    """The power-density leg alone on GPU 0 (for profiler runs)."""
+    import torch
+    from oscars_b200.sr import sr
+    s = sr(gpu=1, device=0)
+    setup(s)
+    s.calculate_trajectory()
+    xyz = s._rectangle([GRID, GRID], "XY", [0.01, 0.01], None, None, [0, 0, 30], 0, False)[0]
+    dev = torch.device("cuda", 0)
+    d_obs = torch.tensor(xyz, dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    return power_density_leg(s._ctx, d_obs, GRID * GRID, stream, flush, steps, warmup, 0)
+
+
 def product_arm(args):
     import ctypes
     import numpy as np
@@ -969,8 +986,8 @@ def main():
                     help="force this compiled variant of the --compute kernel instead of autotuning (profiler runs)")
     ap.add_argument("--batched-steps", type=int, default=3,
                     help="timed steps of the batched workloads (EPU beam, uneven jobs); 0 skips them")
-    ap.add_argument("--only", default="", choices=["", "beam", "uneven", "tuning", "sharded"],
-                    help="run one batched workload alone and print its JSON object (for profiler runs)")
+    ap.add_argument("--only", default="", choices=["", "beam", "uneven", "tuning", "sharded", "power_density"],
+                    help="run one workload alone and print its JSON object (for profiler runs)")
     ap.add_argument("--particles", type=int, default=BEAM_PARTICLES,
                     help="with --only beam: particles of the beam (the first ones of the same seeded sequence)")
     ap.add_argument("--jobs", type=int, default=UNEVEN_JOBS,
@@ -996,7 +1013,9 @@ def main():
     elif args.only:
         import torch
         torch.cuda.set_device(0)
-        if args.only == "beam":
+        if args.only == "power_density":
+            r = power_density_only(args.steps, args.warmup)
+        elif args.only == "beam":
             r = beam_leg(args.batched_steps, args.warmup, particles=args.particles, quick=args.quick)
         elif args.only == "uneven":
             r = uneven_leg(args.batched_steps, args.warmup, n_jobs=args.jobs, quick=args.quick)

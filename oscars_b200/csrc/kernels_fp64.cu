@@ -359,6 +359,9 @@ __global__ void k_fd_finalize(FdFinalArgs A) {
 // ---------------------------------------------------------------------------------------------
 // Power density (src/OSCARSSR.cc:2869-2922):
 //   sum += [(N1 x ((N1 - b) x a/c)) . Nk]^2 / (1 - b.N1)^5 / |O - X|^2 * (N1 . normal),  k = 2, 3
+// N1 and 1 - b.N1 keep the reference's operations (the difference is ill-conditioned, so its value
+// depends on them); the well-conditioned rest is summed as |N1 x W|^2 / ((1 - b.N1)^5 |O - X|^2),
+// equal to the two projections to rounding.
 // ---------------------------------------------------------------------------------------------
 constexpr int kPdThreads = 128;
 constexpr int kPdChunk = 128;
@@ -426,20 +429,10 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
         if (live) {
           for (int j = j0; j < j1; ++j) {
             const double Rx = __dsub_rn(Ox, st.v[buf][1][j]), Ry = __dsub_rn(Oy, st.v[buf][2][j]), Rz = __dsub_rn(Oz, st.v[buf][3][j]);
+            // N1 and 1 - B.N1 with the reference's operations: the difference 1 - B.N1 (~1e-8) carries
+            // the rounding of B.N1, which its result shares
             double n1x, n1y, n1z;
             unit3(Rx, Ry, Rz, n1x, n1y, n1z);
-            // Orthogonal() (include/TVector3D.h:132-142), then unit; N3 = unit(N1 x N2)
-            const double xx = fabs(n1x), yy = fabs(n1y), zz = fabs(n1z);
-            double ox, oy, oz;
-            if (xx < yy) {
-              if (xx < zz) { ox = 0; oy = n1z; oz = -n1y; } else { ox = n1y; oy = -n1x; oz = 0; }
-            } else {
-              if (yy < zz) { ox = -n1z; oy = 0; oz = n1x; } else { ox = n1y; oy = -n1x; oz = 0; }
-            }
-            double n2x, n2y, n2z, n3x, n3y, n3z;
-            unit3(ox, oy, oz, n2x, n2y, n2z);
-            unit3(__dsub_rn(__dmul_rn(n1y, n2z), __dmul_rn(n2y, n1z)), __dsub_rn(__dmul_rn(n1z, n2x), __dmul_rn(n2z, n1x)),
-                  __dsub_rn(__dmul_rn(n1x, n2y), __dmul_rn(n2x, n1y)), n3x, n3y, n3z);
             const double n1dn = A.has_normal
                                     ? __dadd_rn(__dadd_rn(__dmul_rn(n1x, Nx), __dmul_rn(n1y, Ny)), __dmul_rn(n1z, Nz))
                                     : 1.0;
@@ -454,12 +447,12 @@ __global__ void __launch_bounds__(kPdThreads) k_pd_wave_fp64(PdWaveArgs A) {
             const double my = __dsub_rn(__dmul_rn(n1z, wx), __dmul_rn(wz, n1x));
             const double mz = __dsub_rn(__dmul_rn(n1x, wy), __dmul_rn(wx, n1y));
             const double bdn = __dadd_rn(__dadd_rn(__dmul_rn(bx, n1x), __dmul_rn(by, n1y)), __dmul_rn(bz, n1z));
-            const double den = pow(__dsub_rn(1.0, bdn), 5.0);
+            // the rest is well conditioned: the squared projections on N2 and N3 (an orthonormal pair
+            // across N1) sum to |N1 x W|^2, which is across N1; (1 - B.N1)^5 by products; one division
+            const double om = __dsub_rn(1.0, bdn), om2 = om * om;
             const double m2 = __dadd_rn(__dadd_rn(__dmul_rn(Rx, Rx), __dmul_rn(Ry, Ry)), __dmul_rn(Rz, Rz));
-            const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n2x), __dmul_rn(my, n2y)), __dmul_rn(mz, n2z));
-            const double d3 = __dadd_rn(__dadd_rn(__dmul_rn(mx, n3x), __dmul_rn(my, n3y)), __dmul_rn(mz, n3z));
-            sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d2, d2), den), m2), n1dn);
-            sum += __dmul_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(d3, d3), den), m2), n1dn);
+            const double num = fma(mx, mx, fma(my, my, mz * mz));
+            sum = fma(num / (om2 * om2 * om * m2), n1dn, sum);
           }
         }
         __syncthreads();
