@@ -488,7 +488,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   // Flux / spectrum waves finalize their own tiles (one launch per level).  Wave w reads its active
   // count from fz3[w % 3], appends survivors to fz3[(w + 1) % 3] and zeroes fz3[(w + 2) % 3] for the
   // wave after; it takes units from fw[w % 2] and zeroes fw[(w + 1) % 2].
-  const bool fused = !rq.power_density;
+  const bool fused = !rq.power_density || mixed;  // the FP64 power density keeps its finalize kernel
   unsigned* fz3 = nullptr;
   unsigned long long* fw = nullptr;
   if (fused) {
@@ -529,6 +529,34 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     const unsigned* nact_in = first ? nullptr : (fused ? fz3 + wv % 3 : cnt + cur_list);
     unsigned* n_next = fused ? fz3 + (wv + 1) % 3 : cnt + (cur_list ^ 1);
     if (!fused) check(cudaMemsetAsync(n_next, 0, sizeof(unsigned), st), "memset");
+    if (fused && rq.power_density) {
+      PdWaveArgs w{};
+      w.lev = reinterpret_cast<const double*>(mrec_.p);
+      w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
+      w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
+      w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
+      w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = fw + wv % 2;
+      w.fused = 1;
+      w.tile_done = fz3 + 16;
+      w.zero_u32 = fz3 + (wv + 2) % 3;
+      w.zero_u64 = fw + (wv + 1) % 2;
+      PdFinalArgs& f = w.fin;
+      f.part = part_.as<double>(); f.first = first; f.level = L; f.max_level = lstop; f.quantity = o.quantity;
+      f.directional = rq.directional; f.tile_entries = tile; f.min_span = min_span; f.target_units = target;
+      f.dt_prev = L >= 1 ? dt_inclusive(tstart_, tstop_, L - 1) : 0; f.dt_level = dt_inclusive(tstart_, tstop_, L);
+      f.precision = o.precision; f.scale = scale; f.weight = weight; f.two_over_gamma = 2. / P.gamma;
+      f.bdmax_levels = reinterpret_cast<const double*>(mrec_bd_.p);
+      f.n_items = N; f.act = act_in; f.n_act = nact_in; f.state = state_.as<double>();
+      f.act_next = act_[cur_list ^ 1].as<int>(); f.n_next = n_next;
+      f.out = d_out; f.level_out = d_lvl; f.not_converged = c64; f.samples = c64 + 1; f.level_max = level_max;
+      f.work_reset = nullptr;
+      auto ev = timed_begin(st);
+      check(launch_pd_wave_mixed(w, frame_, grid_for(L), st), "power density wave (mixed)");
+      timed_end(ev, st);
+      last_launches += 1;
+      cur_list ^= 1;
+      return;
+    }
     if (fused) {
       FdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();

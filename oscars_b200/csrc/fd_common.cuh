@@ -370,6 +370,82 @@ __device__ __forceinline__ void finalize_bookkeeping(bool finished, bool unconve
   if (survive) act_next[base + __popc(sur & ((1u << lane32) - 1u))] = (int)item;
 }
 
+// One power-density entry after its sum up to level L (src/OSCARSSR.cc:2924-2952): finish it
+// (converged or last level) or keep its state.
+__device__ __forceinline__ void pd_entry_decide(const PdFinalArgs& A, int64_t item, double sum, double last_sum,
+                                                bool& finished, bool& unconverged, bool& survive) {
+  const int L = A.level;
+  const int64_t N = A.n_items;
+  const double this_sum = sum * A.dt_level;
+  double prec = fabs(this_sum - last_sum) / last_sum;
+  const double bd = A.bdmax_levels[L];
+  int result_level = -1;
+  bool stop = false;
+  if ((L > 8 && prec < A.precision && bd < A.two_over_gamma) || (L > 8 && bd < A.two_over_gamma && this_sum == last_sum)) {
+    stop = true;
+    result_level = L;
+  } else if (L > 8 && this_sum == last_sum) {
+    stop = true;
+    result_level = L;
+    prec = 0;
+  }
+  if (stop || L >= A.max_level) {
+    double sv = sum * (A.scale * A.dt_level);
+    sv /= 1e6;
+    if (!A.directional && sv < 0) sv *= -1;
+    double v;
+    if (A.quantity == 1) v = prec * A.weight;
+    else if (A.quantity == 2) v = (double)result_level * A.weight;
+    else v = sv * A.weight;
+    A.out[item] = v;
+    if (A.level_out) A.level_out[item] = result_level;
+    finished = true;
+    unconverged = !stop;
+  } else {
+    A.state[item] = sum;
+    A.state[N + item] = this_sum;
+    survive = true;
+  }
+}
+
+// Fused finalize of one tile of the mixed power-density wave by warp 0 (TE entries, 32 at a time):
+// each entry's span partials summed in span order from the tile-major layout
+// [tile][segment][span][entry in tile], the stop rule of pd_entry_decide, survivors appended.
+__device__ __forceinline__ void pd_tile_finalize(const PdFinalArgs& A, const WavePlan& P, int64_t tile, int64_t n_act,
+                                                 int TE) {
+  if (threadIdx.x >= 32) return;
+  const int64_t N = A.n_items;
+  for (int q0 = 0; q0 < TE; q0 += 32) {
+    const int q = q0 + (int)threadIdx.x;
+    const int64_t slot = tile * TE + q;
+    const bool live = q < TE && slot < n_act;
+    const int64_t item = live ? (A.act ? (int64_t)A.act[slot] : slot) : 0;
+    auto seg_sum = [&](int g) {
+      double t = 0;
+      for (int sp = 0; sp < P.spans; ++sp) t += __ldcg(A.part + ((tile * P.nseg + g) * P.spans + sp) * TE + q);
+      return t;
+    };
+    bool finished = false, unconverged = false, survive = false;
+    if (live) {
+      double sum = 0, last_sum = -1;
+      if (A.first) {
+        if (P.nseg == 2) {
+          sum += seg_sum(0);
+          last_sum = sum * A.dt_prev;
+        }
+        sum += seg_sum(P.nseg - 1);
+      } else {
+        sum = A.state[item];
+        last_sum = A.state[N + item];
+        sum += seg_sum(0);
+      }
+      pd_entry_decide(A, item, sum, last_sum, finished, unconverged, survive);
+    }
+    finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged,
+                         A.samples, A.level_max);
+  }
+}
+
 // One entry after its sum S up to level L: finish it (converged or last level) or keep its state.
 __device__ __forceinline__ void fd_entry_decide(const FdFinalArgs& A, int64_t item, const C3& S, double last_mag,
                                                 double dmax, bool& finished, bool& unconverged, bool& survive) {

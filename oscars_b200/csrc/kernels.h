@@ -110,22 +110,6 @@ struct FdWaveArgs {
   FdFinalArgs fin;
 };
 
-struct PdWaveArgs {
-  const double* lev;
-  int64_t cap;
-  const double* obs;
-  const double* normals;
-  int has_normal, directional;
-  int64_t n_items;
-  const int* act;
-  const unsigned* n_act;
-  int first, level, tile_entries, min_span;
-  int64_t target_units;
-  double* part;             // partials, entry-major: [slot][seg][span]
-  unsigned* err;
-  unsigned long long* work;
-};
-
 struct PdFinalArgs {
   const double* part;
   int first, level, max_level, quantity, directional, tile_entries, min_span;
@@ -144,6 +128,30 @@ struct PdFinalArgs {
   unsigned long long* samples;
   unsigned long long* work_reset;
   unsigned* level_max;      // highest level at which an entry finished (may be NULL)
+};
+
+struct PdWaveArgs {
+  const double* lev;
+  int64_t cap;
+  const double* obs;
+  const double* normals;
+  int has_normal, directional;
+  int64_t n_items;
+  const int* act;
+  const unsigned* n_act;
+  int first, level, tile_entries, min_span;
+  int64_t target_units;
+  double* part;             // partials, entry-major: [slot][seg][span]; fused: [tile][seg][span][entry in tile]
+  unsigned* err;
+  unsigned long long* work;
+  // Fused finalize (the mixed kernel): the last CTA to finish a tile's spans applies the stop rule of
+  // `fin` to the tile's entries and appends survivors; zero_u32 / zero_u64 are the counters of the
+  // following wave, zeroed by block 0 at start.
+  int fused;
+  unsigned* tile_done;
+  unsigned* zero_u32;
+  unsigned long long* zero_u64;
+  PdFinalArgs fin;
 };
 
 // One level of the STL power density (kernels_stl.cu): one CTA per facet not yet done.

@@ -494,39 +494,7 @@ __global__ void k_pd_finalize(PdFinalArgs A) {
     sum += seg_sum(0);
   }
   bool finished = false, unconverged = false, survive = false;
-  if (live && lane == 0) {
-    const int L = A.level;
-    const double this_sum = sum * A.dt_level;
-    double prec = fabs(this_sum - last_sum) / last_sum;
-    const double bd = A.bdmax_levels[L];
-    int result_level = -1;
-    bool stop = false;
-    if ((L > 8 && prec < A.precision && bd < A.two_over_gamma) || (L > 8 && bd < A.two_over_gamma && this_sum == last_sum)) {
-      stop = true;
-      result_level = L;
-    } else if (L > 8 && this_sum == last_sum) {
-      stop = true;
-      result_level = L;
-      prec = 0;
-    }
-    if (stop || L >= A.max_level) {
-      double sv = sum * (A.scale * A.dt_level);
-      sv /= 1e6;
-      if (!A.directional && sv < 0) sv *= -1;
-      double v;
-      if (A.quantity == 1) v = prec * A.weight;
-      else if (A.quantity == 2) v = (double)result_level * A.weight;
-      else v = sv * A.weight;
-      A.out[item] = v;
-      if (A.level_out) A.level_out[item] = result_level;
-      finished = true;
-      unconverged = !stop;
-    } else {
-      A.state[item] = sum;
-      A.state[N + item] = this_sum;
-      survive = true;
-    }
-  }
+  if (live && lane == 0) pd_entry_decide(A, item, sum, last_sum, finished, unconverged, survive);
   finalize_bookkeeping(finished, unconverged, survive, item, A.level, A.act_next, A.n_next, A.not_converged, A.samples,
                        A.level_max);
 }

@@ -312,8 +312,13 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_pd_wave_mixed(PdWaveArgs A
   __shared__ double red[SUB > 1 ? SUB - 1 : 1][TE];
   __shared__ WavePlan P;
   __shared__ int64_t next_unit;
+  __shared__ int s_last;
   const int tid = threadIdx.x;
   const int grp = tid / TE, q = tid % TE;
+  if (A.fused && blockIdx.x == 0 && tid == 0) {  // counters of the following wave
+    if (A.zero_u32) *A.zero_u32 = 0;
+    if (A.zero_u64) *A.zero_u64 = 0;
+  }
   const int64_t n_act = A.act ? (int64_t)*A.n_act : A.n_items;
   if (tid == 0) {
     P = wave_plan(A.first, A.level, n_act, TE, A.target_units, A.min_span);
@@ -386,14 +391,32 @@ __global__ void __launch_bounds__(kMxThreads, MINB) k_pd_wave_mixed(PdWaveArgs A
         }
         __syncthreads();  // everyone is done with `buf` before it is refilled
       }
-      // reduce the groups' sums in group order; group 0 stores the span's partial (entry-major)
+      // reduce the groups' sums in group order; group 0 stores the span's partial (entry-major, or
+      // tile-major for the fused finalize)
       if (SUB > 1 && grp > 0) red[grp - 1][q] = S;
       if (SUB > 1) __syncthreads();
       if (grp == 0) {
         for (int o2 = 0; o2 < SUB - 1; ++o2) S += red[o2][q];
-        if (live) A.part[slot * P.nseg * P.spans + g * P.spans + span] = S;
+        if (live) {
+          if (A.fused) A.part[((tile * P.nseg + g) * P.spans + span) * TE + q] = S;
+          else A.part[slot * P.nseg * P.spans + g * P.spans + span] = S;
+        }
       }
       if (SUB > 1) __syncthreads();
+    }
+    if (A.fused) {  // the CTA that finishes a tile's last span finalizes the tile
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) {
+        const unsigned done = atomicAdd(&A.tile_done[tile], 1u);
+        s_last = done == (unsigned)(P.spans - 1);
+        if (s_last) __threadfence();
+      }
+      __syncthreads();
+      if (s_last) {
+        pd_tile_finalize(A.fin, P, tile, n_act, TE);
+        if (tid == 0) A.tile_done[tile] = 0;
+      }
     }
   }
 }
