@@ -7,7 +7,7 @@ in device memory like the memory levels, up to level 27 (past the reference's me
   mixed path against FP64 at 1e-4;
 * the level cache switching between the memory grid and an extended split on one object (flux and
   power density), each result against its golden fixture;
-* the mixed path on extended levels against FP64 at a fixed level;
+* the mixed path on extended levels against FP64 at a fixed level, and the mixed power density;
 * a level above 30 refused.
 The golden extended-level cases (flux_und_extended, spec_und_extended, pd_und_extended) also run in
 test_gpu_parity.py and through the reference's own seam in test_gpu_seam.py.
@@ -83,6 +83,21 @@ def test_mixed_extended_levels_against_fp64():
     _, f = _flat(run_case(_sr(), calls))
     _, m = _flat(run_case(_sr(), _with(calls, compute="mixed")))
     assert _peak_rel(m, f) <= TOL_MIXED, _peak_rel(m, f)
+
+
+def test_mixed_power_density_on_extended_levels():
+    """The mixed power density on an extended split (levels 10..12 on their own grid): the records and
+    their beta-difference maxima follow the split, so values match FP64 and the stop levels agree."""
+    name = "pd_und_extended"
+    last, kw = CASES[name][-1]
+    out = {}
+    for compute in ("fp64", "mixed"):
+        s = _sr()
+        run_case(s, CASES[name][:-1])
+        out[compute] = (_flat(getattr(s, last)(**dict(kw, gpu=1, compute=compute)))[1],
+                        _flat(getattr(s, last)(**dict(kw, gpu=1, compute=compute, quantity="level")))[1])
+    assert _peak_rel(out["mixed"][0], out["fp64"][0]) <= TOL_MIXED
+    assert np.mean(out["mixed"][1] == out["fp64"][1]) >= 0.97
 
 
 def test_level_above_30_refused():
