@@ -765,6 +765,10 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
                 "ms_per_step": dev_ms / steps, "gpu_launches_per_step": launches // steps}
     run(fp64_particles, "fp64")
     _, ms64, sm64, _, w64 = _profiled(s._ctx, lambda: run(fp64_particles, "fp64"))
+    # the same particles in mixed precision: below the batch threshold they take the per-particle
+    # route (host trajectories, single-trajectory mixed kernels), timed like the FP64 path's kernels
+    run(fp64_particles, "mixed")
+    _, ms_mx, sm_mx, _, w_mx = _profiled(s._ctx, lambda: run(fp64_particles, "mixed"))
     a = run(check_particles, "mixed", precision=0, max_level=check_level)[1]
     b = run(check_particles, "fp64", precision=0, max_level=check_level)[1]
     mixed_e2e = samples / wall / 1e9
@@ -791,6 +795,13 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
                      "path": "sr.calculate_flux_rectangle(nparticles=%d, compute='fp64') (reference method: host RK4 "
                              "per particle, FP64 sums); value = device time of its sample-sum kernels" % fp64_particles},
             "mixed_over_fp64": mixed_dev / fp64_dev, "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
+            "same_particles": {"particles": fp64_particles, "mixed_value": sm_mx / (ms_mx * 1e-3) / 1e9,
+                               "mixed_e2e": sm_mx / w_mx / 1e9, "fp64_value": fp64_dev, "fp64_e2e": fp64_e2e,
+                               "mixed_over_fp64": (sm_mx / ms_mx) / (sm64 / ms64),
+                               "mixed_over_fp64_e2e": (sm_mx / w_mx) / (sm64 / w64),
+                               "path": "the same %d particles through sr.calculate_flux_rectangle, mixed and FP64 "
+                                       "(both per particle: host trajectories on worker threads); device time of the "
+                                       "sample-sum kernels" % fp64_particles},
             "mixed_vs_fp64_peak_rel_err": {"value": _peak_err(a, b), "particles": check_particles,
                                            "fixed_level": check_level},
             "cpu_reference": cpu, "clocks": clk.summary()}

@@ -388,6 +388,13 @@ OSC_API int osc_get_variant(osc_ctx* ctx, int kind, int* variant, int* n_variant
  * (e.g. "k_fd_wave_mixed_pair<4,4>"), NUL-terminated into name[capacity].  No context; errors go
  * to osc_last_error(NULL).  No counterpart in the reference (it has one kernel per quantity). */
 OSC_API int osc_variant_name(int kind, int variant, char* name, long long capacity);
+/* Multi-particle compute='mixed' flux / spectrum requests whose share of particles reaches
+ * `particles` (default 1024) run as one batch with device RK4 trajectories (the route of
+ * osc_batch_flux); smaller ones integrate each particle's trajectory on host worker threads and sum
+ * it with the single-trajectory mixed kernels, as the FP64 path does.  Both routes give the same
+ * results to rounding; 1 forces the batch, a large value the per-particle route.  No counterpart in
+ * the reference. */
+OSC_API int osc_set_beam_batch_threshold(osc_ctx* ctx, int particles);
 /* Drop the device-side level-sample cache (it is rebuilt by the next radiation call). */
 OSC_API int osc_drop_level_cache(osc_ctx* ctx);
 /* Measured arithmetic peak of this GPU: an FMA-throughput loop in FP64 (kind 0) or FP32 (kind 1),

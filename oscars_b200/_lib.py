@@ -100,6 +100,7 @@ SIGNATURES = {
     "osc_flux_vjp": (I, [VP, DP, LL, DP, LL, I, ctypes.POINTER(RadOpts), I, DP, DP, DP, LL, DP]),
     "osc_last_stats": (I, [VP, LLP, LLP]),
     "osc_set_profiling": (I, [VP, I]),
+    "osc_set_beam_batch_threshold": (I, [VP, I]),
     "osc_get_profile": (I, [VP, DP, LLP, LLP, I]),
     "osc_set_variant": (I, [VP, I, I]),
     "osc_get_variant": (I, [VP, I, ctypes.POINTER(I), ctypes.POINTER(I)]),

@@ -837,6 +837,13 @@ OSC_API int osc_last_stats(osc_ctx* ctx, long long* samples, long long* launches
   });
 }
 
+OSC_API int osc_set_beam_batch_threshold(osc_ctx* ctx, int particles) {
+  return guarded(ctx, [&] {
+    if (particles < 1) throw osc::Error{OSC_ERR_RANGE, "the threshold must be at least 1 particle"};
+    ctx->eng->beam_batch_min = particles;
+  });
+}
+
 OSC_API int osc_set_profiling(osc_ctx* ctx, int enable) {
   return guarded(ctx, [&] { ctx->eng->profiling = enable != 0; });
 }

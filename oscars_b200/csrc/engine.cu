@@ -888,9 +888,16 @@ void Engine::radiation(RadRequest& rq) {
   if (!d_lvl) d_lvl = lvl_.as<int32_t>();
 
   const int np = rq.opts.nparticles;
-  // mixed multi-particle requests integrate their trajectories with the device RK4; with RKAS selected
-  // each particle's trajectory comes from the host integrator like the FP64 path's
-  if (np > 0 && rq.opts.precision_mode == OSC_MIXED && !rq.power_density && model.traj_method == Model::kRK4) {
+  // Mixed multi-particle flux / spectrum requests with at least beam_batch_min particles (this
+  // process's share) run as one batch with device RK4 trajectories; smaller ones, and those with RKAS
+  // trajectories, take the host integrator on worker threads like the FP64 path: the device RK4 is a
+  // serial chain per particle (~4 us per step, ~60 ms for 16001 points whatever the batch size), which
+  // only pays once the batch is large.
+  const int shard_n = rq.opts.shard_count > 1 ? rq.opts.shard_count : 1;
+  const int shard_r = shard_n > 1 ? rq.opts.shard_rank % shard_n : 0;
+  const int np_local = np > shard_r ? (np - shard_r + shard_n - 1) / shard_n : 0;
+  if (np > 0 && rq.opts.precision_mode == OSC_MIXED && !rq.power_density && model.traj_method == Model::kRK4 &&
+      np_local >= beam_batch_min) {
     radiation_beam_mixed(rq, N);
     return;
   }

@@ -114,6 +114,9 @@ class Engine {
   void power_density_stl(const double* tri, const double* centers, int64_t n, const osc_rad_opts& o, double* out,
                          int32_t* level_out);
   bool use_graphs = true;            // replay the batched front of a known shape as a CUDA graph
+  // particles (this process's share) from which a mixed multi-particle request runs as one batch
+  // with device trajectories instead of host trajectories and per-particle sums
+  int beam_batch_min = 1024;
   long long graph_launches() const { return graph_launches_; }
 
   // profiling of the sample-integration kernels

@@ -4,7 +4,9 @@ Tolerance as for the single-trajectory mixed path: peak-normalised relative erro
 max_i |F_i - F64_i| / max_i |F64_i| <= 1e-4 against the FP64 GPU path, at a fixed level
 (precision=0, max_level=L) so that both integrate the same samples.  The FP64 path matches the
 reference CPU path to <= 1e-9 (test_gpu_parity.py).  In the batch, trajectories, splines and level
-samples are computed on the device, so these tests also cover those kernels.
+samples are computed on the device, so these tests also cover those kernels.  Multi-particle mixed
+requests run as a batch from a threshold of particles on (osc_set_beam_batch_threshold) and per
+particle with host trajectories below it: the beam tests run both routes.
 """
 import math
 
@@ -15,6 +17,16 @@ from cases import BEAM_GAUSS, E1_EPU, EPU_X, EPU_Y, UND_SETUP, run_case, traj
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-4
+
+
+ROUTES = {"batch": 1, "per_particle": 1 << 30}  # osc_set_beam_batch_threshold for each route
+
+
+def _sr_route(route):
+    from oscars_b200.sr import sr
+    s = sr(gpu=1)
+    s._ctx.call("osc_set_beam_batch_threshold", ROUTES[route])
+    return s
 
 
 def _err(a, ref):
@@ -124,15 +136,15 @@ def test_batch_spectrum_job_matches_sr_spectrum():
     assert _err(out, ref) <= TOL
 
 
+@pytest.mark.parametrize("route", sorted(ROUTES))
 @pytest.mark.parametrize("nparticles", [1, 6])
-def test_beam_mixed_matches_fp64_fixed_level(nparticles):
-    from oscars_b200.sr import sr
+def test_beam_mixed_matches_fp64_fixed_level(nparticles, route):
     setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=17))]
     kw = dict(energy_eV=E1_EPU, npoints=[21, 21], width=[0.008, 0.008], translation=[0, 0, 30],
               nparticles=nparticles, precision=0, max_level=11)
     out = {}
     for compute in ("fp64", "mixed"):
-        s = sr(gpu=1)
+        s = _sr_route(route)
         run_case(s, setup)
         out[compute] = np.array([v[1] for v in s.calculate_flux_rectangle(**dict(kw, compute=compute))])
     e = _err(out["mixed"], out["fp64"])
@@ -140,16 +152,17 @@ def test_beam_mixed_matches_fp64_fixed_level(nparticles):
     assert e <= TOL
 
 
-def test_epu_beam_101x101_64_particles_fixed_level():
+@pytest.mark.parametrize("route", sorted(ROUTES))
+def test_epu_beam_101x101_64_particles_fixed_level(route):
     """The multi-particle EPU configuration on its full 101 x 101 grid (8 mm at 30 m, E1) with a
-    64-particle subset of the beam, device trajectories (mixed) against host RK4 (FP64)."""
-    from oscars_b200.sr import sr
+    64-particle subset of the beam, mixed (device trajectories in the batch route, host ones per
+    particle) against host RK4 (FP64)."""
     setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=42))]
     kw = dict(energy_eV=E1_EPU, npoints=[101, 101], width=[0.008, 0.008], translation=[0, 0, 30],
               nparticles=64, precision=0, max_level=12)
     out = {}
     for compute in ("fp64", "mixed"):
-        s = sr(gpu=1)
+        s = _sr_route(route)
         run_case(s, setup)
         out[compute] = np.array([v[1] for v in s.calculate_flux_rectangle(**dict(kw, compute=compute))])
     e = _err(out["mixed"], out["fp64"])
@@ -157,15 +170,15 @@ def test_epu_beam_101x101_64_particles_fixed_level():
     assert e <= TOL
 
 
-def test_beam_mixed_polarized_and_spectrum():
-    from oscars_b200.sr import sr
+@pytest.mark.parametrize("route", sorted(ROUTES))
+def test_beam_mixed_polarized_and_spectrum(route):
     setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=2))]
     for call, kw in (("calculate_flux_rectangle", dict(energy_eV=E1_EPU, npoints=[11, 11], width=[0.006, 0.006],
                                                        translation=[0, 0, 30], polarization="cl")),
                      ("calculate_spectrum", dict(obs=[0.0005, 0, 30], energy_range_eV=[150, 220], npoints=24))):
         out = {}
         for compute in ("fp64", "mixed"):
-            s = sr(gpu=1)
+            s = _sr_route(route)
             run_case(s, setup)
             out[compute] = np.array([v[1] for v in getattr(s, call)(**dict(kw, nparticles=3, precision=0,
                                                                              max_level=11, compute=compute))])
@@ -203,19 +216,19 @@ def test_batch_grid_and_halfscale_fields_match_fp64():
         assert e <= TOL
 
 
-@pytest.mark.parametrize("compute,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
-def test_particle_shards_add_up_to_the_whole_request(compute, tol):
+@pytest.mark.parametrize("compute,tol,route", [("fp64", 1e-12, "per_particle"), ("mixed", 1e-6, "per_particle"),
+                                               ("mixed", 1e-6, "batch")])
+def test_particle_shards_add_up_to_the_whole_request(compute, tol, route):
     """shard=(rank, count): each share integrates particles rank, rank + count, ... with weight 1/N."""
-    from oscars_b200.sr import sr
     setup = [EPU_Y, EPU_X, BEAM_GAUSS] + traj(16001) + [("set_seed", dict(seed=5))]
     kw = dict(energy_eV=E1_EPU, npoints=[9, 9], width=[0.006, 0.006], translation=[0, 0, 30], nparticles=7,
               precision=0, max_level=10, compute=compute, return_numpy=True)
-    s = sr(gpu=1)
+    s = _sr_route(route)
     run_case(s, setup)
     whole = s.calculate_flux_rectangle(**kw)[1]
     total = np.zeros_like(whole)
     for r in range(3):
-        t = sr(gpu=1)
+        t = _sr_route(route)
         run_case(t, setup)
         total += t.calculate_flux_rectangle(shard=(r, 3), **kw)[1]
     assert _err(total, whole) <= tol
