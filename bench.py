@@ -744,6 +744,7 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
     from oscars_b200.sr import sr
     s = sr(gpu=1, device=local)
     setup_epu_beam(s)
+    s._ctx.call("osc_set_beam_batch_threshold", 1)  # the batched route whatever the particle count
     kw = dict(energy_eV=E1_EPU, npoints=[101, 101], width=[0.008, 0.008], translation=[0, 0, 30], return_numpy=True)
 
     def run(np_, compute, **extra):
@@ -765,10 +766,13 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
                 "ms_per_step": dev_ms / steps, "gpu_launches_per_step": launches // steps}
     run(fp64_particles, "fp64")
     _, ms64, sm64, _, w64 = _profiled(s._ctx, lambda: run(fp64_particles, "fp64"))
-    # the same particles in mixed precision: below the batch threshold they take the per-particle
-    # route (host trajectories, single-trajectory mixed kernels), timed like the FP64 path's kernels
+    # the same particles in mixed precision on the per-particle route (host trajectories,
+    # single-trajectory mixed kernels), the route below the default batch threshold, timed like the
+    # FP64 path's kernels
+    s._ctx.call("osc_set_beam_batch_threshold", 1 << 30)
     run(fp64_particles, "mixed")
     _, ms_mx, sm_mx, _, w_mx = _profiled(s._ctx, lambda: run(fp64_particles, "mixed"))
+    s._ctx.call("osc_set_beam_batch_threshold", 1)
     a = run(check_particles, "mixed", precision=0, max_level=check_level)[1]
     b = run(check_particles, "fp64", precision=0, max_level=check_level)[1]
     mixed_e2e = samples / wall / 1e9
@@ -871,6 +875,7 @@ def sharded_beam_leg(steps, warmup, local, rank, world):
     from oscars_b200.sr import sr
     s = sr(gpu=1, device=local)
     setup_epu_beam(s)
+    s._ctx.call("osc_set_beam_batch_threshold", 1)  # each rank's share runs batched
     kw = dict(energy_eV=E1_EPU, npoints=[101, 101], width=[0.008, 0.008], translation=[0, 0, 30], return_numpy=True,
               nparticles=BEAM_PARTICLES, compute="mixed", shard=(rank, world))
 
