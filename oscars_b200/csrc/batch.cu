@@ -131,51 +131,25 @@ __device__ void grid_field_d(const DevField& f, const double* __restrict__ vals,
   B[2] += F[2] * w;
 }
 
-// Undulator or EPU field i (its value, not yet added): the pole blocks are independent (the second
-// block's term is formed on its own and added, which is the sum the sequential accumulation forms),
-// so their sines can overlap.
-__device__ __forceinline__ void ideal_field_d(const DevField& f, const double* __restrict__ vals, double x, double y,
-                                              double z, double t, double* F) {
-  const double d = (x - f.center[0]) * f.period_unit[0] + (y - f.center[1]) * f.period_unit[1] +
-                   (z - f.center[2]) * f.period_unit[2];
-  const double tc = 1 + d * f.taper;
-  double FA[3] = {0, 0, 0}, FB[3] = {0, 0, 0};
-  pole_block_d(f, vals, f.a, d, f.shift[0], tc, FA);
-  if (f.kind == 1) pole_block_d(f, vals, f.b, d, f.shift[1], tc, FB);  // EPU (src/TField3D_IdealEPU.cc:127-165)
-  const double w = f.frequency == 0 ? 1.0 : cos(2.0 * kPiD * f.frequency * (t + f.time_offset) + f.frequency_phase);
-  F[0] = (FA[0] + FB[0]) * w;
-  F[1] = (FA[1] + FB[1]) * w;
-  F[2] = (FA[2] + FB[2]) * w;
-}
-
 __device__ void field_sum_d(const DevField* __restrict__ fs, int nf, const double* __restrict__ vals, double x,
                             double y, double z, double t, double* B) {
   B[0] = B[1] = B[2] = 0;
-  int i = 0;
-  // two ideal fields at a time: their evaluations are independent and interleave; the sum is formed
-  // in field order as before
-  for (; i + 1 < nf && fs[i].kind != 2 && fs[i + 1].kind != 2; i += 2) {
-    double F0[3], F1[3];
-    ideal_field_d(fs[i], vals, x, y, z, t, F0);
-    ideal_field_d(fs[i + 1], vals, x, y, z, t, F1);
-    B[0] += F0[0];
-    B[1] += F0[1];
-    B[2] += F0[2];
-    B[0] += F1[0];
-    B[1] += F1[1];
-    B[2] += F1[2];
-  }
-  for (; i < nf; ++i) {
+  for (int i = 0; i < nf; ++i) {
     const DevField& f = fs[i];
     if (f.kind == 2) {
       grid_field_d(f, vals, x, y, z, t, B);
       continue;
     }
-    double F[3];
-    ideal_field_d(f, vals, x, y, z, t, F);
-    B[0] += F[0];
-    B[1] += F[1];
-    B[2] += F[2];
+    const double d = (x - f.center[0]) * f.period_unit[0] + (y - f.center[1]) * f.period_unit[1] +
+                     (z - f.center[2]) * f.period_unit[2];
+    const double tc = 1 + d * f.taper;
+    double F[3] = {0, 0, 0};
+    pole_block_d(f, vals, f.a, d, f.shift[0], tc, F);
+    if (f.kind == 1) pole_block_d(f, vals, f.b, d, f.shift[1], tc, F);  // EPU (src/TField3D_IdealEPU.cc:127-165)
+    const double w = f.frequency == 0 ? 1.0 : cos(2.0 * kPiD * f.frequency * (t + f.time_offset) + f.frequency_phase);
+    B[0] += F[0] * w;
+    B[1] += F[1] * w;
+    B[2] += F[2] * w;
   }
 }
 
