@@ -737,8 +737,8 @@ def tuning_cpu_reference(every=16, h=1e-3):
 def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, check_level=12, particles=BEAM_PARTICLES,
              quick=False):
     """EPU beam, 10k particles: mixed (batched) timed on the device and end to end; FP64 (reference
-    path, host RK4 per particle) end to end on the first `fp64_particles`; mixed vs FP64 error at a
-    fixed level on `check_particles`.  `particles` < 10000 and `quick` (the mixed timing alone) give
+    path, host RK4 per particle) on the whole beam; both routes on the first `fp64_particles`; mixed
+    vs FP64 error at a fixed level on `check_particles`.  `particles` < 10000 and `quick` (the mixed timing alone) give
     the small cases of profiler runs."""
     import numpy as np
     from oscars_b200.sr import sr
@@ -766,6 +766,8 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
                 "ms_per_step": dev_ms / steps, "gpu_launches_per_step": launches // steps}
     run(fp64_particles, "fp64")
     _, ms64, sm64, _, w64 = _profiled(s._ctx, lambda: run(fp64_particles, "fp64"))
+    # the FP64 path on the whole beam (the same work as the mixed batch)
+    _, ms64a, sm64a, _, w64a = _profiled(s._ctx, lambda: run(particles, "fp64"))
     # the same particles in mixed precision on the per-particle route (host trajectories,
     # single-trajectory mixed kernels), the route below the default batch threshold, timed like the
     # FP64 path's kernels
@@ -776,8 +778,8 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
     a = run(check_particles, "mixed", precision=0, max_level=check_level)[1]
     b = run(check_particles, "fp64", precision=0, max_level=check_level)[1]
     mixed_e2e = samples / wall / 1e9
-    fp64_e2e = sm64 / w64 / 1e9
-    fp64_dev = sm64 / (ms64 * 1e-3) / 1e9
+    fp64_e2e = sm64a / w64a / 1e9
+    fp64_dev = sm64a / (ms64a * 1e-3) / 1e9
     mixed_dev = samples / (dev_ms * 1e-3) / 1e9
     # the reference CPU path on the first cpu_particles particles (the FP64 GPU path's stop levels --
     # identical to the reference's -- count their samples)
@@ -795,12 +797,15 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
             "samples_per_step": samples // steps, "gpu_launches_per_step": launches // steps,
             "e2e": {"value": mixed_e2e, "unit": "Gsamples/s", "wall_s_per_step": wall / steps,
                     "path": "sr.calculate_flux_rectangle(nparticles=10000, compute='mixed', return_numpy=True)"},
-            "fp64": {"value": fp64_dev, "e2e": fp64_e2e, "unit": "Gsamples/s", "particles": fp64_particles,
+            "fp64": {"value": fp64_dev, "e2e": fp64_e2e, "unit": "Gsamples/s", "particles": particles,
                      "path": "sr.calculate_flux_rectangle(nparticles=%d, compute='fp64') (reference method: host RK4 "
-                             "per particle, FP64 sums); value = device time of its sample-sum kernels" % fp64_particles},
+                             "per particle on worker threads, FP64 sums); value = device time of its sample-sum "
+                             "kernels (the mixed value counts the whole batch, device trajectories included)"
+                             % particles},
             "mixed_over_fp64": mixed_dev / fp64_dev, "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
             "same_particles": {"particles": fp64_particles, "mixed_value": sm_mx / (ms_mx * 1e-3) / 1e9,
-                               "mixed_e2e": sm_mx / w_mx / 1e9, "fp64_value": fp64_dev, "fp64_e2e": fp64_e2e,
+                               "mixed_e2e": sm_mx / w_mx / 1e9, "fp64_value": sm64 / (ms64 * 1e-3) / 1e9,
+                               "fp64_e2e": sm64 / w64 / 1e9,
                                "mixed_over_fp64": (sm_mx / ms_mx) / (sm64 / ms64),
                                "mixed_over_fp64_e2e": (sm_mx / w_mx) / (sm64 / w64),
                                "path": "the same %d particles through sr.calculate_flux_rectangle, mixed and FP64 "
@@ -813,8 +818,8 @@ def beam_leg(steps, warmup, local=0, fp64_particles=32, check_particles=16, chec
 
 def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12, n_jobs=UNEVEN_JOBS, quick=False):
     """512 uneven jobs through osc_batch_flux: mixed timed on the device and end to end; FP64 (jobs
-    one after another through the FP64 path) end to end on the first `fp64_jobs`; mixed vs FP64 error
-    at a fixed level on those jobs.  `n_jobs` < 512 (the first jobs of the same sequence) and `quick`
+    one after another through the FP64 path) on the same jobs; mixed vs FP64 error at a fixed level on
+    the first `fp64_jobs`.  `n_jobs` < 512 (the first jobs of the same sequence) and `quick`
     (the mixed timing alone) give the small cases of profiler runs."""
     from oscars_b200.batch import BatchRunner
     jobs = uneven_jobs()[:n_jobs]
@@ -837,7 +842,7 @@ def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12, n_jobs=UNEV
     sub = jobs[:fp64_jobs]
     r.ctx.call("osc_set_variant", 0, 2)  # FP64 variant fixed: no per-shape tuning runs inside the timing
     r.flux(sub, compute="fp64")
-    _, ms64, sm64, _, w64 = _profiled(r.ctx, lambda: r.flux(sub, compute="fp64"))
+    _, ms64, sm64, _, w64 = _profiled(r.ctx, lambda: r.flux(jobs, compute="fp64"))  # all jobs: the same work
     a = r.flux(sub, compute="mixed", precision=0, max_level=check_level)
     b = r.flux(sub, compute="fp64", precision=0, max_level=check_level)
     err = max(_peak_err(x, y) for x, y in zip(a, b))
@@ -854,9 +859,10 @@ def uneven_leg(steps, warmup, local=0, fp64_jobs=32, check_level=12, n_jobs=UNEV
             "samples_per_step": samples // steps, "gpu_launches_per_step": launches // steps, "variant": variant,
             "e2e": {"value": mixed_e2e, "unit": "Gsamples/s", "wall_s_per_step": wall / steps,
                     "path": "oscars_b200.batch.BatchRunner.flux(jobs, compute='mixed')"},
-            "fp64": {"value": fp64_dev, "e2e": fp64_e2e, "unit": "Gsamples/s", "jobs": fp64_jobs,
-                     "path": "BatchRunner.flux(jobs[:%d], compute='fp64') (jobs one after another, host RK4); value = "
-                             "device time of its sample-sum kernels" % fp64_jobs},
+            "fp64": {"value": fp64_dev, "e2e": fp64_e2e, "unit": "Gsamples/s", "jobs": len(jobs),
+                     "path": "BatchRunner.flux(jobs, compute='fp64') (jobs one after another, host RK4); value = "
+                             "device time of its sample-sum kernels (the mixed value counts the whole batch, device "
+                             "trajectories included)"},
             "mixed_over_fp64": mixed_dev / fp64_dev, "mixed_over_fp64_e2e": mixed_e2e / fp64_e2e,
             "mixed_vs_fp64_peak_rel_err": {"value": err, "jobs": fp64_jobs, "fixed_level": check_level,
                                            "norm": "per job, max over jobs"},
