@@ -628,18 +628,36 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_batch_wave(BatchWaveArgs A)
 
 // Groups of kFinLanes lanes take the active entries of all jobs in act_start order (grid-stride;
 // the loop bound is block-uniform so every warp stays converged for its shuffles and ballots).
+// Lanes of a group summing one entry's spans (LANES = 1: one thread per entry, its spans in order).
+template <int LANES>
+__device__ __forceinline__ double lanes_sum(double v) {
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, LANES);
+  return v;
+}
+template <int LANES>
+__device__ __forceinline__ double lanes_max(double v) {
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o, LANES));
+  return v;
+}
+
+// Span reduction and stop rule of every active entry of the chunk.  LANES threads per entry; with one
+// (the launch below) a warp's 32 entries read their adjacent partial records together, which the
+// waves with one span per entry -- the large ones -- make contiguous.
+template <int LANES>
 __global__ void __launch_bounds__(256) k_batch_finalize(BatchFinalArgs A) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.work_reset = 0;
   const int64_t total = A.plan.act_start[A.njobs];
   const int spans = *A.plan.spans;
   const int L = A.level;
   const int nseg = (A.first && L >= 1) ? 2 : 1;
-  const int lane = threadIdx.x % kFinLanes;
+  const int lane = threadIdx.x % LANES;
   const unsigned full = 0xffffffffu;
   const int lane32 = threadIdx.x & 31;
-  const int64_t per_pass = (int64_t)gridDim.x * blockDim.x / kFinLanes;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x / kFinLanes; base < total; base += per_pass) {
-    const int64_t gidx = base + threadIdx.x / kFinLanes;
+  const int64_t per_pass = (int64_t)gridDim.x * blockDim.x / LANES;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x / LANES; base < total; base += per_pass) {
+    const int64_t gidx = base + threadIdx.x / LANES;
     const bool live = gidx < total;
     const int j = live ? find_job(A.plan.act_start, A.njobs, gidx) : 0;
     const DevJob& J = A.jobs[j];
@@ -651,15 +669,15 @@ __global__ void __launch_bounds__(256) k_batch_finalize(BatchFinalArgs A) {
       C3 t = {0, 0, 0, 0, 0, 0};
       double dm = 0;
       if (live) {
-        for (int sp = lane; sp < spans; sp += kFinLanes) {
+        for (int sp = lane; sp < spans; sp += LANES) {
           const double* p = pbase + (g * spans + sp) * kFdPartials;
           t.xr += p[0]; t.xi += p[1]; t.yr += p[2]; t.yi += p[3]; t.zr += p[4]; t.zi += p[5];
           if (p[8] >= 0) dm = fmax(dm, p[8]);  // the span maxima include the step into each span
         }
       }
-      s.xr += group_sum(t.xr); s.xi += group_sum(t.xi); s.yr += group_sum(t.yr);
-      s.yi += group_sum(t.yi); s.zr += group_sum(t.zr); s.zi += group_sum(t.zi);
-      dmax = fmax(dmax, group_max(dm));
+      s.xr += lanes_sum<LANES>(t.xr); s.xi += lanes_sum<LANES>(t.xi); s.yr += lanes_sum<LANES>(t.yr);
+      s.yi += lanes_sum<LANES>(t.yi); s.zr += lanes_sum<LANES>(t.zr); s.zi += lanes_sum<LANES>(t.zi);
+      dmax = fmax(dmax, lanes_max<LANES>(dm));
     };
     auto mag = [&](C3 v, double scale) {
       C3 t = c3_scale(v, scale);
@@ -1060,7 +1078,7 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
       f.precision = o.precision; f.n_entries = N; f.state = b_state_.as<double>();
       f.act_next = b_act_[cur ^ 1].as<int>(); f.cnt_next = cout; f.out = b_out_.as<double>();
       f.level_out = b_lvl_.as<int32_t>(); f.not_converged = m64; f.samples = m64 + 1; f.work_reset = m64 + 2;
-      dev::k_batch_finalize<<<sms * 8, 256, 0, st>>>(f);
+      dev::k_batch_finalize<1><<<sms * 8, 256, 0, st>>>(f);
       check(cudaGetLastError(), "batch finalize");
       last_launches += 3;
       cur ^= 1;
