@@ -395,6 +395,10 @@ OSC_API int osc_variant_name(int kind, int variant, char* name, long long capaci
  * results to rounding; 1 forces the batch, a large value the per-particle route.  No counterpart in
  * the reference. */
 OSC_API int osc_set_beam_batch_threshold(osc_ctx* ctx, int particles);
+/* Spline kernel of the batched trajectories: 0 (default) picks per chunk, 1 the serial sweeps (one
+ * thread per job and component: the latency of the longest trajectory), 2 the block-parallel sweeps
+ * (the chunk's total work).  Both solve the same system to rounding. */
+OSC_API int osc_set_batch_spline_kernel(osc_ctx* ctx, int kernel);
 /* Drop the device-side level-sample cache (it is rebuilt by the next radiation call). */
 OSC_API int osc_drop_level_cache(osc_ctx* ctx);
 /* Measured arithmetic peak of this GPU: an FMA-throughput loop in FP64 (kind 0) or FP32 (kind 1),

@@ -101,6 +101,7 @@ SIGNATURES = {
     "osc_last_stats": (I, [VP, LLP, LLP]),
     "osc_set_profiling": (I, [VP, I]),
     "osc_set_beam_batch_threshold": (I, [VP, I]),
+    "osc_set_batch_spline_kernel": (I, [VP, I]),
     "osc_get_profile": (I, [VP, DP, LLP, LLP, I]),
     "osc_set_variant": (I, [VP, I, I]),
     "osc_get_variant": (I, [VP, I, ctypes.POINTER(I), ctypes.POINTER(I)]),

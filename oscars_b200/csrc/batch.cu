@@ -242,6 +242,135 @@ __global__ void k_batch_rk4(const DevJob* __restrict__ jobs, int njobs, const De
   if (c.superluminal) atomicOr(err, kErrSuperluminal);
 }
 
+// The same clamped spline with each sweep split across the threads of a block (one block per job
+// and component).  Every sweep is a first-order recurrence: the factor yp_i = (sig_i - 1) /
+// (sig_i yp_{i-1} + 2) a Moebius map of yp_{i-1}, the right side u_i = (6 d_i - sig_i u_{i-1}) / p_i
+// and the back substitution ypp_k = yp_k ypp_{k+1} + u_k affine ones.  Each thread composes the maps
+// of its chunk of points, a block-wide inclusive scan of the chunk maps gives every chunk its entering
+// value, and each thread then runs its chunk with the reference's operations from that value.  The
+// maps contract (|d yp_i / d yp_{i-1}| < 1/4, |sig_i / p_i| < 1/2, |yp_k| < 1/2), so the entering
+// values' rounding does not grow along the chunk.
+constexpr int kSplThreads = 256;
+
+struct Mob { double a, b, c, d; };  // y -> (a y + b) / (c y + d)
+__device__ __forceinline__ Mob mob_then(Mob f, Mob g) {  // g(f(y)), scaled by its largest entry
+  Mob h{g.a * f.a + g.b * f.c, g.a * f.b + g.b * f.d, g.c * f.a + g.d * f.c, g.c * f.b + g.d * f.d};
+  const double m = fmax(fmax(fabs(h.a), fabs(h.b)), fmax(fabs(h.c), fabs(h.d)));
+  const double r = m > 0 ? 1.0 / m : 1.0;
+  return {h.a * r, h.b * r, h.c * r, h.d * r};
+}
+struct Aff { double a, b; };  // x -> a x + b
+__device__ __forceinline__ Aff aff_then(Aff f, Aff g) { return {g.a * f.a, g.a * f.b + g.b}; }
+
+// Inclusive block scan of the threads' maps (kSplThreads of them) in shared memory; returns the
+// composition of the maps of threads 0 .. t-1 (identity for thread 0).
+template <class M, class Then>
+__device__ __forceinline__ M block_prefix(M mine, M identity, M* sh, Then then) {
+  const int t = threadIdx.x;
+  sh[t] = mine;
+  __syncthreads();
+  for (int o = 1; o < kSplThreads; o <<= 1) {
+    M prev = identity;
+    if (t >= o) prev = sh[t - o];
+    __syncthreads();
+    if (t >= o) sh[t] = then(prev, sh[t]);
+    __syncthreads();
+  }
+  const M before = t > 0 ? sh[t - 1] : identity;
+  __syncthreads();
+  return before;
+}
+
+__global__ void __launch_bounds__(kSplThreads) k_batch_spline_scan(const DevJob* __restrict__ jobs,
+                                                                   double* __restrict__ arena,
+                                                                   double* __restrict__ work) {
+  __shared__ Mob shm[kSplThreads];
+  __shared__ Aff sha[kSplThreads];
+  const DevJob& J = jobs[blockIdx.x / 9];
+  const int c = blockIdx.x % 9;
+  const int t = threadIdx.x;
+  const int64_t n = (int64_t)J.nf + J.nb;
+  const double* X = arena + J.knots;
+  const double* Y = X + (1 + c) * n;
+  double* ypp = arena + J.knots + (10 + c) * n;
+  double* u = work + J.u_off + c * n;
+  auto sigma = [&](int64_t i) {
+    return __ddiv_rn(__dsub_rn(X[i], X[i - 1]), __dsub_rn(X[i + 1], X[i - 1]));
+  };
+  // interior points i = 1 .. n-2 in chunks
+  const int64_t m = n - 2;
+  const int64_t chunk = (m + kSplThreads - 1) / kSplThreads;
+  const int64_t i0 = 1 + t * chunk, i1 = min(n - 1, i0 + chunk);
+  // boundary values (src: the clamped first-derivative end conditions of the reference's sweep)
+  const double dydx0 = __ddiv_rn(__dsub_rn(Y[1], Y[0]), __dsub_rn(X[1], X[0]));
+  const double u0 = __dmul_rn(__ddiv_rn(3., __dsub_rn(X[1], X[0])),
+                              __dsub_rn(__ddiv_rn(__dsub_rn(Y[1], Y[0]), __dsub_rn(X[1], X[0])), dydx0));
+  // 1. yp (stored in ypp for now): Moebius maps [[0, sig - 1], [sig, 2]]
+  Mob fm{1, 0, 0, 1};
+  for (int64_t i = i0; i < i1; ++i) {
+    const double sg = sigma(i);
+    fm = mob_then(fm, Mob{0.0, sg - 1.0, sg, 2.0});
+  }
+  const Mob pm = block_prefix<Mob>(fm, Mob{1, 0, 0, 1}, shm, mob_then);
+  double yp_prev = (pm.a * -0.5 + pm.b) / (pm.c * -0.5 + pm.d);  // yp_{i0-1}
+  if (t == 0) {
+    yp_prev = -0.5;
+    ypp[0] = -0.5;
+    u[0] = u0;
+  }
+  for (int64_t i = i0; i < i1; ++i) {
+    const double sg = sigma(i);
+    const double p = __dadd_rn(__dmul_rn(sg, yp_prev), 2.0);
+    yp_prev = __ddiv_rn(__dsub_rn(sg, 1.), p);
+    ypp[i] = yp_prev;
+  }
+  __syncthreads();
+  // 2. u: affine maps u_i = (-sig / p) u_{i-1} + (6 d_i / (x_{i+1} - x_{i-1})) / p
+  auto d_i = [&](int64_t i) {
+    return __dsub_rn(__ddiv_rn(__dsub_rn(Y[i + 1], Y[i]), __dsub_rn(X[i + 1], X[i])),
+                     __ddiv_rn(__dsub_rn(Y[i], Y[i - 1]), __dsub_rn(X[i], X[i - 1])));
+  };
+  Aff fa{1, 0};
+  for (int64_t i = i0; i < i1; ++i) {
+    const double sg = sigma(i);
+    const double p = __dadd_rn(__dmul_rn(sg, i == 1 ? -0.5 : ypp[i - 1]), 2.0);
+    fa = aff_then(fa, Aff{-sg / p, __ddiv_rn(__dmul_rn(6., d_i(i)), __dsub_rn(X[i + 1], X[i - 1])) / p});
+  }
+  const Aff pa = block_prefix<Aff>(fa, Aff{1, 0}, sha, aff_then);
+  double u_prev = t == 0 ? u0 : pa.a * u0 + pa.b;  // u_{i0-1}
+  for (int64_t i = i0; i < i1; ++i) {
+    const double sg = sigma(i);
+    const double p = __dadd_rn(__dmul_rn(sg, i == 1 ? -0.5 : ypp[i - 1]), 2.0);
+    u_prev = __ddiv_rn(__dsub_rn(__ddiv_rn(__dmul_rn(6., d_i(i)), __dsub_rn(X[i + 1], X[i - 1])), __dmul_rn(sg, u_prev)), p);
+    u[i] = u_prev;
+  }
+  __syncthreads();
+  // 3. back substitution from ypp_{n-1}: ypp_k = yp_k ypp_{k+1} + u_k, k = n-2 .. 0, in chunks of the
+  // reversed index
+  const double dydxn = __ddiv_rn(__dsub_rn(Y[n - 1], Y[n - 2]), __dsub_rn(X[n - 1], X[n - 2]));
+  const double un = __dmul_rn(__ddiv_rn(3., __dsub_rn(X[n - 1], X[n - 2])),
+                              __dsub_rn(dydxn, __ddiv_rn(__dsub_rn(Y[n - 1], Y[n - 2]), __dsub_rn(X[n - 1], X[n - 2]))));
+  const double last = __ddiv_rn(__dsub_rn(un, __dmul_rn(0.5, u[n - 2])), __dadd_rn(__dmul_rn(0.5, ypp[n - 2]), 1.));
+  const int64_t mb = n - 1;  // k = n-2 .. 0
+  const int64_t cb = (mb + kSplThreads - 1) / kSplThreads;
+  const int64_t r0 = t * cb, r1 = min(mb, r0 + cb);  // reversed positions r: k = n - 2 - r
+  Aff fb{1, 0};
+  for (int64_t r = r0; r < r1; ++r) {
+    const int64_t k = n - 2 - r;
+    fb = aff_then(fb, Aff{ypp[k], u[k]});
+  }
+  const Aff pb = block_prefix<Aff>(fb, Aff{1, 0}, sha, aff_then);
+  double next = pb.a * last + pb.b;  // ypp_{k+1} entering the chunk
+  if (t == 0) next = last;
+  __syncthreads();  // every chunk has read its yp and u before any is overwritten
+  if (t == 0) ypp[n - 1] = last;
+  for (int64_t r = r0; r < r1; ++r) {
+    const int64_t k = n - 2 - r;
+    next = __dadd_rn(__dmul_rn(ypp[k], next), u[k]);
+    ypp[k] = next;
+  }
+}
+
 // Trajectory extent in the job frame: max transverse distance from the axis, max longitudinal
 // coordinate and max |tau_s| (one block of 256 threads per job).
 __global__ void k_batch_extent(DevJob* __restrict__ jobs, const double* __restrict__ arena) {
@@ -357,6 +486,20 @@ __global__ void k_batch_spline(const DevJob* __restrict__ jobs, int njobs, doubl
     ypp[k] = next;
   }
 }
+
+// Clamped splines of a chunk's trajectories: the serial sweeps (one thread per job and component)
+// take the latency of the longest trajectory's recurrences (~1.6 us per point for both sweeps on
+// B200), the block-parallel ones the chunk's total work (~1.3 ns per point, all 9 components).  mode
+// 0 takes whichever the chunk's shape makes shorter, 1 the serial and 2 the block-parallel kernel.
+void launch_batch_splines(const DevJob* d_jobs, int nj, int64_t n_max, int64_t n_total, double* knots, double* work,
+                          int mode, cudaStream_t st) {
+  const double serial_ms = 1.6e-3 * (double)n_max, parallel_ms = 1.3e-6 * (double)n_total;
+  if (mode == 2 || (mode == 0 && parallel_ms < serial_ms))
+    k_batch_spline_scan<<<9 * nj, kSplThreads, 0, st>>>(d_jobs, knots, work);
+  else
+    k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, knots, work);
+}
+
 
 // Level samples [s_begin, s_end) of every job whose active count is non-zero (all jobs when `cnt` is
 // NULL), evaluated from its spline and written as pair records (fd_common.cuh): job j's records
@@ -1020,10 +1163,12 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
       ++j1;
     }
     const int nj = (int)(j1 - j0);
-    int64_t knots = 0, work = 0, N = 0;
+    int64_t knots = 0, work = 0, N = 0, n_max = 0, n_total = 0;
     for (int k = 0; k < nj; ++k) {
       DevJob& d = dj[j0 + k];
       const int64_t n = (int64_t)d.nf + d.nb;
+      n_max = std::max(n_max, n);
+      n_total += n;
       d.knots = knots;
       knots += 19 * n;
       d.u_off = work;
@@ -1089,7 +1234,8 @@ void Engine::batch(const std::vector<FieldSpec>& fields, const std::vector<Batch
       dev::k_batch_rk4<<<(2 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_fields_.as<DevField>(),
                                                           b_fvals_.as<double>(), b_knots_.as<double>(), misc);
       dev::k_batch_extent<<<nj, 256, 0, st>>>(d_jobs, b_knots_.as<double>());
-      dev::k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(d_jobs, nj, b_knots_.as<double>(), b_work_.as<double>());
+      dev::launch_batch_splines(d_jobs, nj, n_max, n_total, b_knots_.as<double>(), b_work_.as<double>(), spline_kernel,
+                                st);
       const int64_t fill_n = rec_per_job * nj;  // samples 0 .. 2^(Lpre+1) - 1 of every job
       dev::k_batch_fill<<<(unsigned)((fill_n + 255) / 256), 256, 0, st>>>(
           d_jobs, nj, b_knots_.as<double>(), nullptr, b_rec_.as<float>(), rec_per_job, 0, 0, rec_per_job, ext_from);
@@ -1213,13 +1359,15 @@ void Engine::batch_trajectories(const std::vector<FieldSpec>& fields, const std:
                                 int64_t capacity, int64_t* npoints) {
   const double pol[6] = {0, 0, 0, 0, 0, 0};
   std::vector<DevJob> dj = build_dev_jobs(fields.size(), jobs, 0, 0, false, pol, false);
-  int64_t knots = 0, work = 0;
+  int64_t knots = 0, work = 0, n_max = 0, n_total = 0;
   for (DevJob& d : dj) {
     const int64_t n = (int64_t)d.nf + d.nb;
     d.knots = knots;
     knots += 19 * n;
     d.u_off = work;
     work += 9 * n;
+    n_max = std::max(n_max, n);
+    n_total += n;
   }
   if (knots > capacity) throw Error{OSC_ERR_LENGTH, "output capacity below 19 x points summed over the jobs"};
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
@@ -1246,8 +1394,8 @@ void Engine::batch_trajectories(const std::vector<FieldSpec>& fields, const std:
   check(cudaMemsetAsync(err, 0, sizeof(unsigned), st), "memset");
   dev::k_batch_rk4<<<(2 * nj + 63) / 64, 64, 0, st>>>(b_jobs_.as<DevJob>(), nj, b_fields_.as<DevField>(),
                                                       b_fvals_.as<double>(), b_knots_.as<double>(), err);
-  dev::k_batch_spline<<<(9 * nj + 63) / 64, 64, 0, st>>>(b_jobs_.as<DevJob>(), nj, b_knots_.as<double>(),
-                                                         b_work_.as<double>());
+  dev::launch_batch_splines(b_jobs_.as<DevJob>(), nj, n_max, n_total, b_knots_.as<double>(), b_work_.as<double>(),
+                            spline_kernel, st);
   check(cudaGetLastError(), "batch trajectories");
   check(cudaMemcpyAsync(out, b_knots_.p, sizeof(double) * knots, cudaMemcpyDeviceToHost, st), "download");
   unsigned e = 0;

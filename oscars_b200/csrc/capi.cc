@@ -844,6 +844,13 @@ OSC_API int osc_set_beam_batch_threshold(osc_ctx* ctx, int particles) {
   });
 }
 
+OSC_API int osc_set_batch_spline_kernel(osc_ctx* ctx, int kernel) {
+  return guarded(ctx, [&] {
+    if (kernel < 0 || kernel > 2) throw osc::Error{OSC_ERR_RANGE, "kernel must be 0, 1 or 2"};
+    ctx->eng->spline_kernel = kernel;
+  });
+}
+
 OSC_API int osc_set_profiling(osc_ctx* ctx, int enable) {
   return guarded(ctx, [&] { ctx->eng->profiling = enable != 0; });
 }

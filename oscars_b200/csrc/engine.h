@@ -117,6 +117,8 @@ class Engine {
   // particles (this process's share) from which a mixed multi-particle request runs as one batch
   // with device trajectories instead of host trajectories and per-particle sums
   int beam_batch_min = 1024;
+  // spline kernel of the batched trajectories: 0 by the chunk's shape, 1 serial sweeps, 2 block-parallel
+  int spline_kernel = 0;
   long long graph_launches() const { return graph_launches_; }
 
   // profiling of the sample-integration kernels

@@ -85,13 +85,16 @@ def _cases():
     ]
 
 
+@pytest.mark.parametrize("spline", [1, 2])  # the serial and the block-parallel spline kernel
 @pytest.mark.parametrize("case", [c[0] for c in _cases()])
-def test_device_trajectory_matches_host(case):
+def test_device_trajectory_matches_host(case, spline):
     from oscars_b200.batch import BatchRunner, Job
     name, bfields, ofields, energy, x0, d0, ct, npts = next(c for c in _cases() if c[0] == case)
     job = Job(fields=bfields, energy_GeV=energy, ctstartstop=ct, npoints=npts, obs=[[0, 0, 30]],
               energies_eV=[E1_EPU], x0=x0, d0=d0)
-    dev = BatchRunner(0).trajectories([job])[0]
+    runner = BatchRunner(0)
+    runner.ctx.call("osc_set_batch_spline_kernel", spline)
+    dev = runner.trajectories([job])[0]
     host = _oracle_knots(ofields, energy, x0, d0, ct, npts)
     assert dev.shape == host.shape, (dev.shape, host.shape)
     assert np.array_equal(dev[0], host[0]), "knot times differ"
