@@ -210,17 +210,20 @@ __global__ void k_batch_rk4(const DevJob* __restrict__ jobs, int njobs, const De
   double x[6] = {x0[0], J.b0[0] * kCLight, x0[1], J.b0[1] * kCLight, x0[2], J.b0[2] * kCLight};
   double dxdt[6] = {0, 0, 0, 0, 0, 0};
   const double t0 = J.frame.t_ref;
+  // beta and a/c by one product with 1/c (within an ulp of the host's division): divisions here would
+  // sit in the in-order instruction stream of the serial chain
+  constexpr double kInvC = 1.0 / kCLight;
   auto store = [&](int64_t i, double tt) {
     K[i] = tt;
     K[n + i] = x[0];
     K[2 * n + i] = x[2];
     K[3 * n + i] = x[4];
-    K[4 * n + i] = x[1] / kCLight;
-    K[5 * n + i] = x[3] / kCLight;
-    K[6 * n + i] = x[5] / kCLight;
-    K[7 * n + i] = dxdt[1] / kCLight;
-    K[8 * n + i] = dxdt[3] / kCLight;
-    K[9 * n + i] = dxdt[5] / kCLight;
+    K[4 * n + i] = x[1] * kInvC;
+    K[5 * n + i] = x[3] * kInvC;
+    K[6 * n + i] = x[5] * kInvC;
+    K[7 * n + i] = dxdt[1] * kInvC;
+    K[8 * n + i] = dxdt[3] * kInvC;
+    K[9 * n + i] = dxdt[5] * kInvC;
   };
   if (fwd) {
     derivs_d(c, t0, x, dxdt);
