@@ -175,3 +175,34 @@ def test_variant_names():
         _lib.variant_name(2, 4)
     with pytest.raises(ValueError, match="kind"):
         _lib.variant_name(1, 0)
+
+
+def test_tuning_setters_and_vjp_buffers_checked_on_the_host():
+    """The beam routing threshold, the batch spline kernel choice and the adjoint's buffer rules are
+    argument checks of the C ABI: they answer on a host-only context without launching anything."""
+    import ctypes
+    ctx = _lib.Context(-1)
+    ctx.call("osc_set_beam_batch_threshold", 1)
+    ctx.call("osc_set_beam_batch_threshold", 4096)
+    with pytest.raises(ValueError, match="at least 1 particle"):
+        ctx.call("osc_set_beam_batch_threshold", 0)
+    for k in (0, 1, 2):
+        ctx.call("osc_set_batch_spline_kernel", k)
+    for k in (-1, 3):
+        with pytest.raises(ValueError, match="kernel must be 0, 1 or 2"):
+            ctx.call("osc_set_batch_spline_kernel", k)
+    DP = ctypes.POINTER(ctypes.c_double)
+    obs = (ctypes.c_double * 3)(0.0, 0.0, 30.0)
+    en = (ctypes.c_double * 1)(100.0)
+    opts = _lib.RadOpts(precision=0.01, max_level=10, max_level_extended=10, shard_count=1)
+    none = ctypes.cast(None, DP)
+    # forward only (no gradient) needs flux_out; with a gradient, grad_half_scale is required
+    with pytest.raises(ValueError, match="bad buffers"):
+        ctx.call("osc_flux_vjp", obs, 1, en, 1, 8, ctypes.byref(opts), 0, none, none, none, 0, none)
+    g = (ctypes.c_double * 1)(1.0)
+    with pytest.raises(ValueError, match="bad buffers"):
+        ctx.call("osc_flux_vjp", obs, 1, en, 1, 8, ctypes.byref(opts), 0, g, none, none, 0, none)
+    opts.nparticles = 2
+    with pytest.raises(ValueError, match="one particle"):
+        ctx.call("osc_flux_vjp", obs, 1, en, 1, 8, ctypes.byref(opts), 0, g, none, none, 0, none)
+    ctx.close()
