@@ -58,8 +58,8 @@ Engine::Engine(int dev) : device(dev) {
   mrec_bd_.reserve(32 * sizeof(unsigned long long));
   cnt_.reserve(64);
   check(cudaMemset(cnt_.p, 0, 64), "memset");
-  check(cudaHostAlloc(reinterpret_cast<void**>(&stats_host_), 2 * kStatSlots * sizeof(unsigned long long),
-                      cudaHostAllocDefault),
+  check(cudaHostAlloc(reinterpret_cast<void**>(&stats_host_), kStatWords * kStatSlots * sizeof(unsigned long long),
+                      cudaHostAllocMapped),
         "cudaHostAlloc");
   check(cudaHostAlloc(reinterpret_cast<void**>(&stage_host_), kStageDoubles * sizeof(double), cudaHostAllocDefault),
         "cudaHostAlloc");
@@ -73,6 +73,9 @@ Engine::Engine(int dev) : device(dev) {
   check(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&zs_fork_ev_, cudaEventDisableTiming), "event");
   check(cudaEventCreateWithFlags(&zs_ev_, cudaEventDisableTiming), "event");
+  check(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (cudaEvent_t* e : {&in_fork_ev_, &in_ev_})
+    check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
   cur_ = stream;
 }
 
@@ -81,6 +84,7 @@ Engine::~Engine() {
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
   if (aux_) cudaStreamSynchronize(aux_);
+  if (copy_) cudaStreamSynchronize(copy_);
   for (auto& e : ev_pending_) { ev_pool_.push_back(e.first); ev_pool_.push_back(e.second); }
   for (cudaEvent_t e : ev_pool_) cudaEventDestroy(e);
   for (int i = 0; i < kStatSlots; ++i) if (stats_ev_[i]) cudaEventDestroy(stats_ev_[i]);
@@ -90,6 +94,8 @@ Engine::~Engine() {
   if (join_ev_) cudaEventDestroy(join_ev_);
   if (zs_fork_ev_) cudaEventDestroy(zs_fork_ev_);
   if (zs_ev_) cudaEventDestroy(zs_ev_);
+  for (cudaEvent_t e : {in_fork_ev_, in_ev_})
+    if (e) cudaEventDestroy(e);
   if (last_stream_valid_ && last_stream_ != stream) cudaStreamSynchronize(last_stream_);
   if (stats_host_) cudaFreeHost(stats_host_);
   if (stage_host_) cudaFreeHost(stage_host_);
@@ -111,6 +117,7 @@ Engine::~Engine() {
     b->release();
   if (stream) cudaStreamDestroy(stream);
   if (aux_) cudaStreamDestroy(aux_);
+  if (copy_) cudaStreamDestroy(copy_);
 }
 
 void Engine::check(cudaError_t e, const char* what) {
@@ -391,6 +398,20 @@ int Engine::wave_grid(int kind, int variant) {
 // with every compiled variant of the sample-sum kernel into scratch outputs, times them with CUDA
 // events, and keeps the fastest for that shape.  FP64 variants differ only in their register cap,
 // so they give bit-identical sums; mixed variants also change entries per thread.
+// Statistics of one request into its mapped pinned ring slot: not converged, samples, the sticky
+// error word (read by collect() after the slot's event).
+__device__ __forceinline__ void k_stats_store(const unsigned long long* __restrict__ c64,
+                                              const unsigned* __restrict__ err, volatile unsigned long long* slot) {
+  slot[0] = c64[0];
+  slot[1] = c64[1];
+  slot[2] = *err;
+}
+
+__global__ void k_stats_out(const unsigned long long* __restrict__ c64, const unsigned* __restrict__ err,
+                            volatile unsigned long long* slot) {
+  k_stats_store(c64, err, slot);
+}
+
 int Engine::pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out,
                          int32_t* d_lvl, cudaStream_t st) {
   if (forced_variant[kind] >= 0) return forced_variant[kind];
@@ -484,7 +505,10 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   // [0] not converged, [1] samples, [2] unit counter of the running wave
   unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);
   unsigned* level_max = cnt + 12;  // highest level at which an entry finished
-  check(cudaMemsetAsync(cnt, 0, 13 * sizeof(unsigned), st), "memset");  // words 0..12
+  // the counter resets go in behind the input copies when those are still on their way (so that the
+  // request stream goes from the level samples straight to the first wave)
+  cudaStream_t zs = inputs_pending_ ? copy_ : st;
+  check(cudaMemsetAsync(cnt, 0, 13 * sizeof(unsigned), zs), "memset");  // words 0..12
   // Flux / spectrum waves finalize their own tiles (one launch per level).  Wave w reads its active
   // count from fz3[w % 3], appends survivors to fz3[(w + 1) % 3] and zeroes fz3[(w + 2) % 3] for the
   // wave after; it takes units from fw[w % 2] and zeroes fw[(w + 1) % 2].
@@ -495,8 +519,9 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     fused_.reserve(64 + sizeof(unsigned) * (size_t)(ntiles + 1));
     fz3 = fused_.as<unsigned>();
     fw = reinterpret_cast<unsigned long long*>(fz3 + 4);
-    check(cudaMemsetAsync(fused_.p, 0, 64 + sizeof(unsigned) * (size_t)(ntiles + 1), st), "memset");
+    check(cudaMemsetAsync(fused_.p, 0, 64 + sizeof(unsigned) * (size_t)(ntiles + 1), zs), "memset");
   }
+  if (zs != st) check(cudaEventRecord(in_ev_, zs), "event");
 
   const double* d_obs = obs_.as<double>();
   const double* d_nrm = rq.normals ? nrm_.as<double>() : nullptr;
@@ -523,7 +548,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   int cur_list = 0;
   auto launch_wave = [&](int L) {
     const bool first = L == Lfirst;
-    if (!first) join_prefill();  // the levels filled on the side stream
+    if (first) wait_inputs(st);  // observers and frequencies from the host
+    else join_prefill();         // the levels filled on the side stream
     const int wv = L - Lfirst;
     const int* act_in = first ? nullptr : act_[cur_list].as<int>();
     const unsigned* nact_in = first ? nullptr : (fused ? fz3 + wv % 3 : cnt + cur_list);
@@ -635,43 +661,88 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     cur_list ^= 1;
   };
   for (int L = Lfirst; L <= Lpre; ++L) launch_wave(L);
+  bool finished = false;  // statistics (and result downloads) already enqueued behind the last wave
   for (int L = Lpre + 1; L <= lstop; ++L) {  // beyond the prefilled levels the host decides
     // a one-thread kernel writes the active count and the highest finished level into mapped host
     // memory behind a sequence word that the host polls (no copy engine, no stream wake-up)
     const unsigned* active = fused ? fz3 + (L - Lfirst) % 3 : cnt + cur_list;
     unsigned nn = 0, lmax = 0;
-    report_counts(active, level_max, &nn, &lmax, st);
+    // the report also stores the request's statistics into a ring slot, and the downloads of host
+    // outputs go in behind it, before the host knows whether this was the last wave; if it was not,
+    // both are superseded by those the request ends with
+    const bool speculate = !tuning_;
+    const int slot = speculate ? claim_stat_slot() : -1;
+    const unsigned seq = report_launch(active, level_max, st, speculate ? c64 : nullptr,
+                                       speculate ? stats_host_ + kStatWords * slot : nullptr);
+    if (speculate) finish_request(slot, st);
+    report_wait(seq, &nn, &lmax, st);
     if (nn == 0) {
       if (!tuning_) prefill_hist_[hist_key] = std::max<int>(Lfirst, (int)lmax);
+      finished = speculate;
       break;
+    }
+    if (speculate) {
+      pending_.pop_back();
+      tail_.emitted = false;
     }
     if (mixed) ensure_mixed(L);
     else ensure_levels(L);
     launch_wave(L);
   }
   join_prefill();
-  // statistics of this particle go to a pinned ring slot; collect() reads them when asked
+  if (!finished) {
+    const int slot = claim_stat_slot();
+    k_stats_out<<<1, 1, 0, st>>>(c64, cnt_.as<unsigned>() + kCntErr, stats_host_ + kStatWords * slot);
+    check(cudaGetLastError(), "stats");
+    ++last_launches;
+    finish_request(slot, st);
+  }
+}
+
+int Engine::claim_stat_slot() {
   if ((int)pending_.size() >= kStatSlots) collect();
-  const int slot = stats_slot_++ % kStatSlots;
-  check(cudaMemcpyAsync(stats_host_ + 2 * slot, c64, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
-        "stats");
+  return stats_slot_++ % kStatSlots;
+}
+
+// The statistics of the request just enqueued, stored into ring slot `slot` by the last kernel on
+// the stream, are read by collect() when asked (after the slot's event); a
+// single-particle request with host outputs that the kernels cannot write then enqueues its result
+// downloads.
+void Engine::finish_request(int slot, cudaStream_t st) {
   check(cudaEventRecord(stats_ev_[slot], st), "event");
   pending_.push_back(slot);
+  if (!tail_.active || tuning_) return;
+  check(cudaMemcpyAsync(tail_.h_out, tail_.d_out, sizeof(double) * tail_.n, cudaMemcpyDeviceToHost, st), "download");
+  if (tail_.h_lvl)
+    check(cudaMemcpyAsync(tail_.h_lvl, tail_.d_lvl, sizeof(int32_t) * tail_.n, cudaMemcpyDeviceToHost, st),
+          "download");
+  tail_.emitted = true;
+}
+
+void Engine::wait_inputs(cudaStream_t st) {
+  if (!inputs_pending_) return;
+  check(cudaStreamWaitEvent(st, in_ev_, 0), "stream wait");
+  inputs_pending_ = false;
 }
 
 // Wait for the statistics of the enqueued particles of the last request and report device errors.
 void Engine::collect() {
   if (device < 0) return;
+  // the error word rides in the slots (the last one has every earlier error: the word is sticky);
+  // with no slot pending it is read directly
+  unsigned err = 0;
+  const bool direct = pending_.empty();
   for (int slot : pending_) {
     check(cudaEventSynchronize(stats_ev_[slot]), "radiation");
-    last_not_converged += (long long)stats_host_[2 * slot];
-    last_samples += (long long)stats_host_[2 * slot + 1];
-    if (profiling) prof_samples += (long long)stats_host_[2 * slot + 1];
+    const volatile unsigned long long* w = stats_host_ + kStatWords * slot;
+    last_not_converged += (long long)w[0];
+    last_samples += (long long)w[1];
+    err |= (unsigned)w[2];
+    if (profiling) prof_samples += (long long)w[1];
   }
   pending_.clear();
   if (profiling) collect_timings();
-  unsigned err = 0;
-  check(cudaMemcpy(&err, cnt_.as<unsigned>() + kCntErr, sizeof err, cudaMemcpyDeviceToHost), "error word");
+  if (direct) check(cudaMemcpy(&err, cnt_.as<unsigned>() + kCntErr, sizeof err, cudaMemcpyDeviceToHost), "error word");
   if (err) {
     check(cudaMemset(cnt_.as<unsigned>() + kCntErr, 0, sizeof(unsigned)), "error word");
     if (err & 1u) throw Error{OSC_ERR_TIMEOUT, "a staged trajectory copy did not complete (device wait limit reached)"};
@@ -819,7 +890,9 @@ class TrajectoryPipeline {
 };
 
 __global__ void k_report_counts(const unsigned* __restrict__ a, const unsigned* __restrict__ b,
-                                volatile unsigned* host, unsigned seq) {
+                                volatile unsigned* host, unsigned seq, const unsigned long long* __restrict__ c64,
+                                const unsigned* __restrict__ err, volatile unsigned long long* slot) {
+  if (slot) k_stats_store(c64, err, slot);
   host[1] = *a;
   host[2] = *b;
   __threadfence_system();
@@ -831,11 +904,20 @@ __global__ void k_report_counts(const unsigned* __restrict__ a, const unsigned* 
 // which the host polls; every 4096 polls it asks whether the stream has finished, so a failed or
 // lost launch ends in the stream's error instead of a wait that does not end.
 void Engine::report_counts(const unsigned* a, const unsigned* b, unsigned* va, unsigned* vb, cudaStream_t st) {
+  report_wait(report_launch(a, b, st), va, vb, st);
+}
+
+unsigned Engine::report_launch(const unsigned* a, const unsigned* b, cudaStream_t st, const unsigned long long* c64,
+                               unsigned long long* slot) {
   const unsigned seq = ++report_seq_;
-  volatile unsigned* w = ctl_host_;
-  k_report_counts<<<1, 1, 0, st>>>(a, b, ctl_host_, seq);
+  k_report_counts<<<1, 1, 0, st>>>(a, b, ctl_host_, seq, c64, cnt_.as<unsigned>() + kCntErr, slot);
   check(cudaGetLastError(), "count");
   ++last_launches;
+  return seq;
+}
+
+void Engine::report_wait(unsigned seq, unsigned* va, unsigned* vb, cudaStream_t st) {
+  volatile unsigned* w = ctl_host_;
   for (unsigned i = 1; w[0] != seq; ++i) {
     if ((i & 4095u) == 0) {
       const cudaError_t e = cudaStreamQuery(st);
@@ -847,6 +929,17 @@ void Engine::report_counts(const unsigned* a, const unsigned* b, unsigned* va, u
   }
   *va = w[1];
   *vb = w[2];
+}
+
+// The device address of page-locked host memory mapped for the current device, or NULL (pageable
+// memory, or not mapped here).
+static void* mapped_host_pointer(void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the error of an unknown pointer
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
 }
 
 void Engine::radiation(RadRequest& rq) {
@@ -862,32 +955,57 @@ void Engine::radiation(RadRequest& rq) {
   const int64_t N = rq.n_obs * n_e;
   if (N <= 0) return;
   if (N > 2147483647ll) throw Error{OSC_ERR_LENGTH, "more than 2^31-1 (observer, energy) entries in one call"};
-  // inputs
+  // inputs: host buffers go up on copy_ (after the work already on the request stream, which may still
+  // read the previous request's inputs), concurrently with the level samples the request stream
+  // builds; the first wave waits for them (wait_inputs)
   const cudaMemcpyKind in_kind = rq.obs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  cudaStream_t in_st = st;
+  if (!rq.obs_on_device) {
+    check(cudaEventRecord(in_fork_ev_, st), "event");
+    check(cudaStreamWaitEvent(copy_, in_fork_ev_, 0), "stream wait");
+    in_st = copy_;
+  }
   obs_.reserve(sizeof(double) * 3 * rq.n_obs);
-  check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, in_kind, st), "obs");
+  check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, in_kind, in_st), "obs");
   if (rq.normals) {
     nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
-    check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, in_kind, st), "normals");
+    check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, in_kind, in_st), "normals");
   }
   if (!rq.power_density) {
     omega_.reserve(sizeof(double) * n_e);
     if (n_e <= kStageDoubles) {  // small vectors go through pinned memory so the copy stays asynchronous
       check(cudaEventSynchronize(stage_ev_), "stage");
       std::memcpy(stage_host_, rq.omega.data(), sizeof(double) * n_e);
-      check(cudaMemcpyAsync(omega_.p, stage_host_, sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
-      check(cudaEventRecord(stage_ev_, st), "event");
+      check(cudaMemcpyAsync(omega_.p, stage_host_, sizeof(double) * n_e, cudaMemcpyHostToDevice, in_st), "omega");
+      check(cudaEventRecord(stage_ev_, in_st), "event");
     } else {
-      check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
+      check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, in_st), "omega");
     }
+  }
+  if (in_st != st) {
+    check(cudaEventRecord(in_ev_, in_st), "event");
+    inputs_pending_ = true;
   }
   out_.reserve(sizeof(double) * N);
   lvl_.reserve(sizeof(int32_t) * N);
   double* d_out = rq.out_on_device ? rq.out : out_.as<double>();
   int32_t* d_lvl = rq.out_on_device ? rq.level_out : lvl_.as<int32_t>();
   if (!d_lvl) d_lvl = lvl_.as<int32_t>();
-
   const int np = rq.opts.nparticles;
+  // Host outputs in page-locked memory mapped into this device's address space are written by the
+  // kernels themselves (one plain store per entry as it finishes), so no download follows the last
+  // wave; pageable outputs are downloaded.
+  bool direct_out = false;
+  if (!rq.out_on_device && np <= 0) {
+    void* mo = mapped_host_pointer(rq.out);
+    void* ml = rq.level_out ? mapped_host_pointer(rq.level_out) : nullptr;
+    if (mo && (ml || !rq.level_out)) {
+      d_out = static_cast<double*>(mo);
+      if (ml) d_lvl = static_cast<int32_t*>(ml);
+      direct_out = true;
+    }
+  }
+
   // Mixed multi-particle flux / spectrum requests with at least beam_batch_min particles (this
   // process's share) run as one batch with device RK4 trajectories; smaller ones, and those with RKAS
   // trajectories, take the host integrator on worker threads like the FP64 path: the device RK4 is a
@@ -904,7 +1022,15 @@ void Engine::radiation(RadRequest& rq) {
   if (np <= 0) {
     model.ensure_trajectory();
     upload_trajectory();
-    run_single(rq, N, 1.0, d_out, d_lvl, st);
+    tail_ = ResultTail{};
+    if (!rq.out_on_device && !direct_out) tail_ = ResultTail{true, false, d_out, d_lvl, rq.out, rq.level_out, N};
+    try {
+      run_single(rq, N, 1.0, d_out, d_lvl, st);
+    } catch (...) {
+      tail_ = ResultTail{};
+      throw;
+    }
+    tail_.active = false;
   } else {
     // src/OSCARSSR.cc:4026-4062: new random particle, its trajectory, weight 1/N, compensated sum
     const double weight = 1.0 / (double)np;
@@ -943,9 +1069,12 @@ void Engine::radiation(RadRequest& rq) {
     check(cudaMemcpyAsync(d_out, acc_.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "result");
   }
   if (!rq.out_on_device) {
-    check(cudaMemcpyAsync(rq.out, d_out, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
-    if (rq.level_out)
-      check(cudaMemcpyAsync(rq.level_out, d_lvl, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st), "download");
+    if (!tail_.emitted && !direct_out) {  // (run_single enqueues them itself for one particle)
+      check(cudaMemcpyAsync(rq.out, d_out, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
+      if (rq.level_out)
+        check(cudaMemcpyAsync(rq.level_out, d_lvl, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st), "download");
+    }
+    tail_ = ResultTail{};
     check(cudaStreamSynchronize(st), "download");
     collect();
   }

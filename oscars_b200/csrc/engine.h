@@ -152,8 +152,11 @@ class Engine {
   std::pair<cudaEvent_t, cudaEvent_t> timed_begin(cudaStream_t st);
   void timed_end(std::pair<cudaEvent_t, cudaEvent_t> e, cudaStream_t st);
   void collect_timings();
-  // asynchronous statistics: per-particle counters copied to pinned memory, one event per slot
+  // asynchronous statistics: per particle, a one-thread kernel stores the counters and the sticky
+  // error word into a slot of mapped pinned memory (kStatWords words: not converged, samples, error
+  // word), one event per slot
   static constexpr int kStageDoubles = 4096;
+  static constexpr int kStatWords = 4;
   unsigned long long* stats_host_ = nullptr;
   double* stage_host_ = nullptr;
   // Device counter block cnt_ (16 words): [0], [1] survivor-list counts, [4..9] three 64-bit counters
@@ -166,6 +169,11 @@ class Engine {
   unsigned* ctl_host_ = nullptr;  // mapped (cudaHostAllocMapped): also written by k_report_counts
   unsigned report_seq_ = 0;
   void report_counts(const unsigned* a, const unsigned* b, unsigned* va, unsigned* vb, cudaStream_t st);
+  // its sequence number; with `slot`, the kernel also stores the request's statistics there (c64[0..1]
+  // and the error word)
+  unsigned report_launch(const unsigned* a, const unsigned* b, cudaStream_t st, const unsigned long long* c64 = nullptr,
+                         unsigned long long* slot = nullptr);
+  void report_wait(unsigned seq, unsigned* va, unsigned* vb, cudaStream_t st);
   static constexpr int kStatSlots = 64;
   cudaEvent_t stats_ev_[kStatSlots] = {};
   cudaEvent_t stage_ev_ = nullptr;
@@ -250,6 +258,26 @@ class Engine {
   cudaStream_t aux_ = nullptr;
   cudaEvent_t fork_ev_ = nullptr, join_ev_ = nullptr;
   bool join_pending_ = false;
+  // Host-side inputs (observers, normals, frequencies) go up on copy_, followed by the request's
+  // counter resets, while the request stream fills the level samples; the first wave waits for
+  // in_ev_ (wait_inputs).
+  cudaStream_t copy_ = nullptr;
+  cudaEvent_t in_fork_ev_ = nullptr, in_ev_ = nullptr;
+  bool inputs_pending_ = false;
+  void wait_inputs(cudaStream_t st);
+  // Result downloads of a single-particle request with pageable host outputs, enqueued by run_single
+  // right behind its statistics -- ahead of the host's last poll, so the copies need no extra round
+  // trip.
+  struct ResultTail {
+    bool active = false, emitted = false;
+    const double* d_out = nullptr;
+    const int32_t* d_lvl = nullptr;
+    double* h_out = nullptr;
+    int32_t* h_lvl = nullptr;
+    int64_t n = 0;
+  } tail_;
+  int claim_stat_slot();
+  void finish_request(int slot, cudaStream_t st);
   void run_single(const RadRequest& rq, int64_t n_items, double weight, double* d_out, int32_t* d_lvl,
                   cudaStream_t st);
   void check(cudaError_t e, const char* what);

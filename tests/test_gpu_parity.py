@@ -101,6 +101,58 @@ def test_device_entry_point_matches_host_entry_point():
     assert np.array_equal(out.cpu().numpy(), host)
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("power_density", [False, True])
+def test_pinned_host_outputs_match_pageable_outputs(mode, power_density):
+    """Host outputs in page-locked memory are written by the kernels directly; pageable ones are
+    downloaded after the last wave.  Both, with page-locked or pageable observers, give the same
+    values and levels, and the same as device outputs; repeated calls of one request shape (whose
+    later calls enqueue their waves without a host round trip) too."""
+    import ctypes
+    import torch
+    from oscars_b200 import _lib
+    from oscars_b200._lib import RadOpts
+    s = _sr()
+    run_case(s, UND_SETUP)
+    xyz, _, _ = s._rectangle([41, 37], "XY", [0.006, 0.006], None, None, [0, 0, 30], 0, False)
+    xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    n = xyz.shape[0]
+    o = RadOpts(precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, quantity=0, precision_mode=mode)
+    o.horizontal[:] = [1, 0, 0]
+    o.propagation[:] = [0, 0, 1]
+
+    def call(obs, out, lvl):
+        if power_density:
+            s._ctx.call("osc_power_density", _lib.dptr(obs), None, n, 0, ctypes.byref(o), _lib.dptr(out),
+                        _lib.i32ptr(lvl), None)
+        else:
+            s._ctx.call("osc_flux", _lib.dptr(obs), n, E1_U, ctypes.byref(o), _lib.dptr(out), _lib.i32ptr(lvl), None)
+
+    ref_out, ref_lvl = np.zeros(n), np.zeros(n, dtype=np.int32)
+    call(xyz, ref_out, ref_lvl)
+    assert np.all(ref_out != 0) and len(set(ref_lvl.tolist())) > 1
+    pin_obs_t = torch.from_numpy(xyz.copy()).pin_memory()
+    pin_obs = pin_obs_t.numpy()
+    for k in range(3):
+        for obs in (xyz, pin_obs):
+            out_t = torch.full((n,), -1.0, dtype=torch.float64).pin_memory()
+            lvl_t = torch.full((n,), -7, dtype=torch.int32).pin_memory()
+            call(obs, out_t.numpy(), lvl_t.numpy())
+            assert np.array_equal(out_t.numpy(), ref_out), k
+            assert np.array_equal(lvl_t.numpy(), ref_lvl), k
+            out_p, lvl_p = np.full(n, -1.0), np.full(n, -7, dtype=np.int32)
+            call(obs, out_p, lvl_p)
+            assert np.array_equal(out_p, ref_out) and np.array_equal(lvl_p, ref_lvl), k
+    if not power_density:
+        d_obs = torch.tensor(xyz, device="cuda")
+        d_out = torch.zeros(n, dtype=torch.float64, device="cuda")
+        d_lvl = torch.zeros(n, dtype=torch.int32, device="cuda")
+        s._ctx.call("osc_flux_device", ctypes.c_void_p(d_obs.data_ptr()), n, E1_U, ctypes.byref(o),
+                    ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_lvl.data_ptr()), None)
+        torch.cuda.synchronize()
+        assert np.array_equal(d_out.cpu().numpy(), ref_out) and np.array_equal(d_lvl.cpu().numpy(), ref_lvl)
+
+
 def test_flux_multi_matches_single_energy_calls():
     """osc_flux_multi (all observers x energies in one request) against osc_flux per energy and
     osc_spectrum, FP64, fixed level."""
