@@ -61,7 +61,7 @@ Engine::Engine(int dev) : device(dev) {
   check(cudaHostAlloc(reinterpret_cast<void**>(&stats_host_), kStatWords * kStatSlots * sizeof(unsigned long long),
                       cudaHostAllocMapped),
         "cudaHostAlloc");
-  check(cudaHostAlloc(reinterpret_cast<void**>(&stage_host_), kStageDoubles * sizeof(double), cudaHostAllocDefault),
+  check(cudaHostAlloc(reinterpret_cast<void**>(&stage_host_), kStageDoubles * sizeof(double), cudaHostAllocMapped),
         "cudaHostAlloc");
   check(cudaHostAlloc(reinterpret_cast<void**>(&ctl_host_), 16 * sizeof(unsigned), cudaHostAllocMapped),
         "cudaHostAlloc");
@@ -282,17 +282,20 @@ void Engine::reserve_mixed(int L) {
   mrec_filled_ = -1;
 }
 
-void Engine::fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s) {
+void Engine::fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s, bool zero_bd) {
   if (s_end <= s_begin) return;
   // the beta-difference maxima of the levels filled here start from zero
-  const int Lb = s_begin <= 1 ? 0 : 63 - __builtin_clzll((unsigned long long)s_begin);
-  const int Le = 63 - __builtin_clzll((unsigned long long)(s_end - 1));
-  check(cudaMemsetAsync(mrec_bd_.as<unsigned long long>() + Lb, 0, sizeof(unsigned long long) * (Le - Lb + 1), s),
-        "memset");
+  if (zero_bd) {
+    const int Lb = s_begin <= 1 ? 0 : 63 - __builtin_clzll((unsigned long long)s_begin);
+    const int Le = 63 - __builtin_clzll((unsigned long long)(s_end - 1));
+    check(cudaMemsetAsync(mrec_bd_.as<unsigned long long>() + Lb, 0, sizeof(unsigned long long) * (Le - Lb + 1), s),
+          "memset");
+    ++last_launches;
+  }
   check(launch_mixed_records(knots_.as<double>(), nknots_, tstart_, tstop_, s_begin, s_end, mrec_ext_, frame_,
                              mrec_.as<float4>(), mrec_bd_.as<unsigned long long>(), s),
         "mixed records");
-  last_launches += 2;
+  ++last_launches;
 }
 
 void Engine::ensure_mixed(int L) {
@@ -305,12 +308,12 @@ void Engine::ensure_mixed(int L) {
 // Levels 0..Lpre resident for the waves enqueued without a host round trip.  The levels above the
 // first wave's (Lhead) are filled on the side stream, concurrently with the first wave; join_prefill()
 // makes the request stream wait for them before the second wave.
-void Engine::prefill(bool mixed, int Lhead, int Lpre) {
+void Engine::prefill(bool mixed, int Lhead, int Lpre, bool bd_zeroed) {
   if (mixed) reserve_mixed(Lpre);
   else reserve_levels(Lpre);
   int& filled = mixed ? mrec_filled_ : lev_filled_;
   if (Lpre <= filled) return;
-  if (!mixed && filled < 0) {
+  if (!mixed && filled < 0 && !bd_zeroed) {
     check(cudaMemsetAsync(bd_bits_.p, 0, 32 * sizeof(unsigned long long), cur_), "memset");
     ++last_launches;
   }
@@ -318,14 +321,14 @@ void Engine::prefill(bool mixed, int Lhead, int Lpre) {
   if (Lpre > lo) {
     check(cudaEventRecord(fork_ev_, cur_), "event");
     check(cudaStreamWaitEvent(aux_, fork_ev_, 0), "stream wait");
-    if (mixed) fill_mixed((int64_t)2 << lo, (int64_t)2 << Lpre, aux_);
+    if (mixed) fill_mixed((int64_t)2 << lo, (int64_t)2 << Lpre, aux_, !bd_zeroed);
     else fill_levels((int64_t)2 << lo, (int64_t)2 << Lpre, aux_);
     check(cudaEventRecord(join_ev_, aux_), "event");
     join_pending_ = true;
   }
   if (lo > filled) {
     const int64_t b = filled < 0 ? (mixed ? 0 : 1) : ((int64_t)2 << filled);
-    if (mixed) fill_mixed(b, (int64_t)2 << lo, cur_);
+    if (mixed) fill_mixed(b, (int64_t)2 << lo, cur_, !bd_zeroed);
     else fill_levels(b, (int64_t)2 << lo, cur_);
   }
   filled = Lpre;
@@ -412,6 +415,23 @@ __global__ void k_stats_out(const unsigned long long* __restrict__ c64, const un
   k_stats_store(c64, err, slot);
 }
 
+// Start of a request in one launch: zero up to three ranges of 32-bit words (the request's counters,
+// the fused-finalize counters, the beta-step maxima of the levels to fill) and copy the frequencies
+// from the mapped staging buffer.
+struct ZeroRange {
+  unsigned* p;
+  int64_t words;
+};
+__global__ void k_request_prologue(ZeroRange z0, ZeroRange z1, ZeroRange z2, const double* __restrict__ om_src,
+                                   double* __restrict__ om_dst, int64_t n_om) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t i = t0; i < z0.words; i += stride) z0.p[i] = 0u;
+  for (int64_t i = t0; i < z1.words; i += stride) z1.p[i] = 0u;
+  for (int64_t i = t0; i < z2.words; i += stride) z2.p[i] = 0u;
+  for (int64_t i = t0; i < n_om; i += stride) om_dst[i] = om_src[i];
+}
+
 int Engine::pick_variant(int kind, RadRequest& rq, int64_t n_items, int Lfirst, int lstop, double* d_out,
                          int32_t* d_lvl, cudaStream_t st) {
   if (forced_variant[kind] >= 0) return forced_variant[kind];
@@ -472,7 +492,6 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   const int Lpre = std::min(lstop, std::max(Lfirst, Lpre_want));
   const int variant = tuning_ ? current_variant_[kind]
                               : pick_variant(kind, const_cast<RadRequest&>(rq), n_items, Lfirst, lstop, d_out, d_lvl, st);
-  prefill(mixed, Lfirst, Lpre);
   const int resident = wave_grid(kind, variant);  // CTAs resident at once on the device
   const int tile = rq.power_density ? (mixed ? pd_mixed_entries_per_cta() : 128)
                                     : (mixed ? mixed_entries_per_cta(variant) : fp64_entries_per_cta(variant));
@@ -505,10 +524,6 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   // [0] not converged, [1] samples, [2] unit counter of the running wave
   unsigned long long* c64 = reinterpret_cast<unsigned long long*>(cnt + 4);
   unsigned* level_max = cnt + 12;  // highest level at which an entry finished
-  // the counter resets go in behind the input copies when those are still on their way (so that the
-  // request stream goes from the level samples straight to the first wave)
-  cudaStream_t zs = inputs_pending_ ? copy_ : st;
-  check(cudaMemsetAsync(cnt, 0, 13 * sizeof(unsigned), zs), "memset");  // words 0..12
   // Flux / spectrum waves finalize their own tiles (one launch per level).  Wave w reads its active
   // count from fz3[w % 3], appends survivors to fz3[(w + 1) % 3] and zeroes fz3[(w + 2) % 3] for the
   // wave after; it takes units from fw[w % 2] and zeroes fw[(w + 1) % 2].
@@ -519,12 +534,37 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     fused_.reserve(64 + sizeof(unsigned) * (size_t)(ntiles + 1));
     fz3 = fused_.as<unsigned>();
     fw = reinterpret_cast<unsigned long long*>(fz3 + 4);
-    check(cudaMemsetAsync(fused_.p, 0, 64 + sizeof(unsigned) * (size_t)(ntiles + 1), zs), "memset");
   }
-  if (zs != st) check(cudaEventRecord(in_ev_, zs), "event");
+  // One prologue launch zeroes the counters (words 0..12), the fused-finalize counters and the
+  // beta-step maxima of the levels the prefill fills, and copies the staged frequencies.
+  {
+    if (mixed) reserve_mixed(Lpre);
+    else reserve_levels(Lpre);
+    const int filled = mixed ? mrec_filled_ : lev_filled_;
+    ZeroRange z0{cnt, 13}, z1{fz3, fused ? 16 + (ntiles + 1) : 0}, z2{nullptr, 0};
+    if (Lpre > filled) {
+      if (mixed) {
+        const int Lb = filled < 0 ? 0 : filled + 1;
+        z2 = ZeroRange{mrec_bd_.as<unsigned>() + 2 * Lb, 2 * (int64_t)(Lpre - Lb + 1)};
+      } else if (filled < 0) {
+        z2 = ZeroRange{bd_bits_.as<unsigned>(), 64};
+      }
+    }
+    const int64_t n_om = omega_staged_;
+    const int64_t words = std::max<int64_t>(std::max<int64_t>(z0.words, z1.words), std::max<int64_t>(z2.words, n_om));
+    const int blocks = (int)std::min<int64_t>((words + 255) / 256, 148);
+    k_request_prologue<<<blocks, 256, 0, st>>>(z0, z1, z2, stage_host_, omega_.as<double>(), n_om);
+    check(cudaGetLastError(), "request prologue");
+    ++last_launches;
+    if (n_om > 0) {  // the staging buffer is free again once the prologue has run
+      check(cudaEventRecord(stage_ev_, st), "event");
+      omega_staged_ = 0;
+    }
+  }
+  prefill(mixed, Lfirst, Lpre, true);
 
-  const double* d_obs = obs_.as<double>();
-  const double* d_nrm = rq.normals ? nrm_.as<double>() : nullptr;
+  const double* d_obs = req_obs_;
+  const double* d_nrm = rq.normals ? req_nrm_ : nullptr;
   double pol[6];
   bool project = false;
   double c0 = 0, c2 = 0, scale = 0;
@@ -548,8 +588,11 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   int cur_list = 0;
   auto launch_wave = [&](int L) {
     const bool first = L == Lfirst;
-    if (first) wait_inputs(st);  // observers and frequencies from the host
-    else join_prefill();         // the levels filled on the side stream
+    // observers and frequencies from the host (the first wave may read mapped observers in place)
+    const double* wobs = first && first_obs_ ? first_obs_ : d_obs;
+    const double* wnrm = first && first_obs_ ? (rq.normals ? first_nrm_ : nullptr) : d_nrm;
+    if (wobs == d_obs) wait_inputs(st);
+    if (!first) join_prefill();  // the levels filled on the side stream
     const int wv = L - Lfirst;
     const int* act_in = first ? nullptr : act_[cur_list].as<int>();
     const unsigned* nact_in = first ? nullptr : (fused ? fz3 + wv % 3 : cnt + cur_list);
@@ -558,7 +601,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     if (fused && rq.power_density) {
       PdWaveArgs w{};
       w.lev = reinterpret_cast<const double*>(mrec_.p);
-      w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
+      w.cap = lev_cap_; w.obs = wobs; w.normals = wnrm; w.has_normal = wnrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = fw + wv % 2;
@@ -586,7 +629,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     if (fused) {
       FdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
-      w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
+      w.cap = lev_cap_; w.obs = wobs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = fw + wv % 2;
@@ -616,7 +659,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     if (!rq.power_density) {
       FdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
-      w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
+      w.cap = lev_cap_; w.obs = wobs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = c64 + 2;
@@ -638,7 +681,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     } else {
       PdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
-      w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
+      w.cap = lev_cap_; w.obs = wobs; w.normals = wnrm; w.has_normal = wnrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = c64 + 2;
@@ -690,6 +733,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     launch_wave(L);
   }
   join_prefill();
+  wait_inputs(st);  // no upload into the request's buffers stays in flight past the request
   if (!finished) {
     const int slot = claim_stat_slot();
     k_stats_out<<<1, 1, 0, st>>>(c64, cnt_.as<unsigned>() + kCntErr, stats_host_ + kStatWords * slot);
@@ -955,43 +999,58 @@ void Engine::radiation(RadRequest& rq) {
   const int64_t N = rq.n_obs * n_e;
   if (N <= 0) return;
   if (N > 2147483647ll) throw Error{OSC_ERR_LENGTH, "more than 2^31-1 (observer, energy) entries in one call"};
-  // inputs: host buffers go up on copy_ (after the work already on the request stream, which may still
-  // read the previous request's inputs), concurrently with the level samples the request stream
-  // builds; the first wave waits for them (wait_inputs)
-  const cudaMemcpyKind in_kind = rq.obs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  cudaStream_t in_st = st;
-  if (!rq.obs_on_device) {
+  // Inputs.  Device observers (and normals) are read where they are.  Host ones go up on copy_ (after
+  // the work already on the request stream, which may still read the previous request's uploads),
+  // concurrently with the level samples the request stream builds; the waves wait for them
+  // (wait_inputs), except that page-locked observers mapped into this device's address space are
+  // read in place by the first wave.  Up to kStageDoubles frequencies are staged in mapped
+  // page-locked memory for the request prologue to copy; more go up directly.
+  const int np = rq.opts.nparticles;
+  const double* map_obs = nullptr;
+  const double* map_nrm = nullptr;
+  if (rq.obs_on_device) {
+    req_obs_ = rq.obs;
+    req_nrm_ = rq.normals;
+  } else {
+    if (np <= 0) {
+      map_obs = static_cast<const double*>(mapped_host_pointer(const_cast<double*>(rq.obs)));
+      if (map_obs && rq.normals) {
+        map_nrm = static_cast<const double*>(mapped_host_pointer(const_cast<double*>(rq.normals)));
+        if (!map_nrm) map_obs = nullptr;
+      }
+    }
     check(cudaEventRecord(in_fork_ev_, st), "event");
     check(cudaStreamWaitEvent(copy_, in_fork_ev_, 0), "stream wait");
-    in_st = copy_;
+    obs_.reserve(sizeof(double) * 3 * rq.n_obs);
+    check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, cudaMemcpyHostToDevice, copy_), "obs");
+    if (rq.normals) {
+      nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
+      check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, cudaMemcpyHostToDevice, copy_),
+            "normals");
+    }
+    check(cudaEventRecord(in_ev_, copy_), "event");
+    inputs_pending_ = true;
+    req_obs_ = obs_.as<double>();
+    req_nrm_ = rq.normals ? nrm_.as<double>() : nullptr;
   }
-  obs_.reserve(sizeof(double) * 3 * rq.n_obs);
-  check(cudaMemcpyAsync(obs_.p, rq.obs, sizeof(double) * 3 * rq.n_obs, in_kind, in_st), "obs");
-  if (rq.normals) {
-    nrm_.reserve(sizeof(double) * 3 * rq.n_obs);
-    check(cudaMemcpyAsync(nrm_.p, rq.normals, sizeof(double) * 3 * rq.n_obs, in_kind, in_st), "normals");
-  }
+  omega_staged_ = 0;
   if (!rq.power_density) {
     omega_.reserve(sizeof(double) * n_e);
-    if (n_e <= kStageDoubles) {  // small vectors go through pinned memory so the copy stays asynchronous
+    if (n_e <= kStageDoubles) {
       check(cudaEventSynchronize(stage_ev_), "stage");
       std::memcpy(stage_host_, rq.omega.data(), sizeof(double) * n_e);
-      check(cudaMemcpyAsync(omega_.p, stage_host_, sizeof(double) * n_e, cudaMemcpyHostToDevice, in_st), "omega");
-      check(cudaEventRecord(stage_ev_, in_st), "event");
+      omega_staged_ = n_e;
     } else {
-      check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, in_st), "omega");
+      check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
     }
   }
-  if (in_st != st) {
-    check(cudaEventRecord(in_ev_, in_st), "event");
-    inputs_pending_ = true;
-  }
+  first_obs_ = map_obs;
+  first_nrm_ = map_nrm;
   out_.reserve(sizeof(double) * N);
   lvl_.reserve(sizeof(int32_t) * N);
   double* d_out = rq.out_on_device ? rq.out : out_.as<double>();
   int32_t* d_lvl = rq.out_on_device ? rq.level_out : lvl_.as<int32_t>();
   if (!d_lvl) d_lvl = lvl_.as<int32_t>();
-  const int np = rq.opts.nparticles;
   // Host outputs in page-locked memory mapped into this device's address space are written by the
   // kernels themselves (one plain store per entry as it finishes), so no download follows the last
   // wave; pageable outputs are downloaded.
@@ -1028,9 +1087,11 @@ void Engine::radiation(RadRequest& rq) {
       run_single(rq, N, 1.0, d_out, d_lvl, st);
     } catch (...) {
       tail_ = ResultTail{};
+      first_obs_ = first_nrm_ = nullptr;
       throw;
     }
     tail_.active = false;
+    first_obs_ = first_nrm_ = nullptr;
   } else {
     // src/OSCARSSR.cc:4026-4062: new random particle, its trajectory, weight 1/N, compensated sum
     const double weight = 1.0 / (double)np;

@@ -203,7 +203,7 @@ class Engine {
   MixedFrame frame_{};
   void ensure_mixed(int L);
   void reserve_mixed(int L);
-  void fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s);
+  void fill_mixed(int64_t s_begin, int64_t s_end, cudaStream_t s, bool zero_bd = true);
   void compute_frame();
  public:
   int forced_variant[5] = {-1, -1, -1, -1, -1};  // >= 0: use this compiled variant, -1: autotune per shape
@@ -249,7 +249,8 @@ class Engine {
   void ensure_levels(int L);
   void reserve_levels(int L);
   void fill_levels(int64_t s_begin, int64_t s_end, cudaStream_t s);
-  void prefill(bool mixed, int Lhead, int Lpre);
+  // bd_zeroed: the request prologue has zeroed the beta-step words of the levels to fill
+  void prefill(bool mixed, int Lhead, int Lpre, bool bd_zeroed = false);
   void join_prefill();
   std::vector<PinnedStage> pin_pool_;  // trajectory staging of multi-particle requests
   // STL request buffers: facet geometry (A, B - A, C - A), centres, normals, per-facet state and flags
@@ -264,6 +265,13 @@ class Engine {
   cudaStream_t copy_ = nullptr;
   cudaEvent_t in_fork_ev_ = nullptr, in_ev_ = nullptr;
   bool inputs_pending_ = false;
+  const double* first_obs_ = nullptr;  // mapped page-locked observers the first wave reads in place
+  const double* first_nrm_ = nullptr;
+  // observers / normals the waves read: the caller's device buffers, or their uploads
+  const double* req_obs_ = nullptr;
+  const double* req_nrm_ = nullptr;
+  // frequencies staged in mapped page-locked memory (stage_host_) for the request prologue to copy
+  int64_t omega_staged_ = 0;
   void wait_inputs(cudaStream_t st);
   // Result downloads of a single-particle request with pageable host outputs, enqueued by run_single
   // right behind its statistics -- ahead of the host's last poll, so the copies need no extra round

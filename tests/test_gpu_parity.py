@@ -104,10 +104,10 @@ def test_device_entry_point_matches_host_entry_point():
 @pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("power_density", [False, True])
 def test_pinned_host_outputs_match_pageable_outputs(mode, power_density):
-    """Host outputs in page-locked memory are written by the kernels directly; pageable ones are
-    downloaded after the last wave.  Both, with page-locked or pageable observers, give the same
-    values and levels, and the same as device outputs; repeated calls of one request shape (whose
-    later calls enqueue their waves without a host round trip) too."""
+    """Host outputs in page-locked memory are written by the kernels directly, and page-locked
+    observers (and normals) are read in place by the first wave; pageable ones are copied.  Every
+    combination gives the same values and levels, and the same as device buffers; repeated calls
+    of one request shape (whose later calls enqueue their waves without a host round trip) too."""
     import ctypes
     import torch
     from oscars_b200 import _lib
@@ -121,9 +121,13 @@ def test_pinned_host_outputs_match_pageable_outputs(mode, power_density):
     o.horizontal[:] = [1, 0, 0]
     o.propagation[:] = [0, 0, 1]
 
+    nrm = np.ascontiguousarray(np.tile([0.0, 0.0, 1.0], (n, 1)))
+    pin_nrm_t = torch.from_numpy(nrm.copy()).pin_memory()
+
     def call(obs, out, lvl):
-        if power_density:
-            s._ctx.call("osc_power_density", _lib.dptr(obs), None, n, 0, ctypes.byref(o), _lib.dptr(out),
+        if power_density:  # normals page-locked with page-locked observers
+            nv = pin_nrm_t.numpy() if obs is not xyz else nrm
+            s._ctx.call("osc_power_density", _lib.dptr(obs), _lib.dptr(nv), n, 0, ctypes.byref(o), _lib.dptr(out),
                         _lib.i32ptr(lvl), None)
         else:
             s._ctx.call("osc_flux", _lib.dptr(obs), n, E1_U, ctypes.byref(o), _lib.dptr(out), _lib.i32ptr(lvl), None)
