@@ -248,7 +248,11 @@ OSC_API int osc_surface_points(long long n, const double* points, const double* 
  * osc_spectrum      replaces OSCARSSR_Cuda_CalculateSpectrumGPU     (src/OSCARSSR_Cuda.cu:1607)
  * osc_power_density replaces OSCARSSR_Cuda_CalculatePowerDensityGPU (src/OSCARSSR_Cuda.cu:2678)
  * out[i] is the value selected by opts->quantity; level_out (may be NULL) gets the stop level,
- * -1 for entries that did not converge; *n_not_converged (may be NULL) counts those. */
+ * -1 for entries that did not converge; *n_not_converged (may be NULL) counts those.
+ * Any host buffers are accepted.  Page-locked ones (cudaHostAlloc / cudaHostRegister) mapped into
+ * the context device's address space are used in place for single-particle requests: the kernels
+ * store out / level_out there as entries finish (no download after the last wave) and the first
+ * wave reads the observers there; pageable buffers are copied. */
 OSC_API int osc_flux(osc_ctx* ctx, const double* obs_xyz, long long n_obs, double energy_eV,
                      const osc_rad_opts* opts, double* out, int32_t* level_out,
                      long long* n_not_converged);
@@ -356,7 +360,8 @@ OSC_API int osc_flux_vjp(osc_ctx* ctx, const double* obs_xyz, long long n_obs, c
 
 /* ---- device-resident variants: same arithmetic, pointers are device memory on the context's
  *      device, work is queued on `stream` (a cudaStream_t, NULL = the context's stream) and the
- *      call returns without synchronising.  Single particle (opts->nparticles must be 0). */
+ *      call returns without synchronising.  Single particle (opts->nparticles must be 0).  The
+ *      queued work reads the inputs in place: keep them unchanged until it has run. */
 OSC_API int osc_flux_device(osc_ctx* ctx, const double* d_obs_xyz, long long n_obs,
                             double energy_eV, const osc_rad_opts* opts, double* d_out,
                             int32_t* d_level, void* stream);
