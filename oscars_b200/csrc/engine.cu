@@ -588,11 +588,8 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
   int cur_list = 0;
   auto launch_wave = [&](int L) {
     const bool first = L == Lfirst;
-    // observers and frequencies from the host (the first wave may read mapped observers in place)
-    const double* wobs = first && first_obs_ ? first_obs_ : d_obs;
-    const double* wnrm = first && first_obs_ ? (rq.normals ? first_nrm_ : nullptr) : d_nrm;
-    if (wobs == d_obs) wait_inputs(st);
-    if (!first) join_prefill();  // the levels filled on the side stream
+    if (first) wait_inputs(st);  // observers from the host
+    else join_prefill();         // the levels filled on the side stream
     const int wv = L - Lfirst;
     const int* act_in = first ? nullptr : act_[cur_list].as<int>();
     const unsigned* nact_in = first ? nullptr : (fused ? fz3 + wv % 3 : cnt + cur_list);
@@ -601,7 +598,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     if (fused && rq.power_density) {
       PdWaveArgs w{};
       w.lev = reinterpret_cast<const double*>(mrec_.p);
-      w.cap = lev_cap_; w.obs = wobs; w.normals = wnrm; w.has_normal = wnrm != nullptr;
+      w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = fw + wv % 2;
@@ -629,7 +626,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     if (fused) {
       FdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
-      w.cap = lev_cap_; w.obs = wobs; w.omega = omega_.as<double>();
+      w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = fw + wv % 2;
@@ -659,7 +656,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     if (!rq.power_density) {
       FdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
-      w.cap = lev_cap_; w.obs = wobs; w.omega = omega_.as<double>();
+      w.cap = lev_cap_; w.obs = d_obs; w.omega = omega_.as<double>();
       w.n_e = (int64_t)rq.omega.size(); w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = c64 + 2;
@@ -681,7 +678,7 @@ void Engine::run_single(const RadRequest& rq, int64_t n_items, double weight, do
     } else {
       PdWaveArgs w{};
       w.lev = mixed ? reinterpret_cast<const double*>(mrec_.p) : lev_.as<double>();
-      w.cap = lev_cap_; w.obs = wobs; w.normals = wnrm; w.has_normal = wnrm != nullptr;
+      w.cap = lev_cap_; w.obs = d_obs; w.normals = d_nrm; w.has_normal = d_nrm != nullptr;
       w.directional = rq.directional; w.n_items = N; w.act = act_in; w.n_act = nact_in;
       w.first = first; w.level = L; w.tile_entries = tile; w.min_span = min_span; w.target_units = target;
       w.part = part_.as<double>(); w.err = cnt + kCntErr; w.work = c64 + 2;
@@ -1001,24 +998,15 @@ void Engine::radiation(RadRequest& rq) {
   if (N > 2147483647ll) throw Error{OSC_ERR_LENGTH, "more than 2^31-1 (observer, energy) entries in one call"};
   // Inputs.  Device observers (and normals) are read where they are.  Host ones go up on copy_ (after
   // the work already on the request stream, which may still read the previous request's uploads),
-  // concurrently with the level samples the request stream builds; the waves wait for them
-  // (wait_inputs), except that page-locked observers mapped into this device's address space are
-  // read in place by the first wave.  Up to kStageDoubles frequencies are staged in mapped
+  // concurrently with the level samples the request stream builds; the first wave waits for them
+  // (wait_inputs).  (Reading page-locked observers in place over PCIe instead made the first wave
+  // slower than the upload it saves.)  Up to kStageDoubles frequencies are staged in mapped
   // page-locked memory for the request prologue to copy; more go up directly.
   const int np = rq.opts.nparticles;
-  const double* map_obs = nullptr;
-  const double* map_nrm = nullptr;
   if (rq.obs_on_device) {
     req_obs_ = rq.obs;
     req_nrm_ = rq.normals;
   } else {
-    if (np <= 0) {
-      map_obs = static_cast<const double*>(mapped_host_pointer(const_cast<double*>(rq.obs)));
-      if (map_obs && rq.normals) {
-        map_nrm = static_cast<const double*>(mapped_host_pointer(const_cast<double*>(rq.normals)));
-        if (!map_nrm) map_obs = nullptr;
-      }
-    }
     check(cudaEventRecord(in_fork_ev_, st), "event");
     check(cudaStreamWaitEvent(copy_, in_fork_ev_, 0), "stream wait");
     obs_.reserve(sizeof(double) * 3 * rq.n_obs);
@@ -1044,8 +1032,6 @@ void Engine::radiation(RadRequest& rq) {
       check(cudaMemcpyAsync(omega_.p, rq.omega.data(), sizeof(double) * n_e, cudaMemcpyHostToDevice, st), "omega");
     }
   }
-  first_obs_ = map_obs;
-  first_nrm_ = map_nrm;
   out_.reserve(sizeof(double) * N);
   lvl_.reserve(sizeof(int32_t) * N);
   double* d_out = rq.out_on_device ? rq.out : out_.as<double>();
@@ -1087,11 +1073,9 @@ void Engine::radiation(RadRequest& rq) {
       run_single(rq, N, 1.0, d_out, d_lvl, st);
     } catch (...) {
       tail_ = ResultTail{};
-      first_obs_ = first_nrm_ = nullptr;
       throw;
     }
     tail_.active = false;
-    first_obs_ = first_nrm_ = nullptr;
   } else {
     // src/OSCARSSR.cc:4026-4062: new random particle, its trajectory, weight 1/N, compensated sum
     const double weight = 1.0 / (double)np;

@@ -265,8 +265,6 @@ class Engine {
   cudaStream_t copy_ = nullptr;
   cudaEvent_t in_fork_ev_ = nullptr, in_ev_ = nullptr;
   bool inputs_pending_ = false;
-  const double* first_obs_ = nullptr;  // mapped page-locked observers the first wave reads in place
-  const double* first_nrm_ = nullptr;
   // observers / normals the waves read: the caller's device buffers, or their uploads
   const double* req_obs_ = nullptr;
   const double* req_nrm_ = nullptr;

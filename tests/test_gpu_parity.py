@@ -104,8 +104,8 @@ def test_device_entry_point_matches_host_entry_point():
 @pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("power_density", [False, True])
 def test_pinned_host_outputs_match_pageable_outputs(mode, power_density):
-    """Host outputs in page-locked memory are written by the kernels directly, and page-locked
-    observers (and normals) are read in place by the first wave; pageable ones are copied.  Every
+    """Host outputs in page-locked memory are written by the kernels directly; pageable ones are
+    downloaded after the last wave.  With page-locked or pageable observers (and normals), every
     combination gives the same values and levels, and the same as device buffers; repeated calls
     of one request shape (whose later calls enqueue their waves without a host round trip) too."""
     import ctypes
