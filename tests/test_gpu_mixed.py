@@ -177,6 +177,51 @@ def test_far_off_axis_observer_is_rejected():
         s.calculate_spectrum(obs=[3, 0, 30], energy_range_eV=[100, 200], npoints=3, compute="mixed")
 
 
+def test_refusal_reported_once_through_every_entry_point():
+    """The device entry queues its work and returns: a refused observer is reported by the next
+    osc_last_stats, once (the error word is cleared), and the next valid request runs; the host
+    entry with page-locked or pageable buffers reports it from the call itself."""
+    import ctypes
+    import torch
+    from oscars_b200 import _lib
+    from oscars_b200._lib import RadOpts
+    s = _sr()
+    run_case(s, UND_SETUP)
+    o = RadOpts(precision=0.01, max_level=-2, max_level_extended=0, nparticles=0, quantity=0, precision_mode=1)
+    o.horizontal[:] = [1, 0, 0]
+    o.propagation[:] = [0, 0, 1]
+    bad = np.array([[3.0, 0.0, 30.0], [0.0, 0.0, 30.0]])
+    good = np.array([[0.0, 0.0, 30.0], [1e-4, 0.0, 30.0]])
+    d_out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    d_lvl = torch.zeros(2, dtype=torch.int32, device="cuda")
+    sm = ctypes.c_longlong()
+
+    def dev_call(obs):
+        d_obs = torch.tensor(obs, device="cuda")
+        s._ctx.call("osc_flux_device", ctypes.c_void_p(d_obs.data_ptr()), 2, E1_U, ctypes.byref(o),
+                    ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(d_lvl.data_ptr()), None)
+        torch.cuda.synchronize()
+
+    dev_call(bad)
+    with pytest.raises(ValueError, match="compute='mixed' needs observers near the beam axis"):
+        s._ctx.call("osc_last_stats", ctypes.byref(sm), None)
+    s._ctx.call("osc_last_stats", ctypes.byref(sm), None)  # reported once
+    dev_call(good)
+    s._ctx.call("osc_last_stats", ctypes.byref(sm), None)
+    assert sm.value > 0 and np.all(d_out.cpu().numpy() > 0)
+    for pinned in (True, False):
+        obs = torch.from_numpy(bad.copy())
+        out = torch.zeros(2, dtype=torch.float64)
+        if pinned:
+            obs, out = obs.pin_memory(), out.pin_memory()
+        with pytest.raises(ValueError, match="compute='mixed' needs observers near the beam axis"):
+            s._ctx.call("osc_flux", _lib.dptr(obs.numpy()), 2, E1_U, ctypes.byref(o), _lib.dptr(out.numpy()), None,
+                        None)
+    ok = np.zeros(2)
+    s._ctx.call("osc_flux", _lib.dptr(np.ascontiguousarray(good)), 2, E1_U, ctypes.byref(o), _lib.dptr(ok), None, None)
+    assert np.allclose(ok, d_out.cpu().numpy(), rtol=0, atol=0)
+
+
 def _variants(kind):
     import ctypes
     s = _sr()
