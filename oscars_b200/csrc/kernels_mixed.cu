@@ -25,21 +25,28 @@ struct PairStage {
 // sample): the level time (levels above ext_from are extended levels, see level_time), the spline values
 // (include/TOMATH.h:92-121, bit-identical to the FP64 level cache), the particle frame and the record.
 // Sample 0 is the zero-amplitude record at the position and time of sample 1.  The two samples of a
-// pair sit in adjacent lanes (s_begin and the block size are even) and exchange their FP64 values
+// pair sit in adjacent lanes (s_begin and the samples per warp are even) and exchange their FP64 values
 // for the pair's step, so every lane of the grid's last warp takes part (past s_end on a clamped
 // sample, writing nothing).  Also folds, per level, the largest |beta_i - beta_{i-1}| over its
 // samples i >= 1 into bd_bits (the power-density stop rule, src/OSCARSSR.cc:2887-2891; the FP64 values
-// and operations of k_level_betadiff): the predecessor's beta comes from the lane before, or, in
-// lane 0, from the spline at its time.
+// and operations of k_level_betadiff): the predecessor's beta comes from the lane before (lanes 0
+// and 1 of every warp evaluate the warp's two predecessors).
+constexpr int kRecWarpSamples = 30;  // samples per warp of k_mixed_records (32 lanes, 2 of them a halo)
 __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, double tstart, double tstop,
                                 int64_t s_begin, int64_t s_end, int ext_from, MixedFrame F,
                                 float* __restrict__ rec, unsigned long long* __restrict__ bd_bits) {
   __shared__ unsigned long long blk[32];  // per-level maxima of this block
   if (threadIdx.x < 32) blk[threadIdx.x] = 0;
   __syncthreads();
-  const int64_t s_raw = s_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = s_raw < s_end;
-  const int64_t s = active ? s_raw : s_end - 2 + (s_raw & 1);
+  // Each warp holds kRecWarpSamples samples in lanes 2..31 and their two predecessors in lanes 0..1
+  // (a halo: evaluated, not written), so every sample finds the one before it in the lane before and
+  // lane pairs stay (even, odd) samples.
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t s_raw = s_begin + gw * kRecWarpSamples + lane - 2;
+  const bool active = lane >= 2 && s_raw < s_end;
+  // halo lanes before sample 0 and lanes past the end evaluate a valid sample of the same parity
+  const int64_t s = s_raw < 0 ? s_raw + 4 : (s_raw < s_end ? s_raw : s_end - 2 + (s_raw & 1));
   const double t = level_time(tstart, tstop, s == 0 ? 1 : s, ext_from);
   double v[9];
   spline_eval9(knots, n, t, v);
@@ -63,11 +70,6 @@ __global__ void k_mixed_records(const double* __restrict__ knots, int64_t n, dou
   double pbx = __shfl_up_sync(full, v[3], 1), pby = __shfl_up_sync(full, v[4], 1), pbz = __shfl_up_sync(full, v[5], 1);
   const int L = 63 - __clzll((unsigned long long)(s == 0 ? 1 : s));
   const bool step = active && s >= 1 && s - ((int64_t)1 << L) > 0;
-  if (step && (threadIdx.x & 31) == 0) {  // the predecessor belongs to the previous warp
-    double w[9];
-    spline_eval9(knots, n, level_time(tstart, tstop, s - 1, ext_from), w);
-    pbx = w[3]; pby = w[4]; pbz = w[5];
-  }
   if (step && bd_bits) {
     const double dx = __dsub_rn(v[3], pbx), dy = __dsub_rn(v[4], pby), dz = __dsub_rn(v[5], pbz);
     const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
@@ -428,7 +430,8 @@ cudaError_t launch_mixed_records(const double* knots, int64_t n, double tstart, 
                                  unsigned long long* bd_bits, cudaStream_t st) {
   if (s_end <= s_begin) return cudaSuccess;
   const int T = 128;
-  const unsigned grid = (unsigned)((s_end - s_begin + T - 1) / T);
+  const int64_t warps = (s_end - s_begin + dev::kRecWarpSamples - 1) / dev::kRecWarpSamples;
+  const unsigned grid = (unsigned)((warps * 32 + T - 1) / T);
   dev::k_mixed_records<<<grid, T, 0, st>>>(knots, n, tstart, tstop, s_begin, s_end, ext_from, F,
                                             reinterpret_cast<float*>(rec), bd_bits);
   return cudaGetLastError();
