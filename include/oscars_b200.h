@@ -249,10 +249,8 @@ OSC_API int osc_surface_points(long long n, const double* points, const double* 
  * osc_power_density replaces OSCARSSR_Cuda_CalculatePowerDensityGPU (src/OSCARSSR_Cuda.cu:2678)
  * out[i] is the value selected by opts->quantity; level_out (may be NULL) gets the stop level,
  * -1 for entries that did not converge; *n_not_converged (may be NULL) counts those.
- * Any host buffers are accepted.  Page-locked outputs (cudaHostAlloc / cudaHostRegister) mapped into
- * the context device's address space are written in place for single-particle requests: the kernels
- * store out / level_out there as entries finish, with no download after the last wave.  Inputs are
- * uploaded, and pageable outputs downloaded. */
+ * Any host buffers are accepted; page-locked ones (cudaHostAlloc / cudaHostRegister) make the
+ * upload of the inputs and the download of the results faster. */
 OSC_API int osc_flux(osc_ctx* ctx, const double* obs_xyz, long long n_obs, double energy_eV,
                      const osc_rad_opts* opts, double* out, int32_t* level_out,
                      long long* n_not_converged);

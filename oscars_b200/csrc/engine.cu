@@ -746,9 +746,8 @@ int Engine::claim_stat_slot() {
 }
 
 // The statistics of the request just enqueued, stored into ring slot `slot` by the last kernel on
-// the stream, are read by collect() when asked (after the slot's event); a
-// single-particle request with host outputs that the kernels cannot write then enqueues its result
-// downloads.
+// the stream, are read by collect() when asked (after the slot's event); a single-particle request
+// with host outputs then enqueues its result downloads.
 void Engine::finish_request(int slot, cudaStream_t st) {
   check(cudaEventRecord(stats_ev_[slot], st), "event");
   pending_.push_back(slot);
@@ -972,17 +971,6 @@ void Engine::report_wait(unsigned seq, unsigned* va, unsigned* vb, cudaStream_t 
   *vb = w[2];
 }
 
-// The device address of page-locked host memory mapped for the current device, or NULL (pageable
-// memory, or not mapped here).
-static void* mapped_host_pointer(void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();  // clear the error of an unknown pointer
-    return nullptr;
-  }
-  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
-}
-
 void Engine::radiation(RadRequest& rq) {
   if (device < 0) throw Error{OSC_ERR_NO_DEVICE, "this context was created without a GPU (device -1)"};
   check(cudaSetDevice(device), "cudaSetDevice");
@@ -1037,19 +1025,9 @@ void Engine::radiation(RadRequest& rq) {
   double* d_out = rq.out_on_device ? rq.out : out_.as<double>();
   int32_t* d_lvl = rq.out_on_device ? rq.level_out : lvl_.as<int32_t>();
   if (!d_lvl) d_lvl = lvl_.as<int32_t>();
-  // Host outputs in page-locked memory mapped into this device's address space are written by the
-  // kernels themselves (one plain store per entry as it finishes), so no download follows the last
-  // wave; pageable outputs are downloaded.
-  bool direct_out = false;
-  if (!rq.out_on_device && np <= 0) {
-    void* mo = mapped_host_pointer(rq.out);
-    void* ml = rq.level_out ? mapped_host_pointer(rq.level_out) : nullptr;
-    if (mo && (ml || !rq.level_out)) {
-      d_out = static_cast<double*>(mo);
-      if (ml) d_lvl = static_cast<int32_t*>(ml);
-      direct_out = true;
-    }
-  }
+  // Host outputs are downloaded by the copy engine right behind the last report (ResultTail).
+  // (Kernel stores straight into mapped page-locked outputs were measured too: a few microseconds
+  // faster on one box and tens slower on another, so the copies are kept.)
 
   // Mixed multi-particle flux / spectrum requests with at least beam_batch_min particles (this
   // process's share) run as one batch with device RK4 trajectories; smaller ones, and those with RKAS
@@ -1068,7 +1046,7 @@ void Engine::radiation(RadRequest& rq) {
     model.ensure_trajectory();
     upload_trajectory();
     tail_ = ResultTail{};
-    if (!rq.out_on_device && !direct_out) tail_ = ResultTail{true, false, d_out, d_lvl, rq.out, rq.level_out, N};
+    if (!rq.out_on_device) tail_ = ResultTail{true, false, d_out, d_lvl, rq.out, rq.level_out, N};
     try {
       run_single(rq, N, 1.0, d_out, d_lvl, st);
     } catch (...) {
@@ -1114,7 +1092,7 @@ void Engine::radiation(RadRequest& rq) {
     check(cudaMemcpyAsync(d_out, acc_.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "result");
   }
   if (!rq.out_on_device) {
-    if (!tail_.emitted && !direct_out) {  // (run_single enqueues them itself for one particle)
+    if (!tail_.emitted) {  // (run_single enqueues them itself for one particle)
       check(cudaMemcpyAsync(rq.out, d_out, sizeof(double) * N, cudaMemcpyDeviceToHost, st), "download");
       if (rq.level_out)
         check(cudaMemcpyAsync(rq.level_out, d_lvl, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, st), "download");

@@ -271,9 +271,8 @@ class Engine {
   // frequencies staged in mapped page-locked memory (stage_host_) for the request prologue to copy
   int64_t omega_staged_ = 0;
   void wait_inputs(cudaStream_t st);
-  // Result downloads of a single-particle request with pageable host outputs, enqueued by run_single
-  // right behind its statistics -- ahead of the host's last poll, so the copies need no extra round
-  // trip.
+  // Result downloads of a single-particle request with host outputs, enqueued by run_single right
+  // behind its statistics -- ahead of the host's last poll, so the copies need no extra round trip.
   struct ResultTail {
     bool active = false, emitted = false;
     const double* d_out = nullptr;

@@ -104,10 +104,9 @@ def test_device_entry_point_matches_host_entry_point():
 @pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("power_density", [False, True])
 def test_pinned_host_outputs_match_pageable_outputs(mode, power_density):
-    """Host outputs in page-locked memory are written by the kernels directly; pageable ones are
-    downloaded after the last wave.  With page-locked or pageable observers (and normals), every
-    combination gives the same values and levels, and the same as device buffers; repeated calls
-    of one request shape (whose later calls enqueue their waves without a host round trip) too."""
+    """Page-locked and pageable host buffers (observers, normals, outputs) give the same values and
+    levels, and the same as device buffers; so do repeated calls of one request shape, whose later
+    calls enqueue their waves and result downloads without a host round trip."""
     import ctypes
     import torch
     from oscars_b200 import _lib
